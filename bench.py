@@ -1,0 +1,412 @@
+"""Throughput of the LatticeQM k-space hot path, H(k) + eigh + rho_R, on B200.
+
+One step = the batched three-model workload: for each of square 2x2 (n=8),
+kagome 2x2 (n=24) and triangular 4x4 with spin-orbit phases (n=96), a 256x256
+k-grid per GPU processed through ``lqm_bands_dos_rho_dev``: Bloch sum,
+FP64 Hermitian eigendecomposition with vectors, rho_L for the 9 keys of H
+(mu = 0, T = 0.01), DOS (500 points, Gamma = 0.05) and the bands.  Seeded
+synthetic models (no dataset exists for this path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+Prints one JSON line on rank 0.  ``value`` is the device-resident throughput
+(inputs on the device before the timed region); ``e2e`` is the same step
+through the host-pointer C-ABI with host<->device copies inside the timing.
+"""
+import argparse
+import ctypes
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_PY = os.path.join(ROOT, "latticeqm.jl_b200", "python")
+for _p in (ROOT, PKG_PY):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "k-pts/s H(k)+eigh+rho_R (FP64 plain; batched square/kagome/triangular)"
+NK_LIN = 256
+NW = 500
+GAMMA = 0.05
+MU, TEMP = 0.0, 0.01
+WORKLOAD = ("batch3: square2x2 (n=8) + kagome2x2 (n=24) + triangular4x4 3-site SOC (n=96), "
+            "256x256 k-grid each per GPU; bands + DOS(500, Gamma=0.05) + rho_R (9 keys, mu=0, T=0.01)")
+CPU_SAMPLE_PER_CORE = {8: 3072, 24: 1536, 96: 288}  # host k-points per model and core (~8 s per sample)
+
+
+def flops_per_k(n, nR, nL):
+    """Algorithmic real flops per k: H(k) build, eigh with vectors, rho_k, Fourier fold."""
+    return 8.0 * nR * n * n + (16.0 / 3.0 + 8.0) * n ** 3 + 4.0 * n ** 3 + 8.0 * nL * n * n
+
+
+def eigh_flops_per_k(n, nR):
+    return 8.0 * nR * n * n + (16.0 / 3.0 + 8.0) * n ** 3
+
+
+def kgrid(rank, world):
+    """Rank r's 256x256 slice of a (256*world) x 256 grid (first index fastest)."""
+    import numpy as np
+    n1 = NK_LIN * world
+    i = np.arange(NK_LIN) * world + rank
+    kx = np.tile(i / n1, NK_LIN)
+    ky = np.repeat(np.arange(NK_LIN) / NK_LIN, NK_LIN)
+    return np.asfortranarray(np.vstack([kx, ky]))
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def _cpu_worker(args):
+    """Oracle per-k work on a chunk (one BLAS thread): H(k), zheevr with vectors, rho_k,
+    Fourier fold into rho_L, band energy, DOS contribution."""
+    import numpy as np
+    from oracle import kspace as K
+    h, ks, omegas = args
+    keys = list(h.keys())
+    n = next(iter(h.values())).shape[0]
+    rho = np.zeros((len(keys), n, n), complex)
+    dos = np.zeros(len(omegas))
+    eb = 0.0
+    w = 1.0 / ks.shape[1]
+    for j in range(ks.shape[1]):
+        k = ks[:, j]
+        e, U = K.eigh_upper(K.fouriersum(h, k), True)
+        f = K.fermidirac(e, MU, TEMP)
+        rk = (U * f) @ U.conj().T
+        for li, Lk in enumerate(keys):
+            rho[li] += w * np.exp(-2j * math.pi * float(np.dot(k, Lk))) * rk
+        eb += w * float(np.sum(e * f))
+        dos += np.sum(GAMMA / ((omegas[:, None] - e[None, :]) ** 2 + GAMMA ** 2), axis=1)
+    return ks.shape[1]
+
+
+def cpu_time_per_k(models, pool, cores):
+    """Seconds per k-point per model on `cores` host processes (bounded sample)."""
+    import numpy as np
+    out = {}
+    for name, h in models:
+        n = next(iter(h.values())).shape[0]
+        ns = CPU_SAMPLE_PER_CORE.get(n, 256) * cores
+        rng = np.random.default_rng(n)
+        ks = rng.random((2, ns))
+        om = np.linspace(-6, 6, NW)
+        chunks = [(h, np.ascontiguousarray(c), om) for c in np.array_split(ks, cores * 4, axis=1) if c.shape[1]]
+        t0 = time.perf_counter()
+        done = sum(pool.map(_cpu_worker, chunks))
+        out[name] = (time.perf_counter() - t0) / done
+    return out
+
+
+def make_pool(cores):
+    import multiprocessing as mp
+    for var in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"
+    return mp.get_context("spawn").Pool(cores)
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference algorithm on the host cores (oracle port of
+    LatticeQM's :multithreaded k-loop, one BLAS thread per worker)."""
+    if rank != 0:
+        return
+    from lqm_workloads import models as M
+    models = M.batch_models()
+    cores = os.cpu_count() or 1
+    pool = make_pool(cores)
+    nk_total = 3 * NK_LIN * NK_LIN
+    for _ in range(args.warmup):
+        cpu_time_per_k(models, pool, cores)
+    vals = []
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        tpk = cpu_time_per_k(models, pool, cores)
+        t_step = sum(NK_LIN * NK_LIN * t for t in tpk.values())
+        vals.append(nk_total / t_step)
+    wall = time.perf_counter() - t_all
+    pool.close()
+    v = statistics.median(vals)
+    sample = ", ".join(f"n={n}: {c * cores} k" for n, c in CPU_SAMPLE_PER_CORE.items())
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "k-pts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * nk_total / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded models)", "config": {"workload": WORKLOAD, "parallelism": f"cpu{cores}"},
+            "cpu_baseline": {"value": v, "unit": "k-pts/s", "cores": cores, "kind": "port",
+                             "sample": f"per step, random k-points per orbital count ({sample}) timed on "
+                                       f"{cores} processes, extrapolated to 3x256x256 k; wall {wall:.1f}s"},
+            "e2e": {"value": v, "unit": "k-pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def measured_fp64_peak(torch, dev):
+    """cuBLAS DGEMM (8192^3) best of 5, TFLOP/s; the FP64 denominator of the roofline."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    return 2 * 8192 ** 3 / best / 1e12
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if args.warmup < 3:
+        args.warmup = 3
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.join(ROOT, "latticeqm.jl_b200"))
+    import build as lqm_build
+    if not os.path.exists(lqm_build.LIB):
+        lqm_build.build()
+    import lqm_cuda as Q
+    from lqm_workloads import models as M
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    models = M.batch_models()
+    ctx = Q.Context(local, timeout=900)
+
+    # ---- device-resident inputs ----
+    ks_np = kgrid(rank, world)
+    nk = ks_np.shape[1]
+    d_ks = torch.from_numpy(np.ascontiguousarray(ks_np.T)).to(dev)   # (nk, 2) row-major == (2, nk) col-major
+    state = []
+    for name, h in models:
+        Hd = Q.DeviceHops(h, ctx)
+        n = Hd.n
+        Lk = np.asfortranarray(np.array(list(h.keys()), dtype=np.int64).T)
+        d_rho = torch.zeros(len(h), n, n, dtype=torch.complex128, device=dev)
+        d_bands = torch.zeros(nk, n, dtype=torch.float64, device=dev)
+        d_dos = torch.zeros(NW, dtype=torch.float64, device=dev)
+        # DOS window [min eps, max eps] of this model, from one bands pass
+        ctx.check(Q.lib().lqm_bandmatrix_dev(ctx.handle, Hd.handle, nk, Q._ptr(d_ks), 0, 0,
+                                              Q._ptr(d_bands), None))
+        lo, hi = float(d_bands.min()), float(d_bands.max())
+        if world > 1:
+            t = torch.tensor([-lo, hi], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            lo, hi = -float(t[0]), float(t[1])
+        d_om = torch.linspace(lo, hi, NW, dtype=torch.float64, device=dev)
+        state.append(dict(name=name, h=h, Hd=Hd, n=n, nR=len(h), Lk=Lk, rho=d_rho, bands=d_bands, dos=d_dos,
+                          om=d_om))
+
+    eb = ctypes.c_double()
+
+    def step(per_model_ms=None):
+        for s in state:
+            if per_model_ms is not None:
+                m0 = ctx.stats()[0]
+            ctx.check(Q.lib().lqm_bands_dos_rho_dev(
+                ctx.handle, s["Hd"].handle, nk, Q._ptr(d_ks), None, MU, TEMP, s["nR"], Q._ptr(s["Lk"]),
+                Q._ptr(s["rho"]), ctypes.byref(eb), NW, Q._ptr(s["om"]), GAMMA, Q._ptr(s["dos"]),
+                Q._ptr(s["bands"]), 0))
+            if per_model_ms is not None:
+                per_model_ms[s["n"]] = per_model_ms.get(s["n"], 0.0) + ctx.stats()[0] - m0
+            if world > 1:  # rho_L and DOS are sums over the whole grid: one exchange per model
+                dist.all_reduce(s["rho"])
+                dist.all_reduce(s["dos"])
+                s["rho"].div_(world)
+                s["dos"].div_(world)
+
+    fp64_peak = measured_fp64_peak(torch, dev)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region (device resident) ----
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    per_model_ms = {}
+    ctx.reset_stats(timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step(per_model_ms)
+    e1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    eigh_ms, eigh_launches, launches = ctx.stats()
+    clocks = sampler.stop()
+    if world > 1:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t[0])
+    total_k = world * len(state) * nk * args.steps
+    value = total_k / elapsed
+
+    # ---- e2e through the host-pointer C-ABI (pinned host buffers) ----
+    ks_pin = torch.from_numpy(np.ascontiguousarray(ks_np.T)).pin_memory()
+    host = []
+    for s in state:
+        host.append(dict(rho=torch.zeros(s["nR"], s["n"], s["n"], dtype=torch.complex128).pin_memory(),
+                         bands=torch.zeros(nk, s["n"], dtype=torch.float64).pin_memory(),
+                         dos=torch.zeros(NW, dtype=torch.float64).pin_memory(),
+                         om=s["om"].cpu().pin_memory()))
+    h2d = d2h = 0
+    for s, hb in zip(state, host):
+        h2d += s["nR"] * s["n"] ** 2 * 16 + s["Lk"].nbytes + ks_pin.numel() * 8 + NW * 8
+        d2h += hb["rho"].numel() * 16 + hb["bands"].numel() * 8 + NW * 8
+
+    def e2e_step():
+        for s, hb in zip(state, host):
+            Hd = Q.DeviceHops(s["h"], ctx)  # H uploaded per call, as a user call does
+            ctx.check(Q.lib().lqm_bands_dos_rho(
+                ctx.handle, Hd.handle, nk, Q._ptr(ks_pin), None, MU, TEMP, s["nR"], Q._ptr(s["Lk"]),
+                Q._ptr(hb["rho"]), ctypes.byref(eb), NW, Q._ptr(hb["om"]), GAMMA, Q._ptr(hb["dos"]),
+                Q._ptr(hb["bands"]), 0))
+            Hd.free()
+
+    e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_el = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_el], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_el = float(t[0])
+    e2e_val = total_k / e2e_el
+
+    # ---- roofline of the dominant kernel (per-k eigensolver) ----
+    eig_flops = args.steps * nk * sum(eigh_flops_per_k(s["n"], s["nR"]) for s in state)
+    achieved = eig_flops / (eigh_ms / 1e3) / 1e12 if eigh_ms > 0 else None
+    detail = {}
+    for s in state:
+        ms = per_model_ms.get(s["n"], 0.0)
+        if ms > 0:
+            detail[f"n{s['n']}"] = {"eigh_ms_per_step": ms / args.steps,
+                                    "eigh_tflops": args.steps * nk * eigh_flops_per_k(s["n"], s["nR"]) / (ms / 1e3)
+                                    / 1e12}
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "eigh_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
+            "kernel": "eigh_kernel (Bloch sum + Householder + divide&conquer + back-transform, one CTA per k)",
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
+            "eigh_launches": eigh_launches, "eigh_ms": eigh_ms, "per_model": detail}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        pool = make_pool(cores)
+        tpk = cpu_time_per_k(models, pool, cores)
+        pool.close()
+        t_step = sum(NK_LIN * NK_LIN * t for t in tpk.values())
+        sample = ", ".join(f"n={n}: {c * cores} k" for n, c in CPU_SAMPLE_PER_CORE.items())
+        cpu = {"value": len(state) * NK_LIN * NK_LIN / t_step, "unit": "k-pts/s", "cores": cores, "kind": "port",
+               "sample": f"random k-points per model ({sample}), oracle per-k zheevr+rho+fold+DOS on {cores} "
+                         f"processes, extrapolated to 3x256x256 k"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "k-pts/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded models)",
+                "config": {"workload": WORKLOAD, "k_points_per_gpu_per_step": len(state) * nk,
+                           "parallelism": f"dp{world} (k-grid shards; rho_R/DOS all-reduce)",
+                           "l2": "inputs larger than L2 (each step streams ~8 GB of U/rho_k through HBM)"},
+                "e2e": {"value": e2e_val, "unit": "k-pts/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

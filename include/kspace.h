@@ -1,0 +1,144 @@
+/*
+ * libkspace — B200 (sm_100a) k-space hot path for LatticeQM.jl, C ABI.
+ *
+ * Reached from Julia as `multimode=:cuda` on the existing k-loop routines.
+ * All array arguments are plain pointers in the caller's memory, laid out as
+ * Julia stores them: column-major, ComplexF64 as interleaved (re, im) double
+ * pairs, lattice keys as Int64 (d entries per key), fractional k-points.
+ * The `_dev` entry points take device pointers instead of host pointers and
+ * perform no host<->device copies of those arrays.
+ *
+ * Every function returns LQM_OK (0) or a negative status; the message of the
+ * last failure is lqm_last_error(ctx).  A context owns one CUDA stream and is
+ * not thread-safe; distinct contexts are independent.  No entry point falls
+ * back to a CPU implementation: a context cannot be created without a
+ * visible CUDA device.
+ *
+ * Reference paths are relative to the LatticeQM.jl source tree.
+ */
+#ifndef LQM_KSPACE_H
+#define LQM_KSPACE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LQM_OK 0
+#define LQM_EINVAL (-1)   /* invalid argument (sizes, NaN/Inf input, non-Hermitian keys) */
+#define LQM_ECUDA (-2)    /* CUDA runtime error, or no usable device */
+#define LQM_ENOMEM (-3)   /* device allocation failed */
+#define LQM_ETIMEOUT (-4) /* a device wait exceeded the context timeout */
+#define LQM_ENOCONV (-5)  /* SCF did not converge and the caller asked for an error */
+#define LQM_EDEVICE (-6)  /* a device-side check failed (e.g. no sign change for mu) */
+
+typedef struct lqm_ctx lqm_ctx;
+typedef struct lqm_hops lqm_hops;
+
+/* Callback once per SCF iteration: mirrors `log_callback(iter, ϵ, residual, info)`
+ * with info = (ϵkin, ϵband, ϵH, ϵF, μ), src/modules/Meanfield/selfconsistent.jl:172-182,296-302.
+ * A non-zero return value stops the iteration. */
+typedef int (*lqm_scf_log_cb)(int64_t iter, double energy, double residual, double ekin, double eband,
+                              double eH, double eF, double mu, void* user);
+
+/* Context: device selection, one stream, workspace.  New entry point (the
+ * reference selects executors in src/modules/Parallel/Parallel.jl:85-109). */
+int lqm_ctx_create(int device, lqm_ctx** out);
+int lqm_ctx_destroy(lqm_ctx* ctx);
+const char* lqm_last_error(const lqm_ctx* ctx);
+/* Host-side wait limit for device work, seconds (default 600). */
+int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
+/* Milliseconds of device time of the last call's kernels (CUDA events). */
+int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
+
+/* Device-time statistics since the last reset (reset also switches event
+ * timing of the eigensolver kernel on or off): eigh_ms / eigh_launches cover
+ * the per-k eigensolver kernel, launches counts every kernel this library
+ * launched. */
+int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing);
+int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches);
+
+/* Upload a dense Hops (src/modules/TightBinding/types.jl:54-60, DenseHops):
+ * keys d x nR (Int64), blocks n x n x nR column-major ComplexF64 in the same
+ * key order.  The key order is the Bloch-sum order (types.jl:18-25). */
+int lqm_hops_upload_dense(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
+                          const double* blocks, lqm_hops** out);
+/* Upload a SparseHops (types.jl:60): per key a Julia SparseMatrixCSC with
+ * 1-based Int64 colptr (n+1) / rowval (nnz) and ComplexF64 nzval (2*nnz doubles). */
+int lqm_hops_upload_csc(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
+                        const int64_t* const* colptr, const int64_t* const* rowval,
+                        const double* const* nzval, lqm_hops** out);
+int lqm_hops_free(lqm_ctx* ctx, lqm_hops* h);
+int lqm_hops_dims(const lqm_hops* h, int64_t* n, int64_t* nR, int32_t* d);
+
+/* Batched Bloch sum H(k) = Σ_R H_R e^{i2πk·R}, replaces `fouriersum!`
+ * (src/modules/TightBinding/types.jl:18-25) over a k list: Hk is n x n x nk. */
+int lqm_bloch(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, double* Hk);
+int lqm_bloch_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_Hk);
+
+/* Bands (and optionally eigenvectors) on a k list, replaces `bandmatrix`
+ * without projectors (src/modules/Spectrum/bands.jl:164-227; per-k eigen of
+ * `Hermitian(H(k))`, upper triangle, src/modules/Eigen/Eigen.jl:22-23,32).
+ * bands: n x nk ascending per column; U: n x n x nk (may be NULL). */
+int lqm_bandmatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int want_vectors,
+                   int precision, double* bands, double* U);
+int lqm_bandmatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, int want_vectors,
+                       int precision, double* d_bands, double* d_U);
+
+/* ρ_L = Σ_k w_k e^{-i2πk·L} U f(ε-μ;T) U^H for the nL given keys and the band
+ * energy Σ_k w_k Σ_n f ε; replaces `getdensitymatrix!` + `densitymatrix_kpoint!`
+ * (src/modules/Operators/densitymatrix.jl:28-49,107-145).  w == NULL means
+ * uniform 1/nk (densitymatrix.jl:17-20).  rho: n x n x nL, overwritten. */
+int lqm_densitymatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
+                      double mu, double T, int64_t nL, const int64_t* Lkeys, double* rho, double* eband,
+                      int precision);
+int lqm_densitymatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks,
+                          const double* d_w, double mu, double T, int64_t nL, const int64_t* Lkeys,
+                          double* d_rho, double* eband, int precision);
+
+/* Chemical potential from the bands of H on a k list, replaces
+ * `chemicalpotential(H, ks, filling; T)` (src/modules/Spectrum/chemicalpotential.jl:6-46,53-66):
+ * T == 0 midpoint of order statistics, T > 0 float bisection of the filling
+ * on [min ε, max ε].  w == NULL: unweighted mean (chemicalpotential.jl:76). */
+int lqm_chemicalpotential(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
+                          double filling, double T, double* mu);
+/* Same on precomputed device bands (n x nk). */
+int lqm_chemicalpotential_bands_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands,
+                                    const double* d_w, double filling, double T, double* mu);
+
+/* Lorentzian DOS, replaces `getdos!`/`dos_compute!` (src/modules/Spectrum/dos.jl:185-188,202-223):
+ * DOS(ω) = Σ_k w_k Σ_n Im[1/(ω - iΓ - ε)], divided by nk when w == NULL. */
+int lqm_dos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, int64_t nw,
+            const double* omegas, double gamma, double* dos);
+int lqm_dos_bands_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w,
+                      int64_t nw, const double* d_omegas, double gamma, double* d_dos);
+
+/* Bands, DOS and ρ_L from ONE eigen pass over the k list: the outputs of
+ * `bandmatrix` + `getdos` + `getdensitymatrix!` on the same H and ks
+ * (src/modules/Spectrum/bands.jl:164-227, src/modules/Spectrum/dos.jl:202-223,
+ * src/modules/Operators/densitymatrix.jl:28-49,130-145), which the reference
+ * computes with three separate k-loops.  w == NULL: uniform 1/nk for ρ and
+ * the unweighted DOS normalisation.  bands: n x nk; rho: n x n x nL; dos: nw. */
+int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, double mu,
+                      double T, int64_t nL, const int64_t* Lkeys, double* rho, double* eband, int64_t nw,
+                      const double* omegas, double gamma, double* dos, double* bands, int precision);
+int lqm_bands_dos_rho_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w,
+                          double mu, double T, int64_t nL, const int64_t* Lkeys, double* d_rho, double* eband,
+                          int64_t nw, const double* d_omegas, double gamma, double* d_dos, double* d_bands,
+                          int precision);
+
+/* Hartree-Fock SCF with linear mixing, device-resident, replaces
+ * `solvehartreefock` (src/modules/Meanfield/selfconsistent.jl:19,256-336,366-381;
+ * functional hartreefock.jl:143-289,392-410; mixing fixedpoint.jl:39-194).
+ * rho_inout: n x n x nL for the keys Lkeys (initial guess in, converged out).
+ * out_scalars[9] = {E_GS, mu, eH, eF, eband, ekin, residual, converged, iterations}. */
+int lqm_scf_hf(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, const double* ks,
+               const double* w, double filling, double T, double beta, double tol, int64_t maxiter,
+               int64_t nL, const int64_t* Lkeys, double* rho_inout, lqm_scf_log_cb cb, void* cb_user,
+               double* out_scalars);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LQM_KSPACE_H */

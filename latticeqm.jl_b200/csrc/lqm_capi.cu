@@ -1,0 +1,721 @@
+// C ABI of libkspace (declared in include/kspace.h).  Host side: argument
+// validation, device buffers, the k-batch loop and kernel launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "kspace.h"
+#include "lqm_kernels.cuh"
+#include "lqm_hf.cuh"
+#include "lqm_plan.h"
+
+using namespace lqm;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct PlanDev {
+  int n = 0;
+  int* d_buf = nullptr;
+  DCPlan plan{};
+};
+
+struct LqmError {
+  int code;
+  std::string msg;
+};
+
+}  // namespace
+
+struct lqm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  double timeout_s = 600.0;
+  int num_sms = 0;
+  double last_ms = 0.0;
+  std::map<int, PlanDev> plans;
+  DevBuf ws[24];
+  // per-kernel device-time statistics (CUDA events on the context stream)
+  bool stats_on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending, ev_pool;
+  double eigh_ms = 0.0;
+  int64_t eigh_launches = 0, launches = 0;
+};
+
+struct lqm_hops {
+  int64_t n = 0, nR = 0;
+  int32_t d = 0;
+  double2* blocks = nullptr;
+  int64_t* keys = nullptr;
+  std::vector<int64_t> hkeys;
+};
+
+namespace {
+
+[[noreturn]] void fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw LqmError{code, buf};
+}
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) fail(LQM_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+    fail(LQM_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+}
+
+template <class F>
+int guarded(lqm_ctx* ctx, F&& f) {
+  if (!ctx) return LQM_EINVAL;
+  try {
+    ctx->err.clear();
+    ck(cudaSetDevice(ctx->device), "cudaSetDevice");
+    f();
+    return LQM_OK;
+  } catch (const LqmError& e) {
+    ctx->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    ctx->err = "host allocation failed";
+    return LQM_ENOMEM;
+  } catch (...) {
+    ctx->err = "unknown error";
+    return LQM_EINVAL;
+  }
+}
+
+void collect_stats(lqm_ctx* ctx) {
+  for (auto& pr : ctx->ev_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) ctx->eigh_ms += ms;
+    ctx->ev_pool.push_back(pr);
+  }
+  ctx->ev_pending.clear();
+}
+
+void wait_stream(lqm_ctx* ctx) {
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(ctx->stream);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) ck(e, "device execution");
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > ctx->timeout_s) fail(LQM_ETIMEOUT, "device work exceeded the %.1f s timeout", ctx->timeout_s);
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  ck(cudaGetLastError(), "kernel launch");
+  collect_stats(ctx);
+}
+
+std::pair<cudaEvent_t, cudaEvent_t> stat_events(lqm_ctx* ctx) {
+  if (!ctx->ev_pool.empty()) {
+    auto pr = ctx->ev_pool.back();
+    ctx->ev_pool.pop_back();
+    return pr;
+  }
+  std::pair<cudaEvent_t, cudaEvent_t> pr;
+  ck(cudaEventCreate(&pr.first), "event");
+  ck(cudaEventCreate(&pr.second), "event");
+  return pr;
+}
+
+void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
+  DevBuf& b = ctx->ws[slot];
+  if (b.bytes < bytes) {
+    if (b.p) { wait_stream(ctx); cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+    size_t want = std::max(bytes, (size_t)256);
+    ck(cudaMalloc(&b.p, want), "cudaMalloc(workspace)");
+    b.bytes = want;
+  }
+  return b.p;
+}
+
+enum WsSlot {
+  WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
+  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2
+};
+
+// ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
+const DCPlan& get_plan(lqm_ctx* ctx, int n) {
+  auto it = ctx->plans.find(n);
+  if (it != ctx->plans.end()) return it->second.plan;
+  const DCPlanHost P = make_dc_plan_host(n);
+  PlanDev pd;
+  pd.n = n;
+  ck(cudaMalloc(&pd.d_buf, P.buf.size() * sizeof(int)), "cudaMalloc(plan)");
+  ck(cudaMemcpy(pd.d_buf, P.buf.data(), P.buf.size() * sizeof(int), cudaMemcpyHostToDevice), "plan upload");
+  pd.plan.nnodes = P.nnodes;
+  pd.plan.nheights = P.nheights;
+  pd.plan.hstart = pd.d_buf + P.off_hstart;
+  pd.plan.lo = pd.d_buf + P.off_lo;
+  pd.plan.mid = pd.d_buf + P.off_mid;
+  pd.plan.hi = pd.d_buf + P.off_hi;
+  pd.plan.owner = pd.d_buf + P.off_own;
+  return ctx->plans.emplace(n, pd).first->second.plan;
+}
+
+void check_finite(const double* x, int64_t m, const char* what) {
+  for (int64_t i = 0; i < m; ++i)
+    if (!std::isfinite(x[i])) fail(LQM_EINVAL, "%s contains a non-finite value at index %lld", what, (long long)i);
+}
+
+void check_hops(const lqm_hops* H) {
+  if (!H || !H->blocks) fail(LQM_EINVAL, "null hops");
+}
+
+int eigh_threads(int n) { return n <= 16 ? 32 : (n <= 32 ? 64 : (n <= 64 ? 128 : 256)); }
+
+void timer_start(lqm_ctx* ctx) { ck(cudaEventRecord(ctx->ev0, ctx->stream), "event"); }
+void timer_stop(lqm_ctx* ctx) {
+  ck(cudaEventRecord(ctx->ev1, ctx->stream), "event");
+}
+void timer_collect(lqm_ctx* ctx) {
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->last_ms = ms;
+}
+
+// Eigen pass over nk device k-points: bands (n x nk) and optionally U.
+void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands, double2* d_U) {
+  const int n = (int)H->n;
+  const DCPlan& plan = get_plan(ctx, n);
+  const int nt = eigh_threads(n);
+  EighSmemLayout Ls = eigh_smem_layout(n, (int)H->nR, 1);
+  int a_in_smem = Ls.total <= 200 * 1024;
+  if (!a_in_smem) Ls = eigh_smem_layout(n, (int)H->nR, 0);
+  if (Ls.total > 227 * 1024) fail(LQM_EINVAL, "n=%d, nR=%lld exceeds the shared-memory plan", n, (long long)H->nR);
+  ck(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total), "smem attr");
+  int per_sm = 0;
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_kernel, nt, Ls.total), "occupancy");
+  if (per_sm < 1) fail(LQM_EINVAL, "eigh kernel cannot be resident for n=%d", n);
+  const int64_t nn = (int64_t)n * n;
+  const int64_t slot = (a_in_smem ? 3 : 5) * nn;
+  int64_t grid = std::min<int64_t>(nk, (int64_t)per_sm * ctx->num_sms);
+  // keep the scratch below ~16 GB
+  const int64_t max_slots = std::max<int64_t>(1, (int64_t)(16.0e9 / (8.0 * (double)slot)));
+  grid = std::max<int64_t>(1, std::min(grid, max_slots));
+  double* scratch = (double*)ws_get(ctx, WS_SCRATCH, (size_t)grid * slot * sizeof(double));
+  EighArgs a;
+  a.n = n; a.nR = (int)H->nR; a.dim = H->d; a.blocks = H->blocks; a.keys = H->keys;
+  a.nk = nk; a.ks = d_ks; a.plan = plan; a.scratch = scratch; a.slot_doubles = slot;
+  a.a_in_smem = a_in_smem; a.bands = d_bands; a.U = d_U;
+  std::pair<cudaEvent_t, cudaEvent_t> evs{};
+  if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
+  eigh_kernel<<<(unsigned)grid, nt, Ls.total, ctx->stream>>>(a);
+  ck(cudaGetLastError(), "eigh_kernel launch");
+  if (ctx->stats_on) { ck(cudaEventRecord(evs.second, ctx->stream), "event"); ctx->ev_pending.push_back(evs); }
+  ctx->eigh_launches++;
+  ctx->launches++;
+}
+
+int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
+  const double per_k = 32.0 * (double)n * (double)n;
+  int64_t b = (int64_t)(budget_bytes / per_k);
+  return std::max<int64_t>(1, std::min(b, nk));
+}
+
+// Density matrix on device arrays; accumulates eband into d_eb[0].
+// bands_out (n x nk, device) receives every k's eigenvalues when non-null.
+void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w, double mu,
+                 double T, int64_t nL, const int64_t* d_Lkeys, double2* d_rho, double* d_eb,
+                 double* bands_out = nullptr) {
+  const int n = (int)H->n;
+  const int64_t nn = (int64_t)n * n;
+  const int64_t B = batch_size_for(n, nk, 8.0e9);
+  double2* U = (double2*)ws_get(ctx, WS_U, (size_t)B * nn * sizeof(double2));
+  double2* rk = (double2*)ws_get(ctx, WS_RHOK, (size_t)B * nn * sizeof(double2));
+  double* bandsb = bands_out ? nullptr : (double*)ws_get(ctx, WS_BANDS, (size_t)B * n * sizeof(double));
+  double* ebk = (double*)ws_get(ctx, WS_EBK, (size_t)B * sizeof(double));
+  double2* coef = (double2*)ws_get(ctx, WS_COEF, (size_t)B * nL * sizeof(double2));
+  for (int64_t k0 = 0; k0 < nk; k0 += B) {
+    const int64_t nb = std::min(B, nk - k0);
+    double* bands = bands_out ? bands_out + k0 * n : bandsb;
+    launch_eigh(ctx, H, nb, d_ks + k0 * H->d, bands, U);
+    const int nt = 256;
+    const size_t sm = (size_t)(n + 32) * sizeof(double);
+    const int64_t g = std::min<int64_t>(nb, (int64_t)ctx->num_sms * 8);
+    rhok_kernel<<<(unsigned)g, nt, sm, ctx->stream>>>(n, nb, U, bands, mu, T, d_w + k0, rk, ebk);
+    ck(cudaGetLastError(), "rhok_kernel launch");
+    ordered_sum_kernel<<<1, 256, 0, ctx->stream>>>(ebk, nb, d_eb, k0 > 0);
+    fold_coef_kernel<<<(unsigned)std::min<int64_t>((nb * nL + 255) / 256, 4096), 256, 0, ctx->stream>>>(
+        nb, H->d, d_ks + k0 * H->d, d_w + k0, (int)nL, d_Lkeys, coef);
+    const int64_t gf = std::min<int64_t>((nn + 255) / 256, (int64_t)ctx->num_sms * 8);
+    fold_kernel<16><<<(unsigned)gf, 256, 0, ctx->stream>>>(nn, nb, rk, coef, (int)nL, d_rho, k0 > 0);
+    ck(cudaGetLastError(), "fold_kernel launch");
+    ctx->launches += 4;
+  }
+}
+
+double chempot_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, double filling,
+                   double T) {
+  const int64_t nv = n * nk;
+  double* mm = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double));
+  MuState* st = (MuState*)(mm + 4);
+  minmax_kernel<<<1, 1024, 0, ctx->stream>>>(d_bands, nv, mm);
+  ctx->launches += 1;
+  const int64_t nbk = std::max<int64_t>(1, std::min<int64_t>((nv + 4095) / 4096, (int64_t)ctx->num_sms * 4));
+  const int64_t chunk = (nv + nbk - 1) / nbk;
+  if (T > 0) {
+    double* part = (double*)ws_get(ctx, WS_MU, (size_t)nbk * sizeof(double));
+    mu_init_kernel<<<1, 1, 0, ctx->stream>>>(st, mm);
+    const double norm = d_w ? 1.0 / (double)n : 1.0 / (double)nv;
+    for (int it = 0; it < 140; ++it) {
+      filling_partial_kernel<<<(unsigned)nbk, 256, 0, ctx->stream>>>(d_bands, (int)n, nv, d_w, st, T, chunk, part);
+      mu_update_kernel<<<1, 32, 0, ctx->stream>>>(part, (int)nbk, st, filling, norm);
+    }
+    ctx->launches += 1 + 2 * 140;
+    ck(cudaGetLastError(), "chemical potential launch");
+    MuState hs;
+    ck(cudaMemcpyAsync(&hs, st, sizeof(MuState), cudaMemcpyDeviceToHost, ctx->stream), "mu readback");
+    wait_stream(ctx);
+    if (hs.err) fail(LQM_EDEVICE, "filling - target does not change sign on [min ε, max ε]");
+    if (!hs.done) fail(LQM_EDEVICE, "chemical potential bisection did not terminate");
+    return hs.result;
+  }
+  // T == 0: midpoint of order statistics i, i+1 (1-based), chemicalpotential.jl:9-23
+  double hmm[2];
+  ck(cudaMemcpyAsync(hmm, mm, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "minmax readback");
+  wait_stream(ctx);
+  if (filling >= 1.0) return hmm[1];
+  if (filling <= 0.0) return hmm[0] - 1.0;
+  const long long i1 = 1 + (long long)std::floor(filling * (double)(nv - 1));
+  long long* part = (long long*)ws_get(ctx, WS_MU, (size_t)nbk * sizeof(long long));
+  double res[2];
+  for (int s = 0; s < 2; ++s) {
+    os_init_kernel<<<1, 1, 0, ctx->stream>>>(st, mm, i1 + s);
+    for (int it = 0; it < 140; ++it) {
+      count_partial_kernel<<<(unsigned)nbk, 256, 0, ctx->stream>>>(d_bands, nv, st, chunk, part);
+      os_update_kernel<<<1, 32, 0, ctx->stream>>>(part, (int)nbk, st);
+    }
+    ctx->launches += 1 + 2 * 140;
+    ck(cudaGetLastError(), "order statistic launch");
+    MuState hs;
+    ck(cudaMemcpyAsync(&hs, st, sizeof(MuState), cudaMemcpyDeviceToHost, ctx->stream), "os readback");
+    wait_stream(ctx);
+    if (!hs.done) fail(LQM_EDEVICE, "order-statistic bisection did not terminate");
+    res[s] = hs.result;
+  }
+  return (res[0] + res[1]) / 2;
+}
+
+void dos_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, int64_t nw,
+             const double* d_om, double gamma, double* d_dos) {
+  const int64_t nv = n * nk;
+  const int64_t nbk = std::max<int64_t>(1, std::min<int64_t>((nv + 1023) / 1024, (int64_t)ctx->num_sms * 2));
+  const int64_t chunk = (nv + nbk - 1) / nbk;
+  double* part = (double*)ws_get(ctx, WS_PART, (size_t)nbk * nw * sizeof(double));
+  const int nt = nw >= 256 ? 256 : (int)((nw + 31) / 32 * 32);
+  dos_partial_kernel<<<(unsigned)nbk, nt, 0, ctx->stream>>>(d_bands, (int)n, nv, d_w, (int)nw, d_om, gamma, chunk,
+                                                           part);
+  dos_reduce_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, ctx->stream>>>(part, (int)nbk, (int)nw,
+                                                                         d_w ? 1.0 : 1.0 / (double)nk, d_dos);
+  ck(cudaGetLastError(), "dos launch");
+  ctx->launches += 2;
+}
+
+template <class T>
+T* upload(lqm_ctx* ctx, int slot, const T* h, size_t count) {
+  T* d = (T*)ws_get(ctx, slot, count * sizeof(T));
+  ck(cudaMemcpyAsync(d, h, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream), "H2D");
+  return d;
+}
+
+double* uniform_weights(lqm_ctx* ctx, int64_t nk) {
+  std::vector<double> w((size_t)nk, 1.0 / (double)nk);
+  double* d = upload(ctx, WS_W, w.data(), w.size());
+  wait_stream(ctx);
+  return d;
+}
+
+void check_ks(const double* ks, int64_t nk, int d) {
+  if (nk < 1) fail(LQM_EINVAL, "nk must be >= 1");
+  if (!ks) fail(LQM_EINVAL, "null k-point array");
+  check_finite(ks, nk * d, "ks");
+}
+
+void check_precision(int precision) {
+  if (precision != 0) fail(LQM_EINVAL, "precision=%d: only the FP64 path (0) is available", precision);
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+int lqm_ctx_create(int device, lqm_ctx** out) {
+  if (!out) return LQM_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return LQM_ECUDA;
+  if (device < 0 || device >= ndev) return LQM_EINVAL;
+  lqm_ctx* c = new (std::nothrow) lqm_ctx();
+  if (!c) return LQM_ENOMEM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+    delete c;
+    return LQM_ECUDA;
+  }
+  *out = c;
+  return LQM_OK;
+}
+
+int lqm_ctx_destroy(lqm_ctx* ctx) {
+  if (!ctx) return LQM_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& b : ctx->ws)
+    if (b.p) cudaFree(b.p);
+  for (auto& kv : ctx->plans) cudaFree(kv.second.d_buf);
+  cudaEventDestroy(ctx->ev0);
+  cudaEventDestroy(ctx->ev1);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return LQM_OK;
+}
+
+const char* lqm_last_error(const lqm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds) {
+  if (!ctx || !(seconds > 0)) return LQM_EINVAL;
+  ctx->timeout_s = seconds;
+  return LQM_OK;
+}
+
+int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms) {
+  if (!ctx || !ms) return LQM_EINVAL;
+  *ms = ctx->last_ms;
+  return LQM_OK;
+}
+
+int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing) {
+  return guarded(ctx, [&] {
+    wait_stream(ctx);
+    ctx->stats_on = enable_timing != 0;
+    ctx->eigh_ms = 0.0;
+    ctx->eigh_launches = 0;
+    ctx->launches = 0;
+  });
+}
+
+int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches) {
+  if (!ctx) return LQM_EINVAL;
+  if (eigh_ms) *eigh_ms = ctx->eigh_ms;
+  if (eigh_launches) *eigh_launches = ctx->eigh_launches;
+  if (launches) *launches = ctx->launches;
+  return LQM_OK;
+}
+
+int lqm_hops_upload_dense(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
+                          const double* blocks, lqm_hops** out) {
+  return guarded(ctx, [&] {
+    if (!out) fail(LQM_EINVAL, "null output pointer");
+    *out = nullptr;
+    if (n < 1 || nR < 1 || d < 1 || d > 3) fail(LQM_EINVAL, "invalid sizes n=%lld nR=%lld d=%d", (long long)n, (long long)nR, d);
+    if (n > 4096) fail(LQM_EINVAL, "n=%lld exceeds the supported maximum 4096", (long long)n);
+    if (!keys || !blocks) fail(LQM_EINVAL, "null keys or blocks");
+    check_finite(blocks, 2 * n * n * nR, "blocks");
+    lqm_hops* h = new lqm_hops();
+    h->n = n; h->nR = nR; h->d = d;
+    h->hkeys.assign(keys, keys + d * nR);
+    const size_t bb = (size_t)(n * n * nR) * sizeof(double2);
+    cudaError_t e1 = cudaMalloc(&h->blocks, bb);
+    cudaError_t e2 = cudaMalloc(&h->keys, (size_t)(d * nR) * sizeof(int64_t));
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+      cudaFree(h->blocks); cudaFree(h->keys); delete h;
+      fail(LQM_ENOMEM, "device allocation for hops failed");
+    }
+    ck(cudaMemcpyAsync(h->blocks, blocks, bb, cudaMemcpyHostToDevice, ctx->stream), "hops upload");
+    ck(cudaMemcpyAsync(h->keys, keys, (size_t)(d * nR) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream), "keys upload");
+    wait_stream(ctx);
+    *out = h;
+  });
+}
+
+int lqm_hops_upload_csc(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
+                        const int64_t* const* colptr, const int64_t* const* rowval, const double* const* nzval,
+                        lqm_hops** out) {
+  return guarded(ctx, [&] {
+    if (!out || !colptr || !rowval || !nzval) fail(LQM_EINVAL, "null argument");
+    if (n < 1 || nR < 1) fail(LQM_EINVAL, "invalid sizes");
+    std::vector<double> dense((size_t)(2 * n * n * nR), 0.0);
+    for (int64_t r = 0; r < nR; ++r) {
+      const int64_t* cp = colptr[r];
+      for (int64_t j = 0; j < n; ++j) {
+        if (cp[j] < 1 || cp[j + 1] < cp[j]) fail(LQM_EINVAL, "invalid colptr in block %lld", (long long)r);
+        for (int64_t p = cp[j] - 1; p < cp[j + 1] - 1; ++p) {
+          const int64_t i = rowval[r][p] - 1;
+          if (i < 0 || i >= n) fail(LQM_EINVAL, "row index out of range in block %lld", (long long)r);
+          double* dst = &dense[(size_t)(2 * (r * n * n + i + j * n))];
+          dst[0] += nzval[r][2 * p];
+          dst[1] += nzval[r][2 * p + 1];
+        }
+      }
+    }
+    int st = lqm_hops_upload_dense(ctx, n, nR, d, keys, dense.data(), out);
+    if (st != LQM_OK) fail(st, "%s", ctx->err.c_str());
+  });
+}
+
+int lqm_hops_free(lqm_ctx* ctx, lqm_hops* h) {
+  if (!h) return LQM_EINVAL;
+  if (ctx) { cudaSetDevice(ctx->device); cudaStreamSynchronize(ctx->stream); }
+  cudaFree(h->blocks);
+  cudaFree(h->keys);
+  delete h;
+  return LQM_OK;
+}
+
+int lqm_hops_dims(const lqm_hops* h, int64_t* n, int64_t* nR, int32_t* d) {
+  if (!h || !n || !nR || !d) return LQM_EINVAL;
+  *n = h->n; *nR = h->nR; *d = h->d;
+  return LQM_OK;
+}
+
+int lqm_bloch_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_Hk) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    if (nk < 1 || !d_ks || !d_Hk) fail(LQM_EINVAL, "invalid arguments");
+    timer_start(ctx);
+    const int64_t g = std::min<int64_t>(nk, (int64_t)ctx->num_sms * 8);
+    bloch_kernel<<<(unsigned)g, 256, (size_t)H->nR * sizeof(double2), ctx->stream>>>(
+        (int)H->n, (int)H->nR, H->d, H->blocks, H->keys, nk, d_ks, (double2*)d_Hk);
+    ck(cudaGetLastError(), "bloch_kernel launch");
+    ctx->launches += 1;
+    timer_stop(ctx);
+    wait_stream(ctx);
+    timer_collect(ctx);
+  });
+}
+
+int lqm_bloch(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, double* Hk) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_ks(ks, nk, H->d);
+    if (!Hk) fail(LQM_EINVAL, "null output");
+    const double* dks = upload(ctx, WS_KS, ks, (size_t)(nk * H->d));
+    const size_t ob = (size_t)(nk * H->n * H->n) * sizeof(double2);
+    double* dH = (double*)ws_get(ctx, WS_U, ob);
+    int st = lqm_bloch_dev(ctx, H, nk, dks, dH);
+    if (st != LQM_OK) fail(st, "%s", ctx->err.c_str());
+    ck(cudaMemcpyAsync(Hk, dH, ob, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+  });
+}
+
+int lqm_bandmatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, int want_vectors,
+                       int precision, double* d_bands, double* d_U) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_precision(precision);
+    if (nk < 1 || !d_ks || !d_bands || (want_vectors && !d_U)) fail(LQM_EINVAL, "invalid arguments");
+    timer_start(ctx);
+    launch_eigh(ctx, H, nk, d_ks, d_bands, want_vectors ? (double2*)d_U : nullptr);
+    timer_stop(ctx);
+    wait_stream(ctx);
+    timer_collect(ctx);
+  });
+}
+
+int lqm_bandmatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int want_vectors, int precision,
+                   double* bands, double* U) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_precision(precision);
+    check_ks(ks, nk, H->d);
+    if (!bands || (want_vectors && !U)) fail(LQM_EINVAL, "null output");
+    const int64_t n = H->n;
+    const double* dks = upload(ctx, WS_KS, ks, (size_t)(nk * H->d));
+    double* db = (double*)ws_get(ctx, WS_BANDS, (size_t)(n * nk) * sizeof(double));
+    double* dU = want_vectors ? (double*)ws_get(ctx, WS_U, (size_t)(n * n * nk) * sizeof(double2)) : nullptr;
+    timer_start(ctx);
+    launch_eigh(ctx, H, nk, dks, db, (double2*)dU);
+    timer_stop(ctx);
+    ck(cudaMemcpyAsync(bands, db, (size_t)(n * nk) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    if (want_vectors)
+      ck(cudaMemcpyAsync(U, dU, (size_t)(n * n * nk) * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+    timer_collect(ctx);
+  });
+}
+
+int lqm_densitymatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w,
+                          double mu, double T, int64_t nL, const int64_t* Lkeys, double* d_rho, double* eband,
+                          int precision) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_precision(precision);
+    if (nk < 1 || !d_ks || nL < 1 || !Lkeys || !d_rho) fail(LQM_EINVAL, "invalid arguments");
+    if (!std::isfinite(mu) || !(T >= 0) || !std::isfinite(T)) fail(LQM_EINVAL, "invalid mu/T");
+    const int64_t* dL = upload(ctx, WS_LKEYS, Lkeys, (size_t)(nL * H->d));
+    const double* dw = d_w ? d_w : uniform_weights(ctx, nk);
+    double* d_eb = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double)) + 40;
+    timer_start(ctx);
+    density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb);
+    timer_stop(ctx);
+    double eb = 0.0;
+    ck(cudaMemcpyAsync(&eb, d_eb, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+    timer_collect(ctx);
+    if (eband) *eband = eb;
+  });
+}
+
+int lqm_densitymatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, double mu,
+                      double T, int64_t nL, const int64_t* Lkeys, double* rho, double* eband, int precision) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_ks(ks, nk, H->d);
+    if (!rho || !Lkeys || nL < 1) fail(LQM_EINVAL, "invalid arguments");
+    if (w) check_finite(w, nk, "w");
+    const double* dks = upload(ctx, WS_KS, ks, (size_t)(nk * H->d));
+    const double* dw = w ? upload(ctx, WS_W, w, (size_t)nk) : nullptr;
+    const size_t rb = (size_t)(nL * H->n * H->n) * sizeof(double2);
+    double* drho = (double*)ws_get(ctx, WS_RHO, rb);
+    int st = lqm_densitymatrix_dev(ctx, H, nk, dks, dw, mu, T, nL, Lkeys, drho, eband, precision);
+    if (st != LQM_OK) fail(st, "%s", ctx->err.c_str());
+    ck(cudaMemcpyAsync(rho, drho, rb, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+  });
+}
+
+int lqm_chemicalpotential_bands_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w,
+                                    double filling, double T, double* mu) {
+  return guarded(ctx, [&] {
+    if (n < 1 || nk < 1 || !d_bands || !mu) fail(LQM_EINVAL, "invalid arguments");
+    if (!std::isfinite(filling) || !(T >= 0) || !std::isfinite(T)) fail(LQM_EINVAL, "invalid filling/T");
+    *mu = chempot_dev(ctx, n, nk, d_bands, d_w, filling, T);
+  });
+}
+
+int lqm_chemicalpotential(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
+                          double filling, double T, double* mu) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_ks(ks, nk, H->d);
+    if (!mu) fail(LQM_EINVAL, "null output");
+    if (w) check_finite(w, nk, "w");
+    const double* dks = upload(ctx, WS_KS, ks, (size_t)(nk * H->d));
+    const double* dw = w ? upload(ctx, WS_W, w, (size_t)nk) : nullptr;
+    double* db = (double*)ws_get(ctx, WS_BANDS, (size_t)(H->n * nk) * sizeof(double));
+    timer_start(ctx);
+    launch_eigh(ctx, H, nk, dks, db, nullptr);
+    timer_stop(ctx);
+    wait_stream(ctx);
+    timer_collect(ctx);
+    int st = lqm_chemicalpotential_bands_dev(ctx, H->n, nk, db, dw, filling, T, mu);
+    if (st != LQM_OK) fail(st, "%s", ctx->err.c_str());
+  });
+}
+
+int lqm_dos_bands_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, int64_t nw,
+                      const double* d_omegas, double gamma, double* d_dos) {
+  return guarded(ctx, [&] {
+    if (n < 1 || nk < 1 || nw < 1 || !d_bands || !d_omegas || !d_dos) fail(LQM_EINVAL, "invalid arguments");
+    if (!std::isfinite(gamma)) fail(LQM_EINVAL, "invalid gamma");
+    dos_dev(ctx, n, nk, d_bands, d_w, nw, d_omegas, gamma, d_dos);
+    wait_stream(ctx);
+  });
+}
+
+int lqm_dos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, int64_t nw,
+            const double* omegas, double gamma, double* dos) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_ks(ks, nk, H->d);
+    if (nw < 1 || !omegas || !dos) fail(LQM_EINVAL, "invalid arguments");
+    check_finite(omegas, nw, "omegas");
+    if (w) check_finite(w, nk, "w");
+    const double* dks = upload(ctx, WS_KS, ks, (size_t)(nk * H->d));
+    const double* dw = w ? upload(ctx, WS_W, w, (size_t)nk) : nullptr;
+    const double* dom = upload(ctx, WS_OMEGA, omegas, (size_t)nw);
+    double* db = (double*)ws_get(ctx, WS_BANDS, (size_t)(H->n * nk) * sizeof(double));
+    double* dd = (double*)ws_get(ctx, WS_DOS, (size_t)nw * sizeof(double));
+    timer_start(ctx);
+    launch_eigh(ctx, H, nk, dks, db, nullptr);
+    dos_dev(ctx, H->n, nk, db, dw, nw, dom, gamma, dd);
+    timer_stop(ctx);
+    ck(cudaMemcpyAsync(dos, dd, (size_t)nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+    timer_collect(ctx);
+  });
+}
+
+int lqm_bands_dos_rho_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w,
+                          double mu, double T, int64_t nL, const int64_t* Lkeys, double* d_rho, double* eband,
+                          int64_t nw, const double* d_omegas, double gamma, double* d_dos, double* d_bands,
+                          int precision) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_precision(precision);
+    if (nk < 1 || !d_ks || nL < 1 || !Lkeys || !d_rho || nw < 1 || !d_omegas || !d_dos || !d_bands)
+      fail(LQM_EINVAL, "invalid arguments");
+    if (!std::isfinite(mu) || !(T >= 0) || !std::isfinite(T) || !std::isfinite(gamma))
+      fail(LQM_EINVAL, "invalid mu/T/gamma");
+    const int64_t* dL = upload(ctx, WS_LKEYS, Lkeys, (size_t)(nL * H->d));
+    const double* dw = d_w ? d_w : uniform_weights(ctx, nk);
+    double* d_eb = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double)) + 40;
+    timer_start(ctx);
+    density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb, d_bands);
+    dos_dev(ctx, H->n, nk, d_bands, d_w, nw, d_omegas, gamma, d_dos);
+    timer_stop(ctx);
+    double eb = 0.0;
+    ck(cudaMemcpyAsync(&eb, d_eb, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+    timer_collect(ctx);
+    if (eband) *eband = eb;
+  });
+}
+
+int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, double mu,
+                      double T, int64_t nL, const int64_t* Lkeys, double* rho, double* eband, int64_t nw,
+                      const double* omegas, double gamma, double* dos, double* bands, int precision) {
+  return guarded(ctx, [&] {
+    check_hops(H);
+    check_ks(ks, nk, H->d);
+    if (!rho || !Lkeys || nL < 1 || nw < 1 || !omegas || !dos || !bands) fail(LQM_EINVAL, "invalid arguments");
+    if (w) check_finite(w, nk, "w");
+    check_finite(omegas, nw, "omegas");
+    const int64_t n = H->n;
+    const double* dks = upload(ctx, WS_KS, ks, (size_t)(nk * H->d));
+    const double* dw = w ? upload(ctx, WS_W, w, (size_t)nk) : nullptr;
+    const double* dom = upload(ctx, WS_OMEGA, omegas, (size_t)nw);
+    const size_t rb = (size_t)(nL * n * n) * sizeof(double2);
+    double* drho = (double*)ws_get(ctx, WS_RHO, rb);
+    double* db = (double*)ws_get(ctx, WS_BANDS2, (size_t)(n * nk) * sizeof(double));
+    double* dd = (double*)ws_get(ctx, WS_DOS, (size_t)nw * sizeof(double));
+    int st = lqm_bands_dos_rho_dev(ctx, H, nk, dks, dw, mu, T, nL, Lkeys, drho, eband, nw, dom, gamma, dd, db,
+                                   precision);
+    if (st != LQM_OK) fail(st, "%s", ctx->err.c_str());
+    ck(cudaMemcpyAsync(rho, drho, rb, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    ck(cudaMemcpyAsync(bands, db, (size_t)(n * nk) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    ck(cudaMemcpyAsync(dos, dd, (size_t)nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    wait_stream(ctx);
+  });
+}
+
+}  // extern "C"
+
+#include "lqm_scf.inc"

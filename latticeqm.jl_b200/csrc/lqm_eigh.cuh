@@ -1,0 +1,457 @@
+// Per-k dense Hermitian eigensolver, one team (CTA) per k-point, FP64.
+//
+//   1. bloch_build:   H(k) = sum_R H_R exp(+i 2 pi k.R) into A (upper triangle is
+//                     the source, mirrored to the lower one — the reference hands
+//                     LAPACK `Hermitian(M)`, i.e. the upper triangle).
+//   2. hetrd_lower:   Householder reduction to a real symmetric tridiagonal T
+//                     (LAPACK zhetd2/zlarfg conventions, reflectors kept in A).
+//   3. dc_solve:      Cuppen divide and conquer on T: tearing, bottom-up merges
+//                     with dlaed2-style deflation, secular equations solved per
+//                     root by a safeguarded two-pole rational iteration, and
+//                     Gu-Eisenstat recomputed z for orthogonal eigenvectors.
+//   4. backtransform: U = H_0 H_1 ... H_{n-2} Z.
+//
+// Every function is a team phase sequence (see lqm_team.cuh).
+#pragma once
+#include "lqm_team.cuh"
+
+#ifndef LQM_DEPS
+#define LQM_DEPS 1.1102230246251565e-16  /* relative machine precision, LAPACK dlamch('E') */
+#endif
+
+// Divide-and-conquer merge plan for one matrix order n (built on the host).
+struct DCPlan {
+  int nnodes;        // internal (merge) nodes, ordered by height
+  int nheights;      // number of merge heights
+  const int* hstart; // [nheights+1] node ranges per height
+  const int* lo;     // [nnodes]
+  const int* mid;    // [nnodes]
+  const int* hi;     // [nnodes]
+  const int* owner;  // [nheights*n] node id covering row i at that height, or -1
+};
+
+// Shared-memory vectors for one k-point (all length >= n unless noted).
+struct EighVec {
+  double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;
+  int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
+  double2 *tau, *v, *w, *bc;
+};
+
+// ---------------------------------------------------------------------------
+// 1. Bloch sum.  blocks: nR x (n x n) column-major complex; keys: d x nR int64.
+// ---------------------------------------------------------------------------
+LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __restrict__ blocks,
+                        const int64_t* __restrict__ keys, const double* kpt, double2* ph,
+                        double2* A, int lda) {
+  for (int r = T.tid; r < nR; r += T.nt) {
+    double dot = 0.0;
+    for (int c = 0; c < dim; ++c) dot += kpt[c] * (double)keys[(int64_t)r * dim + c];
+    double s, co;
+    lqm_sincospi(2.0 * dot, &s, &co);
+    ph[r] = cmk(co, s);
+  }
+  team_sync();
+  const int64_t nn = (int64_t)n * n;
+  for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
+    int i = (int)(idx % n), j = (int)(idx / n);
+    if (i > j) continue;
+    double2 acc = cmk(0.0, 0.0);
+    for (int r = 0; r < nR; ++r) acc = cadd(acc, cmul(blocks[(int64_t)r * nn + idx], ph[r]));
+    if (i == j) {
+      A[i + (int64_t)j * lda] = cmk(acc.x, 0.0);
+    } else {
+      A[i + (int64_t)j * lda] = acc;
+      A[j + (int64_t)i * lda] = cconj(acc);
+    }
+  }
+  team_sync();
+}
+
+// ---------------------------------------------------------------------------
+// 2. Householder tridiagonalisation (lower storage, full Hermitian updates).
+// Out: d[n], e[n-1] (real), tau[n-1]; reflector j is A[j+1.., j] with v0 = 1.
+// ---------------------------------------------------------------------------
+LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, EighVec& S) {
+  for (int j = 0; j < n - 1; ++j) {
+    const int m = n - j - 1;
+    double2* col = A + (j + 1) + (int64_t)j * lda;
+    double2* A22 = A + (j + 1) + (int64_t)(j + 1) * lda;
+    double s = 0.0;
+    for (int r = 1 + T.tid; r < m; r += T.nt) { double2 x = col[r]; s += x.x * x.x + x.y * x.y; }
+    s = team_sum(T, s, S.red);
+    if (T.tid == 0) {
+      double2 alpha = col[0];
+      double2 tj, scal;
+      double beta;
+      if (s == 0.0 && alpha.y == 0.0) {
+        tj = cmk(0.0, 0.0); scal = cmk(0.0, 0.0); beta = alpha.x;
+      } else {
+        double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s);
+        beta = (alpha.x >= 0.0) ? -nrm : nrm;
+        tj = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+        scal = cdiv(cmk(1.0, 0.0), cmk(alpha.x - beta, alpha.y));
+      }
+      S.tau[j] = tj;
+      S.e[j] = beta;
+      S.d[j] = A[j + (int64_t)j * lda].x;
+      S.bc[0] = tj; S.bc[1] = scal;
+    }
+    team_sync();
+    const double2 tj = S.bc[0], scal = S.bc[1];
+    for (int r = T.tid; r < m; r += T.nt) {
+      double2 x = (r == 0) ? cmk(1.0, 0.0) : cmul(scal, col[r]);
+      S.v[r] = x;
+      col[r] = x;
+    }
+    team_sync();
+    // p = tau * A22 v, using Hermiticity: (A22 v)_c = sum_r conj(A22[r,c]) v_r
+    for (int c = T.wid; c < m; c += T.nw) {
+      const double2* Ac = A22 + (int64_t)c * lda;
+      double sr = 0.0, si = 0.0;
+      for (int r = T.lane; r < m; r += T.nl) {
+        double2 a = Ac[r], x = S.v[r];
+        sr += a.x * x.x + a.y * x.y;
+        si += a.x * x.y - a.y * x.x;
+      }
+      sr = warp_sum(sr); si = warp_sum(si);
+      if (T.lane == 0) S.w[c] = cmul(tj, cmk(sr, si));
+    }
+    team_sync();
+    double pr = 0.0, pi = 0.0;
+    for (int r = T.tid; r < m; r += T.nt) {
+      double2 p = cmulc(S.w[r], S.v[r]);  // conj(w) v
+      pr += p.x; pi += p.y;
+    }
+    pr = team_sum(T, pr, S.red);
+    pi = team_sum(T, pi, S.red);
+    const double2 alpha2 = cmul(cmk(-0.5 * tj.x, -0.5 * tj.y), cmk(pr, pi));
+    for (int r = T.tid; r < m; r += T.nt) S.w[r] = cadd(S.w[r], cmul(alpha2, S.v[r]));
+    team_sync();
+    const int64_t mm = (int64_t)m * m;
+    for (int64_t idx = T.tid; idx < mm; idx += T.nt) {
+      int r = (int)(idx % m), c = (int)(idx / m);
+      double2 vr = S.v[r], wr = S.w[r], vc = S.v[c], wc = S.w[c];
+      double2 upd = cadd(cmul(vr, cconj(wc)), cmul(wr, cconj(vc)));
+      double2* a = A22 + r + (int64_t)c * lda;
+      double2 nv = csub(*a, upd);
+      if (r == c) nv.y = 0.0;
+      *a = nv;
+    }
+    team_sync();
+  }
+  if (T.tid == 0) S.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda].x;
+  team_sync();
+}
+
+// ---------------------------------------------------------------------------
+// 3. Divide and conquer on the symmetric tridiagonal (d, e).
+// ---------------------------------------------------------------------------
+
+// One root of the secular equation 1 + rho sum_j zl_j^2 / (dl_j - lambda) = 0,
+// dl ascending, rho > 0.  lambda = dl[org] + tau; interior roots take the
+// nearer pole as origin.  Safeguarded two-pole rational steps (each step fits
+// the poles left and right of the root separately to value and slope).
+LQM_FN void secular_root(int k, const double* dl, const double* zl, double rho, int i, int* org_out,
+                         double* tau_out) {
+  if (k == 1) { *org_out = 0; *tau_out = rho * zl[0] * zl[0]; return; }
+  int org;
+  double lo, hi;
+  if (i < k - 1) {
+    const double gap = dl[i + 1] - dl[i];
+    const double mid = 0.5 * gap;
+    double f = 1.0;
+    for (int j = 0; j < k; ++j) f += rho * zl[j] * zl[j] / ((dl[j] - dl[i]) - mid);
+    if (f >= 0.0) { org = i; lo = 0.0; hi = mid; }
+    else { org = i + 1; lo = -(gap - mid); hi = 0.0; }
+  } else {
+    double zs = 0.0;
+    for (int j = 0; j < k; ++j) zs += zl[j] * zl[j];
+    org = k - 1; lo = 0.0; hi = rho * zs * (1.0 + 4.0 * LQM_DEPS) + 1e-300;
+  }
+  const double dorg = dl[org];
+  double tau = 0.5 * (lo + hi);
+  for (int it = 0; it < 80; ++it) {
+    double psi1 = 0.0, dpsi1 = 0.0, psi2 = 0.0, dpsi2 = 0.0, abss = 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double del = (dl[j] - dorg) - tau;
+      const double t = zl[j] / del;
+      const double term = rho * zl[j] * t;
+      const double dterm = rho * t * t;
+      if (j <= i) { psi1 += term; dpsi1 += dterm; } else { psi2 += term; dpsi2 += dterm; }
+      abss += fabs(term);
+    }
+    const double f = 1.0 + psi1 + psi2;
+    if (f == 0.0) break;
+    if (f < 0.0) lo = tau; else hi = tau;
+    if (fabs(f) <= 8.0 * LQM_DEPS * (1.0 + abss) * 2.0) break;
+    const double a = (dl[i] - dorg) - tau;
+    double x;
+    bool ok = true;
+    if (i < k - 1) {
+      const double b = (dl[i + 1] - dorg) - tau;
+      const double s1 = a * a * dpsi1, s2 = b * b * dpsi2;
+      const double c = 1.0 + (psi1 - a * dpsi1) + (psi2 - b * dpsi2);
+      const double B = c * (a + b) + s1 + s2;
+      const double C = a * b * f;
+      double disc = B * B - 4.0 * c * C;
+      if (disc < 0.0) disc = 0.0;
+      const double sq = sqrt(disc);
+      if (c == 0.0) { if (B != 0.0) x = C / B; else ok = false; }
+      else if (B > 0.0) x = 2.0 * C / (B + sq);
+      else x = (B - sq) / (2.0 * c);
+    } else {
+      const double s1 = a * a * dpsi1;
+      const double c = 1.0 + psi1 - a * dpsi1;
+      if (c > 0.0) x = a + s1 / c; else ok = false;
+    }
+    double tn = ok ? tau + x : 0.5 * (lo + hi);
+    if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+    const double chg = fabs(tn - tau);
+    tau = tn;
+    if (chg <= 2.0 * LQM_DEPS * fabs(tn)) break;
+    if (hi - lo <= 2.0 * LQM_DEPS * fmax(fabs(lo), fabs(hi))) break;
+  }
+  *org_out = org;
+  *tau_out = tau;
+}
+
+// dlaed2-style deflation for one merge node (single thread).
+LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta) {
+  const int lo = P.lo[node], hi = P.hi[node];
+  const double rho = 2.0 * eabs_beta;
+  double zmax = 0.0, dmax = 0.0;
+  for (int i = lo; i < hi; ++i) { zmax = fmax(zmax, fabs(S.z[i])); dmax = fmax(dmax, fabs(S.D[i])); }
+  const double tol = 8.0 * LQM_DEPS * fmax(dmax, zmax);
+  int k = 0, nd = 0, nr = 0;
+  if (rho * zmax <= tol) {
+    for (int p = lo; p < hi; ++p) { int j = S.perm[p]; S.dval[lo + nd] = S.D[j]; S.dcol[lo + nd] = j; ++nd; }
+  } else {
+    int pj = -1;
+    for (int p = lo; p < hi; ++p) {
+      const int j = S.perm[p];
+      if (rho * fabs(S.z[j]) <= tol) { S.dval[lo + nd] = S.D[j]; S.dcol[lo + nd] = j; ++nd; continue; }
+      if (pj < 0) { pj = j; continue; }
+      double sv = S.z[pj], cv = S.z[j];
+      const double tau = hypot(cv, sv);
+      const double t = S.D[j] - S.D[pj];
+      cv /= tau; sv = -sv / tau;
+      if (fabs(t * cv * sv) <= tol) {
+        S.z[j] = tau; S.z[pj] = 0.0;
+        S.ri[lo + nr] = pj; S.rj[lo + nr] = j; S.rc[lo + nr] = cv; S.rs[lo + nr] = sv; ++nr;
+        const double t2 = S.D[pj] * cv * cv + S.D[j] * sv * sv;
+        S.D[j] = S.D[pj] * sv * sv + S.D[j] * cv * cv;
+        S.D[pj] = t2;
+        S.dval[lo + nd] = S.D[pj]; S.dcol[lo + nd] = pj; ++nd;
+        pj = j;
+      } else {
+        S.dl[lo + k] = S.D[pj]; S.zl[lo + k] = S.z[pj]; S.colnd[lo + k] = pj; ++k;
+        pj = j;
+      }
+    }
+    if (pj >= 0) { S.dl[lo + k] = S.D[pj]; S.zl[lo + k] = S.z[pj]; S.colnd[lo + k] = pj; ++k; }
+  }
+  S.nk[node] = k; S.nrot[node] = nr; S.ndef[node] = nd; S.nrho[node] = rho;
+}
+
+// In: S.d (diag, n), S.e (offdiag, n-1).  Out: S.D ascending eigenvalues, Q (n x n, ld n).
+// Qt, Us: n x n scratch.
+LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
+                              double* Us) {
+  const int64_t nn = (int64_t)n * n;
+  double mx = 0.0;
+  for (int i = T.tid; i < n; i += T.nt) {
+    mx = fmax(mx, fabs(S.d[i]));
+    if (i < n - 1) mx = fmax(mx, fabs(S.e[i]));
+  }
+  mx = team_max(T, mx, S.red);
+  double scale = 1.0;
+  if (mx > 0.0) { int ex; frexp(mx, &ex); scale = ldexp(1.0, ex); }
+  const double inv = 1.0 / scale;
+  for (int i = T.tid; i < n; i += T.nt) { S.D[i] = S.d[i] * inv; if (i < n - 1) S.e[i] *= inv; }
+  for (int64_t idx = T.tid; idx < nn; idx += T.nt) Q[idx] = ((idx % n) == (idx / n)) ? 1.0 : 0.0;
+  team_sync();
+  for (int nd = T.tid; nd < P.nnodes; nd += T.nt) {
+    const int m = P.mid[nd];
+    const double b = fabs(S.e[m - 1]);
+    S.D[m - 1] -= b;
+    S.D[m] -= b;
+  }
+  team_sync();
+  for (int h = 0; h < P.nheights; ++h) {
+    const int h0 = P.hstart[h], h1 = P.hstart[h + 1];
+    const int* own = P.owner + (int64_t)h * n;
+    // A: merge vector z (scaled by 1/sqrt 2) and the merged sort order
+    for (int i = T.tid; i < n; i += T.nt) {
+      const int nd = own[i];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], m = P.mid[nd], hi = P.hi[nd];
+      const double beta = S.e[m - 1];
+      double zi = (i < m) ? Q[(m - 1) + (int64_t)i * n] : ((beta < 0.0) ? -1.0 : 1.0) * Q[m + (int64_t)i * n];
+      S.z[i] = zi * 0.70710678118654752440;
+      const double di = S.D[i];
+      int cnt = 0;
+      if (i < m) {
+        int a = m, b = hi;  // first index in [m,hi) with D >= di
+        while (a < b) { int c = (a + b) >> 1; if (S.D[c] < di) a = c + 1; else b = c; }
+        cnt = a - m;
+        S.perm[lo + (i - lo) + cnt] = i;
+      } else {
+        int a = lo, b = m;  // first index in [lo,m) with D > di
+        while (a < b) { int c = (a + b) >> 1; if (S.D[c] <= di) a = c + 1; else b = c; }
+        cnt = a - lo;
+        S.perm[lo + (i - m) + cnt] = i;
+      }
+    }
+    team_sync();
+    // B: deflation, one thread per node
+    for (int nd = h0 + T.tid; nd < h1; nd += T.nt) deflate_node(nd, P, S, fabs(S.e[P.mid[nd] - 1]));
+    team_sync();
+    // C: secular roots
+    for (int i = T.tid; i < n; i += T.nt) {
+      const int nd = own[i];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], q = i - lo, k = S.nk[nd];
+      if (q >= k) continue;
+      int org; double tr;
+      secular_root(k, S.dl + lo, S.zl + lo, S.nrho[nd], q, &org, &tr);
+      S.org[lo + q] = org; S.troot[lo + q] = tr;
+    }
+    team_sync();
+    // D: Gu-Eisenstat z
+    for (int i = T.tid; i < n; i += T.nt) {
+      const int nd = own[i];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], q = i - lo, k = S.nk[nd];
+      if (q >= k) continue;
+      const double* dl = S.dl + lo;
+      const double rho = S.nrho[nd];
+      double prod = 1.0;
+      for (int j = 0; j < k; ++j) {
+        const double dij = (dl[q] - dl[S.org[lo + j]]) - S.troot[lo + j];
+        if (j == q) prod *= -dij / rho; else prod *= -dij / (dl[j] - dl[q]);
+      }
+      const double zh = sqrt(fabs(prod));
+      S.zhat[lo + q] = (S.zl[lo + q] < 0.0) ? -zh : zh;
+    }
+    team_sync();
+    // E: secular eigenvectors, column q of Us block
+    for (int i = T.tid; i < n; i += T.nt) {
+      const int nd = own[i];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], q = i - lo, k = S.nk[nd];
+      if (q >= k) continue;
+      const double* dl = S.dl + lo;
+      const double lorg = dl[S.org[lo + q]], tq = S.troot[lo + q];
+      double nrm = 0.0;
+      for (int p = 0; p < k; ++p) {
+        const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
+        Us[(lo + p) + (int64_t)(lo + q) * n] = u;
+        nrm += u * u;
+      }
+      const double sc = 1.0 / sqrt(nrm);
+      for (int p = 0; p < k; ++p) Us[(lo + p) + (int64_t)(lo + q) * n] *= sc;
+    }
+    // F: deflation rotations on the rows of Q
+    for (int r = T.tid; r < n; r += T.nt) {
+      const int nd = own[r];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], nr = S.nrot[nd];
+      for (int t = 0; t < nr; ++t) {
+        const int a = S.ri[lo + t], b = S.rj[lo + t];
+        const double c = S.rc[lo + t], s = S.rs[lo + t];
+        const double x = Q[r + (int64_t)a * n], y = Q[r + (int64_t)b * n];
+        Q[r + (int64_t)a * n] = c * x + s * y;
+        Q[r + (int64_t)b * n] = c * y - s * x;
+      }
+    }
+    // G: merged eigenvalue list of each node
+    for (int i = T.tid; i < n; i += T.nt) {
+      const int nd = own[i];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], it = i - lo, k = S.nk[nd];
+      S.vals[i] = (it < k) ? S.dl[lo + S.org[lo + it]] + S.troot[lo + it] : S.dval[lo + it - k];
+    }
+    team_sync();
+    for (int i = T.tid; i < n; i += T.nt) {
+      const int nd = own[i];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], hi = P.hi[nd];
+      const double v = S.vals[i];
+      int cnt = 0;
+      for (int j = lo; j < hi; ++j) { const double vj = S.vals[j]; cnt += (vj < v) || (vj == v && j < i); }
+      S.newpos[i] = lo + cnt;
+    }
+    team_sync();
+    // H: eigenvector update into Qt
+    for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
+      const int r = (int)(idx % n), c = (int)(idx / n);
+      const int nd = own[r];
+      if (nd < 0 || own[c] != nd) continue;
+      const int lo = P.lo[nd], it = c - lo, k = S.nk[nd];
+      double acc;
+      if (it < k) {
+        acc = 0.0;
+        const double* uc = Us + lo + (int64_t)(lo + it) * n;
+        for (int p = 0; p < k; ++p) acc += Q[r + (int64_t)S.colnd[lo + p] * n] * uc[p];
+      } else {
+        acc = Q[r + (int64_t)S.dcol[lo + it - k] * n];
+      }
+      Qt[r + (int64_t)S.newpos[c] * n] = acc;
+    }
+    team_sync();
+    // I: write back
+    for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
+      const int r = (int)(idx % n), c = (int)(idx / n);
+      const int nd = own[r];
+      if (nd < 0 || own[c] != nd) continue;
+      Q[idx] = Qt[idx];
+    }
+    for (int i = T.tid; i < n; i += T.nt) {
+      if (own[i] < 0) continue;
+      S.D[S.newpos[i]] = S.vals[i];
+    }
+    team_sync();
+  }
+  for (int i = T.tid; i < n; i += T.nt) S.D[i] *= scale;
+  team_sync();
+}
+
+// ---------------------------------------------------------------------------
+// 4. Back-transformation U = H_0 ... H_{n-2} Q  (U complex n x n, ld ldu).
+// ---------------------------------------------------------------------------
+LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* A, int lda, EighVec& S,
+                                   const double* Q, double2* U, int64_t ldu) {
+  const int64_t nn = (int64_t)n * n;
+  for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
+    const int r = (int)(idx % n), c = (int)(idx / n);
+    U[r + c * ldu] = cmk(Q[idx], 0.0);
+  }
+  team_sync();
+  for (int j = n - 2; j >= 0; --j) {
+    const int m = n - j - 1;
+    const double2 tj = S.tau[j];
+    if (tj.x == 0.0 && tj.y == 0.0) continue;
+    const double2* v = A + (j + 1) + (int64_t)j * lda;
+    for (int r = T.tid; r < m; r += T.nt) S.v[r] = v[r];
+    team_sync();
+    // y_c = v^H U[j+1.., c]
+    for (int c = T.wid; c < n; c += T.nw) {
+      const double2* Uc = U + (j + 1) + c * ldu;
+      double sr = 0.0, si = 0.0;
+      for (int r = T.lane; r < m; r += T.nl) {
+        double2 p = cmulc(S.v[r], Uc[r]);
+        sr += p.x; si += p.y;
+      }
+      sr = warp_sum(sr); si = warp_sum(si);
+      if (T.lane == 0) S.w[c] = cmul(tj, cmk(sr, si));
+    }
+    team_sync();
+    const int64_t mn = (int64_t)m * n;
+    for (int64_t idx = T.tid; idx < mn; idx += T.nt) {
+      const int r = (int)(idx % m), c = (int)(idx / m);
+      double2* u = U + (j + 1 + r) + c * ldu;
+      *u = csub(*u, cmul(S.v[r], S.w[c]));
+    }
+    team_sync();
+  }
+}

@@ -1,0 +1,387 @@
+// CUDA kernels of the k-space hot path (sm_100a, FP64).
+#pragma once
+#include <cuda_runtime.h>
+#include "lqm_eigh.cuh"
+
+namespace lqm {
+
+// Shared-memory layout of eigh_kernel for order n, nR hopping keys.
+struct EighSmemLayout {
+  size_t offA, offC, offD, offI, total;
+  int a_in_smem;
+};
+
+__host__ __device__ inline size_t lqm_align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+__host__ __device__ inline EighSmemLayout eigh_smem_layout(int n, int nR, int a_in_smem) {
+  EighSmemLayout L;
+  L.a_in_smem = a_in_smem;
+  size_t off = 0;
+  L.offA = off;
+  if (a_in_smem) off += lqm_align16((size_t)n * n * 16);
+  L.offC = off;                                      // double2: tau, v, w (n each), bc (2), ph (nR)
+  off += lqm_align16((size_t)(3 * n + 2 + nR) * 16);
+  L.offD = off;                                      // doubles: 13 n + 32 (red) + 4 (kpt)
+  off += lqm_align16((size_t)(13 * n + 36) * 8);
+  L.offI = off;                                      // ints: 10 n
+  off += lqm_align16((size_t)(10 * n) * 4);
+  L.total = off;
+  return L;
+}
+
+struct EighArgs {
+  int n, nR, dim;
+  const double2* blocks;  // nR x n x n
+  const int64_t* keys;    // dim x nR
+  int64_t nk;             // k-points in this launch
+  const double* ks;       // dim x nk
+  DCPlan plan;
+  double* scratch;        // gridDim.x slots
+  int64_t slot_doubles;
+  int a_in_smem;
+  double* bands;          // n x nk
+  double2* U;             // n x n x nk, or null for eigenvalues only
+};
+
+__global__ void __launch_bounds__(256) eigh_kernel(EighArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Team T = make_team();
+  const int n = a.n;
+  const EighSmemLayout L = eigh_smem_layout(n, a.nR, a.a_in_smem);
+  double2* cbuf = (double2*)(smem + L.offC);
+  double* dbuf = (double*)(smem + L.offD);
+  int* ibuf = (int*)(smem + L.offI);
+  EighVec S;
+  S.tau = cbuf; S.v = cbuf + n; S.w = cbuf + 2 * n; S.bc = cbuf + 3 * n;
+  double2* ph = cbuf + 3 * n + 2;
+  S.d = dbuf; S.e = dbuf + n; S.D = dbuf + 2 * n; S.z = dbuf + 3 * n; S.dl = dbuf + 4 * n;
+  S.zl = dbuf + 5 * n; S.troot = dbuf + 6 * n; S.zhat = dbuf + 7 * n; S.vals = dbuf + 8 * n;
+  S.dval = dbuf + 9 * n; S.rc = dbuf + 10 * n; S.rs = dbuf + 11 * n; S.nrho = dbuf + 12 * n;
+  S.red = dbuf + 13 * n;
+  double* kpt = dbuf + 13 * n + 32;
+  S.perm = ibuf; S.colnd = ibuf + n; S.org = ibuf + 2 * n; S.dcol = ibuf + 3 * n; S.newpos = ibuf + 4 * n;
+  S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
+
+  const int64_t nn = (int64_t)n * n;
+  double* slot = a.scratch + (int64_t)blockIdx.x * a.slot_doubles;
+  double2* A;
+  double* Q;
+  if (a.a_in_smem) { A = (double2*)(smem + L.offA); Q = slot; }
+  else { A = (double2*)slot; Q = slot + 2 * nn; }
+  double* Qt = Q + nn;
+  double* Us = Qt + nn;
+
+  for (int64_t k = blockIdx.x; k < a.nk; k += gridDim.x) {
+    if (T.tid < a.dim) kpt[T.tid] = a.ks[k * a.dim + T.tid];
+    team_sync();
+    bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, n);
+    hetrd_lower(T, n, A, n, S);
+    dc_solve(T, n, a.plan, S, Q, Qt, Us);
+    for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
+    if (a.U) backtransform(T, n, A, n, S, Q, a.U + k * nn, n);
+    team_sync();
+  }
+}
+
+// Batched Bloch sum to HBM: Hk[k] = sum_R H_R exp(i 2 pi k.R); one CTA per k.
+__global__ void __launch_bounds__(256) bloch_kernel(int n, int nR, int dim, const double2* __restrict__ blocks,
+                                                    const int64_t* __restrict__ keys, int64_t nk,
+                                                    const double* __restrict__ ks, double2* __restrict__ Hk) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* ph = (double2*)smem;
+  const int64_t nn = (int64_t)n * n;
+  for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
+    for (int r = threadIdx.x; r < nR; r += blockDim.x) {
+      double dot = 0.0;
+      for (int c = 0; c < dim; ++c) dot += ks[k * dim + c] * (double)keys[(int64_t)r * dim + c];
+      double s, co;
+      sincospi(2.0 * dot, &s, &co);
+      ph[r] = cmk(co, s);
+    }
+    __syncthreads();
+    double2* out = Hk + k * nn;
+    for (int64_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+      double2 acc = cmk(0.0, 0.0);
+      for (int r = 0; r < nR; ++r) acc = cadd(acc, cmul(__ldg(&blocks[(int64_t)r * nn + idx]), ph[r]));
+      out[idx] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ double fermi(double x, double T) {
+  if (T > 0.0) return 1.0 / (exp(x / T) + 1.0);
+  return (-x < 0.0) ? 0.0 : ((-x > 0.0) ? 1.0 : 0.5);
+}
+
+// rho_k = U diag(f) U^H per k; eband_k = w_k sum_j f_j eps_j.
+__global__ void __launch_bounds__(256) rhok_kernel(int n, int64_t nk, const double2* __restrict__ U,
+                                                   const double* __restrict__ bands, double mu, double T,
+                                                   const double* __restrict__ w, double2* __restrict__ rhok,
+                                                   double* __restrict__ eband_k) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* f = (double*)smem;
+  double* red = f + n;
+  const Team Tm = make_team();
+  const int64_t nn = (int64_t)n * n;
+  for (int64_t k = blockIdx.x; k < nk; k += gridDim.x) {
+    double eb = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      const double e = bands[k * n + j];
+      const double fj = fermi(e - mu, T);
+      f[j] = fj;
+      eb += e * fj;
+    }
+    eb = team_sum(Tm, eb, red);
+    if (threadIdx.x == 0) eband_k[k] = w[k] * eb;
+    const double2* Uk = U + k * nn;
+    for (int64_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+      const int aa = (int)(idx % n), bb = (int)(idx / n);
+      double sr = 0.0, si = 0.0;
+      for (int j = 0; j < n; ++j) {
+        const double fj = f[j];
+        if (fj == 0.0) continue;
+        const double2 ua = Uk[aa + (int64_t)j * n], ub = Uk[bb + (int64_t)j * n];
+        // ua * conj(ub) * f
+        sr += fj * (ua.x * ub.x + ua.y * ub.y);
+        si += fj * (ua.y * ub.x - ua.x * ub.y);
+      }
+      rhok[k * nn + idx] = cmk(sr, si);
+    }
+    __syncthreads();
+  }
+}
+
+// coef[kb*nL + l] = w_k exp(-i 2 pi k.L_l)
+__global__ void fold_coef_kernel(int64_t nb, int dim, const double* __restrict__ ks, const double* __restrict__ w,
+                                 int nL, const int64_t* __restrict__ Lkeys, double2* __restrict__ coef) {
+  const int64_t tot = nb * nL;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t kb = t / nL;
+    const int l = (int)(t % nL);
+    double dot = 0.0;
+    for (int c = 0; c < dim; ++c) dot += ks[kb * dim + c] * (double)Lkeys[(int64_t)l * dim + c];
+    double s, co;
+    sincospi(2.0 * dot, &s, &co);
+    coef[t] = cmk(w[kb] * co, -w[kb] * s);
+  }
+}
+
+// rhoL[l] (+)= sum_kb coef[kb,l] * rhok[kb], k in fixed order per element.
+template <int LC>
+__global__ void __launch_bounds__(256) fold_kernel(int64_t nn, int64_t nb, const double2* __restrict__ rhok,
+                                                   const double2* __restrict__ coef, int nL,
+                                                   double2* __restrict__ rhoL, int accumulate) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
+    for (int l0 = 0; l0 < nL; l0 += LC) {
+      double2 acc[LC];
+#pragma unroll
+      for (int l = 0; l < LC; ++l) {
+        acc[l] = cmk(0.0, 0.0);
+        if (accumulate && l0 + l < nL) acc[l] = rhoL[(int64_t)(l0 + l) * nn + e];
+      }
+      for (int64_t kb = 0; kb < nb; ++kb) {
+        const double2 x = rhok[kb * nn + e];
+        const double2* cf = coef + kb * nL + l0;
+#pragma unroll
+        for (int l = 0; l < LC; ++l) {
+          if (l0 + l < nL) acc[l] = cadd(acc[l], cmul(cf[l], x));
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < LC; ++l)
+        if (l0 + l < nL) rhoL[(int64_t)(l0 + l) * nn + e] = acc[l];
+    }
+  }
+}
+
+// Fixed-order sum of x[0..m) into out[0] (single CTA).
+__global__ void ordered_sum_kernel(const double* __restrict__ x, int64_t m, double* out, int accumulate) {
+  __shared__ double red[32];
+  const Team Tm = make_team();
+  // contiguous chunks per thread, then a deterministic team reduction
+  const int64_t chunk = (m + blockDim.x - 1) / blockDim.x;
+  double s = 0.0;
+  const int64_t b = threadIdx.x * chunk, e = (b + chunk < m) ? b + chunk : m;
+  for (int64_t i = b; i < e; ++i) s += x[i];
+  s = team_sum(Tm, s, red);
+  if (threadIdx.x == 0) out[0] = accumulate ? out[0] + s : s;
+}
+
+// DOS: partial[b*nw + i] = sum over this block's values of w * Gamma/((omega_i - eps)^2 + Gamma^2)
+__global__ void __launch_bounds__(256) dos_partial_kernel(const double* __restrict__ bands, int n, int64_t nvals,
+                                                          const double* __restrict__ w, int nw,
+                                                          const double* __restrict__ omegas, double gamma,
+                                                          int64_t chunk, double* __restrict__ partial) {
+  __shared__ double ev[1024];
+  __shared__ double ew[1024];
+  const int64_t b0 = blockIdx.x * chunk;
+  const int64_t b1 = (b0 + chunk < nvals) ? b0 + chunk : nvals;
+  const double g2 = gamma * gamma;
+  for (int i0 = 0; i0 < nw; i0 += blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const double om = (i < nw) ? omegas[i] : 0.0;
+    double acc = 0.0;
+    for (int64_t t0 = b0; t0 < b1; t0 += 1024) {
+      const int cnt = (int)((t0 + 1024 < b1) ? 1024 : (b1 - t0));
+      __syncthreads();
+      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        ev[t] = bands[t0 + t];
+        ew[t] = w ? w[(t0 + t) / n] : 1.0;
+      }
+      __syncthreads();
+      if (i < nw) {
+        for (int t = 0; t < cnt; ++t) {
+          const double x = om - ev[t];
+          acc += ew[t] * gamma / (x * x + g2);
+        }
+      }
+    }
+    if (i < nw) partial[(int64_t)blockIdx.x * nw + i] = acc;
+  }
+}
+
+__global__ void dos_reduce_kernel(const double* __restrict__ partial, int nb, int nw, double scale,
+                                  double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += partial[(int64_t)b * nw + i];
+    out[i] = s * scale;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Chemical potential: bisection over the float64 order (Roots.jl Bisection).
+// ---------------------------------------------------------------------------
+struct MuState {
+  double a, b, fa, fb, x, result;
+  long long target;  // order-statistic search: wanted count
+  int phase, done, iters, err;
+};
+
+__device__ __forceinline__ double float_mid(double a, double b) {
+  if ((a < 0.0 && b > 0.0) || (b < 0.0 && a > 0.0)) return 0.0;
+  unsigned long long ua = (unsigned long long)__double_as_longlong(fabs(a));
+  unsigned long long ub = (unsigned long long)__double_as_longlong(fabs(b));
+  double m = __longlong_as_double((long long)((ua + ub) >> 1));
+  return (a + b < 0.0) ? -m : m;
+}
+
+__global__ void minmax_kernel(const double* __restrict__ x, int64_t m, double* out /* min, max */) {
+  __shared__ double rmin[32], rmax[32];
+  double lo = INFINITY, hi = -INFINITY;
+  for (int64_t i = threadIdx.x; i < m; i += blockDim.x) { lo = fmin(lo, x[i]); hi = fmax(hi, x[i]); }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) { rmin[threadIdx.x >> 5] = lo; rmax[threadIdx.x >> 5] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) { lo = fmin(lo, rmin[w]); hi = fmax(hi, rmax[w]); }
+    lo = fmin(lo, rmin[0]); hi = fmax(hi, rmax[0]);
+    out[0] = lo; out[1] = hi;
+  }
+}
+
+__global__ void mu_init_kernel(MuState* st, const double* mm) {
+  st->a = mm[0]; st->b = mm[1]; st->fa = st->fb = 0.0; st->x = mm[0]; st->result = 0.0;
+  st->phase = 0; st->done = 0; st->iters = 0; st->err = 0;
+}
+
+// partial[b] = sum over block b's chunk of weight * f(v - x)
+__global__ void __launch_bounds__(256) filling_partial_kernel(const double* __restrict__ bands, int n,
+                                                              int64_t nvals, const double* __restrict__ w,
+                                                              const MuState* st, double T, int64_t chunk,
+                                                              double* __restrict__ partial) {
+  __shared__ double red[32];
+  if (st->done) return;
+  const Team Tm = make_team();
+  const double x = st->x;
+  const int64_t b0 = blockIdx.x * chunk;
+  const int64_t b1 = (b0 + chunk < nvals) ? b0 + chunk : nvals;
+  double s = 0.0;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const double f = fermi(bands[i] - x, T);
+    s += w ? w[i / n] * f : f;
+  }
+  s = team_sum(Tm, s, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__device__ __forceinline__ double sgn(double v) { return (v > 0.0) - (v < 0.0); }
+
+__global__ void mu_update_kernel(const double* __restrict__ partial, int nb, MuState* st, double filling,
+                                 double norm) {
+  if (threadIdx.x != 0 || st->done) return;
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += partial[b];
+  const double g = s * norm - filling;
+  st->iters++;
+  if (st->phase == 0) {
+    st->fa = g;
+    if (g == 0.0) { st->result = st->a; st->done = 1; return; }
+    st->phase = 1; st->x = st->b; return;
+  }
+  if (st->phase == 1) {
+    st->fb = g;
+    if (g == 0.0) { st->result = st->b; st->done = 1; return; }
+    if (sgn(st->fa) == sgn(st->fb)) { st->err = 1; st->result = NAN; st->done = 1; return; }
+    st->phase = 2;
+  } else {
+    if (g == 0.0) { st->result = st->x; st->done = 1; return; }
+    if (sgn(g) == sgn(st->fa)) { st->a = st->x; st->fa = g; } else { st->b = st->x; st->fb = g; }
+  }
+  const double m = float_mid(st->a, st->b);
+  if (m == st->a || m == st->b || st->iters > 200) {
+    st->result = (fabs(st->fa) <= fabs(st->fb)) ? st->a : st->b;
+    st->done = 1;
+    return;
+  }
+  st->x = m;
+}
+
+// Order statistic (T = 0): smallest float x in [min,max] with #{v <= x} >= target.
+__global__ void __launch_bounds__(256) count_partial_kernel(const double* __restrict__ v, int64_t m,
+                                                            const MuState* st, int64_t chunk,
+                                                            long long* __restrict__ partial) {
+  __shared__ long long red[32];
+  if (st->done) return;
+  const double x = st->x;
+  const int64_t b0 = blockIdx.x * chunk;
+  const int64_t b1 = (b0 + chunk < m) ? b0 + chunk : m;
+  long long c = 0;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) c += (v[i] <= x);
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    partial[blockIdx.x] = s;
+  }
+}
+
+__global__ void os_init_kernel(MuState* st, const double* mm, long long target) {
+  st->a = mm[0]; st->b = mm[1]; st->x = mm[0]; st->target = target;
+  st->phase = 0; st->done = 0; st->iters = 0; st->err = 0; st->result = 0.0;
+}
+
+__global__ void os_update_kernel(const long long* __restrict__ partial, int nb, MuState* st) {
+  if (threadIdx.x != 0 || st->done) return;
+  long long c = 0;
+  for (int b = 0; b < nb; ++b) c += partial[b];
+  const bool ge = c >= st->target;
+  st->iters++;
+  if (st->phase == 0) {  // evaluated at min
+    if (ge) { st->result = st->a; st->done = 1; return; }
+    st->phase = 1;
+  } else {
+    if (ge) st->b = st->x; else st->a = st->x;
+  }
+  const double m = float_mid(st->a, st->b);
+  if (m == st->a || m == st->b || st->iters > 200) { st->result = st->b; st->done = 1; return; }
+  st->x = m;
+}
+
+}  // namespace lqm

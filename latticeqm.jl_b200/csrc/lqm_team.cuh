@@ -1,0 +1,121 @@
+// Thread-team abstraction shared by the CUDA kernels and their host emulation.
+//
+// Every per-k algorithm in this library is written as a sequence of "team
+// phases": strided loops over work items (threads), warps (for column dot
+// products) or a single thread, separated by team_sync().  Under nvcc the
+// team is one CTA (tid = threadIdx.x, 32-lane warps).  Compiled by a host C++
+// compiler the same code runs with a one-thread, one-lane team, where every
+// loop visits all items in order and team_sync()/warp_sum() are identities.
+// The host build exists only so the index arithmetic can be exercised on a
+// CPU; the product path is the CUDA build.
+#pragma once
+
+#include <stdint.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define LQM_FN __device__ __forceinline__
+#define LQM_FN_NOINLINE __device__ __noinline__
+#else
+#define LQM_FN static inline
+#define LQM_FN_NOINLINE static
+#ifndef LQM_HAVE_DOUBLE2
+#define LQM_HAVE_DOUBLE2
+struct double2 { double x, y; };
+#endif
+#endif
+
+struct Team {
+  int tid, nt;    // thread index / threads in team
+  int lane, nl;   // lane index / lanes per warp
+  int wid, nw;    // warp index / warps in team
+};
+
+#if defined(__CUDACC__)
+LQM_FN Team make_team() {
+  Team t;
+  t.tid = threadIdx.x; t.nt = blockDim.x;
+  t.lane = threadIdx.x & 31; t.nl = 32;
+  t.wid = threadIdx.x >> 5; t.nw = blockDim.x >> 5;
+  return t;
+}
+LQM_FN void team_sync() { __syncthreads(); }
+LQM_FN double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+LQM_FN double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+#else
+LQM_FN Team make_host_team() { Team t = {0, 1, 0, 1, 0, 1}; return t; }
+LQM_FN void team_sync() {}
+LQM_FN double warp_sum(double v) { return v; }
+LQM_FN double warp_max(double v) { return v; }
+#endif
+
+// Deterministic team reduction: warp trees, then every thread sums the warp
+// partials in warp order.  `red` needs >= 32 doubles of shared memory.
+LQM_FN double team_sum(const Team& T, double v, double* red) {
+#if defined(__CUDACC__)
+  v = warp_sum(v);
+  if (T.lane == 0) red[T.wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < T.nw; ++w) s += red[w];
+  __syncthreads();
+  return s;
+#else
+  (void)T; (void)red;
+  return v;
+#endif
+}
+
+LQM_FN double team_max(const Team& T, double v, double* red) {
+#if defined(__CUDACC__)
+  v = warp_max(v);
+  if (T.lane == 0) red[T.wid] = v;
+  __syncthreads();
+  double s = red[0];
+  for (int w = 1; w < T.nw; ++w) s = fmax(s, red[w]);
+  __syncthreads();
+  return s;
+#else
+  (void)T; (void)red;
+  return v;
+#endif
+}
+
+// ---- complex helpers (interleaved re/im, ABI-identical to Julia ComplexF64) ----
+LQM_FN double2 cmk(double re, double im) { double2 z; z.x = re; z.y = im; return z; }
+LQM_FN double2 cadd(double2 a, double2 b) { return cmk(a.x + b.x, a.y + b.y); }
+LQM_FN double2 csub(double2 a, double2 b) { return cmk(a.x - b.x, a.y - b.y); }
+LQM_FN double2 cmul(double2 a, double2 b) { return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// conj(a) * b
+LQM_FN double2 cmulc(double2 a, double2 b) { return cmk(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x); }
+LQM_FN double2 cconj(double2 a) { return cmk(a.x, -a.y); }
+LQM_FN double2 cscale(double s, double2 a) { return cmk(s * a.x, s * a.y); }
+// a / b with Smith's scaling
+LQM_FN double2 cdiv(double2 a, double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    double r = b.y / b.x, den = b.x + b.y * r;
+    return cmk((a.x + a.y * r) / den, (a.y - a.x * r) / den);
+  } else {
+    double r = b.x / b.y, den = b.y + b.x * r;
+    return cmk((a.x * r + a.y) / den, (a.y * r - a.x) / den);
+  }
+}
+
+// (cos(pi x), sin(pi x)) — CUDA's sincospi on the device; the host
+// emulation uses the libm pair, which is only used for index checks.
+LQM_FN void lqm_sincospi(double x, double* s, double* c) {
+#if defined(__CUDACC__)
+  sincospi(x, s, c);
+#else
+  *s = sin(M_PI * x);
+  *c = cos(M_PI * x);
+#endif
+}

@@ -1,0 +1,362 @@
+"""ctypes mirror of LatticeQM's k-space routines on the ``multimode=:cuda`` path.
+
+This is the Python twin of the Julia glue (``latticeqm.jl_b200/julia/LatticeQMCUDA.jl``):
+the same names, argument meanings and layouts as the reference routines, each
+one a thin call into ``libkspace.so`` (include/kspace.h).  There is no CPU
+fallback: importing this module without the built library, or calling it
+without a CUDA device, raises.
+
+Hops are dicts ``{R (tuple of ints): ndarray (n, n) complex128}`` in the
+reference's key order (the Bloch-sum order).  k-points are fractional, shape
+(d, nk).  Arrays follow Julia's column-major layout at the C boundary.
+
+Reference (LatticeQM.jl):
+  bandmatrix / getbands        src/modules/Spectrum/bands.jl:164-204,264-267
+  getdensitymatrix!            src/modules/Operators/densitymatrix.jl:17-49
+  chemicalpotential            src/modules/Spectrum/chemicalpotential.jl:6-66
+  getdos                       src/modules/Spectrum/dos.jl:127-223
+  solvehartreefock             src/modules/Meanfield/selfconsistent.jl:19-104
+"""
+import ctypes
+import os
+from collections import namedtuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get(
+    "LQM_KSPACE_LIB", os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libkspace.so")))
+
+LQM_OK = 0
+STATUS_NAMES = {-1: "LQM_EINVAL", -2: "LQM_ECUDA", -3: "LQM_ENOMEM", -4: "LQM_ETIMEOUT",
+                -5: "LQM_ENOCONV", -6: "LQM_EDEVICE"}
+
+EXPORTS = [
+    "lqm_ctx_create", "lqm_ctx_destroy", "lqm_last_error", "lqm_ctx_set_timeout",
+    "lqm_ctx_last_kernel_ms", "lqm_hops_upload_dense", "lqm_hops_upload_csc", "lqm_hops_free",
+    "lqm_hops_dims", "lqm_bloch", "lqm_bloch_dev", "lqm_bandmatrix", "lqm_bandmatrix_dev",
+    "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
+    "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
+    "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
+]
+
+
+class LQMError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libkspace.so not built at {LIB_PATH}; run latticeqm.jl_b200/build.py")
+
+_lib = ctypes.CDLL(LIB_PATH)
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+LOG_CB = ctypes.CFUNCTYPE(ctypes.c_int, _I64, _D, _D, _D, _D, _D, _D, _D, _P)
+
+_SIG = {
+    "lqm_ctx_create": [ctypes.c_int, ctypes.POINTER(_P)],
+    "lqm_ctx_destroy": [_P],
+    "lqm_ctx_set_timeout": [_P, _D],
+    "lqm_ctx_last_kernel_ms": [_P, ctypes.POINTER(_D)],
+    "lqm_hops_upload_dense": [_P, _I64, _I64, ctypes.c_int32, _P, _P, ctypes.POINTER(_P)],
+    "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(_P)],
+    "lqm_hops_free": [_P, _P],
+    "lqm_hops_dims": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(ctypes.c_int32)],
+    "lqm_bloch": [_P, _P, _I64, _P, _P],
+    "lqm_bloch_dev": [_P, _P, _I64, _P, _P],
+    "lqm_bandmatrix": [_P, _P, _I64, _P, ctypes.c_int, ctypes.c_int, _P, _P],
+    "lqm_bandmatrix_dev": [_P, _P, _I64, _P, ctypes.c_int, ctypes.c_int, _P, _P],
+    "lqm_densitymatrix": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), ctypes.c_int],
+    "lqm_densitymatrix_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D),
+                              ctypes.c_int],
+    "lqm_chemicalpotential": [_P, _P, _I64, _P, _P, _D, _D, ctypes.POINTER(_D)],
+    "lqm_chemicalpotential_bands_dev": [_P, _I64, _I64, _P, _P, _D, _D, ctypes.POINTER(_D)],
+    "lqm_dos": [_P, _P, _I64, _P, _P, _I64, _P, _D, _P],
+    "lqm_dos_bands_dev": [_P, _I64, _I64, _P, _P, _I64, _P, _D, _P],
+    "lqm_scf_hf": [_P, _P, _P, _I64, _P, _P, _D, _D, _D, _D, _I64, _I64, _P, _P, LOG_CB, _P, _P],
+    "lqm_ctx_reset_stats": [_P, ctypes.c_int],
+    "lqm_ctx_stats": [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+    "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
+                          _P, ctypes.c_int],
+    "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
+                              _P, _P, ctypes.c_int],
+}
+for _name, _args in _SIG.items():
+    _f = getattr(_lib, _name)
+    _f.argtypes = _args
+    _f.restype = ctypes.c_int
+_lib.lqm_last_error.argtypes = [_P]
+_lib.lqm_last_error.restype = ctypes.c_char_p
+
+
+def lib():
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):  # device tensor (torch) for the _dev entry points
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(_P)
+
+
+class Context:
+    """One CUDA device + stream (``lqm_ctx``)."""
+
+    def __init__(self, device=0, timeout=None):
+        h = _P()
+        st = _lib.lqm_ctx_create(int(device), ctypes.byref(h))
+        if st != LQM_OK:
+            raise LQMError(st, f"cannot create a context on CUDA device {device}")
+        self._h = h
+        if timeout is not None:
+            self.check(_lib.lqm_ctx_set_timeout(self._h, float(timeout)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, st):
+        if st != LQM_OK:
+            raise LQMError(st, (_lib.lqm_last_error(self._h) or b"").decode())
+
+    def last_kernel_ms(self):
+        v = _D()
+        self.check(_lib.lqm_ctx_last_kernel_ms(self._h, ctypes.byref(v)))
+        return v.value
+
+    def reset_stats(self, timing=True):
+        self.check(_lib.lqm_ctx_reset_stats(self._h, int(bool(timing))))
+
+    def stats(self):
+        """(eigensolver device ms, eigensolver launches, all kernel launches) since reset."""
+        ms, el, al = _D(), _I64(), _I64()
+        self.check(_lib.lqm_ctx_stats(self._h, ctypes.byref(ms), ctypes.byref(el), ctypes.byref(al)))
+        return ms.value, el.value, al.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lqm_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context():
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def pack_hops(h):
+    """dict Hops -> (n, nR, d, keys d x nR int64 (F), blocks n x n x nR complex (F))."""
+    keys = list(h.keys())
+    mats = [np.asarray(h[R], dtype=np.complex128) for R in keys]
+    n = mats[0].shape[0]
+    d = len(keys[0])
+    K = np.asfortranarray(np.array(keys, dtype=np.int64).T)
+    B = np.asfortranarray(np.stack(mats, axis=-1))
+    return n, len(keys), d, K, B
+
+
+class DeviceHops:
+    """A Hops resident on the device (``lqm_hops``)."""
+
+    def __init__(self, h, ctx=None):
+        self.ctx = ctx or default_context()
+        n, nR, d, K, B = pack_hops(h)
+        self.n, self.nR, self.d = n, nR, d
+        self.keys = [tuple(R) for R in h.keys()]
+        out = _P()
+        self.ctx.check(_lib.lqm_hops_upload_dense(self.ctx.handle, n, nR, d, _ptr(K), _ptr(B),
+                                                  ctypes.byref(out)))
+        self._h = out
+
+    @property
+    def handle(self):
+        return self._h
+
+    def free(self):
+        if getattr(self, "_h", None):
+            _lib.lqm_hops_free(self.ctx.handle, self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _as_device_hops(H, ctx):
+    return H if isinstance(H, DeviceHops) else DeviceHops(H, ctx)
+
+
+def _ks(ks, d=None):
+    ks = np.asfortranarray(np.asarray(ks, dtype=np.float64))
+    if ks.ndim == 1:
+        ks = ks.reshape(-1, 1, order="F")
+    if d is not None and ks.shape[0] != d:
+        raise ValueError(f"k-points must have {d} rows, got {ks.shape[0]}")
+    return ks
+
+
+def _check_mode(multimode):
+    if str(multimode).lstrip(":") != "cuda":
+        raise ValueError(f"multimode={multimode!r}: this module implements only :cuda")
+
+
+def bloch(H, ks, ctx=None):
+    """H(k) for every column of ks: array (n, n, nk)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    nk = ks.shape[1]
+    out = np.zeros((Hd.n, Hd.n, nk), dtype=np.complex128, order="F")
+    ctx.check(_lib.lqm_bloch(ctx.handle, Hd.handle, nk, _ptr(ks), _ptr(out)))
+    return out
+
+
+def bandmatrix(H, ks, multimode="cuda", want_vectors=False, precision=0, ctx=None):
+    """``bandmatrix(H, ks)``: bands (n, nk) ascending per column; with
+    ``want_vectors`` also U (n, n, nk) (columns = eigenvectors)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    nk = ks.shape[1]
+    bands = np.zeros((Hd.n, nk), order="F")
+    U = np.zeros((Hd.n, Hd.n, nk), dtype=np.complex128, order="F") if want_vectors else None
+    ctx.check(_lib.lqm_bandmatrix(ctx.handle, Hd.handle, nk, _ptr(ks), int(bool(want_vectors)),
+                                  int(precision), _ptr(bands), _ptr(U)))
+    return bands, U
+
+
+BandData = namedtuple("BandData", ["bands", "obs", "path"])
+
+
+def getbands(H, ks, multimode="cuda", ctx=None):
+    """``getbands(H, ks)`` -> BandData(bands, obs, path) (no projectors)."""
+    bands, _ = bandmatrix(H, ks, multimode=multimode, ctx=ctx)
+    return BandData(bands, np.zeros(bands.shape + (0,)), ks)
+
+
+def getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, multimode="cuda", precision=0,
+                     ctx=None):
+    """``getdensitymatrix!(ρs, H, ks[, kweights], μ; T)``: overwrites every block of
+    ``rhos`` (dict keyed like Hops; only its existing keys are computed) and returns
+    the band energy sum_k w_k sum_n f eps."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    nk = ks.shape[1]
+    Lkeys = list(rhos.keys())
+    nL = len(Lkeys)
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = np.zeros((Hd.n, Hd.n, nL), dtype=np.complex128, order="F")
+    eb = _D()
+    ctx.check(_lib.lqm_densitymatrix(ctx.handle, Hd.handle, nk, _ptr(ks), _ptr(w), float(mu), float(T),
+                                     nL, _ptr(Lk), _ptr(out), ctypes.byref(eb), int(precision)))
+    for i, L in enumerate(Lkeys):
+        rhos[L] = np.array(out[:, :, i])
+    return eb.value
+
+
+def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):
+    """``chemicalpotential(H, ks, filling; T)``."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    mu = _D()
+    ctx.check(_lib.lqm_chemicalpotential(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(w),
+                                         float(filling), float(T), ctypes.byref(mu)))
+    return mu.value
+
+
+def getdos(h, omegas, ks, gamma, kweights=None, multimode="cuda", ctx=None):
+    """``getdos(h, ωs, ks; Γ)`` (no 1/π, divided by nk when unweighted)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(h, ctx)
+    ks = _ks(ks, Hd.d)
+    om = np.ascontiguousarray(omegas, dtype=np.float64)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = np.zeros(len(om))
+    ctx.check(_lib.lqm_dos(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(w), len(om), _ptr(om),
+                           float(gamma), _ptr(out)))
+    return out
+
+
+def bands_dos_rho(rhos, H, ks, omegas, gamma, kweights=None, mu=0.0, T=0.01, multimode="cuda",
+                  precision=0, ctx=None):
+    """bands + DOS + ``getdensitymatrix!`` from one eigen pass (``lqm_bands_dos_rho``).
+    Fills ``rhos`` in place; returns (bands (n, nk), dos (nw,), band energy)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    nk = ks.shape[1]
+    Lkeys = list(rhos.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    om = np.ascontiguousarray(omegas, dtype=np.float64)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    rho = np.zeros((Hd.n, Hd.n, len(Lkeys)), dtype=np.complex128, order="F")
+    bands = np.zeros((Hd.n, nk), order="F")
+    dos = np.zeros(len(om))
+    eb = _D()
+    ctx.check(_lib.lqm_bands_dos_rho(ctx.handle, Hd.handle, nk, _ptr(ks), _ptr(w), float(mu), float(T),
+                                     len(Lkeys), _ptr(Lk), _ptr(rho), ctypes.byref(eb), len(om), _ptr(om),
+                                     float(gamma), _ptr(dos), _ptr(bands), int(precision)))
+    for i, L in enumerate(Lkeys):
+        rhos[L] = np.array(rho[:, :, i])
+    return bands, dos, eb.value
+
+
+HFResult = namedtuple("HFResult", ["rho", "energy", "mf", "converged", "residual"])
+MFInfo = namedtuple("MFInfo", ["mu", "eH", "eF", "eband", "ekin", "iterations"])
+
+
+def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
+                     kweights=None, log_callback=None, multimode="cuda", ctx=None):
+    """``solvehartreefock(h, v, ρ_init, filling, ks; T, β, tol, iterations)`` with linear
+    mixing.  Returns (ρ, ϵ_GS, mf, converged, residual) like the reference."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    hd = _as_device_hops(h, ctx)
+    vd = _as_device_hops(v, ctx)
+    ks = _ks(ks, hd.d)
+    Lkeys = list(rho_init.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    rho = np.asfortranarray(np.stack([np.asarray(rho_init[L], np.complex128) for L in Lkeys], -1))
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = np.zeros(9)
+
+    def _cb(it, E, res, ekin, eband, eH, eF, mu, user):
+        if log_callback is None:
+            return 0
+        r = log_callback(int(it), E, res, dict(ekin=ekin, eband=eband, eH=eH, eF=eF, mu=mu))
+        return 1 if r is False else 0
+
+    cb = LOG_CB(_cb)
+    ctx.check(_lib.lqm_scf_hf(ctx.handle, hd.handle, vd.handle, ks.shape[1], _ptr(ks), _ptr(w),
+                              float(filling), float(T), float(beta), float(tol), int(iterations),
+                              len(Lkeys), _ptr(Lk), _ptr(rho), cb, None, _ptr(out)))
+    rho_out = {L: np.array(rho[:, :, i]) for i, L in enumerate(Lkeys)}
+    mf = MFInfo(mu=out[1], eH=out[2], eF=out[3], eband=out[4], ekin=out[5], iterations=int(out[8]))
+    return HFResult(rho_out, out[0], mf, bool(out[7]), out[6])

@@ -1,0 +1,262 @@
+"""Hopping models (Hops) restated from LatticeQM.jl (input construction for the workloads).
+
+A Hops is a Python dict ``{R (tuple of ints): ndarray (n, n) complex128}``,
+the restatement of ``Hops{K,T}`` (src/modules/TightBinding/types.jl:54-56).
+Dict insertion order is the summation order of the Bloch sum.
+"""
+import math
+import numpy as np
+
+from . import lattice as L
+
+SQRT_EPS = math.sqrt(np.finfo(float).eps)
+SIGMA0 = np.eye(2, dtype=complex)
+SIGMAX = np.array([[0, 1], [1, 0]], dtype=complex)
+SIGMAY = np.array([[0, -1j], [1j, 0]], dtype=complex)
+SIGMAZ = np.array([[1, 0], [0, -1]], dtype=complex)
+
+
+def hopdim(h):
+    return next(iter(h.values())).shape[0]
+
+
+def zerokey(h):
+    return tuple(0 for _ in next(iter(h.keys())))
+
+
+def neighbor_dict(lat, cellrange):
+    # Operators/gethops.jl:58-62 -> Lattices/neighbors.jl:153-165
+    cells = L.getneighborcells(lat.A, cellrange, halfspace=True, innerpoints=True,
+                               excludeorigin=False)
+    nall = 3 + lat.extra.shape[0]
+    out = {}
+    for c in cells:
+        da = np.zeros(nall)
+        da[:3] = lat.A @ np.array(c, float)
+        out[c] = da
+    return out
+
+
+def trim(h):
+    # TightBinding/types.jl:278-286: drop blocks that are exactly zero
+    return {R: M for R, M in h.items() if np.any(M != 0)}
+
+
+def gethops_scalar(lat, t, cellrange=2, precision=SQRT_EPS):
+    """Non-vectorized ``hops!``/``hoppingmatrix!`` (gethops.jl:86-140)."""
+    Rpos = lat.allpositions()
+    h = {}
+    for dL, da in neighbor_dict(lat, cellrange).items():
+        Ri = Rpos + da[:, None]
+        N = Rpos.shape[1]
+        M = np.zeros((N, N), dtype=complex)
+        for i in range(N):
+            for j in range(N):
+                v = t(Ri[:, i], Rpos[:, j])
+                if abs(v) >= precision:
+                    M[i, j] = v
+        h[dL] = M
+        if any(x != 0 for x in dL):
+            h[tuple(-x for x in dL)] = M.conj().T.copy()
+    return trim(h)
+
+
+def distance_window(a=1.0, halfwidth=0.01, t0=-1.0):
+    # Operators/nearestneighbor.jl:22-47 (DistanceWindowHopping, 3-D spatial norm)
+    def t(r1, r2):
+        r = float(np.linalg.norm(r1[:3] - r2[:3]))
+        return t0 if (a + halfwidth > r > a - halfwidth) else 0.0
+    return t
+
+
+def nearestneighbor(lat, t0=-1.0, a=1.0, halfwidth=0.01, cellrange=2):
+    # Operators/nearestneighbor.jl:60-62
+    return gethops_scalar(lat, distance_window(a, halfwidth, t0), cellrange=cellrange)
+
+
+def graphene_block(R1, R2, tmin=1e-5, tz=0.46, t0=1.0, linter=0.125, lintra=0.08, z=3.0,
+                   a=1.0, dmin=0.1, dmax=5.0):
+    """``addgraphenematrix!`` (Operators/graphene.jl:242-274): out[i,j] = t(R1[:,i]-R2[:,j])."""
+    d = R1[:3, :, None] - R2[:3, None, :]
+    D = np.sqrt((d * d).sum(axis=0))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        chi = d[2] ** 2 / D ** 2
+        v = -t0 * (1 - chi) * np.exp(-np.abs(D - a) / lintra) \
+            - tz * chi * np.exp(-np.abs(D - z) / linter)
+    keep = (D <= dmax) & (D >= dmin) & (np.abs(v) >= tmin)
+    return np.where(keep, v, 0.0).astype(complex)
+
+
+def graphene(lat, cellrange=2, spin=False, **kw):
+    """``Operators.graphene`` vectorized path (graphene.jl:17-28, gethops.jl:111-124)."""
+    Rpos = lat.allpositions()
+    h = {}
+    for dL, da in neighbor_dict(lat, cellrange).items():
+        M = graphene_block(Rpos + da[:, None], Rpos, **kw)
+        h[dL] = M
+        if any(x != 0 for x in dL):
+            h[tuple(-x for x in dL)] = M.conj().T.copy()
+    h = trim(h)
+    return addspin(h) if spin else h
+
+
+def addspin(h, mode="spinhalf"):
+    # TightBinding/types.jl:258-270: kron(H, sigma), spin is the fast index
+    s = {"spinhalf": SIGMA0, "σ0": SIGMA0, "σx": SIGMAX}[mode]
+    return {R: np.kron(M, s) for R, M in h.items()}
+
+
+def hermitianize(h):
+    # TightBinding/types.jl:174-189
+    for R in list(h.keys()):
+        mR = tuple(-x for x in R)
+        if mR in h:
+            h[R] = (h[R] + h[mR].conj().T) / 2
+            h[mR] = h[R].conj().T.copy()
+        else:
+            h[mR] = h[R].conj().T.copy()
+    return h
+
+
+def with_keys(h, keys):
+    """Restrict/extend a Hops to exactly ``keys`` (zero blocks kept)."""
+    n = hopdim(h)
+    for R, M in h.items():
+        if R not in keys and np.any(M != 0):
+            raise ValueError(f"nonzero block {R} outside the requested key set")
+    return {R: (h[R].copy() if R in h else np.zeros((n, n), complex)) for R in keys}
+
+
+KEYS9 = [R for R in L.product_first_fastest(range(-1, 2), range(-1, 2))]
+
+
+# --------------------------------------------------------------------------------------
+# Workload builders (seeded synthetic inputs of the named shapes)
+# --------------------------------------------------------------------------------------
+
+def honeycomb_disorder(L_super=6, sigma=0.1, seed=1):
+    """Spinful honeycomb NN model, t=-1, L_super x L_super supercell, onsite disorder
+    N(0, sigma) equal on both spins; keys = the 9 vectors of {-1,0,1}^2 (zero blocks kept).
+    n = 4 * L_super^2 (144 for the 6x6 cell)."""
+    lat = L.superlattice(L.honeycomb(), [L_super, L_super])
+    h = nearestneighbor(lat, -1.0)
+    h = with_keys(addspin(h), KEYS9)
+    rng = np.random.default_rng(seed)
+    eps = rng.normal(0.0, sigma, lat.norb)
+    h[(0, 0)] += np.diag(np.repeat(eps, 2)).astype(complex)
+    return lat, h
+
+
+def _shell_distances(lat, nshell):
+    pos = lat.positions()
+    ds = set()
+    for c in L.product_first_fastest(range(-2, 3), range(-2, 3)):
+        da = lat.A @ np.array(c, float)
+        d = np.linalg.norm(pos[:, :, None] + da[:, None, None] - pos[:, None, :], axis=0)
+        ds.update(np.round(d[d > 1e-9], 9).ravel().tolist())
+    return sorted(ds)[:nshell]
+
+
+def random_bonds(lat, rng, nshell=2, tdist=(-1.0, 1.0), onsite_sigma=0.2, soc=False):
+    """Random real NN+NNN hoppings t~U(tdist) per bond plus onsite N(0, onsite_sigma),
+    spinful.  With ``soc`` each bond carries a spin-orbit phase exp(i phi sigma_z),
+    phi~U(0, 2pi).  The Hermitian partner H_{-R} = H_R^dagger is set per bond
+    (the role of ``hermitianize!``, TightBinding/types.jl:174-189)."""
+    shells = _shell_distances(lat, nshell)
+    pos = lat.positions()
+    N = lat.norb
+    blocks = {R: np.zeros((2 * N, 2 * N), complex) for R in KEYS9}
+    for R in KEYS9:
+        mR = tuple(-x for x in R)
+        if R > mR:
+            continue  # handle each +/-R pair once (R == mR only for R = 0)
+        da = lat.A @ np.array(R, float)
+        for i in range(N):
+            for j in range(N):
+                if R == mR and j <= i:
+                    continue
+                dd = round(float(np.linalg.norm(pos[:, i] + da - pos[:, j])), 9)
+                if not any(abs(dd - s) < 1e-6 for s in shells):
+                    continue
+                t = rng.uniform(*tdist)
+                if soc:
+                    phi = rng.uniform(0.0, 2 * math.pi)
+                    blk = t * np.diag([np.exp(1j * phi), np.exp(-1j * phi)])
+                else:
+                    blk = t * SIGMA0
+                blocks[R][2 * i:2 * i + 2, 2 * j:2 * j + 2] += blk
+                blocks[mR][2 * j:2 * j + 2, 2 * i:2 * i + 2] += blk.conj().T
+    eps = rng.normal(0.0, onsite_sigma, N)
+    blocks[(0, 0)] += np.diag(np.repeat(eps, 2))
+    return blocks
+
+
+def batch_models(seed=2):
+    """The three uneven models of the batched workload: square 2x2 (n=8), kagome 2x2
+    (n=24) and triangular 4x4 with spin-orbit phases (n=96: 4x4 copies of the 3-site
+    ``triangular_supercell`` cell, 2d.jl:87-93, spinful)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    sq = L.superlattice(L.square(), [2, 2])
+    out.append(("square2x2", random_bonds(sq, rng)))
+    kg = L.superlattice(L.kagome(), [2, 2])
+    out.append(("kagome2x2", random_bonds(kg, rng)))
+    tr = L.superlattice(L.triangular_supercell(), [4, 4])
+    out.append(("triangular4x4_soc", random_bonds(tr, rng, soc=True)))
+    return out
+
+
+def hubbard_v(lat, U=4.0, a=0.5, mode="σx"):
+    """``gethubbard(lat; mode, a, U)`` (Operators/interactions.jl:18-28): onsite key only,
+    V_0 = U * kron(I_sites, sigma_x) for mode=σx."""
+    N = lat.norb
+    V = np.zeros((N, N), complex)
+    pos = lat.allpositions()
+    for i in range(N):
+        for j in range(N):
+            r = float(np.linalg.norm(pos[:3, i] - pos[:3, j]))
+            v = U * (0.0 if a - r < 0 else (1.0 if a - r > 0 else 0.5))
+            if abs(v) >= SQRT_EPS:
+                V[i, j] = v
+    return addspin({(0, 0): V}, mode)
+
+
+def triangular_hubbard(L_super=6, t=-1.0, tp=0.2, U=4.0):
+    """Spinful triangular-lattice Hubbard model on an L x L supercell (n = 2 L^2):
+    NN hopping t, NNN hopping tp, v = Hubbard(U) in the sigma_x mode."""
+    lat = L.superlattice(L.triangular(), [L_super, L_super])
+    h1 = nearestneighbor(lat, t, a=1.0)
+    h2 = nearestneighbor(lat, tp, a=math.sqrt(3.0))
+    h = {}
+    for hh in (h1, h2):
+        for R, M in hh.items():
+            h[R] = h.get(R, 0) + M
+    h = addspin(h)
+    v = hubbard_v(lat, U=U)
+    return lat, h, v
+
+
+def random_local_magnetization(n_sites, seed=3):
+    """Seeded ``mapspindensitymatrix(:random, n)`` (Meanfield/initialguess.jl:24-35,48-58,
+    68-80): per site 1/2 (sigma0 + d.sigma) with a random unit vector d."""
+    rng = np.random.default_rng(seed)
+    M = np.zeros((2 * n_sites, 2 * n_sites), complex)
+    for i in range(n_sites):
+        th = math.pi * rng.random()
+        ph = 2 * math.pi * rng.random()
+        d = [math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)]
+        M[2 * i:2 * i + 2, 2 * i:2 * i + 2] = 0.5 * (SIGMA0 + d[0] * SIGMAX + d[1] * SIGMAY
+                                                      + d[2] * SIGMAZ)
+    return M
+
+
+def tbg_slater_koster(N, **kw):
+    """Twisted bilayer (m=N, r=1) with the Slater-Koster parameters of the precision
+    workload: Vppπ=-2.7, Vppσ=+0.48, decay 0.184*a_lat (a_lat = sqrt(3) NN distances),
+    cutoff 3*a_lat; spinless, n = 4 (3N^2+3N+1)."""
+    lat = L.honeycomb_twisted(N)
+    dlt = 0.184 * math.sqrt(3.0)
+    params = dict(t0=2.7, tz=-0.48, lintra=dlt, linter=dlt, a=1.0, z=3.0,
+                  dmax=3 * math.sqrt(3.0), tmin=1e-5)
+    params.update(kw)
+    return lat, graphene(lat, **params)

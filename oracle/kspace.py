@@ -1,0 +1,173 @@
+"""k-space hot path restated from LatticeQM.jl (oracle; test infrastructure only)."""
+import math
+import struct
+
+import numpy as np
+import scipy.linalg as sla
+
+
+def fouriersum(h, k):
+    """H(k) = sum_R H_R exp(+i 2 pi k.R), summed in dict order.
+
+    TightBinding/types.jl:8 (fourierphase) and :18-25 (fouriersum!)."""
+    k = np.atleast_1d(np.asarray(k, float))
+    out = None
+    for R, M in h.items():
+        ph = np.exp(1j * 2 * math.pi * float(np.dot(k, np.array(R, float))))
+        out = M * ph if out is None else out + M * ph
+    return out
+
+
+def eigh_upper(Hk, vectors=True):
+    """LAPACK zheevr on the upper triangle, all pairs, ascending.
+
+    Eigen/Eigen.jl:22-23,32 (``eigen!(Hermitian(M))``, upper triangle), which
+    LinearAlgebra maps to ``zheevr`` (extra/benchmarks/bench_heevr.jl:38,68)."""
+    if vectors:
+        return sla.eigh(Hk, lower=False, driver="evr")
+    return sla.eigh(Hk, lower=False, driver="evr", eigvals_only=True)
+
+
+def bandmatrix(h, ks, vectors=False):
+    """bands (n, nk), optionally U (nk, n, n); Spectrum/bands.jl:164-227."""
+    n = next(iter(h.values())).shape[0]
+    nk = ks.shape[1]
+    bands = np.zeros((n, nk))
+    U = np.zeros((nk, n, n), complex) if vectors else None
+    for j in range(nk):
+        Hk = fouriersum(h, ks[:, j])
+        if vectors:
+            e, u = eigh_upper(Hk, True)
+            U[j] = u
+        else:
+            e = eigh_upper(Hk, False)
+        bands[:, j] = e
+    return bands, U
+
+
+def fermidirac(e, mu=0.0, T=0.0):
+    """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
+    with value 0.5 at equality."""
+    x = np.asarray(e, float) - mu
+    if T > 0:
+        with np.errstate(over="ignore"):
+            return 1.0 / (np.exp(x / T) + 1.0)
+    return np.where(-x < 0, 0.0, np.where(-x > 0, 1.0, 0.5))
+
+
+def chemicalpotential_0(energies, filling):
+    """Spectrum/chemicalpotential.jl:9-23."""
+    en = np.array(energies, float).ravel()
+    if filling >= 1.0:
+        return float(en.max())
+    if filling <= 0.0:
+        return float(en.min() - 1.0)
+    i = 1 + int(math.floor(filling * (len(en) - 1)))  # 1-based
+    s = np.sort(en)
+    return float((s[i - 1] + s[i]) / 2)
+
+
+def _f2u(x):
+    return struct.unpack("<Q", struct.pack("<d", abs(x)))[0]
+
+
+def _u2f(u):
+    return struct.unpack("<d", struct.pack("<Q", u))[0]
+
+
+def float_midpoint(a, b):
+    """Midpoint over the float64 total order, as Roots.jl v2's Bisection uses:
+    0.0 when the ends straddle zero, else the mean of the bit patterns of |a|,|b|
+    carrying their common sign."""
+    if (a < 0 < b) or (b < 0 < a):
+        return 0.0
+    m = _u2f((_f2u(a) + _f2u(b)) >> 1)
+    return -m if (a + b) < 0 else m
+
+
+def bisect_float(g, a, b, maxiter=200):
+    """Bracketing bisection to adjacent floats (Roots.jl v2 ``Bisection``, the
+    default of ``find_zero(f, (a, b))`` called at Spectrum/chemicalpotential.jl:37;
+    Roots is not vendored in the reference, this restates its published algorithm).
+    Returns the root to within one ulp."""
+    fa, fb = g(a), g(b)
+    if fa == 0:
+        return a
+    if fb == 0:
+        return b
+    if np.sign(fa) == np.sign(fb):
+        raise ValueError("bracket does not change sign")
+    for _ in range(maxiter):
+        m = float_midpoint(a, b)
+        if m == a or m == b:
+            break
+        fm = g(m)
+        if fm == 0:
+            return m
+        if np.sign(fm) == np.sign(fa):
+            a, fa = m, fm
+        else:
+            b, fb = m, fm
+    return a if abs(fa) <= abs(fb) else b
+
+
+def getfilling(bands, mu, T, weights=None):
+    """Spectrum/chemicalpotential.jl:74-78: unweighted mean of f over all levels,
+    or sum_k w_k sum_n f / n_bands with weights."""
+    f = fermidirac(bands, mu, T)
+    if weights is None:
+        return float(np.mean(f))
+    return float(np.sum(np.asarray(weights)[None, :] * f) / bands.shape[0])
+
+
+def chemicalpotential(bands, filling, T=0.0, weights=None):
+    """Spectrum/chemicalpotential.jl:6,32-38."""
+    if T == 0:
+        return chemicalpotential_0(bands, filling)
+    g = lambda mu: getfilling(bands, mu, T, weights) - filling
+    return bisect_float(g, float(bands.min()), float(bands.max()))
+
+
+def densitymatrix(h, ks, w, mu, T, Lkeys, return_parts=False):
+    """rho_L = sum_k w_k exp(-i 2 pi k.L) U f U^dagger and band energy sum_k w_k sum f eps.
+
+    Operators/densitymatrix.jl:28-49 (driver) and :130-145 (per-k kernel)."""
+    n = next(iter(h.values())).shape[0]
+    rho = {L: np.zeros((n, n), complex) for L in Lkeys}
+    eband = 0.0
+    for j in range(ks.shape[1]):
+        k = ks[:, j]
+        e, U = eigh_upper(fouriersum(h, k), True)
+        f = fermidirac(e, mu, T)
+        rk = (U * f[None, :]) @ U.conj().T
+        for L in Lkeys:
+            rho[L] += w[j] * np.exp(-1j * 2 * math.pi * float(np.dot(k, np.array(L, float)))) * rk
+        eband += float(np.real(w[j] * np.sum(e * f)))
+    return rho, eband
+
+
+def dos(h, ks, omegas, gamma, w=None):
+    """DOS(w) = sum_k w_k sum_n Im[1/(w - i Gamma - eps)], /L when unweighted.
+    Spectrum/dos.jl:185-188 (dos!) and :202-223 (dos_compute!)."""
+    omegas = np.asarray(omegas, float)
+    out = np.zeros_like(omegas)
+    for j in range(ks.shape[1]):
+        e = eigh_upper(fouriersum(h, ks[:, j]), False)
+        wt = 1.0 if w is None else w[j]
+        out += np.sum(np.imag(wt * 1.0 / (omegas[:, None] - 1j * gamma - e[None, :])), axis=1)
+    if w is None:
+        out /= ks.shape[1]
+    return out
+
+
+def dos_from_bands(bands, omegas, gamma, w=None):
+    """Same Lorentzian sum from precomputed bands (n, nk)."""
+    omegas = np.asarray(omegas, float)
+    nk = bands.shape[1]
+    wt = np.ones(nk) if w is None else np.asarray(w, float)
+    out = np.zeros_like(omegas)
+    for j in range(nk):
+        out += np.sum(np.imag(wt[j] / (omegas[:, None] - 1j * gamma - bands[None, :, j])), axis=1)
+    if w is None:
+        out /= nk
+    return out

@@ -1,0 +1,113 @@
+"""Hartree-Fock SCF restated from LatticeQM.jl (oracle; test infrastructure only)."""
+import numpy as np
+
+from . import kspace as K
+
+
+class HartreeFock:
+    """Meanfield/hartreefock.jl:143-175 (struct), :184-228 (call), :247-289 (fields),
+    :392-410 (energies)."""
+
+    def __init__(self, h, v):
+        self.h = h
+        self.v = v
+        self.V0 = sum(v[L] for L in v)  # hartreefock.jl:159
+        keys = list(h.keys()) + [L for L in v if L not in h]
+        n = next(iter(h.values())).shape[0]
+        self.hMF = {L: np.zeros((n, n), complex) for L in keys}
+        self.mu = 0.0
+        self.eH = self.eF = self.eband = self.ekin = 0.0
+
+    def __call__(self, rho):
+        n = next(iter(self.h.values())).shape[0]
+        # initialize_hMF! (hartreefock.jl:191-205)
+        for L in self.hMF:
+            self.hMF[L] = np.zeros((n, n), complex)
+        for L in self.h:
+            self.hMF[L] = self.hMF[L] + self.h[L]
+        # Fock: hMF[L] -= v[L] .* rho[L] (hartreefock.jl:247-276)
+        for L in self.v:
+            if L in rho:
+                self.hMF[L] = self.hMF[L] - self.v[L] * rho[L]
+        # Hartree: hMF[0][i,i] += (V0 diag rho0)_i (hartreefock.jl:278-289)
+        z = tuple(0 for _ in next(iter(rho.keys())))
+        d = self.V0 @ np.diag(rho[z])
+        self.hMF[z] = self.hMF[z] + np.diag(d)
+        # energies (hartreefock.jl:392-410)
+        nv = np.diag(rho[z])
+        self.eH = float(np.real(0.5 * (nv @ self.V0 @ nv)))
+        self.eF = float(np.real(-0.5 * sum(np.sum(rho[L] * np.conj(rho[L]) * vL)
+                                           for L, vL in self.v.items() if L in rho)))
+        return self
+
+    def doublecounting(self):
+        return self.eH + self.eF
+
+
+def hermitianize(rho):
+    # TightBinding/types.jl:174-189
+    for R in list(rho.keys()):
+        mR = tuple(-x for x in R)
+        if mR in rho:
+            rho[R] = (rho[R] + rho[mR].conj().T) / 2
+            rho[mR] = rho[R].conj().T.copy()
+        else:
+            rho[mR] = rho[R].conj().T.copy()
+    return rho
+
+
+def is_hermitian(rho, tol=np.sqrt(np.finfo(float).eps)):
+    # TightBinding/types.jl:165-172
+    for R in rho:
+        mR = tuple(-x for x in R)
+        if mR not in rho or np.max(np.abs(rho[R] - rho[mR].conj().T)) >= tol:
+            return False
+    return True
+
+
+def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
+                     iterations=500, log=None):
+    """solvehartreefock -> _scf_driver! -> fixedpoint! (linear branch).
+
+    Meanfield/selfconsistent.jl:19,62-69,256-336,366-381 and fixedpoint.jl:39-194.
+    Each iteration: hf(rho0); mu from the eigenvalues of hMF on every k;
+    rho1 = getdensitymatrix!(hMF, mu); linear mixing and the relative residual."""
+    rho0 = {L: M.copy() for L, M in rho_init.items()}
+    if not is_hermitian(rho0):
+        hermitianize(rho0)
+    rho1 = {L: M.copy() for L, M in rho0.items()}
+    hf = HartreeFock(h, v)
+    nk = ks.shape[1]
+    w = np.full(nk, 1.0 / nk)
+    converged = False
+    residual = np.inf
+    E = 0.0
+    it = 0
+    while it < iterations:
+        it += 1
+        hf(rho0)
+        bands, _ = K.bandmatrix(hf.hMF, ks)
+        hf.mu = K.chemicalpotential(bands, filling, T)
+        rho_new, eband = K.densitymatrix(hf.hMF, ks, w, hf.mu, T, list(rho1.keys()))
+        rho1 = rho_new
+        hf.eband = eband
+        hf.ekin = eband - 2 * hf.doublecounting()
+        E = eband - hf.doublecounting()
+        for L in rho0:  # fixedpoint.jl:146-148
+            rho1[L] = beta * rho1[L] + (1 - beta) * rho0[L]
+        diff = np.linalg.norm([np.linalg.norm(rho1[L] - rho0[L]) for L in rho0])
+        nrm = np.linalg.norm([np.linalg.norm(rho1[L]) for L in rho0])
+        residual = diff / nrm if nrm > np.finfo(float).eps else diff
+        for L in rho0:
+            rho0[L] = rho1[L].copy()
+        if log is not None:
+            log(it, E, residual, hf.ekin, hf.eband, hf.eH, hf.eF, hf.mu)
+        if residual < tol:
+            converged = True
+            break
+    hf(rho1)  # selfconsistent.jl:326-328
+    hf.ekin = hf.eband - 2 * hf.doublecounting()
+    E = hf.eband - hf.doublecounting()
+    if not is_hermitian(rho1):
+        hermitianize(rho1)
+    return rho1, E, hf, converged, residual, it

@@ -1,0 +1,46 @@
+"""The C-ABI library builds, loads and exports every entry point include/kspace.h declares.
+
+No compute call is made here: this file runs without a GPU.
+"""
+import ctypes
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "kspace.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lqm_\w+)\s*\(", text)) - {"lqm_scf_log_cb"})
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ["lqm_ctx_create", "lqm_bandmatrix", "lqm_densitymatrix", "lqm_chemicalpotential", "lqm_dos",
+              "lqm_scf_hf", "lqm_hops_upload_dense", "lqm_hops_upload_csc", "lqm_bloch"]:
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol(lqm):
+    lib = lqm.lib()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(lqm.EXPORTS) == set(declared_symbols())
+
+
+def test_null_arguments_are_rejected_without_a_device(lqm):
+    lib = lqm.lib()
+    assert lib.lqm_ctx_create(0, None) == -1          # LQM_EINVAL
+    assert lib.lqm_ctx_destroy(None) == -1
+    assert lib.lqm_hops_free(None, None) == -1
+    assert lib.lqm_last_error(None) == b"null context"
+
+
+def test_context_creation_reports_missing_device(lqm):
+    import torch
+    if torch.cuda.is_available():
+        return
+    h = ctypes.c_void_p()
+    st = lqm.lib().lqm_ctx_create(0, ctypes.byref(h))
+    assert st == -2 and not h.value                   # LQM_ECUDA, no CPU fallback

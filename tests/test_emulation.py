@@ -1,0 +1,90 @@
+"""CPU check of the eigensolver's team code (host build of lqm_eigh.cuh) against the oracle.
+
+The CUDA kernel and this host build share every line of bloch_build / hetrd_lower /
+dc_solve / backtransform; only the team shape differs (one thread, one lane here).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import kspace as K
+from lqm_workloads import lattice as L
+from lqm_workloads import models as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+P = ctypes.c_void_p
+
+
+@pytest.fixture(scope="module")
+def emul(tmp_path_factory):
+    out = tmp_path_factory.mktemp("emul") / "libemul.so"
+    src = os.path.join(ROOT, "tests", "native", "eigh_emul.cpp")
+    inc = os.path.join(ROOT, "latticeqm.jl_b200", "csrc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", inc, src, "-o", str(out)], check=True)
+    return ctypes.CDLL(str(out))
+
+
+def pack(h):
+    keys = np.asfortranarray(np.array(list(h.keys()), dtype=np.int64).T)
+    blocks = np.asfortranarray(np.stack([np.asarray(m, complex) for m in h.values()], axis=-1))
+    return keys, blocks
+
+
+def run(emul, h, k):
+    keys, blocks = pack(h)
+    n, nR = blocks.shape[0], blocks.shape[2]
+    kp = np.array(k, float)
+    ev = np.zeros(n)
+    U = np.zeros((n, n), complex, order="F")
+    emul.lqm_emul_eigh(n, nR, 2, blocks.ctypes.data_as(P), keys.ctypes.data_as(P), kp.ctypes.data_as(P), 1,
+                       ev.ctypes.data_as(P), U.ctypes.data_as(P), None, None)
+    return ev, U
+
+
+def models():
+    out = [("honeycomb144", M.honeycomb_disorder()[1])]
+    out += M.batch_models()
+    out.append(("tbg_n2", M.graphene(L.honeycomb_twisted(2), tz=0.32)))
+    out.append(("single", {(0, 0): np.array([[0.7]], complex), (1, 0): np.array([[0.3]], complex),
+                           (-1, 0): np.array([[0.3]], complex)}))
+    return out
+
+
+@pytest.mark.parametrize("name,h", models(), ids=lambda x: x if isinstance(x, str) else "")
+def test_emulated_eigh_matches_oracle(emul, name, h):
+    for k in [(0.0, 0.0), (1 / 3, -1 / 3), (0.123, 0.77)]:
+        ev, U = run(emul, h, k)
+        Hk = K.fouriersum(h, k)
+        ref = K.eigh_upper(Hk, vectors=False)
+        n = len(ev)
+        scale = max(ref[-1] - ref[0], 1.0)
+        assert np.max(np.abs(ev - ref)) / scale <= 1e-12
+        assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12
+        assert np.max(np.abs(Hk @ U - U * ev)) / scale <= 1e-12
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 16, 33, 64, 100])
+def test_emulated_tridiagonal_dc(emul, n):
+    rng = np.random.default_rng(n)
+    for kind in ("random", "degenerate", "glued"):
+        if kind == "random":
+            d, e = rng.normal(size=n), rng.normal(size=max(n - 1, 0))
+        elif kind == "degenerate":
+            d = np.repeat(rng.normal(size=(n + 1) // 2), 2)[:n]
+            e = np.zeros(max(n - 1, 0))
+        else:
+            d = np.abs(np.arange(n) - n // 2).astype(float)
+            e = np.full(max(n - 1, 0), 1e-9)
+        ev = np.zeros(n)
+        Z = np.zeros((n, n), order="F")
+        emul.lqm_emul_tridiag(n, d.ctypes.data_as(P), e.ctypes.data_as(P), ev.ctypes.data_as(P),
+                              Z.ctypes.data_as(P))
+        T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+        scale = max(np.max(np.abs(d)), 1.0)
+        assert np.max(np.abs(ev - np.linalg.eigvalsh(T))) <= 1e-13 * scale
+        assert np.all(np.diff(ev) >= 0)
+        assert np.max(np.abs(Z.T @ Z - np.eye(n))) <= 1e-13
+        assert np.max(np.abs(T @ Z - Z * ev)) <= 1e-13 * scale

@@ -1,0 +1,265 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle and the reference's pins.
+
+Tolerances (FP64 plain path): bands within 1e-10 of the spectral width, rho_L and
+converged mean fields within 1e-9 (absolute, entries are O(1)), mu within 1e-12.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import kspace as K
+from lqm_workloads import lattice as L
+from oracle import meanfield as MF
+from lqm_workloads import models as M
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+BAND_TOL = 1e-10
+RHO_TOL = 1e-9
+
+
+def rel_band_err(b, ref):
+    return np.max(np.abs(b - ref)) / max(np.max(ref) - np.min(ref), 1.0)
+
+
+def oracle_bands(h, ks):
+    return K.bandmatrix(h, ks)[0]
+
+
+@pytest.fixture(scope="module")
+def c1():
+    _, h = M.honeycomb_disorder()
+    return h
+
+
+# ---------------------------------------------------------------- golden pins
+def test_tbg_golden_eigenvalues(lqm, ctx):
+    pins = json.load(open(os.path.join(GOLD, "reference_pins.json")))["pins"]
+    builders = {"honeycomb_twisted": L.honeycomb_twisted, "honeycomb_twisted_ABBA": L.honeycomb_twisted_ABBA,
+                "honeycomb_twisted_ABAB": L.honeycomb_twisted_ABAB}
+    from test_oracle_pins import pin_index
+    for p in pins:
+        h = M.graphene(builders[p["builder"]](p["N"]), tz=0.32)
+        b, _ = lqm.bandmatrix(h, np.array(p["k"]).reshape(2, 1), ctx=ctx)
+        i = pin_index(p["index"], b.shape[0])
+        assert abs(b[i, 0] - p["value"]) <= p["atol"], p
+
+
+def test_graphene_analytic_bands(lqm, ctx):
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    ks = L.kpath(lat, 200)
+    b = lqm.getbands(h, ks, ctx=ctx).bands
+    from test_oracle_pins import graphene_conduction
+    up = np.array([graphene_conduction(k) for k in ks.T])
+    assert np.sum(np.abs(b[0] + up)) + np.sum(np.abs(b[1] - up)) < 1e-12
+
+
+def test_square_analytic_bands(lqm, ctx):
+    lat = L.square()
+    h = M.nearestneighbor(lat, -1.0)
+    ks = L.kpath(lat, 200)
+    b, _ = lqm.bandmatrix(h, ks, ctx=ctx)
+    ana = -2 * (np.cos(2 * np.pi * ks[0]) + np.cos(2 * np.pi * ks[1]))
+    assert np.max(np.abs(b[0] - ana)) < 1e-12
+
+
+# ---------------------------------------------------------------- bands
+def test_c1_bands_full_grid(lqm, ctx, c1):
+    ks = L.regulargrid(48 * 48)
+    b, _ = lqm.bandmatrix(c1, ks, ctx=ctx)
+    sub = np.arange(0, ks.shape[1], 7)
+    ref = oracle_bands(c1, ks[:, sub])
+    assert rel_band_err(b[:, sub], ref) <= BAND_TOL
+
+
+def test_batch_models_bands(lqm, ctx):
+    rng = np.random.default_rng(7)
+    ks = np.hstack([L.regulargrid(16 * 16), rng.random((2, 40))])
+    for name, h in M.batch_models():
+        b, _ = lqm.bandmatrix(h, ks, ctx=ctx)
+        assert rel_band_err(b, oracle_bands(h, ks)) <= BAND_TOL, name
+
+
+def test_large_n_global_scratch_path(lqm, ctx):
+    # n = 148 keeps the Householder matrix in global scratch (does not fit shared memory)
+    h = M.graphene(L.honeycomb_twisted(3), tz=0.32)
+    ks = np.array([[0.0, 1 / 3, 0.21], [0.0, -1 / 3, 0.55]])
+    b, U = lqm.bandmatrix(h, ks, want_vectors=True, ctx=ctx)
+    assert rel_band_err(b, oracle_bands(h, ks)) <= BAND_TOL
+    for j in range(ks.shape[1]):
+        Hk = K.fouriersum(h, ks[:, j])
+        assert np.max(np.abs(U[:, :, j].conj().T @ U[:, :, j] - np.eye(148))) < 1e-12
+        assert np.max(np.abs(Hk @ U[:, :, j] - U[:, :, j] * b[:, j])) < 1e-11
+
+
+def test_eigenvectors_orthonormal_residual(lqm, ctx, c1):
+    ks = L.regulargrid(6 * 6)
+    b, U = lqm.bandmatrix(c1, ks, want_vectors=True, ctx=ctx)
+    n = b.shape[0]
+    for j in range(ks.shape[1]):
+        Hk = K.fouriersum(c1, ks[:, j])
+        Uj = U[:, :, j]
+        assert np.max(np.abs(Uj.conj().T @ Uj - np.eye(n))) < 1e-12
+        assert np.max(np.abs(Hk @ Uj - Uj * b[:, j])) < 1e-11
+
+
+def test_edge_cases_small_n_and_single_k(lqm, ctx):
+    h1 = {(0, 0): np.array([[0.25]], complex), (1, 0): np.array([[-0.5]], complex),
+          (-1, 0): np.array([[-0.5]], complex)}
+    ks = np.array([[0.1, 0.5], [0.0, 0.0]])
+    b, U = lqm.bandmatrix(h1, ks, want_vectors=True, ctx=ctx)
+    assert np.allclose(b[0], 0.25 - np.cos(2 * np.pi * ks[0]), atol=1e-14)
+    assert np.allclose(np.abs(U[0, 0, :]), 1.0)
+    h = M.batch_models()[0][1]
+    b, _ = lqm.bandmatrix(h, np.array([[0.3], [0.1]]), ctx=ctx)
+    assert rel_band_err(b, oracle_bands(h, np.array([[0.3], [0.1]]))) <= BAND_TOL
+
+
+def test_bloch_sum(lqm, ctx, c1):
+    ks = np.array([[0.0, 0.25, 0.7], [0.0, 0.5, 0.11]])
+    Hk = lqm.bloch(c1, ks, ctx=ctx)
+    for j in range(3):
+        assert np.max(np.abs(Hk[:, :, j] - K.fouriersum(c1, ks[:, j]))) < 1e-13
+
+
+def test_deterministic(lqm, ctx, c1):
+    ks = L.regulargrid(8 * 8)
+    b1, _ = lqm.bandmatrix(c1, ks, ctx=ctx)
+    b2, _ = lqm.bandmatrix(c1, ks, ctx=ctx)
+    assert np.array_equal(b1, b2)
+    r1, r2 = {R: None for R in c1}, {R: None for R in c1}
+    e1 = lqm.getdensitymatrix(r1, c1, ks, mu=0.0, T=0.01, ctx=ctx)
+    e2 = lqm.getdensitymatrix(r2, c1, ks, mu=0.0, T=0.01, ctx=ctx)
+    assert e1 == e2 and all(np.array_equal(r1[R], r2[R]) for R in r1)
+
+
+# ---------------------------------------------------------------- density matrix
+def test_c1_densitymatrix(lqm, ctx, c1):
+    ks = L.regulargrid(12 * 12)
+    w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+    rho = {R: None for R in c1}
+    eb = lqm.getdensitymatrix(rho, c1, ks, mu=0.0, T=0.01, ctx=ctx)
+    ref, eb_ref = K.densitymatrix(c1, ks, w, 0.0, 0.01, list(c1.keys()))
+    for R in c1:
+        assert np.max(np.abs(rho[R] - ref[R])) <= RHO_TOL, R
+    assert abs(eb - eb_ref) <= 1e-9 * max(1.0, abs(eb_ref))
+
+
+def test_densitymatrix_weights_and_zero_T(lqm, ctx):
+    h = M.graphene(L.honeycomb(), spin=True)
+    nk = 9
+    ks = np.array([[i / nk, j / nk] for j in range(nk) for i in range(nk)]).T
+    rng = np.random.default_rng(3)
+    w = rng.random(ks.shape[1])
+    w /= w.sum()
+    rho = {R: None for R in h}
+    eb = lqm.getdensitymatrix(rho, h, ks, kweights=w, mu=-0.5, T=0.0, ctx=ctx)
+    ref, eb_ref = K.densitymatrix(h, ks, w, -0.5, 0.0, list(h.keys()))
+    for R in h:
+        assert np.max(np.abs(rho[R] - ref[R])) <= RHO_TOL
+    assert abs(eb - eb_ref) < 1e-10
+
+
+def test_batch_models_densitymatrix(lqm, ctx):
+    ks = L.regulargrid(8 * 8)
+    w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+    for name, h in M.batch_models():
+        rho = {R: None for R in h}
+        eb = lqm.getdensitymatrix(rho, h, ks, mu=0.0, T=0.01, ctx=ctx)
+        ref, eb_ref = K.densitymatrix(h, ks, w, 0.0, 0.01, list(h.keys()))
+        for R in h:
+            assert np.max(np.abs(rho[R] - ref[R])) <= RHO_TOL, (name, R)
+        assert abs(eb - eb_ref) <= 1e-9 * max(1.0, abs(eb_ref))
+
+
+# ---------------------------------------------------------------- mu, DOS
+@pytest.mark.parametrize("T,filling", [(0.01, 0.5), (0.05, 0.3), (0.0, 0.5), (0.0, 0.37), (0.0, 1.0), (0.0, 0.0)])
+def test_chemicalpotential(lqm, ctx, c1, T, filling):
+    ks = L.regulargrid(8 * 8)
+    mu = lqm.chemicalpotential(c1, ks, filling, T=T, ctx=ctx)
+    ref = K.chemicalpotential(oracle_bands(c1, ks), filling, T)
+    assert abs(mu - ref) <= 1e-12 * max(1.0, abs(ref))
+
+
+def test_dos(lqm, ctx):
+    for name, h in M.batch_models()[:2]:
+        ks = L.regulargrid(16 * 16)
+        b = oracle_bands(h, ks)
+        om = np.linspace(b.min(), b.max(), 500)
+        dos = lqm.getdos(h, om, ks, 0.05, ctx=ctx)
+        ref = K.dos_from_bands(b, om, 0.05)
+        assert np.max(np.abs(dos - ref)) <= 1e-10 * np.max(ref), name
+
+
+def test_graphene_dos_invariants(lqm, ctx):
+    h = M.nearestneighbor(L.honeycomb(), -1.0)
+    om = np.linspace(-3.05, 3.05, 401)
+    dos = lqm.getdos(h, om, L.regulargrid(120 * 120), 0.05, ctx=ctx)
+    assert np.max(np.abs(dos - dos[::-1])) / np.max(np.abs(dos)) < 1e-10
+    assert abs(np.sum(dos) * (om[1] - om[0]) - 2 * math.pi) / (2 * math.pi) < 0.05
+
+
+# ---------------------------------------------------------------- SCF
+def test_hubbard_scf_matches_oracle(lqm, ctx):
+    lat, h, v = M.triangular_hubbard(L_super=2)
+    rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=3)}
+    ks = L.regulargrid(6 * 6)
+    kw = dict(T=0.02, beta=0.3, tol=0.0, iterations=6)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, **kw)
+    rho_ref, E_ref, hf_ref, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, **kw)
+    assert res.mf.iterations == it == 6
+    assert np.max(np.abs(res.rho[(0, 0)] - rho_ref[(0, 0)])) <= RHO_TOL
+    assert abs(res.energy - E_ref) <= 1e-9
+    assert abs(res.mf.mu - hf_ref.mu) <= 1e-9
+    assert abs(res.residual - resid) <= 1e-9
+
+
+def test_hubbard_scf_converges_with_log(lqm, ctx):
+    lat, h, v = M.triangular_hubbard(L_super=2)
+    rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=5)}
+    log = []
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, L.regulargrid(6 * 6), T=0.02, beta=0.3, tol=1e-9,
+                               iterations=400, log_callback=lambda *a: log.append(a), ctx=ctx)
+    assert res.converged and res.residual < 1e-9
+    assert len(log) == res.mf.iterations
+    # energy decomposition identities at the fixed point (selfconsistent.jl:41-56)
+    assert abs(res.energy - (res.mf.eband - res.mf.eH - res.mf.eF)) < 1e-12
+    assert abs(res.mf.ekin - (res.mf.eband - 2 * (res.mf.eH + res.mf.eF))) < 1e-12
+
+
+# ---------------------------------------------------------------- errors (host-side, no device fault)
+def test_invalid_inputs_raise(lqm, ctx, c1):
+    with pytest.raises(lqm.LQMError) as e:
+        lqm.bandmatrix(c1, np.array([[np.nan], [0.0]]), ctx=ctx)
+    assert e.value.status == -1
+    with pytest.raises(lqm.LQMError):
+        lqm.bandmatrix(c1, np.zeros((2, 1)), precision=1, ctx=ctx)
+    with pytest.raises(ValueError):
+        lqm.bandmatrix(c1, np.zeros((2, 1)), multimode="serial", ctx=ctx)
+    bad = {R: m.copy() for R, m in c1.items()}
+    bad[(0, 0)][0, 0] = np.inf
+    with pytest.raises(lqm.LQMError):
+        lqm.DeviceHops(bad, ctx)
+    lat, h, v = M.triangular_hubbard(L_super=2)
+    with pytest.raises(lqm.LQMError):  # rho keys not closed under L -> -L
+        lqm.solvehartreefock(h, v, {(1, 0): np.zeros((8, 8), complex)}, 0.5, np.zeros((2, 1)), ctx=ctx)
+
+
+def test_fused_bands_dos_rho(lqm, ctx):
+    name, h = M.batch_models()[2]
+    ks = L.regulargrid(8 * 8)
+    w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+    b_ref = oracle_bands(h, ks)
+    om = np.linspace(b_ref.min(), b_ref.max(), 500)
+    rho = {R: None for R in h}
+    b, dos, eb = lqm.bands_dos_rho(rho, h, ks, om, 0.05, mu=0.0, T=0.01, ctx=ctx)
+    assert rel_band_err(b, b_ref) <= BAND_TOL
+    assert np.max(np.abs(dos - K.dos_from_bands(b_ref, om, 0.05))) <= 1e-10 * np.max(dos)
+    ref, eb_ref = K.densitymatrix(h, ks, w, 0.0, 0.01, list(h.keys()))
+    for R in h:
+        assert np.max(np.abs(rho[R] - ref[R])) <= RHO_TOL
+    assert abs(eb - eb_ref) <= 1e-9 * max(1.0, abs(eb_ref))

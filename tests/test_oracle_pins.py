@@ -1,0 +1,186 @@
+"""Pin the CPU oracle to the reference's own golden vectors and known answers.
+
+Sources (LatticeQM.jl): test/analyticbands.jl:5-16 with test/test_spectrum_graphene.jl:15-30,
+test/test_spectrum_square.jl:10-35, test/test_spectrum_triangular.jl:10-33,
+test/test_tbg.jl:52-94,213-257 (values extracted to tests/golden/reference_pins.json),
+test/test_spectrum_graphene.jl:42-63 (DOS invariants), test/test_meanfield.jl:228-278
+(HF variational identity).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import kspace as K
+from lqm_workloads import lattice as L
+from oracle import meanfield as MF
+from lqm_workloads import models as M
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def graphene_conduction(k):
+    # test/analyticbands.jl:5-16
+    rs = [[1, 0], [-1, 0], [0, 1], [0, -1], [1, -1], [-1, 1]]
+    return math.sqrt(3.0 + sum(math.cos(2 * math.pi * np.dot(k, r)) for r in rs))
+
+
+def pin_index(expr, n):
+    expr = expr.replace(" ", "")
+    table = {"end": n - 1, "end-1": n - 2, "end÷2": n // 2 - 1, "end÷2+1": n // 2}
+    return table[expr] if expr in table else int(expr) - 1
+
+
+def test_graphene_nn_bands_analytic():
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    ks = L.kpath(lat, 200)
+    b, _ = K.bandmatrix(h, ks)
+    up = np.array([graphene_conduction(k) for k in ks.T])
+    assert np.sum(np.abs(b[0] + up)) + np.sum(np.abs(b[1] - up)) < 1e-12
+
+
+def test_square_nn_bands_analytic():
+    lat = L.square()
+    h = M.nearestneighbor(lat, -1.0)
+    ks = L.kpath(lat, 200)
+    b, _ = K.bandmatrix(h, ks)
+    ana = -2 * (np.cos(2 * np.pi * ks[0]) + np.cos(2 * np.pi * ks[1]))
+    assert np.max(np.abs(b[0] - ana)) < 1e-12
+
+
+def test_triangular_nn_bands_analytic():
+    lat = L.triangular()
+    h = M.nearestneighbor(lat, -1.0)
+    ks = L.kpath(lat, 200)
+    b, _ = K.bandmatrix(h, ks)
+    ana = -2 * (np.cos(2 * np.pi * ks[0]) + np.cos(2 * np.pi * ks[1]) + np.cos(2 * np.pi * (ks[0] - ks[1])))
+    assert np.max(np.abs(b[0] - ana)) < 1e-12
+
+
+def test_tbg_lattice_fixture():
+    # test/test_tbg.jl:19-49
+    lat = L.honeycomb_twisted(1)
+    assert lat.norb == 28
+    layer = lat.extracoord("layer")
+    assert np.sum(layer == 0) == 14 and np.sum(layer == 1) == 14
+    A = lat.A
+    assert abs(np.linalg.norm(A[:, 0]) - math.sqrt(21)) < 1e-12
+    assert abs(L.twistangle(1) - math.acos(6.5 / 7)) < 1e-14
+    assert np.array_equal(L.moire_supercell(1, 1), np.array([[1, -2], [2, 3]]))
+
+
+_BUILDERS = {"honeycomb_twisted": L.honeycomb_twisted, "honeycomb_twisted_ABBA": L.honeycomb_twisted_ABBA,
+             "honeycomb_twisted_ABAB": L.honeycomb_twisted_ABAB}
+
+
+def test_tbg_eigenvalue_pins():
+    pins = json.load(open(os.path.join(GOLD, "reference_pins.json")))["pins"]
+    cache = {}
+    for p in pins:
+        key = (p["builder"], p["N"])
+        if key not in cache:
+            cache[key] = M.graphene(_BUILDERS[p["builder"]](p["N"]), tz=0.32)
+        h = cache[key]
+        ev = K.eigh_upper(K.fouriersum(h, p["k"]), vectors=False)
+        i = pin_index(p["index"], len(ev))
+        assert abs(ev[i] - p["value"]) <= p["atol"], p
+
+
+def test_tbg_near_degenerate_pair_at_K():
+    # test/test_tbg.jl:90-92
+    h = M.graphene(L.honeycomb_twisted(1), tz=0.32)
+    ev = K.eigh_upper(K.fouriersum(h, [1 / 3, -1 / 3]), vectors=False)
+    assert abs(ev[13] - ev[12]) < 1e-12 and abs(ev[14] - ev[15]) < 1e-12
+
+
+def test_graphene_dos_invariants():
+    # test/test_spectrum_graphene.jl:42-63 on a 60x60 grid (the test uses 120x120)
+    h = M.nearestneighbor(L.honeycomb(), -1.0)
+    om = np.linspace(-3.05, 3.05, 401)
+    ks = L.regulargrid(60 * 60)
+    b, _ = K.bandmatrix(h, ks)
+    dos = K.dos_from_bands(b, om, 0.05)
+    assert np.max(np.abs(dos - dos[::-1])) / np.max(np.abs(dos)) < 1e-10
+    assert abs(np.sum(dos) * (om[1] - om[0]) - 2 * math.pi) / (2 * math.pi) < 0.05
+    i0, ip, im = np.argmin(np.abs(om)), np.argmin(np.abs(om - 1)), np.argmin(np.abs(om + 1))
+    assert dos[ip] > 3 * dos[i0] and dos[im] > 3 * dos[i0]
+
+
+def test_densitymatrix_band_energy_matches_direct():
+    # test/test_operators.jl:91-128: getdensitymatrix! band energy == sum_k tr(rho_k H_k)/L
+    h = M.graphene(L.honeycomb(), spin=True)
+    nk = 9
+    ks = np.array([[i / nk, j / nk] for j in range(nk) for i in range(nk)]).T
+    mu = -0.5
+    w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+    rho, eb = K.densitymatrix(h, ks, w, mu, 0.0, list(h.keys()))
+    direct = 0.0
+    for k in ks.T:
+        Hk = K.fouriersum(h, k)
+        e, U = np.linalg.eigh(Hk)
+        rk = (U * (e < mu)) @ U.conj().T
+        direct += np.real(np.trace(rk @ Hk))
+    direct /= ks.shape[1]
+    assert abs(eb - direct) < 1e-10
+    # expval pairing sum_L tr[rho_L H_{-L}] gives the same band energy
+    ev = sum(np.real(np.trace(rho[L] @ h[tuple(-x for x in L)])) for L in rho)
+    assert abs(ev - direct) < 1e-10
+
+
+def test_hf_variational_identity_complex_rho():
+    # test/test_meanfield.jl:228-255
+    lat = L.honeycomb()
+    h = M.graphene(lat, spin=True)
+    v = M.hubbard_v(lat, U=4.0)
+    N = 4
+    ii, jj = np.meshgrid(np.arange(1, N + 1), np.arange(1, N + 1), indexing="ij")
+    Mm = np.exp(1j * (3 * ii + jj)) / (1 + np.abs(ii - jj))
+    Mm = (Mm + Mm.conj().T) / 2
+    rho = {(0, 0): Mm}
+    hf = MF.HartreeFock(h, v)(rho)
+    ks = np.array([[i / 3, j / 3] for j in range(3) for i in range(3)]).T
+
+    def trprod(A, B):
+        return sum(np.real(np.trace(K.fouriersum(A, k) @ K.fouriersum(B, k))) for k in ks.T) / ks.shape[1]
+
+    assert abs(trprod(hf.hMF, rho) - trprod(h, rho) - 2 * (hf.eH + hf.eF)) < 1e-10
+
+
+def test_float_bisection_reaches_adjacent_floats():
+    g = lambda x: x ** 3 - 2.0
+    r = K.bisect_float(g, 0.0, 3.0)
+    assert abs(r - 2 ** (1 / 3)) <= 2 * np.spacing(2 ** (1 / 3))
+    assert K.float_midpoint(-1.0, 2.0) == 0.0
+
+
+def test_chemicalpotential_zero_T_order_statistics():
+    # Spectrum/chemicalpotential.jl:9-23
+    e = np.array([[0.0, 1.0, 2.0], [3.0, 4.0, 5.0]])
+    assert K.chemicalpotential_0(e, 0.5) == 2.5
+    assert K.chemicalpotential_0(e, 1.0) == 5.0
+    assert K.chemicalpotential_0(e, 0.0) == -1.0
+
+
+def test_regulargrid_order():
+    ks = L.regulargrid(16)
+    assert ks.shape == (2, 16)
+    assert np.allclose(ks[:, 1], [0.25, 0.0]) and np.allclose(ks[:, 4], [0.0, 0.25])
+
+
+@pytest.mark.parametrize("builder,n", [("honeycomb_disorder", 144), ("batch", None), ("hubbard", 72)])
+def test_workload_shapes(builder, n):
+    if builder == "honeycomb_disorder":
+        _, h = M.honeycomb_disorder()
+        assert M.hopdim(h) == n and len(h) == 9
+    elif builder == "batch":
+        assert [M.hopdim(h) for _, h in M.batch_models()] == [8, 24, 96]
+    else:
+        _, h, v = M.triangular_hubbard()
+        assert M.hopdim(h) == n and list(v.keys()) == [(0, 0)]
+    # Hermitian as Hops
+    hh = h if builder != "batch" else M.batch_models()[2][1]
+    for R, blk in hh.items():
+        assert np.allclose(blk, hh[tuple(-x for x in R)].conj().T)
