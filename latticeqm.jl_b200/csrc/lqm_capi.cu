@@ -56,6 +56,7 @@ struct lqm_ctx {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending, ev_pool;
   double eigh_ms = 0.0;
   int64_t eigh_launches = 0, launches = 0;
+  unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
 };
 
 struct lqm_hops {
@@ -194,21 +195,30 @@ void timer_collect(lqm_ctx* ctx) {
   if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->last_ms = ms;
 }
 
-// Eigen pass over nk device k-points: bands (n x nk) and optionally U.
-void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands, double2* d_U) {
+// Fused density output of the eigen pass: rho_k = U f(eps - mu) U^H and w_k sum f eps.
+struct RhoOut {
+  double2* rhok;
+  double* ebk;
+  const double* w;
+  double mu, T;
+};
+
+// Eigen pass over nk device k-points: bands (n x nk), optionally U and/or rho_k.
+void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands, double2* d_U,
+                 const RhoOut* ro = nullptr) {
   const int n = (int)H->n;
   const DCPlan& plan = get_plan(ctx, n);
   const int nt = eigh_threads(n);
-  EighSmemLayout Ls = eigh_smem_layout(n, (int)H->nR, 1);
-  int a_in_smem = Ls.total <= 200 * 1024;
-  if (!a_in_smem) Ls = eigh_smem_layout(n, (int)H->nR, 0);
-  if (Ls.total > 227 * 1024) fail(LQM_EINVAL, "n=%d, nR=%lld exceeds the shared-memory plan", n, (long long)H->nR);
+  EighSmemLayout Ls = eigh_smem_layout(n, (int)H->nR, nt, 1);
+  const int a_in_smem = Ls.total <= 225 * 1024;
+  if (!a_in_smem) Ls = eigh_smem_layout(n, (int)H->nR, nt, 0);
+  if (Ls.total > 225 * 1024) fail(LQM_EINVAL, "n=%d, nR=%lld exceeds the shared-memory plan", n, (long long)H->nR);
   ck(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total), "smem attr");
   int per_sm = 0;
   ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_kernel, nt, Ls.total), "occupancy");
   if (per_sm < 1) fail(LQM_EINVAL, "eigh kernel cannot be resident for n=%d", n);
-  const int64_t nn = (int64_t)n * n;
-  const int64_t slot = (a_in_smem ? 3 : 5) * nn;
+  const bool need_uwork = ro && !d_U && !a_in_smem;
+  const int64_t slot = eigh_slot_doubles(n, a_in_smem, need_uwork);
   int64_t grid = std::min<int64_t>(nk, (int64_t)per_sm * ctx->num_sms);
   // keep the scratch below ~16 GB
   const int64_t max_slots = std::max<int64_t>(1, (int64_t)(16.0e9 / (8.0 * (double)slot)));
@@ -218,6 +228,12 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   a.n = n; a.nR = (int)H->nR; a.dim = H->d; a.blocks = H->blocks; a.keys = H->keys;
   a.nk = nk; a.ks = d_ks; a.plan = plan; a.scratch = scratch; a.slot_doubles = slot;
   a.a_in_smem = a_in_smem; a.bands = d_bands; a.U = d_U;
+  a.rhok = ro ? ro->rhok : nullptr;
+  a.eband_k = ro ? ro->ebk : nullptr;
+  a.w = ro ? ro->w : nullptr;
+  a.mu = ro ? ro->mu : 0.0;
+  a.T = ro ? ro->T : 0.0;
+  a.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
   std::pair<cudaEvent_t, cudaEvent_t> evs{};
   if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
   eigh_kernel<<<(unsigned)grid, nt, Ls.total, ctx->stream>>>(a);
@@ -228,7 +244,7 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
 }
 
 int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
-  const double per_k = 32.0 * (double)n * (double)n;
+  const double per_k = 16.0 * (double)n * (double)n;
   int64_t b = (int64_t)(budget_bytes / per_k);
   return std::max<int64_t>(1, std::min(b, nk));
 }
@@ -240,8 +256,7 @@ void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
                  double* bands_out = nullptr) {
   const int n = (int)H->n;
   const int64_t nn = (int64_t)n * n;
-  const int64_t B = batch_size_for(n, nk, 8.0e9);
-  double2* U = (double2*)ws_get(ctx, WS_U, (size_t)B * nn * sizeof(double2));
+  const int64_t B = batch_size_for(n, nk, 4.0e9);
   double2* rk = (double2*)ws_get(ctx, WS_RHOK, (size_t)B * nn * sizeof(double2));
   double* bandsb = bands_out ? nullptr : (double*)ws_get(ctx, WS_BANDS, (size_t)B * n * sizeof(double));
   double* ebk = (double*)ws_get(ctx, WS_EBK, (size_t)B * sizeof(double));
@@ -249,19 +264,15 @@ void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   for (int64_t k0 = 0; k0 < nk; k0 += B) {
     const int64_t nb = std::min(B, nk - k0);
     double* bands = bands_out ? bands_out + k0 * n : bandsb;
-    launch_eigh(ctx, H, nb, d_ks + k0 * H->d, bands, U);
-    const int nt = 256;
-    const size_t sm = (size_t)(n + 32) * sizeof(double);
-    const int64_t g = std::min<int64_t>(nb, (int64_t)ctx->num_sms * 8);
-    rhok_kernel<<<(unsigned)g, nt, sm, ctx->stream>>>(n, nb, U, bands, mu, T, d_w + k0, rk, ebk);
-    ck(cudaGetLastError(), "rhok_kernel launch");
+    const RhoOut ro{rk, ebk, d_w + k0, mu, T};
+    launch_eigh(ctx, H, nb, d_ks + k0 * H->d, bands, nullptr, &ro);
     ordered_sum_kernel<<<1, 256, 0, ctx->stream>>>(ebk, nb, d_eb, k0 > 0);
     fold_coef_kernel<<<(unsigned)std::min<int64_t>((nb * nL + 255) / 256, 4096), 256, 0, ctx->stream>>>(
         nb, H->d, d_ks + k0 * H->d, d_w + k0, (int)nL, d_Lkeys, coef);
     const int64_t gf = std::min<int64_t>((nn + 255) / 256, (int64_t)ctx->num_sms * 8);
     fold_kernel<16><<<(unsigned)gf, 256, 0, ctx->stream>>>(nn, nb, rk, coef, (int)nL, d_rho, k0 > 0);
     ck(cudaGetLastError(), "fold_kernel launch");
-    ctx->launches += 4;
+    ctx->launches += 3;
   }
 }
 
@@ -389,6 +400,7 @@ int lqm_ctx_destroy(lqm_ctx* ctx) {
   for (auto& b : ctx->ws)
     if (b.p) cudaFree(b.p);
   for (auto& kv : ctx->plans) cudaFree(kv.second.d_buf);
+  if (ctx->d_phase) cudaFree(ctx->d_phase);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaStreamDestroy(ctx->stream);
@@ -413,10 +425,24 @@ int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms) {
 int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing) {
   return guarded(ctx, [&] {
     wait_stream(ctx);
+    if (!ctx->d_phase) ck(cudaMalloc(&ctx->d_phase, PH_COUNT * sizeof(unsigned long long)), "cudaMalloc(stats)");
+    ck(cudaMemset(ctx->d_phase, 0, PH_COUNT * sizeof(unsigned long long)), "memset(stats)");
     ctx->stats_on = enable_timing != 0;
     ctx->eigh_ms = 0.0;
     ctx->eigh_launches = 0;
     ctx->launches = 0;
+  });
+}
+
+int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles) {
+  return guarded(ctx, [&] {
+    if (!cycles) fail(LQM_EINVAL, "null output");
+    unsigned long long h[PH_COUNT] = {0};
+    if (ctx->d_phase) {
+      wait_stream(ctx);
+      ck(cudaMemcpy(h, ctx->d_phase, sizeof(h), cudaMemcpyDeviceToHost), "D2H");
+    }
+    for (int i = 0; i < 5; ++i) cycles[i] = (double)h[i];
   });
 }
 

@@ -34,11 +34,12 @@ struct DCPlan {
 struct EighVec {
   double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;
   int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
-  double2 *tau, *v, *w, *bc;
+  double2 *tau, *v, *w, *vn, *pn, *bc, *pbuf;
 };
 
 // ---------------------------------------------------------------------------
 // 1. Bloch sum.  blocks: nR x (n x n) column-major complex; keys: d x nR int64.
+// Column j by warp, rows i <= j by lane; the lower triangle is the mirror.
 // ---------------------------------------------------------------------------
 LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __restrict__ blocks,
                         const int64_t* __restrict__ keys, const double* kpt, double2* ph,
@@ -52,95 +53,161 @@ LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __
   }
   team_sync();
   const int64_t nn = (int64_t)n * n;
-  for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
-    int i = (int)(idx % n), j = (int)(idx / n);
-    if (i > j) continue;
-    double2 acc = cmk(0.0, 0.0);
-    for (int r = 0; r < nR; ++r) acc = cadd(acc, cmul(blocks[(int64_t)r * nn + idx], ph[r]));
-    if (i == j) {
-      A[i + (int64_t)j * lda] = cmk(acc.x, 0.0);
-    } else {
-      A[i + (int64_t)j * lda] = acc;
-      A[j + (int64_t)i * lda] = cconj(acc);
+  for (int j = T.wid; j < n; j += T.nw) {
+    for (int i = T.lane; i <= j; i += T.nl) {
+      const int64_t idx = i + (int64_t)j * n;
+      double2 acc = cmk(0.0, 0.0);
+      for (int r = 0; r < nR; ++r) acc = cadd(acc, cmul(blocks[(int64_t)r * nn + idx], ph[r]));
+      if (i == j) {
+        A[i + (int64_t)j * lda] = cmk(acc.x, 0.0);
+      } else {
+        A[i + (int64_t)j * lda] = acc;
+        A[j + (int64_t)i * lda] = cconj(acc);
+      }
     }
   }
   team_sync();
 }
 
 // ---------------------------------------------------------------------------
-// 2. Householder tridiagonalisation (lower storage, full Hermitian updates).
-// Out: d[n], e[n-1] (real), tau[n-1]; reflector j is A[j+1.., j] with v0 = 1.
+// 2. Householder tridiagonalisation (lower storage, LAPACK zhetd2/zlarfg
+// conventions).  The rank-2 update of step j and the mat-vec of step j+1 are
+// one pass over the trailing block, so each element is read and written once
+// per step.  Out: d[n], e[n-1] (real), tau[n-1]; reflector j is A[j+1.., j]
+// with v0 = 1.
 // ---------------------------------------------------------------------------
+
+// Reflector of column j (rows j+1..n-1): tau[j], e[j] = beta, d[j] = Re A[j,j];
+// v (v0 = 1) goes to vout and back into the column.
+LQM_FN void make_reflector(const Team& T, int n, int j, double2* A, int lda, EighVec& S, double2* vout) {
+  const int m = n - j - 1;
+  double2* col = A + (j + 1) + (int64_t)j * lda;
+  double s = 0.0;
+  for (int r = 1 + T.tid; r < m; r += T.nt) { const double2 x = col[r]; s += x.x * x.x + x.y * x.y; }
+  s = team_sum(T, s, S.red);
+  if (T.tid == 0) {
+    const double2 alpha = col[0];
+    double2 tj, scal;
+    double beta;
+    if (s == 0.0 && alpha.y == 0.0) {
+      tj = cmk(0.0, 0.0); scal = cmk(0.0, 0.0); beta = alpha.x;
+    } else {
+      const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s);
+      beta = (alpha.x >= 0.0) ? -nrm : nrm;
+      tj = cmk((beta - alpha.x) / beta, -alpha.y / beta);
+      scal = cdiv(cmk(1.0, 0.0), cmk(alpha.x - beta, alpha.y));
+    }
+    S.tau[j] = tj;
+    S.e[j] = beta;
+    S.d[j] = A[j + (int64_t)j * lda].x;
+    S.bc[1] = scal;
+  }
+  team_sync();
+  const double2 scal = S.bc[1];
+  for (int r = T.tid; r < m; r += T.nt) {
+    const double2 x = (r == 0) ? cmk(1.0, 0.0) : cmul(scal, col[r]);
+    vout[r] = x;
+    col[r] = x;
+  }
+  team_sync();
+}
+
+// One pass over the trailing block B (order mb, leading dimension lda):
+//   upd:  B[r,c] -= v[r+1] conj(w[c+1]) + w[r+1] conj(v[c+1])   (previous reflector,
+//         whose vectors start one row above B)
+//   p[r] = tau * sum_c B[r,c] x[c]                               (next reflector)
+// Rows across lanes (up to 4 per lane and pass), columns across warps; warp
+// partial sums are added in warp order.
+LQM_FN void trailing_pass(const Team& T, int mb, double2* B, int lda, const double2* v, const double2* w,
+                          bool upd, const double2* x, double2 tau, double2* p, double2* pbuf, int pstride) {
+  for (int r0 = 0; r0 < mb; r0 += 4 * T.nl) {
+    double2 acc[4], vr[4], wr[4];
+    int rr[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      rr[q] = r0 + q * T.nl + T.lane;
+      acc[q] = cmk(0.0, 0.0);
+      vr[q] = cmk(0.0, 0.0);
+      wr[q] = cmk(0.0, 0.0);
+      if (upd && rr[q] < mb) { vr[q] = v[rr[q] + 1]; wr[q] = w[rr[q] + 1]; }
+    }
+    for (int c = T.wid; c < mb; c += T.nw) {
+      const double2 xc = x[c];
+      double2 cw = cmk(0.0, 0.0), cv = cmk(0.0, 0.0);
+      if (upd) { cw = cconj(w[c + 1]); cv = cconj(v[c + 1]); }
+      double2* Bc = B + (int64_t)c * lda;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = rr[q];
+        if (r < mb) {
+          double2 a = Bc[r];
+          if (upd) {
+            a = csub(a, cadd(cmul(vr[q], cw), cmul(wr[q], cv)));
+            if (r == c) a.y = 0.0;
+            Bc[r] = a;
+          }
+          acc[q] = cadd(acc[q], cmul(a, xc));
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (rr[q] < mb) pbuf[T.wid * pstride + rr[q]] = acc[q];
+  }
+  team_sync();
+  for (int r = T.tid; r < mb; r += T.nt) {
+    double2 s = cmk(0.0, 0.0);
+    for (int wv = 0; wv < T.nw; ++wv) s = cadd(s, pbuf[wv * pstride + r]);
+    p[r] = cmul(tau, s);
+  }
+  team_sync();
+}
+
 LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, EighVec& S) {
+  if (n == 1) {
+    if (T.tid == 0) S.d[0] = A[0].x;
+    team_sync();
+    return;
+  }
+  double2* v = S.v;
+  double2* vn = S.vn;
+  double2* w = S.w;
+  double2* p = S.pn;
+  make_reflector(T, n, 0, A, lda, S, v);
+  trailing_pass(T, n - 1, A + 1 + lda, lda, v, w, false, v, S.tau[0], p, S.pbuf, n);
   for (int j = 0; j < n - 1; ++j) {
     const int m = n - j - 1;
-    double2* col = A + (j + 1) + (int64_t)j * lda;
-    double2* A22 = A + (j + 1) + (int64_t)(j + 1) * lda;
-    double s = 0.0;
-    for (int r = 1 + T.tid; r < m; r += T.nt) { double2 x = col[r]; s += x.x * x.x + x.y * x.y; }
-    s = team_sum(T, s, S.red);
-    if (T.tid == 0) {
-      double2 alpha = col[0];
-      double2 tj, scal;
-      double beta;
-      if (s == 0.0 && alpha.y == 0.0) {
-        tj = cmk(0.0, 0.0); scal = cmk(0.0, 0.0); beta = alpha.x;
-      } else {
-        double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s);
-        beta = (alpha.x >= 0.0) ? -nrm : nrm;
-        tj = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-        scal = cdiv(cmk(1.0, 0.0), cmk(alpha.x - beta, alpha.y));
-      }
-      S.tau[j] = tj;
-      S.e[j] = beta;
-      S.d[j] = A[j + (int64_t)j * lda].x;
-      S.bc[0] = tj; S.bc[1] = scal;
-    }
-    team_sync();
-    const double2 tj = S.bc[0], scal = S.bc[1];
-    for (int r = T.tid; r < m; r += T.nt) {
-      double2 x = (r == 0) ? cmk(1.0, 0.0) : cmul(scal, col[r]);
-      S.v[r] = x;
-      col[r] = x;
-    }
-    team_sync();
-    // p = tau * A22 v, using Hermiticity: (A22 v)_c = sum_r conj(A22[r,c]) v_r
-    for (int c = T.wid; c < m; c += T.nw) {
-      const double2* Ac = A22 + (int64_t)c * lda;
-      double sr = 0.0, si = 0.0;
-      for (int r = T.lane; r < m; r += T.nl) {
-        double2 a = Ac[r], x = S.v[r];
-        sr += a.x * x.x + a.y * x.y;
-        si += a.x * x.y - a.y * x.x;
-      }
-      sr = warp_sum(sr); si = warp_sum(si);
-      if (T.lane == 0) S.w[c] = cmul(tj, cmk(sr, si));
-    }
-    team_sync();
+    const double2 tj = S.tau[j];
+    // w = p + alpha v with alpha = -1/2 tau (p^H v)
     double pr = 0.0, pi = 0.0;
     for (int r = T.tid; r < m; r += T.nt) {
-      double2 p = cmulc(S.w[r], S.v[r]);  // conj(w) v
-      pr += p.x; pi += p.y;
+      const double2 c = cmulc(p[r], v[r]);
+      pr += c.x; pi += c.y;
     }
     pr = team_sum(T, pr, S.red);
     pi = team_sum(T, pi, S.red);
-    const double2 alpha2 = cmul(cmk(-0.5 * tj.x, -0.5 * tj.y), cmk(pr, pi));
-    for (int r = T.tid; r < m; r += T.nt) S.w[r] = cadd(S.w[r], cmul(alpha2, S.v[r]));
+    const double2 alpha = cmul(cmk(-0.5 * tj.x, -0.5 * tj.y), cmk(pr, pi));
+    for (int r = T.tid; r < m; r += T.nt) w[r] = cadd(p[r], cmul(alpha, v[r]));
     team_sync();
-    const int64_t mm = (int64_t)m * m;
-    for (int64_t idx = T.tid; idx < mm; idx += T.nt) {
-      int r = (int)(idx % m), c = (int)(idx / m);
-      double2 vr = S.v[r], wr = S.w[r], vc = S.v[c], wc = S.w[c];
-      double2 upd = cadd(cmul(vr, cconj(wc)), cmul(wr, cconj(vc)));
-      double2* a = A22 + r + (int64_t)c * lda;
-      double2 nv = csub(*a, upd);
-      if (r == c) nv.y = 0.0;
-      *a = nv;
+    // column j+1 of the trailing matrix (rows j+1..n-1) gets update j first
+    double2* c1 = A + (j + 1) + (int64_t)(j + 1) * lda;
+    const double2 cw0 = cconj(w[0]), cv0 = cconj(v[0]);
+    for (int r = T.tid; r < m; r += T.nt) {
+      double2 a = csub(c1[r], cadd(cmul(v[r], cw0), cmul(w[r], cv0)));
+      if (r == 0) a.y = 0.0;
+      c1[r] = a;
     }
     team_sync();
+    if (j + 1 < n - 1) {
+      make_reflector(T, n, j + 1, A, lda, S, vn);
+      trailing_pass(T, m - 1, A + (j + 2) + (int64_t)(j + 2) * lda, lda, v, w, true, vn, S.tau[j + 1], p, S.pbuf,
+                    n);
+      double2* t = v; v = vn; vn = t;
+    } else {
+      if (T.tid == 0) S.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda].x;
+      team_sync();
+    }
   }
-  if (T.tid == 0) S.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda].x;
-  team_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -267,15 +334,18 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
   double scale = 1.0;
   if (mx > 0.0) { int ex; frexp(mx, &ex); scale = ldexp(1.0, ex); }
   const double inv = 1.0 / scale;
-  for (int i = T.tid; i < n; i += T.nt) { S.D[i] = S.d[i] * inv; if (i < n - 1) S.e[i] *= inv; }
-  for (int64_t idx = T.tid; idx < nn; idx += T.nt) Q[idx] = ((idx % n) == (idx / n)) ? 1.0 : 0.0;
-  team_sync();
-  for (int nd = T.tid; nd < P.nnodes; nd += T.nt) {
-    const int m = P.mid[nd];
-    const double b = fabs(S.e[m - 1]);
-    S.D[m - 1] -= b;
-    S.D[m] -= b;
+  // Tearing: the leaves are single rows, so every boundary (i, i+1) is the
+  // split point of exactly one merge node and row i loses |e[i-1]| + |e[i]|.
+  // Each row is written by its own thread (no shared read-modify-write).
+  for (int i = T.tid; i < n; i += T.nt) {
+    const double el = (i > 0) ? fabs(S.e[i - 1] * inv) : 0.0;
+    const double er = (i < n - 1) ? fabs(S.e[i] * inv) : 0.0;
+    S.D[i] = (S.d[i] * inv - el) - er;
   }
+  team_sync();
+  for (int i = T.tid; i < n - 1; i += T.nt) S.e[i] *= inv;
+  for (int c = T.wid; c < n; c += T.nw)
+    for (int r = T.lane; r < n; r += T.nl) Q[r + (int64_t)c * n] = (r == c) ? 1.0 : 0.0;
   team_sync();
   for (int h = 0; h < P.nheights; ++h) {
     const int h0 = P.hstart[h], h1 = P.hstart[h + 1];
@@ -382,29 +452,31 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.newpos[i] = lo + cnt;
     }
     team_sync();
-    // H: eigenvector update into Qt
-    for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
-      const int r = (int)(idx % n), c = (int)(idx / n);
-      const int nd = own[r];
-      if (nd < 0 || own[c] != nd) continue;
-      const int lo = P.lo[nd], it = c - lo, k = S.nk[nd];
-      double acc;
+    // H: eigenvector update into Qt (column c by warp, rows of its node by lane)
+    for (int c = T.wid; c < n; c += T.nw) {
+      const int nd = own[c];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];
+      double* dst = Qt + (int64_t)S.newpos[c] * n;
       if (it < k) {
-        acc = 0.0;
         const double* uc = Us + lo + (int64_t)(lo + it) * n;
-        for (int p = 0; p < k; ++p) acc += Q[r + (int64_t)S.colnd[lo + p] * n] * uc[p];
+        for (int r = lo + T.lane; r < hi; r += T.nl) {
+          double acc = 0.0;
+          for (int p = 0; p < k; ++p) acc += Q[r + (int64_t)S.colnd[lo + p] * n] * uc[p];
+          dst[r] = acc;
+        }
       } else {
-        acc = Q[r + (int64_t)S.dcol[lo + it - k] * n];
+        const double* src = Q + (int64_t)S.dcol[lo + it - k] * n;
+        for (int r = lo + T.lane; r < hi; r += T.nl) dst[r] = src[r];
       }
-      Qt[r + (int64_t)S.newpos[c] * n] = acc;
     }
     team_sync();
     // I: write back
-    for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
-      const int r = (int)(idx % n), c = (int)(idx / n);
-      const int nd = own[r];
-      if (nd < 0 || own[c] != nd) continue;
-      Q[idx] = Qt[idx];
+    for (int c = T.wid; c < n; c += T.nw) {
+      const int nd = own[c];
+      if (nd < 0) continue;
+      const int lo = P.lo[nd], hi = P.hi[nd];
+      for (int r = lo + T.lane; r < hi; r += T.nl) Q[r + (int64_t)c * n] = Qt[r + (int64_t)c * n];
     }
     for (int i = T.tid; i < n; i += T.nt) {
       if (own[i] < 0) continue;
@@ -417,41 +489,86 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 }
 
 // ---------------------------------------------------------------------------
-// 4. Back-transformation U = H_0 ... H_{n-2} Q  (U complex n x n, ld ldu).
+// 4. Back-transformation U = H_0 ... H_{n-2} U, U holding Q on entry.
+// Reflector j is R[j+1.., j] (v0 = 1).  y = tau v^H U uses G = nt/n thread
+// groups per column (partials added in group order), the update runs column
+// by warp, rows by lane.
 // ---------------------------------------------------------------------------
-LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* A, int lda, EighVec& S,
-                                   const double* Q, double2* U, int64_t ldu) {
-  const int64_t nn = (int64_t)n * n;
-  for (int64_t idx = T.tid; idx < nn; idx += T.nt) {
-    const int r = (int)(idx % n), c = (int)(idx / n);
-    U[r + c * ldu] = cmk(Q[idx], 0.0);
-  }
-  team_sync();
+LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int ldr, EighVec& S, double2* U,
+                                   int ldu) {
+  const int G = (T.nt >= n) ? T.nt / n : 1;
   for (int j = n - 2; j >= 0; --j) {
     const int m = n - j - 1;
     const double2 tj = S.tau[j];
     if (tj.x == 0.0 && tj.y == 0.0) continue;
-    const double2* v = A + (j + 1) + (int64_t)j * lda;
-    for (int r = T.tid; r < m; r += T.nt) S.v[r] = v[r];
+    for (int r = T.tid; r < m; r += T.nt) S.v[r] = R[(j + 1 + r) + (int64_t)j * ldr];
     team_sync();
-    // y_c = v^H U[j+1.., c]
-    for (int c = T.wid; c < n; c += T.nw) {
-      const double2* Uc = U + (j + 1) + c * ldu;
+    for (int t = T.tid; t < G * n; t += T.nt) {
+      const int c = t % n, g = t / n;
+      const double2* Uc = U + (j + 1) + (int64_t)c * ldu;
       double sr = 0.0, si = 0.0;
-      for (int r = T.lane; r < m; r += T.nl) {
-        double2 p = cmulc(S.v[r], Uc[r]);
-        sr += p.x; si += p.y;
+      for (int r = g; r < m; r += G) {
+        const double2 q = cmulc(S.v[r], Uc[r]);
+        sr += q.x; si += q.y;
       }
-      sr = warp_sum(sr); si = warp_sum(si);
-      if (T.lane == 0) S.w[c] = cmul(tj, cmk(sr, si));
+      S.pbuf[g * n + c] = cmk(sr, si);
     }
     team_sync();
-    const int64_t mn = (int64_t)m * n;
-    for (int64_t idx = T.tid; idx < mn; idx += T.nt) {
-      const int r = (int)(idx % m), c = (int)(idx / m);
-      double2* u = U + (j + 1 + r) + c * ldu;
-      *u = csub(*u, cmul(S.v[r], S.w[c]));
+    for (int c = T.tid; c < n; c += T.nt) {
+      double2 s = cmk(0.0, 0.0);
+      for (int g = 0; g < G; ++g) s = cadd(s, S.pbuf[g * n + c]);
+      S.w[c] = cmul(tj, s);
+    }
+    team_sync();
+    for (int c = T.wid; c < n; c += T.nw) {
+      double2* Uc = U + (j + 1) + (int64_t)c * ldu;
+      const double2 wc = S.w[c];
+      for (int r = T.lane; r < m; r += T.nl) Uc[r] = csub(Uc[r], cmul(S.v[r], wc));
     }
     team_sync();
   }
+}
+
+// ---------------------------------------------------------------------------
+// 5. rho_k = U diag(f) U^H into out (n x n, leading dimension ldo).
+// Rows by lane (up to 4 per lane and pass), 4 columns per warp step; every
+// output entry accumulates over j in order.
+// ---------------------------------------------------------------------------
+LQM_FN_NOINLINE void rho_from_U(const Team& T, int n, const double2* U, int ldu, const double* f, double2* out,
+                                int64_t ldo) {
+  for (int r0 = 0; r0 < n; r0 += 4 * T.nl) {
+    for (int c0 = 4 * T.wid; c0 < n; c0 += 4 * T.nw) {
+      double2 acc[4][4];
+      int rr[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        rr[q] = r0 + q * T.nl + T.lane;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[q][b] = cmk(0.0, 0.0);
+      }
+      for (int j = 0; j < n; ++j) {
+        const double fj = f[j];
+        if (fj == 0.0) continue;
+        const double2* Uj = U + (int64_t)j * ldu;
+        double2 cb[4], ua[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int c = c0 + b;
+          cb[b] = (c < n) ? cscale(fj, cconj(Uj[c])) : cmk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ua[q] = (rr[q] < n) ? Uj[rr[q]] : cmk(0.0, 0.0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[q][b] = cadd(acc[q][b], cmul(ua[q], cb[b]));
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (rr[q] < n && c0 + b < n) out[rr[q] + (int64_t)(c0 + b) * ldo] = acc[q][b];
+    }
+  }
+  team_sync();
 }

@@ -5,28 +5,40 @@
 
 namespace lqm {
 
-// Shared-memory layout of eigh_kernel for order n, nR hopping keys.
+// Shared-memory layout of eigh_kernel for order n, nR hopping keys, nt threads.
+// With a_in_smem the Hermitian matrix lives in shared memory (leading
+// dimension n+1, so column-strided double2 accesses do not conflict); the same
+// region later holds the divide-and-conquer Q/Qt pair and then U.
 struct EighSmemLayout {
   size_t offA, offC, offD, offI, total;
-  int a_in_smem;
+  int a_in_smem, pbuf_len;
 };
 
 __host__ __device__ inline size_t lqm_align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-__host__ __device__ inline EighSmemLayout eigh_smem_layout(int n, int nR, int a_in_smem) {
+__host__ __device__ inline EighSmemLayout eigh_smem_layout(int n, int nR, int nt, int a_in_smem) {
   EighSmemLayout L;
   L.a_in_smem = a_in_smem;
+  const int nw = nt / 32;
+  L.pbuf_len = (nw * n > nt) ? nw * n : nt;
   size_t off = 0;
   L.offA = off;
-  if (a_in_smem) off += lqm_align16((size_t)n * n * 16);
-  L.offC = off;                                      // double2: tau, v, w (n each), bc (2), ph (nR)
-  off += lqm_align16((size_t)(3 * n + 2 + nR) * 16);
-  L.offD = off;                                      // doubles: 13 n + 32 (red) + 4 (kpt)
+  if (a_in_smem) off += lqm_align16((size_t)n * (n + 1) * 16);
+  L.offC = off;  // double2: tau, v, w, vn, pn (n each), bc (2), ph (nR), pbuf
+  off += lqm_align16((size_t)(5 * n + 2 + nR + L.pbuf_len) * 16);
+  L.offD = off;  // doubles: 13 n + 32 (red) + 4 (kpt)
   off += lqm_align16((size_t)(13 * n + 36) * 8);
-  L.offI = off;                                      // ints: 10 n
+  L.offI = off;  // ints: 10 n
   off += lqm_align16((size_t)(10 * n) * 4);
   L.total = off;
   return L;
+}
+
+// doubles of global scratch per CTA
+__host__ __device__ inline int64_t eigh_slot_doubles(int n, int a_in_smem, bool need_uwork) {
+  const int64_t nn = (int64_t)n * n;
+  if (a_in_smem) return 4 * nn;                  // R (2nn) | Qs | Us
+  return 5 * nn + (need_uwork ? 2 * nn : 0);     // A (2nn) | Q | Qt | Us | U work
 }
 
 struct EighArgs {
@@ -40,47 +52,131 @@ struct EighArgs {
   int64_t slot_doubles;
   int a_in_smem;
   double* bands;          // n x nk
-  double2* U;             // n x n x nk, or null for eigenvalues only
+  double2* U;             // n x n x nk, or null
+  double2* rhok;          // n x n x nk: U f(eps - mu) U^H, or null
+  double* eband_k;        // nk: w_k sum_j f_j eps_j (with rhok)
+  const double* w;        // nk weights (with rhok)
+  double mu, T;
+  unsigned long long* phase_cycles;  // [8] per-phase SM cycles summed over CTAs, or null
 };
+
+enum { PH_BLOCH = 0, PH_HETRD = 1, PH_DC = 2, PH_BACK = 3, PH_OUT = 4, PH_COUNT = 8 };
+
+__device__ __forceinline__ double fermi(double x, double T) {
+  if (T > 0.0) return 1.0 / (exp(x / T) + 1.0);
+  return (-x < 0.0) ? 0.0 : ((-x > 0.0) ? 1.0 : 0.5);
+}
+
+__device__ __forceinline__ void carve_vectors(unsigned char* smem, const EighSmemLayout& L, int n, int nR,
+                                              EighVec& S, double2** ph, double** kpt) {
+  double2* cbuf = (double2*)(smem + L.offC);
+  double* dbuf = (double*)(smem + L.offD);
+  int* ibuf = (int*)(smem + L.offI);
+  S.tau = cbuf; S.v = cbuf + n; S.w = cbuf + 2 * n; S.vn = cbuf + 3 * n; S.pn = cbuf + 4 * n;
+  S.bc = cbuf + 5 * n;
+  *ph = cbuf + 5 * n + 2;
+  S.pbuf = cbuf + 5 * n + 2 + nR;
+  S.d = dbuf; S.e = dbuf + n; S.D = dbuf + 2 * n; S.z = dbuf + 3 * n; S.dl = dbuf + 4 * n;
+  S.zl = dbuf + 5 * n; S.troot = dbuf + 6 * n; S.zhat = dbuf + 7 * n; S.vals = dbuf + 8 * n;
+  S.dval = dbuf + 9 * n; S.rc = dbuf + 10 * n; S.rs = dbuf + 11 * n; S.nrho = dbuf + 12 * n;
+  S.red = dbuf + 13 * n;
+  *kpt = dbuf + 13 * n + 32;
+  S.perm = ibuf; S.colnd = ibuf + n; S.org = ibuf + 2 * n; S.dcol = ibuf + 3 * n; S.newpos = ibuf + 4 * n;
+  S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
+}
 
 __global__ void __launch_bounds__(256) eigh_kernel(EighArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Team T = make_team();
   const int n = a.n;
-  const EighSmemLayout L = eigh_smem_layout(n, a.nR, a.a_in_smem);
-  double2* cbuf = (double2*)(smem + L.offC);
-  double* dbuf = (double*)(smem + L.offD);
-  int* ibuf = (int*)(smem + L.offI);
+  const EighSmemLayout L = eigh_smem_layout(n, a.nR, T.nt, a.a_in_smem);
   EighVec S;
-  S.tau = cbuf; S.v = cbuf + n; S.w = cbuf + 2 * n; S.bc = cbuf + 3 * n;
-  double2* ph = cbuf + 3 * n + 2;
-  S.d = dbuf; S.e = dbuf + n; S.D = dbuf + 2 * n; S.z = dbuf + 3 * n; S.dl = dbuf + 4 * n;
-  S.zl = dbuf + 5 * n; S.troot = dbuf + 6 * n; S.zhat = dbuf + 7 * n; S.vals = dbuf + 8 * n;
-  S.dval = dbuf + 9 * n; S.rc = dbuf + 10 * n; S.rs = dbuf + 11 * n; S.nrho = dbuf + 12 * n;
-  S.red = dbuf + 13 * n;
-  double* kpt = dbuf + 13 * n + 32;
-  S.perm = ibuf; S.colnd = ibuf + n; S.org = ibuf + 2 * n; S.dcol = ibuf + 3 * n; S.newpos = ibuf + 4 * n;
-  S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
+  double2* ph;
+  double* kpt;
+  carve_vectors(smem, L, n, a.nR, S, &ph, &kpt);
 
   const int64_t nn = (int64_t)n * n;
   double* slot = a.scratch + (int64_t)blockIdx.x * a.slot_doubles;
-  double2* A;
-  double* Q;
-  if (a.a_in_smem) { A = (double2*)(smem + L.offA); Q = slot; }
-  else { A = (double2*)slot; Q = slot + 2 * nn; }
+  const bool in_smem = a.a_in_smem != 0;
+  const int lda = in_smem ? n + 1 : n;
+  double2* A = in_smem ? (double2*)(smem + L.offA) : (double2*)slot;
+  double2* R = in_smem ? (double2*)slot : A;          // reflectors, leading dimension ldr
+  const int ldr = in_smem ? n : lda;
+  double* Q = in_smem ? (double*)(smem + L.offA) : slot + 2 * nn;
   double* Qt = Q + nn;
-  double* Us = Qt + nn;
+  double* Qs = slot + 2 * nn;                         // smem path: saved Q
+  double* Us = in_smem ? slot + 3 * nn : slot + 4 * nn;
+  const bool need_vec = (a.U != nullptr) || (a.rhok != nullptr);
+
+  const bool prof = a.phase_cycles != nullptr;
+  unsigned long long acc[5] = {0, 0, 0, 0, 0};
+  long long tc = 0;
+#define LQM_TICK(ph_)                                                                   \
+  if (prof) {                                                                          \
+    long long t_ = clock64();                                                          \
+    acc[ph_] += (unsigned long long)(t_ - tc);                                         \
+    tc = t_;                                                                           \
+  }
 
   for (int64_t k = blockIdx.x; k < a.nk; k += gridDim.x) {
+    if (prof) tc = clock64();
     if (T.tid < a.dim) kpt[T.tid] = a.ks[k * a.dim + T.tid];
     team_sync();
-    bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, n);
-    hetrd_lower(T, n, A, n, S);
+    bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, lda);
+    LQM_TICK(PH_BLOCH);
+    hetrd_lower(T, n, A, lda, S);
+    if (in_smem) {
+      for (int c = T.wid; c < n - 1; c += T.nw)
+        for (int r = c + 1 + T.lane; r < n; r += T.nl) R[r + (int64_t)c * n] = A[r + (int64_t)c * lda];
+      team_sync();
+    }
+    LQM_TICK(PH_HETRD);
     dc_solve(T, n, a.plan, S, Q, Qt, Us);
     for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
-    if (a.U) backtransform(T, n, A, n, S, Q, a.U + k * nn, n);
+    LQM_TICK(PH_DC);
+    if (need_vec) {
+      double2* U;
+      int ldu;
+      if (in_smem) {
+        for (int c = T.wid; c < n; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) Qs[r + (int64_t)c * n] = Q[r + (int64_t)c * n];
+        team_sync();
+        U = (double2*)(smem + L.offA);
+        ldu = n + 1;
+        for (int c = T.wid; c < n; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Qs[r + (int64_t)c * n], 0.0);
+      } else {
+        U = a.U ? a.U + k * nn : (double2*)(slot + 5 * nn);
+        ldu = n;
+        for (int c = T.wid; c < n; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Q[r + (int64_t)c * n], 0.0);
+      }
+      team_sync();
+      backtransform(T, n, R, ldr, S, U, ldu);
+      LQM_TICK(PH_BACK);
+      if (in_smem && a.U) {
+        double2* Uo = a.U + k * nn;
+        for (int c = T.wid; c < n; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) Uo[r + (int64_t)c * n] = U[r + (int64_t)c * ldu];
+      }
+      if (a.rhok) {
+        double eb = 0.0;
+        for (int j = T.tid; j < n; j += T.nt) {
+          const double fj = fermi(S.D[j] - a.mu, a.T);
+          S.vals[j] = fj;
+          eb += S.D[j] * fj;
+        }
+        eb = team_sum(T, eb, S.red);
+        if (T.tid == 0) a.eband_k[k] = a.w[k] * eb;
+        rho_from_U(T, n, U, ldu, S.vals, a.rhok + k * nn, n);
+      }
+    }
     team_sync();
+    LQM_TICK(PH_OUT);
   }
+#undef LQM_TICK
+  if (prof && T.tid == 0)
+    for (int i = 0; i < 5; ++i) atomicAdd(&a.phase_cycles[i], acc[i]);
 }
 
 // Batched Bloch sum to HBM: Hk[k] = sum_R H_R exp(i 2 pi k.R); one CTA per k.
@@ -109,12 +205,7 @@ __global__ void __launch_bounds__(256) bloch_kernel(int n, int nR, int dim, cons
   }
 }
 
-__device__ __forceinline__ double fermi(double x, double T) {
-  if (T > 0.0) return 1.0 / (exp(x / T) + 1.0);
-  return (-x < 0.0) ? 0.0 : ((-x > 0.0) ? 1.0 : 0.5);
-}
-
-// rho_k = U diag(f) U^H per k; eband_k = w_k sum_j f_j eps_j.
+// rho_k = U diag(f) U^H per k from eigenvectors in HBM; eband_k = w_k sum_j f_j eps_j.
 __global__ void __launch_bounds__(256) rhok_kernel(int n, int64_t nk, const double2* __restrict__ U,
                                                    const double* __restrict__ bands, double mu, double T,
                                                    const double* __restrict__ w, double2* __restrict__ rhok,
@@ -134,21 +225,7 @@ __global__ void __launch_bounds__(256) rhok_kernel(int n, int64_t nk, const doub
     }
     eb = team_sum(Tm, eb, red);
     if (threadIdx.x == 0) eband_k[k] = w[k] * eb;
-    const double2* Uk = U + k * nn;
-    for (int64_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
-      const int aa = (int)(idx % n), bb = (int)(idx / n);
-      double sr = 0.0, si = 0.0;
-      for (int j = 0; j < n; ++j) {
-        const double fj = f[j];
-        if (fj == 0.0) continue;
-        const double2 ua = Uk[aa + (int64_t)j * n], ub = Uk[bb + (int64_t)j * n];
-        // ua * conj(ub) * f
-        sr += fj * (ua.x * ub.x + ua.y * ub.y);
-        si += fj * (ua.y * ub.x - ua.x * ub.y);
-      }
-      rhok[k * nn + idx] = cmk(sr, si);
-    }
-    __syncthreads();
+    rho_from_U(Tm, n, U + k * nn, n, f, rhok + k * nn, n);
   }
 }
 

@@ -38,6 +38,7 @@ EXPORTS = [
     "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
     "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
+    "lqm_ctx_phase_cycles",
 ]
 
 
@@ -78,6 +79,7 @@ _SIG = {
     "lqm_dos_bands_dev": [_P, _I64, _I64, _P, _P, _I64, _P, _D, _P],
     "lqm_scf_hf": [_P, _P, _P, _I64, _P, _P, _D, _D, _D, _D, _I64, _I64, _P, _P, LOG_CB, _P, _P],
     "lqm_ctx_reset_stats": [_P, ctypes.c_int],
+    "lqm_ctx_phase_cycles": [_P, ctypes.POINTER(_D)],
     "lqm_ctx_stats": [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
@@ -137,6 +139,12 @@ class Context:
         ms, el, al = _D(), _I64(), _I64()
         self.check(_lib.lqm_ctx_stats(self._h, ctypes.byref(ms), ctypes.byref(el), ctypes.byref(al)))
         return ms.value, el.value, al.value
+
+    def phase_cycles(self):
+        """Eigensolver SM cycles per stage (bloch, householder, d&c, back-transform, sync)."""
+        out = (_D * 5)()
+        self.check(_lib.lqm_ctx_phase_cycles(self._h, out))
+        return list(out)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -88,3 +88,14 @@ def test_emulated_tridiagonal_dc(emul, n):
         assert np.all(np.diff(ev) >= 0)
         assert np.max(np.abs(Z.T @ Z - np.eye(n))) <= 1e-13
         assert np.max(np.abs(T @ Z - Z * ev)) <= 1e-13 * scale
+
+
+@pytest.mark.parametrize("n", [1, 5, 37, 96, 130])
+def test_emulated_rho_from_U(emul, n):
+    rng = np.random.default_rng(n)
+    U = np.asfortranarray(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    f = rng.random(n)
+    f[::3] = 0.0
+    out = np.zeros((n, n), complex, order="F")
+    emul.lqm_emul_rho(n, U.ctypes.data_as(P), f.ctypes.data_as(P), out.ctypes.data_as(P))
+    assert np.max(np.abs(out - (U * f) @ U.conj().T)) < 1e-12 * n
