@@ -214,6 +214,27 @@ def measured_fp64_peak(torch, dev):
     return 2 * 8192 ** 3 / best / 1e12
 
 
+def profile_case(Q, ctx, h, torch, dev, np):
+    """A small case of the bench's dominant kernel for profilers: 2048 k-points of the
+    n=96 model through lqm_bands_dos_rho_dev (one eigh_kernel launch)."""
+    nk = 2048
+    ks = np.random.default_rng(0).random((2, nk))
+    d_ks = torch.from_numpy(np.ascontiguousarray(ks.T)).to(dev)
+    Hd = Q.DeviceHops(h, ctx)
+    n = Hd.n
+    Lk = np.asfortranarray(np.array(list(h.keys()), dtype=np.int64).T)
+    rho = torch.zeros(len(h), n, n, dtype=torch.complex128, device=dev)
+    bands = torch.zeros(nk, n, dtype=torch.float64, device=dev)
+    dos = torch.zeros(NW, dtype=torch.float64, device=dev)
+    om = torch.linspace(-6.0, 6.0, NW, dtype=torch.float64, device=dev)
+    eb = ctypes.c_double()
+    for _ in range(2):
+        ctx.check(Q.lib().lqm_bands_dos_rho_dev(ctx.handle, Hd.handle, nk, Q._ptr(d_ks), None, MU, TEMP, len(h),
+                                                 Q._ptr(Lk), Q._ptr(rho), ctypes.byref(eb), NW, Q._ptr(om), GAMMA,
+                                                 Q._ptr(dos), Q._ptr(bands), 0))
+    print(json.dumps({"profile_case": "n=96 batch model, 2048 k", "kernel_ms": ctx.last_kernel_ms()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -221,6 +242,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="one fused call on the n=96 model over 2048 k-points (small case for ncu)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
@@ -246,6 +269,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     models = M.batch_models()
     ctx = Q.Context(local, timeout=900)
+    if args.profile_case:
+        return profile_case(Q, ctx, models[2][1], torch, dev, np)
 
     # ---- device-resident inputs ----
     ks_np = kgrid(rank, world)
