@@ -142,6 +142,25 @@ int lqm_scf_hf(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, c
                int64_t nL, const int64_t* Lkeys, double* rho_inout, lqm_scf_log_cb cb, void* cb_user,
                double* out_scalars);
 
+/* Allocation-free eigen pass.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory, e.g. a host whose device memory
+ * is owned by another allocator (a Julia CUDA.jl pool, a framework's caching
+ * allocator) that must not see foreign cudaMalloc/cudaFree, or a
+ * latency-sensitive loop that cannot afford their implicit device-wide
+ * synchronisation.  Same computation as lqm_bandmatrix_dev (bands n x nk; U
+ * n x n x nk when d_U is not NULL) with every array a caller-owned device
+ * pointer and H given as device keys (d x nR Int64) and blocks (n x n x nR
+ * ComplexF64), launched on `stream` (a cudaStream_t; NULL = legacy default).
+ * Scratch comes from a fixed 64 MiB device array inside the library (held on
+ * every GPU that loads it until exit); n <= 1024 and one k-point's scratch
+ * must fit, larger n returns LQM_EINVAL.  The first call on a device resolves
+ * that array's address and should come before any stream capture.  Calls that
+ * overlap on the GPU share the array and race.  Returns LQM_OK, LQM_EINVAL
+ * (sizes/pointers) or LQM_ECUDA (launch/runtime error); it does not wait for
+ * the kernels to finish. */
+int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32_t d, const int64_t* d_keys,
+                           const double* d_blocks, int64_t nk, const double* d_ks, double* d_bands, double* d_U);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <thread>
@@ -745,3 +746,114 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 }  // extern "C"
 
 #include "lqm_scf.inc"
+
+// ============================================================================
+// Allocation-free eigen pass.
+//
+// For callers that cannot allocate device memory themselves or through this
+// library: hosts whose device memory belongs to another allocator (a Julia
+// CUDA.jl memory pool, a framework's caching allocator) and that must not see
+// foreign cudaMalloc/cudaFree calls, or latency-sensitive loops that cannot
+// afford the device-wide synchronisation cudaMalloc/cudaFree imply.  The
+// caller passes every input and output as a device pointer and a stream; the
+// eigensolver's scratch and its divide-and-conquer plan live in the two
+// file-scope device arrays below, which every GPU that loads this library
+// holds until the process exits.  No cudaMalloc, cudaFree or allocating
+// library routine is called.
+//
+// Host code must not use the array names as addresses (on the host they are
+// stand-ins, not device pointers): the first call on each device, with that
+// device current, resolves their device addresses with cudaGetSymbolAddress
+// and caches them; make that first call before any stream capture.  All calls
+// share the arrays, so calls that overlap on the GPU race; serialise them
+// (one stream, or events).  Each call writes every scratch entry it later
+// reads and rebuilds the plan for its own n, so nothing has to start at zero.
+// ============================================================================
+namespace {
+
+constexpr int64_t kNoAllocScratchBytes = (int64_t)64 << 20;  // 64 MiB of FP64 scratch per device
+constexpr int64_t kNoAllocScratchDoubles = kNoAllocScratchBytes / 8;
+constexpr int kNoAllocMaxN = 1024;                           // matrix order limit
+constexpr int kNoAllocPlanInts = 16384;                      // >= dc_plan_ints(1024)
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+static __device__ __align__(256) int g_noalloc_plan[kNoAllocPlanInts];
+
+// Builds the divide-and-conquer plan for order n in place (device code may
+// name the array directly).
+__global__ void noalloc_plan_kernel(int n) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) dc_plan_fill(n, g_noalloc_plan);
+}
+
+struct NoAllocDevice {
+  bool ready = false;
+  double* scratch = nullptr;
+  int* plan = nullptr;
+  int sms = 0;
+};
+std::mutex g_noalloc_mutex;
+NoAllocDevice g_noalloc_dev[64];
+
+}  // namespace
+
+extern "C" int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32_t d, const int64_t* d_keys,
+                                      const double* d_blocks, int64_t nk, const double* d_ks, double* d_bands,
+                                      double* d_U) {
+  if (n < 1 || n > kNoAllocMaxN || nR < 1 || nR > 4096 || d < 1 || d > 3 || nk < 1) return LQM_EINVAL;
+  if (!d_keys || !d_blocks || !d_ks || !d_bands) return LQM_EINVAL;
+  if (dc_plan_ints((int)n) > kNoAllocPlanInts) return LQM_EINVAL;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return LQM_ECUDA;
+  NoAllocDevice& D = g_noalloc_dev[dev];
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!D.ready) {  // once per device, with that device current
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return LQM_ECUDA;
+      D.scratch = (double*)p;
+      p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_plan) != cudaSuccess || !p) return LQM_ECUDA;
+      D.plan = (int*)p;
+      if (cudaDeviceGetAttribute(&D.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return LQM_ECUDA;
+      D.ready = true;
+    }
+  }
+  const int ni = (int)n;
+  const int nt = eigh_threads(ni);
+  EighSmemLayout Ls = eigh_smem_layout(ni, (int)nR, nt, 1);
+  const int a_in_smem = Ls.total <= 225 * 1024;
+  if (!a_in_smem) Ls = eigh_smem_layout(ni, (int)nR, nt, 0);
+  if (Ls.total > 225 * 1024) return LQM_EINVAL;
+  const int64_t slot = eigh_slot_doubles(ni, a_in_smem, false);
+  const int64_t max_slots = kNoAllocScratchDoubles / slot;
+  if (max_slots < 1) return LQM_EINVAL;  // one k-point's scratch exceeds the 64 MiB array
+  if (cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total) != cudaSuccess)
+    return LQM_ECUDA;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_kernel, nt, Ls.total) != cudaSuccess ||
+      per_sm < 1)
+    return LQM_ECUDA;
+  const int64_t grid = std::min<int64_t>(std::min<int64_t>(nk, (int64_t)per_sm * D.sms), max_slots);
+  const int H = dc_plan_height(ni);
+  const int nnodes = ni - 1;
+  EighArgs a{};
+  a.n = ni; a.nR = (int)nR; a.dim = d; a.blocks = (const double2*)d_blocks; a.keys = d_keys;
+  a.nk = nk; a.ks = d_ks;
+  a.plan.nnodes = nnodes;
+  a.plan.nheights = H;
+  a.plan.hstart = D.plan;
+  a.plan.lo = D.plan + (H + 1);
+  a.plan.mid = a.plan.lo + nnodes;
+  a.plan.hi = a.plan.mid + nnodes;
+  a.plan.owner = a.plan.hi + nnodes;
+  a.scratch = D.scratch;
+  a.slot_doubles = slot;
+  a.a_in_smem = a_in_smem;
+  a.bands = d_bands;
+  a.U = (double2*)d_U;
+  cudaStream_t st = (cudaStream_t)stream;
+  noalloc_plan_kernel<<<1, 1, 0, st>>>(ni);
+  eigh_kernel<<<(unsigned)grid, nt, Ls.total, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? LQM_OK : LQM_ECUDA;
+}
+

@@ -38,7 +38,7 @@ EXPORTS = [
     "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
     "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
-    "lqm_ctx_phase_cycles",
+    "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc",
 ]
 
 
@@ -80,6 +80,7 @@ _SIG = {
     "lqm_scf_hf": [_P, _P, _P, _I64, _P, _P, _D, _D, _D, _D, _I64, _I64, _P, _P, LOG_CB, _P, _P],
     "lqm_ctx_reset_stats": [_P, ctypes.c_int],
     "lqm_ctx_phase_cycles": [_P, ctypes.POINTER(_D)],
+    "lqm_bandmatrix_noalloc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _I64, _P, _P, _P],
     "lqm_ctx_stats": [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
