@@ -60,8 +60,10 @@ int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing);
 int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches);
 /* SM cycles spent by the eigensolver kernel per stage, summed over CTAs while
  * timing is enabled: [0] Bloch sum, [1] Householder, [2] divide and conquer,
- * [3] bands + back-transformation, [4] end-of-k barrier.  New (profiling). */
-int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles /* [5] */);
+ * [3] bands + back-transformation, [4] end-of-k barrier, [5..12] the divide
+ * and conquer merge steps (z/sort, deflation, secular roots, Gu-Eisenstat z,
+ * vectors/rotations/values, ranks, update, copy back).  New (profiling). */
+int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles /* [13] */);
 
 /* Upload a dense Hops (src/modules/TightBinding/types.jl:54-60, DenseHops):
  * keys d x nR (Int64), blocks n x n x nR column-major ComplexF64 in the same

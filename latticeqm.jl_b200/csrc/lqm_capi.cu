@@ -154,7 +154,7 @@ void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
 
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
-  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2
+  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD
 };
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
@@ -251,6 +251,24 @@ int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
 }
 
 // Density matrix on device arrays; accumulates eband into d_eb[0].
+// rho_L (+)= sum_k coef[k,L] rho_k over a batch: split-k partials, then an
+// ordered reduction (deterministic for a fixed batch size).
+void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const double2* coef, int nL,
+                 double2* d_rho, int accumulate) {
+  const int64_t tiles = (nn + 255) / 256;
+  int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(nb, (4 * (int64_t)ctx->num_sms + tiles - 1) / tiles));
+  chunks = std::min<int64_t>(chunks, 65535);
+  const int64_t kchunk = (nb + chunks - 1) / chunks;
+  chunks = (nb + kchunk - 1) / kchunk;
+  double2* part = (double2*)ws_get(ctx, WS_FOLD, (size_t)(chunks * nL * nn) * sizeof(double2));
+  fold_partial_kernel<16><<<dim3((unsigned)tiles, (unsigned)chunks), 256, 0, ctx->stream>>>(nn, nb, kchunk, rk, coef,
+                                                                                          nL, part);
+  const int64_t m = nL * nn;
+  fold_reduce_kernel<<<(unsigned)std::min<int64_t>((m + 255) / 256, 8192), 256, 0, ctx->stream>>>(
+      m, (int)chunks, part, d_rho, accumulate);
+  ck(cudaGetLastError(), "fold launch");
+}
+
 // bands_out (n x nk, device) receives every k's eigenvalues when non-null.
 void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w, double mu,
                  double T, int64_t nL, const int64_t* d_Lkeys, double2* d_rho, double* d_eb,
@@ -270,10 +288,8 @@ void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
     ordered_sum_kernel<<<1, 256, 0, ctx->stream>>>(ebk, nb, d_eb, k0 > 0);
     fold_coef_kernel<<<(unsigned)std::min<int64_t>((nb * nL + 255) / 256, 4096), 256, 0, ctx->stream>>>(
         nb, H->d, d_ks + k0 * H->d, d_w + k0, (int)nL, d_Lkeys, coef);
-    const int64_t gf = std::min<int64_t>((nn + 255) / 256, (int64_t)ctx->num_sms * 8);
-    fold_kernel<16><<<(unsigned)gf, 256, 0, ctx->stream>>>(nn, nb, rk, coef, (int)nL, d_rho, k0 > 0);
-    ck(cudaGetLastError(), "fold_kernel launch");
-    ctx->launches += 3;
+    launch_fold(ctx, nn, nb, rk, coef, (int)nL, d_rho, k0 > 0);
+    ctx->launches += 2;
   }
 }
 
@@ -443,7 +459,7 @@ int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles) {
       wait_stream(ctx);
       ck(cudaMemcpy(h, ctx->d_phase, sizeof(h), cudaMemcpyDeviceToHost), "D2H");
     }
-    for (int i = 0; i < 5; ++i) cycles[i] = (double)h[i];
+    for (int i = 0; i < 13; ++i) cycles[i] = (double)h[i];
   });
 }
 

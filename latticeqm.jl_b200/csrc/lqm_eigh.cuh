@@ -32,7 +32,7 @@ struct DCPlan {
 
 // Shared-memory vectors for one k-point (all length >= n unless noted).
 struct EighVec {
-  double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;
+  double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;  // red: 128
   int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
   double2 *tau, *v, *w, *vn, *pn, *bc, *pbuf;
 };
@@ -77,49 +77,32 @@ LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __
 // with v0 = 1.
 // ---------------------------------------------------------------------------
 
-// Reflector of column j (rows j+1..n-1): tau[j], e[j] = beta, d[j] = Re A[j,j];
-// v (v0 = 1) goes to vout and back into the column.
-LQM_FN void make_reflector(const Team& T, int n, int j, double2* A, int lda, EighVec& S, double2* vout) {
-  const int m = n - j - 1;
-  double2* col = A + (j + 1) + (int64_t)j * lda;
-  double s = 0.0;
-  for (int r = 1 + T.tid; r < m; r += T.nt) { const double2 x = col[r]; s += x.x * x.x + x.y * x.y; }
-  s = team_sum(T, s, S.red);
-  if (T.tid == 0) {
-    const double2 alpha = col[0];
-    double2 tj, scal;
-    double beta;
-    if (s == 0.0 && alpha.y == 0.0) {
-      tj = cmk(0.0, 0.0); scal = cmk(0.0, 0.0); beta = alpha.x;
-    } else {
-      const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s);
-      beta = (alpha.x >= 0.0) ? -nrm : nrm;
-      tj = cmk((beta - alpha.x) / beta, -alpha.y / beta);
-      scal = cdiv(cmk(1.0, 0.0), cmk(alpha.x - beta, alpha.y));
-    }
-    S.tau[j] = tj;
-    S.e[j] = beta;
-    S.d[j] = A[j + (int64_t)j * lda].x;
-    S.bc[1] = scal;
+// zlarfg on (alpha, ||x||^2): tau, beta and the scale 1/(alpha - beta) of x.
+// Every thread evaluates it on the same inputs (no serial section).
+LQM_FN void zlarfg_scalars(double2 alpha, double xnorm2, double2* tau, double* beta, double2* scal) {
+  if (xnorm2 == 0.0 && alpha.y == 0.0) {
+    *tau = cmk(0.0, 0.0); *scal = cmk(0.0, 0.0); *beta = alpha.x;
+    return;
   }
-  team_sync();
-  const double2 scal = S.bc[1];
-  for (int r = T.tid; r < m; r += T.nt) {
-    const double2 x = (r == 0) ? cmk(1.0, 0.0) : cmul(scal, col[r]);
-    vout[r] = x;
-    col[r] = x;
-  }
-  team_sync();
+  const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
+  const double b = (alpha.x >= 0.0) ? -nrm : nrm;
+  const double ib = 1.0 / b;
+  *beta = b;
+  *tau = cmk((b - alpha.x) * ib, -alpha.y * ib);
+  *scal = cdiv(cmk(1.0, 0.0), cmk(alpha.x - b, alpha.y));
 }
 
-// One pass over the trailing block B (order mb, leading dimension lda):
-//   upd:  B[r,c] -= v[r+1] conj(w[c+1]) + w[r+1] conj(v[c+1])   (previous reflector,
+// One pass over the trailing block B = A[o:, o:] (order mb, o >= 1):
+//   upd:  B[r,c] -= v[r+1] conj(w[c+1]) + w[r+1] conj(v[c+1])  (reflector o-2,
 //         whose vectors start one row above B)
-//   p[r] = tau * sum_c B[r,c] x[c]                               (next reflector)
-// Rows across lanes (up to 4 per lane and pass), columns across warps; warp
-// partial sums are added in warp order.
-LQM_FN void trailing_pass(const Team& T, int mb, double2* B, int lda, const double2* v, const double2* w,
-                          bool upd, const double2* x, double2 tau, double2* p, double2* pbuf, int pstride) {
+//   x[c] = (c == 0) ? 1 : scal * A[o+c, o-1]  (next reflector, formed on the fly
+//         by the warp owning column c, stored to xs[] and back into A)
+//   pbuf[warp][r] = sum over the warp's columns of B_new[r,c] x[c]
+// Rows across lanes (up to 4 per lane and pass), columns across warps.
+LQM_FN void trailing_pass(const Team& T, int mb, double2* A, int lda, int o, const double2* v, const double2* w,
+                          bool upd, double2 scal, double2* xs, double2* pbuf, int pstride) {
+  double2* B = A + o + (int64_t)o * lda;
+  double2* xcol = A + o + (int64_t)(o - 1) * lda;
   for (int r0 = 0; r0 < mb; r0 += 4 * T.nl) {
     double2 acc[4], vr[4], wr[4];
     int rr[4];
@@ -132,7 +115,7 @@ LQM_FN void trailing_pass(const Team& T, int mb, double2* B, int lda, const doub
       if (upd && rr[q] < mb) { vr[q] = v[rr[q] + 1]; wr[q] = w[rr[q] + 1]; }
     }
     for (int c = T.wid; c < mb; c += T.nw) {
-      const double2 xc = x[c];
+      const double2 xc = (c == 0) ? cmk(1.0, 0.0) : cmul(scal, xcol[c]);
       double2 cw = cmk(0.0, 0.0), cv = cmk(0.0, 0.0);
       if (upd) { cw = cconj(w[c + 1]); cv = cconj(v[c + 1]); }
       double2* Bc = B + (int64_t)c * lda;
@@ -154,60 +137,87 @@ LQM_FN void trailing_pass(const Team& T, int mb, double2* B, int lda, const doub
     for (int q = 0; q < 4; ++q)
       if (rr[q] < mb) pbuf[T.wid * pstride + rr[q]] = acc[q];
   }
-  team_sync();
-  for (int r = T.tid; r < mb; r += T.nt) {
-    double2 s = cmk(0.0, 0.0);
-    for (int wv = 0; wv < T.nw; ++wv) s = cadd(s, pbuf[wv * pstride + r]);
-    p[r] = cmul(tau, s);
-  }
-  team_sync();
 }
 
+// Stores the next reflector x (formed from column o-1 rows o..) into xs[] and
+// back into A.  Called after trailing_pass and a barrier.
+LQM_FN void store_reflector(const Team& T, int mb, double2* A, int lda, int o, double2 scal, double2* xs) {
+  double2* xcol = A + o + (int64_t)(o - 1) * lda;
+  for (int c = T.tid; c < mb; c += T.nt) {
+    const double2 x = (c == 0) ? cmk(1.0, 0.0) : cmul(scal, xcol[c]);
+    xs[c] = x;
+    xcol[c] = x;
+  }
+}
+
+// Householder tridiagonalisation with 3 barriers per step:
+//   pass (update j, mat-vec with reflector j+1) | p, p^H v -> alpha |
+//   w, update of the next column, its norm -> next reflector scalars.
 LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, EighVec& S) {
   if (n == 1) {
     if (T.tid == 0) S.d[0] = A[0].x;
     team_sync();
     return;
   }
-  double2* v = S.v;
-  double2* vn = S.vn;
-  double2* w = S.w;
+  double* redA = S.red;
+  double* redB = S.red + 64;
+  double2* vc = S.v;   // current reflector
+  double2* vx = S.vn;  // next reflector
+  double2* wc = S.w;   // w of the current reflector
   double2* p = S.pn;
-  make_reflector(T, n, 0, A, lda, S, v);
-  trailing_pass(T, n - 1, A + 1 + lda, lda, v, w, false, v, S.tau[0], p, S.pbuf, n);
-  for (int j = 0; j < n - 1; ++j) {
-    const int m = n - j - 1;
-    const double2 tj = S.tau[j];
-    // w = p + alpha v with alpha = -1/2 tau (p^H v)
+  // reflector 0 from column 0
+  double s0 = 0.0, dummy = 0.0;
+  for (int r = 2 + T.tid; r < n; r += T.nt) { const double2 x = A[r]; s0 += x.x * x.x + x.y * x.y; }
+  team_sum2_1b(T, s0, dummy, redA);
+  double2 tnext, scal;
+  double beta;
+  zlarfg_scalars(A[1], s0, &tnext, &beta, &scal);
+  if (T.tid == 0) { S.tau[0] = tnext; S.e[0] = beta; S.d[0] = A[0].x; }
+  // step j = -1 .. n-3: pass over A[j+2:, j+2:] (update j if j >= 0) with reflector j+1
+  for (int j = -1; j <= n - 3; ++j) {
+    const int o = j + 2;
+    const int mb = n - o;
+    trailing_pass(T, mb, A, lda, o, vc, wc, j >= 0, scal, vx, S.pbuf, n);
+    team_sync();
+    store_reflector(T, mb, A, lda, o, scal, vx);
+    // p = tau_{j+1} * row sums; alpha = -1/2 tau (p^H x)
     double pr = 0.0, pi = 0.0;
-    for (int r = T.tid; r < m; r += T.nt) {
-      const double2 c = cmulc(p[r], v[r]);
-      pr += c.x; pi += c.y;
+    for (int r = T.tid; r < mb; r += T.nt) {
+      double2 sacc = cmk(0.0, 0.0);
+      for (int wv = 0; wv < T.nw; ++wv) sacc = cadd(sacc, S.pbuf[wv * n + r]);
+      const double2 pv = cmul(tnext, sacc);
+      p[r] = pv;
+      const double2 q = cmulc(pv, vx[r]);  // vx[r] was stored by this same thread above
+      pr += q.x; pi += q.y;
     }
-    pr = team_sum(T, pr, S.red);
-    pi = team_sum(T, pi, S.red);
-    const double2 alpha = cmul(cmk(-0.5 * tj.x, -0.5 * tj.y), cmk(pr, pi));
-    for (int r = T.tid; r < m; r += T.nt) w[r] = cadd(p[r], cmul(alpha, v[r]));
-    team_sync();
-    // column j+1 of the trailing matrix (rows j+1..n-1) gets update j first
-    double2* c1 = A + (j + 1) + (int64_t)(j + 1) * lda;
-    const double2 cw0 = cconj(w[0]), cv0 = cconj(v[0]);
-    for (int r = T.tid; r < m; r += T.nt) {
-      double2 a = csub(c1[r], cadd(cmul(v[r], cw0), cmul(w[r], cv0)));
+    team_sum2_1b(T, pr, pi, redA);
+    const double2 alpha = cmul(cmk(-0.5 * tnext.x, -0.5 * tnext.y), cmk(pr, pi));
+    // w = p + alpha x; column o gets update j+1; norm of its rows o+2.. for reflector j+2
+    const double2 w0 = cadd(p[0], alpha);  // x[0] = 1
+    const double2 cw0 = cconj(w0);
+    double2* col = A + o + (int64_t)o * lda;
+    double sn = 0.0;
+    for (int r = T.tid; r < mb; r += T.nt) {
+      const double2 x = vx[r];
+      const double2 wr = cadd(p[r], cmul(alpha, x));
+      wc[r] = wr;  // the old w is no longer read (the pass ended at the barrier)
+      double2 a = csub(col[r], cadd(cmul(x, cw0), wr));  // x conj(w0) + w conj(x0), x0 = 1
       if (r == 0) a.y = 0.0;
-      c1[r] = a;
+      col[r] = a;
+      if (r >= 2) sn += a.x * a.x + a.y * a.y;
     }
-    team_sync();
-    if (j + 1 < n - 1) {
-      make_reflector(T, n, j + 1, A, lda, S, vn);
-      trailing_pass(T, m - 1, A + (j + 2) + (int64_t)(j + 2) * lda, lda, v, w, true, vn, S.tau[j + 1], p, S.pbuf,
-                    n);
-      double2* t = v; v = vn; vn = t;
+    double dn = 0.0;
+    team_sum2_1b(T, sn, dn, redB);
+    // swap: x becomes the current reflector
+    double2* t = vc; vc = vx; vx = t;
+    if (o <= n - 2) {  // reflector j+2 = o exists
+      zlarfg_scalars(col[1], sn, &tnext, &beta, &scal);
+      if (T.tid == 0) { S.tau[o] = tnext; S.e[o] = beta; S.d[o] = col[0].x; }
     } else {
-      if (T.tid == 0) S.d[n - 1] = A[(n - 1) + (int64_t)(n - 1) * lda].x;
-      team_sync();
+      if (T.tid == 0) S.d[n - 1] = col[0].x;
     }
   }
+  team_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -322,8 +332,28 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 
 // In: S.d (diag, n), S.e (offdiag, n-1).  Out: S.D ascending eigenvalues, Q (n x n, ld n).
 // Qt, Us: n x n scratch.
+// Optional per-step cycle accounting (device only): sub[0..7] += cycles of
+// merge steps A (z, sort), B (deflation), C (secular), D (zhat), E-G (vectors,
+// rotations, values), ranks, H (update), I (copy back).
+#if defined(__CUDA_ARCH__)
+#define LQM_SUBTICK(i_)                                                     \
+  if (sub) {                                                                \
+    const long long t_ = clock64();                                         \
+    sub[i_] += (unsigned long long)(t_ - tsub);                             \
+    tsub = t_;                                                              \
+  }
+#else
+#define LQM_SUBTICK(i_)
+#endif
+
 LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
-                              double* Us) {
+                              double* Us, unsigned long long* sub = nullptr) {
+#if defined(__CUDA_ARCH__)
+  long long tsub = clock64();
+  if (T.tid != 0) sub = nullptr;
+#else
+  (void)sub;
+#endif
   const int64_t nn = (int64_t)n * n;
   double mx = 0.0;
   for (int i = T.tid; i < n; i += T.nt) {
@@ -373,9 +403,11 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       }
     }
     team_sync();
+    LQM_SUBTICK(0);
     // B: deflation, one thread per node
     for (int nd = h0 + T.tid; nd < h1; nd += T.nt) deflate_node(nd, P, S, fabs(S.e[P.mid[nd] - 1]));
     team_sync();
+    LQM_SUBTICK(1);
     // C: secular roots
     for (int i = T.tid; i < n; i += T.nt) {
       const int nd = own[i];
@@ -387,6 +419,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.org[lo + q] = org; S.troot[lo + q] = tr;
     }
     team_sync();
+    LQM_SUBTICK(2);
     // D: Gu-Eisenstat z
     for (int i = T.tid; i < n; i += T.nt) {
       const int nd = own[i];
@@ -404,6 +437,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.zhat[lo + q] = (S.zl[lo + q] < 0.0) ? -zh : zh;
     }
     team_sync();
+    LQM_SUBTICK(3);
     // E: secular eigenvectors, column q of Us block
     for (int i = T.tid; i < n; i += T.nt) {
       const int nd = own[i];
@@ -442,6 +476,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.vals[i] = (it < k) ? S.dl[lo + S.org[lo + it]] + S.troot[lo + it] : S.dval[lo + it - k];
     }
     team_sync();
+    LQM_SUBTICK(4);
     for (int i = T.tid; i < n; i += T.nt) {
       const int nd = own[i];
       if (nd < 0) continue;
@@ -452,6 +487,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.newpos[i] = lo + cnt;
     }
     team_sync();
+    LQM_SUBTICK(5);
     // H: eigenvector update into Qt (column c by warp, rows of its node by lane)
     for (int c = T.wid; c < n; c += T.nw) {
       const int nd = own[c];
@@ -471,6 +507,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       }
     }
     team_sync();
+    LQM_SUBTICK(6);
     // I: write back
     for (int c = T.wid; c < n; c += T.nw) {
       const int nd = own[c];
@@ -483,6 +520,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.D[S.newpos[i]] = S.vals[i];
     }
     team_sync();
+    LQM_SUBTICK(7);
   }
   for (int i = T.tid; i < n; i += T.nt) S.D[i] *= scale;
   team_sync();

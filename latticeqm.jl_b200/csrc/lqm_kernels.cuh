@@ -26,8 +26,8 @@ __host__ __device__ inline EighSmemLayout eigh_smem_layout(int n, int nR, int nt
   if (a_in_smem) off += lqm_align16((size_t)n * (n + 1) * 16);
   L.offC = off;  // double2: tau, v, w, vn, pn (n each), bc (2), ph (nR), pbuf
   off += lqm_align16((size_t)(5 * n + 2 + nR + L.pbuf_len) * 16);
-  L.offD = off;  // doubles: 13 n + 32 (red) + 4 (kpt)
-  off += lqm_align16((size_t)(13 * n + 36) * 8);
+  L.offD = off;  // doubles: 13 n + 128 (red) + 4 (kpt)
+  off += lqm_align16((size_t)(13 * n + 132) * 8);
   L.offI = off;  // ints: 10 n
   off += lqm_align16((size_t)(10 * n) * 4);
   L.total = off;
@@ -57,10 +57,10 @@ struct EighArgs {
   double* eband_k;        // nk: w_k sum_j f_j eps_j (with rhok)
   const double* w;        // nk weights (with rhok)
   double mu, T;
-  unsigned long long* phase_cycles;  // [8] per-phase SM cycles summed over CTAs, or null
+  unsigned long long* phase_cycles;  // [16] per-phase SM cycles summed over CTAs, or null
 };
 
-enum { PH_BLOCH = 0, PH_HETRD = 1, PH_DC = 2, PH_BACK = 3, PH_OUT = 4, PH_COUNT = 8 };
+enum { PH_BLOCH = 0, PH_HETRD = 1, PH_DC = 2, PH_BACK = 3, PH_OUT = 4, PH_DCSUB = 5, PH_COUNT = 16 };
 
 __device__ __forceinline__ double fermi(double x, double T) {
   if (T > 0.0) return 1.0 / (exp(x / T) + 1.0);
@@ -80,7 +80,7 @@ __device__ __forceinline__ void carve_vectors(unsigned char* smem, const EighSme
   S.zl = dbuf + 5 * n; S.troot = dbuf + 6 * n; S.zhat = dbuf + 7 * n; S.vals = dbuf + 8 * n;
   S.dval = dbuf + 9 * n; S.rc = dbuf + 10 * n; S.rs = dbuf + 11 * n; S.nrho = dbuf + 12 * n;
   S.red = dbuf + 13 * n;
-  *kpt = dbuf + 13 * n + 32;
+  *kpt = dbuf + 13 * n + 128;
   S.perm = ibuf; S.colnd = ibuf + n; S.org = ibuf + 2 * n; S.dcol = ibuf + 3 * n; S.newpos = ibuf + 4 * n;
   S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
 }
@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(256) eigh_kernel(EighArgs a) {
 
   const bool prof = a.phase_cycles != nullptr;
   unsigned long long acc[5] = {0, 0, 0, 0, 0};
+  unsigned long long dsub[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   long long tc = 0;
 #define LQM_TICK(ph_)                                                                   \
   if (prof) {                                                                          \
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(256) eigh_kernel(EighArgs a) {
       team_sync();
     }
     LQM_TICK(PH_HETRD);
-    dc_solve(T, n, a.plan, S, Q, Qt, Us);
+    dc_solve(T, n, a.plan, S, Q, Qt, Us, prof ? dsub : nullptr);
     for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
     LQM_TICK(PH_DC);
     if (need_vec) {
@@ -175,8 +176,10 @@ __global__ void __launch_bounds__(256) eigh_kernel(EighArgs a) {
     LQM_TICK(PH_OUT);
   }
 #undef LQM_TICK
-  if (prof && T.tid == 0)
+  if (prof && T.tid == 0) {
     for (int i = 0; i < 5; ++i) atomicAdd(&a.phase_cycles[i], acc[i]);
+    for (int i = 0; i < 8; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + i], dsub[i]);
+  }
 }
 
 // Batched Bloch sum to HBM: Hk[k] = sum_R H_R exp(i 2 pi k.R); one CTA per k.
@@ -244,31 +247,42 @@ __global__ void fold_coef_kernel(int64_t nb, int dim, const double* __restrict__
   }
 }
 
-// rhoL[l] (+)= sum_kb coef[kb,l] * rhok[kb], k in fixed order per element.
+// Split-k Fourier fold, stage 1: part[chunk][l][e] = sum over the chunk's k
+// (in order) of coef[kb,l] * rhok[kb][e].  Grid: (element tiles, k-chunks).
 template <int LC>
-__global__ void __launch_bounds__(256) fold_kernel(int64_t nn, int64_t nb, const double2* __restrict__ rhok,
-                                                   const double2* __restrict__ coef, int nL,
-                                                   double2* __restrict__ rhoL, int accumulate) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nn; e += (int64_t)gridDim.x * blockDim.x) {
-    for (int l0 = 0; l0 < nL; l0 += LC) {
-      double2 acc[LC];
+__global__ void __launch_bounds__(256) fold_partial_kernel(int64_t nn, int64_t nb, int64_t kchunk,
+                                                           const double2* __restrict__ rhok,
+                                                           const double2* __restrict__ coef, int nL,
+                                                           double2* __restrict__ part) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t k0 = blockIdx.y * kchunk;
+  const int64_t k1 = (k0 + kchunk < nb) ? k0 + kchunk : nb;
+  if (e >= nn) return;
+  double2* out = part + (int64_t)blockIdx.y * nL * nn;
+  for (int l0 = 0; l0 < nL; l0 += LC) {
+    double2 acc[LC];
 #pragma unroll
-      for (int l = 0; l < LC; ++l) {
-        acc[l] = cmk(0.0, 0.0);
-        if (accumulate && l0 + l < nL) acc[l] = rhoL[(int64_t)(l0 + l) * nn + e];
-      }
-      for (int64_t kb = 0; kb < nb; ++kb) {
-        const double2 x = rhok[kb * nn + e];
-        const double2* cf = coef + kb * nL + l0;
-#pragma unroll
-        for (int l = 0; l < LC; ++l) {
-          if (l0 + l < nL) acc[l] = cadd(acc[l], cmul(cf[l], x));
-        }
-      }
+    for (int l = 0; l < LC; ++l) acc[l] = cmk(0.0, 0.0);
+    for (int64_t kb = k0; kb < k1; ++kb) {
+      const double2 x = rhok[kb * nn + e];
+      const double2* cf = coef + kb * nL + l0;
 #pragma unroll
       for (int l = 0; l < LC; ++l)
-        if (l0 + l < nL) rhoL[(int64_t)(l0 + l) * nn + e] = acc[l];
+        if (l0 + l < nL) acc[l] = cadd(acc[l], cmul(cf[l], x));
     }
+#pragma unroll
+    for (int l = 0; l < LC; ++l)
+      if (l0 + l < nL) out[(int64_t)(l0 + l) * nn + e] = acc[l];
+  }
+}
+
+// Stage 2: rhoL[l][e] (+)= sum over chunks in order of part[chunk][l][e].
+__global__ void fold_reduce_kernel(int64_t m /* nL * nn */, int nchunks, const double2* __restrict__ part,
+                                   double2* __restrict__ rhoL, int accumulate) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    double2 s = accumulate ? rhoL[t] : cmk(0.0, 0.0);
+    for (int c = 0; c < nchunks; ++c) s = cadd(s, part[(int64_t)c * m + t]);
+    rhoL[t] = s;
   }
 }
 

@@ -89,6 +89,24 @@ LQM_FN double team_max(const Team& T, double v, double* red) {
 #endif
 }
 
+// Two sums with ONE barrier: each caller alternates between two disjoint
+// `red` halves (>= 64 doubles each) so that a half is only rewritten after
+// another barrier has separated it from its last reads.
+LQM_FN void team_sum2_1b(const Team& T, double& a, double& b, double* red) {
+#if defined(__CUDACC__)
+  a = warp_sum(a);
+  b = warp_sum(b);
+  if (T.lane == 0) { red[2 * T.wid] = a; red[2 * T.wid + 1] = b; }
+  __syncthreads();
+  double sa = 0.0, sb = 0.0;
+  for (int w = 0; w < T.nw; ++w) { sa += red[2 * w]; sb += red[2 * w + 1]; }
+  a = sa;
+  b = sb;
+#else
+  (void)T; (void)red; (void)a; (void)b;
+#endif
+}
+
 // ---- complex helpers (interleaved re/im, ABI-identical to Julia ComplexF64) ----
 LQM_FN double2 cmk(double re, double im) { double2 z; z.x = re; z.y = im; return z; }
 LQM_FN double2 cadd(double2 a, double2 b) { return cmk(a.x + b.x, a.y + b.y); }

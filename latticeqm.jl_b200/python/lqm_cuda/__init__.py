@@ -142,8 +142,9 @@ class Context:
         return ms.value, el.value, al.value
 
     def phase_cycles(self):
-        """Eigensolver SM cycles per stage (bloch, householder, d&c, back-transform, sync)."""
-        out = (_D * 5)()
+        """Eigensolver SM cycles per stage: bloch, householder, d&c, back-transform, sync,
+        then the d&c merge steps (zsort, deflate, secular, zhat, vectors, ranks, update, copy)."""
+        out = (_D * 13)()
         self.check(_lib.lqm_ctx_phase_cycles(self._h, out))
         return list(out)
 

@@ -26,7 +26,7 @@ extern "C" int lqm_emul_eigh(int n, int nR, int dim, const double* blocks, const
   const size_t nn = (size_t)n * n;
   const int lda = n + 1;  // padded leading dimension, as the shared-memory path
   std::vector<double2> A((size_t)n * lda), cbuf(5 * n + 2 + nR + 8 * n + 256);
-  std::vector<double> dbuf(13 * (size_t)n + 36), Q(nn), Qt(nn), Us(nn);
+  std::vector<double> dbuf(13 * (size_t)n + 132), Q(nn), Qt(nn), Us(nn);
   std::vector<int> ibuf(10 * (size_t)n);
   EighVec S;
   S.tau = cbuf.data(); S.v = S.tau + n; S.w = S.tau + 2 * n; S.vn = S.tau + 3 * n; S.pn = S.tau + 4 * n;
@@ -69,7 +69,7 @@ extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double*
   P.hi = PH.buf.data() + PH.off_hi;
   P.owner = PH.buf.data() + PH.off_own;
   const size_t nn = (size_t)n * n;
-  std::vector<double> dbuf(13 * (size_t)n + 36), Qt(nn), Us(nn);
+  std::vector<double> dbuf(13 * (size_t)n + 132), Qt(nn), Us(nn);
   std::vector<int> ibuf(10 * (size_t)n);
   std::vector<double2> cbuf(5 * n + 2 + 8 * n + 256);
   EighVec S;
