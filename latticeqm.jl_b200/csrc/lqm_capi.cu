@@ -185,7 +185,11 @@ void check_hops(const lqm_hops* H) {
   if (!H || !H->blocks) fail(LQM_EINVAL, "null hops");
 }
 
-int eigh_threads(int n) { return n <= 16 ? 32 : (n <= 32 ? 64 : (n <= 64 ? 128 : 256)); }
+int eigh_threads(int n) { return n <= 16 ? 32 : (n <= 32 ? 64 : (n < 64 ? 128 : 512)); }
+
+// eigh_kernel instantiation for a block size (512 threads from n = 64 on).
+using EighFn = void (*)(EighArgs);
+EighFn eigh_fn(int nt) { return nt > 256 ? &eigh_kernel<512> : &eigh_kernel<256>; }
 
 void timer_start(lqm_ctx* ctx) { ck(cudaEventRecord(ctx->ev0, ctx->stream), "event"); }
 void timer_stop(lqm_ctx* ctx) {
@@ -214,9 +218,10 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   const int a_in_smem = Ls.total <= 225 * 1024;
   if (!a_in_smem) Ls = eigh_smem_layout(n, (int)H->nR, nt, 0);
   if (Ls.total > 225 * 1024) fail(LQM_EINVAL, "n=%d, nR=%lld exceeds the shared-memory plan", n, (long long)H->nR);
-  ck(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total), "smem attr");
+  const EighFn kfn = eigh_fn(nt);
+  ck(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total), "smem attr");
   int per_sm = 0;
-  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_kernel, nt, Ls.total), "occupancy");
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, Ls.total), "occupancy");
   if (per_sm < 1) fail(LQM_EINVAL, "eigh kernel cannot be resident for n=%d", n);
   const bool need_uwork = ro && !d_U && !a_in_smem;
   const int64_t slot = eigh_slot_doubles(n, a_in_smem, need_uwork);
@@ -237,7 +242,7 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   a.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
   std::pair<cudaEvent_t, cudaEvent_t> evs{};
   if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
-  eigh_kernel<<<(unsigned)grid, nt, Ls.total, ctx->stream>>>(a);
+  kfn<<<(unsigned)grid, nt, Ls.total, ctx->stream>>>(a);
   ck(cudaGetLastError(), "eigh_kernel launch");
   if (ctx->stats_on) { ck(cudaEventRecord(evs.second, ctx->stream), "event"); ctx->ev_pending.push_back(evs); }
   ctx->eigh_launches++;
@@ -843,10 +848,11 @@ extern "C" int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32
   const int64_t slot = eigh_slot_doubles(ni, a_in_smem, false);
   const int64_t max_slots = kNoAllocScratchDoubles / slot;
   if (max_slots < 1) return LQM_EINVAL;  // one k-point's scratch exceeds the 64 MiB array
-  if (cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total) != cudaSuccess)
+  const EighFn kfn = eigh_fn(nt);
+  if (cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Ls.total) != cudaSuccess)
     return LQM_ECUDA;
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eigh_kernel, nt, Ls.total) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nt, Ls.total) != cudaSuccess ||
       per_sm < 1)
     return LQM_ECUDA;
   const int64_t grid = std::min<int64_t>(std::min<int64_t>(nk, (int64_t)per_sm * D.sms), max_slots);
@@ -869,7 +875,7 @@ extern "C" int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32
   a.U = (double2*)d_U;
   cudaStream_t st = (cudaStream_t)stream;
   noalloc_plan_kernel<<<1, 1, 0, st>>>(ni);
-  eigh_kernel<<<(unsigned)grid, nt, Ls.total, st>>>(a);
+  kfn<<<(unsigned)grid, nt, Ls.total, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? LQM_OK : LQM_ECUDA;
 }
 

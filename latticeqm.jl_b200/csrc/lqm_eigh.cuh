@@ -225,31 +225,35 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
 // ---------------------------------------------------------------------------
 
 // One root of the secular equation 1 + rho sum_j zl_j^2 / (dl_j - lambda) = 0,
-// dl ascending, rho > 0.  lambda = dl[org] + tau; interior roots take the
-// nearer pole as origin.  Safeguarded two-pole rational steps (each step fits
-// the poles left and right of the root separately to value and slope).
-LQM_FN void secular_root(int k, const double* dl, const double* zl, double rho, int i, int* org_out,
-                         double* tau_out) {
+// dl ascending, rho > 0, solved by one warp: the lanes split the k terms of
+// every sum and all lanes then hold identical scalars.  lambda = dl[org] + tau;
+// interior roots take the nearer pole as origin.  Safeguarded two-pole
+// rational steps (each step fits the poles left and right of the root
+// separately to value and slope), bisection when a step leaves the bracket.
+LQM_FN void secular_root_warp(const Team& T, int k, const double* dl, const double* zl, double rho, int i,
+                              int* org_out, double* tau_out) {
   if (k == 1) { *org_out = 0; *tau_out = rho * zl[0] * zl[0]; return; }
   int org;
   double lo, hi;
   if (i < k - 1) {
     const double gap = dl[i + 1] - dl[i];
     const double mid = 0.5 * gap;
-    double f = 1.0;
-    for (int j = 0; j < k; ++j) f += rho * zl[j] * zl[j] / ((dl[j] - dl[i]) - mid);
+    double f = 0.0;
+    for (int j = T.lane; j < k; j += T.nl) f += rho * zl[j] * zl[j] / ((dl[j] - dl[i]) - mid);
+    f = 1.0 + warp_sum_bcast(f);
     if (f >= 0.0) { org = i; lo = 0.0; hi = mid; }
     else { org = i + 1; lo = -(gap - mid); hi = 0.0; }
   } else {
     double zs = 0.0;
-    for (int j = 0; j < k; ++j) zs += zl[j] * zl[j];
+    for (int j = T.lane; j < k; j += T.nl) zs += zl[j] * zl[j];
+    zs = warp_sum_bcast(zs);
     org = k - 1; lo = 0.0; hi = rho * zs * (1.0 + 4.0 * LQM_DEPS) + 1e-300;
   }
   const double dorg = dl[org];
   double tau = 0.5 * (lo + hi);
   for (int it = 0; it < 80; ++it) {
     double psi1 = 0.0, dpsi1 = 0.0, psi2 = 0.0, dpsi2 = 0.0, abss = 0.0;
-    for (int j = 0; j < k; ++j) {
+    for (int j = T.lane; j < k; j += T.nl) {
       const double del = (dl[j] - dorg) - tau;
       const double t = zl[j] / del;
       const double term = rho * zl[j] * t;
@@ -257,12 +261,17 @@ LQM_FN void secular_root(int k, const double* dl, const double* zl, double rho, 
       if (j <= i) { psi1 += term; dpsi1 += dterm; } else { psi2 += term; dpsi2 += dterm; }
       abss += fabs(term);
     }
+    psi1 = warp_sum_bcast(psi1);
+    dpsi1 = warp_sum_bcast(dpsi1);
+    psi2 = warp_sum_bcast(psi2);
+    dpsi2 = warp_sum_bcast(dpsi2);
+    abss = warp_sum_bcast(abss);
     const double f = 1.0 + psi1 + psi2;
     if (f == 0.0) break;
     if (f < 0.0) lo = tau; else hi = tau;
     if (fabs(f) <= 8.0 * LQM_DEPS * (1.0 + abss) * 2.0) break;
     const double a = (dl[i] - dorg) - tau;
-    double x;
+    double x = 0.0;
     bool ok = true;
     if (i < k - 1) {
       const double b = (dl[i + 1] - dorg) - tau;
@@ -308,11 +317,12 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
       const int j = S.perm[p];
       if (rho * fabs(S.z[j]) <= tol) { S.dval[lo + nd] = S.D[j]; S.dcol[lo + nd] = j; ++nd; continue; }
       if (pj < 0) { pj = j; continue; }
-      double sv = S.z[pj], cv = S.z[j];
-      const double tau = hypot(cv, sv);
+      const double zp = S.z[pj], zj = S.z[j];
       const double t = S.D[j] - S.D[pj];
-      cv /= tau; sv = -sv / tau;
-      if (fabs(t * cv * sv) <= tol) {
+      // |t c s| <= tol with c = zj/tau, s = -zp/tau, tau^2 = zj^2 + zp^2 (no division)
+      if (fabs(t * zj * zp) <= tol * (zj * zj + zp * zp)) {
+        const double tau = hypot(zj, zp);
+        const double cv = zj / tau, sv = -zp / tau;
         S.z[j] = tau; S.z[pj] = 0.0;
         S.ri[lo + nr] = pj; S.rj[lo + nr] = j; S.rc[lo + nr] = cv; S.rs[lo + nr] = sv; ++nr;
         const double t2 = S.D[pj] * cv * cv + S.D[j] * sv * sv;
@@ -409,14 +419,14 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     team_sync();
     LQM_SUBTICK(1);
     // C: secular roots
-    for (int i = T.tid; i < n; i += T.nt) {
+    for (int i = T.wid; i < n; i += T.nw) {  // one warp per root
       const int nd = own[i];
       if (nd < 0) continue;
       const int lo = P.lo[nd], q = i - lo, k = S.nk[nd];
       if (q >= k) continue;
       int org; double tr;
-      secular_root(k, S.dl + lo, S.zl + lo, S.nrho[nd], q, &org, &tr);
-      S.org[lo + q] = org; S.troot[lo + q] = tr;
+      secular_root_warp(T, k, S.dl + lo, S.zl + lo, S.nrho[nd], q, &org, &tr);
+      if (T.lane == 0) { S.org[lo + q] = org; S.troot[lo + q] = tr; }
     }
     team_sync();
     LQM_SUBTICK(2);
@@ -496,10 +506,20 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       double* dst = Qt + (int64_t)S.newpos[c] * n;
       if (it < k) {
         const double* uc = Us + lo + (int64_t)(lo + it) * n;
-        for (int r = lo + T.lane; r < hi; r += T.nl) {
-          double acc = 0.0;
-          for (int p = 0; p < k; ++p) acc += Q[r + (int64_t)S.colnd[lo + p] * n] * uc[p];
-          dst[r] = acc;
+        for (int r0 = lo + T.lane; r0 < hi; r0 += 3 * T.nl) {
+          const int r1 = r0 + T.nl, r2 = r0 + 2 * T.nl;
+          const bool h1 = r1 < hi, h2 = r2 < hi;
+          double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+          for (int p = 0; p < k; ++p) {
+            const double* qc = Q + (int64_t)S.colnd[lo + p] * n;
+            const double u = uc[p];
+            a0 += qc[r0] * u;
+            if (h1) a1 += qc[r1] * u;
+            if (h2) a2 += qc[r2] * u;
+          }
+          dst[r0] = a0;
+          if (h1) dst[r1] = a1;
+          if (h2) dst[r2] = a2;
         }
       } else {
         const double* src = Q + (int64_t)S.dcol[lo + it - k] * n;

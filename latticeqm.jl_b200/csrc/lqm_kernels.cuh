@@ -85,7 +85,8 @@ __device__ __forceinline__ void carve_vectors(unsigned char* smem, const EighSme
   S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
 }
 
-__global__ void __launch_bounds__(256) eigh_kernel(EighArgs a) {
+template <int NT>
+__global__ void __launch_bounds__(NT) eigh_kernel(EighArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Team T = make_team();
   const int n = a.n;

@@ -50,11 +50,18 @@ LQM_FN double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+// Butterfly sum whose result is then taken from lane 0, so every lane holds
+// bit-identical values (uniform control flow may branch on it).
+LQM_FN double warp_sum_bcast(double v) {
+  v = warp_sum(v);
+  return __shfl_sync(0xffffffffu, v, 0);
+}
 #else
 LQM_FN Team make_host_team() { Team t = {0, 1, 0, 1, 0, 1}; return t; }
 LQM_FN void team_sync() {}
 LQM_FN double warp_sum(double v) { return v; }
 LQM_FN double warp_max(double v) { return v; }
+LQM_FN double warp_sum_bcast(double v) { return v; }
 #endif
 
 // Deterministic team reduction: warp trees, then every thread sums the warp
