@@ -62,8 +62,10 @@ int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, i
  * timing is enabled: [0] Bloch sum, [1] Householder, [2] divide and conquer,
  * [3] bands + back-transformation, [4] end-of-k barrier, [5..12] the divide
  * and conquer merge steps (z/sort, deflation, secular roots, Gu-Eisenstat z,
- * vectors/rotations/values, ranks, update, copy back).  New (profiling). */
-int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles /* [13] */);
+ * vectors/rotations/values, ranks, update, copy back), [13..15] the
+ * Householder steps (trailing pass, mat-vec reduction, next column and
+ * reflector).  New (profiling). */
+int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles /* [16] */);
 
 /* Upload a dense Hops (src/modules/TightBinding/types.jl:54-60, DenseHops):
  * keys d x nR (Int64), blocks n x n x nR column-major ComplexF64 in the same

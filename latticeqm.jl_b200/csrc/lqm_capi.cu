@@ -464,7 +464,7 @@ int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles) {
       wait_stream(ctx);
       ck(cudaMemcpy(h, ctx->d_phase, sizeof(h), cudaMemcpyDeviceToHost), "D2H");
     }
-    for (int i = 0; i < 13; ++i) cycles[i] = (double)h[i];
+    for (int i = 0; i < 16; ++i) cycles[i] = (double)h[i];
   });
 }
 

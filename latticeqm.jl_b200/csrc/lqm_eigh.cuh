@@ -153,7 +153,21 @@ LQM_FN void store_reflector(const Team& T, int mb, double2* A, int lda, int o, d
 // Householder tridiagonalisation with 3 barriers per step:
 //   pass (update j, mat-vec with reflector j+1) | p, p^H v -> alpha |
 //   w, update of the next column, its norm -> next reflector scalars.
-LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, EighVec& S) {
+LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, EighVec& S,
+                                 unsigned long long* sub = nullptr) {
+#if defined(__CUDA_ARCH__)
+  long long tsub = clock64();
+  if (T.tid != 0) sub = nullptr;
+#define LQM_HTICK(i_)                                          \
+  if (sub) {                                                   \
+    const long long t_ = clock64();                            \
+    sub[i_] += (unsigned long long)(t_ - tsub);                \
+    tsub = t_;                                                 \
+  }
+#else
+  (void)sub;
+#define LQM_HTICK(i_)
+#endif
   if (n == 1) {
     if (T.tid == 0) S.d[0] = A[0].x;
     team_sync();
@@ -177,8 +191,10 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
   for (int j = -1; j <= n - 3; ++j) {
     const int o = j + 2;
     const int mb = n - o;
+    LQM_HTICK(2);
     trailing_pass(T, mb, A, lda, o, vc, wc, j >= 0, scal, vx, S.pbuf, n);
     team_sync();
+    LQM_HTICK(0);
     store_reflector(T, mb, A, lda, o, scal, vx);
     // p = tau_{j+1} * row sums; alpha = -1/2 tau (p^H x)
     double pr = 0.0, pi = 0.0;
@@ -191,6 +207,7 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
       pr += q.x; pi += q.y;
     }
     team_sum2_1b(T, pr, pi, redA);
+    LQM_HTICK(1);
     const double2 alpha = cmul(cmk(-0.5 * tnext.x, -0.5 * tnext.y), cmk(pr, pi));
     // w = p + alpha x; column o gets update j+1; norm of its rows o+2.. for reflector j+2
     const double2 w0 = cadd(p[0], alpha);  // x[0] = 1
@@ -218,62 +235,89 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
     }
   }
   team_sync();
+  LQM_HTICK(2);
+#undef LQM_HTICK
 }
 
 // ---------------------------------------------------------------------------
 // 3. Divide and conquer on the symmetric tridiagonal (d, e).
 // ---------------------------------------------------------------------------
 
+// Lane-group width for the secular roots of a merge with k non-deflated
+// values: about four terms per lane, at most a warp.
+LQM_FN int secular_width(int k, int nl) {
+  int w = 1;
+  while (w < nl && 4 * w < k) w <<= 1;
+  return w;
+}
+
 // One root of the secular equation 1 + rho sum_j zl_j^2 / (dl_j - lambda) = 0,
-// dl ascending, rho > 0, solved by one warp: the lanes split the k terms of
-// every sum and all lanes then hold identical scalars.  lambda = dl[org] + tau;
+// dl ascending, rho > 0, solved by a group of `gw` lanes (g = lane within the
+// group): the lanes split the k terms of every sum and all lanes of the group
+// then hold identical scalars.  `active` is false for lanes without a root;
+// they still take part in every shuffle of their warp.  lambda = dl[org] + tau;
 // interior roots take the nearer pole as origin.  Safeguarded two-pole
 // rational steps (each step fits the poles left and right of the root
 // separately to value and slope), bisection when a step leaves the bracket.
-LQM_FN void secular_root_warp(const Team& T, int k, const double* dl, const double* zl, double rho, int i,
-                              int* org_out, double* tau_out) {
-  if (k == 1) { *org_out = 0; *tau_out = rho * zl[0] * zl[0]; return; }
-  int org;
-  double lo, hi;
-  if (i < k - 1) {
-    const double gap = dl[i + 1] - dl[i];
-    const double mid = 0.5 * gap;
-    double f = 0.0;
-    for (int j = T.lane; j < k; j += T.nl) f += rho * zl[j] * zl[j] / ((dl[j] - dl[i]) - mid);
-    f = 1.0 + warp_sum_bcast(f);
-    if (f >= 0.0) { org = i; lo = 0.0; hi = mid; }
-    else { org = i + 1; lo = -(gap - mid); hi = 0.0; }
-  } else {
-    double zs = 0.0;
-    for (int j = T.lane; j < k; j += T.nl) zs += zl[j] * zl[j];
-    zs = warp_sum_bcast(zs);
-    org = k - 1; lo = 0.0; hi = rho * zs * (1.0 + 4.0 * LQM_DEPS) + 1e-300;
+LQM_FN void secular_root_group(bool active, int gw, int g, int k, const double* dl, const double* zl, double rho,
+                               int i, int* org_out, double* tau_out) {
+  int org = 0;
+  double lo = 0.0, hi = 0.0, f0 = 0.0, zs = 0.0;
+  const bool last = active && (i >= k - 1);
+  double gap = 0.0, mid = 0.0;
+  if (active && !last) {
+    gap = dl[i + 1] - dl[i];
+    mid = 0.5 * gap;
+    for (int j = g; j < k; j += gw) f0 += rho * zl[j] * zl[j] / ((dl[j] - dl[i]) - mid);
   }
-  const double dorg = dl[org];
-  double tau = 0.5 * (lo + hi);
-  for (int it = 0; it < 80; ++it) {
-    double psi1 = 0.0, dpsi1 = 0.0, psi2 = 0.0, dpsi2 = 0.0, abss = 0.0;
-    for (int j = T.lane; j < k; j += T.nl) {
-      const double del = (dl[j] - dorg) - tau;
-      const double t = zl[j] / del;
-      const double term = rho * zl[j] * t;
-      const double dterm = rho * t * t;
-      if (j <= i) { psi1 += term; dpsi1 += dterm; } else { psi2 += term; dpsi2 += dterm; }
-      abss += fabs(term);
+  if (last)
+    for (int j = g; j < k; j += gw) zs += zl[j] * zl[j];
+  f0 = group_sum_bcast(f0, gw);
+  zs = group_sum_bcast(zs, gw);
+  if (active) {
+    if (k == 1) {
+      org = 0; lo = hi = rho * zl[0] * zl[0];
+    } else if (!last) {
+      if (1.0 + f0 >= 0.0) { org = i; lo = 0.0; hi = mid; }
+      else { org = i + 1; lo = -(gap - mid); hi = 0.0; }
+    } else {
+      org = k - 1; lo = 0.0; hi = rho * zs * (1.0 + 4.0 * LQM_DEPS) + 1e-300;
     }
-    psi1 = warp_sum_bcast(psi1);
-    dpsi1 = warp_sum_bcast(dpsi1);
-    psi2 = warp_sum_bcast(psi2);
-    dpsi2 = warp_sum_bcast(dpsi2);
-    abss = warp_sum_bcast(abss);
+  }
+  bool done = !active || k == 1;
+  const double dorg = active ? dl[org] : 0.0;
+  double tau = (k == 1 && active) ? lo : 0.5 * (lo + hi);
+  for (int it = 0; it < 80; ++it) {
+#if defined(__CUDA_ARCH__)
+    if (__all_sync(0xffffffffu, done)) break;
+#else
+    if (done) break;
+#endif
+    double psi1 = 0.0, dpsi1 = 0.0, psi2 = 0.0, dpsi2 = 0.0, abss = 0.0;
+    if (!done) {
+      for (int j = g; j < k; j += gw) {
+        const double del = (dl[j] - dorg) - tau;
+        const double t = zl[j] / del;
+        const double term = rho * zl[j] * t;
+        const double dterm = rho * t * t;
+        if (j <= i) { psi1 += term; dpsi1 += dterm; } else { psi2 += term; dpsi2 += dterm; }
+        abss += fabs(term);
+      }
+    }
+    psi1 = group_sum_bcast(psi1, gw);
+    dpsi1 = group_sum_bcast(dpsi1, gw);
+    psi2 = group_sum_bcast(psi2, gw);
+    dpsi2 = group_sum_bcast(dpsi2, gw);
+    abss = group_sum_bcast(abss, gw);
+    if (done) continue;
     const double f = 1.0 + psi1 + psi2;
-    if (f == 0.0) break;
+    if (f == 0.0) { done = true; continue; }
     if (f < 0.0) lo = tau; else hi = tau;
-    if (fabs(f) <= 8.0 * LQM_DEPS * (1.0 + abss) * 2.0) break;
+    if (fabs(f) <= 8.0 * LQM_DEPS * (1.0 + abss) * 2.0) { done = true; continue; }
     const double a = (dl[i] - dorg) - tau;
     double x = 0.0;
     bool ok = true;
-    if (i < k - 1) {
+    if (!last) {
       const double b = (dl[i + 1] - dorg) - tau;
       const double s1 = a * a * dpsi1, s2 = b * b * dpsi2;
       const double c = 1.0 + (psi1 - a * dpsi1) + (psi2 - b * dpsi2);
@@ -294,8 +338,8 @@ LQM_FN void secular_root_warp(const Team& T, int k, const double* dl, const doub
     if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
     const double chg = fabs(tn - tau);
     tau = tn;
-    if (chg <= 2.0 * LQM_DEPS * fabs(tn)) break;
-    if (hi - lo <= 2.0 * LQM_DEPS * fmax(fabs(lo), fabs(hi))) break;
+    if (chg <= 2.0 * LQM_DEPS * fabs(tn)) done = true;
+    else if (hi - lo <= 2.0 * LQM_DEPS * fmax(fabs(lo), fabs(hi))) done = true;
   }
   *org_out = org;
   *tau_out = tau;
@@ -419,14 +463,29 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     team_sync();
     LQM_SUBTICK(1);
     // C: secular roots
-    for (int i = T.wid; i < n; i += T.nw) {  // one warp per root
-      const int nd = own[i];
-      if (nd < 0) continue;
-      const int lo = P.lo[nd], q = i - lo, k = S.nk[nd];
-      if (q >= k) continue;
-      int org; double tr;
-      secular_root_warp(T, k, S.dl + lo, S.zl + lo, S.nrho[nd], q, &org, &tr);
-      if (T.lane == 0) { S.org[lo + q] = org; S.troot[lo + q] = tr; }
+    {
+      // lane-group width from the largest merge of this height (uniform)
+      int kmax = 1;
+      for (int nd = h0; nd < h1; ++nd) kmax = (S.nk[nd] > kmax) ? S.nk[nd] : kmax;
+      const int gw = secular_width(kmax, T.nl);
+      const int gpw = T.nl / gw;               // root groups per warp
+      const int g = T.lane % gw;
+      for (int base = T.wid * gpw; base < n; base += T.nw * gpw) {  // warp-uniform loop
+        const int i = base + T.lane / gw;
+        bool active = false;
+        int lo = 0, q = 0, k = 0, nd = -1;
+        if (i < n) {
+          nd = own[i];
+          if (nd >= 0) {
+            lo = P.lo[nd]; q = i - lo; k = S.nk[nd];
+            active = q < k;
+          }
+        }
+        int org = 0; double tr = 0.0;
+        secular_root_group(active, gw, g, active ? k : 1, active ? S.dl + lo : S.dl,
+                           active ? S.zl + lo : S.zl, active ? S.nrho[nd] : 1.0, q, &org, &tr);
+        if (active && g == 0) { S.org[lo + q] = org; S.troot[lo + q] = tr; }
+      }
     }
     team_sync();
     LQM_SUBTICK(2);

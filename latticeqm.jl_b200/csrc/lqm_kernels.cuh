@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(NT) eigh_kernel(EighArgs a) {
   const bool prof = a.phase_cycles != nullptr;
   unsigned long long acc[5] = {0, 0, 0, 0, 0};
   unsigned long long dsub[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long hsub[3] = {0, 0, 0};
   long long tc = 0;
 #define LQM_TICK(ph_)                                                                   \
   if (prof) {                                                                          \
@@ -126,7 +127,7 @@ __global__ void __launch_bounds__(NT) eigh_kernel(EighArgs a) {
     team_sync();
     bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, lda);
     LQM_TICK(PH_BLOCH);
-    hetrd_lower(T, n, A, lda, S);
+    hetrd_lower(T, n, A, lda, S, prof ? hsub : nullptr);
     if (in_smem) {
       for (int c = T.wid; c < n - 1; c += T.nw)
         for (int r = c + 1 + T.lane; r < n; r += T.nl) R[r + (int64_t)c * n] = A[r + (int64_t)c * lda];
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(NT) eigh_kernel(EighArgs a) {
   if (prof && T.tid == 0) {
     for (int i = 0; i < 5; ++i) atomicAdd(&a.phase_cycles[i], acc[i]);
     for (int i = 0; i < 8; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + i], dsub[i]);
+    for (int i = 0; i < 3; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + 8 + i], hsub[i]);
   }
 }
 

@@ -56,12 +56,19 @@ LQM_FN double warp_sum_bcast(double v) {
   v = warp_sum(v);
   return __shfl_sync(0xffffffffu, v, 0);
 }
+// Sum over aligned groups of `width` lanes (power of two); every lane of a
+// group receives its group leader's value.  All 32 lanes must call it.
+LQM_FN double group_sum_bcast(double v, int width) {
+  for (int o = width >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, width);
+  return __shfl_sync(0xffffffffu, v, 0, width);
+}
 #else
 LQM_FN Team make_host_team() { Team t = {0, 1, 0, 1, 0, 1}; return t; }
 LQM_FN void team_sync() {}
 LQM_FN double warp_sum(double v) { return v; }
 LQM_FN double warp_max(double v) { return v; }
 LQM_FN double warp_sum_bcast(double v) { return v; }
+LQM_FN double group_sum_bcast(double v, int width) { (void)width; return v; }
 #endif
 
 // Deterministic team reduction: warp trees, then every thread sums the warp

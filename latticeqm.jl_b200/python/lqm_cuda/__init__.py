@@ -144,7 +144,7 @@ class Context:
     def phase_cycles(self):
         """Eigensolver SM cycles per stage: bloch, householder, d&c, back-transform, sync,
         then the d&c merge steps (zsort, deflate, secular, zhat, vectors, ranks, update, copy)."""
-        out = (_D * 13)()
+        out = (_D * 16)()
         self.check(_lib.lqm_ctx_phase_cycles(self._h, out))
         return list(out)
 
