@@ -50,14 +50,23 @@ def eigh_flops_per_k(n, nR):
     return 8.0 * nR * n * n + (16.0 / 3.0 + 8.0) * n ** 3
 
 
-def kgrid(rank, world):
-    """Rank r's 256x256 slice of a (256*world) x 256 grid (first index fastest)."""
+def kgrid(rank, world, nk_lin=NK_LIN):
+    """Rank r's nk_lin x nk_lin slice of a (nk_lin*world) x nk_lin grid (first index
+    fastest): rank r takes the k1 values (i*world + r)/(nk_lin*world)."""
     import numpy as np
-    n1 = NK_LIN * world
-    i = np.arange(NK_LIN) * world + rank
-    kx = np.tile(i / n1, NK_LIN)
-    ky = np.repeat(np.arange(NK_LIN) / NK_LIN, NK_LIN)
+    n1 = nk_lin * world
+    i = np.arange(nk_lin) * world + rank
+    kx = np.tile(i / n1, nk_lin)
+    ky = np.repeat(np.arange(nk_lin) / nk_lin, nk_lin)
     return np.asfortranarray(np.vstack([kx, ky]))
+
+
+def reduce_shards(dist, tensors, world):
+    """rho_L and DOS are averages over the whole grid: sum the per-rank averages
+    and divide by the number of ranks (each rank weights its own k by 1/nk_local)."""
+    for t in tensors:
+        dist.all_reduce(t)
+        t.div_(world)
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -309,10 +318,7 @@ def main():
             if per_model_ms is not None:
                 per_model_ms[s["n"]] = per_model_ms.get(s["n"], 0.0) + ctx.stats()[0] - m0
             if world > 1:  # rho_L and DOS are sums over the whole grid: one exchange per model
-                dist.all_reduce(s["rho"])
-                dist.all_reduce(s["dos"])
-                s["rho"].div_(world)
-                s["dos"].div_(world)
+                reduce_shards(dist, (s["rho"], s["dos"]), world)
 
     fp64_peak = measured_fp64_peak(torch, dev)
     for _ in range(args.warmup):

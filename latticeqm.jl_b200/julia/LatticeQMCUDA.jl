@@ -1,0 +1,243 @@
+"""
+    LatticeQMCUDA
+
+`multimode=:cuda` for LatticeQM.jl: the k-space routines `bandmatrix`/`getbands`,
+`getdensitymatrix!`, `getdos`, `chemicalpotential` and `solvehartreefock` run on one
+B200 through `libkspace.so` (C ABI declared in `include/kspace.h`).  No CPU
+fallback: a routine that cannot run on the device throws.
+
+Usage:
+
+    using LatticeQM, LatticeQMCUDA
+    LatticeQMCUDA.enable!()              # adds :cuda to Parallel.to_executor
+    bands = getbands(h, ks; multimode=:cuda)
+
+`enable!` installs the executor; the routine-level hooks listed in INTEGRATION.md
+(a few lines in LatticeQM's `bandmatrix`, `densitymatrix_compute_add!`,
+`dos_compute!` and `solveselfconsistent!`) call the `cuda_*` functions below when
+the executor is a `CudaExec`.
+"""
+module LatticeQMCUDA
+
+using LatticeQM
+import LatticeQM.Parallel
+import LatticeQM.TightBinding: Hops
+import SparseArrays: SparseMatrixCSC
+
+const LIB = Ref{String}(joinpath(@__DIR__, "..", "lib", "libkspace.so"))
+
+struct CudaExec <: Parallel.Executor
+    device::Int
+    precision::Symbol   # :fp64 (only :fp64 is built)
+end
+CudaExec() = CudaExec(0, :fp64)
+
+# ---------------------------------------------------------------- context
+mutable struct Context
+    ptr::Ptr{Cvoid}
+end
+const CONTEXTS = Dict{Int,Context}()
+
+function context(device::Int=0)
+    get!(CONTEXTS, device) do
+        out = Ref{Ptr{Cvoid}}(C_NULL)
+        st = ccall((:lqm_ctx_create, LIB[]), Cint, (Cint, Ref{Ptr{Cvoid}}), device, out)
+        st == 0 || error("libkspace: cannot create a context on CUDA device $device (status $st)")
+        ctx = Context(out[])
+        finalizer(c -> ccall((:lqm_ctx_destroy, LIB[]), Cint, (Ptr{Cvoid},), c.ptr), ctx)
+        ctx
+    end
+end
+
+function check(ctx::Context, st::Integer)
+    st == 0 && return nothing
+    msg = unsafe_string(ccall((:lqm_last_error, LIB[]), Cstring, (Ptr{Cvoid},), ctx.ptr))
+    st == -1 ? throw(ArgumentError(msg)) : error("libkspace status $st: $msg")
+end
+
+# ---------------------------------------------------------------- Hops upload
+mutable struct DeviceHops
+    ptr::Ptr{Cvoid}
+    ctx::Context
+    keys::Vector{Vector{Int}}
+end
+
+"""Upload H in its own key order (the Bloch-sum order of `fouriersum!`)."""
+function upload(ctx::Context, H)
+    ks = collect(keys(H))
+    d = length(first(ks))
+    n = size(H[first(ks)], 1)
+    K = Int64[k[i] for i in 1:d, k in ks]                 # d x nR
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    if first(values(H)) isa SparseMatrixCSC
+        mats = [H[k] for k in ks]
+        colptr = [Ptr{Int64}(pointer(m.colptr)) for m in mats]
+        rowval = [Ptr{Int64}(pointer(m.rowval)) for m in mats]
+        nzval = [Ptr{Float64}(pointer(m.nzval)) for m in mats]
+        GC.@preserve mats colptr rowval nzval begin
+            check(ctx, ccall((:lqm_hops_upload_csc, LIB[]), Cint,
+                (Ptr{Cvoid}, Int64, Int64, Int32, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Ptr{Ptr{Float64}},
+                 Ref{Ptr{Cvoid}}), ctx.ptr, n, length(ks), d, K, colptr, rowval, nzval, out))
+        end
+    else
+        B = Array{ComplexF64}(undef, n, n, length(ks))
+        for (r, k) in enumerate(ks)
+            B[:, :, r] .= H[k]
+        end
+        check(ctx, ccall((:lqm_hops_upload_dense, LIB[]), Cint,
+            (Ptr{Cvoid}, Int64, Int64, Int32, Ptr{Int64}, Ptr{ComplexF64}, Ref{Ptr{Cvoid}}),
+            ctx.ptr, n, length(ks), d, K, B, out))
+    end
+    dh = DeviceHops(out[], ctx, ks)
+    finalizer(h -> ccall((:lqm_hops_free, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), h.ctx.ptr, h.ptr), dh)
+    dh
+end
+
+precision_code(e::CudaExec) = e.precision === :fp64 ? Cint(0) :
+    throw(ArgumentError("precision=$(e.precision): only :fp64 is built"))
+
+# ---------------------------------------------------------------- routines
+"""bands (n x nk) and, with `vectors=true`, U (n x n x nk): `bandmatrix` without projectors."""
+function cuda_bandmatrix(H, ks::AbstractMatrix{Float64}, exec::CudaExec; vectors::Bool=false)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    nk = size(ks, 2)
+    bands = zeros(Float64, n, nk)
+    U = vectors ? zeros(ComplexF64, n, n, nk) : ComplexF64[]
+    check(ctx, ccall((:lqm_bandmatrix, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ptr{ComplexF64}),
+        ctx.ptr, dh.ptr, nk, Matrix{Float64}(ks), vectors, precision_code(exec), bands,
+        vectors ? U : Ptr{ComplexF64}(C_NULL)))
+    vectors ? (bands, U) : bands
+end
+
+"""`getdensitymatrix!(ρs, H, ks, kweights, μ; T)` on the device; returns the band energy."""
+function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
+                             μ::Float64, T::Real, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    Lk = collect(keys(ρs))
+    d = length(first(Lk))
+    n = size(H[first(keys(H))], 1)
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    rho = zeros(ComplexF64, n, n, length(Lk))
+    eb = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_densitymatrix, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Int64, Ptr{Int64},
+         Ptr{ComplexF64}, Ref{Float64}, Cint),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Vector{Float64}(kweights), μ, Float64(T),
+        length(Lk), L, rho, eb, precision_code(exec)))
+    for (i, k) in enumerate(Lk)
+        ρs[k] .= view(rho, :, :, i)
+    end
+    eb[]
+end
+
+"""`chemicalpotential(H, ks, filling; T)` from device bands (unweighted mean, as the reference)."""
+function cuda_chemicalpotential(H, ks::AbstractMatrix{Float64}, filling::Real, exec::CudaExec; T::Real=0.0)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    μ = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_chemicalpotential, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Ref{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Ptr{Float64}(C_NULL), Float64(filling),
+        Float64(T), μ))
+    μ[]
+end
+
+"""`dos_compute!` on the device: DOS(ω) = Σ_k w_k Σ_n Im[1/(ω - iΓ - ε)] (/nk when unweighted)."""
+function cuda_dos!(DOS::AbstractVector, h, ωs::AbstractVector, ks::AbstractMatrix{Float64}, exec::CudaExec;
+                   Γ::Real, kweights=nothing)
+    ctx = context(exec.device)
+    dh = upload(ctx, h)
+    out = zeros(Float64, length(ωs))
+    w = kweights === nothing ? Ptr{Float64}(C_NULL) : Vector{Float64}(kweights)
+    check(ctx, ccall((:lqm_dos, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Int64, Ptr{Float64}, Float64, Ptr{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), w, length(ωs), Vector{Float64}(ωs), Float64(Γ), out))
+    DOS .= out
+end
+
+const LOG_CB = Ref{Any}(nothing)
+function _log_trampoline(it::Int64, E::Float64, res::Float64, ekin::Float64, eband::Float64, eH::Float64,
+                         eF::Float64, μ::Float64, user::Ptr{Cvoid})::Cint
+    cb = LOG_CB[]
+    cb === nothing && return Cint(0)
+    info = (ϵkin=ekin, ϵband=eband, ϵH=eH, ϵF=eF, μ=μ)
+    applicable(cb, it, E, res, info) ? cb(it, E, res, info) : cb(it, E, res)
+    Cint(0)
+end
+
+"""Device-resident `solvehartreefock` with linear mixing; returns (ρ, ϵ_GS, info, converged, residual)."""
+function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractMatrix{Float64}, exec::CudaExec;
+                               T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
+                               log_callback=nothing)
+    ctx = context(exec.device)
+    dh = upload(ctx, h)
+    dv = upload(ctx, v)
+    Lk = collect(keys(ρ_init))
+    d = length(first(Lk))
+    n = size(h[first(keys(h))], 1)
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    rho = Array{ComplexF64}(undef, n, n, length(Lk))
+    for (i, k) in enumerate(Lk)
+        rho[:, :, i] .= ρ_init[k]
+    end
+    out = zeros(Float64, 9)
+    LOG_CB[] = log_callback
+    cb = @cfunction(_log_trampoline, Cint, (Int64, Float64, Float64, Float64, Float64, Float64, Float64,
+                                             Float64, Ptr{Cvoid}))
+    check(ctx, ccall((:lqm_scf_hf, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Float64,
+         Float64, Int64, Int64, Ptr{Int64}, Ptr{ComplexF64}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}),
+        ctx.ptr, dh.ptr, dv.ptr, size(ks, 2), Matrix{Float64}(ks), Ptr{Float64}(C_NULL), Float64(filling),
+        Float64(T), Float64(β), Float64(tol), iterations, length(Lk), L, rho, cb, C_NULL, out))
+    LOG_CB[] = nothing
+    ρ = Hops(Dict(k => rho[:, :, i] for (i, k) in enumerate(Lk)))
+    info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
+    ρ, out[1], info, out[8] != 0, out[7]
+end
+
+# ---------------------------------------------------------------- executor hooks
+# Per-k closures cannot run on the device: the generic k-loops refuse CudaExec.
+Parallel.kspace_foreach!(body!, ks::AbstractMatrix, exec::CudaExec; kwargs...) =
+    throw(ArgumentError("routine not ported to :cuda"))
+Parallel.kspace_reduce!(body!, output, ks::AbstractMatrix, exec::CudaExec; kwargs...) =
+    throw(ArgumentError("routine not ported to :cuda"))
+Parallel.configure_blas!(::CudaExec; kwargs...) = nothing
+
+"""
+    enable!()
+
+Adds `:cuda` to `Parallel.to_executor(::Symbol)` (src/modules/Parallel/Parallel.jl:87-109).
+Must run at runtime (Julia does not allow overwriting a method of another
+module during precompilation); the other symbols keep their behaviour.
+"""
+function enable!()
+    @eval Parallel function to_executor(s::Symbol)
+        if s === :cuda
+            $(CudaExec)()
+        elseif s === :serial
+            SerialExec()
+        elseif s === :multithreaded || s === :threaded
+            Threads.nthreads() > 1 ? ThreadedExec() : SerialExec()
+        elseif s === :distributed
+            if nworkers() > 1
+                DistributedExec()
+            elseif Threads.nthreads() > 1
+                ThreadedExec()
+            else
+                SerialExec()
+            end
+        elseif s === :auto
+            auto()
+        else
+            @warn "Unknown executor symbol $s; falling back to :serial"
+            SerialExec()
+        end
+    end
+    nothing
+end
+
+end # module
