@@ -606,41 +606,87 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 }
 
 // ---------------------------------------------------------------------------
-// 4. Back-transformation U = H_0 ... H_{n-2} U, U holding Q on entry.
-// Reflector j is R[j+1.., j] (v0 = 1).  y = tau v^H U uses G = nt/n thread
-// groups per column (partials added in group order), the update runs column
-// by warp, rows by lane.
+// 4. Back-transformation U = H_0 ... H_{n-2} U (U holds Q on entry), applied
+// in blocks of 8 reflectors with the compact WY form (LAPACK zlarft, forward,
+// column-wise):  H_{j0} ... H_{j0+7} = I - V T V^H,  U_sub -= V (T (V^H U_sub)).
+// Reflector j is R[j+1.., j] with v0 = 1.  V (zero-padded, ld n), T and the
+// Gram matrix G = V^H V live in S.pbuf; one thread per column of U computes
+// V^H u, T (V^H u) and the update with 8 independent accumulators.
 // ---------------------------------------------------------------------------
 LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int ldr, EighVec& S, double2* U,
                                    int ldu) {
-  const int G = (T.nt >= n) ? T.nt / n : 1;
-  for (int j = n - 2; j >= 0; --j) {
-    const int m = n - j - 1;
-    const double2 tj = S.tau[j];
-    if (tj.x == 0.0 && tj.y == 0.0) continue;
-    for (int r = T.tid; r < m; r += T.nt) S.v[r] = R[(j + 1 + r) + (int64_t)j * ldr];
-    team_sync();
-    for (int t = T.tid; t < G * n; t += T.nt) {
-      const int c = t % n, g = t / n;
-      const double2* Uc = U + (j + 1) + (int64_t)c * ldu;
-      double sr = 0.0, si = 0.0;
-      for (int r = g; r < m; r += G) {
-        const double2 q = cmulc(S.v[r], Uc[r]);
-        sr += q.x; si += q.y;
+  constexpr int NB = 8;
+  double2* Vs = S.pbuf;                  // m x NB, leading dimension n
+  double2* Ts = S.pbuf + (int64_t)NB * n;  // NB x NB
+  double2* Gs = Ts + NB * NB;            // NB x NB
+  for (int j1 = n - 2; j1 >= 0; j1 -= NB) {
+    const int j0 = (j1 - NB + 1 > 0) ? j1 - NB + 1 : 0;
+    const int b = j1 - j0 + 1;
+    const int m = n - j0 - 1;  // rows j0+1 .. n-1 of U
+    for (int i = T.wid; i < NB; i += T.nw)
+      for (int r = T.lane; r < m; r += T.nl) {
+        double2 v = cmk(0.0, 0.0);
+        if (i < b && r >= i) v = R[(j0 + 1 + r) + (int64_t)(j0 + i) * ldr];
+        Vs[r + (int64_t)i * n] = v;
       }
-      S.pbuf[g * n + c] = cmk(sr, si);
+    team_sync();
+    for (int pidx = T.wid; pidx < NB * NB; pidx += T.nw) {
+      const int q = pidx % NB, i = pidx / NB;
+      if (!(q < i && i < b)) continue;
+      double sr = 0.0, si = 0.0;
+      for (int r = i + T.lane; r < m; r += T.nl) {
+        const double2 x = cmulc(Vs[r + (int64_t)q * n], Vs[r + (int64_t)i * n]);
+        sr += x.x; si += x.y;
+      }
+      sr = warp_sum(sr); si = warp_sum(si);
+      if (T.lane == 0) Gs[q + i * NB] = cmk(sr, si);
+    }
+    team_sync();
+    for (int l = T.tid; l < NB; l += T.nt) {  // row l of T: T[l,l] = tau_l, T[l,i] = -tau_i sum_{q=l}^{i-1} T[l,q] G[q,i]
+      double2 trow[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) trow[i] = cmk(0.0, 0.0);
+      if (l < b) trow[l] = S.tau[j0 + l];
+#pragma unroll
+      for (int i = 1; i < NB; ++i) {
+        if (i > l && i < b) {
+          double2 acc = cmk(0.0, 0.0);
+#pragma unroll
+          for (int q = 0; q < NB - 1; ++q)
+            if (q >= l && q < i) acc = cadd(acc, cmul(trow[q], Gs[q + i * NB]));
+          const double2 ti = S.tau[j0 + i];
+          trow[i] = cmul(cmk(-ti.x, -ti.y), acc);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < NB; ++i) Ts[l + i * NB] = trow[i];
     }
     team_sync();
     for (int c = T.tid; c < n; c += T.nt) {
-      double2 s = cmk(0.0, 0.0);
-      for (int g = 0; g < G; ++g) s = cadd(s, S.pbuf[g * n + c]);
-      S.w[c] = cmul(tj, s);
-    }
-    team_sync();
-    for (int c = T.wid; c < n; c += T.nw) {
-      double2* Uc = U + (j + 1) + (int64_t)c * ldu;
-      const double2 wc = S.w[c];
-      for (int r = T.lane; r < m; r += T.nl) Uc[r] = csub(Uc[r], cmul(S.v[r], wc));
+      double2* Uc = U + (j0 + 1) + (int64_t)c * ldu;
+      double2 w[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) w[i] = cmk(0.0, 0.0);
+      for (int r = 0; r < m; ++r) {
+        const double2 u = Uc[r];
+#pragma unroll
+        for (int i = 0; i < NB; ++i) w[i] = cadd(w[i], cmulc(Vs[r + (int64_t)i * n], u));
+      }
+      double2 wp[NB];
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        double2 acc = cmk(0.0, 0.0);
+#pragma unroll
+        for (int l = 0; l < NB; ++l)
+          if (l >= i) acc = cadd(acc, cmul(Ts[i + l * NB], w[l]));
+        wp[i] = acc;
+      }
+      for (int r = 0; r < m; ++r) {
+        double2 u = Uc[r];
+#pragma unroll
+        for (int i = 0; i < NB; ++i) u = csub(u, cmul(Vs[r + (int64_t)i * n], wp[i]));
+        Uc[r] = u;
+      }
     }
     team_sync();
   }

@@ -21,6 +21,7 @@ __host__ __device__ inline EighSmemLayout eigh_smem_layout(int n, int nR, int nt
   L.a_in_smem = a_in_smem;
   const int nw = nt / 32;
   L.pbuf_len = (nw * n > nt) ? nw * n : nt;
+  if (L.pbuf_len < 8 * n + 128) L.pbuf_len = 8 * n + 128;  // blocked back-transformation: V (n x 8), T, G
   size_t off = 0;
   L.offA = off;
   if (a_in_smem) off += lqm_align16((size_t)n * (n + 1) * 16);
@@ -85,8 +86,8 @@ __device__ __forceinline__ void carve_vectors(unsigned char* smem, const EighSme
   S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT) eigh_kernel(EighArgs a) {
+template <int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Team T = make_team();
   const int n = a.n;

@@ -25,7 +25,7 @@ extern "C" int lqm_emul_eigh(int n, int nR, int dim, const double* blocks, const
 
   const size_t nn = (size_t)n * n;
   const int lda = n + 1;  // padded leading dimension, as the shared-memory path
-  std::vector<double2> A((size_t)n * lda), cbuf(5 * n + 2 + nR + 8 * n + 256);
+  std::vector<double2> A((size_t)n * lda), cbuf(5 * n + 2 + nR + 8 * n + 256 + 128);
   std::vector<double> dbuf(13 * (size_t)n + 132), Q(nn), Qt(nn), Us(nn);
   std::vector<int> ibuf(10 * (size_t)n);
   EighVec S;
@@ -71,7 +71,7 @@ extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double*
   const size_t nn = (size_t)n * n;
   std::vector<double> dbuf(13 * (size_t)n + 132), Qt(nn), Us(nn);
   std::vector<int> ibuf(10 * (size_t)n);
-  std::vector<double2> cbuf(5 * n + 2 + 8 * n + 256);
+  std::vector<double2> cbuf(5 * n + 2 + 8 * n + 256 + 128);
   EighVec S;
   S.tau = cbuf.data(); S.v = S.tau + n; S.w = S.tau + 2 * n; S.vn = S.tau + 3 * n; S.pn = S.tau + 4 * n;
   S.bc = S.tau + 5 * n; S.pbuf = S.bc + 2;
