@@ -86,10 +86,14 @@ LQM_FN void zlarfg_scalars(double2 alpha, double xnorm2, double2* tau, double* b
   }
   const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xnorm2);
   const double b = (alpha.x >= 0.0) ? -nrm : nrm;
+  // 1/b and 1/(alpha - b) = conj(alpha - b)/|alpha - b|^2 are independent
+  // divisions (|alpha - b| >= |b| > 0 by the sign choice)
+  const double dr = alpha.x - b, di = alpha.y;
   const double ib = 1.0 / b;
+  const double idn = 1.0 / (dr * dr + di * di);
   *beta = b;
   *tau = cmk((b - alpha.x) * ib, -alpha.y * ib);
-  *scal = cdiv(cmk(1.0, 0.0), cmk(alpha.x - b, alpha.y));
+  *scal = cmk(dr * idn, -di * idn);
 }
 
 // One pass over the trailing block B = A[o:, o:] (order mb, o >= 1):
@@ -114,6 +118,7 @@ LQM_FN void trailing_pass(const Team& T, int mb, double2* A, int lda, int o, con
       wr[q] = cmk(0.0, 0.0);
       if (upd && rr[q] < mb) { vr[q] = v[rr[q] + 1]; wr[q] = w[rr[q] + 1]; }
     }
+#pragma unroll 2
     for (int c = T.wid; c < mb; c += T.nw) {
       const double2 xc = (c == 0) ? cmk(1.0, 0.0) : cmul(scal, xcol[c]);
       double2 cw = cmk(0.0, 0.0), cv = cmk(0.0, 0.0);
@@ -175,6 +180,10 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
   }
   double* redA = S.red;
   double* redB = S.red + 64;
+  double2* pb = S.pbuf;
+  double2* tau_out = S.tau;
+  double* d_out = S.d;
+  double* e_out = S.e;
   double2* vc = S.v;   // current reflector
   double2* vx = S.vn;  // next reflector
   double2* wc = S.w;   // w of the current reflector
@@ -186,21 +195,29 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
   double2 tnext, scal;
   double beta;
   zlarfg_scalars(A[1], s0, &tnext, &beta, &scal);
-  if (T.tid == 0) { S.tau[0] = tnext; S.e[0] = beta; S.d[0] = A[0].x; }
+  if (T.tid == 0) { tau_out[0] = tnext; e_out[0] = beta; d_out[0] = A[0].x; }
   // step j = -1 .. n-3: pass over A[j+2:, j+2:] (update j if j >= 0) with reflector j+1
   for (int j = -1; j <= n - 3; ++j) {
     const int o = j + 2;
     const int mb = n - o;
     LQM_HTICK(2);
-    trailing_pass(T, mb, A, lda, o, vc, wc, j >= 0, scal, vx, S.pbuf, n);
+    trailing_pass(T, mb, A, lda, o, vc, wc, j >= 0, scal, vx, pb, n);
     team_sync();
     LQM_HTICK(0);
     store_reflector(T, mb, A, lda, o, scal, vx);
     // p = tau_{j+1} * row sums; alpha = -1/2 tau (p^H x)
     double pr = 0.0, pi = 0.0;
     for (int r = T.tid; r < mb; r += T.nt) {
-      double2 sacc = cmk(0.0, 0.0);
-      for (int wv = 0; wv < T.nw; ++wv) sacc = cadd(sacc, S.pbuf[wv * n + r]);
+      double2 s0 = cmk(0.0, 0.0), s1 = s0, s2 = s0, s3 = s0;
+      int wv = 0;
+      for (; wv + 4 <= T.nw; wv += 4) {
+        s0 = cadd(s0, pb[wv * n + r]);
+        s1 = cadd(s1, pb[(wv + 1) * n + r]);
+        s2 = cadd(s2, pb[(wv + 2) * n + r]);
+        s3 = cadd(s3, pb[(wv + 3) * n + r]);
+      }
+      for (; wv < T.nw; ++wv) s0 = cadd(s0, pb[wv * n + r]);
+      const double2 sacc = cadd(cadd(s0, s1), cadd(s2, s3));
       const double2 pv = cmul(tnext, sacc);
       p[r] = pv;
       const double2 q = cmulc(pv, vx[r]);  // vx[r] was stored by this same thread above
@@ -229,9 +246,9 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
     double2* t = vc; vc = vx; vx = t;
     if (o <= n - 2) {  // reflector j+2 = o exists
       zlarfg_scalars(col[1], sn, &tnext, &beta, &scal);
-      if (T.tid == 0) { S.tau[o] = tnext; S.e[o] = beta; S.d[o] = col[0].x; }
+      if (T.tid == 0) { tau_out[o] = tnext; e_out[o] = beta; d_out[o] = col[0].x; }
     } else {
-      if (T.tid == 0) S.d[n - 1] = col[0].x;
+      if (T.tid == 0) d_out[n - 1] = col[0].x;
     }
   }
   team_sync();
@@ -345,47 +362,46 @@ LQM_FN void secular_root_group(bool active, int gw, int g, int k, const double* 
   *tau_out = tau;
 }
 
-// dlaed2-style deflation for one merge node (single thread).
-LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta) {
+// dlaed2-style deflation for one merge node (single thread), on the values in
+// merged order: zs/ds[lo+p] = z/D of the p-th smallest (gathered in parallel
+// before the scan, so the scan's loads do not wait on each other).
+LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta, double* zs, double* ds) {
   const int lo = P.lo[node], hi = P.hi[node];
   const double rho = 2.0 * eabs_beta;
   double zmax = 0.0, dmax = 0.0;
-  for (int i = lo; i < hi; ++i) { zmax = fmax(zmax, fabs(S.z[i])); dmax = fmax(dmax, fabs(S.D[i])); }
+  for (int p = lo; p < hi; ++p) { zmax = fmax(zmax, fabs(zs[p])); dmax = fmax(dmax, fabs(ds[p])); }
   const double tol = 8.0 * LQM_DEPS * fmax(dmax, zmax);
   int k = 0, nd = 0, nr = 0;
   if (rho * zmax <= tol) {
-    for (int p = lo; p < hi; ++p) { int j = S.perm[p]; S.dval[lo + nd] = S.D[j]; S.dcol[lo + nd] = j; ++nd; }
+    for (int p = lo; p < hi; ++p) { S.dval[lo + nd] = ds[p]; S.dcol[lo + nd] = S.perm[p]; ++nd; }
   } else {
-    int pj = -1;
+    int jp = -1;
+    double zp = 0.0, dp = 0.0;
     for (int p = lo; p < hi; ++p) {
       const int j = S.perm[p];
-      if (rho * fabs(S.z[j]) <= tol) { S.dval[lo + nd] = S.D[j]; S.dcol[lo + nd] = j; ++nd; continue; }
-      if (pj < 0) { pj = j; continue; }
-      const double zp = S.z[pj], zj = S.z[j];
-      const double t = S.D[j] - S.D[pj];
+      const double zj = zs[p], dj = ds[p];
+      if (rho * fabs(zj) <= tol) { S.dval[lo + nd] = dj; S.dcol[lo + nd] = j; ++nd; continue; }
+      if (jp < 0) { jp = j; zp = zj; dp = dj; continue; }
+      const double t = dj - dp;
       // |t c s| <= tol with c = zj/tau, s = -zp/tau, tau^2 = zj^2 + zp^2 (no division)
       if (fabs(t * zj * zp) <= tol * (zj * zj + zp * zp)) {
         const double tau = hypot(zj, zp);
         const double cv = zj / tau, sv = -zp / tau;
-        S.z[j] = tau; S.z[pj] = 0.0;
-        S.ri[lo + nr] = pj; S.rj[lo + nr] = j; S.rc[lo + nr] = cv; S.rs[lo + nr] = sv; ++nr;
-        const double t2 = S.D[pj] * cv * cv + S.D[j] * sv * sv;
-        S.D[j] = S.D[pj] * sv * sv + S.D[j] * cv * cv;
-        S.D[pj] = t2;
-        S.dval[lo + nd] = S.D[pj]; S.dcol[lo + nd] = pj; ++nd;
-        pj = j;
+        S.ri[lo + nr] = jp; S.rj[lo + nr] = j; S.rc[lo + nr] = cv; S.rs[lo + nr] = sv; ++nr;
+        const double t2 = dp * cv * cv + dj * sv * sv;
+        const double dnew = dp * sv * sv + dj * cv * cv;
+        S.dval[lo + nd] = t2; S.dcol[lo + nd] = jp; ++nd;
+        jp = j; zp = tau; dp = dnew;
       } else {
-        S.dl[lo + k] = S.D[pj]; S.zl[lo + k] = S.z[pj]; S.colnd[lo + k] = pj; ++k;
-        pj = j;
+        S.dl[lo + k] = dp; S.zl[lo + k] = zp; S.colnd[lo + k] = jp; ++k;
+        jp = j; zp = zj; dp = dj;
       }
     }
-    if (pj >= 0) { S.dl[lo + k] = S.D[pj]; S.zl[lo + k] = S.z[pj]; S.colnd[lo + k] = pj; ++k; }
+    if (jp >= 0) { S.dl[lo + k] = dp; S.zl[lo + k] = zp; S.colnd[lo + k] = jp; ++k; }
   }
   S.nk[node] = k; S.nrot[node] = nr; S.ndef[node] = nd; S.nrho[node] = rho;
 }
 
-// In: S.d (diag, n), S.e (offdiag, n-1).  Out: S.D ascending eigenvalues, Q (n x n, ld n).
-// Qt, Us: n x n scratch.
 // Optional per-step cycle accounting (device only): sub[0..7] += cycles of
 // merge steps A (z, sort), B (deflation), C (secular), D (zhat), E-G (vectors,
 // rotations, values), ranks, H (update), I (copy back).
@@ -401,7 +417,8 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 #endif
 
 LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
-                              double* Us, unsigned long long* sub = nullptr) {
+                              unsigned long long* sub = nullptr) {
+  double* ubuf = (double*)S.pbuf;  // per-warp secular eigenvector (n doubles each)
 #if defined(__CUDA_ARCH__)
   long long tsub = clock64();
   if (T.tid != 0) sub = nullptr;
@@ -458,8 +475,16 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     }
     team_sync();
     LQM_SUBTICK(0);
-    // B: deflation, one thread per node
-    for (int nd = h0 + T.tid; nd < h1; nd += T.nt) deflate_node(nd, P, S, fabs(S.e[P.mid[nd] - 1]));
+    // B: gather z and D in merged order, then deflation, one thread per node
+    for (int i = T.tid; i < n; i += T.nt) {
+      if (own[i] < 0) continue;
+      const int j = S.perm[i];
+      S.zhat[i] = S.z[j];
+      S.vals[i] = S.D[j];
+    }
+    team_sync();
+    for (int nd = h0 + T.tid; nd < h1; nd += T.nt)
+      deflate_node(nd, P, S, fabs(S.e[P.mid[nd] - 1]), S.zhat, S.vals);
     team_sync();
     LQM_SUBTICK(1);
     // C: secular roots
@@ -507,23 +532,6 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     }
     team_sync();
     LQM_SUBTICK(3);
-    // E: secular eigenvectors, column q of Us block
-    for (int i = T.tid; i < n; i += T.nt) {
-      const int nd = own[i];
-      if (nd < 0) continue;
-      const int lo = P.lo[nd], q = i - lo, k = S.nk[nd];
-      if (q >= k) continue;
-      const double* dl = S.dl + lo;
-      const double lorg = dl[S.org[lo + q]], tq = S.troot[lo + q];
-      double nrm = 0.0;
-      for (int p = 0; p < k; ++p) {
-        const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
-        Us[(lo + p) + (int64_t)(lo + q) * n] = u;
-        nrm += u * u;
-      }
-      const double sc = 1.0 / sqrt(nrm);
-      for (int p = 0; p < k; ++p) Us[(lo + p) + (int64_t)(lo + q) * n] *= sc;
-    }
     // F: deflation rotations on the rows of Q
     for (int r = T.tid; r < n; r += T.nt) {
       const int nd = own[r];
@@ -557,21 +565,34 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     }
     team_sync();
     LQM_SUBTICK(5);
-    // H: eigenvector update into Qt (column c by warp, rows of its node by lane)
+    // H: eigenvector update into Qt.  Column c by warp: the warp first forms
+    // the normalised secular eigenvector u_p = zhat_p / (d_p - lambda_it) in its
+    // shared buffer, then rows of the node by lane (3 independent chains).
     for (int c = T.wid; c < n; c += T.nw) {
       const int nd = own[c];
       if (nd < 0) continue;
       const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];
       double* dst = Qt + (int64_t)S.newpos[c] * n;
       if (it < k) {
-        const double* uc = Us + lo + (int64_t)(lo + it) * n;
+        double* ub = ubuf + (int64_t)T.wid * n;
+        const double* dl = S.dl + lo;
+        const double lorg = dl[S.org[lo + it]], tq = S.troot[lo + it];
+        double ss = 0.0;
+        for (int p = T.lane; p < k; p += T.nl) {
+          const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
+          ub[p] = u;
+          ss += u * u;
+        }
+        const double sc = 1.0 / sqrt(warp_sum_bcast(ss));
+        for (int p = T.lane; p < k; p += T.nl) ub[p] *= sc;
+        team_syncwarp();
         for (int r0 = lo + T.lane; r0 < hi; r0 += 3 * T.nl) {
           const int r1 = r0 + T.nl, r2 = r0 + 2 * T.nl;
           const bool h1 = r1 < hi, h2 = r2 < hi;
           double a0 = 0.0, a1 = 0.0, a2 = 0.0;
           for (int p = 0; p < k; ++p) {
             const double* qc = Q + (int64_t)S.colnd[lo + p] * n;
-            const double u = uc[p];
+            const double u = ub[p];
             a0 += qc[r0] * u;
             if (h1) a1 += qc[r1] * u;
             if (h2) a2 += qc[r2] * u;
@@ -580,6 +601,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
           if (h1) dst[r1] = a1;
           if (h2) dst[r2] = a2;
         }
+        team_syncwarp();
       } else {
         const double* src = Q + (int64_t)S.dcol[lo + it - k] * n;
         for (int r = lo + T.lane; r < hi; r += T.nl) dst[r] = src[r];

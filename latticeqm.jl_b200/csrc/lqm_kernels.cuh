@@ -38,8 +38,8 @@ __host__ __device__ inline EighSmemLayout eigh_smem_layout(int n, int nR, int nt
 // doubles of global scratch per CTA
 __host__ __device__ inline int64_t eigh_slot_doubles(int n, int a_in_smem, bool need_uwork) {
   const int64_t nn = (int64_t)n * n;
-  if (a_in_smem) return 4 * nn;                  // R (2nn) | Qs | Us
-  return 5 * nn + (need_uwork ? 2 * nn : 0);     // A (2nn) | Q | Qt | Us | U work
+  if (a_in_smem) return 3 * nn;                  // R (2nn) | Qs
+  return 4 * nn + (need_uwork ? 2 * nn : 0);     // A (2nn) | Q | Qt | U work
 }
 
 struct EighArgs {
@@ -107,7 +107,6 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
   double* Q = in_smem ? (double*)(smem + L.offA) : slot + 2 * nn;
   double* Qt = Q + nn;
   double* Qs = slot + 2 * nn;                         // smem path: saved Q
-  double* Us = in_smem ? slot + 3 * nn : slot + 4 * nn;
   const bool need_vec = (a.U != nullptr) || (a.rhok != nullptr);
 
   const bool prof = a.phase_cycles != nullptr;
@@ -135,7 +134,7 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
       team_sync();
     }
     LQM_TICK(PH_HETRD);
-    dc_solve(T, n, a.plan, S, Q, Qt, Us, prof ? dsub : nullptr);
+    dc_solve(T, n, a.plan, S, Q, Qt, prof ? dsub : nullptr);
     for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
     LQM_TICK(PH_DC);
     if (need_vec) {
@@ -150,7 +149,7 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
         for (int c = T.wid; c < n; c += T.nw)
           for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Qs[r + (int64_t)c * n], 0.0);
       } else {
-        U = a.U ? a.U + k * nn : (double2*)(slot + 5 * nn);
+        U = a.U ? a.U + k * nn : (double2*)(slot + 4 * nn);
         ldu = n;
         for (int c = T.wid; c < n; c += T.nw)
           for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Q[r + (int64_t)c * n], 0.0);

@@ -40,6 +40,7 @@ LQM_FN Team make_team() {
   return t;
 }
 LQM_FN void team_sync() { __syncthreads(); }
+LQM_FN void team_syncwarp() { __syncwarp(); }
 LQM_FN double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -65,6 +66,7 @@ LQM_FN double group_sum_bcast(double v, int width) {
 #else
 LQM_FN Team make_host_team() { Team t = {0, 1, 0, 1, 0, 1}; return t; }
 LQM_FN void team_sync() {}
+LQM_FN void team_syncwarp() {}
 LQM_FN double warp_sum(double v) { return v; }
 LQM_FN double warp_max(double v) { return v; }
 LQM_FN double warp_sum_bcast(double v) { return v; }
@@ -112,10 +114,19 @@ LQM_FN void team_sum2_1b(const Team& T, double& a, double& b, double* red) {
   b = warp_sum(b);
   if (T.lane == 0) { red[2 * T.wid] = a; red[2 * T.wid + 1] = b; }
   __syncthreads();
-  double sa = 0.0, sb = 0.0;
-  for (int w = 0; w < T.nw; ++w) { sa += red[2 * w]; sb += red[2 * w + 1]; }
-  a = sa;
-  b = sb;
+  // four interleaved partial sums (in warp order within each) keep the
+  // dependent-add chain short; the result is still fixed for a given team size
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+  int w = 0;
+  for (; w + 4 <= T.nw; w += 4) {
+    a0 += red[2 * w]; b0 += red[2 * w + 1];
+    a1 += red[2 * w + 2]; b1 += red[2 * w + 3];
+    a2 += red[2 * w + 4]; b2 += red[2 * w + 5];
+    a3 += red[2 * w + 6]; b3 += red[2 * w + 7];
+  }
+  for (; w < T.nw; ++w) { a0 += red[2 * w]; b0 += red[2 * w + 1]; }
+  a = (a0 + a1) + (a2 + a3);
+  b = (b0 + b1) + (b2 + b3);
 #else
   (void)T; (void)red; (void)a; (void)b;
 #endif

@@ -26,7 +26,7 @@ extern "C" int lqm_emul_eigh(int n, int nR, int dim, const double* blocks, const
   const size_t nn = (size_t)n * n;
   const int lda = n + 1;  // padded leading dimension, as the shared-memory path
   std::vector<double2> A((size_t)n * lda), cbuf(5 * n + 2 + nR + 8 * n + 256 + 128);
-  std::vector<double> dbuf(13 * (size_t)n + 132), Q(nn), Qt(nn), Us(nn);
+  std::vector<double> dbuf(13 * (size_t)n + 132), Q(nn), Qt(nn);
   std::vector<int> ibuf(10 * (size_t)n);
   EighVec S;
   S.tau = cbuf.data(); S.v = S.tau + n; S.w = S.tau + 2 * n; S.vn = S.tau + 3 * n; S.pn = S.tau + 4 * n;
@@ -45,7 +45,7 @@ extern "C" int lqm_emul_eigh(int n, int nR, int dim, const double* blocks, const
   hetrd_lower(T, n, A.data(), lda, S);
   if (tri_d) std::memcpy(tri_d, S.d, sizeof(double) * n);
   if (tri_e && n > 1) std::memcpy(tri_e, S.e, sizeof(double) * (n - 1));
-  dc_solve(T, n, P, S, Q.data(), Qt.data(), Us.data());
+  dc_solve(T, n, P, S, Q.data(), Qt.data());
   std::memcpy(evals, S.D, sizeof(double) * n);
   if (want_vectors) {
     double2* Uc = (double2*)U;
@@ -69,7 +69,7 @@ extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double*
   P.hi = PH.buf.data() + PH.off_hi;
   P.owner = PH.buf.data() + PH.off_own;
   const size_t nn = (size_t)n * n;
-  std::vector<double> dbuf(13 * (size_t)n + 132), Qt(nn), Us(nn);
+  std::vector<double> dbuf(13 * (size_t)n + 132), Qt(nn);
   std::vector<int> ibuf(10 * (size_t)n);
   std::vector<double2> cbuf(5 * n + 2 + 8 * n + 256 + 128);
   EighVec S;
@@ -84,7 +84,7 @@ extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double*
   S.ri = ib + 5 * n; S.rj = ib + 6 * n; S.nk = ib + 7 * n; S.nrot = ib + 8 * n; S.ndef = ib + 9 * n;
   std::memcpy(S.d, d, sizeof(double) * n);
   if (n > 1) std::memcpy(S.e, e, sizeof(double) * (n - 1));
-  dc_solve(T, n, P, S, Z, Qt.data(), Us.data());
+  dc_solve(T, n, P, S, Z, Qt.data());
   std::memcpy(evals, S.D, sizeof(double) * n);
   return 0;
 }
