@@ -389,28 +389,38 @@ def main():
         e2e_el = float(t[0])
     e2e_val = total_k / e2e_el
 
-    # ---- roofline of the dominant kernel (per-k eigensolver) ----
-    eig_flops = args.steps * nk * sum(eigh_flops_per_k(s["n"], s["nR"]) for s in state)
-    achieved = eig_flops / (eigh_ms / 1e3) / 1e12 if eigh_ms > 0 else None
+    # ---- roofline of the dominant kernel: the per-k eigensolver on the n=96 model ----
     detail = {}
-    for s in state:
-        ms = per_model_ms.get(s["n"], 0.0)
+    for s_ in state:
+        ms = per_model_ms.get(s_["n"], 0.0)
         if ms > 0:
-            detail[f"n{s['n']}"] = {"eigh_ms_per_step": ms / args.steps,
-                                    "eigh_tflops": args.steps * nk * eigh_flops_per_k(s["n"], s["nR"]) / (ms / 1e3)
-                                    / 1e12}
+            detail[f"n{s_['n']}"] = {"eigh_ms_per_step": ms / args.steps,
+                                     "eigh_tflops": args.steps * nk * eigh_flops_per_k(s_["n"], s_["nR"])
+                                     / (ms / 1e3) / 1e12}
+    dom = max(state, key=lambda s_: s_["n"])
+    dom_ms = per_model_ms.get(dom["n"], 0.0)
+    achieved = (args.steps * nk * eigh_flops_per_k(dom["n"], dom["nR"]) / (dom_ms / 1e3) / 1e12
+                if dom_ms > 0 else None)
+    # k-points per launch of the dominant model (the library's rho_k batch: 4 GB / (16 n^2) k)
+    kb = max(1, min(nk, int(4.0e9 // (16.0 * dom["n"] ** 2))))
+    k_per_launch = nk / math.ceil(nk / kb)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "eigh_traffic.json")
     if os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile)).get("bytes_per_launch")
+            traffic = json.load(open(tfile))["bytes_per_k"] * k_per_launch
         except Exception:
             traffic = None
     roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
-            "kernel": "eigh_kernel (Bloch sum + Householder + divide&conquer + back-transform, one CTA per k)",
+            "kernel": f"eigh_kernel on the n={dom['n']} model (Bloch sum + Householder + divide&conquer + "
+                      f"back-transform + fused rho_k, one CTA per k)",
+            "algorithmic_flops_per_k": eigh_flops_per_k(dom["n"], dom["nR"]),
+            "k_per_launch": k_per_launch,
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
-            "eigh_launches": eigh_launches, "eigh_ms": eigh_ms, "per_model": detail}
+            "traffic_source": "ncu dram bytes per k-point of the 2048-k capture (profiles/eigh_kernel_n96_2048k.md) "
+                              "x k-points per launch",
+            "eigh_launches_all_models": eigh_launches, "eigh_ms_all_models": eigh_ms, "per_model": detail}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
