@@ -58,6 +58,7 @@ struct lqm_ctx {
   double eigh_ms = 0.0;
   int64_t eigh_launches = 0, launches = 0;
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
+  bool scf_graph_used = false;            // the last SCF replayed a captured iteration
 };
 
 struct lqm_hops {
@@ -298,11 +299,17 @@ void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   }
 }
 
-double chempot_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, double filling,
-                   double T) {
+// Chemical potential entirely on the device: mu_out (device double) receives
+// mu and err_out (device double, cleared here) counts failed searches.  No host
+// synchronisation, so the sequence can be captured in a CUDA graph.
+// WS_MISC layout (64 doubles): [0,1] min/max, [4..13] MuState, [16] mu,
+// [17,18] order statistics, [19] error count, [40..44] SCF scalars.
+void chempot_enqueue(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, double filling,
+                     double T, double* mu_out, double* err_out) {
   const int64_t nv = n * nk;
   double* mm = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double));
   MuState* st = (MuState*)(mm + 4);
+  ck(cudaMemsetAsync(err_out, 0, sizeof(double), ctx->stream), "memset");
   minmax_kernel<<<1, 1024, 0, ctx->stream>>>(d_bands, nv, mm);
   ctx->launches += 1;
   const int64_t nbk = std::max<int64_t>(1, std::min<int64_t>((nv + 4095) / 4096, (int64_t)ctx->num_sms * 4));
@@ -315,39 +322,45 @@ double chempot_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, c
       filling_partial_kernel<<<(unsigned)nbk, 256, 0, ctx->stream>>>(d_bands, (int)n, nv, d_w, st, T, chunk, part);
       mu_update_kernel<<<1, 32, 0, ctx->stream>>>(part, (int)nbk, st, filling, norm);
     }
-    ctx->launches += 1 + 2 * 140;
+    mu_store_kernel<<<1, 32, 0, ctx->stream>>>(st, mu_out, err_out);
+    ctx->launches += 2 + 2 * 140;
     ck(cudaGetLastError(), "chemical potential launch");
-    MuState hs;
-    ck(cudaMemcpyAsync(&hs, st, sizeof(MuState), cudaMemcpyDeviceToHost, ctx->stream), "mu readback");
-    wait_stream(ctx);
-    if (hs.err) fail(LQM_EDEVICE, "filling - target does not change sign on [min ε, max ε]");
-    if (!hs.done) fail(LQM_EDEVICE, "chemical potential bisection did not terminate");
-    return hs.result;
+    return;
   }
   // T == 0: midpoint of order statistics i, i+1 (1-based), chemicalpotential.jl:9-23
-  double hmm[2];
-  ck(cudaMemcpyAsync(hmm, mm, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "minmax readback");
-  wait_stream(ctx);
-  if (filling >= 1.0) return hmm[1];
-  if (filling <= 0.0) return hmm[0] - 1.0;
+  if (filling >= 1.0 || filling <= 0.0) {
+    mu_special_kernel<<<1, 32, 0, ctx->stream>>>(mm, mu_out, filling >= 1.0);
+    ctx->launches += 1;
+    ck(cudaGetLastError(), "chemical potential launch");
+    return;
+  }
   const long long i1 = 1 + (long long)std::floor(filling * (double)(nv - 1));
   long long* part = (long long*)ws_get(ctx, WS_MU, (size_t)nbk * sizeof(long long));
-  double res[2];
   for (int s = 0; s < 2; ++s) {
     os_init_kernel<<<1, 1, 0, ctx->stream>>>(st, mm, i1 + s);
     for (int it = 0; it < 140; ++it) {
       count_partial_kernel<<<(unsigned)nbk, 256, 0, ctx->stream>>>(d_bands, nv, st, chunk, part);
       os_update_kernel<<<1, 32, 0, ctx->stream>>>(part, (int)nbk, st);
     }
-    ctx->launches += 1 + 2 * 140;
-    ck(cudaGetLastError(), "order statistic launch");
-    MuState hs;
-    ck(cudaMemcpyAsync(&hs, st, sizeof(MuState), cudaMemcpyDeviceToHost, ctx->stream), "os readback");
-    wait_stream(ctx);
-    if (!hs.done) fail(LQM_EDEVICE, "order-statistic bisection did not terminate");
-    res[s] = hs.result;
+    mu_store_kernel<<<1, 32, 0, ctx->stream>>>(st, mm + 17 + s, err_out);
+    ctx->launches += 2 + 2 * 140;
   }
-  return (res[0] + res[1]) / 2;
+  mu_avg_kernel<<<1, 32, 0, ctx->stream>>>(mm + 17, mm + 18, mu_out);
+  ctx->launches += 1;
+  ck(cudaGetLastError(), "order statistic launch");
+}
+
+double chempot_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, double filling,
+                   double T) {
+  double* mm = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double));
+  chempot_enqueue(ctx, n, nk, d_bands, d_w, filling, T, mm + 16, mm + 19);
+  double h[4];
+  ck(cudaMemcpyAsync(h, mm + 16, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "mu readback");
+  wait_stream(ctx);
+  if (h[3] != 0.0)
+    fail(LQM_EDEVICE, T > 0 ? "filling - target does not change sign on [min eps, max eps]"
+                            : "order-statistic bisection did not terminate");
+  return h[0];
 }
 
 void dos_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, int64_t nw,

@@ -213,10 +213,12 @@ __global__ void __launch_bounds__(256) bloch_kernel(int n, int nR, int dim, cons
 
 // rho_k = U diag(f) U^H per k from eigenvectors in HBM; eband_k = w_k sum_j f_j eps_j.
 __global__ void __launch_bounds__(256) rhok_kernel(int n, int64_t nk, const double2* __restrict__ U,
-                                                   const double* __restrict__ bands, double mu, double T,
+                                                   const double* __restrict__ bands, double mu_val,
+                                                   const double* mu_ptr, double T,
                                                    const double* __restrict__ w, double2* __restrict__ rhok,
                                                    double* __restrict__ eband_k) {
   extern __shared__ __align__(16) unsigned char smem[];
+  const double mu = mu_ptr ? *mu_ptr : mu_val;  // device-resident mu (SCF) or a host value
   double* f = (double*)smem;
   double* red = f + n;
   const Team Tm = make_team();
@@ -433,6 +435,24 @@ __global__ void mu_update_kernel(const double* __restrict__ partial, int nb, MuS
     return;
   }
   st->x = m;
+}
+
+// mu result of a finished bisection into out; err accumulates 1 (no sign
+// change) or 2 (not terminated).
+__global__ void mu_store_kernel(const MuState* st, double* out, double* err) {
+  if (threadIdx.x != 0) return;
+  *out = st->result;
+  if (st->err) *err += 1.0;
+  else if (!st->done) *err += 2.0;
+}
+
+// filling >= 1: mu = max eps; filling <= 0: mu = min eps - 1 (chemicalpotential.jl:12-17)
+__global__ void mu_special_kernel(const double* mm, double* out, int upper) {
+  if (threadIdx.x == 0) *out = upper ? mm[1] : mm[0] - 1.0;
+}
+
+__global__ void mu_avg_kernel(const double* a, const double* b, double* out) {
+  if (threadIdx.x == 0) *out = (*a + *b) / 2;
 }
 
 // Order statistic (T = 0): smallest float x in [min,max] with #{v <= x} >= target.
