@@ -416,9 +416,17 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 #define LQM_SUBTICK(i_)
 #endif
 
+// vec == false: eigenvalues only.  The merges then need just the first and
+// last rows of each node's eigenvector matrix (they form z), so Q (>= 4n
+// doubles) holds QF/QL (those rows, indexed by column) and FT/LT (the rows of
+// the node being merged), and every merge is O(size^2).
 LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
-                              unsigned long long* sub = nullptr) {
+                              unsigned long long* sub = nullptr, bool vec = true) {
   double* ubuf = (double*)S.pbuf;  // per-warp secular eigenvector (n doubles each)
+  double* QF = Q;
+  double* QL = Q + n;
+  double* FT = Q + 2 * n;
+  double* LT = Q + 3 * n;
 #if defined(__CUDA_ARCH__)
   long long tsub = clock64();
   if (T.tid != 0) sub = nullptr;
@@ -445,8 +453,12 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
   }
   team_sync();
   for (int i = T.tid; i < n - 1; i += T.nt) S.e[i] *= inv;
-  for (int c = T.wid; c < n; c += T.nw)
-    for (int r = T.lane; r < n; r += T.nl) Q[r + (int64_t)c * n] = (r == c) ? 1.0 : 0.0;
+  if (vec) {
+    for (int c = T.wid; c < n; c += T.nw)
+      for (int r = T.lane; r < n; r += T.nl) Q[r + (int64_t)c * n] = (r == c) ? 1.0 : 0.0;
+  } else {
+    for (int i = T.tid; i < n; i += T.nt) { QF[i] = 1.0; QL[i] = 1.0; }
+  }
   team_sync();
   for (int h = 0; h < P.nheights; ++h) {
     const int h0 = P.hstart[h], h1 = P.hstart[h + 1];
@@ -457,7 +469,14 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       if (nd < 0) continue;
       const int lo = P.lo[nd], m = P.mid[nd], hi = P.hi[nd];
       const double beta = S.e[m - 1];
-      double zi = (i < m) ? Q[(m - 1) + (int64_t)i * n] : ((beta < 0.0) ? -1.0 : 1.0) * Q[m + (int64_t)i * n];
+      double zi;
+      if (vec) {
+        zi = (i < m) ? Q[(m - 1) + (int64_t)i * n] : ((beta < 0.0) ? -1.0 : 1.0) * Q[m + (int64_t)i * n];
+      } else {
+        zi = (i < m) ? QL[i] : ((beta < 0.0) ? -1.0 : 1.0) * QF[i];
+        FT[i] = (i < m) ? QF[i] : 0.0;
+        LT[i] = (i < m) ? 0.0 : QL[i];
+      }
       S.z[i] = zi * 0.70710678118654752440;
       const double di = S.D[i];
       int cnt = 0;
@@ -532,8 +551,22 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     }
     team_sync();
     LQM_SUBTICK(3);
-    // F: deflation rotations on the rows of Q
-    for (int r = T.tid; r < n; r += T.nt) {
+    // F: deflation rotations on the rows of Q (or on the two boundary rows)
+    if (!vec) {
+      for (int t2 = T.tid; t2 < 2 * (h1 - h0); t2 += T.nt) {
+        const int nd = h0 + t2 / 2;
+        double* row = (t2 & 1) ? LT : FT;
+        const int lo = P.lo[nd], nr = S.nrot[nd];
+        for (int t = 0; t < nr; ++t) {
+          const int a = S.ri[lo + t], b = S.rj[lo + t];
+          const double c = S.rc[lo + t], s = S.rs[lo + t];
+          const double x = row[a], y = row[b];
+          row[a] = c * x + s * y;
+          row[b] = c * y - s * x;
+        }
+      }
+    }
+    for (int r = T.tid; r < n && vec; r += T.nt) {
       const int nd = own[r];
       if (nd < 0) continue;
       const int lo = P.lo[nd], nr = S.nrot[nd];
@@ -568,7 +601,40 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     // H: eigenvector update into Qt.  Column c by warp: the warp first forms
     // the normalised secular eigenvector u_p = zhat_p / (d_p - lambda_it) in its
     // shared buffer, then rows of the node by lane (3 independent chains).
-    for (int c = T.wid; c < n; c += T.nw) {
+    // Eigenvalues only: the two boundary rows, lanes splitting p.
+    if (!vec) {
+      for (int c = T.wid; c < n; c += T.nw) {
+        const int nd = own[c];
+        if (nd < 0) continue;
+        const int lo = P.lo[nd], it = c - lo, k = S.nk[nd];
+        const int dstc = S.newpos[c];
+        if (it < k) {
+          const double* dl = S.dl + lo;
+          const double lorg = dl[S.org[lo + it]], tq = S.troot[lo + it];
+          double ss = 0.0, f = 0.0, l = 0.0;
+          for (int p = T.lane; p < k; p += T.nl) {
+            const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
+            const int col = S.colnd[lo + p];
+            ss += u * u;
+            f += FT[col] * u;
+            l += LT[col] * u;
+          }
+          ss = warp_sum_bcast(ss);
+          f = warp_sum_bcast(f);
+          l = warp_sum_bcast(l);
+          if (T.lane == 0) {
+            const double sc = 1.0 / sqrt(ss);
+            QF[dstc] = f * sc;
+            QL[dstc] = l * sc;
+          }
+        } else if (T.lane == 0) {
+          const int src = S.dcol[lo + it - k];
+          QF[dstc] = FT[src];
+          QL[dstc] = LT[src];
+        }
+      }
+    }
+    for (int c = T.wid; c < n && vec; c += T.nw) {
       const int nd = own[c];
       if (nd < 0) continue;
       const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];
@@ -610,7 +676,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     team_sync();
     LQM_SUBTICK(6);
     // I: write back
-    for (int c = T.wid; c < n; c += T.nw) {
+    for (int c = T.wid; c < n && vec; c += T.nw) {
       const int nd = own[c];
       if (nd < 0) continue;
       const int lo = P.lo[nd], hi = P.hi[nd];

@@ -128,13 +128,13 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
     bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, lda);
     LQM_TICK(PH_BLOCH);
     hetrd_lower(T, n, A, lda, S, prof ? hsub : nullptr);
-    if (in_smem) {
+    if (in_smem && need_vec) {
       for (int c = T.wid; c < n - 1; c += T.nw)
         for (int r = c + 1 + T.lane; r < n; r += T.nl) R[r + (int64_t)c * n] = A[r + (int64_t)c * lda];
       team_sync();
     }
     LQM_TICK(PH_HETRD);
-    dc_solve(T, n, a.plan, S, Q, Qt, prof ? dsub : nullptr);
+    dc_solve(T, n, a.plan, S, Q, Qt, prof ? dsub : nullptr, need_vec);
     for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
     LQM_TICK(PH_DC);
     if (need_vec) {

@@ -57,7 +57,7 @@ extern "C" int lqm_emul_eigh(int n, int nR, int dim, const double* blocks, const
 }
 
 // D&C alone on a given symmetric tridiagonal (d, e): eigenvalues and Z.
-extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double* evals, double* Z) {
+extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double* evals, double* Z, int vec) {
   const Team T = make_host_team();
   const lqm::DCPlanHost PH = lqm::make_dc_plan_host(n);
   DCPlan P;
@@ -84,7 +84,8 @@ extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double*
   S.ri = ib + 5 * n; S.rj = ib + 6 * n; S.nk = ib + 7 * n; S.nrot = ib + 8 * n; S.ndef = ib + 9 * n;
   std::memcpy(S.d, d, sizeof(double) * n);
   if (n > 1) std::memcpy(S.e, e, sizeof(double) * (n - 1));
-  dc_solve(T, n, P, S, Z, Qt.data());
+  std::vector<double> rows(4 * (size_t)n + 4);
+  dc_solve(T, n, P, S, vec ? Z : rows.data(), Qt.data(), nullptr, vec != 0);
   std::memcpy(evals, S.D, sizeof(double) * n);
   return 0;
 }

@@ -81,10 +81,14 @@ def test_emulated_tridiagonal_dc(emul, n):
         ev = np.zeros(n)
         Z = np.zeros((n, n), order="F")
         emul.lqm_emul_tridiag(n, d.ctypes.data_as(P), e.ctypes.data_as(P), ev.ctypes.data_as(P),
-                              Z.ctypes.data_as(P))
+                              Z.ctypes.data_as(P), 1)
+        ev_only = np.zeros(n)
+        emul.lqm_emul_tridiag(n, d.ctypes.data_as(P), e.ctypes.data_as(P), ev_only.ctypes.data_as(P),
+                              Z.ctypes.data_as(P), 0)
         T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
         scale = max(np.max(np.abs(d)), 1.0)
         assert np.max(np.abs(ev - np.linalg.eigvalsh(T))) <= 1e-13 * scale
+        assert np.max(np.abs(ev_only - np.linalg.eigvalsh(T))) <= 1e-13 * scale  # eigenvalue-only merges
         assert np.all(np.diff(ev) >= 0)
         assert np.max(np.abs(Z.T @ Z - np.eye(n))) <= 1e-13
         assert np.max(np.abs(T @ Z - Z * ev)) <= 1e-13 * scale
