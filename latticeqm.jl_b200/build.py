@@ -13,7 +13,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libkspace.so")
 SOURCES = ["lqm_capi.cu"]
-DEPS = ["lqm_capi.cu", "lqm_kernels.cuh", "lqm_eigh.cuh", "lqm_team.cuh", "lqm_hf.cuh", "lqm_scf.inc", "lqm_plan.h"]
+DEPS = ["lqm_capi.cu", "lqm_kernels.cuh", "lqm_eigh.cuh", "lqm_team.cuh", "lqm_hf.cuh", "lqm_scf.inc", "lqm_plan.h",
+        "lqm_blocked.cuh", "lqm_large.cuh"]
+CUDA_LIB = "/usr/local/cuda/lib64"
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -42,7 +44,8 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-I", CSRC, "-I", os.path.join(ROOT, "include"),
-           *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
+           *[os.path.join(CSRC, s) for s in SOURCES], "-L", CUDA_LIB, "-lcublas",
+           "-Xlinker", "-rpath=" + CUDA_LIB, "-o", LIB + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

@@ -1,5 +1,6 @@
 // C ABI of libkspace (declared in include/kspace.h).  Host side: argument
 // validation, device buffers, the k-batch loop and kernel launches.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +18,7 @@
 
 #include "kspace.h"
 #include "lqm_kernels.cuh"
+#include "lqm_large.cuh"
 #include "lqm_hf.cuh"
 #include "lqm_plan.h"
 
@@ -51,7 +53,7 @@ struct lqm_ctx {
   int num_sms = 0;
   double last_ms = 0.0;
   std::map<int, PlanDev> plans;
-  DevBuf ws[24];
+  DevBuf ws[32];
   // per-kernel device-time statistics (CUDA events on the context stream)
   bool stats_on = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending, ev_pool;
@@ -59,6 +61,8 @@ struct lqm_ctx {
   int64_t eigh_launches = 0, launches = 0;
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
+  cublasHandle_t blas = nullptr;          // batched GEMMs of the blocked large-n path
+  int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: only beyond the one-CTA plan)
 };
 
 struct lqm_hops {
@@ -155,7 +159,8 @@ void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
 
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
-  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD
+  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD,
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS
 };
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
@@ -209,10 +214,153 @@ struct RhoOut {
   double mu, T;
 };
 
+// ---- blocked large-n path (lqm_large.cuh) ----
+void blas_ck(cublasStatus_t st, const char* what) {
+  if (st != CUBLAS_STATUS_SUCCESS) fail(st == CUBLAS_STATUS_ALLOC_FAILED ? LQM_ENOMEM : LQM_ECUDA, "%s: cuBLAS status %d", what, (int)st);
+}
+
+cublasHandle_t blas_handle(lqm_ctx* ctx) {
+  if (!ctx->blas) blas_ck(cublasCreate(&ctx->blas), "cublasCreate");
+  blas_ck(cublasSetStream(ctx->blas, ctx->stream), "cublasSetStream");
+  const size_t wsb = (size_t)32 << 20;  // fixed workspace: no allocation inside captured sequences
+  blas_ck(cublasSetWorkspace(ctx->blas, ws_get(ctx, WS_LBLAS, wsb), wsb), "cublasSetWorkspace");
+  return ctx->blas;
+}
+
+// C_b = alpha op(A_b) op(B_b) + beta C_b for b < batch (column-major, strided).
+void zgemm_sb(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, double alpha_re,
+              const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB, double beta_re,
+              double2* C, int ldc, long long sC, int batch) {
+  if (m <= 0 || n <= 0 || batch <= 0) return;
+  const cuDoubleComplex al = make_cuDoubleComplex(alpha_re, 0.0), be = make_cuDoubleComplex(beta_re, 0.0);
+  blas_ck(cublasZgemmStridedBatched(h, ta, tb, m, n, k, &al, (const cuDoubleComplex*)A, lda, sA,
+                                    (const cuDoubleComplex*)B, ldb, sB, &be, (cuDoubleComplex*)C, ldc, sC, batch),
+          "cublasZgemmStridedBatched");
+}
+
+struct RhoOut;
+bool use_blocked(const lqm_ctx* ctx, int n, int nR);
+
+// Eigen pass of the blocked path: same outputs as launch_eigh.  Reduction by
+// zlatrd panels (column kernels + batched rank-2nb updates), divide and
+// conquer per k, compact-WY back-transformation and rho_k = U f U^H as batched
+// GEMMs.  k-points are processed in batches sized to ~24 GB of work buffers.
+void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands,
+                       double2* d_U, double2* rhok, double* ebk, const double* w, double mu, double T) {
+  const int n = (int)H->n;
+  const int nb = kBlkNB;
+  const int P = (n + nb - 1) / nb;
+  const bool vec = d_U || rhok;
+  const int64_t nn = (int64_t)n * n;
+  const int64_t auxk = 2 * (int64_t)n * nb /*W, Y*/ + (int64_t)nb * nb * P /*Tm*/ + n /*tau*/ + 2 * nb /*t12*/;
+  const double per_k = 16.0 * (double)nn * ((vec && !d_U) ? 2.0 : 1.0) + 16.0 * (double)auxk + 16.0 * n;
+  int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(24.0e9 / per_k)));
+  B = std::min<int64_t>(B, 65535);
+  const int64_t slotd = dc_large_slot_doubles(n, vec);
+  const int64_t G = std::min<int64_t>(B, (int64_t)ctx->num_sms);
+  double2* A = (double2*)ws_get(ctx, WS_LA, (size_t)B * nn * sizeof(double2));
+  double2* Uw = (vec && !d_U) ? (double2*)ws_get(ctx, WS_LU, (size_t)B * nn * sizeof(double2)) : nullptr;
+  double2* aux = (double2*)ws_get(ctx, WS_LAUX, (size_t)B * (auxk + n) * sizeof(double2));
+  double2* W = aux;                                   // B x (n x nb); reused as X (nb x n) in the back-transform
+  double2* Yb = W + B * (int64_t)n * nb;              // B x (nb x n)
+  double2* Tm = Yb + B * (int64_t)n * nb;             // B x P x (nb x nb)
+  double2* tau = Tm + B * (int64_t)nb * nb * P;       // B x n
+  double2* t12 = tau + B * (int64_t)n;                // B x 2nb
+  double* dd = (double*)(t12 + B * 2 * (int64_t)nb);  // B x n
+  double* ee = dd + B * (int64_t)n;                   // B x n
+  double* slots = (double*)ws_get(ctx, WS_LDC, (size_t)G * slotd * sizeof(double));
+  const DCPlan& plan = get_plan(ctx, n);
+  cublasHandle_t h = blas_handle(ctx);
+  const int gemv_smem = (n + (kBlkThreads / 32) * kBlkRows) * (int)sizeof(double2);
+  ck(cudaFuncSetAttribute(blk_gemv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, gemv_smem), "smem attr");
+  std::pair<cudaEvent_t, cudaEvent_t> evs{};
+  if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
+  for (int64_t k0 = 0; k0 < nk; k0 += B) {
+    const int nbk = (int)std::min<int64_t>(B, nk - k0);
+    const size_t bsm = (size_t)H->nR * sizeof(double2) + (size_t)H->d * sizeof(double) + 16;
+    blk_bloch_kernel<<<nbk, kBlkThreads, bsm, ctx->stream>>>(n, (int)H->nR, H->d, H->blocks, H->keys, nbk,
+                                                              d_ks + k0 * H->d, A);
+    ctx->launches++;
+    const BlkArgs ba{n, nb, A, W, tau, dd, ee, t12};
+    for (int p = 0; p < P; ++p) {
+      const int j0 = p * nb;
+      const int nbp = std::min(nb, n - j0);
+      for (int i = 0; i < nbp; ++i) {
+        const int j = j0 + i;
+        blk_column_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
+        ctx->launches++;
+        if (j <= n - 2) {
+          const int m = n - j - 1;
+          const dim3 grid((unsigned)((m + kBlkRows - 1) / kBlkRows), (unsigned)nbk);
+          const int sm = (m + (kBlkThreads / 32) * kBlkRows) * (int)sizeof(double2);
+          blk_gemv_kernel<<<grid, kBlkThreads, sm, ctx->stream>>>(ba, j0, i);
+          ctx->launches++;
+        }
+      }
+      if (j0 + nbp < n) {
+        blk_finish_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0 + nbp - 1, nbp - 1);
+        ctx->launches++;
+        const int m2 = n - j0 - nbp;
+        double2* A22 = A + (j0 + nbp) + (int64_t)(j0 + nbp) * n;
+        const double2* V = A + (j0 + nbp) + (int64_t)j0 * n;
+        const double2* Wt = W + (j0 + nbp);
+        zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, m2, m2, nbp, -1.0, V, n, nn, Wt, n, (long long)n * nb, 1.0, A22, n,
+                 nn, nbk);
+        zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, m2, m2, nbp, -1.0, Wt, n, (long long)n * nb, V, n, nn, 1.0, A22, n,
+                 nn, nbk);
+        ctx->launches += 2;
+      }
+    }
+    ck(cudaGetLastError(), "blocked reduction launch");
+    double2* Ucur = d_U ? d_U + k0 * nn : Uw;
+    DCLargeArgs da;
+    da.n = n; da.nk = nbk; da.plan = plan; da.d = dd; da.e = ee; da.bands = d_bands + k0 * n;
+    da.U = vec ? Ucur : nullptr; da.slots = slots; da.slot_doubles = slotd;
+    dc_large_kernel<<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, 0, ctx->stream>>>(da);
+    ctx->launches++;
+    ck(cudaGetLastError(), "divide-and-conquer launch");
+    if (!vec) continue;
+    blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A);
+    blk_larft_kernel<<<dim3((unsigned)P, (unsigned)nbk), kBlkThreads, nb * nb * sizeof(double2), ctx->stream>>>(
+        n, nb, P, A, tau, Tm);
+    ctx->launches += 2;
+    for (int p = P - 1; p >= 0; --p) {
+      const int j0 = p * nb;
+      const int nbr = std::min(nb, n - 1 - j0);
+      if (nbr <= 0) continue;
+      const int m = n - j0 - 1;
+      const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
+      double2* Us = Ucur + (j0 + 1);
+      // X = V^H Us (nbr x n), Y = Tm X, Us -= V Y
+      zgemm_sb(h, CUBLAS_OP_C, CUBLAS_OP_N, nbr, n, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nb, (long long)n * nb,
+               nbk);
+      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, nbr, n, nbr, 1.0, Tm + (int64_t)p * nb * nb, nb,
+               (long long)nb * nb * P, W, nb, (long long)n * nb, 0.0, Yb, nb, (long long)n * nb, nbk);
+      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, nbr, -1.0, V, n, nn, Yb, nb, (long long)n * nb, 1.0, Us, n, nn,
+               nbk);
+      ctx->launches += 3;
+    }
+    if (rhok) {
+      blk_scale_f_kernel<<<nbk, kBlkThreads, n * sizeof(double), ctx->stream>>>(
+          n, nbk, Ucur, d_bands + k0 * n, mu, nullptr, T, w + k0, A, ebk + k0);
+      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, n, 1.0, A, n, nn, Ucur, n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
+      ctx->launches += 2;
+    }
+    ck(cudaGetLastError(), "back-transformation launch");
+  }
+  if (ctx->stats_on) { ck(cudaEventRecord(evs.second, ctx->stream), "event"); ctx->ev_pending.push_back(evs); }
+  ctx->eigh_launches++;
+}
+
 // Eigen pass over nk device k-points: bands (n x nk), optionally U and/or rho_k.
 void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands, double2* d_U,
                  const RhoOut* ro = nullptr) {
   const int n = (int)H->n;
+  if (use_blocked(ctx, n, (int)H->nR)) {
+    launch_eigh_large(ctx, H, nk, d_ks, d_bands, d_U, ro ? ro->rhok : nullptr, ro ? ro->ebk : nullptr,
+                      ro ? ro->w : nullptr, ro ? ro->mu : 0.0, ro ? ro->T : 0.0);
+    return;
+  }
   const DCPlan& plan = get_plan(ctx, n);
   const int nt = eigh_threads(n);
   EighSmemLayout Ls = eigh_smem_layout(n, (int)H->nR, nt, 1);
@@ -248,6 +396,13 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   if (ctx->stats_on) { ck(cudaEventRecord(evs.second, ctx->stream), "event"); ctx->ev_pending.push_back(evs); }
   ctx->eigh_launches++;
   ctx->launches++;
+}
+
+// The one-CTA kernel holds the vectors of one k-point in shared memory; beyond
+// that (or from ctx->blocked_min_n on) the blocked path runs.
+bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
+  if (ctx->blocked_min_n > 0 && n >= ctx->blocked_min_n) return true;
+  return eigh_smem_layout(n, nR, eigh_threads(n), 0).total > 225 * 1024;
 }
 
 int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
@@ -436,6 +591,7 @@ int lqm_ctx_destroy(lqm_ctx* ctx) {
     if (b.p) cudaFree(b.p);
   for (auto& kv : ctx->plans) cudaFree(kv.second.d_buf);
   if (ctx->d_phase) cudaFree(ctx->d_phase);
+  if (ctx->blas) cublasDestroy(ctx->blas);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaStreamDestroy(ctx->stream);
@@ -448,6 +604,12 @@ const char* lqm_last_error(const lqm_ctx* ctx) { return ctx ? ctx->err.c_str() :
 int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds) {
   if (!ctx || !(seconds > 0)) return LQM_EINVAL;
   ctx->timeout_s = seconds;
+  return LQM_OK;
+}
+
+int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min) {
+  if (!ctx || n_min < 0) return LQM_EINVAL;
+  ctx->blocked_min_n = n_min;
   return LQM_OK;
 }
 

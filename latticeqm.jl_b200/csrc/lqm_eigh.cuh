@@ -35,6 +35,7 @@ struct EighVec {
   double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;  // red: 128
   int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
   double2 *tau, *v, *w, *vn, *pn, *bc, *pbuf;
+  double* tile = nullptr;  // 2048 doubles of team scratch for the tiled merge update (large n), or null
 };
 
 // ---------------------------------------------------------------------------
@@ -416,12 +417,79 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 #define LQM_SUBTICK(i_)
 #endif
 
+// Merge update of one node as a tiled GEMM (large merges):
+//   Qt[lo + r, newpos[it]] = sum_p Q[lo + r, colnd[p]] * Ubn[p + it*k],
+// r < hi - lo, it < k; p is summed in ascending order.  A 512-thread team uses
+// 64 x 64 output tiles staged through `tile` (16 p per stage, 4 x 2 outputs per
+// thread); other team sizes (the host emulation) take the plain loop.
+LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int* colnd, const int* newpos,
+                         const double* Q, double* Qt, const double* Ubn, double* tile) {
+  const int s = hi - lo;
+#if defined(__CUDA_ARCH__)
+  if (T.nt == 512 && tile != nullptr) {
+    double* As = tile;         // [16][64]: As[pp*64 + rr] = Q[lo + r0 + rr, colnd[p0 + pp]]
+    double* Bs = tile + 1024;  // [16][64]: Bs[pp*64 + cc] = Ubn[p0 + pp, c0 + cc]
+    const int tr = T.tid & 15, tc = T.tid >> 4;
+    for (int r0 = 0; r0 < s; r0 += 64) {
+      for (int c0 = 0; c0 < k; c0 += 64) {
+        double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0, a20 = 0.0, a21 = 0.0, a30 = 0.0, a31 = 0.0;
+        for (int p0 = 0; p0 < k; p0 += 16) {
+          for (int e = T.tid; e < 1024; e += 512) {
+            const int pp = e >> 6, rr = e & 63;
+            const int p = p0 + pp, r = r0 + rr;
+            As[e] = (p < k && r < s) ? Q[(lo + r) + (int64_t)colnd[p] * n] : 0.0;
+            const int pb = e & 15, cb = e >> 4;
+            const int pq = p0 + pb, cc = c0 + cb;
+            Bs[pb * 64 + cb] = (pq < k && cc < k) ? Ubn[pq + (int64_t)cc * k] : 0.0;
+          }
+          team_sync();
+#pragma unroll
+          for (int pp = 0; pp < 16; ++pp) {
+            const double2 x01 = *(const double2*)(As + pp * 64 + tr * 4);
+            const double2 x23 = *(const double2*)(As + pp * 64 + tr * 4 + 2);
+            const double2 y = *(const double2*)(Bs + pp * 64 + tc * 2);
+            a00 += x01.x * y.x; a01 += x01.x * y.y;
+            a10 += x01.y * y.x; a11 += x01.y * y.y;
+            a20 += x23.x * y.x; a21 += x23.x * y.y;
+            a30 += x23.y * y.x; a31 += x23.y * y.y;
+          }
+          team_sync();
+        }
+        const double acc[4][2] = {{a00, a01}, {a10, a11}, {a20, a21}, {a30, a31}};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int b = 0; b < 2; ++b) {
+            const int r = r0 + tr * 4 + q, cc = c0 + tc * 2 + b;
+            if (r < s && cc < k) Qt[(lo + r) + (int64_t)newpos[cc] * n] = acc[q][b];
+          }
+      }
+    }
+    return;
+  }
+#else
+  (void)tile;
+#endif
+  for (int it = T.wid; it < k; it += T.nw) {
+    double* dst = Qt + (int64_t)newpos[it] * n;
+    for (int r = T.lane; r < s; r += T.nl) {
+      double acc = 0.0;
+      for (int p = 0; p < k; ++p) acc += Q[(lo + r) + (int64_t)colnd[p] * n] * Ubn[p + (int64_t)it * k];
+      dst[lo + r] = acc;
+    }
+  }
+}
+
 // vec == false: eigenvalues only.  The merges then need just the first and
 // last rows of each node's eigenvector matrix (they form z), so Q (>= 4n
 // doubles) holds QF/QL (those rows, indexed by column) and FT/LT (the rows of
 // the node being merged), and every merge is O(size^2).
+// Ub (n*n doubles, or null) enables the tiled update for heights whose largest
+// merge has >= tile_min rows: node [lo, hi) keeps its normalised secular
+// vectors at Ub + lo*n (k x k, leading dimension k).
 LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
-                              unsigned long long* sub = nullptr, bool vec = true) {
+                              unsigned long long* sub = nullptr, bool vec = true, double* Ub = nullptr,
+                              int tile_min = 1 << 30) {
   double* ubuf = (double*)S.pbuf;  // per-warp secular eigenvector (n doubles each)
   double* QF = Q;
   double* QL = Q + n;
@@ -433,7 +501,6 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 #else
   (void)sub;
 #endif
-  const int64_t nn = (int64_t)n * n;
   double mx = 0.0;
   for (int i = T.tid; i < n; i += T.nt) {
     mx = fmax(mx, fabs(S.d[i]));
@@ -634,7 +701,41 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
         }
       }
     }
-    for (int c = T.wid; c < n && vec; c += T.nw) {
+    bool tiled = false;
+    if (vec && Ub != nullptr)
+      for (int nd = h0; nd < h1; ++nd) tiled = tiled || (P.hi[nd] - P.lo[nd] >= tile_min);
+    if (tiled) {
+      // secular vectors into Ub (warp per column), deflated columns copied
+      for (int c = T.wid; c < n; c += T.nw) {
+        const int nd = own[c];
+        if (nd < 0) continue;
+        const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];
+        if (it < k) {
+          double* ub = Ub + (int64_t)lo * n + (int64_t)it * k;
+          const double* dl = S.dl + lo;
+          const double lorg = dl[S.org[lo + it]], tq = S.troot[lo + it];
+          double ss = 0.0;
+          for (int p = T.lane; p < k; p += T.nl) {
+            const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
+            ub[p] = u;
+            ss += u * u;
+          }
+          const double sc = 1.0 / sqrt(warp_sum_bcast(ss));
+          for (int p = T.lane; p < k; p += T.nl) ub[p] *= sc;
+        } else {
+          double* dst = Qt + (int64_t)S.newpos[c] * n;
+          const double* src = Q + (int64_t)S.dcol[lo + it - k] * n;
+          for (int r = lo + T.lane; r < hi; r += T.nl) dst[r] = src[r];
+        }
+      }
+      team_sync();
+      for (int nd = h0; nd < h1; ++nd) {
+        const int lo = P.lo[nd];
+        dc_tile_gemm(T, n, lo, P.hi[nd], S.nk[nd], S.colnd + lo, S.newpos + lo, Q, Qt, Ub + (int64_t)lo * n,
+                     S.tile);
+      }
+    }
+    for (int c = T.wid; c < n && vec && !tiled; c += T.nw) {
       const int nd = own[c];
       if (nd < 0) continue;
       const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];

@@ -32,7 +32,7 @@ STATUS_NAMES = {-1: "LQM_EINVAL", -2: "LQM_ECUDA", -3: "LQM_ENOMEM", -4: "LQM_ET
                 -5: "LQM_ENOCONV", -6: "LQM_EDEVICE"}
 
 EXPORTS = [
-    "lqm_ctx_create", "lqm_ctx_destroy", "lqm_last_error", "lqm_ctx_set_timeout",
+    "lqm_ctx_create", "lqm_ctx_destroy", "lqm_last_error", "lqm_ctx_set_timeout", "lqm_ctx_set_blocked_min_n",
     "lqm_ctx_last_kernel_ms", "lqm_hops_upload_dense", "lqm_hops_upload_csc", "lqm_hops_free",
     "lqm_hops_dims", "lqm_bloch", "lqm_bloch_dev", "lqm_bandmatrix", "lqm_bandmatrix_dev",
     "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
@@ -61,6 +61,7 @@ _SIG = {
     "lqm_ctx_create": [ctypes.c_int, ctypes.POINTER(_P)],
     "lqm_ctx_destroy": [_P],
     "lqm_ctx_set_timeout": [_P, _D],
+    "lqm_ctx_set_blocked_min_n": [_P, _I64],
     "lqm_ctx_last_kernel_ms": [_P, ctypes.POINTER(_D)],
     "lqm_hops_upload_dense": [_P, _I64, _I64, ctypes.c_int32, _P, _P, ctypes.POINTER(_P)],
     "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(_P)],
@@ -126,6 +127,11 @@ class Context:
     def check(self, st):
         if st != LQM_OK:
             raise LQMError(st, (_lib.lqm_last_error(self._h) or b"").decode())
+
+    def set_blocked_min_n(self, n_min):
+        """Orders n >= n_min use the batched blocked eigensolver (0: only where the
+        one-CTA-per-k kernel does not fit)."""
+        self.check(_lib.lqm_ctx_set_blocked_min_n(self._h, int(n_min)))
 
     def last_kernel_ms(self):
         v = _D()

@@ -4,9 +4,11 @@
 // arithmetic of bloch_build / hetrd_lower / dc_solve / backtransform from
 // latticeqm.jl_b200/csrc/lqm_eigh.cuh against LAPACK, without a GPU.
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
+#include "lqm_blocked.cuh"
 #include "lqm_eigh.cuh"
 #include "lqm_plan.h"
 
@@ -87,6 +89,108 @@ extern "C" int lqm_emul_tridiag(int n, const double* d, const double* e, double*
   std::vector<double> rows(4 * (size_t)n + 4);
   dc_solve(T, n, P, S, vec ? Z : rows.data(), Qt.data(), nullptr, vec != 0);
   std::memcpy(evals, S.D, sizeof(double) * n);
+  return 0;
+}
+
+static DCPlan plan_view(const lqm::DCPlanHost& PH) {
+  DCPlan P;
+  P.nnodes = PH.nnodes;
+  P.nheights = PH.nheights;
+  P.hstart = PH.buf.data() + PH.off_hstart;
+  P.lo = PH.buf.data() + PH.off_lo;
+  P.mid = PH.buf.data() + PH.off_mid;
+  P.hi = PH.buf.data() + PH.off_hi;
+  P.owner = PH.buf.data() + PH.off_own;
+  return P;
+}
+
+// The blocked large-n path on one k-point: panel reduction (blk_column,
+// blk_gemv_rows, blk_finish_w with the rank-2nb update done here as loops),
+// divide and conquer with the tiled merge update from tile_min rows on, and
+// the compact-WY back-transformation (blk_larft, products done here).
+extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* blocks, const int64_t* keys,
+                                     const double* kpt, int nb, int tile_min, int want_vectors, double* evals,
+                                     double* U) {
+  const Team T = make_host_team();
+  const size_t nn = (size_t)n * n;
+  std::vector<double2> A(nn), W((size_t)n * nb), tau(n), t12(2 * nb), vs(n + 1), part(4), ph(nR + 1);
+  std::vector<double> d(n), e(n), red(128);
+  bloch_build(T, n, nR, dim, (const double2*)blocks, keys, kpt, ph.data(), A.data(), n);
+  const int P = (n + nb - 1) / nb;
+  for (int p = 0; p < P; ++p) {
+    const int j0 = p * nb, nbp = std::min(nb, n - j0);
+    for (int i = 0; i < nbp; ++i) {
+      const int j = j0 + i;
+      blk_column(T, n, nb, j0, i, A.data(), n, W.data(), n, tau.data(), d.data(), e.data(), t12.data(), red.data());
+      if (j <= n - 2)
+        blk_gemv_rows(T, n, nb, j0, i, j + 1, n, A.data(), n, W.data(), n, tau.data(), t12.data(), vs.data(),
+                      part.data());
+    }
+    if (j0 + nbp < n) {
+      blk_finish_w(T, n, j0 + nbp - 1, nbp - 1, A.data(), n, W.data(), n, tau.data(), red.data());
+      for (int c = j0 + nbp; c < n; ++c)
+        for (int r = j0 + nbp; r < n; ++r) {
+          double2 a = A[r + (size_t)c * n];
+          for (int l = 0; l < nbp; ++l) {
+            const double2 vr = A[r + (size_t)(j0 + l) * n], vc = A[c + (size_t)(j0 + l) * n];
+            const double2 wr = W[r + (size_t)l * n], wc = W[c + (size_t)l * n];
+            a = csub(a, cadd(cmul(vr, cconj(wc)), cmul(wr, cconj(vc))));
+          }
+          A[r + (size_t)c * n] = a;
+        }
+    }
+  }
+  const lqm::DCPlanHost PH = lqm::make_dc_plan_host(n);
+  const DCPlan PV = plan_view(PH);
+  std::vector<double> dbuf(13 * (size_t)n + 132), Q(nn + 4 * (size_t)n + 4), Qt(nn), Ub(nn);
+  std::vector<int> ibuf(10 * (size_t)n);
+  std::vector<double2> pb((size_t)n + 8);
+  EighVec S;
+  double* db = dbuf.data();
+  S.d = db; S.e = db + n; S.D = db + 2 * n; S.z = db + 3 * n; S.dl = db + 4 * n; S.zl = db + 5 * n;
+  S.troot = db + 6 * n; S.zhat = db + 7 * n; S.vals = db + 8 * n; S.dval = db + 9 * n; S.rc = db + 10 * n;
+  S.rs = db + 11 * n; S.nrho = db + 12 * n; S.red = db + 13 * n;
+  int* ib = ibuf.data();
+  S.perm = ib; S.colnd = ib + n; S.org = ib + 2 * n; S.dcol = ib + 3 * n; S.newpos = ib + 4 * n;
+  S.ri = ib + 5 * n; S.rj = ib + 6 * n; S.nk = ib + 7 * n; S.nrot = ib + 8 * n; S.ndef = ib + 9 * n;
+  S.pbuf = pb.data();
+  std::memcpy(S.d, d.data(), sizeof(double) * n);
+  std::memcpy(S.e, e.data(), sizeof(double) * n);
+  if (n > 0) S.e[n - 1] = 0.0;
+  dc_solve(T, n, PV, S, Q.data(), Qt.data(), nullptr, want_vectors != 0, Ub.data(), tile_min);
+  std::memcpy(evals, S.D, sizeof(double) * n);
+  if (!want_vectors) return 0;
+  double2* Uc = (double2*)U;
+  for (size_t i = 0; i < nn; ++i) Uc[i] = cmk(Q[i], 0.0);
+  blk_prep_reflectors(T, n, A.data(), n);
+  std::vector<double2> Tm((size_t)nb * nb), G((size_t)nb * nb), X((size_t)nb * n);
+  for (int p = P - 1; p >= 0; --p) {
+    const int j0 = p * nb, nbr = std::min(nb, n - 1 - j0);
+    if (nbr <= 0) continue;
+    const int m = n - j0 - 1;
+    blk_larft(T, n, nb, j0, nbr, A.data(), n, tau.data(), Tm.data(), G.data());
+    const double2* V = A.data() + (j0 + 1) + (size_t)j0 * n;
+    double2* Us = Uc + (j0 + 1);
+    for (int c = 0; c < n; ++c)
+      for (int l = 0; l < nbr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int r = 0; r < m; ++r) acc = cadd(acc, cmulc(V[r + (size_t)l * n], Us[r + (size_t)c * n]));
+        X[l + (size_t)c * nb] = acc;
+      }
+    for (int c = 0; c < n; ++c) {
+      double2 y[64];
+      for (int l = 0; l < nbr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int q = 0; q < nbr; ++q) acc = cadd(acc, cmul(Tm[l + (size_t)q * nb], X[q + (size_t)c * nb]));
+        y[l] = acc;
+      }
+      for (int r = 0; r < m; ++r) {
+        double2 u = Us[r + (size_t)c * n];
+        for (int l = 0; l < nbr; ++l) u = csub(u, cmul(V[r + (size_t)l * n], y[l]));
+        Us[r + (size_t)c * n] = u;
+      }
+    }
+  }
   return 0;
 }
 

@@ -66,6 +66,30 @@ def test_emulated_eigh_matches_oracle(emul, name, h):
         assert np.max(np.abs(Hk @ U - U * ev)) / scale <= 1e-12
 
 
+@pytest.mark.parametrize("nb,tile_min", [(32, 16), (5, 8), (8, 1 << 30)])
+@pytest.mark.parametrize("name,h", models(), ids=lambda x: x if isinstance(x, str) else "")
+def test_emulated_blocked_eigh_matches_oracle(emul, name, h, nb, tile_min):
+    """The large-n path (panel reduction, tiled merge updates, compact-WY back-transformation)."""
+    keys, blocks = pack(h)
+    n, nR = blocks.shape[0], blocks.shape[2]
+    for k in [(0.0, 0.0), (0.123, 0.77)]:
+        kp = np.array(k, float)
+        ev = np.zeros(n)
+        ev_only = np.zeros(n)
+        U = np.zeros((n, n), complex, order="F")
+        emul.lqm_emul_eigh_blocked(n, nR, 2, blocks.ctypes.data_as(P), keys.ctypes.data_as(P),
+                                   kp.ctypes.data_as(P), nb, tile_min, 1, ev.ctypes.data_as(P), U.ctypes.data_as(P))
+        emul.lqm_emul_eigh_blocked(n, nR, 2, blocks.ctypes.data_as(P), keys.ctypes.data_as(P),
+                                   kp.ctypes.data_as(P), nb, tile_min, 0, ev_only.ctypes.data_as(P), None)
+        Hk = K.fouriersum(h, k)
+        ref = K.eigh_upper(Hk, vectors=False)
+        scale = max(ref[-1] - ref[0], 1.0)
+        assert np.max(np.abs(ev - ref)) / scale <= 1e-12
+        assert np.max(np.abs(ev_only - ref)) / scale <= 1e-12
+        assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12
+        assert np.max(np.abs(Hk @ U - U * ev)) / scale <= 1e-12
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 7, 16, 33, 64, 100])
 def test_emulated_tridiagonal_dc(emul, n):
     rng = np.random.default_rng(n)

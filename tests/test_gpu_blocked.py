@@ -1,0 +1,118 @@
+"""Parity of the batched blocked eigensolver (large-n path) with the oracle.
+
+The blocked path is what orders beyond the one-CTA shared-memory plan run
+(the twisted-bilayer workloads, n = 1324 and 2884).  Here it is also forced on
+small orders (``set_blocked_min_n(1)``) so that every model and pin of the
+plain path is checked through it.  Tolerances as in test_gpu_parity.py.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import kspace as K
+from lqm_workloads import lattice as L
+from lqm_workloads import models as M
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+BAND_TOL = 1e-10
+RHO_TOL = 1e-9
+
+
+def rel_band_err(b, ref):
+    return np.max(np.abs(b - ref)) / max(np.max(ref) - np.min(ref), 1.0)
+
+
+@pytest.fixture(scope="module")
+def bctx(lqm):
+    c = lqm.Context(0, timeout=900)
+    c.set_blocked_min_n(1)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def tbg10():
+    return M.tbg_slater_koster(10)[1]
+
+
+def test_blocked_tbg_golden_eigenvalues(lqm, bctx):
+    pins = json.load(open(os.path.join(GOLD, "reference_pins.json")))["pins"]
+    builders = {"honeycomb_twisted": L.honeycomb_twisted, "honeycomb_twisted_ABBA": L.honeycomb_twisted_ABBA,
+                "honeycomb_twisted_ABAB": L.honeycomb_twisted_ABAB}
+    from test_oracle_pins import pin_index
+    for p in pins:
+        h = M.graphene(builders[p["builder"]](p["N"]), tz=0.32)
+        b, _ = lqm.bandmatrix(h, np.array(p["k"]).reshape(2, 1), ctx=bctx)
+        i = pin_index(p["index"], b.shape[0])
+        assert abs(b[i, 0] - p["value"]) <= p["atol"], p
+
+
+def test_blocked_batch_models_bands_and_vectors(lqm, bctx):
+    rng = np.random.default_rng(11)
+    ks = np.hstack([L.regulargrid(8 * 8), rng.random((2, 9))])
+    for name, h in M.batch_models():
+        b, _ = lqm.bandmatrix(h, ks, ctx=bctx)
+        assert rel_band_err(b, K.bandmatrix(h, ks)[0]) <= BAND_TOL, name
+        b2, U = lqm.bandmatrix(h, ks[:, :5], want_vectors=True, ctx=bctx)
+        n = b2.shape[0]
+        for j in range(5):
+            Hk = K.fouriersum(h, ks[:, j])
+            assert np.max(np.abs(U[:, :, j].conj().T @ U[:, :, j] - np.eye(n))) < 1e-12, name
+            assert np.max(np.abs(Hk @ U[:, :, j] - U[:, :, j] * b2[:, j])) < 1e-11, name
+
+
+def test_blocked_densitymatrix_matches_oracle(lqm, bctx):
+    _, c1 = M.honeycomb_disorder()
+    for name, h in [("c1", c1)] + M.batch_models():
+        ks = L.regulargrid(6 * 6)
+        w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+        keys = list(h.keys())
+        rho = {R: None for R in keys}
+        eb = lqm.getdensitymatrix(rho, h, ks, mu=0.0, T=0.01, ctx=bctx)
+        rref, ebref = K.densitymatrix(h, ks, w, 0.0, 0.01, keys)
+        err = max(np.max(np.abs(rho[L_] - rref[L_])) for L_ in keys)
+        assert err <= RHO_TOL, (name, err)
+        assert abs(eb - ebref) <= 1e-9 * max(1.0, abs(ebref)), name
+
+
+def test_blocked_matches_one_cta_path(lqm, ctx, bctx):
+    """Same model through both eigensolvers: bands agree to rounding."""
+    h = M.batch_models()[2][1]
+    ks = np.random.default_rng(5).random((2, 300))
+    b1, _ = lqm.bandmatrix(h, ks, ctx=ctx)
+    b2, _ = lqm.bandmatrix(h, ks, ctx=bctx)
+    assert rel_band_err(b2, b1) <= 1e-12
+
+
+def test_tbg_1324_bands_vectors_rho(lqm, ctx, tbg10):
+    """Twisted bilayer m=10 (n = 1324): beyond the one-CTA plan, so the default context
+    takes the blocked path.  Bands, eigenpairs and rho_L on a few k-points."""
+    h = tbg10
+    n = next(iter(h.values())).shape[0]
+    assert n == 1324
+    ks = np.array([[0.0, 1 / 3, 0.137], [0.0, -1 / 3, 0.61]])
+    b, U = lqm.bandmatrix(h, ks, want_vectors=True, ctx=ctx)
+    ref = K.bandmatrix(h, ks)[0]
+    assert rel_band_err(b, ref) <= BAND_TOL
+    for j in range(ks.shape[1]):
+        Hk = K.fouriersum(h, ks[:, j])
+        assert np.max(np.abs(U[:, :, j].conj().T @ U[:, :, j] - np.eye(n))) < 1e-11
+        assert np.max(np.abs(Hk @ U[:, :, j] - U[:, :, j] * b[:, j])) < 1e-10
+    w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+    keys = list(h.keys())
+    rho = {R: None for R in keys}
+    eb = lqm.getdensitymatrix(rho, h, ks, kweights=w, mu=0.0, T=0.01, ctx=ctx)
+    rref, ebref = K.densitymatrix(h, ks, w, 0.0, 0.01, keys)
+    assert max(np.max(np.abs(rho[L_] - rref[L_])) for L_ in keys) <= RHO_TOL
+    assert abs(eb - ebref) <= 1e-9 * max(1.0, abs(ebref))
+
+
+def test_tbg_1324_kpath_eigenvalues_only(lqm, ctx, tbg10):
+    """Eigenvalue-only merges on the large path (the k-path part of the precision workload)."""
+    h = tbg10
+    ks = np.vstack([np.linspace(0, 0.5, 6), np.linspace(0, 0.25, 6)])
+    b, _ = lqm.bandmatrix(h, ks, ctx=ctx)
+    assert rel_band_err(b, K.bandmatrix(h, ks)[0]) <= BAND_TOL
