@@ -252,9 +252,11 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   const int P = (n + nb - 1) / nb;
   const bool vec = d_U || rhok;
   const int64_t nn = (int64_t)n * n;
-  const int64_t auxk = 2 * (int64_t)n * nb /*W, Y*/ + (int64_t)nb * nb * P /*Tm*/ + n /*tau*/ + 2 * nb /*t12*/;
+  const int64_t pstride = symv_part_stride(n), tstride = t12_part_stride(n, nb);
+  const int64_t auxk = 2 * (int64_t)n * nb /*W, Y*/ + (int64_t)nb * nb * P /*Tm*/ + n /*tau*/ + 2 * nb /*t12*/ +
+                       pstride /*mat-vec partials*/ + tstride /*panel-product partials*/;
   const double per_k = 16.0 * (double)nn * ((vec && !d_U) ? 2.0 : 1.0) + 16.0 * (double)auxk + 16.0 * n;
-  int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(24.0e9 / per_k)));
+  int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(48.0e9 / per_k)));
   B = std::min<int64_t>(B, 65535);
   const int64_t slotd = dc_large_slot_doubles(n, vec);
   const int64_t G = std::min<int64_t>(B, (int64_t)ctx->num_sms);
@@ -266,13 +268,16 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   double2* Tm = Yb + B * (int64_t)n * nb;             // B x P x (nb x nb)
   double2* tau = Tm + B * (int64_t)nb * nb * P;       // B x n
   double2* t12 = tau + B * (int64_t)n;                // B x 2nb
-  double* dd = (double*)(t12 + B * 2 * (int64_t)nb);  // B x n
+  double2* part = t12 + B * 2 * (int64_t)nb;          // B x pstride
+  double2* tpart = part + B * pstride;                // B x tstride
+  double* dd = (double*)(tpart + B * tstride);        // B x n
   double* ee = dd + B * (int64_t)n;                   // B x n
   double* slots = (double*)ws_get(ctx, WS_LDC, (size_t)G * slotd * sizeof(double));
   const DCPlan& plan = get_plan(ctx, n);
   cublasHandle_t h = blas_handle(ctx);
-  const int gemv_smem = (n + (kBlkThreads / 32) * kBlkRows) * (int)sizeof(double2);
-  ck(cudaFuncSetAttribute(blk_gemv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, gemv_smem), "smem attr");
+  ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
+     "smem attr");
+  ck(cudaFuncSetAttribute(dc_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDcTileSmem), "smem attr");
   std::pair<cudaEvent_t, cudaEvent_t> evs{};
   if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
   for (int64_t k0 = 0; k0 < nk; k0 += B) {
@@ -281,7 +286,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     blk_bloch_kernel<<<nbk, kBlkThreads, bsm, ctx->stream>>>(n, (int)H->nR, H->d, H->blocks, H->keys, nbk,
                                                               d_ks + k0 * H->d, A);
     ctx->launches++;
-    const BlkArgs ba{n, nb, A, W, tau, dd, ee, t12};
+    const BlkArgs ba{n, nb, A, W, tau, dd, ee, t12, part, pstride, tpart, tstride};
     for (int p = 0; p < P; ++p) {
       const int j0 = p * nb;
       const int nbp = std::min(nb, n - j0);
@@ -290,25 +295,36 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
         blk_column_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
         ctx->launches++;
         if (j <= n - 2) {
-          const int m = n - j - 1;
-          const dim3 grid((unsigned)((m + kBlkRows - 1) / kBlkRows), (unsigned)nbk);
-          const int sm = (m + (kBlkThreads / 32) * kBlkRows) * (int)sizeof(double2);
-          blk_gemv_kernel<<<grid, kBlkThreads, sm, ctx->stream>>>(ba, j0, i);
+          const int64_t nbl = (n - j - 1 + kSymvTB - 1) / kSymvTB;
+          const int64_t nitems = nbl * (nbl + 1) / 2 * nbk;
+          const int64_t grid = std::min<int64_t>(nitems, (int64_t)ctx->num_sms);
+          blk_symv_pipe_kernel<<<(unsigned)grid, kBlkThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
           ctx->launches++;
+          if (i > 0) {
+            const dim3 g2((unsigned)((n - j - 1 + 127) / 128), (unsigned)nbk);
+            blk_t12_kernel<<<g2, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
+            ctx->launches++;
+          }
         }
       }
       if (j0 + nbp < n) {
-        blk_finish_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0 + nbp - 1, nbp - 1);
+        blk_finish_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0, nbp - 1);
         ctx->launches++;
+        // A22 -= V W^H + W V^H on the lower triangle: column blocks [c0, c1) x rows [c0, m2)
         const int m2 = n - j0 - nbp;
-        double2* A22 = A + (j0 + nbp) + (int64_t)(j0 + nbp) * n;
-        const double2* V = A + (j0 + nbp) + (int64_t)j0 * n;
-        const double2* Wt = W + (j0 + nbp);
-        zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, m2, m2, nbp, -1.0, V, n, nn, Wt, n, (long long)n * nb, 1.0, A22, n,
-                 nn, nbk);
-        zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, m2, m2, nbp, -1.0, Wt, n, (long long)n * nb, V, n, nn, 1.0, A22, n,
-                 nn, nbk);
-        ctx->launches += 2;
+        const int cbw = 256;
+        for (int c0 = 0; c0 < m2; c0 += cbw) {
+          const int cw = std::min(cbw, m2 - c0);
+          const int rows = m2 - c0;
+          double2* Cb = A + (j0 + nbp + c0) + (int64_t)(j0 + nbp + c0) * n;
+          const double2* Vr = A + (j0 + nbp + c0) + (int64_t)j0 * n;
+          const double2* Wr = W + (j0 + nbp + c0);
+          zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, rows, cw, nbp, -1.0, Vr, n, nn, Wr, n, (long long)n * nb, 1.0, Cb, n,
+                   nn, nbk);
+          zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, rows, cw, nbp, -1.0, Wr, n, (long long)n * nb, Vr, n, nn, 1.0, Cb, n,
+                   nn, nbk);
+          ctx->launches += 2;
+        }
       }
     }
     ck(cudaGetLastError(), "blocked reduction launch");
@@ -316,7 +332,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     DCLargeArgs da;
     da.n = n; da.nk = nbk; da.plan = plan; da.d = dd; da.e = ee; da.bands = d_bands + k0 * n;
     da.U = vec ? Ucur : nullptr; da.slots = slots; da.slot_doubles = slotd;
-    dc_large_kernel<<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, 0, ctx->stream>>>(da);
+    da.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
+    dc_large_kernel<<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, kDcTileSmem, ctx->stream>>>(da);
     ctx->launches++;
     ck(cudaGetLastError(), "divide-and-conquer launch");
     if (!vec) continue;
@@ -436,7 +453,10 @@ void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
                  double* bands_out = nullptr) {
   const int n = (int)H->n;
   const int64_t nn = (int64_t)n * n;
-  const int64_t B = batch_size_for(n, nk, 4.0e9);
+  // rho_k batch: 4 GB, or one k-point per SM for large n (the blocked path
+  // runs one divide-and-conquer CTA per k-point)
+  const double budget = std::max(4.0e9, 16.0 * (double)nn * (double)std::min<int64_t>(nk, ctx->num_sms));
+  const int64_t B = batch_size_for(n, nk, budget);
   double2* rk = (double2*)ws_get(ctx, WS_RHOK, (size_t)B * nn * sizeof(double2));
   double* bandsb = bands_out ? nullptr : (double*)ws_get(ctx, WS_BANDS, (size_t)B * n * sizeof(double));
   double* ebk = (double*)ws_get(ctx, WS_EBK, (size_t)B * sizeof(double));

@@ -35,7 +35,7 @@ struct EighVec {
   double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;  // red: 128
   int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
   double2 *tau, *v, *w, *vn, *pn, *bc, *pbuf;
-  double* tile = nullptr;  // 2048 doubles of team scratch for the tiled merge update (large n), or null
+  double* tile = nullptr;  // 6144 doubles of team scratch for the tiled merge update (large n), or null
 };
 
 // ---------------------------------------------------------------------------
@@ -418,49 +418,83 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 #endif
 
 // Merge update of one node as a tiled GEMM (large merges):
-//   Qt[lo + r, newpos[it]] = sum_p Q[lo + r, colnd[p]] * Ubn[p + it*k],
-// r < hi - lo, it < k; p is summed in ascending order.  A 512-thread team uses
-// 64 x 64 output tiles staged through `tile` (16 p per stage, 4 x 2 outputs per
-// thread); other team sizes (the host emulation) take the plain loop.
+//   Qt[lo + r, newpos[it]] = sum_p Q[lo + r, colnd[p]] * Ubn[it + p*k],
+// r < hi - lo, it < k (Ubn holds the secular vectors as rows); p is summed in
+// ascending order.  A 512-thread team uses 128 x 128 output tiles (4 x 8 per
+// thread) and 8-deep p stages moved by cp.async through a 3-stage ring in
+// `tile` (3 x 2048 doubles), two stages in flight while one is summed; other
+// team sizes (the host emulation) take the plain loop.
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ void lqm_cp_async8(void* sdst, const void* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  const int nbytes = valid ? 8 : 0;  // 0: zero-filled, nothing is read
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(nbytes) : "memory");
+}
+#endif
 LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int* colnd, const int* newpos,
                          const double* Q, double* Qt, const double* Ubn, double* tile) {
   const int s = hi - lo;
 #if defined(__CUDA_ARCH__)
   if (T.nt == 512 && tile != nullptr) {
-    double* As = tile;         // [16][64]: As[pp*64 + rr] = Q[lo + r0 + rr, colnd[p0 + pp]]
-    double* Bs = tile + 1024;  // [16][64]: Bs[pp*64 + cc] = Ubn[p0 + pp, c0 + cc]
-    const int tr = T.tid & 15, tc = T.tid >> 4;
-    for (int r0 = 0; r0 < s; r0 += 64) {
-      for (int c0 = 0; c0 < k; c0 += 64) {
-        double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0, a20 = 0.0, a21 = 0.0, a30 = 0.0, a31 = 0.0;
-        for (int p0 = 0; p0 < k; p0 += 16) {
-          for (int e = T.tid; e < 1024; e += 512) {
-            const int pp = e >> 6, rr = e & 63;
-            const int p = p0 + pp, r = r0 + rr;
-            As[e] = (p < k && r < s) ? Q[(lo + r) + (int64_t)colnd[p] * n] : 0.0;
-            const int pb = e & 15, cb = e >> 4;
-            const int pq = p0 + pb, cc = c0 + cb;
-            Bs[pb * 64 + cb] = (pq < k && cc < k) ? Ubn[pq + (int64_t)cc * k] : 0.0;
-          }
-          team_sync();
-#pragma unroll
-          for (int pp = 0; pp < 16; ++pp) {
-            const double2 x01 = *(const double2*)(As + pp * 64 + tr * 4);
-            const double2 x23 = *(const double2*)(As + pp * 64 + tr * 4 + 2);
-            const double2 y = *(const double2*)(Bs + pp * 64 + tc * 2);
-            a00 += x01.x * y.x; a01 += x01.x * y.y;
-            a10 += x01.y * y.x; a11 += x01.y * y.y;
-            a20 += x23.x * y.x; a21 += x23.x * y.y;
-            a30 += x23.y * y.x; a31 += x23.y * y.y;
-          }
-          team_sync();
-        }
-        const double acc[4][2] = {{a00, a01}, {a10, a11}, {a20, a21}, {a30, a31}};
+    constexpr int BM = 128, BN = 128, BK = 8, STG = BK * BM + BK * BN, NS = 3;
+    const int tr = T.tid & 31, tc = T.tid >> 5;  // rows tr*4 .. +3, columns tc*8 .. +7
+    for (int r0 = 0; r0 < s; r0 += BM) {
+      for (int c0 = 0; c0 < k; c0 += BN) {
+        double acc[4][8];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int b = 0; b < 2; ++b) {
-            const int r = r0 + tr * 4 + q, cc = c0 + tc * 2 + b;
+          for (int b = 0; b < 8; ++b) acc[q][b] = 0.0;
+        // stage element e = tid + 512 h: A (pp = e / BM, rr = e % BM), B (pb = e / BN, cb = e % BN)
+        auto issue = [&](int p0, int st) {
+          double* As = tile + st * STG;
+          double* Bs = As + BK * BM;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int e = T.tid + 512 * h;
+            const int p = p0 + (e >> 7), r = r0 + (e & 127), cc = c0 + (e & 127);
+            const bool oka = p < k && r < s, okb = p < k && cc < k;
+            lqm_cp_async8(As + e, oka ? (const void*)(Q + (lo + r) + (int64_t)colnd[p] * n) : (const void*)Q, oka);
+            lqm_cp_async8(Bs + e, okb ? (const void*)(Ubn + cc + (int64_t)p * k) : (const void*)Ubn, okb);
+          }
+        };
+        const int nst = (k + BK - 1) / BK;
+        issue(0, 0);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        if (nst > 1) issue(BK, 1);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        for (int it = 0; it < nst; ++it) {
+          asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+          team_sync();
+          if (it + 2 < nst) issue((it + 2) * BK, (it + 2) % NS);
+          asm volatile("cp.async.commit_group;\n" ::: "memory");
+          const double* As = tile + (it % NS) * STG;
+          const double* Bs = As + BK * BM;
+#pragma unroll
+          for (int pp = 0; pp < BK; ++pp) {
+            const double2 x01 = *(const double2*)(As + pp * BM + tr * 4);
+            const double2 x23 = *(const double2*)(As + pp * BM + tr * 4 + 2);
+            const double xa[4] = {x01.x, x01.y, x23.x, x23.y};
+            double ya[8];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+              const double2 y2 = *(const double2*)(Bs + pp * BN + tc * 8 + 2 * b);
+              ya[2 * b] = y2.x;
+              ya[2 * b + 1] = y2.y;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+              for (int b = 0; b < 8; ++b) acc[q][b] += xa[q] * ya[b];
+          }
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        team_sync();  // the ring is free before the next tile's prologue
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            const int r = r0 + tr * 4 + q, cc = c0 + tc * 8 + b;
             if (r < s && cc < k) Qt[(lo + r) + (int64_t)newpos[cc] * n] = acc[q][b];
           }
       }
@@ -474,7 +508,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
     double* dst = Qt + (int64_t)newpos[it] * n;
     for (int r = T.lane; r < s; r += T.nl) {
       double acc = 0.0;
-      for (int p = 0; p < k; ++p) acc += Q[(lo + r) + (int64_t)colnd[p] * n] * Ubn[p + (int64_t)it * k];
+      for (int p = 0; p < k; ++p) acc += Q[(lo + r) + (int64_t)colnd[p] * n] * Ubn[it + (int64_t)p * k];
       dst[lo + r] = acc;
     }
   }
@@ -486,7 +520,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
 // the node being merged), and every merge is O(size^2).
 // Ub (n*n doubles, or null) enables the tiled update for heights whose largest
 // merge has >= tile_min rows: node [lo, hi) keeps its normalised secular
-// vectors at Ub + lo*n (k x k, leading dimension k).
+// vectors at Ub + lo*n as the rows of a k x k block (vector it at it + p*k).
 LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
                               unsigned long long* sub = nullptr, bool vec = true, double* Ub = nullptr,
                               int tile_min = 1 << 30) {
@@ -711,17 +745,17 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
         if (nd < 0) continue;
         const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];
         if (it < k) {
-          double* ub = Ub + (int64_t)lo * n + (int64_t)it * k;
+          double* ub = Ub + (int64_t)lo * n + it;  // row it of the node's k x k block (stride k)
           const double* dl = S.dl + lo;
           const double lorg = dl[S.org[lo + it]], tq = S.troot[lo + it];
           double ss = 0.0;
           for (int p = T.lane; p < k; p += T.nl) {
             const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
-            ub[p] = u;
+            ub[(int64_t)p * k] = u;
             ss += u * u;
           }
           const double sc = 1.0 / sqrt(warp_sum_bcast(ss));
-          for (int p = T.lane; p < k; p += T.nl) ub[p] *= sc;
+          for (int p = T.lane; p < k; p += T.nl) ub[(int64_t)p * k] *= sc;
         } else {
           double* dst = Qt + (int64_t)S.newpos[c] * n;
           const double* src = Q + (int64_t)S.dcol[lo + it - k] * n;

@@ -4,7 +4,9 @@
 //
 //   blk_bloch_kernel    H(k) (full Hermitian, from the upper triangle), CTA per k
 //   blk_column_kernel   zlatrd column step (lqm_blocked.cuh), CTA per k
-//   blk_gemv_kernel     w = tau (A22 v - corrections), 128-row slabs x k
+//   blk_symv_kernel     y = A22 v from the lower triangle, 64 x 64 tiles x k,
+//                       plus row slabs of the panel products t1, t2; ordered
+//                       partials (summed by the next column step)
 //   blk_finish_kernel   last w of a panel, CTA per k
 //   (host)              rank-2nb trailing update, batched ZGEMM
 //   dc_large_kernel     divide and conquer per k (vectors in global memory,
@@ -19,8 +21,8 @@
 namespace lqm {
 
 constexpr int kBlkNB = 32;      // panel width (reflectors per panel)
-constexpr int kBlkRows = 128;   // rows per mat-vec CTA (4 per lane)
 constexpr int kBlkThreads = 256;
+constexpr int kSymvTB = 64;     // mat-vec tile (2 rows per lane of a 32-lane warp)
 constexpr int kDcThreads = 512;
 constexpr int kDcTileMin = 160; // merges with at least this many rows use the tiled update
 
@@ -32,7 +34,23 @@ struct BlkArgs {
   double* d;     // B x n
   double* e;     // B x n
   double2* t12;  // B x 2nb
+  double2* part; // B x part_stride: mat-vec tile partials
+  int64_t part_stride;
+  double2* tpart;  // B x tpart_stride: panel-product slab partials
+  int64_t tpart_stride;
 };
+
+// complex per k-point for the panel-product partials: slabs of 128 rows x 2nb
+__host__ __device__ inline int64_t t12_part_stride(int n, int nb) {
+  const int64_t nsl = (n - 1 + 127) / 128;
+  return (nsl < 1 ? 1 : nsl) * 2 * nb;
+}
+
+// complex per k-point for the mat-vec partials: nblk^2 tiles of kSymvTB
+__host__ __device__ inline int64_t symv_part_stride(int n) {
+  const int64_t nbk = (n - 1 + kSymvTB - 1) / kSymvTB;
+  return (nbk < 1 ? 1 : nbk * nbk) * kSymvTB;
+}
 
 __global__ void __launch_bounds__(kBlkThreads) blk_bloch_kernel(int n, int nR, int dim,
                                                                 const double2* __restrict__ blocks,
@@ -50,34 +68,159 @@ __global__ void __launch_bounds__(kBlkThreads) blk_bloch_kernel(int n, int nR, i
 
 __global__ void __launch_bounds__(kBlkThreads) blk_column_kernel(BlkArgs a, int j0, int i) {
   __shared__ double red[128];
+  __shared__ __align__(16) double2 t12[2 * kBlkNB];
   const Team T = make_team();
   const int64_t b = blockIdx.x;
   const int n = a.n;
   blk_column(T, n, a.nb, j0, i, a.A + b * (int64_t)n * n, n, a.W + b * (int64_t)n * a.nb, n, a.tau + b * n,
-             a.d + b * n, a.e + b * n, a.t12 + b * 2 * a.nb, red);
+             a.d + b * n, a.e + b * n, t12, red, a.part + b * a.part_stride, a.tpart + b * a.tpart_stride);
 }
 
-__global__ void __launch_bounds__(kBlkThreads) blk_finish_kernel(BlkArgs a, int jp, int ip) {
+// Last column of a panel: finish its w from the partials.
+__global__ void __launch_bounds__(kBlkThreads) blk_finish_kernel(BlkArgs a, int j0, int ip) {
   __shared__ double red[128];
+  __shared__ __align__(16) double2 t12[2 * kBlkNB];
   const Team T = make_team();
   const int64_t b = blockIdx.x;
   const int n = a.n;
-  blk_finish_w(T, n, jp, ip, a.A + b * (int64_t)n * n, n, a.W + b * (int64_t)n * a.nb, n, a.tau + b * n, red);
+  blk_prev_w(T, n, a.nb, j0, ip, a.A + b * (int64_t)n * n, n, a.W + b * (int64_t)n * a.nb, n, a.tau + b * n, t12,
+             red, a.part + b * a.part_stride, a.tpart + b * a.tpart_stride, nullptr);
 }
 
-// grid (ceil((n-j-1)/kBlkRows), B); dynamic smem: vs (n-j-1) | part (nw x 128), double2
-__global__ void __launch_bounds__(kBlkThreads) blk_gemv_kernel(BlkArgs a, int j0, int i) {
-  extern __shared__ __align__(16) unsigned char smem[];
+// grid (nslabs, B): row slabs of the panel products of column j = j0 + i.
+__global__ void __launch_bounds__(kBlkThreads) blk_t12_kernel(BlkArgs a, int j0, int i) {
   const Team T = make_team();
-  const int n = a.n, j = j0 + i;
-  const int m = n - j - 1;
-  double2* vs = (double2*)smem;
-  double2* part = vs + m;
   const int64_t b = blockIdx.y;
-  const int r0 = j + 1 + blockIdx.x * kBlkRows;
-  const int r1 = (r0 + kBlkRows < n) ? r0 + kBlkRows : n;
-  blk_gemv_rows(T, n, a.nb, j0, i, r0, r1, a.A + b * (int64_t)n * n, n, a.W + b * (int64_t)n * a.nb, n,
-                a.tau + b * n, a.t12 + b * 2 * a.nb, vs, part);
+  blk_t12_slab(T, a.n, a.nb, j0, i, blockIdx.x, a.A + b * (int64_t)a.n * a.n, a.n, a.W + b * (int64_t)a.n * a.nb, a.n,
+               a.tpart + b * a.tpart_stride);
+}
+
+// ---- Hermitian mat-vec of one column, persistent and pipelined ----
+// The same arithmetic and partial layout as blk_symv_tile (64 x 64 lower
+// tiles, direct + transposed partials), but each CTA walks a list of tiles
+// (all k-points of the batch) with a kSymvStages-deep cp.async pipeline, so
+// that two tiles are in flight from HBM while a third is summed.
+constexpr int kSymvStages = 3;
+constexpr int kSymvLd = kSymvTB + 1;
+constexpr int kSymvStageC = kSymvTB * kSymvLd + 2 * kSymvTB;  // complex per stage: tile + v_R, v_C
+constexpr int kSymvPipeSmem = (kSymvStages * kSymvStageC + 2 * (kBlkThreads / kSymvTB) * kSymvTB) * 16;
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  const int nbytes = valid ? 16 : 0;  // 0: the 16 bytes are zero-filled, nothing is read
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(nbytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_keep1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// tile t of the lower block triangle -> (R, C), R >= C, row-major
+__device__ __forceinline__ void symv_tile_rc(int t, int* R, int* C) {
+  int r = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((r + 1) * (r + 2) / 2 <= t) ++r;
+  while (r * (r + 1) / 2 > t) --r;
+  *R = r;
+  *C = t - r * (r + 1) / 2;
+}
+
+// Issue the copies of work item `it` (k-point it / ntiles, tile it % ntiles)
+// into stage buffer `st`; rows/columns beyond m are zero-filled.
+__device__ __forceinline__ void symv_issue(const BlkArgs& a, int j, int m, int ntiles, int64_t it, double2* st) {
+  const int64_t b = it / ntiles;
+  int R, C;
+  symv_tile_rc((int)(it - b * ntiles), &R, &C);
+  const double2* A = a.A + b * (int64_t)a.n * a.n;
+  const double2* B = A + (j + 1) + (int64_t)(j + 1) * a.n;
+  const double2* v = A + (j + 1) + (int64_t)j * a.n;
+  const int x0 = R * kSymvTB, y0 = C * kSymvTB;
+#pragma unroll
+  for (int h = 0; h < (kSymvTB * kSymvTB) / kBlkThreads; ++h) {
+    const int idx = threadIdx.x + h * kBlkThreads, rr = idx % kSymvTB, cc = idx / kSymvTB;
+    const int x = x0 + rr, y = y0 + cc;
+    const bool ok = x < m && y < m;
+    cp_async16(st + rr + cc * kSymvLd, ok ? (const void*)(B + x + (int64_t)y * a.n) : (const void*)B, ok);
+  }
+  if (threadIdx.x < 2 * kSymvTB) {
+    const int t = threadIdx.x;
+    const int x = (t < kSymvTB) ? x0 + t : y0 + (t - kSymvTB);
+    cp_async16(st + kSymvTB * kSymvLd + t, x < m ? (const void*)(v + x) : (const void*)v, x < m);
+  }
+}
+
+// grid: persistent (about one CTA per SM), kSymvPipeSmem dynamic smem.
+__global__ void __launch_bounds__(kBlkThreads, 1) blk_symv_pipe_kernel(BlkArgs a, int j, int64_t nitems) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  double2* stg = (double2*)smem;
+  double2* rd = stg + kSymvStages * kSymvStageC;           // [ng][TB] direct
+  constexpr int ng = kBlkThreads / kSymvTB;
+  double2* rt = rd + ng * kSymvTB;                         // [ng][TB] transposed
+  const int m = a.n - j - 1;
+  const int nbk = (m + kSymvTB - 1) / kSymvTB;
+  const int ntiles = nbk * (nbk + 1) / 2;
+  const int64_t first = blockIdx.x, step = gridDim.x;
+  // prologue: stages 0 .. kSymvStages-2
+#pragma unroll
+  for (int s = 0; s < kSymvStages - 1; ++s) {
+    const int64_t it = first + s * step;
+    if (it < nitems) symv_issue(a, j, m, ntiles, it, stg + s * kSymvStageC);
+    cp_async_commit();
+  }
+  int stage = 0;
+  for (int64_t it = first; it < nitems; it += step) {
+    cp_async_wait_keep1();  // the group of item `it` has landed (kSymvStages == 3)
+    __syncthreads();
+    {
+      const int64_t nx = it + (kSymvStages - 1) * step;
+      const int ns = (stage + kSymvStages - 1) % kSymvStages;
+      if (nx < nitems) symv_issue(a, j, m, ntiles, nx, stg + ns * kSymvStageC);
+      cp_async_commit();
+    }
+    const double2* ts = stg + stage * kSymvStageC;
+    const double2* vR = ts + kSymvTB * kSymvLd;
+    const double2* vC = vR + kSymvTB;
+    const int64_t b = it / ntiles;
+    int R, C;
+    symv_tile_rc((int)(it - b * ntiles), &R, &C);
+    const bool diag = (R == C);
+    {
+      const int q = threadIdx.x % kSymvTB, g = threadIdx.x / kSymvTB;
+      double2 ad = cmk(0.0, 0.0), at = cmk(0.0, 0.0);
+#pragma unroll 4
+      for (int u = g; u < kSymvTB; u += ng) {
+        // direct: row q, column u (lower part only on a diagonal tile, diagonal real)
+        double2 x = ts[q + u * kSymvLd];
+        if (diag) {
+          if (u > q) x = cmk(0.0, 0.0);
+          else if (u == q) x.y = 0.0;
+        }
+        ad = cadd(ad, cmul(x, vC[u]));
+        // transposed: row u, column q (strictly lower on a diagonal tile)
+        double2 y = ts[u + q * kSymvLd];
+        if (diag && u <= q) y = cmk(0.0, 0.0);
+        at = cadd(at, cmulc(y, vR[u]));
+      }
+      rd[threadIdx.x] = ad;
+      rt[threadIdx.x] = at;
+    }
+    __syncthreads();
+    if (threadIdx.x < kSymvTB) {
+      const int x = threadIdx.x;
+      double2 yd = cmk(0.0, 0.0), yt = cmk(0.0, 0.0);
+#pragma unroll
+      for (int g = 0; g < ng; ++g) {
+        yd = cadd(yd, rd[g * kSymvTB + x]);
+        yt = cadd(yt, rt[g * kSymvTB + x]);
+      }
+      double2* part = a.part + b * a.part_stride;
+      if (diag) {
+        part[((int64_t)R * nbk + C) * kSymvTB + x] = cadd(yd, yt);
+      } else {
+        part[((int64_t)R * nbk + C) * kSymvTB + x] = yd;
+        part[((int64_t)C * nbk + R) * kSymvTB + x] = yt;
+      }
+    }
+    stage = (stage + 1) % kSymvStages;
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 __global__ void __launch_bounds__(kBlkThreads) blk_prep_kernel(int n, double2* A) {
@@ -113,6 +256,7 @@ struct DCLargeArgs {
   double2* U;        // nk x (n x n): Z as complex, or null (eigenvalues only)
   double* slots;     // gridDim.x slots
   int64_t slot_doubles;
+  unsigned long long* phase_cycles;  // [16] as eigh_kernel's (d&c total and merge steps), or null
 };
 
 __host__ __device__ inline int64_t dc_large_slot_doubles(int n, bool vec) {
@@ -121,9 +265,11 @@ __host__ __device__ inline int64_t dc_large_slot_doubles(int n, bool vec) {
   return (vec ? 3 * nn : 4 * (int64_t)n + 4) + vecs;
 }
 
+constexpr int kDcTileSmem = 6144 * 8;  // dynamic: the merge GEMM's cp.async ring
+
 __global__ void __launch_bounds__(kDcThreads) dc_large_kernel(DCLargeArgs a) {
   __shared__ double red[128];
-  __shared__ __align__(16) double tile[2048];
+  extern __shared__ __align__(16) double tile[];
   const Team T = make_team();
   const int n = a.n;
   const bool vec = a.U != nullptr;
@@ -145,13 +291,18 @@ __global__ void __launch_bounds__(kDcThreads) dc_large_kernel(DCLargeArgs a) {
   S.pbuf = (double2*)(((uintptr_t)pb + 15) & ~(uintptr_t)15);
   S.tau = S.v = S.w = S.vn = S.pn = S.bc = nullptr;
   S.tile = tile;
+  const bool prof = a.phase_cycles != nullptr;
+  unsigned long long dsub[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long dtot = 0;
   for (int64_t k = blockIdx.x; k < a.nk; k += gridDim.x) {
     for (int i = T.tid; i < n; i += T.nt) {
       S.d[i] = a.d[k * n + i];
       S.e[i] = (i < n - 1) ? a.e[k * n + i] : 0.0;
     }
     team_sync();
-    dc_solve(T, n, a.plan, S, Q, Qt, nullptr, vec, Ub, kDcTileMin);
+    const long long t0 = prof ? clock64() : 0;
+    dc_solve(T, n, a.plan, S, Q, Qt, prof ? dsub : nullptr, vec, Ub, kDcTileMin);
+    if (prof) dtot += (unsigned long long)(clock64() - t0);
     for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
     if (vec) {
       double2* Uk = a.U + k * nn;
@@ -159,6 +310,10 @@ __global__ void __launch_bounds__(kDcThreads) dc_large_kernel(DCLargeArgs a) {
         for (int r = T.lane; r < n; r += T.nl) Uk[r + (int64_t)c * n] = cmk(Q[r + (int64_t)c * n], 0.0);
     }
     team_sync();
+  }
+  if (prof && T.tid == 0) {
+    atomicAdd(&a.phase_cycles[PH_DC], dtot);
+    for (int i = 0; i < 8; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + i], dsub[i]);
   }
 }
 

@@ -105,7 +105,7 @@ static DCPlan plan_view(const lqm::DCPlanHost& PH) {
 }
 
 // The blocked large-n path on one k-point: panel reduction (blk_column,
-// blk_gemv_rows, blk_finish_w with the rank-2nb update done here as loops),
+// blk_symv_tile, blk_t12_slab, blk_prev_w; the rank-2nb update done here as loops),
 // divide and conquer with the tiled merge update from tile_min rows on, and
 // the compact-WY back-transformation (blk_larft, products done here).
 extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* blocks, const int64_t* keys,
@@ -113,7 +113,12 @@ extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* block
                                      double* U) {
   const Team T = make_host_team();
   const size_t nn = (size_t)n * n;
-  std::vector<double2> A(nn), W((size_t)n * nb), tau(n), t12(2 * nb), vs(n + 1), part(4), ph(nR + 1);
+  const int nbk = std::max(1, symv_nblk(T, n - 1));
+  std::vector<double2> A(nn), W((size_t)n * nb), tau(n), t12(2 * nb), ph(nR + 1);
+  const int TB = symv_tb(T);
+  std::vector<double2> part((size_t)nbk * nbk * TB), ts((size_t)TB * (TB + 1)), svs(2 * TB), sred(2 * TB);
+  const int nsl_max = std::max(1, (n - 1 + t12_rows(T) - 1) / t12_rows(T));
+  std::vector<double2> tpart((size_t)nsl_max * 2 * nb);
   std::vector<double> d(n), e(n), red(128);
   bloch_build(T, n, nR, dim, (const double2*)blocks, keys, kpt, ph.data(), A.data(), n);
   const int P = (n + nb - 1) / nb;
@@ -121,15 +126,23 @@ extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* block
     const int j0 = p * nb, nbp = std::min(nb, n - j0);
     for (int i = 0; i < nbp; ++i) {
       const int j = j0 + i;
-      blk_column(T, n, nb, j0, i, A.data(), n, W.data(), n, tau.data(), d.data(), e.data(), t12.data(), red.data());
-      if (j <= n - 2)
-        blk_gemv_rows(T, n, nb, j0, i, j + 1, n, A.data(), n, W.data(), n, tau.data(), t12.data(), vs.data(),
-                      part.data());
+      blk_column(T, n, nb, j0, i, A.data(), n, W.data(), n, tau.data(), d.data(), e.data(), t12.data(), red.data(),
+                 part.data(), tpart.data());
+      if (j <= n - 2) {
+        const int nbl = symv_nblk(T, n - j - 1);
+        for (int R = 0; R < nbl; ++R)
+          for (int C = 0; C <= R; ++C)
+            blk_symv_tile(T, n, j, R, C, A.data(), n, part.data(), ts.data(), svs.data(), sred.data());
+        const int nsl = (n - j - 1 + t12_rows(T) - 1) / t12_rows(T);
+        for (int sl = 0; i > 0 && sl < nsl; ++sl)
+          blk_t12_slab(T, n, nb, j0, i, sl, A.data(), n, W.data(), n, tpart.data());
+      }
     }
     if (j0 + nbp < n) {
-      blk_finish_w(T, n, j0 + nbp - 1, nbp - 1, A.data(), n, W.data(), n, tau.data(), red.data());
+      blk_prev_w(T, n, nb, j0, nbp - 1, A.data(), n, W.data(), n, tau.data(), t12.data(), red.data(), part.data(),
+                 tpart.data(), nullptr);
       for (int c = j0 + nbp; c < n; ++c)
-        for (int r = j0 + nbp; r < n; ++r) {
+        for (int r = c; r < n; ++r) {
           double2 a = A[r + (size_t)c * n];
           for (int l = 0; l < nbp; ++l) {
             const double2 vr = A[r + (size_t)(j0 + l) * n], vc = A[c + (size_t)(j0 + l) * n];
