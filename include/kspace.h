@@ -170,6 +170,26 @@ int lqm_scf_hf(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, c
 int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32_t d, const int64_t* d_keys,
                            const double* d_blocks, int64_t nk, const double* d_ks, double* d_bands, double* d_U);
 
+/* ---- Reverse-mode derivatives (no reference counterpart: the reference has
+ * no derivatives; the forward maps are lqm_densitymatrix and lqm_bandmatrix).
+ *
+ * Density response at fixed mu and T.  Gbar: nL blocks (2*n*n doubles each,
+ * keys Lkeys, d x nL) holding dLoss/d rho_L; output Hbar: one block per key
+ * of H (H's key order) such that dLoss = Re sum_R <Hbar_R, dH_R> for every
+ * Hermitian-consistent perturbation (dH_{-R} = dH_R^H), <A,B> = sum conj(A) B:
+ *   Hbar_R = sum_k e^{-i2pi k.R} w_k U [F o (U^H B_k U)] U^H,
+ *   B_k = sum_L e^{+i2pi k.L} Gbar_L,
+ *   F_ij = (f_i - f_j)/(eps_i - eps_j), f'((eps_i+eps_j)/2) for |eps_i - eps_j| <= 1e-6 T.
+ * w == NULL: uniform weights 1/nk.  The gradient of the grand potential
+ * -T sum_k w_k sum_j log(1 + e^{-(eps_j - mu)/T}) with respect to H_R is rho_R
+ * itself (lqm_densitymatrix). */
+int lqm_densitymatrix_vjp(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
+                          double mu, double T, int64_t nL, const int64_t* Lkeys, const double* Gbar,
+                          double* Hbar);
+/* Band cotangent: eps_bar (n x nk, dLoss/d eps) -> Hbar_R = sum_k e^{-i2pi k.R} U diag(eps_bar_k) U^H. */
+int lqm_bands_vjp(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* eps_bar,
+                  double* Hbar);
+
 #ifdef __cplusplus
 }
 #endif

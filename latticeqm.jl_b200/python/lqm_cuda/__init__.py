@@ -38,7 +38,7 @@ EXPORTS = [
     "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
     "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
-    "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc",
+    "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
 ]
 
 
@@ -83,6 +83,8 @@ _SIG = {
     "lqm_ctx_phase_cycles": [_P, ctypes.POINTER(_D)],
     "lqm_bandmatrix_noalloc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _I64, _P, _P, _P],
     "lqm_ctx_stats": [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+    "lqm_densitymatrix_vjp": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, _P],
+    "lqm_bands_vjp": [_P, _P, _I64, _P, _P, _P],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -290,6 +292,38 @@ def getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, multimode="cuda
     for i, L in enumerate(Lkeys):
         rhos[L] = np.array(out[:, :, i])
     return eb.value
+
+
+def densitymatrix_vjp(H, ks, Gbar, kweights=None, mu=0.0, T=0.01, ctx=None):
+    """Reverse-mode derivative of ``getdensitymatrix!`` at fixed mu and T
+    (``lqm_densitymatrix_vjp``).  ``Gbar``: dict L -> n x n cotangent dLoss/d rho_L.
+    Returns dict R -> n x n (H's keys) with dLoss = Re sum_R <Hbar_R, dH_R> for
+    Hermitian-consistent dH."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    Lkeys = list(Gbar.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    G = np.asfortranarray(np.stack([np.asarray(Gbar[L], dtype=np.complex128) for L in Lkeys], axis=-1))
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = np.zeros((Hd.n, Hd.n, Hd.nR), dtype=np.complex128, order="F")
+    ctx.check(_lib.lqm_densitymatrix_vjp(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(w), float(mu),
+                                         float(T), len(Lkeys), _ptr(Lk), _ptr(G), _ptr(out)))
+    return {R: np.array(out[:, :, i]) for i, R in enumerate(Hd.keys)}
+
+
+def bands_vjp(H, ks, eps_bar, ctx=None):
+    """Reverse-mode derivative of ``bandmatrix``: eps_bar (n, nk) = dLoss/d bands ->
+    dict R -> n x n with Hbar_R = sum_k e^{-i2pi k.R} U diag(eps_bar_k) U^H."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    eb = np.asfortranarray(np.asarray(eps_bar, dtype=np.float64))
+    if eb.shape != (Hd.n, ks.shape[1]):
+        raise ValueError("eps_bar must have shape (n, nk)")
+    out = np.zeros((Hd.n, Hd.n, Hd.nR), dtype=np.complex128, order="F")
+    ctx.check(_lib.lqm_bands_vjp(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(eb), _ptr(out)))
+    return {R: np.array(out[:, :, i]) for i, R in enumerate(Hd.keys)}
 
 
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):

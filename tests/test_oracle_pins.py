@@ -184,3 +184,75 @@ def test_workload_shapes(builder, n):
     hh = h if builder != "batch" else M.batch_models()[2][1]
     for R, blk in hh.items():
         assert np.allclose(blk, hh[tuple(-x for x in R)].conj().T)
+
+
+# ---------------------------------------------------------------- adjoints (finite differences)
+def _small_model():
+    from lqm_workloads import models as M
+    return M.batch_models()[0][1]  # square 2x2 spinful, n = 8
+
+
+def test_densitymatrix_vjp_matches_finite_differences():
+    from oracle import adjoint as AD
+    h = _small_model()
+    rng = np.random.default_rng(4)
+    ks = rng.random((2, 5))
+    w = np.full(5, 0.2)
+    mu, T = 0.1, 0.05
+    keys = list(h.keys())
+    Gbar = {L: rng.normal(size=h[L].shape) + 1j * rng.normal(size=h[L].shape) for L in keys}
+    Hbar = AD.densitymatrix_vjp(h, ks, w, mu, T, Gbar)
+    dH = AD.hermitian_direction(h, rng)
+
+    def loss(hh):
+        rho, _ = K.densitymatrix(hh, ks, w, mu, T, keys)
+        return AD.pairing(Gbar, rho)
+
+    step = 1e-6
+    hp = {R: h[R] + step * dH[R] for R in h}
+    hm = {R: h[R] - step * dH[R] for R in h}
+    fd = (loss(hp) - loss(hm)) / (2 * step)
+    an = AD.pairing(Hbar, dH)
+    assert abs(fd - an) <= 1e-6 * max(1.0, abs(an))
+
+
+def test_bands_vjp_matches_finite_differences():
+    from oracle import adjoint as AD
+    h = _small_model()
+    rng = np.random.default_rng(8)
+    ks = rng.random((2, 4))
+    n = h[(0, 0)].shape[0]
+    # the spinful bands come in degenerate pairs: a loss that weights both members of
+    # a pair alike is differentiable (the pair's projector is smooth)
+    eb = np.repeat(rng.normal(size=(n // 2, ks.shape[1])), 2, axis=0)
+    Hbar = AD.bands_vjp(h, ks, eb)
+    dH = AD.hermitian_direction(h, rng)
+
+    def loss(hh):
+        return float(np.sum(eb * K.bandmatrix(hh, ks)[0]))
+
+    step = 1e-6
+    fd = (loss({R: h[R] + step * dH[R] for R in h}) - loss({R: h[R] - step * dH[R] for R in h})) / (2 * step)
+    an = AD.pairing(Hbar, dH)
+    assert abs(fd - an) <= 1e-6 * max(1.0, abs(an))
+
+
+def test_grand_potential_gradient_is_rho():
+    """d/dH_R of -T sum_k w_k sum_j log(1 + exp(-(eps_j - mu)/T)) equals rho_R (Hellmann-Feynman)."""
+    from oracle import adjoint as AD
+    h = _small_model()
+    rng = np.random.default_rng(9)
+    ks = rng.random((2, 4))
+    w = np.full(4, 0.25)
+    mu, T = 0.0, 0.1
+    keys = list(h.keys())
+    rho, _ = K.densitymatrix(h, ks, w, mu, T, keys)
+    dH = AD.hermitian_direction(h, rng)
+
+    def omega(hh):
+        b = K.bandmatrix(hh, ks)[0]
+        return float(-T * np.sum(w * np.sum(np.logaddexp(0.0, -(b - mu) / T), axis=0)))
+
+    step = 1e-6
+    fd = (omega({R: h[R] + step * dH[R] for R in h}) - omega({R: h[R] - step * dH[R] for R in h})) / (2 * step)
+    assert abs(fd - AD.pairing(rho, dH)) <= 1e-6 * max(1.0, abs(fd))
