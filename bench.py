@@ -163,6 +163,98 @@ def cpu_time_per_k(models, pool, cores):
     return out
 
 
+def _cpu_density_worker(args):
+    """Oracle per-k work of a density-matrix call (one BLAS thread): H(k), zheevr with
+    vectors, rho_k = U f U^H and its Fourier fold into every key of H."""
+    import numpy as np
+    from oracle import kspace as K
+    h, ks = args
+    keys = list(h.keys())
+    n = next(iter(h.values())).shape[0]
+    rho = np.zeros((len(keys), n, n), complex)
+    for j in range(ks.shape[1]):
+        k = ks[:, j]
+        e, U = K.eigh_upper(K.fouriersum(h, k), True)
+        rk = (U * K.fermidirac(e, MU, TEMP)) @ U.conj().T
+        for li, Lk in enumerate(keys):
+            rho[li] += np.exp(-2j * math.pi * float(np.dot(k, Lk))) * rk
+    return ks.shape[1]
+
+
+def cpu_density_rate(h, pool, cores, per_core, seed=0):
+    """Host k-points per second of the oracle density-matrix k-loop on `cores` processes."""
+    import numpy as np
+    ks = np.random.default_rng(seed).random((2, per_core * cores))
+    chunks = [(h, np.ascontiguousarray(c)) for c in np.array_split(ks, cores, axis=1) if c.shape[1]]
+    t0 = time.perf_counter()
+    done = sum(pool.map(_cpu_density_worker, chunks))
+    return done / (time.perf_counter() - t0)
+
+
+def large_configs(Q, ctx, M, pool, cores):
+    """The other configurations of the hot path, one call each after a warm-up call,
+    through the host-pointer C-ABI: device time of the call's kernels (CUDA events
+    inside the library) and wall time including uploads and result copies."""
+    import numpy as np
+    from lqm_workloads import lattice as LL
+    out = {}
+
+    def timed(fn, reps=1):
+        fn()
+        best_dev, best_wall = 1e30, 1e30
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            best_wall = min(best_wall, time.perf_counter() - t0)
+            best_dev = min(best_dev, ctx.last_kernel_ms() / 1e3)
+        return best_dev, best_wall
+
+    def density_call(h, ks):
+        rho = {R: None for R in h}
+        return lambda: Q.getdensitymatrix(rho, h, ks, mu=MU, T=TEMP, ctx=ctx)
+
+    # honeycomb 6x6 spinful with onsite disorder, n = 144, 48 x 48 grid
+    _, h1 = M.honeycomb_disorder()
+    ks1 = LL.regulargrid(48 * 48)
+    dv, wl = timed(lambda: Q.bandmatrix(h1, ks1, ctx=ctx), reps=3)
+    dd, wd = timed(density_call(h1, ks1), reps=3)
+    out["honeycomb6x6_n144"] = {
+        "grid": "48x48", "bands_kpts_per_s": ks1.shape[1] / dv, "bands_wall_kpts_per_s": ks1.shape[1] / wl,
+        "rho_kpts_per_s": ks1.shape[1] / dd, "rho_wall_kpts_per_s": ks1.shape[1] / wd,
+        "cpu_rho_kpts_per_s": cpu_density_rate(h1, pool, cores, 8) if pool else None,
+        "path": "one-CTA-per-k eigensolver (global-memory scratch)"}
+    # twisted bilayer m=10, n = 1324: 24 x 24 grid (bands + rho) and a 400-point k-path (bands)
+    lat3, h3 = M.tbg_slater_koster(10)
+    ks3 = LL.regulargrid(24 * 24)
+    kp3 = LL.kpath(lat3, 400)
+    dd, wd = timed(density_call(h3, ks3))
+    db, wb = timed(lambda: Q.bandmatrix(h3, kp3, ctx=ctx))
+    out["tbg_m10_n1324"] = {
+        "grid": "24x24", "rho_kpts_per_s": ks3.shape[1] / dd, "rho_wall_kpts_per_s": ks3.shape[1] / wd,
+        "kpath_points": kp3.shape[1], "kpath_bands_kpts_per_s": kp3.shape[1] / db,
+        "kpath_bands_wall_kpts_per_s": kp3.shape[1] / wb,
+        "cpu_rho_kpts_per_s": cpu_density_rate(h3, pool, cores, 1) if pool else None,
+        "path": "batched blocked eigensolver"}
+    # twisted bilayer m=15, n = 2884: one eigen + rho pass over the 12 x 12 grid (the
+    # k-space work of one SCF iteration)
+    _, h5 = M.tbg_slater_koster(15)
+    ks5 = LL.regulargrid(12 * 12)
+    dd, wd = timed(density_call(h5, ks5))
+    out["tbg_m15_n2884"] = {"grid": "12x12", "rho_pass_s": dd, "rho_pass_wall_s": wd,
+                            "rho_kpts_per_s": ks5.shape[1] / dd, "path": "batched blocked eigensolver",
+                            "cpu": "not sampled (about a minute per k-point and core)"}
+    # adjoint: density-response VJP on the triangular Hubbard model (n = 72, 36 x 36)
+    _, h4, _ = M.triangular_hubbard(L_super=6)
+    ks4 = LL.regulargrid(36 * 36)
+    n4 = h4[(0, 0)].shape[0]
+    rng = np.random.default_rng(1)
+    G = {(0, 0): rng.normal(size=(n4, n4)) + 1j * rng.normal(size=(n4, n4))}
+    dv, wv = timed(lambda: Q.densitymatrix_vjp(h4, ks4, G, mu=0.0, T=0.02, ctx=ctx), reps=3)
+    out["vjp_triangular_n72"] = {"grid": "36x36", "vjp_kpts_per_s": ks4.shape[1] / dv,
+                                 "vjp_wall_kpts_per_s": ks4.shape[1] / wv}
+    return out
+
+
 def make_pool(cores):
     import multiprocessing as mp
     for var in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
@@ -251,6 +343,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (n=144, 1324, 2884 and the adjoint)")
     ap.add_argument("--profile-case", action="store_true",
                     help="one fused call on the n=96 model over 2048 k-points (small case for ncu)")
     args = ap.parse_args()
@@ -442,16 +536,21 @@ def main():
                        "iterations 2+ replay a captured CUDA graph"}
 
     cpu = None
+    configs = None
+    pool = None
+    cores = os.cpu_count() or 1
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cores = os.cpu_count() or 1
         pool = make_pool(cores)
         tpk = cpu_time_per_k(models, pool, cores)
-        pool.close()
         t_step = sum(NK_LIN * NK_LIN * t for t in tpk.values())
         sample = ", ".join(f"n={n}: {c * cores} k" for n, c in CPU_SAMPLE_PER_CORE.items())
         cpu = {"value": len(state) * NK_LIN * NK_LIN / t_step, "unit": "k-pts/s", "cores": cores, "kind": "port",
                "sample": f"random k-points per model ({sample}), oracle per-k zheevr+rho+fold+DOS on {cores} "
                          f"processes, extrapolated to 3x256x256 k"}
+    if rank == 0 and world == 1 and not args.no_configs:
+        configs = large_configs(Q, ctx, M, pool, cores)
+    if pool is not None:
+        pool.close()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "k-pts/s", "n_gpus": world, "steps": args.steps,
@@ -461,7 +560,8 @@ def main():
                            "parallelism": f"dp{world} (k-grid shards; rho_R/DOS all-reduce)",
                            "l2": "inputs larger than L2 (each step streams ~8 GB of U/rho_k through HBM)"},
                 "e2e": {"value": e2e_val, "unit": "k-pts/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "scf": scf}
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "scf": scf,
+                "configs": configs}
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

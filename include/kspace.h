@@ -161,8 +161,9 @@ int lqm_scf_hf(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, c
  * pointer and H given as device keys (d x nR Int64) and blocks (n x n x nR
  * ComplexF64), launched on `stream` (a cudaStream_t; NULL = legacy default).
  * Scratch comes from a fixed 64 MiB device array inside the library (held on
- * every GPU that loads it until exit); n <= 1024 and one k-point's scratch
- * must fit, larger n returns LQM_EINVAL.  The first call on a device resolves
+ * every GPU that loads it until exit); n <= 1024, within the one-CTA
+ * shared-memory plan (about 470), and one k-point's scratch must fit; other
+ * orders return LQM_EINVAL.  The first call on a device resolves
  * that array's address and should come before any stream capture.  Calls that
  * overlap on the GPU share the array and race.  Returns LQM_OK, LQM_EINVAL
  * (sizes/pointers) or LQM_ECUDA (launch/runtime error); it does not wait for

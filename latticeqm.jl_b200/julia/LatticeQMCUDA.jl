@@ -199,6 +199,77 @@ function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractM
     ρ, out[1], info, out[8] != 0, out[7]
 end
 
+# ---------------------------------------------------------------- derivatives
+"""
+    cuda_densitymatrix(H, ks, kweights, μ, T, Lkeys, exec) -> Dict(L => ρ_L)
+
+Out-of-place `getdensitymatrix!` (keys `Lkeys`), the differentiable form: the
+ChainRulesCore extension (`LatticeQMCUDAChainRulesExt.jl`) gives it an `rrule`
+through `cuda_densitymatrix_vjp`.
+"""
+function cuda_densitymatrix(H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64}, μ::Real, T::Real,
+                            Lkeys, exec::CudaExec)
+    n = size(H[first(keys(H))], 1)
+    ρs = Dict(L => zeros(ComplexF64, n, n) for L in Lkeys)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    Lk = collect(Lkeys)
+    d = length(first(Lk))
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    rho = zeros(ComplexF64, n, n, length(Lk))
+    eb = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_densitymatrix, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Int64, Ptr{Int64},
+         Ptr{ComplexF64}, Ref{Float64}, Cint),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Vector{Float64}(kweights), Float64(μ), Float64(T),
+        length(Lk), L, rho, eb, precision_code(exec)))
+    for (i, k) in enumerate(Lk)
+        ρs[k] .= view(rho, :, :, i)
+    end
+    ρs
+end
+
+"""
+    cuda_densitymatrix_vjp(Ḡ, H, ks, kweights, μ, T, exec) -> Dict(R => H̄_R)
+
+Reverse-mode derivative of the density matrix at fixed μ and T
+(`lqm_densitymatrix_vjp`): from Ḡ_L = ∂Loss/∂ρ_L to H̄_R = ∂Loss/∂H_R, with
+dLoss = Re Σ_R ⟨H̄_R, dH_R⟩ for Hermitian-consistent perturbations
+(dH_{-R} = dH_R'), the ChainRulesCore convention for complex entries.
+"""
+function cuda_densitymatrix_vjp(Ḡ, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64}, μ::Real,
+                                T::Real, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    Lk = collect(keys(Ḡ))
+    d = length(first(Lk))
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    G = Array{ComplexF64}(undef, n, n, length(Lk))
+    for (i, k) in enumerate(Lk)
+        G[:, :, i] .= Ḡ[k]
+    end
+    out = zeros(ComplexF64, n, n, length(dh.keys))
+    check(ctx, ccall((:lqm_densitymatrix_vjp, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Int64, Ptr{Int64},
+         Ptr{ComplexF64}, Ptr{ComplexF64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Vector{Float64}(kweights), Float64(μ), Float64(T),
+        length(Lk), L, G, out))
+    Dict(R => out[:, :, i] for (i, R) in enumerate(dh.keys))
+end
+
+"""Reverse-mode derivative of the bands (`lqm_bands_vjp`): ε̄ (n x nk) -> Dict(R => H̄_R)."""
+function cuda_bands_vjp(ε̄::AbstractMatrix{Float64}, H, ks::AbstractMatrix{Float64}, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    out = zeros(ComplexF64, n, n, length(dh.keys))
+    check(ctx, ccall((:lqm_bands_vjp, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Matrix{Float64}(ε̄), out))
+    Dict(R => out[:, :, i] for (i, R) in enumerate(dh.keys))
+end
+
 # ---------------------------------------------------------------- executor hooks
 # Per-k closures cannot run on the device: the generic k-loops refuse CudaExec.
 Parallel.kspace_foreach!(body!, ks::AbstractMatrix, exec::CudaExec; kwargs...) =
