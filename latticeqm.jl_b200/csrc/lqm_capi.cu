@@ -278,7 +278,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   cublasHandle_t h = blas_handle(ctx);
   ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
      "smem attr");
-  ck(cudaFuncSetAttribute(dc_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDcTileSmem), "smem attr");
+  ck(cudaFuncSetAttribute(dc_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dc_tile_smem(n)),
+     "smem attr");
   std::pair<cudaEvent_t, cudaEvent_t> evs{};
   if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
   for (int64_t k0 = 0; k0 < nk; k0 += B) {
@@ -299,7 +300,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           const int64_t nbl = (n - j - 1 + kSymvTB - 1) / kSymvTB;
           const int64_t nitems = nbl * (nbl + 1) / 2 * nbk;
           const int64_t grid = std::min<int64_t>(nitems, (int64_t)ctx->num_sms);
-          blk_symv_pipe_kernel<<<(unsigned)grid, kBlkThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
+          blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
           ctx->launches++;
           if (i > 0) {
             const dim3 g2((unsigned)((n - j - 1 + 127) / 128), (unsigned)nbk);
@@ -334,7 +335,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     da.n = n; da.nk = nbk; da.plan = plan; da.d = dd; da.e = ee; da.bands = d_bands + k0 * n;
     da.U = vec ? Ucur : nullptr; da.slots = slots; da.slot_doubles = slotd;
     da.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
-    dc_large_kernel<<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, kDcTileSmem, ctx->stream>>>(da);
+    dc_large_kernel<<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, dc_tile_smem(n), ctx->stream>>>(da);
     ctx->launches++;
     ck(cudaGetLastError(), "divide-and-conquer launch");
     if (!vec) continue;

@@ -35,7 +35,7 @@ struct EighVec {
   double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;  // red: 128
   int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
   double2 *tau, *v, *w, *vn, *pn, *bc, *pbuf;
-  double* tile = nullptr;  // 6144 doubles of team scratch for the tiled merge update (large n), or null
+  double* tile = nullptr;  // team scratch for the tiled merge update (large n): 6144 doubles + n ints, or null
 };
 
 // ---------------------------------------------------------------------------
@@ -421,9 +421,11 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 //   Qt[lo + r, newpos[it]] = sum_p Q[lo + r, colnd[p]] * Ubn[it + p*k],
 // r < hi - lo, it < k (Ubn holds the secular vectors as rows); p is summed in
 // ascending order.  A 512-thread team uses 128 x 128 output tiles (4 x 8 per
-// thread) and 8-deep p stages moved by cp.async through a 3-stage ring in
-// `tile` (3 x 2048 doubles), two stages in flight while one is summed; other
-// team sizes (the host emulation) take the plain loop.
+// thread: rows 2t, 2t+1, 64+2t, 65+2t of the tile so that the lanes of a warp
+// read consecutive 16-byte words) and 8-deep p stages moved by cp.async
+// through a 3-stage ring in `tile` (3 x 2048 doubles, followed by room for k
+// column indices), two stages in flight while one is summed; other team sizes
+// (the host emulation) take the plain loop.
 #if defined(__CUDA_ARCH__)
 __device__ __forceinline__ void lqm_cp_async8(void* sdst, const void* gsrc, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
@@ -437,7 +439,10 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
 #if defined(__CUDA_ARCH__)
   if (T.nt == 512 && tile != nullptr) {
     constexpr int BM = 128, BN = 128, BK = 8, STG = BK * BM + BK * BN, NS = 3;
-    const int tr = T.tid & 31, tc = T.tid >> 5;  // rows tr*4 .. +3, columns tc*8 .. +7
+    const int tr = T.tid & 31, tc = T.tid >> 5;  // rows 2tr, 2tr+1, 64+2tr, 65+2tr; columns tc*8 .. +7
+    int* cidx = (int*)(tile + NS * STG);         // the node's column indices, staged once
+    for (int p = T.tid; p < k; p += T.nt) cidx[p] = colnd[p];
+    team_sync();
     for (int r0 = 0; r0 < s; r0 += BM) {
       for (int c0 = 0; c0 < k; c0 += BN) {
         double acc[4][8];
@@ -454,7 +459,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
             const int e = T.tid + 512 * h;
             const int p = p0 + (e >> 7), r = r0 + (e & 127), cc = c0 + (e & 127);
             const bool oka = p < k && r < s, okb = p < k && cc < k;
-            lqm_cp_async8(As + e, oka ? (const void*)(Q + (lo + r) + (int64_t)colnd[p] * n) : (const void*)Q, oka);
+            lqm_cp_async8(As + e, oka ? (const void*)(Q + (lo + r) + (int64_t)cidx[p] * n) : (const void*)Q, oka);
             lqm_cp_async8(Bs + e, okb ? (const void*)(Ubn + cc + (int64_t)p * k) : (const void*)Ubn, okb);
           }
         };
@@ -472,8 +477,8 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
           const double* Bs = As + BK * BM;
 #pragma unroll
           for (int pp = 0; pp < BK; ++pp) {
-            const double2 x01 = *(const double2*)(As + pp * BM + tr * 4);
-            const double2 x23 = *(const double2*)(As + pp * BM + tr * 4 + 2);
+            const double2 x01 = *(const double2*)(As + pp * BM + tr * 2);
+            const double2 x23 = *(const double2*)(As + pp * BM + 64 + tr * 2);
             const double xa[4] = {x01.x, x01.y, x23.x, x23.y};
             double ya[8];
 #pragma unroll
@@ -494,7 +499,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
         for (int q = 0; q < 4; ++q)
 #pragma unroll
           for (int b = 0; b < 8; ++b) {
-            const int r = r0 + tr * 4 + q, cc = c0 + tc * 8 + b;
+            const int r = r0 + ((q < 2) ? tr * 2 + q : 64 + tr * 2 + (q - 2)), cc = c0 + tc * 8 + b;
             if (r < s && cc < k) Qt[(lo + r) + (int64_t)newpos[cc] * n] = acc[q][b];
           }
       }

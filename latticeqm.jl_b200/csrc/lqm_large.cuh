@@ -101,9 +101,11 @@ __global__ void __launch_bounds__(kBlkThreads) blk_t12_kernel(BlkArgs a, int j0,
 // (all k-points of the batch) with a kSymvStages-deep cp.async pipeline, so
 // that two tiles are in flight from HBM while a third is summed.
 constexpr int kSymvStages = 3;
+constexpr int kSymvThreads = 512;
 constexpr int kSymvLd = kSymvTB + 1;
 constexpr int kSymvStageC = kSymvTB * kSymvLd + 2 * kSymvTB;  // complex per stage: tile + v_R, v_C
-constexpr int kSymvPipeSmem = (kSymvStages * kSymvStageC + 2 * (kBlkThreads / kSymvTB) * kSymvTB) * 16;
+constexpr int kSymvPipeSmem = (kSymvStages * kSymvStageC + 2 * (kSymvThreads / kSymvTB) * kSymvTB) * 16;
+static_assert(kSymvPipeSmem <= 227 * 1024, "mat-vec pipeline exceeds shared memory");
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -133,8 +135,8 @@ __device__ __forceinline__ void symv_issue(const BlkArgs& a, int j, int m, int n
   const double2* v = A + (j + 1) + (int64_t)j * a.n;
   const int x0 = R * kSymvTB, y0 = C * kSymvTB;
 #pragma unroll
-  for (int h = 0; h < (kSymvTB * kSymvTB) / kBlkThreads; ++h) {
-    const int idx = threadIdx.x + h * kBlkThreads, rr = idx % kSymvTB, cc = idx / kSymvTB;
+  for (int h = 0; h < (kSymvTB * kSymvTB) / kSymvThreads; ++h) {
+    const int idx = threadIdx.x + h * kSymvThreads, rr = idx % kSymvTB, cc = idx / kSymvTB;
     const int x = x0 + rr, y = y0 + cc;
     const bool ok = x < m && y < m;
     cp_async16(st + rr + cc * kSymvLd, ok ? (const void*)(B + x + (int64_t)y * a.n) : (const void*)B, ok);
@@ -147,11 +149,11 @@ __device__ __forceinline__ void symv_issue(const BlkArgs& a, int j, int m, int n
 }
 
 // grid: persistent (about one CTA per SM), kSymvPipeSmem dynamic smem.
-__global__ void __launch_bounds__(kBlkThreads, 1) blk_symv_pipe_kernel(BlkArgs a, int j, int64_t nitems) {
+__global__ void __launch_bounds__(kSymvThreads, 1) blk_symv_pipe_kernel(BlkArgs a, int j, int64_t nitems) {
   extern __shared__ __align__(16) unsigned char smem[];
   double2* stg = (double2*)smem;
   double2* rd = stg + kSymvStages * kSymvStageC;           // [ng][TB] direct
-  constexpr int ng = kBlkThreads / kSymvTB;
+  constexpr int ng = kSymvThreads / kSymvTB;
   double2* rt = rd + ng * kSymvTB;                         // [ng][TB] transposed
   const int m = a.n - j - 1;
   const int nbk = (m + kSymvTB - 1) / kSymvTB;
@@ -182,24 +184,40 @@ __global__ void __launch_bounds__(kBlkThreads, 1) blk_symv_pipe_kernel(BlkArgs a
     symv_tile_rc((int)(it - b * ntiles), &R, &C);
     const bool diag = (R == C);
     {
+      // thread (q, g): direct product of row q and transposed product of column q
+      // over u = g, g + ng, ... (two interleaved accumulators each)
       const int q = threadIdx.x % kSymvTB, g = threadIdx.x / kSymvTB;
-      double2 ad = cmk(0.0, 0.0), at = cmk(0.0, 0.0);
-#pragma unroll 4
-      for (int u = g; u < kSymvTB; u += ng) {
-        // direct: row q, column u (lower part only on a diagonal tile, diagonal real)
-        double2 x = ts[q + u * kSymvLd];
-        if (diag) {
+      double2 ad0 = cmk(0.0, 0.0), ad1 = ad0, at0 = ad0, at1 = ad0;
+      if (!diag) {
+#pragma unroll
+        for (int h = 0; h < kSymvTB / ng; h += 2) {
+          const int u0 = g + h * ng, u1 = u0 + ng;
+          ad0 = cadd(ad0, cmul(ts[q + u0 * kSymvLd], vC[u0]));
+          at0 = cadd(at0, cmulc(ts[u0 + q * kSymvLd], vR[u0]));
+          ad1 = cadd(ad1, cmul(ts[q + u1 * kSymvLd], vC[u1]));
+          at1 = cadd(at1, cmulc(ts[u1 + q * kSymvLd], vR[u1]));
+        }
+      } else {
+        // lower part only: direct uses columns u <= q (diagonal real), transposed rows u > q
+#pragma unroll
+        for (int h = 0; h < kSymvTB / ng; ++h) {
+          const int u = g + h * ng;
+          double2 x = ts[q + u * kSymvLd];
           if (u > q) x = cmk(0.0, 0.0);
           else if (u == q) x.y = 0.0;
+          double2 y = ts[u + q * kSymvLd];
+          if (u <= q) y = cmk(0.0, 0.0);
+          if (h & 1) {
+            ad1 = cadd(ad1, cmul(x, vC[u]));
+            at1 = cadd(at1, cmulc(y, vR[u]));
+          } else {
+            ad0 = cadd(ad0, cmul(x, vC[u]));
+            at0 = cadd(at0, cmulc(y, vR[u]));
+          }
         }
-        ad = cadd(ad, cmul(x, vC[u]));
-        // transposed: row u, column q (strictly lower on a diagonal tile)
-        double2 y = ts[u + q * kSymvLd];
-        if (diag && u <= q) y = cmk(0.0, 0.0);
-        at = cadd(at, cmulc(y, vR[u]));
       }
-      rd[threadIdx.x] = ad;
-      rt[threadIdx.x] = at;
+      rd[threadIdx.x] = cadd(ad0, ad1);
+      rt[threadIdx.x] = cadd(at0, at1);
     }
     __syncthreads();
     if (threadIdx.x < kSymvTB) {
@@ -265,7 +283,8 @@ __host__ __device__ inline int64_t dc_large_slot_doubles(int n, bool vec) {
   return (vec ? 3 * nn : 4 * (int64_t)n + 4) + vecs;
 }
 
-constexpr int kDcTileSmem = 6144 * 8;  // dynamic: the merge GEMM's cp.async ring
+// dynamic shared memory: the merge GEMM's cp.async ring and the column indices of one merge
+__host__ __device__ inline int dc_tile_smem(int n) { return 6144 * 8 + ((n + 3) / 4) * 16; }
 
 __global__ void __launch_bounds__(kDcThreads) dc_large_kernel(DCLargeArgs a) {
   __shared__ double red[128];
