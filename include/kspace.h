@@ -50,9 +50,8 @@ const char* lqm_last_error(const lqm_ctx* ctx);
 /* Host-side wait limit for device work, seconds (default 600). */
 int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
 /* Eigensolver path selection: orders n >= n_min use the batched blocked path
- * (panel reduction + batched GEMMs); 0 (default) selects it only where the
- * one-CTA-per-k kernel's shared-memory plan does not fit (n above ~470).  No
- * reference counterpart (the reference always calls LAPACK zheevr). */
+ * (panel reduction + batched GEMMs); 0 (default) selects it from n = 128 on.
+ * No reference counterpart (the reference always calls LAPACK zheevr). */
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
 /* Milliseconds of device time of the last call's kernels (CUDA events). */
 int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);

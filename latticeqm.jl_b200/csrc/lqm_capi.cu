@@ -260,7 +260,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(48.0e9 / per_k)));
   B = std::min<int64_t>(B, 65535);
   const int64_t slotd = dc_large_slot_doubles(n, vec);
-  const int64_t G = std::min<int64_t>(B, (int64_t)ctx->num_sms);
+  const bool dc_small = n < kDcTileMin;  // no tiled merges: 128-thread CTAs, four per SM
+  const int64_t G = std::min<int64_t>(B, (int64_t)ctx->num_sms * (dc_small ? 4 : 1));
   double2* A = (double2*)ws_get(ctx, WS_LA, (size_t)B * nn * sizeof(double2));
   double2* Uw = (vec && !d_U) ? (double2*)ws_get(ctx, WS_LU, (size_t)B * nn * sizeof(double2)) : nullptr;
   double2* aux = (double2*)ws_get(ctx, WS_LAUX, (size_t)B * (auxk + n) * sizeof(double2));
@@ -278,7 +279,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   cublasHandle_t h = blas_handle(ctx);
   ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
      "smem attr");
-  ck(cudaFuncSetAttribute(dc_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dc_tile_smem(n)),
+  ck(cudaFuncSetAttribute(dc_large_kernel<kDcThreads, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          dc_tile_smem(n)),
      "smem attr");
   std::pair<cudaEvent_t, cudaEvent_t> evs{};
   if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
@@ -335,7 +337,10 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     da.n = n; da.nk = nbk; da.plan = plan; da.d = dd; da.e = ee; da.bands = d_bands + k0 * n;
     da.U = vec ? Ucur : nullptr; da.slots = slots; da.slot_doubles = slotd;
     da.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
-    dc_large_kernel<<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, dc_tile_smem(n), ctx->stream>>>(da);
+    if (dc_small)
+      dc_large_kernel<128, 4><<<(unsigned)std::min<int64_t>(G, nbk), 128, 0, ctx->stream>>>(da);
+    else
+      dc_large_kernel<kDcThreads, 1><<<(unsigned)std::min<int64_t>(G, nbk), kDcThreads, dc_tile_smem(n), ctx->stream>>>(da);
     ctx->launches++;
     ck(cudaGetLastError(), "divide-and-conquer launch");
     if (!vec) continue;
@@ -417,10 +422,14 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   ctx->launches++;
 }
 
-// The one-CTA kernel holds the vectors of one k-point in shared memory; beyond
-// that (or from ctx->blocked_min_n on) the blocked path runs.
+// Path choice: the blocked path from n = 128 on (measured on B200: 18% faster
+// than the one-CTA kernel's global-memory variant at n = 144, 21% slower at
+// n = 96), or from ctx->blocked_min_n when set, and always beyond the one-CTA
+// kernel's shared-memory plan.
+constexpr int kBlockedDefaultMinN = 128;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
-  if (ctx->blocked_min_n > 0 && n >= ctx->blocked_min_n) return true;
+  const int64_t nmin = ctx->blocked_min_n > 0 ? ctx->blocked_min_n : kBlockedDefaultMinN;
+  if (n >= nmin) return true;
   return eigh_smem_layout(n, nR, eigh_threads(n), 0).total > 225 * 1024;
 }
 

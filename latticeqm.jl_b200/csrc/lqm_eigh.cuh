@@ -262,10 +262,12 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
 // ---------------------------------------------------------------------------
 
 // Lane-group width for the secular roots of a merge with k non-deflated
-// values: about four terms per lane, at most a warp.
+// values: about twelve terms per lane, at most a warp.  Narrow groups keep
+// several roots per warp in flight and their sums need fewer shuffle levels;
+// the per-lane terms are independent divisions that pipeline.
 LQM_FN int secular_width(int k, int nl) {
   int w = 1;
-  while (w < nl && 4 * w < k) w <<= 1;
+  while (w < nl && 12 * w < k) w <<= 1;
   return w;
 }
 

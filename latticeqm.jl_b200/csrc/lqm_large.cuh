@@ -286,7 +286,11 @@ __host__ __device__ inline int64_t dc_large_slot_doubles(int n, bool vec) {
 // dynamic shared memory: the merge GEMM's cp.async ring and the column indices of one merge
 __host__ __device__ inline int dc_tile_smem(int n) { return 6144 * 8 + ((n + 3) / 4) * 16; }
 
-__global__ void __launch_bounds__(kDcThreads) dc_large_kernel(DCLargeArgs a) {
+// NT = 512 (one CTA per SM) for orders with tiled merges; below kDcTileMin the
+// merges are small and latency-bound, and NT = 128 with four CTAs per SM keeps
+// four k-points in flight per SM.
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) dc_large_kernel(DCLargeArgs a) {
   __shared__ double red[128];
   extern __shared__ __align__(16) double tile[];
   const Team T = make_team();

@@ -84,8 +84,11 @@ def test_batch_models_bands(lqm, ctx):
         assert rel_band_err(b, oracle_bands(h, ks)) <= BAND_TOL, name
 
 
-def test_large_n_global_scratch_path(lqm, ctx):
-    # n = 148 keeps the Householder matrix in global scratch (does not fit shared memory)
+def test_large_n_global_scratch_path(lqm):
+    # n = 148 on the one-CTA kernel (the default context takes the blocked path from
+    # n = 128 on): the Householder matrix lives in global scratch (does not fit shared memory)
+    ctx = lqm.Context(0, timeout=600)
+    ctx.set_blocked_min_n(10 ** 9)
     h = M.graphene(L.honeycomb_twisted(3), tz=0.32)
     ks = np.array([[0.0, 1 / 3, 0.21], [0.0, -1 / 3, 0.55]])
     b, U = lqm.bandmatrix(h, ks, want_vectors=True, ctx=ctx)
