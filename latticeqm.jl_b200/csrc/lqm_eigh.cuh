@@ -840,8 +840,10 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 // in blocks of 8 reflectors with the compact WY form (LAPACK zlarft, forward,
 // column-wise):  H_{j0} ... H_{j0+7} = I - V T V^H,  U_sub -= V (T (V^H U_sub)).
 // Reflector j is R[j+1.., j] with v0 = 1.  V (zero-padded, ld n), T and the
-// Gram matrix G = V^H V live in S.pbuf; one thread per column of U computes
-// V^H u, T (V^H u) and the update with 8 independent accumulators.
+// Gram matrix G = V^H V live in S.pbuf.  Each column of U belongs to a group
+// of G lanes (G = 4 for n = 96 on 512 threads) that split its rows: partial
+// V^H u over the group's rows, a group sum, T (V^H u), and the update of the
+// group's rows, with 8 independent accumulators per lane.
 // ---------------------------------------------------------------------------
 LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int ldr, EighVec& S, double2* U,
                                    int ldu) {
@@ -892,15 +894,30 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
       for (int i = 0; i < NB; ++i) Ts[l + i * NB] = trow[i];
     }
     team_sync();
-    for (int c = T.tid; c < n; c += T.nt) {
-      double2* Uc = U + (j0 + 1) + (int64_t)c * ldu;
+    // lanes per column: the largest power of two <= 8 with n * G <= nt (within a warp)
+    int G = 1;
+    while (G < 8 && 2 * G <= T.nl && n * (2 * G) <= T.nt) G *= 2;
+    const int ngr = T.nt / G;                 // column groups
+    const int g = T.tid % G;
+    const int rounds = (n + ngr - 1) / ngr;   // uniform trip count (every lane takes part in the sums)
+    for (int rd = 0; rd < rounds; ++rd) {
+      const int c = rd * ngr + T.tid / G;
+      const bool act = c < n;
+      double2* Uc = U + (j0 + 1) + (int64_t)(act ? c : 0) * ldu;
       double2 w[NB];
 #pragma unroll
       for (int i = 0; i < NB; ++i) w[i] = cmk(0.0, 0.0);
-      for (int r = 0; r < m; ++r) {
-        const double2 u = Uc[r];
+      if (act) {
+        for (int r = g; r < m; r += G) {
+          const double2 u = Uc[r];
 #pragma unroll
-        for (int i = 0; i < NB; ++i) w[i] = cadd(w[i], cmulc(Vs[r + (int64_t)i * n], u));
+          for (int i = 0; i < NB; ++i) w[i] = cadd(w[i], cmulc(Vs[r + (int64_t)i * n], u));
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < NB; ++i) {
+        w[i].x = group_sum_bcast(w[i].x, G);
+        w[i].y = group_sum_bcast(w[i].y, G);
       }
       double2 wp[NB];
 #pragma unroll
@@ -911,11 +928,13 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
           if (l >= i) acc = cadd(acc, cmul(Ts[i + l * NB], w[l]));
         wp[i] = acc;
       }
-      for (int r = 0; r < m; ++r) {
-        double2 u = Uc[r];
+      if (act) {
+        for (int r = g; r < m; r += G) {
+          double2 u = Uc[r];
 #pragma unroll
-        for (int i = 0; i < NB; ++i) u = csub(u, cmul(Vs[r + (int64_t)i * n], wp[i]));
-        Uc[r] = u;
+          for (int i = 0; i < NB; ++i) u = csub(u, cmul(Vs[r + (int64_t)i * n], wp[i]));
+          Uc[r] = u;
+        }
       }
     }
     team_sync();
