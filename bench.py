@@ -336,6 +336,23 @@ def profile_case(Q, ctx, h, torch, dev, np):
     print(json.dumps({"profile_case": "n=96 batch model, 2048 k", "kernel_ms": ctx.last_kernel_ms()}))
 
 
+def profile_case_tbg(Q, ctx, M, case):
+    """Small cases of the blocked path for profilers: one call on the twisted
+    bilayer m=10 (n=1324) over the first nk points of the 24x24 grid."""
+    from lqm_workloads import lattice as LL
+    kind = "bands" if case.startswith("tbg10-bands") else "density"
+    nk = int(case.rsplit("bands", 1)[-1]) if kind == "bands" else int(case.rsplit("density", 1)[-1])
+    _, h = M.tbg_slater_koster(10)
+    ks = LL.regulargrid(24 * 24)[:, :nk]
+    t0 = time.perf_counter()
+    if kind == "bands":
+        Q.bandmatrix(h, ks, ctx=ctx)
+    else:
+        rho = {R: None for R in h}
+        Q.getdensitymatrix(rho, h, ks, mu=MU, T=TEMP, ctx=ctx)
+    print(json.dumps({"profile_case": case, "kernel_ms": ctx.last_kernel_ms(), "wall_s": time.perf_counter() - t0}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,8 +362,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (n=144, 1324, 2884 and the adjoint)")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="one fused call on the n=96 model over 2048 k-points (small case for ncu)")
+    ap.add_argument("--profile-case", nargs="?", const="n96", default=None,
+                    choices=["n96", "tbg10-bands576", "tbg10-density142", "tbg10-density16"],
+                    help="one call of a small profiling case: n96 = the fused bench call on the n=96 model "
+                         "over 2048 k; tbg10-* = bands or density of the n=1324 twisted bilayer over the "
+                         "first 576 / 142 / 16 points of the 24x24 grid")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
@@ -372,8 +392,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     models = M.batch_models()
     ctx = Q.Context(local, timeout=900)
-    if args.profile_case:
+    if args.profile_case == "n96":
         return profile_case(Q, ctx, models[2][1], torch, dev, np)
+    if args.profile_case:
+        return profile_case_tbg(Q, ctx, M, args.profile_case)
 
     # ---- device-resident inputs ----
     ks_np = kgrid(rank, world)

@@ -531,7 +531,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
 LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
                               unsigned long long* sub = nullptr, bool vec = true, double* Ub = nullptr,
                               int tile_min = 1 << 30) {
-  double* ubuf = (double*)S.pbuf;  // per-warp secular eigenvector (n doubles each)
+  double* ubuf = (double*)S.pbuf;  // per-warp secular eigenvectors (2n doubles each)
   double* QF = Q;
   double* QL = Q + n;
   double* FT = Q + 2 * n;
@@ -776,23 +776,29 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
                      S.tile);
       }
     }
-    for (int c = T.wid; c < n && vec && !tiled; c += T.nw) {
+    // Columns in pairs (2t, 2t+1) by warp: when both are non-deflated columns
+    // of the same merge, every Q element loaded serves both (the sums over p
+    // keep their order, so the values are those of the one-column form).
+    auto form_u = [&](int c, int lo, int it, int k, double* ub) {
+      const double* dl = S.dl + lo;
+      const double lorg = dl[S.org[lo + it]], tq = S.troot[lo + it];
+      double ss = 0.0;
+      for (int p = T.lane; p < k; p += T.nl) {
+        const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
+        ub[p] = u;
+        ss += u * u;
+      }
+      const double sc = 1.0 / sqrt(warp_sum_bcast(ss));
+      for (int p = T.lane; p < k; p += T.nl) ub[p] *= sc;
+    };
+    auto one_col = [&](int c) {
       const int nd = own[c];
-      if (nd < 0) continue;
+      if (nd < 0) return;
       const int lo = P.lo[nd], hi = P.hi[nd], it = c - lo, k = S.nk[nd];
       double* dst = Qt + (int64_t)S.newpos[c] * n;
       if (it < k) {
-        double* ub = ubuf + (int64_t)T.wid * n;
-        const double* dl = S.dl + lo;
-        const double lorg = dl[S.org[lo + it]], tq = S.troot[lo + it];
-        double ss = 0.0;
-        for (int p = T.lane; p < k; p += T.nl) {
-          const double u = S.zhat[lo + p] / ((dl[p] - lorg) - tq);
-          ub[p] = u;
-          ss += u * u;
-        }
-        const double sc = 1.0 / sqrt(warp_sum_bcast(ss));
-        for (int p = T.lane; p < k; p += T.nl) ub[p] *= sc;
+        double* ub = ubuf + (int64_t)T.wid * 2 * n;
+        form_u(c, lo, it, k, ub);
         team_syncwarp();
         for (int r0 = lo + T.lane; r0 < hi; r0 += 3 * T.nl) {
           const int r1 = r0 + T.nl, r2 = r0 + 2 * T.nl;
@@ -814,6 +820,47 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
         const double* src = Q + (int64_t)S.dcol[lo + it - k] * n;
         for (int r = lo + T.lane; r < hi; r += T.nl) dst[r] = src[r];
       }
+    };
+    for (int t = T.wid; 2 * t < n && vec && !tiled; t += T.nw) {
+      const int ca = 2 * t, cb = 2 * t + 1;
+      const int nda = own[ca], ndb = (cb < n) ? own[cb] : -1;
+      bool pair = false;
+      if (nda >= 0 && ndb == nda) {
+        const int lo = P.lo[nda], k = S.nk[nda];
+        pair = (cb - lo) < k;  // ca < cb, so both are non-deflated
+      }
+      if (!pair) {
+        one_col(ca);
+        if (cb < n) one_col(cb);
+        continue;
+      }
+      const int lo = P.lo[nda], hi = P.hi[nda], k = S.nk[nda];
+      double* ua = ubuf + (int64_t)T.wid * 2 * n;
+      double* ubb = ua + n;
+      form_u(ca, lo, ca - lo, k, ua);
+      form_u(cb, lo, cb - lo, k, ubb);
+      team_syncwarp();
+      double* da = Qt + (int64_t)S.newpos[ca] * n;
+      double* db = Qt + (int64_t)S.newpos[cb] * n;
+      for (int r0 = lo + T.lane; r0 < hi; r0 += 3 * T.nl) {
+        const int r1 = r0 + T.nl, r2 = r0 + 2 * T.nl;
+        const bool h1 = r1 < hi, h2 = r2 < hi;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+        for (int p = 0; p < k; ++p) {
+          const double* qc = Q + (int64_t)S.colnd[lo + p] * n;
+          const double u = ua[p], v = ubb[p];
+          const double q0 = qc[r0];
+          a0 += q0 * u;
+          b0 += q0 * v;
+          if (h1) { const double q1 = qc[r1]; a1 += q1 * u; b1 += q1 * v; }
+          if (h2) { const double q2 = qc[r2]; a2 += q2 * u; b2 += q2 * v; }
+        }
+        da[r0] = a0;
+        db[r0] = b0;
+        if (h1) { da[r1] = a1; db[r1] = b1; }
+        if (h2) { da[r2] = a2; db[r2] = b2; }
+      }
+      team_syncwarp();
     }
     team_sync();
     LQM_SUBTICK(6);

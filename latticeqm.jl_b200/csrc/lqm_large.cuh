@@ -279,7 +279,7 @@ struct DCLargeArgs {
 
 __host__ __device__ inline int64_t dc_large_slot_doubles(int n, bool vec) {
   const int64_t nn = (int64_t)n * n;
-  const int64_t vecs = 13 * (int64_t)n + 8 + (10 * (int64_t)n + 1) / 2 + 1 + (int64_t)(kDcThreads / 32) * n + 2;
+  const int64_t vecs = 13 * (int64_t)n + 8 + (10 * (int64_t)n + 1) / 2 + 1 + 2 * (int64_t)(kDcThreads / 32) * n + 2;
   return (vec ? 3 * nn : 4 * (int64_t)n + 4) + vecs;
 }
 
