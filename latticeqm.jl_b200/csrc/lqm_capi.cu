@@ -192,11 +192,17 @@ void check_hops(const lqm_hops* H) {
   if (!H || !H->blocks) fail(LQM_EINVAL, "null hops");
 }
 
-int eigh_threads(int n) { return n <= 16 ? 32 : (n <= 32 ? 64 : (n < 64 ? 128 : 512)); }
+// Threads of the one-CTA eigensolver for n >= 64 (a compile-time choice; 384
+// measured fastest at n = 96 on B200: 168 registers per thread instead of the
+// 128 that 512 threads allow).
+#ifndef LQM_EIGH_NT_LARGE
+#define LQM_EIGH_NT_LARGE 384
+#endif
+int eigh_threads(int n) { return n <= 16 ? 32 : (n <= 32 ? 64 : (n < 64 ? 128 : LQM_EIGH_NT_LARGE)); }
 
 // eigh_kernel instantiation for a block size (512 threads from n = 64 on).
 using EighFn = void (*)(EighArgs);
-EighFn eigh_fn(int nt) { return nt > 256 ? &eigh_kernel<512> : &eigh_kernel<256>; }
+EighFn eigh_fn(int nt) { return nt > 384 ? &eigh_kernel<512> : (nt > 256 ? &eigh_kernel<384> : &eigh_kernel<256>); }
 
 void timer_start(lqm_ctx* ctx) { ck(cudaEventRecord(ctx->ev0, ctx->stream), "event"); }
 void timer_stop(lqm_ctx* ctx) {
