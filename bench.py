@@ -222,7 +222,7 @@ def large_configs(Q, ctx, M, pool, cores):
         "grid": "48x48", "bands_kpts_per_s": ks1.shape[1] / dv, "bands_wall_kpts_per_s": ks1.shape[1] / wl,
         "rho_kpts_per_s": ks1.shape[1] / dd, "rho_wall_kpts_per_s": ks1.shape[1] / wd,
         "cpu_rho_kpts_per_s": cpu_density_rate(h1, pool, cores, 8) if pool else None,
-        "path": "one-CTA-per-k eigensolver (global-memory scratch)"}
+        "path": "batched blocked eigensolver (n >= 128)"}
     # twisted bilayer m=10, n = 1324: 24 x 24 grid (bands + rho) and a 400-point k-path (bands)
     lat3, h3 = M.tbg_slater_koster(10)
     ks3 = LL.regulargrid(24 * 24)
