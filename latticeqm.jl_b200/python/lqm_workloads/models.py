@@ -260,3 +260,30 @@ def tbg_slater_koster(N, **kw):
                   dmax=3 * math.sqrt(3.0), tmin=1e-5)
     params.update(kw)
     return lat, graphene(lat, **params)
+
+
+def screened_coulomb_v(lat, V0=1.4 * math.sqrt(3.0), lam=10.0 * math.sqrt(3.0), onsite=1.4, cellrange=1):
+    """Density-density interaction v_R[i, j] = V0 exp(-d/lam) / d with d = |r_i + R - r_j|
+    (``Hops(lat, V; cellrange)``, gethops.jl:33-36, with V(r) = V0 e^{-r/lam}/r), the
+    divergent d = 0 entries replaced by ``onsite``.  Defaults: the large twisted-bilayer
+    workload, V0 = 1.4 eV * a and lam = 10 a with a = sqrt(3) (graphene lattice constant
+    in units of the nearest-neighbour distance) and the cap V0 / a = 1.4 eV on site."""
+    Rpos = lat.allpositions()
+    v = {}
+    for dL, da in neighbor_dict(lat, cellrange).items():
+        R1 = Rpos + da[:, None]
+        d = R1[:3, :, None] - Rpos[:3, None, :]
+        D = np.sqrt((d * d).sum(axis=0))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            M = np.where(D > 1e-9, V0 * np.exp(-D / lam) / D, onsite)
+        v[dL] = M.astype(complex)
+        if any(x != 0 for x in dL):
+            v[tuple(-x for x in dL)] = v[dL].T.copy()
+    return v
+
+
+def tbg_screened_hf(N):
+    """Twisted bilayer (m=N, r=1) Slater-Koster hopping with the screened Coulomb
+    interaction of the large Hartree-Fock workload: (lat, h, v)."""
+    lat, h = tbg_slater_koster(N)
+    return lat, h, screened_coulomb_v(lat)
