@@ -191,6 +191,10 @@ def cpu_density_rate(h, pool, cores, per_core, seed=0):
     return done / (time.perf_counter() - t0)
 
 
+def ctx_device(ctx):
+    return 0 if not hasattr(ctx, "device") else ctx.device
+
+
 def large_configs(Q, ctx, M, pool, cores):
     """The other configurations of the hot path, one call each after a warm-up call,
     through the host-pointer C-ABI: device time of the call's kernels (CUDA events
@@ -235,14 +239,39 @@ def large_configs(Q, ctx, M, pool, cores):
         "kpath_bands_wall_kpts_per_s": kp3.shape[1] / wb,
         "cpu_rho_kpts_per_s": cpu_density_rate(h3, pool, cores, 1) if pool else None,
         "path": "batched blocked eigensolver"}
-    # twisted bilayer m=15, n = 2884: one eigen + rho pass over the 12 x 12 grid (the
-    # k-space work of one SCF iteration)
-    _, h5 = M.tbg_slater_koster(15)
+    # twisted bilayer m=15, n = 2884: one eigen + rho pass over the 12 x 12 grid, then
+    # the Hartree-Fock SCF with the screened Coulomb interaction (3 iterations, the
+    # 2nd and 3rd replayed from a captured CUDA graph), on a context of its own so that
+    # its ~80 GB of work buffers are released afterwards
+    ctx5 = Q.Context(ctx_device(ctx), timeout=1800)
+    lat5, h5, v5 = M.tbg_screened_hf(15)
+    n5 = h5[(0, 0)].shape[0]
     ks5 = LL.regulargrid(12 * 12)
-    dd, wd = timed(density_call(h5, ks5))
+    rho5 = {R: None for R in h5}
+    Q.getdensitymatrix(rho5, h5, ks5, mu=MU, T=TEMP, ctx=ctx5)
+    t0 = time.perf_counter()
+    Q.getdensitymatrix(rho5, h5, ks5, mu=MU, T=TEMP, ctx=ctx5)
+    wd = time.perf_counter() - t0
+    dd = ctx5.last_kernel_ms() / 1e3
+    rng = np.random.default_rng(11)
+    X = rng.normal(size=(n5, n5)) * 0.01
+    r0 = {R: np.zeros((n5, n5), complex) for R in v5}
+    r0[(0, 0)] = 0.5 * np.eye(n5) + (X + X.T)
+    iters = 3
+    t0 = time.perf_counter()
+    res = Q.solvehartreefock(h5, v5, r0, 0.5, ks5, T=0.05, beta=0.3, tol=0.0, iterations=iters, ctx=ctx5)
+    t_scf = time.perf_counter() - t0
     out["tbg_m15_n2884"] = {"grid": "12x12", "rho_pass_s": dd, "rho_pass_wall_s": wd,
                             "rho_kpts_per_s": ks5.shape[1] / dd, "path": "batched blocked eigensolver",
+                            "scf": {"interaction": "screened Coulomb V0 e^{-r/lam}/r, V0 = 1.4 eV a, lam = 10 a, "
+                                                   "onsite 1.4 eV, 9 keys", "iterations": iters,
+                                    "s_per_iter": t_scf / iters,
+                                    "device_s_per_iter": ctx5.last_kernel_ms() / 1e3 / iters,
+                                    "residual": res.residual,
+                                    "note": "wall time of lqm_scf_hf incl. the first (uncaptured) iteration "
+                                            "and the h/v/rho uploads"},
                             "cpu": "not sampled (about a minute per k-point and core)"}
+    ctx5.close()
     # adjoint: density-response VJP on the triangular Hubbard model (n = 72, 36 x 36)
     _, h4, _ = M.triangular_hubbard(L_super=6)
     ks4 = LL.regulargrid(36 * 36)

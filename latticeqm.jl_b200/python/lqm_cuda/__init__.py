@@ -119,6 +119,7 @@ class Context:
         if st != LQM_OK:
             raise LQMError(st, f"cannot create a context on CUDA device {device}")
         self._h = h
+        self.device = int(device)
         if timeout is not None:
             self.check(_lib.lqm_ctx_set_timeout(self._h, float(timeout)))
 
