@@ -170,6 +170,15 @@ int lqm_scf_hf(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, c
 int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32_t d, const int64_t* d_keys,
                            const double* d_blocks, int64_t nk, const double* d_ks, double* d_bands, double* d_U);
 
+/* bandmatrix(H, ks, projectors...) with band expectation values
+ * (src/modules/Spectrum/bands.jl:52-60,107-112,164-227): bands (n x nk) and
+ * obs[i + n*(j + nk*p)] = Re <u_i(k_j)| P_p(k_j) |u_i(k_j)> for the nproj
+ * operators P_p(k) = sum_R P_p,R e^{+i2pi k.R} (device Hops of order n; a
+ * k-independent matrix is a Hops with the single key 0).  nproj = 0 gives
+ * the bands only. */
+int lqm_bandmatrix_obs(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t nproj,
+                       const lqm_hops* const* P, double* bands, double* obs);
+
 /* ---- Reverse-mode derivatives (no reference counterpart: the reference has
  * no derivatives; the forward maps are lqm_densitymatrix and lqm_bandmatrix).
  *

@@ -22,6 +22,7 @@ module LatticeQMCUDA
 using LatticeQM
 import LatticeQM.Parallel
 import LatticeQM.TightBinding: Hops
+import LatticeQM.Spectrum
 import SparseArrays: SparseMatrixCSC
 
 const LIB = Ref{String}(joinpath(@__DIR__, "..", "lib", "libkspace.so"))
@@ -110,6 +111,43 @@ function cuda_bandmatrix(H, ks::AbstractMatrix{Float64}, exec::CudaExec; vectors
         ctx.ptr, dh.ptr, nk, Matrix{Float64}(ks), vectors, precision_code(exec), bands,
         vectors ? U : Ptr{ComplexF64}(C_NULL)))
     vectors ? (bands, U) : bands
+end
+
+"""
+    cuda_bandmatrix_obs(H, ks, projectors, exec) -> (bands, obs)
+
+`bandmatrix(H, ks, projectors...)` (Spectrum/bands.jl:164-227) with the band
+expectation values obs[i, j, p] = Re ⟨u_i(k_j)| O_p(k_j) |u_i(k_j)⟩
+(`lqm_bandmatrix_obs`).  Each projector is an `ExpvalMap` whose operand is a
+matrix (k-independent) or a Hops (Bloch-summed at each k); other callables
+cannot run on the device and throw.
+"""
+function cuda_bandmatrix_obs(H, ks::AbstractMatrix{Float64}, projectors, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    d = length(first(keys(H)))
+    dps = DeviceHops[]
+    for P in projectors
+        op = P isa Spectrum.ExpvalMap ? P.op : P
+        if op isa AbstractMatrix
+            push!(dps, upload(ctx, Dict(zeros(Int, d) => Matrix{ComplexF64}(op))))
+        elseif op isa Hops || op isa AbstractDict
+            push!(dps, upload(ctx, op))
+        else
+            throw(ArgumentError("projector of type $(typeof(op)) cannot run on :cuda (use a matrix or Hops)"))
+        end
+    end
+    nk = size(ks, 2)
+    bands = zeros(Float64, n, nk)
+    obs = zeros(Float64, n, nk, length(dps))
+    ptrs = Ptr{Cvoid}[p.ptr for p in dps]
+    GC.@preserve dps begin
+        check(ctx, ccall((:lqm_bandmatrix_obs, LIB[]), Cint,
+            (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Ptr{Ptr{Cvoid}}, Ptr{Float64}, Ptr{Float64}),
+            ctx.ptr, dh.ptr, nk, Matrix{Float64}(ks), length(dps), ptrs, bands, obs))
+    end
+    bands, obs
 end
 
 """`getdensitymatrix!(ρs, H, ks, kweights, μ; T)` on the device; returns the band energy."""

@@ -39,6 +39,7 @@ EXPORTS = [
     "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
+    "lqm_bandmatrix_obs",
 ]
 
 
@@ -85,6 +86,7 @@ _SIG = {
     "lqm_ctx_stats": [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     "lqm_densitymatrix_vjp": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, _P],
     "lqm_bands_vjp": [_P, _P, _I64, _P, _P, _P],
+    "lqm_bandmatrix_obs": [_P, _P, _I64, _P, _I64, _P, _P, _P],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -266,10 +268,42 @@ def bandmatrix(H, ks, multimode="cuda", want_vectors=False, precision=0, ctx=Non
 BandData = namedtuple("BandData", ["bands", "obs", "path"])
 
 
-def getbands(H, ks, multimode="cuda", ctx=None):
-    """``getbands(H, ks)`` -> BandData(bands, obs, path) (no projectors)."""
-    bands, _ = bandmatrix(H, ks, multimode=multimode, ctx=ctx)
-    return BandData(bands, np.zeros(bands.shape + (0,)), ks)
+def _projector_hops(op, n):
+    """ExpvalMap operand (bands.jl:52-60) as Hops: a matrix -> {0: matrix}; a dict Hops as is."""
+    if isinstance(op, dict):
+        return op
+    M = np.asarray(op, dtype=np.complex128)
+    if M.shape != (n, n):
+        raise ValueError(f"projector must be an {n} x {n} matrix or a Hops dict")
+    return {(0, 0): M}
+
+
+def bandmatrix_obs(H, ks, projectors, multimode="cuda", ctx=None):
+    """``bandmatrix(H, ks, projectors...)``: bands (n, nk) and obs (n, nk, nproj) with
+    obs[i, j, p] = Re <u_i(k_j)| P_p(k_j) |u_i(k_j)> (``lqm_bandmatrix_obs``)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    nk = ks.shape[1]
+    Pd = [DeviceHops(_projector_hops(op, Hd.n), ctx) for op in projectors]
+    arr = (_P * max(1, len(Pd)))(*[p.handle for p in Pd])
+    bands = np.zeros((Hd.n, nk), order="F")
+    obs = np.zeros((Hd.n, nk, len(Pd)), order="F")
+    ctx.check(_lib.lqm_bandmatrix_obs(ctx.handle, Hd.handle, nk, _ptr(ks), len(Pd), arr, _ptr(bands),
+                                      _ptr(obs) if Pd else None))
+    return bands, obs
+
+
+def getbands(H, ks, projectors=(), multimode="cuda", ctx=None):
+    """``getbands(H, ks[, projectors])`` -> BandData(bands, obs, path)."""
+    if projectors is None or (not isinstance(projectors, (list, tuple))):
+        projectors = [] if projectors is None else [projectors]
+    if len(projectors) == 0:
+        bands, _ = bandmatrix(H, ks, multimode=multimode, ctx=ctx)
+        return BandData(bands, np.zeros(bands.shape + (0,)), ks)
+    bands, obs = bandmatrix_obs(H, ks, projectors, multimode=multimode, ctx=ctx)
+    return BandData(bands, obs, ks)
 
 
 def getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, multimode="cuda", precision=0,

@@ -45,6 +45,24 @@ def bandmatrix(h, ks, vectors=False):
     return bands, U
 
 
+def bandmatrix_obs(h, ks, projectors):
+    """bands (n, nk) and obs (n, nk, nproj): obs[i, j, p] = Re <u_i| O_p(k_j) |u_i>;
+    Spectrum/bands.jl:52-60 (ExpvalMap: a matrix, or a k-dependent operator, here a
+    Hops dict Bloch-summed like H), :107-112 (compute_bandexpvals!), :212-227."""
+    n = next(iter(h.values())).shape[0]
+    nk = ks.shape[1]
+    bands = np.zeros((n, nk))
+    obs = np.zeros((n, nk, len(projectors)))
+    for j in range(nk):
+        k = ks[:, j]
+        e, U = eigh_upper(fouriersum(h, k), True)
+        bands[:, j] = e
+        for p, op in enumerate(projectors):
+            O = fouriersum(op, k) if isinstance(op, dict) else np.asarray(op)
+            obs[:, j, p] = np.real(np.einsum("ri,rs,si->i", U.conj(), O, U))
+    return bands, obs
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

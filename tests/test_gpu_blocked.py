@@ -157,3 +157,33 @@ def test_screened_coulomb_hf_blocked_path_matches_oracle(lqm, ctx):
     assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in rho0) <= RHO_TOL
     assert abs(res.energy - E_ref) <= 1e-9 * max(1.0, abs(E_ref))
     assert abs(res.mf.mu - hf_ref.mu) <= 1e-9
+
+
+@pytest.mark.parametrize("blocked", [False, True], ids=["default", "blocked"])
+def test_band_expectation_values_match_oracle(lqm, ctx, bctx, blocked):
+    """bandmatrix(H, ks, projectors...) through lqm_bandmatrix_obs: a k-independent
+    random Hermitian matrix, H itself (k-dependent Hops: obs = bands) and the identity."""
+    c = bctx if blocked else ctx
+    rng = np.random.default_rng(13)
+    cases = M.batch_models() + [("honeycomb144", M.honeycomb_disorder()[1])]
+    for name, h in cases:
+        n = h[(0, 0)].shape[0]
+        X = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+        P = X + X.conj().T
+        ks = rng.random((2, 7))
+        res = lqm.getbands(h, ks, [P, h, np.eye(n)], ctx=c)
+        bref, oref = K.bandmatrix_obs(h, ks, [P, h, np.eye(n)])
+        scale = max(np.max(bref) - np.min(bref), 1.0)
+        assert np.max(np.abs(res.bands - bref)) <= BAND_TOL * scale, name
+        # within a degenerate group (spin pairs) only the sum of <u|P|u> is basis-independent
+        for j in range(ks.shape[1]):
+            b_ = bref[:, j]
+            start = 0
+            for i in range(1, n + 1):
+                if i == n or b_[i] - b_[i - 1] > 1e-8 * scale:
+                    g = slice(start, i)
+                    d = abs(res.obs[g, j, 0].sum() - oref[g, j, 0].sum())
+                    assert d <= 1e-10 * np.max(np.abs(P)) * n, (name, j, start, i)
+                    start = i
+        assert np.max(np.abs(res.obs[:, :, 1] - res.bands)) <= BAND_TOL * scale, name
+        assert np.max(np.abs(res.obs[:, :, 2] - 1.0)) <= 1e-12, name

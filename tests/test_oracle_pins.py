@@ -256,3 +256,20 @@ def test_grand_potential_gradient_is_rho():
     step = 1e-6
     fd = (omega({R: h[R] + step * dH[R] for R in h}) - omega({R: h[R] - step * dH[R] for R in h})) / (2 * step)
     assert abs(fd - AD.pairing(rho, dH)) <= 1e-6 * max(1.0, abs(fd))
+
+
+def test_band_expectation_values_known_answers():
+    """bandmatrix(H, ks, projectors...) (bands.jl:52-60,107-112): with H itself as the
+    projector the expectation values are the bands, with the identity they are 1, and
+    graphene's sublattice polarisation vanishes away from the Dirac points."""
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    ks = L.kpath(lat, 64)
+    n = h[(0, 0)].shape[0]
+    sz = np.diag([1.0, -1.0]).astype(complex)
+    bands, obs = K.bandmatrix_obs(h, ks, [h, np.eye(n), sz])
+    assert np.max(np.abs(obs[:, :, 0] - bands)) < 1e-13
+    assert np.max(np.abs(obs[:, :, 1] - 1.0)) < 1e-13
+    gap = bands[1] - bands[0]
+    away = gap > 1e-3
+    assert np.max(np.abs(obs[:, away, 2])) < 1e-12
