@@ -53,6 +53,11 @@ int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
  * (panel reduction + batched GEMMs); 0 (default) selects it from n = 128 on.
  * No reference counterpart (the reference always calls LAPACK zheevr). */
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
+/* SCF acceleration of lqm_scf_hf on this context: 0 (default) linear damped
+ * mixing, 1..8 Anderson (Type-II) acceleration with that history depth
+ * (src/modules/Meanfield/fixedpoint.jl:39-194,201-231: acceleration=:anderson,
+ * anderson_depth), including its Hermitian projection of each iterate. */
+int lqm_ctx_set_scf_acceleration(lqm_ctx* ctx, int anderson_depth);
 /* Milliseconds of device time of the last call's kernels (CUDA events). */
 int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
 

@@ -62,7 +62,8 @@ struct lqm_ctx {
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
   cublasHandle_t blas = nullptr;          // batched GEMMs of the blocked large-n path
-  int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: only beyond the one-CTA plan)
+  int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: the default switch)
+  int scf_anderson_depth = 0;             // SCF acceleration: 0 linear mixing, > 0 Anderson history depth
 };
 
 struct lqm_hops {
@@ -160,9 +161,9 @@ void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND
 };
-static_assert(WS_SCFY < 32, "workspace slots");
+static_assert(WS_AND < 32, "workspace slots");
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
 const DCPlan& get_plan(lqm_ctx* ctx, int n) {
@@ -644,6 +645,12 @@ int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds) {
   return LQM_OK;
 }
 
+int lqm_ctx_set_scf_acceleration(lqm_ctx* ctx, int anderson_depth) {
+  if (!ctx || anderson_depth < 0 || anderson_depth > 8) return LQM_EINVAL;  // kAndMaxDepth (lqm_anderson.inc)
+  ctx->scf_anderson_depth = anderson_depth;
+  return LQM_OK;
+}
+
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min) {
   if (!ctx || n_min < 0) return LQM_EINVAL;
   ctx->blocked_min_n = n_min;
@@ -978,6 +985,7 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 
 }  // extern "C"
 
+#include "lqm_anderson.inc"
 #include "lqm_scf.inc"
 #include "lqm_adjoint.inc"
 #include "lqm_obs.inc"

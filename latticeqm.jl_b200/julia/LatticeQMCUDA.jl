@@ -210,8 +210,12 @@ end
 """Device-resident `solvehartreefock` with linear mixing; returns (ρ, ϵ_GS, info, converged, residual)."""
 function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractMatrix{Float64}, exec::CudaExec;
                                T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
-                               log_callback=nothing)
+                               log_callback=nothing, acceleration::Symbol=:linear, anderson_depth::Int=5)
     ctx = context(exec.device)
+    acceleration in (:linear, :anderson) ||
+        throw(ArgumentError("acceleration must be :linear or :anderson, got $(acceleration)"))
+    depth = acceleration === :anderson ? anderson_depth : 0
+    check(ctx, ccall((:lqm_ctx_set_scf_acceleration, LIB[]), Cint, (Ptr{Cvoid}, Cint), ctx.ptr, depth))
     dh = upload(ctx, h)
     dv = upload(ctx, v)
     Lk = collect(keys(ρ_init))

@@ -39,7 +39,7 @@ EXPORTS = [
     "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
-    "lqm_bandmatrix_obs",
+    "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration",
 ]
 
 
@@ -87,6 +87,7 @@ _SIG = {
     "lqm_densitymatrix_vjp": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, _P],
     "lqm_bands_vjp": [_P, _P, _I64, _P, _P, _P],
     "lqm_bandmatrix_obs": [_P, _P, _I64, _P, _I64, _P, _P, _P],
+    "lqm_ctx_set_scf_acceleration": [_P, ctypes.c_int],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -418,11 +419,17 @@ MFInfo = namedtuple("MFInfo", ["mu", "eH", "eF", "eband", "ekin", "iterations"])
 
 
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
-                     kweights=None, log_callback=None, multimode="cuda", ctx=None):
-    """``solvehartreefock(h, v, ρ_init, filling, ks; T, β, tol, iterations)`` with linear
-    mixing.  Returns (ρ, ϵ_GS, mf, converged, residual) like the reference."""
+                     kweights=None, log_callback=None, multimode="cuda", ctx=None, acceleration="linear",
+                     anderson_depth=5):
+    """``solvehartreefock(h, v, ρ_init, filling, ks; T, β, tol, iterations, acceleration,
+    anderson_depth)``: linear damped mixing (default) or Anderson acceleration.
+    Returns (ρ, ϵ_GS, mf, converged, residual) like the reference."""
     _check_mode(multimode)
+    if acceleration not in ("linear", "anderson"):
+        raise ValueError(f"acceleration must be 'linear' or 'anderson', got {acceleration!r}")
     ctx = ctx or default_context()
+    depth = int(anderson_depth) if acceleration == "anderson" else 0
+    ctx.check(_lib.lqm_ctx_set_scf_acceleration(ctx.handle, depth))
     hd = _as_device_hops(h, ctx)
     vd = _as_device_hops(v, ctx)
     ks = _ks(ks, hd.d)

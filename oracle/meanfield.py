@@ -65,13 +65,47 @@ def is_hermitian(rho, tol=np.sqrt(np.finfo(float).eps)):
     return True
 
 
+def anderson_update(flat_x, flat_f, hist_x, hist_f, beta):
+    """fixedpoint.jl:201-231 (_anderson_update): Type-II update with damping beta;
+    plain damped mixing without history or for a non-finite least-squares solution.
+    The least-squares solve `dG \\ g` is restated with numpy's lstsq (the same
+    solution for a full-rank history)."""
+    m = len(hist_x) - 1
+    if m == 0:
+        return beta * flat_f + (1 - beta) * flat_x
+    dX = np.stack([hist_x[i + 1] - hist_x[i] for i in range(m)], axis=1)
+    dF = np.stack([hist_f[i + 1] - hist_f[i] for i in range(m)], axis=1)
+    dG = dF - dX
+    g = flat_f - flat_x
+    gamma = np.linalg.lstsq(dG, g, rcond=None)[0]
+    if not np.all(np.isfinite(gamma)):
+        return beta * flat_f + (1 - beta) * flat_x
+    return (1 - beta) * flat_x + beta * flat_f - ((1 - beta) * dX + beta * dF) @ gamma
+
+
+def _flatten(rho, keys):
+    return np.concatenate([rho[k].ravel(order="F") for k in keys])
+
+
+def _unflatten(rho, flat, keys):
+    off = 0
+    for k in keys:
+        sz = rho[k].size
+        rho[k] = flat[off:off + sz].reshape(rho[k].shape, order="F").copy()
+        off += sz
+
+
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
-                     iterations=500, log=None):
-    """solvehartreefock -> _scf_driver! -> fixedpoint! (linear branch).
+                     iterations=500, log=None, acceleration="linear", anderson_depth=5):
+    """solvehartreefock -> _scf_driver! -> fixedpoint!.
 
     Meanfield/selfconsistent.jl:19,62-69,256-336,366-381 and fixedpoint.jl:39-194.
     Each iteration: hf(rho0); mu from the eigenvalues of hMF on every k;
-    rho1 = getdensitymatrix!(hMF, mu); linear mixing and the relative residual."""
+    rho1 = getdensitymatrix!(hMF, mu); linear mixing (or, with
+    acceleration="anderson", the Anderson update of fixedpoint.jl:64-142 with
+    its Hermitian projection) and the relative residual."""
+    use_anderson = acceleration == "anderson" and anderson_depth > 0
+    hist_x, hist_f = [], []
     rho0 = {L: M.copy() for L, M in rho_init.items()}
     if not is_hermitian(rho0):
         hermitianize(rho0)
@@ -93,10 +127,24 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
         hf.eband = eband
         hf.ekin = eband - 2 * hf.doublecounting()
         E = eband - hf.doublecounting()
-        for L in rho0:  # fixedpoint.jl:146-148
-            rho1[L] = beta * rho1[L] + (1 - beta) * rho0[L]
-        diff = np.linalg.norm([np.linalg.norm(rho1[L] - rho0[L]) for L in rho0])
-        nrm = np.linalg.norm([np.linalg.norm(rho1[L]) for L in rho0])
+        if use_anderson:  # fixedpoint.jl:101-142
+            keys = sorted(rho0.keys())
+            fx, ff = _flatten(rho0, keys), _flatten(rho1, keys)
+            hist_x.append(fx.copy())
+            hist_f.append(ff.copy())
+            while len(hist_x) > anderson_depth + 1:
+                hist_x.pop(0)
+                hist_f.pop(0)
+            _unflatten(rho1, anderson_update(fx, ff, hist_x, hist_f, beta), keys)
+            hermitianize(rho1)
+            fn = _flatten(rho1, keys)
+            diff = np.linalg.norm(fn - fx)
+            nrm = np.linalg.norm(fn)
+        else:
+            for L in rho0:  # fixedpoint.jl:146-148
+                rho1[L] = beta * rho1[L] + (1 - beta) * rho0[L]
+            diff = np.linalg.norm([np.linalg.norm(rho1[L] - rho0[L]) for L in rho0])
+            nrm = np.linalg.norm([np.linalg.norm(rho1[L]) for L in rho0])
         residual = diff / nrm if nrm > np.finfo(float).eps else diff
         for L in rho0:
             rho0[L] = rho1[L].copy()

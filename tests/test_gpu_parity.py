@@ -266,3 +266,22 @@ def test_fused_bands_dos_rho(lqm, ctx):
     for R in h:
         assert np.max(np.abs(rho[R] - ref[R])) <= RHO_TOL
     assert abs(eb - eb_ref) <= 1e-9 * max(1.0, abs(eb_ref))
+
+
+def test_hubbard_scf_anderson_matches_oracle(lqm, ctx):
+    """acceleration = :anderson (fixedpoint.jl:64-142, 201-231) on the device against the
+    oracle's restatement, 8 iterations with depth 3 (the history fills and rolls over;
+    iterations 2+ replay the captured graph).  Bound 1e-8: the two least-squares solves
+    (Gram-Schmidt QR here, SVD in the oracle) round differently and the iteration carries
+    the difference forward."""
+    lat, h, v = M.triangular_hubbard(L_super=2)
+    rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=3)}
+    ks = L.regulargrid(6 * 6)
+    kw = dict(T=0.02, beta=0.3, tol=0.0, iterations=8)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, acceleration="anderson", anderson_depth=3, **kw)
+    rho_ref, E_ref, hf_ref, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, acceleration="anderson",
+                                                                  anderson_depth=3, **kw)
+    assert res.mf.iterations == it == 8
+    assert np.max(np.abs(res.rho[(0, 0)] - rho_ref[(0, 0)])) <= 1e-8
+    assert abs(res.energy - E_ref) <= 1e-8
+    assert abs(res.residual - resid) <= 1e-8 * max(1.0, resid)
