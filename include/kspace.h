@@ -184,6 +184,17 @@ int lqm_bandmatrix_noalloc(void* stream, int64_t n, int64_t nR, int32_t d, const
 int lqm_bandmatrix_obs(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t nproj,
                        const lqm_hops* const* P, double* bands, double* obs);
 
+/* Site-resolved density (src/modules/Spectrum/dos.jl:20-52): n_i = 1/nk sum_k
+ * sum_{eps_j(k) <= mu} |U_ij(k)|^2, written to n_out (n doubles). */
+int lqm_density(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, double mu, double* n_out);
+/* Local density of states (src/modules/Spectrum/dos.jl:56-98): n_i = 1/(nk pi)
+ * sum_k sum_j |U_ij|^2 (1/nw) sum_w gamma / ((w - eps_j)^2 + gamma^2).  Every
+ * k-point contributes the frequency average once (the reference's per-k
+ * routine divides its running accumulator by nw at each k-point; the two
+ * agree for nw = 1, the ldos(H, ks, frequency) form). */
+int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t nw, const double* omegas,
+             double gamma, double* n_out);
+
 /* ---- Reverse-mode derivatives (no reference counterpart: the reference has
  * no derivatives; the forward maps are lqm_densitymatrix and lqm_bandmatrix).
  *

@@ -39,7 +39,7 @@ EXPORTS = [
     "lqm_chemicalpotential_bands_dev", "lqm_dos", "lqm_dos_bands_dev", "lqm_scf_hf",
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
-    "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration",
+    "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
 ]
 
 
@@ -88,6 +88,8 @@ _SIG = {
     "lqm_bands_vjp": [_P, _P, _I64, _P, _P, _P],
     "lqm_bandmatrix_obs": [_P, _P, _I64, _P, _I64, _P, _P, _P],
     "lqm_ctx_set_scf_acceleration": [_P, ctypes.c_int],
+    "lqm_density": [_P, _P, _I64, _P, _D, _P],
+    "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -360,6 +362,32 @@ def bands_vjp(H, ks, eps_bar, ctx=None):
     out = np.zeros((Hd.n, Hd.n, Hd.nR), dtype=np.complex128, order="F")
     ctx.check(_lib.lqm_bands_vjp(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(eb), _ptr(out)))
     return {R: np.array(out[:, :, i]) for i, R in enumerate(Hd.keys)}
+
+
+def density(H, ks, mu=0.0, multimode="cuda", ctx=None):
+    """``density(H, ks, μ)`` (Spectrum/dos.jl:20-52): per-orbital occupation of the
+    states with eps <= mu, averaged over ks (``lqm_density``)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    out = np.zeros(Hd.n)
+    ctx.check(_lib.lqm_density(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), float(mu), _ptr(out)))
+    return out
+
+
+def ldos(H, ks, frequencies, gamma=0.1, multimode="cuda", ctx=None):
+    """``ldos(H, ks, frequencies; Γ)`` (Spectrum/dos.jl:56-98), with 1/π, averaged over
+    the frequencies (``lqm_ldos``)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    om = np.ascontiguousarray(np.atleast_1d(frequencies), dtype=np.float64)
+    out = np.zeros(Hd.n)
+    ctx.check(_lib.lqm_ldos(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), len(om), _ptr(om), float(gamma),
+                            _ptr(out)))
+    return out
 
 
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):

@@ -63,6 +63,29 @@ def bandmatrix_obs(h, ks, projectors):
     return bands, obs
 
 
+def density(h, ks, mu=0.0):
+    """Spectrum/dos.jl:20-52: n_i = 1/L sum_k sum_{eps_j <= mu} |U_ij|^2."""
+    n = next(iter(h.values())).shape[0]
+    out = np.zeros(n)
+    for j in range(ks.shape[1]):
+        e, U = eigh_upper(fouriersum(h, ks[:, j]), True)
+        out += np.sum(np.abs(U[:, e <= mu]) ** 2, axis=1)
+    return out / ks.shape[1]
+
+
+def ldos(h, ks, omegas, gamma=0.1):
+    """Spectrum/dos.jl:56-98: n_i = 1/(L pi) sum_k sum_j |U_ij|^2 (1/F) sum_w
+    Gamma / ((w - eps_j)^2 + Gamma^2) (the k-point's frequency average counted once)."""
+    omegas = np.atleast_1d(np.asarray(omegas, float))
+    n = next(iter(h.values())).shape[0]
+    out = np.zeros(n)
+    for j in range(ks.shape[1]):
+        e, U = eigh_upper(fouriersum(h, ks[:, j]), True)
+        a = np.mean(gamma / ((omegas[:, None] - e[None, :]) ** 2 + gamma ** 2), axis=0)
+        out += (np.abs(U) ** 2) @ a
+    return out / (ks.shape[1] * np.pi)
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

@@ -187,3 +187,19 @@ def test_band_expectation_values_match_oracle(lqm, ctx, bctx, blocked):
                     start = i
         assert np.max(np.abs(res.obs[:, :, 1] - res.bands)) <= BAND_TOL * scale, name
         assert np.max(np.abs(res.obs[:, :, 2] - 1.0)) <= 1e-12, name
+
+
+@pytest.mark.parametrize("blocked", [False, True], ids=["default", "blocked"])
+def test_density_and_ldos_match_oracle(lqm, ctx, bctx, blocked):
+    """density (dos.jl:20-52) and ldos (dos.jl:56-98) through lqm_density / lqm_ldos:
+    basis-independent per-orbital sums, so degenerate bands do not matter."""
+    c = bctx if blocked else ctx
+    cases = M.batch_models() + [("honeycomb144", M.honeycomb_disorder()[1])]
+    ks = L.regulargrid(6 * 6)
+    for name, h in cases:
+        n_ref = K.density(h, ks, mu=0.1)
+        assert np.max(np.abs(lqm.density(h, ks, mu=0.1, ctx=c) - n_ref)) <= 1e-12 * h[(0, 0)].shape[0], name
+        for om in ([0.2], [-1.0, 0.0, 0.7]):
+            ld_ref = K.ldos(h, ks, om, gamma=0.05)
+            ld = lqm.ldos(h, ks, om, gamma=0.05, ctx=c)
+            assert np.max(np.abs(ld - ld_ref)) <= 1e-10 * max(1.0, np.max(ld_ref)), (name, om)

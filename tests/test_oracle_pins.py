@@ -288,3 +288,19 @@ def test_anderson_scf_oracle_converges_faster_than_linear():
     assert a[3] and lin[3]
     assert a[5] < lin[5] / 3
     assert abs(a[1] - lin[1]) < 1e-9
+
+
+def test_density_and_ldos_sum_rules():
+    """density (dos.jl:20-52): the orbital sum counts the states below mu per k-point;
+    ldos (dos.jl:56-98): the orbital sum is the DOS over pi (the getdos normalisation
+    has no 1/pi, dos.jl:138-144), for one frequency and for a window."""
+    lat = L.honeycomb()
+    h = M.graphene(lat, spin=True)
+    ks = L.regulargrid(12 * 12)
+    n = K.density(h, ks, mu=0.3)
+    bands = K.bandmatrix(h, ks)[0]
+    assert abs(n.sum() - np.mean(np.sum(bands <= 0.3, axis=0))) < 1e-12
+    for om in ([0.4], [0.2, 0.5, 0.9]):
+        ld = K.ldos(h, ks, om, gamma=0.05)
+        dos = np.mean([K.dos_from_bands(bands, np.array([w]), 0.05)[0] for w in om])
+        assert abs(ld.sum() - dos / np.pi) < 1e-12 * max(1.0, dos)
