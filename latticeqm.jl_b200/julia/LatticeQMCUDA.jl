@@ -150,6 +150,31 @@ function cuda_bandmatrix_obs(H, ks::AbstractMatrix{Float64}, projectors, exec::C
     bands, obs
 end
 
+"""`density(H, ks, μ)` (Spectrum/dos.jl:20-52) on the device (`lqm_density`)."""
+function cuda_density(H, ks::AbstractMatrix{Float64}, μ::Real, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    out = zeros(Float64, n)
+    check(ctx, ccall((:lqm_density, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Float64, Ptr{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Float64(μ), out))
+    out
+end
+
+"""`ldos(H, ks, frequencies; Γ)` (Spectrum/dos.jl:56-98) on the device (`lqm_ldos`); the
+frequency average counts once per k-point (equal to the reference for one frequency)."""
+function cuda_ldos(H, ks::AbstractMatrix{Float64}, ωs::AbstractVector, exec::CudaExec; Γ::Real=0.1)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    out = zeros(Float64, n)
+    check(ctx, ccall((:lqm_ldos, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Ptr{Float64}, Float64, Ptr{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), length(ωs), Vector{Float64}(ωs), Float64(Γ), out))
+    out
+end
+
 """`getdensitymatrix!(ρs, H, ks, kweights, μ; T)` on the device; returns the band energy."""
 function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
                              μ::Float64, T::Real, exec::CudaExec)
