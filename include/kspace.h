@@ -195,6 +195,13 @@ int lqm_density(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, d
 int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t nw, const double* omegas,
              double gamma, double* n_out);
 
+/* Berry curvature plaquette phases, berry(H, NX, NY, bandindices)
+ * (src/modules/Spectrum/berry.jl:48-82,107-155): eigenvectors of the nb bands
+ * `bands` (0-based) on k = (i/(NX-1), j/(NY-1)) + 1.34e-8, link variables
+ * det(S^H S')/|det|, and F[i + (NX-1) j] = arg(plaquette product)/(2 pi) for
+ * the (NX-1) x (NY-1) plaquettes.  Two-dimensional Hops only. */
+int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, double* F);
+
 /* ---- Reverse-mode derivatives (no reference counterpart: the reference has
  * no derivatives; the forward maps are lqm_densitymatrix and lqm_bandmatrix).
  *

@@ -175,6 +175,23 @@ function cuda_ldos(H, ks::AbstractMatrix{Float64}, ωs::AbstractVector, exec::Cu
     out
 end
 
+"""`berry(H, NX, NY, bandindices)` (Spectrum/berry.jl:140-155) on the device (`lqm_berry`):
+(midkgrid, F) with F the (NX-1) x (NY-1) plaquette phases; `bandindices` are 1-based as in
+the reference."""
+function cuda_berry(H, NX::Int, NY::Int, bandindices::AbstractVector{<:Integer}, exec::CudaExec)
+    NY = NY < 1 ? NX : NY
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    b = Int64[i - 1 for i in bandindices]
+    F = zeros(Float64, NX - 1, NY - 1)
+    check(ctx, ccall((:lqm_berry, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int64, Int64, Ptr{Int64}, Ptr{Float64}),
+        ctx.ptr, dh.ptr, NX, NY, length(b), b, F))
+    midkgrid = [[x; y] for x = range(0.5 / (NX - 1); stop=1 - 0.5 / (NX - 1), length=NX - 1),
+                           y = range(0.5 / (NY - 1); stop=1 - 0.5 / (NY - 1), length=NY - 1)]
+    midkgrid, F
+end
+
 """`getdensitymatrix!(ρs, H, ks, kweights, μ; T)` on the device; returns the band energy."""
 function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
                              μ::Float64, T::Real, exec::CudaExec)

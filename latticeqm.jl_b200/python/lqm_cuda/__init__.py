@@ -40,6 +40,7 @@ EXPORTS = [
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
     "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
+    "lqm_berry",
 ]
 
 
@@ -90,6 +91,7 @@ _SIG = {
     "lqm_ctx_set_scf_acceleration": [_P, ctypes.c_int],
     "lqm_density": [_P, _P, _I64, _P, _D, _P],
     "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
+    "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -388,6 +390,22 @@ def ldos(H, ks, frequencies, gamma=0.1, multimode="cuda", ctx=None):
     ctx.check(_lib.lqm_ldos(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), len(om), _ptr(om), float(gamma),
                             _ptr(out)))
     return out
+
+
+def berry(H, NX, NY=0, bands=(0,), multimode="cuda", ctx=None):
+    """``berry(H, NX, NY, bandindices)`` (Spectrum/berry.jl:140-155) with 0-based band
+    indices: returns (midkgrid (2, NX-1, NY-1), F (NX-1, NY-1)) like the reference."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    NY = NX if NY < 1 else NY
+    b = np.ascontiguousarray(bands, dtype=np.int64)
+    F = np.zeros((NX - 1, NY - 1), order="F")
+    ctx.check(_lib.lqm_berry(ctx.handle, Hd.handle, int(NX), int(NY), len(b), _ptr(b), _ptr(F)))
+    mx = np.linspace(0.5 / (NX - 1), 1 - 0.5 / (NX - 1), NX - 1)
+    my = np.linspace(0.5 / (NY - 1), 1 - 0.5 / (NY - 1), NY - 1)
+    mid = np.stack(np.meshgrid(mx, my, indexing="ij"))
+    return mid, F
 
 
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):

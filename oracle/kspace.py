@@ -86,6 +86,30 @@ def ldos(h, ks, omegas, gamma=0.1):
     return out / (ks.shape[1] * np.pi)
 
 
+def berry(h, NX, NY, bands):
+    """Spectrum/berry.jl:48-82 (statesgrid on range(0,1,N) x range(0,1,N) + 1.34e-8)
+    and :107-137 (link L = det(A^H B)/|det|, plaquette phase real(log(...)/(2 pi i)));
+    0-based band indices; F (NX-1, NY-1)."""
+    S = {}
+    for j in range(NY):
+        for i in range(NX):
+            k = np.array([i / (NX - 1), j / (NY - 1)]) + 1.34e-8
+            _, U = eigh_upper(fouriersum(h, k), True)
+            S[i, j] = U[:, list(bands)]
+
+    def link(A, B):
+        d = np.linalg.det(A.conj().T @ B)
+        return d / abs(d)
+
+    F = np.zeros((NX - 1, NY - 1))
+    for i in range(NX - 1):
+        for j in range(NY - 1):
+            z = link(S[i, j], S[i + 1, j]) * link(S[i + 1, j], S[i + 1, j + 1]) \
+                / link(S[i, j + 1], S[i + 1, j + 1]) / link(S[i, j], S[i, j + 1])
+            F[i, j] = np.real(np.log(z) / (2j * math.pi))
+    return F
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

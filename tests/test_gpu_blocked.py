@@ -203,3 +203,18 @@ def test_density_and_ldos_match_oracle(lqm, ctx, bctx, blocked):
             ld_ref = K.ldos(h, ks, om, gamma=0.05)
             ld = lqm.ldos(h, ks, om, gamma=0.05, ctx=c)
             assert np.max(np.abs(ld - ld_ref)) <= 1e-10 * max(1.0, np.max(ld_ref)), (name, om)
+
+
+def test_berry_plaquettes_match_oracle(lqm, ctx):
+    """berry(H, NX, NY, bandindices) through lqm_berry against the oracle: gapped graphene
+    (one band) and the spin-orbit triangular model (its four lowest bands, whole
+    degenerate groups so the plaquette phases are gauge invariant)."""
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    h[(0, 0)] = h[(0, 0)] + np.diag([0.3, -0.3])
+    _, F = lqm.berry(h, 12, 12, [0], ctx=ctx)
+    assert np.max(np.abs(F - K.berry(h, 12, 12, [0]))) <= 1e-10
+    h3 = M.batch_models()[2][1]
+    _, F3 = lqm.berry(h3, 8, 8, [0, 1, 2, 3], ctx=ctx)
+    assert np.max(np.abs(F3 - K.berry(h3, 8, 8, [0, 1, 2, 3]))) <= 1e-10
+    assert abs(F3.sum()) <= 1e-9  # integer total (zero for this model)

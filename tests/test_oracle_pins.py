@@ -304,3 +304,15 @@ def test_density_and_ldos_sum_rules():
         ld = K.ldos(h, ks, om, gamma=0.05)
         dos = np.mean([K.dos_from_bands(bands, np.array([w]), 0.05)[0] for w in om])
         assert abs(ld.sum() - dos / np.pi) < 1e-12 * max(1.0, dos)
+
+
+def test_berry_massive_graphene_valley_curvature():
+    """berry.jl:107-155 restated: gapped graphene (staggered onsite) has zero total Chern
+    number and opposite curvature at the two valleys (the plaquette phases sum to 0 and
+    the grid's extreme values are negatives of each other)."""
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    h[(0, 0)] = h[(0, 0)] + np.diag([0.3, -0.3])
+    F = K.berry(h, 12, 12, [0])
+    assert abs(F.sum()) < 1e-12
+    assert abs(F.max() + F.min()) < 1e-12 and F.max() > 0.05
