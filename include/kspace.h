@@ -202,6 +202,18 @@ int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int6
  * the (NX-1) x (NY-1) plaquettes.  Two-dimensional Hops only. */
 int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, double* F);
 
+/* Kubo current-current correlator, opticalconductivity(frequencies, H, J1, J2,
+ * ks; mu, Gamma, T) (src/modules/LinearResponse/opticalconductivity.jl:101-127
+ * with kubo! of src/modules/LinearResponse/kubo.jl:11-26):
+ *   chi(w) = -(i/nk) sum_k sum_{i != j} (f_i - f_j) (U^H J1 U)_ij (U^H J2^H U)_ji
+ *            / ((e_i - e_j) - (w + i Gamma)),
+ * f = fermidirac(e; T, mu).  J1 and J2 are Hops of H's order and key dimension
+ * (the current operators of getcurrentoperators, src/modules/Operators/current.jl:20-37).
+ * chi receives nw complex values (interleaved re, im).  nw <= 524280. */
+int lqm_opticalconductivity(lqm_ctx* ctx, const lqm_hops* H, const lqm_hops* J1, const lqm_hops* J2, int64_t nk,
+                            const double* ks, int64_t nw, const double* omegas, double mu, double gamma, double T,
+                            double* chi);
+
 /* ---- Reverse-mode derivatives (no reference counterpart: the reference has
  * no derivatives; the forward maps are lqm_densitymatrix and lqm_bandmatrix).
  *

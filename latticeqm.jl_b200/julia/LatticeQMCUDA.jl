@@ -192,6 +192,22 @@ function cuda_berry(H, NX::Int, NY::Int, bandindices::AbstractVector{<:Integer},
     midkgrid, F
 end
 
+"""`opticalconductivity(frequencies, H, J1, J2, ks; μ, Γ, T)`
+(LinearResponse/opticalconductivity.jl:101-127) on the device (`lqm_opticalconductivity`):
+the Kubo correlator χ(ω).  `J1`, `J2` are Hops (e.g. from `getcurrentoperators(lat, H)`)."""
+function cuda_opticalconductivity(frequencies::AbstractVector, H, J1, J2, ks::AbstractMatrix{Float64},
+                                  exec::CudaExec; μ::Float64=0.0, Γ::Float64=0.025, T::Float64=0.1)
+    ctx = context(exec.device)
+    dh, d1, d2 = upload(ctx, H), upload(ctx, J1), upload(ctx, J2)
+    out = zeros(ComplexF64, length(frequencies))
+    check(ctx, ccall((:lqm_opticalconductivity, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Ptr{Float64}, Float64,
+         Float64, Float64, Ptr{ComplexF64}),
+        ctx.ptr, dh.ptr, d1.ptr, d2.ptr, size(ks, 2), Matrix{Float64}(ks), length(frequencies),
+        Vector{Float64}(frequencies), μ, Γ, T, out))
+    out
+end
+
 """`getdensitymatrix!(ρs, H, ks, kweights, μ; T)` on the device; returns the band energy."""
 function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
                              μ::Float64, T::Real, exec::CudaExec)

@@ -40,7 +40,7 @@ EXPORTS = [
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
     "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
-    "lqm_berry",
+    "lqm_berry", "lqm_opticalconductivity",
 ]
 
 
@@ -92,6 +92,7 @@ _SIG = {
     "lqm_density": [_P, _P, _I64, _P, _D, _P],
     "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
+    "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -406,6 +407,23 @@ def berry(H, NX, NY=0, bands=(0,), multimode="cuda", ctx=None):
     my = np.linspace(0.5 / (NY - 1), 1 - 0.5 / (NY - 1), NY - 1)
     mid = np.stack(np.meshgrid(mx, my, indexing="ij"))
     return mid, F
+
+
+def opticalconductivity(frequencies, H, J1, J2, ks, mu=0.0, Gamma=0.025, T=0.1, multimode="cuda", ctx=None):
+    """``opticalconductivity(frequencies, H, J1, J2, ks; μ, Γ, T)``
+    (LinearResponse/opticalconductivity.jl:101-127): the Kubo current-current
+    correlator chi(w) (complex, one per frequency; ``lqm_opticalconductivity``).
+    J1, J2 are Hops of H's order (the current operators)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    J1d, J2d = _as_device_hops(J1, ctx), _as_device_hops(J2, ctx)
+    om = np.ascontiguousarray(np.atleast_1d(frequencies), dtype=np.float64)
+    out = np.zeros(len(om), dtype=np.complex128)
+    ctx.check(_lib.lqm_opticalconductivity(ctx.handle, Hd.handle, J1d.handle, J2d.handle, ks.shape[1], _ptr(ks),
+                                           len(om), _ptr(om), float(mu), float(Gamma), float(T), _ptr(out)))
+    return out
 
 
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):

@@ -118,6 +118,30 @@ def hermitianize(h):
     return h
 
 
+def currentoperators(lat, h):
+    """``getcurrentoperators(lat, hops)`` (Operators/current.jl:20-37 with
+    _apply_position_factor_dense!, :65-75): one Hops per lattice direction alpha,
+    J_alpha[R] = H_R with block (i, j) (orbital pair, size D/N for the internal
+    multiplicity) multiplied by -i (r_i + A R - r_j)_alpha, r the Cartesian
+    positions, alpha the Cartesian component."""
+    r = lat.positions()
+    A = lat.basis[:, :2]
+    N = r.shape[1]
+    D = hopdim(h)
+    if D < N or D % N:
+        raise ValueError("Hops dimension is not a multiple of the orbital count")
+    m = D // N
+    Js = []
+    for a in range(A.shape[1]):
+        J = {}
+        for R, M in h.items():
+            r0 = r[a] + (A @ np.array(R, float))[a]
+            fac = -1j * (r0[:, None] - r[a][None, :])  # (i, j) -> -i (r0_i - r_j)
+            J[R] = M * np.kron(fac, np.ones((m, m)))
+        Js.append(J)
+    return Js
+
+
 def with_keys(h, keys):
     """Restrict/extend a Hops to exactly ``keys`` (zero blocks kept)."""
     n = hopdim(h)

@@ -110,6 +110,33 @@ def berry(h, NX, NY, bands):
     return F
 
 
+def kubo(omegas, e, U, A, B, mu=0.0, gamma=0.025, T=0.1):
+    """LinearResponse/kubo.jl:11-26 (kubo!): sum_{i != j} (f_i - f_j) M_ij /
+    ((e_i - e_j) - (w + i Gamma)) with M = (U^H A U) .* transpose(U^H B U), the pairs
+    in the reference's order (i fastest)."""
+    omegas = np.asarray(omegas, float)
+    M = (U.conj().T @ A @ U) * (U.conj().T @ B @ U).T
+    fd = fermidirac(e, mu, T)
+    out = np.zeros(len(omegas), complex)
+    n = len(e)
+    for j in range(n):
+        for i in range(n):
+            if i != j:
+                out += (fd[i] - fd[j]) * M[i, j] / ((e[i] - e[j]) - (omegas + 1j * gamma))
+    return out
+
+
+def opticalconductivity(omegas, h, J1, J2, ks, mu=0.0, gamma=0.025, T=0.1):
+    """LinearResponse/opticalconductivity.jl:101-127: chi(w) = -(i/N) sum_k
+    kubo!(w, e_k, U_k, J1(k), J2(k)^H)."""
+    out = np.zeros(len(np.atleast_1d(omegas)), complex)
+    for j in range(ks.shape[1]):
+        k = ks[:, j]
+        e, U = eigh_upper(fouriersum(h, k), True)
+        out += kubo(np.atleast_1d(omegas), e, U, fouriersum(J1, k), fouriersum(J2, k).conj().T, mu, gamma, T)
+    return out * (-1j / ks.shape[1])
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

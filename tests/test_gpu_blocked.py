@@ -218,3 +218,40 @@ def test_berry_plaquettes_match_oracle(lqm, ctx):
     _, F3 = lqm.berry(h3, 8, 8, [0, 1, 2, 3], ctx=ctx)
     assert np.max(np.abs(F3 - K.berry(h3, 8, 8, [0, 1, 2, 3]))) <= 1e-10
     assert abs(F3.sum()) <= 1e-9  # integer total (zero for this model)
+
+
+def test_optical_conductivity_matches_oracle(lqm, ctx, bctx):
+    """opticalconductivity(frequencies, H, J1, J2, ks; mu, Gamma, T) through
+    lqm_opticalconductivity against the oracle: graphene on the klin=30 grid of
+    test/test_linearresponse.jl (with its sigma invariants on the device result), and
+    the disordered spinful honeycomb 6x6 cell (n=144) on both eigensolver paths."""
+    lat = L.honeycomb()
+    h = M.graphene(lat)
+    Js = M.currentoperators(lat, h)
+    om = np.linspace(0.05, 3.0, 30)
+    gam, T, mu = 0.05, 0.01, 0.0
+    ks = L.regulargrid(nk=30 ** 2)
+    sig = {}
+    for a, b in ((0, 0), (1, 1), (0, 1)):
+        chi = lqm.opticalconductivity(om, h, Js[a], Js[b], ks, mu=mu, Gamma=gam, T=T, ctx=ctx)
+        ref = K.opticalconductivity(om, h, Js[a], Js[b], ks, mu, gam, T)
+        assert np.max(np.abs(chi - ref)) <= 1e-10 * max(1.0, np.max(np.abs(ref))), (a, b)
+        sig[a, b] = -(chi - chi[0]) / (om + 1j * gam)
+    assert np.max(np.abs(sig[0, 0].real - sig[1, 1].real)) < 1e-10
+    assert np.max(np.abs(sig[0, 1].real)) < 1e-10
+    assert np.all(sig[0, 0].real > -1e-6)
+
+    lat6, h6 = M.honeycomb_disorder(6)
+    J6 = M.currentoperators(lat6, h6)
+    rng = np.random.default_rng(11)
+    ks6 = rng.uniform(-0.5, 0.5, (2, 6))
+    om6 = np.linspace(0.0, 4.0, 21)
+    ref = K.opticalconductivity(om6, h6, J6[0], J6[1], ks6, 0.05, 0.04, 0.1)
+    c1 = lqm.Context(0, timeout=900)
+    c1.set_blocked_min_n(10 ** 9)  # the one-CTA eigensolver
+    try:
+        for c in (c1, bctx):
+            chi = lqm.opticalconductivity(om6, h6, J6[0], J6[1], ks6, mu=0.05, Gamma=0.04, T=0.1, ctx=c)
+            assert np.max(np.abs(chi - ref)) <= 1e-9 * max(1.0, np.max(np.abs(ref)))
+    finally:
+        c1.close()

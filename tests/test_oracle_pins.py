@@ -316,3 +316,29 @@ def test_berry_massive_graphene_valley_curvature():
     F = K.berry(h, 12, 12, [0])
     assert abs(F.sum()) < 1e-12
     assert abs(F.max() + F.min()) < 1e-12 and F.max() > 0.05
+
+
+def test_optical_conductivity_graphene_invariants():
+    """test/test_linearresponse.jl:33-58 (graphene, half filling, klin=30, 30 frequencies:
+    sigma_xx = sigma_yy, Re sigma_xy = 0, Re sigma_xx >= 0) and test/test_operators.jl:135-151
+    (the current operators are Hermitian) on the oracle."""
+    lat = L.honeycomb()
+    h = M.graphene(lat)
+    Js = M.currentoperators(lat, M.nearestneighbor(lat, -1.0))
+    assert len(Js) == 2
+    for k in ([0.0, 0.0], [1 / 3, -1 / 3], [0.5, 0.5], [-0.2, 0.7]):
+        for J in Js:
+            Jk = K.fouriersum(J, k)
+            assert np.max(np.abs(Jk - Jk.conj().T)) < 1e-10
+    Js = M.currentoperators(lat, h)
+    om = np.linspace(0.05, 3.0, 30)
+    gam, T, mu = 0.05, 0.01, 0.0
+    ks = L.regulargrid(nk=30 ** 2)
+    sig = {}
+    for a, b in ((0, 0), (1, 1), (0, 1)):
+        chi = K.opticalconductivity(om, h, Js[a], Js[b], ks, mu, gam, T)
+        sig[a, b] = -(chi - chi[0]) / (om + 1j * gam)
+    assert np.max(np.abs(sig[0, 0].real - sig[1, 1].real)) < 1e-10
+    assert np.max(np.abs(sig[0, 1].real)) < 1e-10
+    assert np.all(sig[0, 0].real > -1e-6)
+    assert np.max(sig[0, 0].real) > 1e-3  # an interband response is present
