@@ -281,6 +281,22 @@ def large_configs(Q, ctx, M, pool, cores):
     dv, wv = timed(lambda: Q.densitymatrix_vjp(h4, ks4, G, mu=0.0, T=0.02, ctx=ctx), reps=3)
     out["vjp_triangular_n72"] = {"grid": "36x36", "vjp_kpts_per_s": ks4.shape[1] / dv,
                                  "vjp_wall_kpts_per_s": ks4.shape[1] / wv}
+    # Kubo correlator chi_xx(w) and chi_xy(w) (64 frequencies, Gamma = 0.05, T = 0.01) on the
+    # honeycomb 6x6 cell (48 x 48 grid) and the m=10 twisted bilayer (8 x 8 grid)
+    om = np.linspace(0.0, 3.0, 64)
+    kubo = {}
+    for name, lat, h, ks in (("honeycomb6x6_n144", *M.honeycomb_disorder(), ks1),
+                             ("tbg_m10_n1324", lat3, h3, LL.regulargrid(8 * 8))):
+        J = M.currentoperators(lat, h)
+        Hd, J0, J1 = Q.DeviceHops(h, ctx), Q.DeviceHops(J[0], ctx), Q.DeviceHops(J[1], ctx)
+        dxx, wxx = timed(lambda: Q.opticalconductivity(om, Hd, J0, J0, ks, Gamma=0.05, T=0.01, ctx=ctx))
+        dxy, wxy = timed(lambda: Q.opticalconductivity(om, Hd, J0, J1, ks, Gamma=0.05, T=0.01, ctx=ctx))
+        dbv, _ = timed(lambda: Q.bandmatrix(Hd, ks, want_vectors=True, ctx=ctx))
+        kubo[name] = {"kpoints": ks.shape[1], "frequencies": len(om),
+                      "xx_kpts_per_s": ks.shape[1] / dxx, "xx_wall_kpts_per_s": ks.shape[1] / wxx,
+                      "xy_kpts_per_s": ks.shape[1] / dxy, "xy_wall_kpts_per_s": ks.shape[1] / wxy,
+                      "eigen_pass_with_vectors_kpts_per_s": ks.shape[1] / dbv}
+    out["optical_conductivity"] = kubo
     return out
 
 

@@ -209,7 +209,8 @@ int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t n
  *            / ((e_i - e_j) - (w + i Gamma)),
  * f = fermidirac(e; T, mu).  J1 and J2 are Hops of H's order and key dimension
  * (the current operators of getcurrentoperators, src/modules/Operators/current.jl:20-37).
- * chi receives nw complex values (interleaved re, im).  nw <= 524280. */
+ * chi receives nw complex values (interleaved re, im).  nw <= 524280.
+ * Passing the same handle for J1 and J2 computes U^H J U once. */
 int lqm_opticalconductivity(lqm_ctx* ctx, const lqm_hops* H, const lqm_hops* J1, const lqm_hops* J2, int64_t nk,
                             const double* ks, int64_t nw, const double* omegas, double mu, double gamma, double T,
                             double* chi);

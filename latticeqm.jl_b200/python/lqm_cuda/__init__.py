@@ -418,7 +418,8 @@ def opticalconductivity(frequencies, H, J1, J2, ks, mu=0.0, Gamma=0.025, T=0.1, 
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
     ks = _ks(ks, Hd.d)
-    J1d, J2d = _as_device_hops(J1, ctx), _as_device_hops(J2, ctx)
+    J1d = _as_device_hops(J1, ctx)
+    J2d = J1d if J2 is J1 else _as_device_hops(J2, ctx)  # one handle: the J2 = J1 shortcut
     om = np.ascontiguousarray(np.atleast_1d(frequencies), dtype=np.float64)
     out = np.zeros(len(om), dtype=np.complex128)
     ctx.check(_lib.lqm_opticalconductivity(ctx.handle, Hd.handle, J1d.handle, J2d.handle, ks.shape[1], _ptr(ks),
