@@ -202,6 +202,22 @@ int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int6
  * the (NX-1) x (NY-1) plaquettes.  Two-dimensional Hops only. */
 int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, double* F);
 
+/* Partial spectrum, the `format=:sparse, num_bands` path of bandmatrix and
+ * getdensitymatrix! (src/modules/Eigen/eigen_sparse_krylovkit.jl:44-88,
+ * src/modules/Operators/densitymatrix.jl:100-104,131-147): per k the
+ * num_bands eigenpairs nearest sigma (which = 0, the reference's :LM
+ * shift-invert default, sigma defaulting to 1e-8 there), the smallest (1, :SR)
+ * or the largest (2, :LR), in ascending order.  Computed by the dense
+ * eigensolver and a window selection (on a tie in distance the lower
+ * eigenvalue is taken).  bands: num_bands x nk; U: n x num_bands x nk.
+ * lqm_densitymatrix_partial is lqm_densitymatrix with rho_k = U_w f U_w^H
+ * over the selected states only. */
+int lqm_bandmatrix_partial(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t num_bands,
+                           double sigma, int which, int want_vectors, double* bands, double* U);
+int lqm_densitymatrix_partial(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
+                              double mu, double T, int64_t num_bands, double sigma, int which, int64_t nL,
+                              const int64_t* Lkeys, double* rho, double* eband);
+
 /* Kubo current-current correlator, opticalconductivity(frequencies, H, J1, J2,
  * ks; mu, Gamma, T) (src/modules/LinearResponse/opticalconductivity.jl:101-127
  * with kubo! of src/modules/LinearResponse/kubo.jl:11-26):

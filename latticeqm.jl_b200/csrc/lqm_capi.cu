@@ -992,6 +992,7 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 #include "lqm_sitedos.inc"
 #include "lqm_berry.inc"
 #include "lqm_kubo.inc"
+#include "lqm_partial.inc"
 
 // ============================================================================
 // Allocation-free eigen pass.

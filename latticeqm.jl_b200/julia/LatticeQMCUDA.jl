@@ -230,6 +230,50 @@ function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights
     eb[]
 end
 
+const WHICH_CODE = Dict(:LM => Cint(0), :SR => Cint(1), :LR => Cint(2))
+
+"""`bandmatrix(H, ks; format=:sparse, num_bands, sigma, which)` on the device
+(`lqm_bandmatrix_partial`): per k the `num_bands` eigenpairs of `eigen_sparse`
+(Eigen/eigen_sparse_krylovkit.jl:44-88), ascending."""
+function cuda_bandmatrix_partial(H, ks::AbstractMatrix{Float64}, num_bands::Int, exec::CudaExec;
+                                 sigma::Float64=1e-8, which::Symbol=:LM, vectors::Bool=false)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    nk = size(ks, 2)
+    bands = zeros(Float64, num_bands, nk)
+    U = vectors ? zeros(ComplexF64, n, num_bands, nk) : ComplexF64[]
+    check(ctx, ccall((:lqm_bandmatrix_partial, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Float64, Cint, Cint, Ptr{Float64}, Ptr{ComplexF64}),
+        ctx.ptr, dh.ptr, nk, Matrix{Float64}(ks), num_bands, sigma, WHICH_CODE[which], vectors, bands,
+        vectors ? U : Ptr{ComplexF64}(C_NULL)))
+    vectors ? (bands, U) : bands
+end
+
+"""`getdensitymatrix!(ρs, H, ks, kweights, μ; T, format=:sparse, num_bands)` on the device
+(`lqm_densitymatrix_partial`): ρ from the selected states only; returns the band energy."""
+function cuda_densitymatrix_partial!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
+                                     μ::Float64, T::Real, num_bands::Int, exec::CudaExec;
+                                     sigma::Float64=1e-8, which::Symbol=:LM)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    Lk = collect(keys(ρs))
+    d = length(first(Lk))
+    n = size(H[first(keys(H))], 1)
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    rho = zeros(ComplexF64, n, n, length(Lk))
+    eb = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_densitymatrix_partial, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Int64, Float64, Cint, Int64,
+         Ptr{Int64}, Ptr{ComplexF64}, Ref{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Vector{Float64}(kweights), μ, Float64(T), num_bands,
+        sigma, WHICH_CODE[which], length(Lk), L, rho, eb))
+    for (i, k) in enumerate(Lk)
+        ρs[k] .= view(rho, :, :, i)
+    end
+    eb[]
+end
+
 """`chemicalpotential(H, ks, filling; T)` from device bands (unweighted mean, as the reference)."""
 function cuda_chemicalpotential(H, ks::AbstractMatrix{Float64}, filling::Real, exec::CudaExec; T::Real=0.0)
     ctx = context(exec.device)

@@ -40,7 +40,7 @@ EXPORTS = [
     "lqm_ctx_reset_stats", "lqm_ctx_stats", "lqm_bands_dos_rho", "lqm_bands_dos_rho_dev",
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
     "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
-    "lqm_berry", "lqm_opticalconductivity",
+    "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
 ]
 
 
@@ -93,6 +93,9 @@ _SIG = {
     "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
+    "lqm_bandmatrix_partial": [_P, _P, _I64, _P, _I64, _D, ctypes.c_int, ctypes.c_int, _P, _P],
+    "lqm_densitymatrix_partial": [_P, _P, _I64, _P, _P, _D, _D, _I64, _D, ctypes.c_int, _I64, _P, _P,
+                                  ctypes.POINTER(_D)],
     "lqm_bands_dos_rho": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D, _P,
                           _P, ctypes.c_int],
     "lqm_bands_dos_rho_dev": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D), _I64, _P, _D,
@@ -256,10 +259,14 @@ def bloch(H, ks, ctx=None):
     return out
 
 
-def bandmatrix(H, ks, multimode="cuda", want_vectors=False, precision=0, ctx=None):
+def bandmatrix(H, ks, multimode="cuda", want_vectors=False, precision=0, ctx=None, format="dense",
+               num_bands=None, sigma=1e-8, which="LM"):
     """``bandmatrix(H, ks)``: bands (n, nk) ascending per column; with
-    ``want_vectors`` also U (n, n, nk) (columns = eigenvectors)."""
+    ``want_vectors`` also U (n, n, nk) (columns = eigenvectors).  ``format="sparse"``
+    with ``num_bands`` is the partial spectrum of ``bandmatrix_partial``."""
     _check_mode(multimode)
+    if str(format).lstrip(":") == "sparse" and num_bands is not None:
+        return bandmatrix_partial(H, ks, num_bands, sigma=sigma, which=which, want_vectors=want_vectors, ctx=ctx)
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
     ks = _ks(ks, Hd.d)
@@ -312,11 +319,39 @@ def getbands(H, ks, projectors=(), multimode="cuda", ctx=None):
     return BandData(bands, obs, ks)
 
 
+_WHICH = {"LM": 0, "SR": 1, "LR": 2}
+
+
+def _which(which):
+    key = str(which).lstrip(":")
+    if key not in _WHICH:
+        raise ValueError(f"which={which!r}: use :LM, :SR or :LR")
+    return _WHICH[key]
+
+
+def bandmatrix_partial(H, ks, num_bands, sigma=1e-8, which="LM", want_vectors=False, ctx=None):
+    """``bandmatrix(H, ks; format=:sparse, num_bands, sigma, which)``: per k the
+    ``num_bands`` eigenvalues nearest ``sigma`` (:LM), smallest (:SR) or largest (:LR),
+    ascending; bands (num_bands, nk) and optionally U (n, num_bands, nk)
+    (``lqm_bandmatrix_partial``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    nk = ks.shape[1]
+    bands = np.zeros((int(num_bands), nk), order="F")
+    U = np.zeros((Hd.n, int(num_bands), nk), dtype=np.complex128, order="F") if want_vectors else None
+    ctx.check(_lib.lqm_bandmatrix_partial(ctx.handle, Hd.handle, nk, _ptr(ks), int(num_bands), float(sigma),
+                                          _which(which), int(bool(want_vectors)), _ptr(bands), _ptr(U)))
+    return bands, U
+
+
 def getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, multimode="cuda", precision=0,
-                     ctx=None):
-    """``getdensitymatrix!(ρs, H, ks[, kweights], μ; T)``: overwrites every block of
-    ``rhos`` (dict keyed like Hops; only its existing keys are computed) and returns
-    the band energy sum_k w_k sum_n f eps."""
+                     ctx=None, format="dense", num_bands=None, sigma=1e-8, which="LM"):
+    """``getdensitymatrix!(ρs, H, ks[, kweights], μ; T[, format=:sparse, num_bands])``:
+    overwrites every block of ``rhos`` (dict keyed like Hops; only its existing keys are
+    computed) and returns the band energy sum_k w_k sum_n f eps.  With
+    ``format="sparse"`` only the ``num_bands`` states selected as in
+    ``bandmatrix_partial`` enter (``lqm_densitymatrix_partial``)."""
     _check_mode(multimode)
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
@@ -328,8 +363,14 @@ def getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, multimode="cuda
     w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
     out = np.zeros((Hd.n, Hd.n, nL), dtype=np.complex128, order="F")
     eb = _D()
-    ctx.check(_lib.lqm_densitymatrix(ctx.handle, Hd.handle, nk, _ptr(ks), _ptr(w), float(mu), float(T),
-                                     nL, _ptr(Lk), _ptr(out), ctypes.byref(eb), int(precision)))
+    if str(format).lstrip(":") == "sparse":
+        nbands = Hd.n if num_bands is None else int(num_bands)
+        ctx.check(_lib.lqm_densitymatrix_partial(ctx.handle, Hd.handle, nk, _ptr(ks), _ptr(w), float(mu),
+                                                 float(T), nbands, float(sigma), _which(which), nL, _ptr(Lk),
+                                                 _ptr(out), ctypes.byref(eb)))
+    else:
+        ctx.check(_lib.lqm_densitymatrix(ctx.handle, Hd.handle, nk, _ptr(ks), _ptr(w), float(mu), float(T),
+                                         nL, _ptr(Lk), _ptr(out), ctypes.byref(eb), int(precision)))
     for i, L in enumerate(Lkeys):
         rhos[L] = np.array(out[:, :, i])
     return eb.value

@@ -238,6 +238,57 @@ def densitymatrix(h, ks, w, mu, T, Lkeys, return_parts=False):
     return rho, eband
 
 
+def select_window(e, num_bands, sigma=1e-8, which="LM"):
+    """Indices of the eigenpairs eigen_sparse returns (Eigen/eigen_sparse_krylovkit.jl:44-88),
+    ascending: the num_bands eigenvalues nearest sigma (:LM; shift-invert Lanczos
+    converged to its 1e-12 tolerance returns exactly those), the smallest (:SR) or the
+    largest (:LR).  On a tie in distance the lower eigenvalue is taken (KrylovKit leaves
+    ties unspecified; the reference's default sigma = 1e-8 avoids the symmetric ones)."""
+    n = len(e)
+    which = str(which).lstrip(":")
+    if which == "SR":
+        return np.arange(num_bands)
+    if which == "LR":
+        return np.arange(n - num_bands, n)
+    order = sorted(range(n), key=lambda i: (abs(e[i] - sigma), e[i]))
+    return np.sort(np.array(order[:num_bands]))
+
+
+def bandmatrix_partial(h, ks, num_bands, sigma=1e-8, which="LM", vectors=False):
+    """bandmatrix(H, ks; format=:sparse, num_bands) (Spectrum/bands.jl:78-87 with
+    Eigen/Eigen.jl:35-39): bands (num_bands, nk), optionally U (nk, n, num_bands)."""
+    n = next(iter(h.values())).shape[0]
+    nk = ks.shape[1]
+    bands = np.zeros((num_bands, nk))
+    U = np.zeros((nk, n, num_bands), complex) if vectors else None
+    for j in range(nk):
+        e, u = eigh_upper(fouriersum(h, ks[:, j]), True)
+        idx = select_window(e, num_bands, sigma, which)
+        bands[:, j] = e[idx]
+        if vectors:
+            U[j] = u[:, idx]
+    return bands, U
+
+
+def densitymatrix_partial(h, ks, w, mu, T, Lkeys, num_bands, sigma=1e-8, which="LM"):
+    """getdensitymatrix! with format=:sparse (Operators/densitymatrix.jl:100-104,131-147):
+    rho_k = U_w f U_w^dagger over the selected states only."""
+    n = next(iter(h.values())).shape[0]
+    rho = {L: np.zeros((n, n), complex) for L in Lkeys}
+    eband = 0.0
+    for j in range(ks.shape[1]):
+        k = ks[:, j]
+        e, U = eigh_upper(fouriersum(h, k), True)
+        idx = select_window(e, num_bands, sigma, which)
+        e, U = e[idx], U[:, idx]
+        f = fermidirac(e, mu, T)
+        rk = (U * f[None, :]) @ U.conj().T
+        for L in Lkeys:
+            rho[L] += w[j] * np.exp(-1j * 2 * math.pi * float(np.dot(k, np.array(L, float)))) * rk
+        eband += float(np.real(w[j] * np.sum(e * f)))
+    return rho, eband
+
+
 def dos(h, ks, omegas, gamma, w=None):
     """DOS(w) = sum_k w_k sum_n Im[1/(w - i Gamma - eps)], /L when unweighted.
     Spectrum/dos.jl:185-188 (dos!) and :202-223 (dos_compute!)."""

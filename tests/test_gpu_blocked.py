@@ -255,3 +255,54 @@ def test_optical_conductivity_matches_oracle(lqm, ctx, bctx):
             assert np.max(np.abs(chi - ref)) <= 1e-9 * max(1.0, np.max(np.abs(ref)))
     finally:
         c1.close()
+
+
+def test_partial_spectrum_matches_oracle(lqm, ctx):
+    """bandmatrix / getdensitymatrix! with format=:sparse, num_bands through
+    lqm_bandmatrix_partial and lqm_densitymatrix_partial: the selection tests of
+    test/test_eigen.jl:11-85 (a seeded 60 x 60 matrix as a single-key Hops: :LM at
+    sigma = 0 and 0.2, :SR, :LR, ascending, residuals, determinism), the residual and
+    orthonormality contract of test/test_eigen.jl:42-65 on the twisted bilayer N = 5
+    (n = 364, blocked eigensolver) against the oracle, and the partial density matrix
+    on the disordered honeycomb 6x6 cell."""
+    rng = np.random.default_rng(0x123456789ABCDEF)
+    A = rng.random((60, 60)) - 0.5
+    A = np.triu(A) + np.triu(A, 1).T
+    h = {(0, 0): A.astype(complex)}
+    ks = np.zeros((2, 1))
+    e = np.sort(np.linalg.eigvalsh(A))
+    lm, _ = lqm.bandmatrix_partial(h, ks, 10, sigma=0.0, ctx=ctx)
+    assert np.allclose(lm[:, 0], np.sort(sorted(e, key=abs)[:10]), atol=1e-10)
+    sr, _ = lqm.bandmatrix_partial(h, ks, 10, which="SR", ctx=ctx)
+    lr, _ = lqm.bandmatrix_partial(h, ks, 10, which=":LR", ctx=ctx)
+    assert np.allclose(sr[:, 0], e[:10], atol=1e-10) and np.allclose(lr[:, 0], e[-10:], atol=1e-10)
+    for which, sig in (("LM", 0.2), ("SR", 1e-8), ("LR", 1e-8)):
+        b, U = lqm.bandmatrix_partial(h, ks, 6, sigma=sig, which=which, want_vectors=True, ctx=ctx)
+        assert np.all(np.diff(b[:, 0]) >= 0)
+        assert np.max(np.abs(A @ U[:, :, 0] - U[:, :, 0] * b[:, 0][None, :])) < 1e-8
+        ref, _ = K.bandmatrix_partial(h, ks, 6, sigma=sig, which=which)
+        assert np.max(np.abs(b - ref)) < 1e-10
+    b1, _ = lqm.bandmatrix_partial(h, ks, 4, ctx=ctx)
+    b2, _ = lqm.bandmatrix_partial(h, ks, 4, ctx=ctx)
+    assert np.array_equal(b1, b2)
+
+    lat = L.honeycomb_twisted(5)
+    ht = M.graphene(lat)
+    kp = L.kpath(lat, 4)[:, 1:3]
+    b, U = lqm.bandmatrix(ht, kp, format="sparse", num_bands=10, want_vectors=True, ctx=ctx)
+    ref, _ = K.bandmatrix_partial(ht, kp, 10)
+    assert rel_band_err(b, ref) <= BAND_TOL
+    for j in range(kp.shape[1]):
+        Hk = K.fouriersum(ht, kp[:, j])
+        Uj = U[:, :, j]
+        assert max(np.linalg.norm(Hk @ Uj[:, m] - b[m, j] * Uj[:, m]) for m in range(10)) < 1e-9
+        assert np.linalg.norm(Uj.conj().T @ Uj - np.eye(10), 2) < 1e-10
+
+    _, h6 = M.honeycomb_disorder(6)
+    ks6 = rng.uniform(-0.5, 0.5, (2, 16))
+    w6 = np.full(16, 1.0 / 16)
+    rho = {R: None for R in M.KEYS9}
+    eb = lqm.getdensitymatrix(rho, h6, ks6, mu=0.0, T=0.01, format="sparse", num_bands=24, ctx=ctx)
+    rref, ebref = K.densitymatrix_partial(h6, ks6, w6, 0.0, 0.01, M.KEYS9, 24)
+    assert max(np.max(np.abs(rho[R] - rref[R])) for R in M.KEYS9) <= RHO_TOL
+    assert abs(eb - ebref) <= 1e-10 * max(1.0, abs(ebref))

@@ -342,3 +342,27 @@ def test_optical_conductivity_graphene_invariants():
     assert np.max(np.abs(sig[0, 1].real)) < 1e-10
     assert np.all(sig[0, 0].real > -1e-6)
     assert np.max(sig[0, 0].real) > 1e-3  # an interband response is present
+
+
+def test_partial_spectrum_selection_rules():
+    """test/test_eigen.jl:11-40,69-85 restated on the oracle's window selection: :LM at
+    sigma=0 gives the num_bands eigenvalues of smallest modulus, :SR/:LR the ends of the
+    spectrum, all ascending (a seeded 60 x 60 real symmetric matrix, entries U(-0.5, 0.5),
+    stands in for the reference's Xoshiro draw)."""
+    rng = np.random.default_rng(0x123456789ABCDEF)
+    A = rng.random((60, 60)) - 0.5
+    A = np.triu(A) + np.triu(A, 1).T
+    h = {(0, 0): A.astype(complex)}
+    ks = np.zeros((2, 1))
+    e = np.sort(np.linalg.eigvalsh(A))
+    lm, _ = K.bandmatrix_partial(h, ks, 10, sigma=0.0)
+    assert np.allclose(lm[:, 0], np.sort(sorted(e, key=abs)[:10]), atol=1e-12)
+    sr, _ = K.bandmatrix_partial(h, ks, 10, which="SR")
+    lr, _ = K.bandmatrix_partial(h, ks, 10, which="LR")
+    assert np.allclose(sr[:, 0], e[:10], atol=1e-12) and np.allclose(lr[:, 0], e[-10:], atol=1e-12)
+    for which, sig in (("LM", 0.2), ("SR", 1e-8), ("LR", 1e-8)):
+        b, U = K.bandmatrix_partial(h, ks, 6, sigma=sig, which=which, vectors=True)
+        assert np.all(np.diff(b[:, 0]) >= 0)
+        assert np.max(np.abs(A @ U[0] - U[0] * b[:, 0][None, :])) < 1e-10
+    # a tie in distance takes the lower eigenvalue
+    assert list(K.select_window(np.array([-1.0, 1.0, 3.0]), 1, sigma=0.0)) == [0]
