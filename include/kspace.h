@@ -58,6 +58,11 @@ int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
  * (src/modules/Meanfield/fixedpoint.jl:39-194,201-231: acceleration=:anderson,
  * anderson_depth), including its Hermitian projection of each iterate. */
 int lqm_ctx_set_scf_acceleration(lqm_ctx* ctx, int anderson_depth);
+/* SCF residual of lqm_scf_hf on this context: 0 (default) the relative density
+ * change ||rho1 - rho0|| / ||rho1|| (fixedpoint.jl:150-156), 1 the commutator
+ * norm ||[H_MF[rho0], rho0]||_F over the SCF's k-points with weights 1/nk
+ * (src/modules/Meanfield/selfconsistent.jl:399-405, residual_norm=:commutator). */
+int lqm_ctx_set_scf_residual(lqm_ctx* ctx, int mode);
 /* Milliseconds of device time of the last call's kernels (CUDA events). */
 int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
 
@@ -201,6 +206,13 @@ int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int6
  * det(S^H S')/|det|, and F[i + (NX-1) j] = arg(plaquette product)/(2 pi) for
  * the (NX-1) x (NY-1) plaquettes.  Two-dimensional Hops only. */
 int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, double* F);
+
+/* Commutator norm ||[H, rho]||_F = sqrt(sum_k w_k ||H(k) rho(k) - rho(k) H(k)||_F^2),
+ * commutator_kspace_norm (src/modules/Meanfield/selfconsistent.jl:130-166);
+ * w NULL means 1/nk.  H and rho are Hops of the same order and key dimension
+ * (their key sets may differ). */
+int lqm_commutator_norm(lqm_ctx* ctx, const lqm_hops* H, const lqm_hops* rho, int64_t nk, const double* ks,
+                        const double* w, double* out);
 
 /* Partial spectrum, the `format=:sparse, num_bands` path of bandmatrix and
  * getdensitymatrix! (src/modules/Eigen/eigen_sparse_krylovkit.jl:44-88,

@@ -64,6 +64,7 @@ struct lqm_ctx {
   cublasHandle_t blas = nullptr;          // batched GEMMs of the blocked large-n path
   int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: the default switch)
   int scf_anderson_depth = 0;             // SCF acceleration: 0 linear mixing, > 0 Anderson history depth
+  int scf_residual = 0;                   // SCF residual: 0 relative density change, 1 commutator norm
 };
 
 struct lqm_hops {
@@ -651,6 +652,12 @@ int lqm_ctx_set_scf_acceleration(lqm_ctx* ctx, int anderson_depth) {
   return LQM_OK;
 }
 
+int lqm_ctx_set_scf_residual(lqm_ctx* ctx, int mode) {
+  if (!ctx || mode < 0 || mode > 1) return LQM_EINVAL;
+  ctx->scf_residual = mode;
+  return LQM_OK;
+}
+
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min) {
   if (!ctx || n_min < 0) return LQM_EINVAL;
   ctx->blocked_min_n = n_min;
@@ -985,6 +992,7 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 
 }  // extern "C"
 
+#include "lqm_commutator.inc"
 #include "lqm_anderson.inc"
 #include "lqm_scf.inc"
 #include "lqm_adjoint.inc"

@@ -309,15 +309,21 @@ function _log_trampoline(it::Int64, E::Float64, res::Float64, ekin::Float64, eba
     Cint(0)
 end
 
-"""Device-resident `solvehartreefock` with linear mixing; returns (ρ, ϵ_GS, info, converged, residual)."""
+"""Device-resident `solvehartreefock` (linear mixing or Anderson acceleration; density or
+commutator residual); returns (ρ, ϵ_GS, info, converged, residual)."""
 function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractMatrix{Float64}, exec::CudaExec;
                                T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
-                               log_callback=nothing, acceleration::Symbol=:linear, anderson_depth::Int=5)
+                               log_callback=nothing, acceleration::Symbol=:linear, anderson_depth::Int=5,
+                               residual_norm::Symbol=:density)
     ctx = context(exec.device)
     acceleration in (:linear, :anderson) ||
         throw(ArgumentError("acceleration must be :linear or :anderson, got $(acceleration)"))
+    residual_norm in (:density, :commutator) ||
+        throw(ArgumentError("residual_norm must be :density or :commutator, got $(residual_norm)"))
     depth = acceleration === :anderson ? anderson_depth : 0
     check(ctx, ccall((:lqm_ctx_set_scf_acceleration, LIB[]), Cint, (Ptr{Cvoid}, Cint), ctx.ptr, depth))
+    check(ctx, ccall((:lqm_ctx_set_scf_residual, LIB[]), Cint, (Ptr{Cvoid}, Cint), ctx.ptr,
+                     residual_norm === :commutator ? 1 : 0))
     dh = upload(ctx, h)
     dv = upload(ctx, v)
     Lk = collect(keys(ρ_init))
@@ -341,6 +347,20 @@ function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractM
     ρ = Hops(Dict(k => rho[:, :, i] for (i, k) in enumerate(Lk)))
     info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
     ρ, out[1], info, out[8] != 0, out[7]
+end
+
+"""`commutator_kspace_norm(H, ρ, ks; kweights)` (Meanfield/selfconsistent.jl:130-166) on the
+device (`lqm_commutator_norm`)."""
+function cuda_commutator_kspace_norm(H, ρ, ks::AbstractMatrix{Float64}, exec::CudaExec;
+                                     kweights::Union{Nothing,AbstractVector{Float64}}=nothing)
+    ctx = context(exec.device)
+    dh, dr = upload(ctx, H), upload(ctx, ρ)
+    out = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_commutator_norm, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Ref{Float64}),
+        ctx.ptr, dh.ptr, dr.ptr, size(ks, 2), Matrix{Float64}(ks),
+        kweights === nothing ? Ptr{Float64}(C_NULL) : Vector{Float64}(kweights), out))
+    out[]
 end
 
 # ---------------------------------------------------------------- derivatives

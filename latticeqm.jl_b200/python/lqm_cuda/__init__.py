@@ -41,6 +41,7 @@ EXPORTS = [
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
     "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
+    "lqm_commutator_norm", "lqm_ctx_set_scf_residual",
 ]
 
 
@@ -93,6 +94,8 @@ _SIG = {
     "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
+    "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
+    "lqm_ctx_set_scf_residual": [_P, ctypes.c_int],
     "lqm_bandmatrix_partial": [_P, _P, _I64, _P, _I64, _D, ctypes.c_int, ctypes.c_int, _P, _P],
     "lqm_densitymatrix_partial": [_P, _P, _I64, _P, _P, _D, _D, _I64, _D, ctypes.c_int, _I64, _P, _P,
                                   ctypes.POINTER(_D)],
@@ -468,6 +471,22 @@ def opticalconductivity(frequencies, H, J1, J2, ks, mu=0.0, Gamma=0.025, T=0.1, 
     return out
 
 
+def commutator_kspace_norm(H, rho, ks, kweights=None, multimode="cuda", ctx=None):
+    """``commutator_kspace_norm(H, ρ, ks; kweights)`` (Meanfield/selfconsistent.jl:130-166):
+    sqrt(sum_k w_k ||H(k) ρ(k) - ρ(k) H(k)||_F^2), w = 1/nk by default
+    (``lqm_commutator_norm``)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    Rd = _as_device_hops(rho, ctx)
+    ks = _ks(ks, Hd.d)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = _D()
+    ctx.check(_lib.lqm_commutator_norm(ctx.handle, Hd.handle, Rd.handle, ks.shape[1], _ptr(ks), _ptr(w),
+                                       ctypes.byref(out)))
+    return out.value
+
+
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):
     """``chemicalpotential(H, ks, filling; T)``."""
     _check_mode(multimode)
@@ -526,16 +545,23 @@ MFInfo = namedtuple("MFInfo", ["mu", "eH", "eF", "eband", "ekin", "iterations"])
 
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
                      kweights=None, log_callback=None, multimode="cuda", ctx=None, acceleration="linear",
-                     anderson_depth=5):
+                     anderson_depth=5, residual_norm="density"):
     """``solvehartreefock(h, v, ρ_init, filling, ks; T, β, tol, iterations, acceleration,
-    anderson_depth)``: linear damped mixing (default) or Anderson acceleration.
-    Returns (ρ, ϵ_GS, mf, converged, residual) like the reference."""
+    anderson_depth, residual_norm)``: linear damped mixing (default) or Anderson
+    acceleration; the relative density change (default) or the commutator norm
+    ||[H_MF, ρ]|| as the residual.  Returns (ρ, ϵ_GS, mf, converged, residual) like the
+    reference."""
     _check_mode(multimode)
+    acceleration = str(acceleration).lstrip(":")
+    residual_norm = str(residual_norm).lstrip(":")
     if acceleration not in ("linear", "anderson"):
         raise ValueError(f"acceleration must be 'linear' or 'anderson', got {acceleration!r}")
+    if residual_norm not in ("density", "commutator"):
+        raise ValueError(f"residual_norm must be :density or :commutator, got {residual_norm!r}")
     ctx = ctx or default_context()
     depth = int(anderson_depth) if acceleration == "anderson" else 0
     ctx.check(_lib.lqm_ctx_set_scf_acceleration(ctx.handle, depth))
+    ctx.check(_lib.lqm_ctx_set_scf_residual(ctx.handle, 1 if residual_norm == "commutator" else 0))
     hd = _as_device_hops(h, ctx)
     vd = _as_device_hops(v, ctx)
     ks = _ks(ks, hd.d)

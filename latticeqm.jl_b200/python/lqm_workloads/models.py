@@ -260,6 +260,27 @@ def triangular_hubbard(L_super=6, t=-1.0, tp=0.2, U=4.0):
     return lat, h, v
 
 
+def antiferro_density(lat):
+    """``initialguess(v, :antiferro; lat)`` (Meanfield/initialguess.jl:186-193):
+    rho_0 = kron(P_A, rho_up) + kron(P_B, sigma0 - rho_up), rho_up = diag(1, 0), P_A/P_B the
+    projectors on sublattice 0/1 (spin the fast index)."""
+    sub = lat.extracoord("sublattice")
+    up = np.diag([1.0, 0.0]).astype(complex)
+    PA = np.diag((sub == 0).astype(float))
+    PB = np.diag((sub == 1).astype(float))
+    return np.kron(PA, up) + np.kron(PB, SIGMA0 - up)
+
+
+def graphene_hubbard(U=4.0):
+    """The commutator-residual SCF case of test/test_meanfield.jl:84-112: spinful
+    ``Operators.graphene`` on the honeycomb cell, Hubbard v (mode sigma_x, a = 0.5, U)
+    and the antiferromagnetic initial guess (n = 4)."""
+    lat = L.honeycomb()
+    h = graphene(lat, spin=True)
+    v = hubbard_v(lat, U=U, a=0.5)
+    return lat, h, v, {(0, 0): antiferro_density(lat)}
+
+
 def random_local_magnetization(n_sites, seed=3):
     """Seeded ``mapspindensitymatrix(:random, n)`` (Meanfield/initialguess.jl:24-35,48-58,
     68-80): per site 1/2 (sigma0 + d.sigma) with a random unit vector d."""

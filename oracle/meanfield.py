@@ -1,4 +1,6 @@
 """Hartree-Fock SCF restated from LatticeQM.jl (oracle; test infrastructure only)."""
+import math
+
 import numpy as np
 
 from . import kspace as K
@@ -95,15 +97,50 @@ def _unflatten(rho, flat, keys):
         off += sz
 
 
+def commutator_kspace_norm(H, rho, ks, w=None):
+    """Meanfield/selfconsistent.jl:130-166: sqrt(sum_k w_k ||H(k) rho(k) - rho(k) H(k)||_F^2),
+    w = 1/nk by default."""
+    nk = ks.shape[1]
+    w = np.full(nk, 1.0 / nk) if w is None else w
+    s = 0.0
+    for j in range(nk):
+        Hk = K.fouriersum(H, ks[:, j])
+        Rk = K.fouriersum(rho, ks[:, j])
+        C = Hk @ Rk - Rk @ Hk
+        s += w[j] * float(np.sum(np.abs(C) ** 2))
+    return math.sqrt(s)
+
+
+def enrichkeys(rho, klin):
+    """Meanfield/initialguess.jl:262-277 (enrichkeys!): add zero blocks for every key of
+    {-klin//2 .. klin//2}^d (first index fastest) that rho lacks."""
+    sample = next(iter(rho.values()))
+    d = len(next(iter(rho.keys())))
+    Lmax = klin // 2
+    for L in _product_first_fastest([range(-Lmax, Lmax + 1)] * d):
+        if L not in rho:
+            rho[L] = np.zeros_like(sample)
+    return rho
+
+
+def _product_first_fastest(ranges):
+    out = [()]
+    for r in ranges:
+        out = [o + (x,) for x in r for o in out]
+    return out
+
+
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
-                     iterations=500, log=None, acceleration="linear", anderson_depth=5):
+                     iterations=500, log=None, acceleration="linear", anderson_depth=5,
+                     residual_norm="density"):
     """solvehartreefock -> _scf_driver! -> fixedpoint!.
 
     Meanfield/selfconsistent.jl:19,62-69,256-336,366-381 and fixedpoint.jl:39-194.
     Each iteration: hf(rho0); mu from the eigenvalues of hMF on every k;
     rho1 = getdensitymatrix!(hMF, mu); linear mixing (or, with
     acceleration="anderson", the Anderson update of fixedpoint.jl:64-142 with
-    its Hermitian projection) and the relative residual."""
+    its Hermitian projection) and the relative residual (or, with
+    residual_norm="commutator", ||[hMF, rho0]|| of selfconsistent.jl:399-405)."""
     use_anderson = acceleration == "anderson" and anderson_depth > 0
     hist_x, hist_f = [], []
     rho0 = {L: M.copy() for L, M in rho_init.items()}
@@ -120,6 +157,7 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
     while it < iterations:
         it += 1
         hf(rho0)
+        comm = commutator_kspace_norm(hf.hMF, rho0, ks) if residual_norm == "commutator" else None
         bands, _ = K.bandmatrix(hf.hMF, ks)
         hf.mu = K.chemicalpotential(bands, filling, T)
         rho_new, eband = K.densitymatrix(hf.hMF, ks, w, hf.mu, T, list(rho1.keys()))
@@ -146,6 +184,8 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
             diff = np.linalg.norm([np.linalg.norm(rho1[L] - rho0[L]) for L in rho0])
             nrm = np.linalg.norm([np.linalg.norm(rho1[L]) for L in rho0])
         residual = diff / nrm if nrm > np.finfo(float).eps else diff
+        if comm is not None:  # selfconsistent.jl:399-405, evaluated before the mixing
+            residual = comm
         for L in rho0:
             rho0[L] = rho1[L].copy()
         if log is not None:

@@ -285,3 +285,36 @@ def test_hubbard_scf_anderson_matches_oracle(lqm, ctx):
     assert np.max(np.abs(res.rho[(0, 0)] - rho_ref[(0, 0)])) <= 1e-8
     assert abs(res.energy - E_ref) <= 1e-8
     assert abs(res.residual - resid) <= 1e-8 * max(1.0, resid)
+
+
+def test_commutator_residual_scf_matches_oracle(lqm, ctx):
+    """residual_norm = :commutator (selfconsistent.jl:130-166,399-405) through
+    lqm_ctx_set_scf_residual: the commutatorresidual case of test/test_meanfield.jl:84-112
+    (graphene Hubbard U = 4, antiferromagnetic guess, klin = 9 Wigner-Seitz keys, Anderson
+    depth 5) converges below 1e-7 with a residual drop above 1e6, in the oracle's iteration
+    count and energy; and lqm_commutator_norm against the oracle on a random rho."""
+    _, h, v, rho0 = M.graphene_hubbard(4.0)
+    MF.enrichkeys(rho0, 9)
+    ks = L.regulargrid(9 * 9)
+    kw = dict(T=0.01, beta=1.0, tol=1e-7, iterations=50, acceleration="anderson", anderson_depth=5,
+              residual_norm="commutator")
+    log = []
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, log_callback=lambda i, e, r, d: log.append(r), **kw)
+    rho_ref, E_ref, _, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, **kw)
+    assert res.converged and res.residual < 1e-7 and conv
+    assert log[0] / log[-1] > 1e6
+    assert res.mf.iterations == it
+    assert abs(res.energy - E_ref) <= 1e-8
+
+    _, h6 = M.honeycomb_disorder(6)
+    rng = np.random.default_rng(5)
+    n6 = h6[(0, 0)].shape[0]
+    rho = {}
+    for R in M.KEYS9:
+        X = rng.normal(size=(n6, n6)) + 1j * rng.normal(size=(n6, n6))
+        rho[R] = X
+    rho = MF.hermitianize(rho)
+    ks6 = rng.uniform(-0.5, 0.5, (2, 12))
+    c = lqm.commutator_kspace_norm(h6, rho, ks6, ctx=ctx)
+    c_ref = MF.commutator_kspace_norm(h6, rho, ks6)
+    assert abs(c - c_ref) <= 1e-12 * c_ref
