@@ -63,6 +63,21 @@ int lqm_ctx_set_scf_acceleration(lqm_ctx* ctx, int anderson_depth);
  * norm ||[H_MF[rho0], rho0]||_F over the SCF's k-points with weights 1/nk
  * (src/modules/Meanfield/selfconsistent.jl:399-405, residual_norm=:commutator). */
 int lqm_ctx_set_scf_residual(lqm_ctx* ctx, int mode);
+/* Terms of the HartreeFock functional used by lqm_scf_hf and lqm_hartreefock_eval
+ * on this context, HartreeFock(h, v; hartree, fock) (src/modules/Meanfield/hartreefock.jl:143-175):
+ * nonzero switches the Hartree / Fock field on (both on by default). */
+int lqm_ctx_set_scf_terms(lqm_ctx* ctx, int hartree, int fock);
+/* ExchangeKernel(j, siteof, flavorof) of the J-augmented functional
+ * (src/modules/Meanfield/hartreefock.jl:24-76,298-381) for the following SCF and
+ * functional evaluations on this context: j is a site-space Hops given on the
+ * host (keys d x nJ, blocks ns x ns x nJ complex, column-major; the zero key
+ * present, its diagonal zero); siteof/flavorof (length n, 0-based) map each
+ * orbital to its site and flavor, every pair once.  ns = 0 removes the kernel.
+ * The exchange energy eJ enters the double counting (E = eband - eH - eF - eJ);
+ * lqm_ctx_scf_exchange_energy returns the last SCF's eJ. */
+int lqm_ctx_set_scf_exchange(lqm_ctx* ctx, int64_t ns, int64_t nJ, int32_t d, const int64_t* jkeys,
+                             const double* jblocks, int64_t n, const int64_t* siteof, const int64_t* flavorof);
+int lqm_ctx_scf_exchange_energy(const lqm_ctx* ctx, double* eJ);
 /* Milliseconds of device time of the last call's kernels (CUDA events). */
 int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
 
@@ -206,6 +221,15 @@ int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int6
  * det(S^H S')/|det|, and F[i + (NX-1) j] = arg(plaquette product)/(2 pi) for
  * the (NX-1) x (NY-1) plaquettes.  Two-dimensional Hops only. */
 int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, double* F);
+
+/* The HartreeFock functional hf(rho) (src/modules/Meanfield/hartreefock.jl:184-228,
+ * 247-289,298-410): hMF = h - v .* rho (Fock) + the Hartree diagonal (+ the
+ * exchange fields of the context's ExchangeKernel), with the context's terms.
+ * rho: n x n x nL for keys Lkeys (d x nL, the zero key present).  hmf_out
+ * receives hMF at the nM keys Mkeys (zero blocks for keys outside hMF's key set
+ * keys(h) + keys(v) + exchange keys present in rho); energies = {eH, eF, eJ}. */
+int lqm_hartreefock_eval(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nL, const int64_t* Lkeys,
+                         const double* rho, int64_t nM, const int64_t* Mkeys, double* hmf_out, double* energies);
 
 /* Commutator norm ||[H, rho]||_F = sqrt(sum_k w_k ||H(k) rho(k) - rho(k) H(k)||_F^2),
  * commutator_kspace_norm (src/modules/Meanfield/selfconsistent.jl:130-166);

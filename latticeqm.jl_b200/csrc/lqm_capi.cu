@@ -53,7 +53,7 @@ struct lqm_ctx {
   int num_sms = 0;
   double last_ms = 0.0;
   std::map<int, PlanDev> plans;
-  DevBuf ws[32];
+  DevBuf ws[40];
   // per-kernel device-time statistics (CUDA events on the context stream)
   bool stats_on = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending, ev_pool;
@@ -65,6 +65,14 @@ struct lqm_ctx {
   int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: the default switch)
   int scf_anderson_depth = 0;             // SCF acceleration: 0 linear mixing, > 0 Anderson history depth
   int scf_residual = 0;                   // SCF residual: 0 relative density change, 1 commutator norm
+  bool scf_hartree = true, scf_fock = true;  // HartreeFock(h, v; hartree, fock)
+  // ExchangeKernel(j, siteof, flavorof) of the next SCF calls (ns == 0: none)
+  int64_t ex_ns = 0, ex_nf = 0, ex_nJ = 0;
+  int ex_d = 0;
+  std::vector<int64_t> ex_keys;   // d x nJ
+  std::vector<double> ex_blocks;  // ns x ns x nJ complex (interleaved)
+  std::vector<int> ex_sf2idx;     // ns x nf, column-major: (site a, flavor f) -> orbital
+  double scf_eJ = 0.0;            // exchange energy of the last SCF
 };
 
 struct lqm_hops {
@@ -162,9 +170,9 @@ void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART
 };
-static_assert(WS_AND < 32, "workspace slots");
+static_assert(WS_HFPART < 40, "workspace slots");
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
 const DCPlan& get_plan(lqm_ctx* ctx, int n) {
@@ -655,6 +663,68 @@ int lqm_ctx_set_scf_acceleration(lqm_ctx* ctx, int anderson_depth) {
 int lqm_ctx_set_scf_residual(lqm_ctx* ctx, int mode) {
   if (!ctx || mode < 0 || mode > 1) return LQM_EINVAL;
   ctx->scf_residual = mode;
+  return LQM_OK;
+}
+
+int lqm_ctx_set_scf_terms(lqm_ctx* ctx, int hartree, int fock) {
+  if (!ctx) return LQM_EINVAL;
+  ctx->scf_hartree = hartree != 0;
+  ctx->scf_fock = fock != 0;
+  return LQM_OK;
+}
+
+int lqm_ctx_set_scf_exchange(lqm_ctx* ctx, int64_t ns, int64_t nJ, int32_t d, const int64_t* jkeys,
+                             const double* jblocks, int64_t n, const int64_t* siteof, const int64_t* flavorof) {
+  return guarded(ctx, [&] {
+    if (ns == 0) {  // no exchange kernel
+      ctx->ex_ns = ctx->ex_nf = ctx->ex_nJ = 0;
+      ctx->ex_keys.clear();
+      ctx->ex_blocks.clear();
+      ctx->ex_sf2idx.clear();
+      return;
+    }
+    if (ns < 1 || nJ < 1 || d < 1 || d > 3 || !jkeys || !jblocks || n < 1 || !siteof || !flavorof)
+      fail(LQM_EINVAL, "invalid exchange kernel arguments");
+    // ExchangeKernel(j, siteof, flavorof), hartreefock.jl:47-76 (0-based sites and flavors here)
+    int64_t nf = 0;
+    for (int64_t I = 0; I < n; ++I) {
+      if (siteof[I] < 0 || siteof[I] >= ns) fail(LQM_EINVAL, "siteof[%lld] outside 0..%lld", (long long)I, (long long)(ns - 1));
+      if (flavorof[I] < 0) fail(LQM_EINVAL, "flavorof[%lld] is negative", (long long)I);
+      nf = std::max<int64_t>(nf, flavorof[I] + 1);
+    }
+    if (ns * nf != n) fail(LQM_EINVAL, "every (site, flavor) pair must appear once");
+    std::vector<int> sf((size_t)(ns * nf), -1);
+    for (int64_t I = 0; I < n; ++I) {
+      int& slot = sf[(size_t)(siteof[I] + ns * flavorof[I])];
+      if (slot >= 0) fail(LQM_EINVAL, "duplicate (site, flavor) = (%lld, %lld)", (long long)siteof[I], (long long)flavorof[I]);
+      slot = (int)I;
+    }
+    check_finite(jblocks, 2 * ns * ns * nJ, "exchange kernel");
+    int64_t z = -1;
+    for (int64_t l = 0; l < nJ && z < 0; ++l) {
+      bool zero = true;
+      for (int c = 0; c < d; ++c) zero = zero && jkeys[l * d + c] == 0;
+      if (zero) z = l;
+    }
+    if (z < 0) fail(LQM_EINVAL, "the exchange kernel needs the zero key");
+    for (int64_t a = 0; a < ns; ++a) {
+      const double* e = jblocks + 2 * (z * ns * ns + a + a * ns);
+      if (e[0] != 0.0 || e[1] != 0.0)
+        fail(LQM_EINVAL, "onsite self-exchange j[0][a,a] must be zero (it is part of the direct interaction)");
+    }
+    ctx->ex_ns = ns;
+    ctx->ex_nf = nf;
+    ctx->ex_nJ = nJ;
+    ctx->ex_d = d;
+    ctx->ex_keys.assign(jkeys, jkeys + nJ * d);
+    ctx->ex_blocks.assign(jblocks, jblocks + 2 * ns * ns * nJ);
+    ctx->ex_sf2idx = sf;
+  });
+}
+
+int lqm_ctx_scf_exchange_energy(const lqm_ctx* ctx, double* eJ) {
+  if (!ctx || !eJ) return LQM_EINVAL;
+  *eJ = ctx->scf_eJ;
   return LQM_OK;
 }
 

@@ -309,13 +309,46 @@ function _log_trampoline(it::Int64, E::Float64, res::Float64, ekin::Float64, eba
     Cint(0)
 end
 
+"""Install `HartreeFock(h, v; hartree, fock, exchange)`'s terms on the context
+(`lqm_ctx_set_scf_terms`, `lqm_ctx_set_scf_exchange`; `exchange` an `ExchangeKernel` or
+`nothing`)."""
+function set_functional!(ctx::Context, hartree::Bool, fock::Bool, exchange)
+    check(ctx, ccall((:lqm_ctx_set_scf_terms, LIB[]), Cint, (Ptr{Cvoid}, Cint, Cint), ctx.ptr, hartree, fock))
+    if exchange === nothing
+        check(ctx, ccall((:lqm_ctx_set_scf_exchange, LIB[]), Cint,
+            (Ptr{Cvoid}, Int64, Int64, Int32, Ptr{Int64}, Ptr{ComplexF64}, Int64, Ptr{Int64}, Ptr{Int64}),
+            ctx.ptr, 0, 0, 0, C_NULL, C_NULL, 0, C_NULL, C_NULL))
+        return nothing
+    end
+    jk = collect(keys(exchange.j))
+    d = length(first(jk))
+    ns, nf = size(exchange.sf2idx)
+    K = Int64[k[i] for i in 1:d, k in jk]
+    B = Array{ComplexF64}(undef, ns, ns, length(jk))
+    for (r, k) in enumerate(jk)
+        B[:, :, r] .= exchange.j[k]
+    end
+    siteof = zeros(Int64, ns * nf)
+    flavorof = zeros(Int64, ns * nf)
+    for a in 1:ns, f in 1:nf
+        siteof[exchange.sf2idx[a, f]] = a - 1
+        flavorof[exchange.sf2idx[a, f]] = f - 1
+    end
+    check(ctx, ccall((:lqm_ctx_set_scf_exchange, LIB[]), Cint,
+        (Ptr{Cvoid}, Int64, Int64, Int32, Ptr{Int64}, Ptr{ComplexF64}, Int64, Ptr{Int64}, Ptr{Int64}),
+        ctx.ptr, ns, length(jk), d, K, B, ns * nf, siteof, flavorof))
+    nothing
+end
+
 """Device-resident `solvehartreefock` (linear mixing or Anderson acceleration; density or
 commutator residual); returns (ρ, ϵ_GS, info, converged, residual)."""
 function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractMatrix{Float64}, exec::CudaExec;
                                T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
                                log_callback=nothing, acceleration::Symbol=:linear, anderson_depth::Int=5,
-                               residual_norm::Symbol=:density)
+                               residual_norm::Symbol=:density, hartree::Bool=true, fock::Bool=true,
+                               exchange=nothing)
     ctx = context(exec.device)
+    set_functional!(ctx, hartree, fock, exchange)
     acceleration in (:linear, :anderson) ||
         throw(ArgumentError("acceleration must be :linear or :anderson, got $(acceleration)"))
     residual_norm in (:density, :commutator) ||
@@ -345,7 +378,9 @@ function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractM
         Float64(T), Float64(β), Float64(tol), iterations, length(Lk), L, rho, cb, C_NULL, out))
     LOG_CB[] = nothing
     ρ = Hops(Dict(k => rho[:, :, i] for (i, k) in enumerate(Lk)))
-    info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
+    eJ = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_ctx_scf_exchange_energy, LIB[]), Cint, (Ptr{Cvoid}, Ref{Float64}), ctx.ptr, eJ))
+    info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵJ=eJ[], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
     ρ, out[1], info, out[8] != 0, out[7]
 end
 

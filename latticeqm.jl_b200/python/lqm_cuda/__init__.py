@@ -41,7 +41,8 @@ EXPORTS = [
     "lqm_ctx_phase_cycles", "lqm_bandmatrix_noalloc", "lqm_densitymatrix_vjp", "lqm_bands_vjp",
     "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
-    "lqm_commutator_norm", "lqm_ctx_set_scf_residual",
+    "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
+    "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval",
 ]
 
 
@@ -96,6 +97,10 @@ _SIG = {
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
     "lqm_ctx_set_scf_residual": [_P, ctypes.c_int],
+    "lqm_ctx_set_scf_terms": [_P, ctypes.c_int, ctypes.c_int],
+    "lqm_ctx_set_scf_exchange": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _I64, _P, _P],
+    "lqm_ctx_scf_exchange_energy": [_P, ctypes.POINTER(_D)],
+    "lqm_hartreefock_eval": [_P, _P, _P, _I64, _P, _P, _I64, _P, _P, _P],
     "lqm_bandmatrix_partial": [_P, _P, _I64, _P, _I64, _D, ctypes.c_int, ctypes.c_int, _P, _P],
     "lqm_densitymatrix_partial": [_P, _P, _I64, _P, _P, _D, _D, _I64, _D, ctypes.c_int, _I64, _P, _P,
                                   ctypes.POINTER(_D)],
@@ -540,12 +545,70 @@ def bands_dos_rho(rhos, H, ks, omegas, gamma, kweights=None, mu=0.0, T=0.01, mul
 
 
 HFResult = namedtuple("HFResult", ["rho", "energy", "mf", "converged", "residual"])
-MFInfo = namedtuple("MFInfo", ["mu", "eH", "eF", "eband", "ekin", "iterations"])
+MFInfo = namedtuple("MFInfo", ["mu", "eH", "eF", "eband", "ekin", "iterations", "eJ"], defaults=(0.0,))
+
+
+class ExchangeKernel:
+    """``ExchangeKernel(j, siteof, flavorof)`` (Meanfield/hartreefock.jl:24-76) with 0-based
+    sites and flavors: ``j`` a site-space Hops (dict key -> ns x ns), ``siteof[I]`` and
+    ``flavorof[I]`` the site and flavor of orbital I.  Validated when it is installed
+    on a context."""
+
+    def __init__(self, j, siteof, flavorof):
+        self.j = {tuple(int(x) for x in L): np.asarray(M, np.complex128) for L, M in j.items()}
+        self.siteof = np.ascontiguousarray(siteof, dtype=np.int64)
+        self.flavorof = np.ascontiguousarray(flavorof, dtype=np.int64)
+        if len(self.siteof) != len(self.flavorof):
+            raise ValueError("siteof and flavorof must have equal length")
+
+    def install(self, ctx):
+        keys = list(self.j.keys())
+        d = len(keys[0])
+        ns = self.j[keys[0]].shape[0]
+        K = np.asfortranarray(np.array(keys, dtype=np.int64).T)
+        B = np.asfortranarray(np.stack([self.j[L] for L in keys], -1))
+        ctx.check(_lib.lqm_ctx_set_scf_exchange(ctx.handle, ns, len(keys), d, _ptr(K), _ptr(B), len(self.siteof),
+                                                _ptr(self.siteof), _ptr(self.flavorof)))
+
+
+def _set_functional(ctx, hartree, fock, exchange):
+    ctx.check(_lib.lqm_ctx_set_scf_terms(ctx.handle, int(bool(hartree)), int(bool(fock))))
+    if exchange is None:
+        ctx.check(_lib.lqm_ctx_set_scf_exchange(ctx.handle, 0, 0, 0, None, None, 0, None, None))
+    else:
+        exchange.install(ctx)
+
+
+def hartreefock_eval(h, v, rho, hartree=True, fock=True, exchange=None, keys=None, ctx=None):
+    """``hf(ρ)`` of ``HartreeFock(h, v; hartree, fock, exchange)``
+    (Meanfield/hartreefock.jl:184-228,247-410) on the device (``lqm_hartreefock_eval``):
+    returns (hMF dict, eH, eF, eJ); hMF on ``keys`` (default keys(h) + keys(v) + the
+    exchange keys present in rho)."""
+    ctx = ctx or default_context()
+    _set_functional(ctx, hartree, fock, exchange)
+    hd = _as_device_hops(h, ctx)
+    vd = _as_device_hops(v, ctx)
+    Lkeys = list(rho.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    R = np.asfortranarray(np.stack([np.asarray(rho[L], np.complex128) for L in Lkeys], -1))
+    if keys is None:
+        keys = list(hd.keys) if isinstance(h, DeviceHops) else [tuple(L) for L in h.keys()]
+        vkeys = vd.keys if isinstance(v, DeviceHops) else [tuple(L) for L in v.keys()]
+        keys += [L for L in vkeys if L not in keys]
+        if exchange is not None:
+            keys += [L for L in exchange.j if L in rho and L not in keys]
+    keys = [tuple(L) for L in keys]
+    Mk = np.asfortranarray(np.array(keys, dtype=np.int64).T)
+    out = np.zeros((hd.n, hd.n, len(keys)), dtype=np.complex128, order="F")
+    en = np.zeros(3)
+    ctx.check(_lib.lqm_hartreefock_eval(ctx.handle, hd.handle, vd.handle, len(Lkeys), _ptr(Lk), _ptr(R), len(keys),
+                                        _ptr(Mk), _ptr(out), _ptr(en)))
+    return {L: np.array(out[:, :, i]) for i, L in enumerate(keys)}, en[0], en[1], en[2]
 
 
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
                      kweights=None, log_callback=None, multimode="cuda", ctx=None, acceleration="linear",
-                     anderson_depth=5, residual_norm="density"):
+                     anderson_depth=5, residual_norm="density", hartree=True, fock=True, exchange=None):
     """``solvehartreefock(h, v, ρ_init, filling, ks; T, β, tol, iterations, acceleration,
     anderson_depth, residual_norm)``: linear damped mixing (default) or Anderson
     acceleration; the relative density change (default) or the commutator norm
@@ -562,6 +625,7 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, ite
     depth = int(anderson_depth) if acceleration == "anderson" else 0
     ctx.check(_lib.lqm_ctx_set_scf_acceleration(ctx.handle, depth))
     ctx.check(_lib.lqm_ctx_set_scf_residual(ctx.handle, 1 if residual_norm == "commutator" else 0))
+    _set_functional(ctx, hartree, fock, exchange)
     hd = _as_device_hops(h, ctx)
     vd = _as_device_hops(v, ctx)
     ks = _ks(ks, hd.d)
@@ -582,5 +646,7 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, ite
                               float(filling), float(T), float(beta), float(tol), int(iterations),
                               len(Lkeys), _ptr(Lk), _ptr(rho), cb, None, _ptr(out)))
     rho_out = {L: np.array(rho[:, :, i]) for i, L in enumerate(Lkeys)}
-    mf = MFInfo(mu=out[1], eH=out[2], eF=out[3], eband=out[4], ekin=out[5], iterations=int(out[8]))
+    eJ = _D()
+    ctx.check(_lib.lqm_ctx_scf_exchange_energy(ctx.handle, ctypes.byref(eJ)))
+    mf = MFInfo(mu=out[1], eH=out[2], eF=out[3], eband=out[4], ekin=out[5], iterations=int(out[8]), eJ=eJ.value)
     return HFResult(rho_out, out[0], mf, bool(out[7]), out[6])

@@ -6,19 +6,46 @@ import numpy as np
 from . import kspace as K
 
 
+class ExchangeKernel:
+    """Meanfield/hartreefock.jl:24-76 (ExchangeKernel) with 0-based sites and flavors:
+    j a site-space Hops, sf2idx[a, f] the orbital of (site a, flavor f), Jtot = sum_L j[L]."""
+
+    def __init__(self, j, siteof, flavorof):
+        siteof, flavorof = list(siteof), list(flavorof)
+        if len(siteof) != len(flavorof):
+            raise ValueError("siteof and flavorof must have equal length")
+        ns, nf = max(siteof) + 1, max(flavorof) + 1
+        z = tuple(0 for _ in next(iter(j.keys())))
+        if j[z].shape[0] != ns:
+            raise ValueError("exchange kernel dimension does not match the number of sites")
+        if np.any(np.diag(j[z]) != 0):
+            raise ValueError("onsite self-exchange j[0][a,a] must be zero")
+        sf = -np.ones((ns, nf), int)
+        for I, (a_, f_) in enumerate(zip(siteof, flavorof)):
+            if sf[a_, f_] >= 0:
+                raise ValueError("duplicate (site, flavor)")
+            sf[a_, f_] = I
+        if np.any(sf < 0):
+            raise ValueError("every (site, flavor) pair must appear once")
+        self.j = {L: np.asarray(M, complex) for L, M in j.items()}
+        self.sf2idx = sf
+        self.Jtot = sum(self.j[L] for L in self.j)
+
+
 class HartreeFock:
     """Meanfield/hartreefock.jl:143-175 (struct), :184-228 (call), :247-289 (fields),
-    :392-410 (energies)."""
+    :298-381 (exchange), :392-410 (energies)."""
 
-    def __init__(self, h, v):
+    def __init__(self, h, v, hartree=True, fock=True, exchange=None):
         self.h = h
         self.v = v
+        self.hartree, self.fock, self.exchange = hartree, fock, exchange
         self.V0 = sum(v[L] for L in v)  # hartreefock.jl:159
         keys = list(h.keys()) + [L for L in v if L not in h]
         n = next(iter(h.values())).shape[0]
         self.hMF = {L: np.zeros((n, n), complex) for L in keys}
         self.mu = 0.0
-        self.eH = self.eF = self.eband = self.ekin = 0.0
+        self.eH = self.eF = self.eJ = self.eband = self.ekin = 0.0
 
     def __call__(self, rho):
         n = next(iter(self.h.values())).shape[0]
@@ -27,23 +54,85 @@ class HartreeFock:
             self.hMF[L] = np.zeros((n, n), complex)
         for L in self.h:
             self.hMF[L] = self.hMF[L] + self.h[L]
-        # Fock: hMF[L] -= v[L] .* rho[L] (hartreefock.jl:247-276)
-        for L in self.v:
-            if L in rho:
-                self.hMF[L] = self.hMF[L] - self.v[L] * rho[L]
-        # Hartree: hMF[0][i,i] += (V0 diag rho0)_i (hartreefock.jl:278-289)
         z = tuple(0 for _ in next(iter(rho.keys())))
-        d = self.V0 @ np.diag(rho[z])
-        self.hMF[z] = self.hMF[z] + np.diag(d)
-        # energies (hartreefock.jl:392-410)
+        # Fock: hMF[L] -= v[L] .* rho[L] (hartreefock.jl:247-276)
+        if self.fock:
+            for L in self.v:
+                if L in rho:
+                    self.hMF[L] = self.hMF[L] - self.v[L] * rho[L]
+        # Hartree: hMF[0][i,i] += (V0 diag rho0)_i (hartreefock.jl:278-289)
+        if self.hartree:
+            d = self.V0 @ np.diag(rho[z])
+            self.hMF[z] = self.hMF[z] + np.diag(d)
+        if self.exchange is not None:
+            self._add_exchange(rho, z)
+        # energies (hartreefock.jl:345-410)
         nv = np.diag(rho[z])
-        self.eH = float(np.real(0.5 * (nv @ self.V0 @ nv)))
+        self.eH = float(np.real(0.5 * (nv @ self.V0 @ nv))) if self.hartree else 0.0
         self.eF = float(np.real(-0.5 * sum(np.sum(rho[L] * np.conj(rho[L]) * vL)
-                                           for L, vL in self.v.items() if L in rho)))
+                                           for L, vL in self.v.items() if L in rho))) if self.fock else 0.0
+        self.eJ = self._exchange_energy(rho, z) if self.exchange is not None else 0.0
         return self
 
+    def _add_exchange(self, rho, z):
+        """meanfieldOperator_addexchange! (hartreefock.jl:298-337)."""
+        ek = self.exchange
+        ix = ek.sf2idx
+        ns, nf = ix.shape
+        H0, r0 = self.hMF[z], rho[z]
+        for a in range(ns):
+            for b in range(ns):
+                J = ek.Jtot[a, b]
+                if J == 0:
+                    continue
+                for al in range(nf):
+                    for be in range(nf):
+                        H0[ix[a, al], ix[a, be]] -= J * r0[ix[b, al], ix[b, be]]
+        n = H0.shape[0]
+        for L, jL in ek.j.items():
+            if L not in rho:
+                continue
+            if L not in self.hMF:
+                self.hMF[L] = np.zeros((n, n), complex)
+            hL, rL = self.hMF[L], rho[L]
+            for a in range(ns):
+                for b in range(ns):
+                    J = jL[a, b]
+                    if J == 0:
+                        continue
+                    tau = sum(rL[ix[a, al], ix[b, al]] for al in range(nf))
+                    for al in range(nf):
+                        hL[ix[a, al], ix[b, al]] += J * tau
+
+    def _exchange_energy(self, rho, z):
+        """exchange_energy (hartreefock.jl:345-381)."""
+        ek = self.exchange
+        ix = ek.sf2idx
+        ns, nf = ix.shape
+        r0 = rho[z]
+        e = 0.0 + 0.0j
+        for a in range(ns):
+            for b in range(ns):
+                J = ek.Jtot[a, b]
+                if J == 0:
+                    continue
+                s = sum(r0[ix[a, al], ix[a, be]] * r0[ix[b, be], ix[b, al]] for al in range(nf) for be in range(nf))
+                e -= J * s / 2
+        for L, jL in ek.j.items():
+            if L not in rho:
+                continue
+            rL = rho[L]
+            for a in range(ns):
+                for b in range(ns):
+                    J = jL[a, b]
+                    if J == 0:
+                        continue
+                    tau = sum(rL[ix[a, al], ix[b, al]] for al in range(nf))
+                    e += J * abs(tau) ** 2 / 2
+        return float(np.real(e))
+
     def doublecounting(self):
-        return self.eH + self.eF
+        return self.eH + self.eF + self.eJ  # hartreefock.jl:236
 
 
 def hermitianize(rho):
@@ -132,7 +221,7 @@ def _product_first_fastest(ranges):
 
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
                      iterations=500, log=None, acceleration="linear", anderson_depth=5,
-                     residual_norm="density"):
+                     residual_norm="density", hartree=True, fock=True, exchange=None):
     """solvehartreefock -> _scf_driver! -> fixedpoint!.
 
     Meanfield/selfconsistent.jl:19,62-69,256-336,366-381 and fixedpoint.jl:39-194.
@@ -147,7 +236,7 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
     if not is_hermitian(rho0):
         hermitianize(rho0)
     rho1 = {L: M.copy() for L, M in rho0.items()}
-    hf = HartreeFock(h, v)
+    hf = HartreeFock(h, v, hartree=hartree, fock=fock, exchange=exchange)
     nk = ks.shape[1]
     w = np.full(nk, 1.0 / nk)
     converged = False

@@ -306,3 +306,28 @@ def test_partial_spectrum_matches_oracle(lqm, ctx):
     rref, ebref = K.densitymatrix_partial(h6, ks6, w6, 0.0, 0.01, M.KEYS9, 24)
     assert max(np.max(np.abs(rho[R] - rref[R])) for R in M.KEYS9) <= RHO_TOL
     assert abs(eb - ebref) <= 1e-10 * max(1.0, abs(ebref))
+
+
+def test_exchange_scf_blocked_path_matches_oracle(lqm, ctx):
+    """J-augmented SCF on the blocked eigensolver path: the disordered spinful honeycomb
+    6x6 cell (n = 144, 72 sites x 2 spin flavors, spin the fast index) with Hubbard U = 2
+    and a nearest-neighbour exchange kernel J = 0.1 on every bond (its zero-key diagonal
+    empty), 4 iterations from a random local magnetization, against the oracle."""
+    lat, h = M.honeycomb_disorder(6)
+    v = M.hubbard_v(lat, U=2.0)
+    nn_site = M.nearestneighbor(lat, -1.0)
+    j = {R: 0.1 * (np.abs(B) > 0).astype(complex) for R, B in nn_site.items()}
+    ns = lat.norb
+    siteof = [I // 2 for I in range(2 * ns)]
+    flavorof = [I % 2 for I in range(2 * ns)]
+    rho0 = {R: np.zeros((2 * ns, 2 * ns), complex) for R in M.KEYS9}
+    rho0[(0, 0)] = M.random_local_magnetization(ns, seed=4)
+    ks = L.regulargrid(4 * 4)
+    kw = dict(T=0.05, beta=0.4, tol=0.0, iterations=4)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, exchange=lqm.ExchangeKernel(j, siteof, flavorof), **kw)
+    rho_ref, E_ref, hf_ref, _, _, it = MF.solvehartreefock(h, v, rho0, 0.5, ks,
+                                                           exchange=MF.ExchangeKernel(j, siteof, flavorof), **kw)
+    assert res.mf.iterations == it == 4
+    assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in M.KEYS9) <= RHO_TOL
+    assert abs(res.energy - E_ref) <= 1e-9 * max(1.0, abs(E_ref))
+    assert abs(res.mf.eJ - hf_ref.eJ) <= 1e-9 * max(1.0, abs(hf_ref.eJ))

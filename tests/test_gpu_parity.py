@@ -318,3 +318,62 @@ def test_commutator_residual_scf_matches_oracle(lqm, ctx):
     c = lqm.commutator_kspace_norm(h6, rho, ks6, ctx=ctx)
     c_ref = MF.commutator_kspace_norm(h6, rho, ks6)
     assert abs(c - c_ref) <= 1e-12 * c_ref
+
+
+def _jkernel(J1, Jnn):
+    # test/test_exchange.jl:14-20
+    j0 = np.array([[0.0, J1], [J1, 0.0]], complex)
+    jp = np.array([[Jnn, 0.0], [0.0, 0.0]], complex)
+    return {(0, 0): j0, (1, 0): jp, (-1, 0): jp.conj().T}
+
+
+def test_exchange_functional_and_scf_match_oracle(lqm, ctx):
+    """J-augmented Hartree-Fock (ExchangeKernel, hartreefock.jl:24-76,298-381) through
+    lqm_hartreefock_eval and lqm_scf_hf: hMF and (eH, eF, eJ) for a random complex rho
+    with bond keys against the oracle, with each of the Hartree / Fock terms switched off
+    too; the analytic dimer limits of test/test_exchange.jl:43-60; and the SCF case of
+    test/test_exchange.jl:85-123 (exchange selects the polarized state) in the oracle's
+    iterations and energies."""
+    siteof, flavorof = [0, 1, 0, 1], [0, 0, 1, 1]
+    t, U = 0.1, 1.0
+    h = {(0, 0): np.kron(np.eye(2), np.array([[0.0, t], [t, 0.0]], complex))}
+    v = {(0, 0): (U * np.ones((4, 4)) - U * np.eye(4)).astype(complex)}
+    rng = np.random.default_rng(7)
+    r0 = rng.random((4, 4)) + 1j * rng.random((4, 4))
+    r1 = rng.random((4, 4)) + 1j * rng.random((4, 4))
+    rho = {(0, 0): (r0 + r0.conj().T) / 2, (1, 0): r1, (-1, 0): r1.conj().T}
+    for hartree, fock in ((True, True), (False, True), (True, False)):
+        ekd = lqm.ExchangeKernel(_jkernel(0.8, 0.35), siteof, flavorof)
+        hmf, eH, eF, eJ = lqm.hartreefock_eval(h, v, rho, hartree=hartree, fock=fock, exchange=ekd, ctx=ctx)
+        ref = MF.HartreeFock(h, v, hartree=hartree, fock=fock,
+                             exchange=MF.ExchangeKernel(_jkernel(0.8, 0.35), siteof, flavorof))(rho)
+        assert set(hmf) == set(ref.hMF)
+        assert max(np.max(np.abs(hmf[L] - ref.hMF[L])) for L in hmf) <= 1e-12
+        assert max(abs(eH - ref.eH), abs(eF - ref.eF), abs(eJ - ref.eJ)) <= 1e-12
+    hz = {(0, 0): np.zeros((4, 4), complex)}
+    ekd = lqm.ExchangeKernel(_jkernel(0.7, 0.0), siteof, flavorof)
+    _, _, _, eJ = lqm.hartreefock_eval(hz, hz, {(0, 0): np.diag([1.0, 1, 0, 0]).astype(complex)}, exchange=ekd,
+                                       ctx=ctx)
+    assert abs(eJ + 0.7) < 1e-12
+    _, _, _, eJ = lqm.hartreefock_eval(hz, hz, {(0, 0): 0.5 * np.eye(4, dtype=complex)}, exchange=ekd, ctx=ctx)
+    assert abs(eJ + 0.35) < 1e-12
+    with pytest.raises(lqm.LQMError):
+        lqm.hartreefock_eval(hz, hz, rho, exchange=lqm.ExchangeKernel(
+            {(0, 0): np.array([[0.5, 0], [0, 0]], complex)}, siteof, flavorof), ctx=ctx)
+
+    ks = L.regulargrid(8 * 8)
+    Es = {}
+    for label, occs, J in (("pol_J", [0.9, 0.9, 0.1, 0.1], 0.4), ("unp_J", [0.5] * 4, 0.4),
+                           ("pol_0", [0.9, 0.9, 0.1, 0.1], None), ("unp_0", [0.5] * 4, None)):
+        rho0 = {(0, 0): np.diag(occs).astype(complex)}
+        kw = dict(T=0.02, beta=0.5, tol=1e-9, iterations=600)
+        res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, **kw,
+                                   exchange=lqm.ExchangeKernel(_jkernel(J, 0.0), siteof, flavorof) if J else None)
+        _, E_ref, hf_ref, conv, _, it = MF.solvehartreefock(
+            h, v, rho0, 0.5, ks, **kw, exchange=MF.ExchangeKernel(_jkernel(J, 0.0), siteof, flavorof) if J else None)
+        assert res.converged and conv
+        assert abs(res.energy - (res.mf.ekin + res.mf.eH + res.mf.eF + res.mf.eJ)) <= 1e-6 + 1e-8 * abs(res.energy)
+        assert abs(res.energy - E_ref) <= 1e-8 and abs(res.mf.eJ - hf_ref.eJ) <= 1e-8
+        assert abs(res.mf.iterations - it) <= 1
+        Es[label] = res.energy
+    assert (Es["unp_J"] - Es["pol_J"]) - (Es["unp_0"] - Es["pol_0"]) > 0.3 * 0.4

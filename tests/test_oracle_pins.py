@@ -386,3 +386,74 @@ def test_commutator_residual_scf_oracle():
     # at the fixed point the commutator vanishes (the converged rho re-evaluated)
     hf(rho)
     assert MF.commutator_kspace_norm(hf.hMF, rho, ks) < 1e-6
+
+
+def _jkernel(J1, Jnn):
+    # test/test_exchange.jl:14-20: intra-cell J1 between sites 0-1, inter-cell site0-site0 Jnn
+    j0 = np.array([[0.0, J1], [J1, 0.0]], complex)
+    jp = np.array([[Jnn, 0.0], [0.0, 0.0]], complex)
+    return {(0, 0): j0, (1, 0): jp, (-1, 0): jp.conj().T}
+
+
+SITEOF0, FLAVOROF0 = [0, 1, 0, 1], [0, 0, 1, 1]  # flavor-outer layout of test_exchange.jl:11-12
+
+
+def test_exchange_kernel_oracle_pins():
+    """test/test_exchange.jl:29-83 on the oracle: construction rules, the analytic dimer
+    limits (eJ = -J1 polarized, -J1/2 unpolarized) and the variational identity
+    Tr[Sigma_J rho] = 2 eJ with Hermitian Sigma_J for a random complex rho."""
+    ek = MF.ExchangeKernel(_jkernel(1.0, 0.3), SITEOF0, FLAVOROF0)
+    assert ek.sf2idx.shape == (2, 2) and ek.sf2idx[0, 0] == 0 and ek.sf2idx[1, 1] == 3
+    with pytest.raises(ValueError):
+        MF.ExchangeKernel({(0, 0): np.array([[0.5, 0], [0, 0]], complex)}, SITEOF0, FLAVOROF0)
+    with pytest.raises(ValueError):
+        MF.ExchangeKernel(_jkernel(1.0, 0.0), [0, 0, 0, 0], FLAVOROF0)
+    J1 = 0.7
+    h = {(0, 0): np.zeros((4, 4), complex)}
+    v = {(0, 0): np.zeros((4, 4), complex)}
+    hf = MF.HartreeFock(h, v, exchange=MF.ExchangeKernel(_jkernel(J1, 0.0), SITEOF0, FLAVOROF0))
+    hf({(0, 0): np.diag([1.0, 1.0, 0.0, 0.0]).astype(complex)})
+    assert abs(hf.eJ + J1) < 1e-12
+    hf({(0, 0): np.diag([0.5, 0.5, 0.5, 0.5]).astype(complex)})
+    assert abs(hf.eJ + J1 / 2) < 1e-12
+    rng = np.random.default_rng(7)
+    r0 = rng.random((4, 4)) + 1j * rng.random((4, 4))
+    r1 = rng.random((4, 4)) + 1j * rng.random((4, 4))
+    rho = {(0, 0): (r0 + r0.conj().T) / 2, (1, 0): r1, (-1, 0): r1.conj().T}
+    hf0 = MF.HartreeFock(h, v)(rho)
+    hfJ = MF.HartreeFock(h, v, exchange=MF.ExchangeKernel(_jkernel(0.8, 0.35), SITEOF0, FLAVOROF0))(rho)
+    SJ = {L: hfJ.hMF[L] - hf0.hMF.get(L, 0) for L in hfJ.hMF}
+    for L in SJ:
+        assert np.max(np.abs(SJ[L] - SJ[tuple(-x for x in L)].conj().T)) < 1e-12
+    tr = sum(np.sum(rho[tuple(-x for x in L)].T * SJ[L]) for L in SJ if tuple(-x for x in L) in rho)
+    assert abs(tr.real - 2 * hfJ.eJ) < 1e-10
+
+
+def exchange_scf_case():
+    """test/test_exchange.jl:85-123: two sites x two flavors, hopping t = 0.1 inside each
+    flavor, U = 1 between different orbitals, J1 = 0.4."""
+    t, U = 0.1, 1.0
+    h1 = np.array([[0.0, t], [t, 0.0]], complex)
+    h = {(0, 0): np.kron(np.eye(2), h1)}
+    v = {(0, 0): (U * np.ones((4, 4)) - U * np.eye(4)).astype(complex)}
+    return h, v
+
+
+def test_exchange_scf_selects_polarized_state_oracle():
+    """test/test_exchange.jl:85-123 on the oracle: with J the polarized solution wins by
+    more than 0.3 J over the gain without J; every run converges and satisfies
+    E = ekin + eH + eF + eJ."""
+    h, v = exchange_scf_case()
+    J1 = 0.4
+    ks = L.regulargrid(8 * 8)
+    Es = {}
+    for label, occs, J in (("pol_J", [0.9, 0.9, 0.1, 0.1], J1), ("unp_J", [0.5] * 4, J1),
+                           ("pol_0", [0.9, 0.9, 0.1, 0.1], None), ("unp_0", [0.5] * 4, None)):
+        ek = MF.ExchangeKernel(_jkernel(J, 0.0), SITEOF0, FLAVOROF0) if J else None
+        rho0 = {(0, 0): np.diag(occs).astype(complex)}
+        rho, E, hf, conv, res, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, T=0.02, beta=0.5, tol=1e-9,
+                                                        iterations=600, exchange=ek)
+        assert conv
+        assert abs(E - (hf.ekin + hf.eH + hf.eF + hf.eJ)) <= 1e-6 + 1e-8 * abs(E)
+        Es[label] = E
+    assert (Es["unp_J"] - Es["pol_J"]) - (Es["unp_0"] - Es["pol_0"]) > 0.3 * J1
