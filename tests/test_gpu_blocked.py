@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import kspace as K
+from oracle import meanfield as MF
 from lqm_workloads import lattice as L
 from lqm_workloads import models as M
 
