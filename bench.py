@@ -398,6 +398,20 @@ def profile_case_tbg(Q, ctx, M, case):
     print(json.dumps({"profile_case": case, "kernel_ms": ctx.last_kernel_ms(), "wall_s": time.perf_counter() - t0}))
 
 
+def profile_case_kubo(Q, ctx, M):
+    """One Kubo correlator call for profilers: chi_xy(w) of the disordered honeycomb 6x6
+    cell (n = 144) over the 48 x 48 grid, 64 frequencies."""
+    import numpy as np
+    from lqm_workloads import lattice as LL
+    lat, h = M.honeycomb_disorder()
+    J = M.currentoperators(lat, h)
+    ks = LL.regulargrid(48 * 48)
+    t0 = time.perf_counter()
+    Q.opticalconductivity(np.linspace(0.0, 3.0, 64), h, J[0], J[1], ks, Gamma=0.05, T=0.01, ctx=ctx)
+    print(json.dumps({"profile_case": "kubo144", "kernel_ms": ctx.last_kernel_ms(),
+                      "wall_s": time.perf_counter() - t0}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -408,10 +422,11 @@ def main():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the other configurations (n=144, 1324, 2884 and the adjoint)")
     ap.add_argument("--profile-case", nargs="?", const="n96", default=None,
-                    choices=["n96", "tbg10-bands576", "tbg10-density142", "tbg10-density16"],
+                    choices=["n96", "tbg10-bands576", "tbg10-density142", "tbg10-density16", "kubo144"],
                     help="one call of a small profiling case: n96 = the fused bench call on the n=96 model "
                          "over 2048 k; tbg10-* = bands or density of the n=1324 twisted bilayer over the "
-                         "first 576 / 142 / 16 points of the 24x24 grid")
+                         "first 576 / 142 / 16 points of the 24x24 grid; kubo144 = the Kubo correlator "
+                         "of the n=144 honeycomb cell over 48x48 k and 64 frequencies")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
@@ -439,6 +454,8 @@ def main():
     ctx = Q.Context(local, timeout=900)
     if args.profile_case == "n96":
         return profile_case(Q, ctx, models[2][1], torch, dev, np)
+    if args.profile_case == "kubo144":
+        return profile_case_kubo(Q, ctx, M)
     if args.profile_case:
         return profile_case_tbg(Q, ctx, M, args.profile_case)
 

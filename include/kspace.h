@@ -254,6 +254,24 @@ int lqm_densitymatrix_partial(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const
                               double mu, double T, int64_t num_bands, double sigma, int which, int64_t nL,
                               const int64_t* Lkeys, double* rho, double* eband);
 
+/* Nambu (BdG) Hamiltonians: a Hops of order 2d, electron block first, as
+ * BdGOperator.h builds it (src/modules/Superconductivity/types.jl:36-97).
+ * lqm_bdg_densitymatrix: getdensitymatrix!(rho::BdGOperator, H::BdGOperator, ks,
+ * kweights, mu) (src/modules/Superconductivity/green.jl:38-54): rho_L of H - mu tau_z
+ * at mu = 0 (n x n x nL, n = 2d) and *energy = <H - mu N> = (band sum)/2 +
+ * (Re tr h_e[0] - d mu)/2.  lqm_bdg_filling: Spectrum.filling(H::BdGOperator, ks, mu;
+ * T) (src/modules/Superconductivity/operators.jl:117-122), the electron trace of
+ * rho_0 over d.  lqm_bdg_chemicalpotential: Spectrum.chemicalpotential(H::BdGOperator,
+ * ks, target; T, mu_lo, mu_hi) (operators.jl:139-155), float bisection of the
+ * filling on the bracket from the electron-sector bands (one eigen pass with
+ * vectors per step).  w NULL means 1/nk.  H is not modified. */
+int lqm_bdg_densitymatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, double mu,
+                          double T, int64_t nL, const int64_t* Lkeys, double* rho, double* energy);
+int lqm_bdg_filling(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w, double mu,
+                    double T, double* out);
+int lqm_bdg_chemicalpotential(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
+                              double filling, double T, double mu_lo, double mu_hi, double* out);
+
 /* Kubo current-current correlator, opticalconductivity(frequencies, H, J1, J2,
  * ks; mu, Gamma, T) (src/modules/LinearResponse/opticalconductivity.jl:101-127
  * with kubo! of src/modules/LinearResponse/kubo.jl:11-26):

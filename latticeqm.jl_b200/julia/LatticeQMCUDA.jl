@@ -230,6 +230,56 @@ function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights
     eb[]
 end
 
+"""`getdensitymatrix!(ρ::BdGOperator, H::BdGOperator, ks, kweights, μ; T)`
+(Superconductivity/green.jl:38-54) on the device (`lqm_bdg_densitymatrix`): `ρB` and `HB`
+are the Nambu Hops (`ρ.h`, `H.h`); returns ⟨H − μN⟩.  `HB` is not modified."""
+function cuda_bdg_densitymatrix!(ρB::Hops, HB, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
+                                 μ::Real, T::Real, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, HB)
+    Lk = collect(keys(ρB))
+    d = length(first(Lk))
+    n = size(HB[first(keys(HB))], 1)
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    rho = zeros(ComplexF64, n, n, length(Lk))
+    e = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_bdg_densitymatrix, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Int64, Ptr{Int64},
+         Ptr{ComplexF64}, Ref{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Vector{Float64}(kweights), Float64(μ), Float64(T),
+        length(Lk), L, rho, e))
+    for (i, k) in enumerate(Lk)
+        ρB[k] .= view(rho, :, :, i)
+    end
+    e[]
+end
+
+"""`Spectrum.filling(H::BdGOperator, ks, μ; T)` (Superconductivity/operators.jl:117-122) on
+the device (`lqm_bdg_filling`); `HB = H.h`."""
+function cuda_bdg_filling(HB, ks::AbstractMatrix{Float64}, μ::Real, exec::CudaExec; T::Real=0.01)
+    ctx = context(exec.device)
+    dh = upload(ctx, HB)
+    out = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_bdg_filling, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Ref{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Ptr{Float64}(C_NULL), Float64(μ), Float64(T), out))
+    out[]
+end
+
+"""`Spectrum.chemicalpotential(H::BdGOperator, ks, target; T, μ_lo, μ_hi)`
+(Superconductivity/operators.jl:139-155) on the device (`lqm_bdg_chemicalpotential`)."""
+function cuda_bdg_chemicalpotential(HB, ks::AbstractMatrix{Float64}, target::Real, exec::CudaExec;
+                                    T::Real=0.01, μ_lo::Real=-100.0, μ_hi::Real=100.0)
+    ctx = context(exec.device)
+    dh = upload(ctx, HB)
+    out = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_bdg_chemicalpotential, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}, Float64, Float64, Float64, Float64, Ref{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), Ptr{Float64}(C_NULL), Float64(target), Float64(T),
+        Float64(μ_lo), Float64(μ_hi), out))
+    out[]
+end
+
 const WHICH_CODE = Dict(:LM => Cint(0), :SR => Cint(1), :LR => Cint(2))
 
 """`bandmatrix(H, ks; format=:sparse, num_bands, sigma, which)` on the device

@@ -42,7 +42,8 @@ EXPORTS = [
     "lqm_bandmatrix_obs", "lqm_ctx_set_scf_acceleration", "lqm_density", "lqm_ldos",
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
-    "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval",
+    "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
+    "lqm_bdg_chemicalpotential",
 ]
 
 
@@ -101,6 +102,9 @@ _SIG = {
     "lqm_ctx_set_scf_exchange": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _I64, _P, _P],
     "lqm_ctx_scf_exchange_energy": [_P, ctypes.POINTER(_D)],
     "lqm_hartreefock_eval": [_P, _P, _P, _I64, _P, _P, _I64, _P, _P, _P],
+    "lqm_bdg_densitymatrix": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D)],
+    "lqm_bdg_filling": [_P, _P, _I64, _P, _P, _D, _D, ctypes.POINTER(_D)],
+    "lqm_bdg_chemicalpotential": [_P, _P, _I64, _P, _P, _D, _D, _D, _D, ctypes.POINTER(_D)],
     "lqm_bandmatrix_partial": [_P, _P, _I64, _P, _I64, _D, ctypes.c_int, ctypes.c_int, _P, _P],
     "lqm_densitymatrix_partial": [_P, _P, _I64, _P, _P, _D, _D, _I64, _D, ctypes.c_int, _I64, _P, _P,
                                   ctypes.POINTER(_D)],
@@ -474,6 +478,51 @@ def opticalconductivity(frequencies, H, J1, J2, ks, mu=0.0, Gamma=0.025, T=0.1, 
     ctx.check(_lib.lqm_opticalconductivity(ctx.handle, Hd.handle, J1d.handle, J2d.handle, ks.shape[1], _ptr(ks),
                                            len(om), _ptr(om), float(mu), float(Gamma), float(T), _ptr(out)))
     return out
+
+
+def bdg_getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, ctx=None):
+    """``getdensitymatrix!(ρ::BdGOperator, H::BdGOperator, ks[, kweights], μ; T)``
+    (Superconductivity/green.jl:38-54) for a Nambu Hops ``H`` (order 2d): overwrites the
+    blocks of ``rhos`` and returns ⟨H − μN⟩ (``lqm_bdg_densitymatrix``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    Lkeys = list(rhos.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = np.zeros((Hd.n, Hd.n, len(Lkeys)), dtype=np.complex128, order="F")
+    e = _D()
+    ctx.check(_lib.lqm_bdg_densitymatrix(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(w), float(mu), float(T),
+                                         len(Lkeys), _ptr(Lk), _ptr(out), ctypes.byref(e)))
+    for i, L in enumerate(Lkeys):
+        rhos[L] = np.array(out[:, :, i])
+    return e.value
+
+
+def bdg_filling(H, ks, mu=0.0, T=0.01, kweights=None, ctx=None):
+    """``Spectrum.filling(H::BdGOperator, ks, μ; T)`` (Superconductivity/operators.jl:117-122)
+    (``lqm_bdg_filling``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = _D()
+    ctx.check(_lib.lqm_bdg_filling(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(w), float(mu), float(T),
+                                   ctypes.byref(out)))
+    return out.value
+
+
+def bdg_chemicalpotential(H, ks, filling, T=0.01, kweights=None, mu_lo=-100.0, mu_hi=100.0, ctx=None):
+    """``Spectrum.chemicalpotential(H::BdGOperator, ks, target; T, μ_lo, μ_hi)``
+    (Superconductivity/operators.jl:139-155) (``lqm_bdg_chemicalpotential``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    out = _D()
+    ctx.check(_lib.lqm_bdg_chemicalpotential(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), _ptr(w), float(filling),
+                                             float(T), float(mu_lo), float(mu_hi), ctypes.byref(out)))
+    return out.value
 
 
 def commutator_kspace_norm(H, rho, ks, kweights=None, multimode="cuda", ctx=None):

@@ -260,6 +260,28 @@ def triangular_hubbard(L_super=6, t=-1.0, tp=0.2, U=4.0):
     return lat, h, v
 
 
+def bdg_operator(h, delta=None):
+    """``BdGOperator(h[, Δ])`` (Superconductivity/types.jl:43-60,76-97): the Nambu Hops of
+    order 2d with blocks [h_R 0; 0 -conj(h_R)] and, for every pairing key R (its partner
+    -R present), [0 Δ_R; Δ_{-R}^H 0]."""
+    d = hopdim(h)
+    H = {}
+    for R, M in h.items():
+        B = np.zeros((2 * d, 2 * d), complex)
+        B[:d, :d] = M
+        B[d:, d:] = -np.conj(M)
+        H[R] = B
+    for R, D in (delta or {}).items():
+        mR = tuple(-x for x in R)
+        if mR not in delta:
+            raise ValueError(f"pairing key {R} has no partner {mR}")
+        B = np.zeros((2 * d, 2 * d), complex)
+        B[:d, d:] = D
+        B[d:, :d] = np.asarray(delta[mR]).conj().T
+        H[R] = H[R] + B if R in H else B
+    return H
+
+
 def antiferro_density(lat):
     """``initialguess(v, :antiferro; lat)`` (Meanfield/initialguess.jl:186-193):
     rho_0 = kron(P_A, rho_up) + kron(P_B, sigma0 - rho_up), rho_up = diag(1, 0), P_A/P_B the

@@ -377,3 +377,47 @@ def test_exchange_functional_and_scf_match_oracle(lqm, ctx):
         assert abs(res.mf.iterations - it) <= 1
         Es[label] = res.energy
     assert (Es["unp_J"] - Es["pol_J"]) - (Es["unp_0"] - Es["pol_0"]) > 0.3 * 0.4
+
+
+def test_bdg_paths_match_oracle(lqm, ctx):
+    """Nambu (BdG) Hamiltonians through lqm_bdg_densitymatrix, lqm_bdg_filling and
+    lqm_bdg_chemicalpotential: the checks of test/test_superconductivity.jl (+-E pairs,
+    the 2 Delta gap at the Dirac point, the BdG kinetic energy -3 at Gamma, filling 1/2
+    with weak pairing) on the device, and parity with the oracle for the disordered
+    honeycomb 3x3 cell (n = 36, BdG order 72) with complex onsite and bond pairing."""
+    from oracle import bdg as BDG
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    H = M.bdg_operator(h)
+    b, _ = lqm.bandmatrix(H, np.array([[0.1, 0.3, 0.0], [0.2, -0.1, 0.0]]), ctx=ctx)
+    assert np.max(np.abs(b + b[::-1, :])) < 1e-10
+    Hs = M.bdg_operator(h, {(0, 0): 0.25 * np.eye(2, dtype=complex)})
+    b, _ = lqm.bandmatrix(Hs, np.array([[1 / 3], [-1 / 3]]), ctx=ctx)
+    assert abs(b[2, 0] - 0.25) < 1e-10 and abs(b[1, 0] + 0.25) < 1e-10
+    rho = {R: None for R in H}
+    e = lqm.bdg_getdensitymatrix(rho, H, np.zeros((2, 1)), mu=0.0, T=1e-6, ctx=ctx)
+    assert abs(e + 3.0) < 1e-3
+    Hw = M.bdg_operator(h, {(0, 0): 0.05 * np.eye(2, dtype=complex)})
+    assert abs(lqm.bdg_filling(Hw, L.regulargrid(12 * 12), 0.0, T=0.05, ctx=ctx) - 0.5) < 5e-3
+
+    _, h3 = M.honeycomb_disorder(3)
+    n = h3[(0, 0)].shape[0]
+    rng = np.random.default_rng(9)
+    D0 = 0.1 * (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    D1 = 0.05 * (rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    delta = {(0, 0): D0 - D0.T, (1, 0): D1, (-1, 0): -D1.T}
+    HB = M.bdg_operator(h3, delta)
+    assert HB.keys() == BDG.bdg_operator(h3, delta).keys()
+    ks = rng.uniform(-0.5, 0.5, (2, 10))
+    w = np.full(10, 0.1)
+    rho = {R: None for R in M.KEYS9}
+    e = lqm.bdg_getdensitymatrix(rho, HB, ks, mu=0.3, T=0.02, ctx=ctx)
+    rref, eref = BDG.bdg_densitymatrix(BDG.bdg_operator(h3, delta), ks, w, 0.3, 0.02, M.KEYS9)
+    assert max(np.max(np.abs(rho[R] - rref[R])) for R in M.KEYS9) <= 1e-9
+    assert abs(e - eref) <= 1e-10 * max(1.0, abs(eref))
+    f = lqm.bdg_filling(HB, ks, 0.3, T=0.05, ctx=ctx)
+    assert abs(f - BDG.bdg_filling(HB, ks, 0.3, T=0.05)) <= 1e-12
+    mu = lqm.bdg_chemicalpotential(HB, ks, 0.45, T=0.05, ctx=ctx)
+    mu_ref = BDG.bdg_chemicalpotential(HB, ks, 0.45, T=0.05)
+    assert abs(mu - mu_ref) <= 1e-9
+    assert abs(lqm.bdg_filling(HB, ks, mu, T=0.05, ctx=ctx) - 0.45) <= 1e-10

@@ -457,3 +457,36 @@ def test_exchange_scf_selects_polarized_state_oracle():
         assert abs(E - (hf.ekin + hf.eH + hf.eF + hf.eJ)) <= 1e-6 + 1e-8 * abs(E)
         Es[label] = E
     assert (Es["unp_J"] - Es["pol_J"]) - (Es["unp_0"] - Es["pol_0"]) > 0.3 * J1
+
+
+def test_bdg_oracle_pins():
+    """test/test_superconductivity.jl on the oracle: Nambu doubling gives +-E pairs,
+    s-wave Delta = 0.25 opens +-Delta at the Dirac point, bond pairing stays Hermitian,
+    the BdG kinetic energy of NN graphene at Gamma is -3, the filling with weak pairing
+    at mu = 0 is 1/2, and the chemical potential reproduces its filling target."""
+    from oracle import bdg as BDG
+    lat = L.honeycomb()
+    h = M.nearestneighbor(lat, -1.0)
+    H = BDG.bdg_operator(h)
+    for k in ([0.1, 0.2], [0.3, -0.1], [0.0, 0.0]):
+        ev = np.sort(np.linalg.eigvalsh(K.fouriersum(H, k)))
+        assert np.max(np.abs(ev + ev[::-1])) < 1e-10
+    Hs = BDG.bdg_operator(h, {(0, 0): 0.25 * np.eye(2, dtype=complex)})
+    ev = np.sort(np.linalg.eigvalsh(K.fouriersum(Hs, [1 / 3, -1 / 3])))
+    assert abs(ev[2] - 0.25) < 1e-10 and abs(ev[1] + 0.25) < 1e-10
+    bond = np.array([[0, 0.05], [0, 0]], complex)
+    Hb = BDG.bdg_operator(h, {(1, 0): bond, (-1, 0): bond.conj().T})
+    for k in ([0.1, 0.2], [1 / 3, -1 / 3]):
+        Hk = K.fouriersum(Hb, k)
+        assert np.max(np.abs(Hk - Hk.conj().T)) < 1e-12
+        ev = np.sort(np.linalg.eigvalsh(Hk))
+        assert np.max(np.abs(ev + ev[::-1])) < 1e-10
+    z = (0, 0)
+    _, e = BDG.bdg_densitymatrix(H, np.zeros((2, 1)), np.ones(1), 0.0, 1e-6, list(H.keys()))
+    assert abs(e + 3.0) < 1e-3
+    Hw = BDG.bdg_operator(h, {z: 0.05 * np.eye(2, dtype=complex)})
+    assert abs(BDG.bdg_filling(Hw, L.regulargrid(12 * 12), 0.0, T=0.05) - 0.5) < 5e-3
+    ks8 = L.regulargrid(8 * 8)
+    Hp = BDG.bdg_operator(h, {z: 0.2 * np.eye(2, dtype=complex)})
+    mu = BDG.bdg_chemicalpotential(Hp, ks8, 0.4, T=0.05)
+    assert abs(BDG.bdg_filling(Hp, ks8, mu, T=0.05) - 0.4) < 1e-12
