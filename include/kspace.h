@@ -272,6 +272,19 @@ int lqm_bdg_filling(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* k
 int lqm_bdg_chemicalpotential(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* w,
                               double filling, double T, double mu_lo, double mu_hi, double* out);
 
+/* Hartree-Fock with pairing on Nambu density matrices: solvehartreefock with
+ * HartreeFock(h::BdGOperator, v) = HartreeFockBDG (src/modules/Superconductivity/
+ * hartreefock.jl:5-159) in the SCF loop of src/modules/Meanfield/selfconsistent.jl:256-336
+ * with the BdG chemical potential and density matrix (operators.jl:139-155,
+ * green.jl:38-54).  h, v: the electron-sector Hops (order d); rho_inout: the Nambu
+ * density matrix, order 2d, nL keys (closed under L -> -L, the zero key present);
+ * k-weights 1/nk; linear mixing with beta and the relative residual; the context's
+ * Hartree/Fock switches (no exchange kernel).  out[10] = {E, mu, eH, eF, eband, ekin,
+ * residual, converged, iterations, eP} with E = eband - (eH + eF + eP). */
+int lqm_scf_hf_bdg(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, const double* ks,
+                   double filling, double T, double beta, double tol, int64_t maxiter, int64_t nL,
+                   const int64_t* Lkeys, double* rho_inout, lqm_scf_log_cb cb, void* cb_user, double* out);
+
 /* Kubo current-current correlator, opticalconductivity(frequencies, H, J1, J2,
  * ks; mu, Gamma, T) (src/modules/LinearResponse/opticalconductivity.jl:101-127
  * with kubo! of src/modules/LinearResponse/kubo.jl:11-26):

@@ -170,9 +170,9 @@ void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB
 };
-static_assert(WS_BDGE < 40, "workspace slots");
+static_assert(WS_BDGB < 40, "workspace slots");
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
 const DCPlan& get_plan(lqm_ctx* ctx, int n) {
@@ -1072,6 +1072,7 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 #include "lqm_kubo.inc"
 #include "lqm_partial.inc"
 #include "lqm_bdg.inc"
+#include "lqm_scf_bdg.inc"
 
 // ============================================================================
 // Allocation-free eigen pass.

@@ -434,6 +434,40 @@ function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractM
     ρ, out[1], info, out[8] != 0, out[7]
 end
 
+"""Device-resident `solvehartreefock` for `HartreeFockBDG` (Superconductivity/hartreefock.jl:5-159):
+`h`, `v` the electron-sector Hops, `ρ_init` the Nambu density matrix Hops (`ρ.h`); linear
+mixing, the BdG chemical potential and density matrix per iteration (`lqm_scf_hf_bdg`).
+Returns (ρ (Nambu Hops), ϵ_GS, info, converged, residual)."""
+function cuda_solvehartreefock_bdg(h, v, ρ_init::Hops, filling::Real, ks::AbstractMatrix{Float64}, exec::CudaExec;
+                                   T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
+                                   log_callback=nothing, hartree::Bool=true, fock::Bool=true)
+    ctx = context(exec.device)
+    set_functional!(ctx, hartree, fock, nothing)
+    dh = upload(ctx, h)
+    dv = upload(ctx, v)
+    Lk = collect(keys(ρ_init))
+    d = length(first(Lk))
+    n2 = size(ρ_init[first(Lk)], 1)
+    L = Int64[k[i] for i in 1:d, k in Lk]
+    rho = Array{ComplexF64}(undef, n2, n2, length(Lk))
+    for (i, k) in enumerate(Lk)
+        rho[:, :, i] .= ρ_init[k]
+    end
+    out = zeros(Float64, 10)
+    LOG_CB[] = log_callback
+    cb = @cfunction(_log_trampoline, Cint, (Int64, Float64, Float64, Float64, Float64, Float64, Float64,
+                                             Float64, Ptr{Cvoid}))
+    check(ctx, ccall((:lqm_scf_hf_bdg, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Float64, Float64, Float64, Float64, Int64, Int64,
+         Ptr{Int64}, Ptr{ComplexF64}, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}),
+        ctx.ptr, dh.ptr, dv.ptr, size(ks, 2), Matrix{Float64}(ks), Float64(filling), Float64(T), Float64(β),
+        Float64(tol), iterations, length(Lk), L, rho, cb, C_NULL, out))
+    LOG_CB[] = nothing
+    ρ = Hops(Dict(k => rho[:, :, i] for (i, k) in enumerate(Lk)))
+    info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵP=out[10], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
+    ρ, out[1], info, out[8] != 0, out[7]
+end
+
 """`commutator_kspace_norm(H, ρ, ks; kweights)` (Meanfield/selfconsistent.jl:130-166) on the
 device (`lqm_commutator_norm`)."""
 function cuda_commutator_kspace_norm(H, ρ, ks::AbstractMatrix{Float64}, exec::CudaExec;

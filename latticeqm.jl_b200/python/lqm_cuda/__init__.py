@@ -43,7 +43,7 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg",
 ]
 
 
@@ -105,6 +105,7 @@ _SIG = {
     "lqm_bdg_densitymatrix": [_P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, ctypes.POINTER(_D)],
     "lqm_bdg_filling": [_P, _P, _I64, _P, _P, _D, _D, ctypes.POINTER(_D)],
     "lqm_bdg_chemicalpotential": [_P, _P, _I64, _P, _P, _D, _D, _D, _D, ctypes.POINTER(_D)],
+    "lqm_scf_hf_bdg": [_P, _P, _P, _I64, _P, _D, _D, _D, _D, _I64, _I64, _P, _P, LOG_CB, _P, _P],
     "lqm_bandmatrix_partial": [_P, _P, _I64, _P, _I64, _D, ctypes.c_int, ctypes.c_int, _P, _P],
     "lqm_densitymatrix_partial": [_P, _P, _I64, _P, _P, _D, _D, _I64, _D, ctypes.c_int, _I64, _P, _P,
                                   ctypes.POINTER(_D)],
@@ -698,4 +699,39 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, ite
     eJ = _D()
     ctx.check(_lib.lqm_ctx_scf_exchange_energy(ctx.handle, ctypes.byref(eJ)))
     mf = MFInfo(mu=out[1], eH=out[2], eF=out[3], eband=out[4], ekin=out[5], iterations=int(out[8]), eJ=eJ.value)
+    return HFResult(rho_out, out[0], mf, bool(out[7]), out[6])
+
+
+BdGMFInfo = namedtuple("BdGMFInfo", ["mu", "eH", "eF", "eP", "eband", "ekin", "iterations"])
+
+
+def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
+                         log_callback=None, hartree=True, fock=True, ctx=None):
+    """``solvehartreefock(h::BdGOperator, v, ρ_init::BdGOperator, filling, ks; T, β, tol,
+    iterations)``: Hartree-Fock with the pairing channel (HartreeFockBDG,
+    Superconductivity/hartreefock.jl:5-159) on the device (``lqm_scf_hf_bdg``).  ``h`` and
+    ``v`` are the electron-sector Hops (order d), ``rho_init`` the Nambu density matrix
+    (order 2d).  Returns (ρ, ϵ_GS, mf, converged, residual)."""
+    ctx = ctx or default_context()
+    _set_functional(ctx, hartree, fock, None)
+    hd = _as_device_hops(h, ctx)
+    vd = _as_device_hops(v, ctx)
+    ks = _ks(ks, hd.d)
+    Lkeys = list(rho_init.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    rho = np.asfortranarray(np.stack([np.asarray(rho_init[L], np.complex128) for L in Lkeys], -1))
+    out = np.zeros(10)
+
+    def _cb(it, E, res, ekin, eband, eH, eF, mu, user):
+        if log_callback is None:
+            return 0
+        r = log_callback(int(it), E, res, dict(ekin=ekin, eband=eband, eH=eH, eF=eF, mu=mu))
+        return 1 if r is False else 0
+
+    cb = LOG_CB(_cb)
+    ctx.check(_lib.lqm_scf_hf_bdg(ctx.handle, hd.handle, vd.handle, ks.shape[1], _ptr(ks), float(filling), float(T),
+                                  float(beta), float(tol), int(iterations), len(Lkeys), _ptr(Lk), _ptr(rho), cb, None,
+                                  _ptr(out)))
+    rho_out = {L: np.array(rho[:, :, i]) for i, L in enumerate(Lkeys)}
+    mf = BdGMFInfo(mu=out[1], eH=out[2], eF=out[3], eP=out[9], eband=out[4], ekin=out[5], iterations=int(out[8]))
     return HFResult(rho_out, out[0], mf, bool(out[7]), out[6])

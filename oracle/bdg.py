@@ -75,3 +75,89 @@ def bdg_chemicalpotential(H, ks, filling, T=0.01, w=None, mu_lo=-100.0, mu_hi=10
     lo = max(mu_lo, float(bands.min()) - 1.0)
     hi = min(mu_hi, float(bands.max()) + 1.0)
     return K.bisect_float(lambda m: bdg_filling(H, ks, m, T, w) - filling, lo, hi)
+
+
+class HartreeFockBDG:
+    """Superconductivity/hartreefock.jl:5-159 (HartreeFockBDG): the electron functional of
+    HartreeFock on rho_e (Fock -v .* rho_e, Hartree diag(V0 diag rho_e[0])) and the pairing
+    field DeltaMF[L] = v[L] .* rhoD[L] (keys h + v + rhoD), with eP = 1/2 sum Re(|rhoD|^2 v);
+    hMF = BdGOperator(hMF_e, DeltaMF).  rho is a Nambu Hops of order 2d."""
+
+    def __init__(self, h, v, hartree=True, fock=True):
+        from .meanfield import HartreeFock
+        self.hf = HartreeFock(h, v, hartree=hartree, fock=fock)
+        self.h, self.v, self.fock = h, v, fock
+        self.mu = 0.0
+        self.eH = self.eF = self.eP = self.eband = self.ekin = 0.0
+        self.hMF_e = None
+        self.DMF = None
+
+    def __call__(self, rho):
+        d = next(iter(self.h.values())).shape[0]
+        rho_e = {L: M[:d, :d] for L, M in rho.items()}
+        rhoD = {L: M[:d, d:] for L, M in rho.items()}
+        self.hf(rho_e)
+        self.hMF_e = self.hf.hMF
+        keys = list(self.h.keys()) + [L for L in list(self.v.keys()) + list(rhoD.keys()) if L not in self.h]
+        seen, ordered = set(), []
+        for L in keys:
+            if L not in seen:
+                seen.add(L)
+                ordered.append(L)
+        self.DMF = {L: np.zeros((d, d), complex) for L in ordered}
+        if self.fock:
+            for L, vL in self.v.items():
+                if L in rhoD:
+                    self.DMF[L] = self.DMF[L] + vL * rhoD[L]
+        self.eH, self.eF = self.hf.eH, self.hf.eF
+        self.eP = float(np.real(0.5 * sum(np.sum(rhoD[L] * np.conj(rhoD[L]) * vL)
+                                          for L, vL in self.v.items() if L in rhoD))) if self.fock else 0.0
+        return self
+
+    def hMF(self):
+        return bdg_operator(self.hMF_e, self.DMF)
+
+    def doublecounting(self):
+        return self.eH + self.eF + self.eP
+
+
+def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
+                         hartree=True, fock=True, log=None):
+    """solvehartreefock with a Nambu h (Meanfield/selfconsistent.jl:256-336 with the BdG
+    methods of Superconductivity: mu from chemicalpotential(::BdGOperator), rho and the band
+    energy from getdensitymatrix!(::BdGOperator)); linear mixing (fixedpoint.jl:143-161).
+    h is the electron-sector Hops (HartreeFock(h::BdGOperator, v) keeps copyelectronsector(h))."""
+    from .meanfield import hermitianize, is_hermitian
+    rho0 = {L: M.copy() for L, M in rho_init.items()}
+    if not is_hermitian(rho0):
+        hermitianize(rho0)
+    rho1 = {L: M.copy() for L, M in rho0.items()}
+    hf = HartreeFockBDG(h, v, hartree=hartree, fock=fock)
+    nk = ks.shape[1]
+    w = np.full(nk, 1.0 / nk)
+    converged, residual, it, E = False, np.inf, 0, 0.0
+    while it < iterations:
+        it += 1
+        hf(rho0)
+        HB = hf.hMF()
+        hf.mu = bdg_chemicalpotential(HB, ks, filling, T)
+        rho_new, eband = bdg_densitymatrix(HB, ks, w, hf.mu, T, list(rho1.keys()))
+        hf.eband = eband
+        hf.ekin = eband - 2 * hf.doublecounting()
+        E = eband - hf.doublecounting()
+        for L in rho0:
+            rho1[L] = beta * rho_new[L] + (1 - beta) * rho0[L]
+        diff = np.linalg.norm([np.linalg.norm(rho1[L] - rho0[L]) for L in rho0])
+        nrm = np.linalg.norm([np.linalg.norm(rho1[L]) for L in rho0])
+        residual = diff / nrm if nrm > np.finfo(float).eps else diff
+        for L in rho0:
+            rho0[L] = rho1[L].copy()
+        if log is not None:
+            log(it, E, residual, hf.ekin, hf.eband, hf.eH, hf.eF, hf.mu)
+        if residual < tol:
+            converged = True
+            break
+    hf(rho1)
+    hf.ekin = hf.eband - 2 * hf.doublecounting()
+    E = hf.eband - hf.doublecounting()
+    return rho1, E, hf, converged, residual, it

@@ -421,3 +421,34 @@ def test_bdg_paths_match_oracle(lqm, ctx):
     mu_ref = BDG.bdg_chemicalpotential(HB, ks, 0.45, T=0.05)
     assert abs(mu - mu_ref) <= 1e-9
     assert abs(lqm.bdg_filling(HB, ks, mu, T=0.05, ctx=ctx) - 0.45) <= 1e-10
+
+
+def test_bdg_scf_matches_oracle(lqm, ctx):
+    """HartreeFockBDG SCF (Superconductivity/hartreefock.jl:5-159 in the SCF loop, BdG mu and
+    rho) through lqm_scf_hf_bdg against the oracle: spinful graphene with attractive Hubbard
+    U = -3 (sigma_x mode) from a small singlet pairing guess, 6 iterations of linear mixing
+    (beta = 0.5, T = 0.05) on a 6 x 6 grid; then a superconducting solution holds eP < 0."""
+    from oracle import bdg as BDG
+    lat = L.honeycomb()
+    h = M.graphene(lat, spin=True)
+    v = M.hubbard_v(lat, U=-3.0)
+    r0 = np.zeros((8, 8), complex)
+    r0[:4, :4] = 0.5 * np.eye(4)
+    r0[4:, 4:] = 0.5 * np.eye(4)
+    D = np.zeros((4, 4), complex)
+    for i in range(2):
+        D[2 * i, 2 * i + 1], D[2 * i + 1, 2 * i] = 0.1, -0.1
+    r0[:4, 4:] = D
+    r0[4:, :4] = D.conj().T
+    rho = {R: np.zeros((8, 8), complex) for R in h}
+    rho[(0, 0)] = r0
+    ks = L.regulargrid(6 * 6)
+    kw = dict(T=0.05, beta=0.5, tol=0.0, iterations=6)
+    res = lqm.solvehartreefock_bdg(h, v, rho, 0.5, ks, ctx=ctx, **kw)
+    rho_ref, E_ref, hf_ref, _, resid, it = BDG.solvehartreefock_bdg(h, v, rho, 0.5, ks, **kw)
+    assert res.mf.iterations == it == 6
+    assert abs(res.mf.mu - hf_ref.mu) <= 1e-9
+    assert abs(res.energy - E_ref) <= 1e-9 and abs(res.mf.eP - hf_ref.eP) <= 1e-9
+    assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in rho) <= 1e-9
+    assert abs(res.residual - resid) <= 1e-9
+    assert res.mf.eP < -1e-3

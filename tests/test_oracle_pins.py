@@ -490,3 +490,27 @@ def test_bdg_oracle_pins():
     Hp = BDG.bdg_operator(h, {z: 0.2 * np.eye(2, dtype=complex)})
     mu = BDG.bdg_chemicalpotential(Hp, ks8, 0.4, T=0.05)
     assert abs(BDG.bdg_filling(Hp, ks8, mu, T=0.05) - 0.4) < 1e-12
+
+
+def test_bdg_pairing_functional_oracle_pins():
+    """test/test_superconductivity.jl:230-275 on the oracle's HartreeFockBDG: the pairing
+    field DeltaMF = v .* rhoD follows the phase of rhoD (phase covariance), and
+    eP = 1/2 sum v |rhoD|^2 = -0.09 enters the double counting."""
+    from oracle import bdg as BDG
+    h = {(0,): np.zeros((2, 2), complex)}
+    v = {(0,): np.array([[0, -1], [-1, 0]], complex)}
+    F = np.array([[0, 1], [-1, 0]], complex)
+
+    def pairing_update(theta):
+        rho = BDG.bdg_operator({(0,): np.zeros((2, 2), complex)}, {(0,): np.exp(1j * theta) * F})
+        hf = BDG.HartreeFockBDG(h, v, hartree=False, fock=True)(rho)
+        return hf.DMF[(0,)].copy()
+
+    th = 0.37 * math.pi
+    D0, Dt = pairing_update(0.0), pairing_update(th)
+    assert abs(Dt[0, 1] / D0[0, 1] - np.exp(1j * th)) < 1e-12
+    assert abs(Dt[1, 0] / D0[1, 0] - np.exp(1j * th)) < 1e-12
+    rho = BDG.bdg_operator({(0,): np.zeros((2, 2), complex)}, {(0,): np.array([[0, 0.3], [-0.3, 0]], complex)})
+    hf = BDG.HartreeFockBDG(h, v, hartree=False, fock=True)(rho)
+    assert abs(hf.eP + 0.09) < 1e-12
+    assert abs(hf.doublecounting() - (hf.eH + hf.eF + hf.eP)) < 1e-14
