@@ -278,8 +278,9 @@ int lqm_bdg_chemicalpotential(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const
  * with the BdG chemical potential and density matrix (operators.jl:139-155,
  * green.jl:38-54).  h, v: the electron-sector Hops (order d); rho_inout: the Nambu
  * density matrix, order 2d, nL keys (closed under L -> -L, the zero key present);
- * k-weights 1/nk; linear mixing with beta and the relative residual; the context's
- * Hartree/Fock switches (no exchange kernel).  out[10] = {E, mu, eH, eF, eband, ekin,
+ * k-weights 1/nk; the context's SCF acceleration (linear or Anderson), residual
+ * (relative density change or ||[HB, rho0]||) and Hartree/Fock switches (no
+ * exchange kernel).  out[10] = {E, mu, eH, eF, eband, ekin,
  * residual, converged, iterations, eP} with E = eband - (eH + eF + eP). */
 int lqm_scf_hf_bdg(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, const double* ks,
                    double filling, double T, double beta, double tol, int64_t maxiter, int64_t nL,

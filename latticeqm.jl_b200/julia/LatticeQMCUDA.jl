@@ -436,12 +436,23 @@ end
 
 """Device-resident `solvehartreefock` for `HartreeFockBDG` (Superconductivity/hartreefock.jl:5-159):
 `h`, `v` the electron-sector Hops, `ρ_init` the Nambu density matrix Hops (`ρ.h`); linear
-mixing, the BdG chemical potential and density matrix per iteration (`lqm_scf_hf_bdg`).
+mixing or Anderson acceleration, the density or commutator residual, the BdG chemical
+potential and density matrix per iteration (`lqm_scf_hf_bdg`).
 Returns (ρ (Nambu Hops), ϵ_GS, info, converged, residual)."""
 function cuda_solvehartreefock_bdg(h, v, ρ_init::Hops, filling::Real, ks::AbstractMatrix{Float64}, exec::CudaExec;
                                    T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
-                                   log_callback=nothing, hartree::Bool=true, fock::Bool=true)
+                                   log_callback=nothing, hartree::Bool=true, fock::Bool=true,
+                                   acceleration::Symbol=:linear, anderson_depth::Int=5,
+                                   residual_norm::Symbol=:density)
     ctx = context(exec.device)
+    acceleration in (:linear, :anderson) ||
+        throw(ArgumentError("acceleration must be :linear or :anderson, got $(acceleration)"))
+    residual_norm in (:density, :commutator) ||
+        throw(ArgumentError("residual_norm must be :density or :commutator, got $(residual_norm)"))
+    check(ctx, ccall((:lqm_ctx_set_scf_acceleration, LIB[]), Cint, (Ptr{Cvoid}, Cint), ctx.ptr,
+                     acceleration === :anderson ? anderson_depth : 0))
+    check(ctx, ccall((:lqm_ctx_set_scf_residual, LIB[]), Cint, (Ptr{Cvoid}, Cint), ctx.ptr,
+                     residual_norm === :commutator ? 1 : 0))
     set_functional!(ctx, hartree, fock, nothing)
     dh = upload(ctx, h)
     dv = upload(ctx, v)

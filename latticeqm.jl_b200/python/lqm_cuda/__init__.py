@@ -706,13 +706,22 @@ BdGMFInfo = namedtuple("BdGMFInfo", ["mu", "eH", "eF", "eP", "eband", "ekin", "i
 
 
 def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
-                         log_callback=None, hartree=True, fock=True, ctx=None):
+                         log_callback=None, hartree=True, fock=True, acceleration="linear", anderson_depth=5,
+                         residual_norm="density", ctx=None):
     """``solvehartreefock(h::BdGOperator, v, ρ_init::BdGOperator, filling, ks; T, β, tol,
     iterations)``: Hartree-Fock with the pairing channel (HartreeFockBDG,
     Superconductivity/hartreefock.jl:5-159) on the device (``lqm_scf_hf_bdg``).  ``h`` and
     ``v`` are the electron-sector Hops (order d), ``rho_init`` the Nambu density matrix
     (order 2d).  Returns (ρ, ϵ_GS, mf, converged, residual)."""
     ctx = ctx or default_context()
+    acceleration = str(acceleration).lstrip(":")
+    residual_norm = str(residual_norm).lstrip(":")
+    if acceleration not in ("linear", "anderson"):
+        raise ValueError(f"acceleration must be 'linear' or 'anderson', got {acceleration!r}")
+    if residual_norm not in ("density", "commutator"):
+        raise ValueError(f"residual_norm must be :density or :commutator, got {residual_norm!r}")
+    ctx.check(_lib.lqm_ctx_set_scf_acceleration(ctx.handle, int(anderson_depth) if acceleration == "anderson" else 0))
+    ctx.check(_lib.lqm_ctx_set_scf_residual(ctx.handle, 1 if residual_norm == "commutator" else 0))
     _set_functional(ctx, hartree, fock, None)
     hd = _as_device_hops(h, ctx)
     vd = _as_device_hops(v, ctx)

@@ -122,12 +122,18 @@ class HartreeFockBDG:
 
 
 def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
-                         hartree=True, fock=True, log=None):
+                         hartree=True, fock=True, log=None, acceleration="linear", anderson_depth=5,
+                         residual_norm="density"):
     """solvehartreefock with a Nambu h (Meanfield/selfconsistent.jl:256-336 with the BdG
     methods of Superconductivity: mu from chemicalpotential(::BdGOperator), rho and the band
-    energy from getdensitymatrix!(::BdGOperator)); linear mixing (fixedpoint.jl:143-161).
+    energy from getdensitymatrix!(::BdGOperator)); linear mixing (fixedpoint.jl:143-161), or
+    Anderson acceleration with the Hermitian projection of the Nambu iterate
+    (Superconductivity/hartreefock.jl:57-58); the relative or the commutator residual.
     h is the electron-sector Hops (HartreeFock(h::BdGOperator, v) keeps copyelectronsector(h))."""
-    from .meanfield import hermitianize, is_hermitian
+    from .meanfield import (hermitianize, is_hermitian, anderson_update, _flatten, _unflatten,
+                            commutator_kspace_norm)
+    use_anderson = acceleration == "anderson" and anderson_depth > 0
+    hist_x, hist_f = [], []
     rho0 = {L: M.copy() for L, M in rho_init.items()}
     if not is_hermitian(rho0):
         hermitianize(rho0)
@@ -140,16 +146,30 @@ def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
         it += 1
         hf(rho0)
         HB = hf.hMF()
+        comm = commutator_kspace_norm(HB, rho0, ks) if residual_norm == "commutator" else None
         hf.mu = bdg_chemicalpotential(HB, ks, filling, T)
         rho_new, eband = bdg_densitymatrix(HB, ks, w, hf.mu, T, list(rho1.keys()))
         hf.eband = eband
         hf.ekin = eband - 2 * hf.doublecounting()
         E = eband - hf.doublecounting()
-        for L in rho0:
-            rho1[L] = beta * rho_new[L] + (1 - beta) * rho0[L]
+        if use_anderson:
+            keys = sorted(rho0.keys())
+            fx, ff = _flatten(rho0, keys), _flatten(rho_new, keys)
+            hist_x.append(fx.copy())
+            hist_f.append(ff.copy())
+            while len(hist_x) > anderson_depth + 1:
+                hist_x.pop(0)
+                hist_f.pop(0)
+            _unflatten(rho1, anderson_update(fx, ff, hist_x, hist_f, beta), keys)
+            hermitianize(rho1)
+        else:
+            for L in rho0:
+                rho1[L] = beta * rho_new[L] + (1 - beta) * rho0[L]
         diff = np.linalg.norm([np.linalg.norm(rho1[L] - rho0[L]) for L in rho0])
         nrm = np.linalg.norm([np.linalg.norm(rho1[L]) for L in rho0])
         residual = diff / nrm if nrm > np.finfo(float).eps else diff
+        if comm is not None:
+            residual = comm
         for L in rho0:
             rho0[L] = rho1[L].copy()
         if log is not None:

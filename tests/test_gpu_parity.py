@@ -452,3 +452,32 @@ def test_bdg_scf_matches_oracle(lqm, ctx):
     assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in rho) <= 1e-9
     assert abs(res.residual - resid) <= 1e-9
     assert res.mf.eP < -1e-3
+
+
+def test_bdg_scf_anderson_and_commutator_match_oracle(lqm, ctx):
+    """lqm_scf_hf_bdg with Anderson acceleration (depth 3, the Nambu iterate projected
+    Hermitian) and with the commutator residual ||[HB, rho]|| against the oracle, 6
+    iterations of the attractive-U graphene case.  Bound 1e-8 for Anderson (its
+    least-squares solves round differently)."""
+    from oracle import bdg as BDG
+    lat = L.honeycomb()
+    h = M.graphene(lat, spin=True)
+    v = M.hubbard_v(lat, U=-3.0)
+    r0 = np.zeros((8, 8), complex)
+    r0[:4, :4] = 0.5 * np.eye(4)
+    r0[4:, 4:] = 0.5 * np.eye(4)
+    for i in range(2):
+        r0[2 * i, 4 + 2 * i + 1], r0[2 * i + 1, 4 + 2 * i] = 0.1, -0.1
+    r0[4:, :4] = r0[:4, 4:].conj().T
+    rho = {R: np.zeros((8, 8), complex) for R in h}
+    rho[(0, 0)] = r0
+    ks = L.regulargrid(6 * 6)
+    for extra, tolr in ((dict(acceleration="anderson", anderson_depth=3), 1e-8),
+                        (dict(residual_norm="commutator"), 1e-9)):
+        kw = dict(T=0.05, beta=0.5, tol=0.0, iterations=6, **extra)
+        res = lqm.solvehartreefock_bdg(h, v, rho, 0.5, ks, ctx=ctx, **kw)
+        rho_ref, E_ref, hf_ref, _, resid, it = BDG.solvehartreefock_bdg(h, v, rho, 0.5, ks, **kw)
+        assert res.mf.iterations == it == 6
+        assert abs(res.energy - E_ref) <= tolr
+        assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in rho) <= tolr
+        assert abs(res.residual - resid) <= tolr * max(1.0, resid)
