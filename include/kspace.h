@@ -221,6 +221,13 @@ int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int6
  * det(S^H S')/|det|, and F[i + (NX-1) j] = arg(plaquette product)/(2 pi) for
  * the (NX-1) x (NY-1) plaquettes.  Two-dimensional Hops only. */
 int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, double* F);
+/* Berry flux of several band manifolds on one state grid: flux[s] = sum of the
+ * plaquette phases of lqm_berry over the bands set_bands[set_ptr[s] .. set_ptr[s+1])
+ * (0-based; set_ptr has nsets + 1 entries).  Single-band sets give getcherns
+ * (src/modules/Spectrum/berry.jl:378-382), the sets {0..n-1} the gap Chern numbers
+ * of gapcherns (:470-487) before rounding.  One eigen pass over the NX x NY grid. */
+int lqm_berry_flux(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nsets, const int64_t* set_ptr,
+                   const int64_t* set_bands, double* flux);
 
 /* The HartreeFock functional hf(rho) (src/modules/Meanfield/hartreefock.jl:184-228,
  * 247-289,298-410): hMF = h - v .* rho (Fock) + the Hartree diagonal (+ the

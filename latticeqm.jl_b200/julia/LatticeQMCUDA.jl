@@ -192,6 +192,42 @@ function cuda_berry(H, NX::Int, NY::Int, bandindices::AbstractVector{<:Integer},
     midkgrid, F
 end
 
+"""Summed plaquette phases of each band manifold (1-based band index vectors) on one
+NX x NY state grid (`lqm_berry_flux`)."""
+function cuda_berry_flux(H, NX::Int, NY::Int, sets::AbstractVector, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    ptr = Int64[0; cumsum(length.(sets))]
+    cols = Int64[b - 1 for s in sets for b in s]
+    out = zeros(Float64, length(sets))
+    check(ctx, ccall((:lqm_berry_flux, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int64, Int64, Ptr{Int64}, Ptr{Int64}, Ptr{Float64}),
+        ctx.ptr, dh.ptr, NX, NY, length(sets), ptr, cols, out))
+    out
+end
+
+"""`getcherns(H, NX, NY, bands)` (Spectrum/berry.jl:378-382) on the device; `bands` 1-based,
+all bands when empty."""
+function cuda_getcherns(H, NX::Int, NY::Int, bands::AbstractVector, exec::CudaExec)
+    NY = NY < 1 ? NX : NY
+    n = size(H[first(keys(H))], 1)
+    bs = isempty(bands) ? collect(1:n) : collect(bands)
+    cuda_berry_flux(H, NX, NY, [[b] for b in bs], exec)
+end
+
+"""`gapcherns(H, NX, NY; gaptol)` (Spectrum/berry.jl:470-487) on the device: the gaps from
+the device bands on the statesgrid k-points, their Chern numbers from one state grid."""
+function cuda_gapcherns(H, NX::Int, NY::Int, exec::CudaExec; gaptol::Real=1e-6)
+    NY = NY < 1 ? NX : NY
+    ks = reduce(hcat, vec([[x; y] for x in range(0; stop=1, length=NX), y in range(0; stop=1, length=NY)])) .+ 1.34e-8
+    E = cuda_bandmatrix(H, Matrix{Float64}(ks), exec)
+    emin, emax = vec(minimum(E; dims=2)), vec(maximum(E; dims=2))
+    gaps = [(; n=m, elo=emax[m], ehi=emin[m+1]) for m in 1:size(E, 1)-1 if emin[m+1] - emax[m] > gaptol]
+    isempty(gaps) && return @NamedTuple{n::Int, elo::Float64, ehi::Float64, chern::Int}[]
+    flux = cuda_berry_flux(H, NX, NY, [collect(1:g.n) for g in gaps], exec)
+    [(; g.n, g.elo, g.ehi, chern=round(Int, f)) for (g, f) in zip(gaps, flux)]
+end
+
 """`opticalconductivity(frequencies, H, J1, J2, ks; μ, Γ, T)`
 (LinearResponse/opticalconductivity.jl:101-127) on the device (`lqm_opticalconductivity`):
 the Kubo correlator χ(ω).  `J1`, `J2` are Hops (e.g. from `getcurrentoperators(lat, H)`)."""

@@ -43,7 +43,7 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux",
 ]
 
 
@@ -95,6 +95,7 @@ _SIG = {
     "lqm_density": [_P, _P, _I64, _P, _D, _P],
     "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
+    "lqm_berry_flux": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
     "lqm_ctx_set_scf_residual": [_P, ctypes.c_int],
@@ -540,6 +541,64 @@ def commutator_kspace_norm(H, rho, ks, kweights=None, multimode="cuda", ctx=None
     ctx.check(_lib.lqm_commutator_norm(ctx.handle, Hd.handle, Rd.handle, ks.shape[1], _ptr(ks), _ptr(w),
                                        ctypes.byref(out)))
     return out.value
+
+
+def berry_flux(H, NX, NY, band_sets, ctx=None):
+    """Summed plaquette phases of each band manifold in ``band_sets`` (lists of 0-based
+    band indices) on one NX x NY state grid (``lqm_berry_flux``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    sets = [list(map(int, s)) for s in band_sets]
+    ptr = np.ascontiguousarray(np.cumsum([0] + [len(s) for s in sets]), dtype=np.int64)
+    cols = np.ascontiguousarray([b for s in sets for b in s], dtype=np.int64)
+    out = np.zeros(len(sets))
+    ctx.check(_lib.lqm_berry_flux(ctx.handle, Hd.handle, int(NX), int(NY), len(sets), _ptr(ptr), _ptr(cols),
+                                  _ptr(out)))
+    return out
+
+
+def getcherns(H, NX, NY=0, bands=None, multimode="cuda", ctx=None):
+    """``getcherns(H, NX, NY, bands)`` (Spectrum/berry.jl:378-382) with 0-based band
+    indices (all bands when None): the Chern number of each band, unrounded."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    NY = NX if NY < 1 else NY
+    bands = list(range(Hd.n)) if bands is None else list(bands)
+    return list(berry_flux(Hd, NX, NY, [[b] for b in bands], ctx=ctx))
+
+
+def _berry_grid(NX, NY):
+    i = np.tile(np.arange(NX), NY)
+    j = np.repeat(np.arange(NY), NX)
+    return np.asfortranarray(np.vstack([i / (NX - 1), j / (NY - 1)]) + 1.34e-8)
+
+
+def spectralgaps(H, NX, NY=0, gaptol=1e-6, multimode="cuda", ctx=None):
+    """``spectralgaps(H, NX, NY; gaptol)`` (Spectrum/berry.jl:421-442): [(n, elo, ehi)] for
+    every gap wider than gaptol between the grid maximum of band n and the grid minimum of
+    band n + 1 (n the number of bands below), from the device bands on the statesgrid
+    k-points."""
+    _check_mode(multimode)
+    NY = NX if NY < 1 else NY
+    E, _ = bandmatrix(H, _berry_grid(NX, NY), ctx=ctx)
+    emin, emax = E.min(axis=1), E.max(axis=1)
+    return [(m + 1, float(emax[m]), float(emin[m + 1])) for m in range(E.shape[0] - 1)
+            if emin[m + 1] - emax[m] > gaptol]
+
+
+def gapcherns(H, NX, NY=0, gaptol=1e-6, multimode="cuda", ctx=None):
+    """``gapcherns(H, NX, NY; gaptol)`` (Spectrum/berry.jl:470-487): [(n, elo, ehi, chern)]
+    with chern the rounded Berry flux of the lowest n bands (one state grid for all gaps)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    NY = NX if NY < 1 else NY
+    gaps = spectralgaps(Hd, NX, NY, gaptol, ctx=ctx)
+    if not gaps:
+        return []
+    flux = berry_flux(Hd, NX, NY, [list(range(m)) for m, _, _ in gaps], ctx=ctx)
+    return [(m, lo, hi, int(round(f))) for (m, lo, hi), f in zip(gaps, flux)]
 
 
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):

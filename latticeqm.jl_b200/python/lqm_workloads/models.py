@@ -260,6 +260,66 @@ def triangular_hubbard(L_super=6, t=-1.0, tp=0.2, U=4.0):
     return lat, h, v
 
 
+def nn_bond_length(lat):
+    """The shortest nonzero distance between orbitals of neighbouring cells
+    (Operators/haldane.jl, _nnbondlength)."""
+    pos = lat.positions()
+    d = math.inf
+    for c in L.product_first_fastest(range(-1, 2), range(-1, 2)):
+        sh = lat.A @ np.array(c, float)
+        dist = np.linalg.norm(pos[:, :, None] + sh[:, None, None] - pos[:, None, :], axis=0)
+        nz = dist[dist > SQRT_EPS]
+        if nz.size:
+            d = min(d, float(nz.min()))
+    return d
+
+
+def add_haldane(h, lat, t2, phi=math.pi / 2, cellrange=1):
+    """``addhaldane!(hops, lat, t2; ϕ)`` (Operators/haldane.jl, naive path): for every pair
+    (i in cell R, j in cell 0) at distance sqrt(3) a0, with R0 their first common nearest
+    neighbour found over the cells {-1..1}^2 and the orbitals, x = r_i + A R - R0,
+    y = r_j - R0: h[R][i, j] += t2 exp(i phi sign(cross(-y, x))).  Returns a new dict."""
+    pos = lat.positions()
+    N = lat.norb
+    a0 = nn_bond_length(lat)
+    cells = L.product_first_fastest(range(-cellrange, cellrange + 1), range(-cellrange, cellrange + 1))
+    near = L.product_first_fastest(range(-1, 2), range(-1, 2))
+    out = {R: M.copy() for R, M in h.items()}
+    cross = lambda x, y: x[0] * y[1] - x[1] * y[0]
+    for R in cells:
+        sh = lat.A @ np.array(R, float)
+        for i in range(N):
+            for j in range(N):
+                ri, rj = pos[:, i] + sh, pos[:, j]
+                if not math.isclose(float(np.linalg.norm(ri - rj)), math.sqrt(3) * a0, rel_tol=1e-6):
+                    continue
+                found = None
+                for c in near:
+                    dc = lat.A @ np.array(c, float)
+                    for m in range(N):
+                        r0 = dc + pos[:, m]
+                        if (math.isclose(float(np.linalg.norm(ri - r0)), a0, rel_tol=1e-6)
+                                and math.isclose(float(np.linalg.norm(rj - r0)), a0, rel_tol=1e-6)):
+                            found = r0
+                            break
+                    if found is not None:
+                        break
+                if found is None:
+                    continue
+                x, y = ri - found, rj - found
+                if R not in out:
+                    out[R] = np.zeros((N, N), complex)
+                out[R][i, j] += t2 * np.exp(1j * phi * np.sign(cross(-y, x)))
+    return out
+
+
+def haldane_model(t1=-1.0, t2=0.1, phi=math.pi / 2):
+    """Honeycomb nearest-neighbour model t1 with the Haldane term t2 e^{±i phi}
+    (the model of test/test_haldane.jl)."""
+    lat = L.honeycomb()
+    return lat, add_haldane(nearestneighbor(lat, t1), lat, t2, phi)
+
+
 def bdg_operator(h, delta=None):
     """``BdGOperator(h[, Δ])`` (Superconductivity/types.jl:43-60,76-97): the Nambu Hops of
     order 2d with blocks [h_R 0; 0 -conj(h_R)] and, for every pairing key R (its partner

@@ -137,6 +137,40 @@ def opticalconductivity(omegas, h, J1, J2, ks, mu=0.0, gamma=0.025, T=0.1):
     return out * (-1j / ks.shape[1])
 
 
+def berry_grid(NX, NY):
+    """k-points of statesgrid (Spectrum/berry.jl:49-82): range(0, 1, length=N) per
+    direction, first index fastest, + 1.34e-8."""
+    return np.array([[i / (NX - 1), j / (NY - 1)] for j in range(NY) for i in range(NX)]).T + 1.34e-8
+
+
+def getcherns(h, NX, NY=0, bands=None):
+    """getcherns(H, NX, NY, bands) (Spectrum/berry.jl:378-382): per band the summed
+    plaquette phases of its single-band state grid (bands 0-based; all when None)."""
+    NY = NX if NY < 1 else NY
+    n = next(iter(h.values())).shape[0]
+    bands = list(range(n)) if bands is None else list(bands)
+    return [float(np.sum(berry(h, NX, NY, [b]))) for b in bands]
+
+
+def spectralgaps(h, NX, NY=0, gaptol=1e-6):
+    """spectralgaps(H, NX, NY; gaptol) (Spectrum/berry.jl:421-442): gaps between the
+    grid maximum of band n and the grid minimum of band n+1 wider than gaptol, as
+    (n, elo, ehi) with n the number of bands below (1-based count)."""
+    NY = NX if NY < 1 else NY
+    E, _ = bandmatrix(h, berry_grid(NX, NY))
+    emin, emax = E.min(axis=1), E.max(axis=1)
+    return [(m + 1, float(emax[m]), float(emin[m + 1])) for m in range(E.shape[0] - 1)
+            if emin[m + 1] - emax[m] > gaptol]
+
+
+def gapcherns(h, NX, NY=0, gaptol=1e-6):
+    """gapcherns(H, NX, NY; gaptol) (Spectrum/berry.jl:470-487): (n, elo, ehi, chern) per
+    gap, chern = round(sum(berry(states[:, :, :, 1:n])))."""
+    NY = NX if NY < 1 else NY
+    return [(m, lo, hi, int(round(float(np.sum(berry(h, NX, NY, list(range(m)))))))) for m, lo, hi in
+            spectralgaps(h, NX, NY, gaptol)]
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

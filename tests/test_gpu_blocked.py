@@ -6,6 +6,7 @@ small orders (``set_blocked_min_n(1)``) so that every model and pin of the
 plain path is checked through it.  Tolerances as in test_gpu_parity.py.
 """
 import json
+import math
 import os
 
 import numpy as np
@@ -332,3 +333,24 @@ def test_exchange_scf_blocked_path_matches_oracle(lqm, ctx):
     assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in M.KEYS9) <= RHO_TOL
     assert abs(res.energy - E_ref) <= 1e-9 * max(1.0, abs(E_ref))
     assert abs(res.mf.eJ - hf_ref.eJ) <= 1e-9 * max(1.0, abs(hf_ref.eJ))
+
+
+def test_chern_numbers_match_oracle(lqm, ctx):
+    """getcherns / spectralgaps / gapcherns (Spectrum/berry.jl:378-487) through
+    lqm_berry_flux and the device bands: the Haldane cases of test/test_haldane.jl:78-122
+    (band Chern numbers +-1, one gap at half filling with Chern +-1), and parity of the
+    unrounded band fluxes with the oracle on the spin-orbit triangular model (n = 96)."""
+    for phi, sgn in ((math.pi / 2, 1), (-math.pi / 2, -1)):
+        _, h = M.haldane_model(t2=0.1, phi=phi)
+        c = lqm.getcherns(h, 30, 30, ctx=ctx)
+        assert abs(c[0] - sgn) < 0.05 and abs(c[1] + sgn) < 0.05
+        assert max(abs(a - b) for a, b in zip(c, K.getcherns(h, 30, 30))) <= 1e-10
+        gaps = lqm.gapcherns(h, 30, gaptol=1e-3, ctx=ctx)
+        assert len(gaps) == 1 and gaps[0][0] == 1 and gaps[0][3] == sgn and gaps[0][1] < 0 < gaps[0][2]
+        ref = K.gapcherns(h, 30, gaptol=1e-3)
+        assert abs(gaps[0][1] - ref[0][1]) <= 1e-12 and abs(gaps[0][2] - ref[0][2]) <= 1e-12
+    h3 = M.batch_models()[2][1]
+    sets = [[0, 1, 2, 3], [0, 1], list(range(8))]
+    flux = lqm.berry_flux(h3, 8, 8, sets, ctx=ctx)
+    for f, s_ in zip(flux, sets):
+        assert abs(f - float(np.sum(K.berry(h3, 8, 8, s_)))) <= 1e-9

@@ -514,3 +514,18 @@ def test_bdg_pairing_functional_oracle_pins():
     hf = BDG.HartreeFockBDG(h, v, hartree=False, fock=True)(rho)
     assert abs(hf.eP + 0.09) < 1e-12
     assert abs(hf.doublecounting() - (hf.eH + hf.eF + hf.eP)) < 1e-14
+
+
+def test_haldane_chern_pins():
+    """test/test_haldane.jl:10-20,63-73,78-122 on the oracle: the Haldane model (t2 = 0.1,
+    phi = +-pi/2) has E(K) = -+3 sqrt(3) t2, band Chern numbers +-1 on a 30 x 30 grid, and
+    one gap at half filling with gap Chern number +-1."""
+    for phi, sgn in ((math.pi / 2, 1), (-math.pi / 2, -1)):
+        lat, h = M.haldane_model(t2=0.1, phi=phi)
+        e = np.linalg.eigvalsh(K.fouriersum(h, [1 / 3, -1 / 3]))
+        assert abs(e[0] + 0.5196152422706632) < 1e-12 and abs(e[1] - 0.5196152422706632) < 1e-12
+        c = K.getcherns(h, 30, 30)
+        assert abs(c[0] - sgn) < 0.05 and abs(c[1] + sgn) < 0.05
+        gaps = K.gapcherns(h, 30, gaptol=1e-3)
+        assert len(gaps) == 1 and gaps[0][0] == 1 and gaps[0][3] == sgn
+        assert gaps[0][1] < 0 < gaps[0][2]
