@@ -226,6 +226,12 @@ int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t n
  * (0-based; set_ptr has nsets + 1 entries).  Single-band sets give getcherns
  * (src/modules/Spectrum/berry.jl:378-382), the sets {0..n-1} the gap Chern numbers
  * of gapcherns (:470-487) before rounding.  One eigen pass over the NX x NY grid. */
+/* Abelian Berry curvature along a k-path, berryalongpath(H, kpoints)
+ * (src/modules/Spectrum/berry.jl:170-238): the path (2 x N, N >= 2) padded at both
+ * ends and shifted by 1.34e-6 |k_2 - k_1| (1, 1/sqrt 2); per point the plaquette of
+ * the four corners k +- (neighbour differences)/2 and their rotations by +-pi/2;
+ * out[i + n j] = the plaquette phase of band i at point j (n x N). */
+int lqm_berry_path(lqm_ctx* ctx, const lqm_hops* H, int64_t N, const double* kpoints, double* out);
 int lqm_berry_flux(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nsets, const int64_t* set_ptr,
                    const int64_t* set_bands, double* flux);
 

@@ -192,6 +192,18 @@ function cuda_berry(H, NX::Int, NY::Int, bandindices::AbstractVector{<:Integer},
     midkgrid, F
 end
 
+"""`berryalongpath(H, kpoints)` (Spectrum/berry.jl:170-238) on the device (`lqm_berry_path`):
+the n x N abelian plaquette phases along the path."""
+function cuda_berryalongpath(H, kpoints::AbstractMatrix{Float64}, exec::CudaExec)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    n = size(H[first(keys(H))], 1)
+    out = zeros(Float64, n, size(kpoints, 2))
+    check(ctx, ccall((:lqm_berry_path, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Ptr{Float64}),
+                     ctx.ptr, dh.ptr, size(kpoints, 2), Matrix{Float64}(kpoints), out))
+    out
+end
+
 """Summed plaquette phases of each band manifold (1-based band index vectors) on one
 NX x NY state grid (`lqm_berry_flux`)."""
 function cuda_berry_flux(H, NX::Int, NY::Int, sets::AbstractVector, exec::CudaExec)

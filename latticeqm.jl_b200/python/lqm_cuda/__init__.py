@@ -43,7 +43,7 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path",
 ]
 
 
@@ -96,6 +96,7 @@ _SIG = {
     "lqm_ldos": [_P, _P, _I64, _P, _I64, _P, _D, _P],
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
     "lqm_berry_flux": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
+    "lqm_berry_path": [_P, _P, _I64, _P, _P],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
     "lqm_ctx_set_scf_residual": [_P, ctypes.c_int],
@@ -554,6 +555,19 @@ def berry_flux(H, NX, NY, band_sets, ctx=None):
     out = np.zeros(len(sets))
     ctx.check(_lib.lqm_berry_flux(ctx.handle, Hd.handle, int(NX), int(NY), len(sets), _ptr(ptr), _ptr(cols),
                                   _ptr(out)))
+    return out
+
+
+def berryalongpath(H, kpoints, multimode="cuda", ctx=None):
+    """``berryalongpath(H, kpoints)`` (Spectrum/berry.jl:170-238): the abelian Berry
+    curvature (plaquette phase) of every band at every path point, (n, N)
+    (``lqm_berry_path``)."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    kp = _ks(kpoints, Hd.d)
+    out = np.zeros((Hd.n, kp.shape[1]), order="F")
+    ctx.check(_lib.lqm_berry_path(ctx.handle, Hd.handle, kp.shape[1], _ptr(kp), _ptr(out)))
     return out
 
 

@@ -137,6 +137,41 @@ def opticalconductivity(omegas, h, J1, J2, ks, mu=0.0, gamma=0.025, T=0.1):
     return out * (-1j / ks.shape[1])
 
 
+def _rot2(t):
+    # Structure/rotate.jl:8
+    return np.array([[math.cos(t), -math.sin(t)], [math.sin(t), math.cos(t)]])
+
+
+def berryalongpath(h, kpoints):
+    """Spectrum/berry.jl:170-238: per band and path point the abelian plaquette phase of
+    the corners kc + dR, dU, dD, dL (padded path, shifted by 1.34e-6 |k2 - k1| (1, 1/sqrt2))."""
+    kpoints = np.asarray(kpoints, float)
+    N = kpoints.shape[1]
+    n = next(iter(h.values())).shape[0]
+    k0 = kpoints[:, 0] - (kpoints[:, 1] - kpoints[:, 0])
+    kN1 = kpoints[:, N - 1] + (kpoints[:, N - 1] - kpoints[:, N - 2])
+    kp = np.hstack([k0[:, None], kpoints, kN1[:, None]])
+    kp = kp + 1.34e-6 * np.linalg.norm(kp[:, 1] - kp[:, 0]) * np.array([1.0, 0.7071067811865476])[:, None]
+    out = np.zeros((n, N))
+
+    def link(a, b):
+        z = np.vdot(a, b)
+        return z / abs(z)
+
+    for j in range(N):
+        kc = kp[:, j + 1]
+        dR = (kp[:, j + 2] - kc) / 2
+        dL = (kp[:, j] - kc) / 2
+        dU = (_rot2(math.pi / 2) @ dR + _rot2(-math.pi / 2) @ dL) / 2
+        dD = (_rot2(-math.pi / 2) @ dR + _rot2(math.pi / 2) @ dL) / 2
+        Us = [eigh_upper(fouriersum(h, kc + dk), True)[1] for dk in (dR, dU, dD, dL)]
+        for i in range(n):
+            R, U, D, Lf = (X[:, i] for X in Us)
+            z = link(R, U) * link(U, Lf) / link(D, Lf) / link(R, D)
+            out[i, j] = np.real(np.log(z) / (2j * math.pi))
+    return out
+
+
 def berry_grid(NX, NY):
     """k-points of statesgrid (Spectrum/berry.jl:49-82): range(0, 1, length=N) per
     direction, first index fastest, + 1.34e-8."""

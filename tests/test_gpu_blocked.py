@@ -354,3 +354,16 @@ def test_chern_numbers_match_oracle(lqm, ctx):
     flux = lqm.berry_flux(h3, 8, 8, sets, ctx=ctx)
     for f, s_ in zip(flux, sets):
         assert abs(f - float(np.sum(K.berry(h3, 8, 8, s_)))) <= 1e-9
+
+
+def test_berry_along_path_matches_oracle(lqm, ctx):
+    """berryalongpath(H, kpoints) (Spectrum/berry.jl:170-238) through lqm_berry_path against
+    the oracle: the Haldane model (gapped, non-degenerate bands) along its 60-point
+    Gamma-K-M-K'-Gamma-M path, and the two bands' phases of opposite sign at each point."""
+    lat, h = M.haldane_model(t2=0.1, phi=math.pi / 2)
+    kp = L.kpath(lat, 60)
+    b = lqm.berryalongpath(h, kp, ctx=ctx)
+    ref = K.berryalongpath(h, kp)
+    assert b.shape == ref.shape
+    assert np.max(np.abs(b - ref)) <= 1e-9
+    assert np.max(np.abs(b[0] + b[1])) <= 1e-9  # the two bands' curvatures cancel
