@@ -989,14 +989,27 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
 }
 
 // ---------------------------------------------------------------------------
-// 5. rho_k = U diag(f) U^H into out (n x n, leading dimension ldo).
-// Rows by lane (up to 4 per lane and pass), 4 columns per warp step; every
-// output entry accumulates over j in order.
+// 5. rho_k = U diag(f) U^H into out (n x n, leading dimension ldo), U unitary.
+// rho_k is Hermitian: only entries r <= c are accumulated (tiles of 4 rows per
+// lane by 4 columns per warp step; row slices entirely below the tile's columns
+// are skipped) and the lower triangle is written as their conjugates.  When
+// more occupations are exactly 1 than exactly 0 the complement
+// rho_k = I - sum_j (1 - f_j) u_j u_j^H skips the filled states, otherwise the
+// sum skips the empty ones.  Every output entry accumulates over j in order.
 // ---------------------------------------------------------------------------
 LQM_FN_NOINLINE void rho_from_U(const Team& T, int n, const double2* U, int ldu, const double* f, double2* out,
                                 int64_t ldo) {
+  int n0 = 0, n1 = 0;
+  for (int j = 0; j < n; ++j) {
+    n0 += (f[j] == 0.0);
+    n1 += (f[j] == 1.0);
+  }
+  const bool comp = n1 > n0;
   for (int r0 = 0; r0 < n; r0 += 4 * T.nl) {
     for (int c0 = 4 * T.wid; c0 < n; c0 += 4 * T.nw) {
+      // row slices q with a row <= c0 + 3 (uniform across the warp)
+      const int qn = (c0 + 3 < r0) ? 0 : ((c0 + 3 - r0) / T.nl + 1 < 4 ? (c0 + 3 - r0) / T.nl + 1 : 4);
+      if (qn == 0) continue;
       double2 acc[4][4];
       int rr[4];
 #pragma unroll
@@ -1006,27 +1019,35 @@ LQM_FN_NOINLINE void rho_from_U(const Team& T, int n, const double2* U, int ldu,
         for (int b = 0; b < 4; ++b) acc[q][b] = cmk(0.0, 0.0);
       }
       for (int j = 0; j < n; ++j) {
-        const double fj = f[j];
-        if (fj == 0.0) continue;
+        const double gj = comp ? 1.0 - f[j] : f[j];
+        if (gj == 0.0) continue;
         const double2* Uj = U + (int64_t)j * ldu;
         double2 cb[4], ua[4];
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
           const int c = c0 + b;
-          cb[b] = (c < n) ? cscale(fj, cconj(Uj[c])) : cmk(0.0, 0.0);
+          cb[b] = (c < n) ? cscale(gj, cconj(Uj[c])) : cmk(0.0, 0.0);
         }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) ua[q] = (rr[q] < n) ? Uj[rr[q]] : cmk(0.0, 0.0);
+        for (int q = 0; q < 4; ++q) ua[q] = (q < qn && rr[q] < n) ? Uj[rr[q]] : cmk(0.0, 0.0);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
+          if (q < qn)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[q][b] = cadd(acc[q][b], cmul(ua[q], cb[b]));
+            for (int b = 0; b < 4; ++b) acc[q][b] = cadd(acc[q][b], cmul(ua[q], cb[b]));
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (rr[q] < n && c0 + b < n) out[rr[q] + (int64_t)(c0 + b) * ldo] = acc[q][b];
+        for (int b = 0; b < 4; ++b) {
+          const int r = rr[q], c = c0 + b;
+          if (q < qn && r < n && c < n && r <= c) {
+            double2 v = acc[q][b];
+            if (comp) v = cmk(((r == c) ? 1.0 : 0.0) - v.x, -v.y);
+            out[r + (int64_t)c * ldo] = v;
+            if (r != c) out[c + (int64_t)r * ldo] = cconj(v);
+          }
+        }
     }
   }
   team_sync();

@@ -120,10 +120,17 @@ def test_emulated_tridiagonal_dc(emul, n):
 
 @pytest.mark.parametrize("n", [1, 5, 37, 96, 130])
 def test_emulated_rho_from_U(emul, n):
+    """rho = U f U^H for a unitary U, through both forms: the direct sum (more exact
+    zeros than ones among f) and the complement I - U (1 - f) U^H (more exact ones)."""
     rng = np.random.default_rng(n)
-    U = np.asfortranarray(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
-    f = rng.random(n)
-    f[::3] = 0.0
-    out = np.zeros((n, n), complex, order="F")
-    emul.lqm_emul_rho(n, U.ctypes.data_as(P), f.ctypes.data_as(P), out.ctypes.data_as(P))
-    assert np.max(np.abs(out - (U * f) @ U.conj().T)) < 1e-12 * n
+    U, _ = np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    U = np.asfortranarray(U)
+    for zeros, ones in ((slice(None, None, 3), slice(1, None, 5)), (slice(1, None, 5), slice(None, None, 3))):
+        f = rng.random(n)
+        f[zeros] = 0.0
+        f[ones] = 1.0
+        out = np.zeros((n, n), complex, order="F")
+        emul.lqm_emul_rho(n, U.ctypes.data_as(P), f.ctypes.data_as(P), out.ctypes.data_as(P))
+        assert np.max(np.abs(out - (U * f) @ U.conj().T)) < 1e-13 * max(n, 1)
+        off = ~np.eye(n, dtype=bool)
+        assert np.all(out[off] == out.conj().T[off])  # the lower triangle mirrors the upper exactly
