@@ -214,6 +214,15 @@ int lqm_density(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, d
  * agree for nw = 1, the ldos(H, ks, frequency) form). */
 int lqm_ldos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t nw, const double* omegas,
              double gamma, double* n_out);
+/* Fermi-surface density, fermisurfacedensity_fromdata(bands, energies[, obs]; broadening)
+ * of src/modules/Spectrum/fermisurface.jl on the bands of a k list:
+ * density[e + nE k] = sum_b (1/pi) w_bk g^2 / (g^2 + (eps_bk - E_e)^2), w = weights
+ * (n x nk, e.g. band expectation values) or 1 when NULL; g = broadening, or for
+ * broadening <= 0 the reference's :auto (mean over bands of the band's standard
+ * deviation over k, divided by sqrt(nk)); *broadening_used receives g. */
+int lqm_fermisurface(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int64_t nE,
+                     const double* energies, double broadening, const double* weights, double* density,
+                     double* broadening_used);
 
 /* Berry curvature plaquette phases, berry(H, NX, NY, bandindices)
  * (src/modules/Spectrum/berry.jl:48-82,107-155): eigenvectors of the nb bands

@@ -175,6 +175,24 @@ function cuda_ldos(H, ks::AbstractMatrix{Float64}, ωs::AbstractVector, exec::Cu
     out
 end
 
+"""`fermisurfacedensity_fromdata(bandmatrix(H, ks), energies[, obs]; broadening)`
+(Spectrum/fermisurface.jl) on the device (`lqm_fermisurface`): (density (nE x nk),
+broadening); `broadening=:auto` uses the reference's automatic width."""
+function cuda_fermisurfacedensity(H, ks::AbstractMatrix{Float64}, energies::AbstractVector, exec::CudaExec;
+                                  broadening=:auto, obs::Union{Nothing,AbstractMatrix}=nothing)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    out = zeros(Float64, length(energies), size(ks, 2))
+    g = Ref{Float64}(0.0)
+    check(ctx, ccall((:lqm_fermisurface, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Int64, Ptr{Float64}, Float64, Ptr{Float64}, Ptr{Float64},
+         Ref{Float64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), length(energies), Vector{Float64}(energies),
+        broadening isa Number ? Float64(broadening) : 0.0,
+        obs === nothing ? Ptr{Float64}(C_NULL) : Matrix{Float64}(obs), out, g))
+    out, g[]
+end
+
 """`berry(H, NX, NY, bandindices)` (Spectrum/berry.jl:140-155) on the device (`lqm_berry`):
 (midkgrid, F) with F the (NX-1) x (NY-1) plaquette phases; `bandindices` are 1-based as in
 the reference."""

@@ -43,7 +43,7 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface",
 ]
 
 
@@ -97,6 +97,7 @@ _SIG = {
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
     "lqm_berry_flux": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
     "lqm_berry_path": [_P, _P, _I64, _P, _P],
+    "lqm_fermisurface": [_P, _P, _I64, _P, _I64, _P, _D, _P, _P, ctypes.POINTER(_D)],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
     "lqm_ctx_set_scf_residual": [_P, ctypes.c_int],
@@ -613,6 +614,32 @@ def gapcherns(H, NX, NY=0, gaptol=1e-6, multimode="cuda", ctx=None):
         return []
     flux = berry_flux(Hd, NX, NY, [list(range(m)) for m, _, _ in gaps], ctx=ctx)
     return [(m, lo, hi, int(round(f))) for (m, lo, hi), f in zip(gaps, flux)]
+
+
+def fermisurfacedensity(H, energies, ks=None, broadening="auto", obs=None, num_points=15, multimode="cuda",
+                        ctx=None):
+    """``fermisurfacedensity(H, energies; broadening, num_points)`` (Spectrum/fermisurface.jl)
+    on the device (``lqm_fermisurface``): (ks, density (nE, nk), broadening).  ``ks``
+    defaults to ``regulargrid(nk=num_points^2)``; ``obs`` (n, nk) weights the bands as
+    fermisurfacedensity_fromdata(bands, energies, obs) does."""
+    _check_mode(multimode)
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    if ks is None:
+        n1 = int(num_points)
+        it = np.arange(n1) / n1
+        ks = np.vstack([np.tile(it, n1), np.repeat(it, n1)])
+    ks = _ks(ks, Hd.d)
+    E = np.ascontiguousarray(np.atleast_1d(energies), dtype=np.float64)
+    w = None if obs is None else np.asfortranarray(obs, dtype=np.float64)
+    g = 0.0 if (broadening is None or isinstance(broadening, str)) else float(broadening)
+    if not isinstance(broadening, str) and broadening is not None and not g > 0:
+        raise ValueError("broadening must be positive or 'auto'")
+    out = np.zeros((len(E), ks.shape[1]), order="F")
+    gu = _D()
+    ctx.check(_lib.lqm_fermisurface(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), len(E), _ptr(E), g, _ptr(w),
+                                    _ptr(out), ctypes.byref(gu)))
+    return ks, out, gu.value
 
 
 def chemicalpotential(H, ks, filling, T=0.0, kweights=None, multimode="cuda", ctx=None):

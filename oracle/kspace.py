@@ -86,6 +86,24 @@ def ldos(h, ks, omegas, gamma=0.1):
     return out / (ks.shape[1] * np.pi)
 
 
+def fermisurfacedensity_fromdata(bands, energies, obs=None, broadening="auto"):
+    """Spectrum/fermisurface.jl (fermisurfacedensity_fromdata, getbroadening): per energy
+    and k, sum_b (1/pi) w g^2 / (g^2 + (eps - E)^2); :auto g = mean_b std_k(eps_b) / sqrt(nk)
+    (std with n - 1)."""
+    bands = np.asarray(bands, float)
+    energies = np.atleast_1d(np.asarray(energies, float))
+    if not isinstance(broadening, (int, float)) or broadening == "auto":
+        broadening = float(np.mean([np.std(b, ddof=1) for b in bands])) / math.sqrt(bands.shape[1])
+    g2 = broadening ** 2
+    out = np.zeros((len(energies), bands.shape[1]))
+    for j in range(bands.shape[1]):
+        t = (1 / math.pi) * g2 / (g2 + (bands[:, j][:, None] - energies[None, :]) ** 2)
+        if obs is not None:
+            t = obs[:, j][:, None] * t
+        out[:, j] = np.sum(t, axis=0)
+    return out, broadening
+
+
 def berry(h, NX, NY, bands):
     """Spectrum/berry.jl:48-82 (statesgrid on range(0,1,N) x range(0,1,N) + 1.34e-8)
     and :107-137 (link L = det(A^H B)/|det|, plaquette phase real(log(...)/(2 pi i)));

@@ -367,3 +367,28 @@ def test_berry_along_path_matches_oracle(lqm, ctx):
     assert b.shape == ref.shape
     assert np.max(np.abs(b - ref)) <= 1e-9
     assert np.max(np.abs(b[0] + b[1])) <= 1e-9  # the two bands' curvatures cancel
+
+
+def test_fermisurface_density_matches_oracle(lqm, ctx):
+    """fermisurfacedensity (Spectrum/fermisurface.jl) through lqm_fermisurface against the
+    oracle: graphene on the default 15 x 15 grid with the :auto broadening, the disordered
+    honeycomb 6x6 cell (n = 144, blocked eigensolver) with a fixed broadening, and the
+    weighted form with the sublattice-0 projector's band expectation values."""
+    h = M.nearestneighbor(L.honeycomb(), -1.0)
+    ks, d, g = lqm.fermisurfacedensity(h, [0.0, 0.5, 1.0], ctx=ctx)
+    b, _ = K.bandmatrix(h, ks)
+    ref, gref = K.fermisurfacedensity_fromdata(b, [0.0, 0.5, 1.0])
+    assert abs(g - gref) <= 1e-14 and np.max(np.abs(d - ref)) <= 1e-9 * np.max(ref)
+    lat6, h6 = M.honeycomb_disorder(6)
+    rng = np.random.default_rng(3)
+    ks6 = rng.uniform(-0.5, 0.5, (2, 40))
+    E = np.linspace(-1.0, 1.0, 9)
+    _, d6, g6 = lqm.fermisurfacedensity(h6, E, ks=ks6, broadening=0.05, ctx=ctx)
+    b6, _ = K.bandmatrix(h6, ks6)
+    ref6, _ = K.fermisurfacedensity_fromdata(b6, E, broadening=0.05)
+    assert g6 == 0.05 and np.max(np.abs(d6 - ref6)) <= 1e-9 * np.max(ref6)
+    P = np.diag(np.repeat((lat6.extracoord("sublattice") == 0).astype(float), 2)).astype(complex)
+    bo, obs = lqm.bandmatrix_obs(h6, ks6, [P], ctx=ctx)
+    _, dw, _ = lqm.fermisurfacedensity(h6, E, ks=ks6, broadening=0.05, obs=obs[:, :, 0], ctx=ctx)
+    refw, _ = K.fermisurfacedensity_fromdata(b6, E, obs=obs[:, :, 0], broadening=0.05)
+    assert np.max(np.abs(dw - refw)) <= 1e-9 * np.max(np.abs(refw))

@@ -529,3 +529,20 @@ def test_haldane_chern_pins():
         gaps = K.gapcherns(h, 30, gaptol=1e-3)
         assert len(gaps) == 1 and gaps[0][0] == 1 and gaps[0][3] == sgn
         assert gaps[0][1] < 0 < gaps[0][2]
+
+
+def test_fermisurface_density_known_answers():
+    """Spectrum/fermisurface.jl on the oracle: a flat band at the requested energy gives
+    1/pi at every k for any broadening; the :auto broadening is the mean band standard
+    deviation over sqrt(nk); graphene's density on a 15 x 15 grid peaks near the Dirac
+    points at E = 0."""
+    ks = L.regulargrid(15 * 15)
+    flat = {(0, 0): np.array([[0.3]], complex)}
+    b, _ = K.bandmatrix(flat, ks)
+    d, g = K.fermisurfacedensity_fromdata(b, [0.3], broadening=0.05)
+    assert np.max(np.abs(d - 1 / math.pi)) < 1e-15 and g == 0.05
+    h = M.nearestneighbor(L.honeycomb(), -1.0)
+    b, _ = K.bandmatrix(h, ks)
+    d, g = K.fermisurfacedensity_fromdata(b, [0.0, 1.0])
+    assert abs(g - np.mean([np.std(x, ddof=1) for x in b]) / 15.0) < 1e-15
+    assert np.argmax(d[0]) in [int(np.argmin(np.abs(b[0]))), int(np.argmin(np.abs(b[1])))]
