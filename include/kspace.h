@@ -241,6 +241,16 @@ int lqm_berry(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t n
  * the four corners k +- (neighbour differences)/2 and their rotations by +-pi/2;
  * out[i + n j] = the plaquette phase of band i at point j (n x N). */
 int lqm_berry_path(lqm_ctx* ctx, const lqm_hops* H, int64_t N, const double* kpoints, double* out);
+/* Wilson loops over the statesgrid of bands `bands` (0-based, nb <= 8): the loops of
+ * WilsonSlice1D in Wilson2D (src/modules/Spectrum/berry.jl:258-268,312-367) on the
+ * periodic grid of the first NX-1 x NY-1 points; dir 1: one loop along k_y per k_x
+ * (NX - 1 loops), dir 2: along k_x per k_y (NY - 1 loops).  Per loop the product of the
+ * polar factors (U V^H of the SVD) of the link overlaps S_a^H S_b and its eigenphases
+ * angle/(2 pi) in ascending order: en[loop nb + m]; U (may be NULL) receives the
+ * eigenvectors (nb x nb per loop, complex, in the order of en; normalised, phase
+ * arbitrary). */
+int lqm_wilson(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, int dir,
+               double* en, double* U);
 int lqm_berry_flux(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nsets, const int64_t* set_ptr,
                    const int64_t* set_bands, double* flux);
 

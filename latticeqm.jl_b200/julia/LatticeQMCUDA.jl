@@ -222,6 +222,29 @@ function cuda_berryalongpath(H, kpoints::AbstractMatrix{Float64}, exec::CudaExec
     out
 end
 
+"""`WilsonSlice1D(statesgrid(H, NX, NY, bands)[1:NX-1, 1:NY-1, :, :], dir)` (Spectrum/berry.jl:312-367)
+on the device (`lqm_wilson`): (en (nloops x nb), U (nloops x nb x nb)); `bands` 1-based."""
+function cuda_wilson_slices(H, NX::Int, NY::Int, bands::AbstractVector{<:Integer}, dir::Int, exec::CudaExec)
+    NY = NY < 1 ? NX : NY
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    b = Int64[i - 1 for i in bands]
+    nl = dir == 1 ? NX - 1 : NY - 1
+    en = zeros(Float64, length(b), nl)
+    U = zeros(ComplexF64, length(b), length(b), nl)
+    check(ctx, ccall((:lqm_wilson, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int64, Int64, Ptr{Int64}, Cint, Ptr{Float64}, Ptr{ComplexF64}),
+        ctx.ptr, dh.ptr, NX, NY, length(b), b, dir, en, U))
+    permutedims(en), permutedims(U, (3, 1, 2))
+end
+
+"""`Wilson2D(H, NX, NY, bandindices)` (Spectrum/berry.jl:258-268) on the device."""
+function cuda_wilson2d(H, NX::Int, NY::Int, bands::AbstractVector{<:Integer}, exec::CudaExec)
+    en1, U1 = cuda_wilson_slices(H, NX, NY, bands, 1, exec)
+    en2, U2 = cuda_wilson_slices(H, NX, NY, bands, 2, exec)
+    en1, U1, en2, U2
+end
+
 """Summed plaquette phases of each band manifold (1-based band index vectors) on one
 NX x NY state grid (`lqm_berry_flux`)."""
 function cuda_berry_flux(H, NX::Int, NY::Int, sets::AbstractVector, exec::CudaExec)

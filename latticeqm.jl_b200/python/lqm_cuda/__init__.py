@@ -43,7 +43,7 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface", "lqm_wilson",
 ]
 
 
@@ -97,6 +97,7 @@ _SIG = {
     "lqm_berry": [_P, _P, _I64, _I64, _I64, _P, _P],
     "lqm_berry_flux": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
     "lqm_berry_path": [_P, _P, _I64, _P, _P],
+    "lqm_wilson": [_P, _P, _I64, _I64, _I64, _P, ctypes.c_int, _P, _P],
     "lqm_fermisurface": [_P, _P, _I64, _P, _I64, _P, _D, _P, _P, ctypes.POINTER(_D)],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
@@ -570,6 +571,33 @@ def berryalongpath(H, kpoints, multimode="cuda", ctx=None):
     out = np.zeros((Hd.n, kp.shape[1]), order="F")
     ctx.check(_lib.lqm_berry_path(ctx.handle, Hd.handle, kp.shape[1], _ptr(kp), _ptr(out)))
     return out
+
+
+def wilson_slices(H, NX, NY=0, bands=(0,), direction=1, want_vectors=False, ctx=None):
+    """The Wilson loops of WilsonSlice1D (Spectrum/berry.jl:312-367) on the statesgrid of
+    ``bands`` (0-based): (en (nloops, nb), U (nloops, nb, nb) or None); direction 1 loops
+    along k_y per k_x, direction 2 along k_x per k_y (``lqm_wilson``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    NY = NX if NY < 1 else NY
+    b = np.ascontiguousarray(bands, dtype=np.int64)
+    nloops = (NX - 1) if direction == 1 else (NY - 1)
+    en = np.zeros((nloops, len(b)))
+    U = np.zeros((nloops, len(b), len(b)), dtype=np.complex128) if want_vectors else None
+    Uc = np.zeros((len(b), len(b), nloops), dtype=np.complex128, order="F") if want_vectors else None
+    ctx.check(_lib.lqm_wilson(ctx.handle, Hd.handle, int(NX), int(NY), len(b), _ptr(b), int(direction), _ptr(en),
+                              _ptr(Uc)))
+    if want_vectors:
+        U = np.moveaxis(Uc, 2, 0)
+    return en, U
+
+
+def wilson2d(H, NX, NY=0, bands=(0,), ctx=None):
+    """``Wilson2D(H, NX, NY, bandindices)`` (Spectrum/berry.jl:258-268) with 0-based bands:
+    (en1, U1, en2, U2)."""
+    en1, U1 = wilson_slices(H, NX, NY, bands, 1, True, ctx)
+    en2, U2 = wilson_slices(H, NX, NY, bands, 2, True, ctx)
+    return en1, U1, en2, U2
 
 
 def getcherns(H, NX, NY=0, bands=None, multimode="cuda", ctx=None):

@@ -224,6 +224,49 @@ def gapcherns(h, NX, NY=0, gaptol=1e-6):
             spectralgaps(h, NX, NY, gaptol)]
 
 
+def statesgrid(h, NX, NY, bands):
+    """statesgrid(H, NX, NY, bandindices) (Spectrum/berry.jl:49-82): S[i, j] = the n x nb
+    eigenvector columns at k = (i/(NX-1), j/(NY-1)) + 1.34e-8."""
+    n = next(iter(h.values())).shape[0]
+    S = np.zeros((NX, NY, n, len(bands)), complex)
+    for i in range(NX):
+        for j in range(NY):
+            k = np.array([i / (NX - 1), j / (NY - 1)]) + 1.34e-8
+            _, U = eigh_upper(fouriersum(h, k), True)
+            S[i, j] = U[:, list(bands)]
+    return S
+
+
+def wilson1d(grid3):
+    """Wilson1D(statesgrid (NY, M1, M2)) (Spectrum/berry.jl:312-327, j0 = 0): F = prod over the
+    periodic links of U V^H from svd(S_j^H S_{j+1}); eigenphases angle/(2 pi) ascending."""
+    NY = grid3.shape[0]
+    m = grid3.shape[2]
+    F = np.eye(m, dtype=complex)
+    for j in range(NY):
+        A = grid3[j].conj().T @ grid3[(j + 1) % NY]
+        Us, _, Vh = np.linalg.svd(A)
+        F = F @ (Us @ Vh)
+    ev, U = np.linalg.eig(F)
+    en = np.angle(ev) / (2 * math.pi)
+    p = np.argsort(en, kind="stable")
+    return en[p], U[:, p]
+
+
+def wilson_slices(h, NX, NY, bands, direction=1):
+    """WilsonSlice1D of Wilson2D (Spectrum/berry.jl:258-268,340-367) on the periodic grid of the
+    first NX-1 x NY-1 points: direction 1 one loop along j per i, direction 2 along i per j."""
+    S = statesgrid(h, NX, NY, bands)[: NX - 1, : NY - 1]
+    if direction == 2:
+        S = np.transpose(S, (1, 0, 2, 3))
+    en, Us = [], []
+    for i in range(S.shape[0]):
+        e, U = wilson1d(S[i])
+        en.append(e)
+        Us.append(U)
+    return np.array(en), np.array(Us)
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

@@ -392,3 +392,24 @@ def test_fermisurface_density_matches_oracle(lqm, ctx):
     _, dw, _ = lqm.fermisurfacedensity(h6, E, ks=ks6, broadening=0.05, obs=obs[:, :, 0], ctx=ctx)
     refw, _ = K.fermisurfacedensity_fromdata(b6, E, obs=obs[:, :, 0], broadening=0.05)
     assert np.max(np.abs(dw - refw)) <= 1e-9 * np.max(np.abs(refw))
+
+
+def test_wilson_loops_match_oracle(lqm, ctx):
+    """Wilson loops (WilsonSlice1D / Wilson2D, Spectrum/berry.jl:258-367) through lqm_wilson
+    against the oracle: the lower Haldane band (one band; its phase winds by the Chern
+    number) in both directions, and the four lowest bands of the spin-orbit triangular model
+    (whole degenerate pairs), whose eigenvectors also diagonalise the loop the oracle builds."""
+    _, h = M.haldane_model(t2=0.1, phi=math.pi / 2)
+    for direction, wind in ((1, 1), (2, -1)):
+        en, _ = lqm.wilson_slices(h, 21, 21, [0], direction, ctx=ctx)
+        ref, _ = K.wilson_slices(h, 21, 21, [0], direction)
+        assert np.max(np.abs(en - ref)) <= 1e-9
+        d = (np.diff(np.append(en[:, 0], en[0, 0])) + 0.5) % 1.0 - 0.5
+        assert abs(d.sum() - wind) < 1e-9
+    h3 = M.batch_models()[2][1]
+    en1, U1, en2, U2 = lqm.wilson2d(h3, 9, 9, [0, 1, 2, 3], ctx=ctx)
+    for en, U, direction in ((en1, U1, 1), (en2, U2, 2)):
+        ref, _ = K.wilson_slices(h3, 9, 9, [0, 1, 2, 3], direction)
+        assert np.max(np.abs(en - ref)) <= 1e-9
+        for u in U:
+            assert np.max(np.abs(u.conj().T @ u - np.eye(4))) <= 1e-12

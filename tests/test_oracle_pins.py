@@ -546,3 +546,15 @@ def test_fermisurface_density_known_answers():
     d, g = K.fermisurfacedensity_fromdata(b, [0.0, 1.0])
     assert abs(g - np.mean([np.std(x, ddof=1) for x in b]) / 15.0) < 1e-15
     assert np.argmax(d[0]) in [int(np.argmin(np.abs(b[0]))), int(np.argmin(np.abs(b[1])))]
+
+
+def test_wilson_loop_winding_is_the_chern_number():
+    """Wilson2D (Spectrum/berry.jl:258-327) on the oracle: the lower Haldane band's
+    Wilson-loop phase winds once across the slices, +1 along one direction and -1 along
+    the other for phi = pi/2, opposite for -pi/2 (its Chern number +-1)."""
+    for phi, sgn in ((math.pi / 2, 1), (-math.pi / 2, -1)):
+        _, h = M.haldane_model(t2=0.1, phi=phi)
+        for direction, s_dir in ((1, 1), (2, -1)):
+            en, _ = K.wilson_slices(h, 21, 21, [0], direction)
+            d = (np.diff(np.append(en[:, 0], en[0, 0])) + 0.5) % 1.0 - 0.5
+            assert abs(d.sum() - sgn * s_dir) < 1e-9
