@@ -251,6 +251,13 @@ int lqm_berry_path(lqm_ctx* ctx, const lqm_hops* H, int64_t N, const double* kpo
  * arbitrary). */
 int lqm_wilson(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands, int dir,
                double* en, double* U);
+/* WilsonWannier2D(H, NX, NY, bandindices) (src/modules/Spectrum/berry.jl:274-301): the
+ * states of every point rotated by the eigenvectors of the Wilson loop through it (loops
+ * along k_y for p1, along k_x for p2, based at that point), then per band the mean over
+ * the other direction of the abelian Wilson loops of the rotated band: p1[nb], p2[nb].
+ * The same grid and band limit (nb <= 8) as lqm_wilson. */
+int lqm_wilson_wannier(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nb, const int64_t* bands,
+                       double* p1, double* p2);
 int lqm_berry_flux(lqm_ctx* ctx, const lqm_hops* H, int64_t NX, int64_t NY, int64_t nsets, const int64_t* set_ptr,
                    const int64_t* set_bands, double* flux);
 

@@ -238,6 +238,20 @@ function cuda_wilson_slices(H, NX::Int, NY::Int, bands::AbstractVector{<:Integer
     permutedims(en), permutedims(U, (3, 1, 2))
 end
 
+"""`WilsonWannier2D(H, NX, NY, bandindices)` (Spectrum/berry.jl:274-301) on the device
+(`lqm_wilson_wannier`): (p1, p2); `bands` 1-based."""
+function cuda_wilson_wannier2d(H, NX::Int, NY::Int, bands::AbstractVector{<:Integer}, exec::CudaExec)
+    NY = NY < 1 ? NX : NY
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    b = Int64[i - 1 for i in bands]
+    p1, p2 = zeros(Float64, length(b)), zeros(Float64, length(b))
+    check(ctx, ccall((:lqm_wilson_wannier, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Int64, Int64, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}),
+        ctx.ptr, dh.ptr, NX, NY, length(b), b, p1, p2))
+    p1, p2
+end
+
 """`Wilson2D(H, NX, NY, bandindices)` (Spectrum/berry.jl:258-268) on the device."""
 function cuda_wilson2d(H, NX::Int, NY::Int, bands::AbstractVector{<:Integer}, exec::CudaExec)
     en1, U1 = cuda_wilson_slices(H, NX, NY, bands, 1, exec)

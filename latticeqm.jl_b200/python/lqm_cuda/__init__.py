@@ -43,7 +43,7 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface", "lqm_wilson",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface", "lqm_wilson", "lqm_wilson_wannier",
 ]
 
 
@@ -98,6 +98,7 @@ _SIG = {
     "lqm_berry_flux": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
     "lqm_berry_path": [_P, _P, _I64, _P, _P],
     "lqm_wilson": [_P, _P, _I64, _I64, _I64, _P, ctypes.c_int, _P, _P],
+    "lqm_wilson_wannier": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
     "lqm_fermisurface": [_P, _P, _I64, _P, _I64, _P, _D, _P, _P, ctypes.POINTER(_D)],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
@@ -598,6 +599,18 @@ def wilson2d(H, NX, NY=0, bands=(0,), ctx=None):
     en1, U1 = wilson_slices(H, NX, NY, bands, 1, True, ctx)
     en2, U2 = wilson_slices(H, NX, NY, bands, 2, True, ctx)
     return en1, U1, en2, U2
+
+
+def wilson_wannier2d(H, NX, NY=0, bands=(0,), ctx=None):
+    """``WilsonWannier2D(H, NX, NY, bandindices)`` (Spectrum/berry.jl:274-301) with 0-based
+    bands: (p1, p2), the mean nested-Wilson-loop phases per band (``lqm_wilson_wannier``)."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    NY = NX if NY < 1 else NY
+    b = np.ascontiguousarray(bands, dtype=np.int64)
+    p1, p2 = np.zeros(len(b)), np.zeros(len(b))
+    ctx.check(_lib.lqm_wilson_wannier(ctx.handle, Hd.handle, int(NX), int(NY), len(b), _ptr(b), _ptr(p1), _ptr(p2)))
+    return p1, p2
 
 
 def getcherns(H, NX, NY=0, bands=None, multimode="cuda", ctx=None):

@@ -267,6 +267,41 @@ def wilson_slices(h, NX, NY, bands, direction=1):
     return np.array(en), np.array(Us)
 
 
+def wilson1d_base(grid3, j0):
+    """Wilson1D(statesgrid, j0) (Spectrum/berry.jl:312-327) with the loop started at point j0."""
+    NY = grid3.shape[0]
+    return wilson1d(np.roll(grid3, -j0, axis=0))
+
+
+def _abelian_loop(grid2):
+    # Wilson1D(statesgrid (NY, M1)) (Spectrum/berry.jl:329-338)
+    F = 1.0 + 0j
+    for j in range(grid2.shape[0]):
+        F *= np.vdot(grid2[j], grid2[(j + 1) % grid2.shape[0]])
+    return np.angle(F) / (2 * math.pi)
+
+
+def wilson_wannier2d(h, NX, NY, bands):
+    """WilsonWannier2D(H, NX, NY, bandindices) (Spectrum/berry.jl:274-301): the states rotated
+    by the eigenvectors of the loops through each point (Wilson1D with that base point),
+    then per band the mean over the other direction's abelian Wilson loops: (p1, p2)."""
+    S = statesgrid(h, NX, NY, bands)[: NX - 1, : NY - 1]
+    nx, ny, _, m = S.shape
+    new1 = np.empty_like(S)
+    for i in range(nx):
+        for j in range(ny):
+            _, U = wilson1d_base(S[i, :, :, :], j)
+            new1[i, j] = S[i, j] @ U
+    new2 = np.empty_like(S)
+    for i in range(nx):
+        for j in range(ny):
+            _, U = wilson1d_base(S[:, j, :, :], i)
+            new2[i, j] = S[i, j] @ U
+    p1 = [float(np.mean([_abelian_loop(new1[:, j, :, q]) for j in range(ny)])) for q in range(m)]
+    p2 = [float(np.mean([_abelian_loop(new2[i, :, :, q]) for i in range(nx)])) for q in range(m)]
+    return p1, p2
+
+
 def fermidirac(e, mu=0.0, T=0.0):
     """Utils/fermidirac.jl:1-5: 1/(exp((e-mu)/T)+1) for T>0, else Heaviside(mu-e)
     with value 0.5 at equality."""

@@ -413,3 +413,16 @@ def test_wilson_loops_match_oracle(lqm, ctx):
         assert np.max(np.abs(en - ref)) <= 1e-9
         for u in U:
             assert np.max(np.abs(u.conj().T @ u - np.eye(4))) <= 1e-12
+
+
+def test_wilson_wannier_matches_oracle(lqm, ctx):
+    """WilsonWannier2D (Spectrum/berry.jl:274-301) through lqm_wilson_wannier against the
+    oracle: the Haldane model's lower band and both bands (non-degenerate loop spectra),
+    and gapped graphene's lower band, on a 13 x 13 grid."""
+    _, h = M.haldane_model(t2=0.1, phi=math.pi / 2)
+    h0 = M.nearestneighbor(L.honeycomb(), -1.0)
+    h0[(0, 0)] = h0[(0, 0)] + np.diag([0.3, -0.3])
+    for hh, bands in ((h, [0]), (h, [0, 1]), (h0, [0])):
+        p1, p2 = lqm.wilson_wannier2d(hh, 13, 13, bands, ctx=ctx)
+        r1, r2 = K.wilson_wannier2d(hh, 13, 13, bands)
+        assert np.max(np.abs(p1 - np.array(r1))) <= 1e-9 and np.max(np.abs(p2 - np.array(r2))) <= 1e-9
