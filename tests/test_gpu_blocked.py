@@ -417,12 +417,14 @@ def test_wilson_loops_match_oracle(lqm, ctx):
 
 def test_wilson_wannier_matches_oracle(lqm, ctx):
     """WilsonWannier2D (Spectrum/berry.jl:274-301) through lqm_wilson_wannier against the
-    oracle: the Haldane model's lower band and both bands (non-degenerate loop spectra),
-    and gapped graphene's lower band, on a 13 x 13 grid."""
+    oracle: the lower band of the Haldane model and of gapped graphene on a 13 x 13 grid.
+    (The rotation is gauge invariant only for non-degenerate loop spectra: a band set
+    spanning every band, for one, has the identity as its loop and no preferred
+    eigenvectors.)"""
     _, h = M.haldane_model(t2=0.1, phi=math.pi / 2)
     h0 = M.nearestneighbor(L.honeycomb(), -1.0)
     h0[(0, 0)] = h0[(0, 0)] + np.diag([0.3, -0.3])
-    for hh, bands in ((h, [0]), (h, [0, 1]), (h0, [0])):
+    for hh, bands in ((h, [0]), (h0, [0])):
         p1, p2 = lqm.wilson_wannier2d(hh, 13, 13, bands, ctx=ctx)
         r1, r2 = K.wilson_wannier2d(hh, 13, 13, bands)
         assert np.max(np.abs(p1 - np.array(r1))) <= 1e-9 and np.max(np.abs(p2 - np.array(r2))) <= 1e-9
