@@ -883,7 +883,8 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 }
 
 // ---------------------------------------------------------------------------
-// 4. Back-transformation U = H_0 ... H_{n-2} U (U holds Q on entry), applied
+// 4. Back-transformation U = H_0 ... H_{n-2} U (U holds Q on entry; with a column
+// range [cbeg, cend) only those columns are read and transformed), applied
 // in blocks of 8 reflectors with the compact WY form (LAPACK zlarft, forward,
 // column-wise):  H_{j0} ... H_{j0+7} = I - V T V^H,  U_sub -= V (T (V^H U_sub)).
 // Reflector j is R[j+1.., j] with v0 = 1.  V (zero-padded, ld n), T and the
@@ -893,7 +894,11 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 // group's rows, with 8 independent accumulators per lane.
 // ---------------------------------------------------------------------------
 LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int ldr, EighVec& S, double2* U,
-                                   int ldu) {
+                                   int ldu, int cbeg = 0, int cend = -1) {
+  // only the columns [cbeg, cend) of U are transformed (and read)
+  if (cend < 0) cend = n;
+  const int ncol = cend - cbeg;
+  if (ncol <= 0) return;
   constexpr int NB = 8;
   double2* Vs = S.pbuf;                  // m x NB, leading dimension n
   double2* Ts = S.pbuf + (int64_t)NB * n;  // NB x NB
@@ -941,15 +946,15 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
       for (int i = 0; i < NB; ++i) Ts[l + i * NB] = trow[i];
     }
     team_sync();
-    // lanes per column: the largest power of two <= 8 with n * G <= nt (within a warp)
+    // lanes per column: the largest power of two <= 8 with ncol * G <= nt (within a warp)
     int G = 1;
-    while (G < 8 && 2 * G <= T.nl && n * (2 * G) <= T.nt) G *= 2;
-    const int ngr = T.nt / G;                 // column groups
+    while (G < 8 && 2 * G <= T.nl && ncol * (2 * G) <= T.nt) G *= 2;
+    const int ngr = T.nt / G;                    // column groups
     const int g = T.tid % G;
-    const int rounds = (n + ngr - 1) / ngr;   // uniform trip count (every lane takes part in the sums)
+    const int rounds = (ncol + ngr - 1) / ngr;   // uniform trip count (every lane takes part in the sums)
     for (int rd = 0; rd < rounds; ++rd) {
-      const int c = rd * ngr + T.tid / G;
-      const bool act = c < n;
+      const int c = cbeg + rd * ngr + T.tid / G;
+      const bool act = c < cend;
       double2* Uc = U + (j0 + 1) + (int64_t)(act ? c : 0) * ldu;
       double2 w[NB];
 #pragma unroll

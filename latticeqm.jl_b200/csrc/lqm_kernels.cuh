@@ -138,30 +138,11 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
     for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
     LQM_TICK(PH_DC);
     if (need_vec) {
-      double2* U;
-      int ldu;
-      if (in_smem) {
-        for (int c = T.wid; c < n; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) Qs[r + (int64_t)c * n] = Q[r + (int64_t)c * n];
-        team_sync();
-        U = (double2*)(smem + L.offA);
-        ldu = n + 1;
-        for (int c = T.wid; c < n; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Qs[r + (int64_t)c * n], 0.0);
-      } else {
-        U = a.U ? a.U + k * nn : (double2*)(slot + 4 * nn);
-        ldu = n;
-        for (int c = T.wid; c < n; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Q[r + (int64_t)c * n], 0.0);
-      }
-      team_sync();
-      backtransform(T, n, R, ldr, S, U, ldu);
-      LQM_TICK(PH_BACK);
-      if (in_smem && a.U) {
-        double2* Uo = a.U + k * nn;
-        for (int c = T.wid; c < n; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) Uo[r + (int64_t)c * n] = U[r + (int64_t)c * ldu];
-      }
+      // Columns of U to form: all of them when U is an output; for rho_k alone only
+      // the eigenvectors rho_from_U reads (its complement form skips the states with
+      // f = 1, the direct form those with f = 0), a contiguous range since f falls
+      // with the ascending eigenvalues.
+      int cbeg = 0, cend = n;
       if (a.rhok) {
         double eb = 0.0;
         for (int j = T.tid; j < n; j += T.nt) {
@@ -169,10 +150,50 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
           S.vals[j] = fj;
           eb += S.D[j] * fj;
         }
-        eb = team_sum(T, eb, S.red);
+        eb = team_sum(T, eb, S.red);  // (its barriers publish S.vals)
         if (T.tid == 0) a.eband_k[k] = a.w[k] * eb;
-        rho_from_U(T, n, U, ldu, S.vals, a.rhok + k * nn, n);
+        if (!a.U) {
+          int n0 = 0, n1 = 0;
+          for (int j = 0; j < n; ++j) {
+            n0 += (S.vals[j] == 0.0);
+            n1 += (S.vals[j] == 1.0);
+          }
+          const double skip = (n1 > n0) ? 1.0 : 0.0;
+          cbeg = n;
+          cend = 0;
+          for (int j = 0; j < n; ++j)
+            if (S.vals[j] != skip) {
+              cbeg = cbeg < j ? cbeg : j;
+              cend = j + 1;
+            }
+          if (cend < cbeg) cend = cbeg;
+        }
       }
+      double2* U;
+      int ldu;
+      if (in_smem) {
+        for (int c = cbeg + T.wid; c < cend; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) Qs[r + (int64_t)c * n] = Q[r + (int64_t)c * n];
+        team_sync();
+        U = (double2*)(smem + L.offA);
+        ldu = n + 1;
+        for (int c = cbeg + T.wid; c < cend; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Qs[r + (int64_t)c * n], 0.0);
+      } else {
+        U = a.U ? a.U + k * nn : (double2*)(slot + 4 * nn);
+        ldu = n;
+        for (int c = cbeg + T.wid; c < cend; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Q[r + (int64_t)c * n], 0.0);
+      }
+      team_sync();
+      backtransform(T, n, R, ldr, S, U, ldu, cbeg, cend);
+      LQM_TICK(PH_BACK);
+      if (in_smem && a.U) {
+        double2* Uo = a.U + k * nn;
+        for (int c = T.wid; c < n; c += T.nw)
+          for (int r = T.lane; r < n; r += T.nl) Uo[r + (int64_t)c * n] = U[r + (int64_t)c * ldu];
+      }
+      if (a.rhok) rho_from_U(T, n, U, ldu, S.vals, a.rhok + k * nn, n);
     }
     team_sync();
     LQM_TICK(PH_OUT);

@@ -134,3 +134,20 @@ def test_emulated_rho_from_U(emul, n):
         assert np.max(np.abs(out - (U * f) @ U.conj().T)) < 1e-13 * max(n, 1)
         off = ~np.eye(n, dtype=bool)
         assert np.all(out[off] == out.conj().T[off])  # the lower triangle mirrors the upper exactly
+
+
+@pytest.mark.parametrize("name,h", models()[1:4], ids=lambda x: x if isinstance(x, str) else "")
+def test_emulated_backtransform_column_range(emul, name, h):
+    """The rho-only path transforms only a contiguous range of eigenvector columns: those
+    columns come out bit-identical to the full back-transformation's."""
+    keys, blocks = pack(h)
+    n, nR = blocks.shape[0], blocks.shape[2]
+    kp = np.array((0.123, 0.77), float)
+    ev, Ufull = run(emul, h, (0.123, 0.77))
+    for cb, ce in ((0, n // 2), (n // 3, n), (1, n - 1)):
+        ev2 = np.zeros(n)
+        U = np.zeros((n, n), complex, order="F")
+        emul.lqm_emul_eigh_cols(n, nR, 2, blocks.ctypes.data_as(P), keys.ctypes.data_as(P), kp.ctypes.data_as(P),
+                                cb, ce, ev2.ctypes.data_as(P), U.ctypes.data_as(P))
+        assert np.array_equal(ev2, ev)
+        assert np.array_equal(U[:, cb:ce], Ufull[:, cb:ce])
