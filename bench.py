@@ -483,6 +483,16 @@ def main():
         state.append(dict(name=name, h=h, Hd=Hd, n=n, nR=len(h), Lk=Lk, rho=d_rho, bands=d_bands, dos=d_dos,
                           om=d_om))
 
+    # block size of the one-CTA eigensolver per model, chosen by the library's
+    # autotuner on 4096 of the grid's k-points (outside the timed region)
+    block_sizes = {}
+    ks_tune = np.asfortranarray(ks_np[:, :: max(1, nk // 4096)][:, :4096])
+    for s in state:
+        if s["n"] < 128:
+            best, _, table = Q.autotune_eigh(s["Hd"], ks_tune, want_rho=True, ctx=ctx)
+            block_sizes[f"n{s['n']}"] = {"chosen": best, "ms_by_block_size": {str(k): round(v, 3) for k, v in
+                                                                              table.items()}}
+
     eb = ctypes.c_double()
 
     def step(per_model_ms=None):
@@ -642,7 +652,8 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded models)",
                 "config": {"workload": WORKLOAD, "k_points_per_gpu_per_step": len(state) * nk,
                            "parallelism": f"dp{world} (k-grid shards; rho_R/DOS all-reduce)",
-                           "l2": "inputs larger than L2 (each step streams ~8 GB of U/rho_k through HBM)"},
+                           "l2": "inputs larger than L2 (each step streams ~8 GB of U/rho_k through HBM)",
+                           "eigh_block_size": block_sizes},
                 "e2e": {"value": e2e_val, "unit": "k-pts/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "scf": scf,
                 "configs": configs}

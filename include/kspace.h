@@ -78,6 +78,20 @@ int lqm_ctx_set_scf_terms(lqm_ctx* ctx, int hartree, int fock);
 int lqm_ctx_set_scf_exchange(lqm_ctx* ctx, int64_t ns, int64_t nJ, int32_t d, const int64_t* jkeys,
                              const double* jblocks, int64_t n, const int64_t* siteof, const int64_t* flavorof);
 int lqm_ctx_scf_exchange_energy(const lqm_ctx* ctx, double* eJ);
+/* Block size (threads, a multiple of 32 up to 512; 0 restores the built-in rule)
+ * of the one-CTA eigensolver for order n on this context.  No reference
+ * counterpart (a device launch parameter). */
+int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt);
+/* Autotuner of that block size for H's order (below the blocked path): every
+ * candidate (multiples of 32 around the built-in rule whose shared-memory plan
+ * fits) runs the eigen pass on the nk sample k-points (rho_k at mu = 0, T = 0.01
+ * when want_rho, else eigenvectors), warmed up once and timed once with CUDA
+ * events; the fastest becomes the context's block size for n.  best_nt/best_ms
+ * receive the choice, cand_nt/cand_ms (up to ncand_max, may be NULL) every
+ * candidate, *ncand their number.  Block sizes differ in rounding, so a choice is
+ * meant to be made once and reused.  No reference counterpart. */
+int lqm_autotune_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int want_rho, int* best_nt,
+                      double* best_ms, int64_t ncand_max, int* cand_nt, double* cand_ms, int64_t* ncand);
 /* Milliseconds of device time of the last call's kernels (CUDA events). */
 int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
 

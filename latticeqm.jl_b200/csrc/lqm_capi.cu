@@ -53,6 +53,7 @@ struct lqm_ctx {
   int num_sms = 0;
   double last_ms = 0.0;
   std::map<int, PlanDev> plans;
+  std::map<int, int> eigh_nt;  // one-CTA eigensolver block size per order n (autotuned or set), else the rule
   DevBuf ws[40];
   // per-kernel device-time statistics (CUDA events on the context stream)
   bool stats_on = false;
@@ -209,6 +210,12 @@ void check_hops(const lqm_hops* H) {
 #define LQM_EIGH_NT_LARGE 384
 #endif
 int eigh_threads(int n) { return n <= 16 ? 32 : (n <= 32 ? 64 : (n < 64 ? 128 : LQM_EIGH_NT_LARGE)); }
+// The block size of the one-CTA eigensolver for order n on this context: the value
+// set by lqm_ctx_set_eigh_threads / lqm_autotune_eigh, else the rule above.
+int eigh_threads_for(const lqm_ctx* ctx, int n) {
+  const auto it = ctx->eigh_nt.find(n);
+  return it != ctx->eigh_nt.end() ? it->second : eigh_threads(n);
+}
 
 // eigh_kernel instantiation for a block size (512 threads from n = 64 on).
 using EighFn = void (*)(EighArgs);
@@ -402,7 +409,7 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
     return;
   }
   const DCPlan& plan = get_plan(ctx, n);
-  const int nt = eigh_threads(n);
+  const int nt = eigh_threads_for(ctx, n);
   EighSmemLayout Ls = eigh_smem_layout(n, (int)H->nR, nt, 1);
   const int a_in_smem = Ls.total <= 225 * 1024;
   if (!a_in_smem) Ls = eigh_smem_layout(n, (int)H->nR, nt, 0);
@@ -446,7 +453,7 @@ constexpr int kBlockedDefaultMinN = 128;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
   const int64_t nmin = ctx->blocked_min_n > 0 ? ctx->blocked_min_n : kBlockedDefaultMinN;
   if (n >= nmin) return true;
-  return eigh_smem_layout(n, nR, eigh_threads(n), 0).total > 225 * 1024;
+  return eigh_smem_layout(n, nR, eigh_threads_for(ctx, n), 0).total > 225 * 1024;
 }
 
 int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
@@ -725,6 +732,13 @@ int lqm_ctx_set_scf_exchange(lqm_ctx* ctx, int64_t ns, int64_t nJ, int32_t d, co
 int lqm_ctx_scf_exchange_energy(const lqm_ctx* ctx, double* eJ) {
   if (!ctx || !eJ) return LQM_EINVAL;
   *eJ = ctx->scf_eJ;
+  return LQM_OK;
+}
+
+int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt) {
+  if (!ctx || n < 1 || nt < 0 || nt > 512 || nt % 32 != 0) return LQM_EINVAL;
+  if (nt == 0) ctx->eigh_nt.erase((int)n);
+  else ctx->eigh_nt[(int)n] = nt;
   return LQM_OK;
 }
 
@@ -1073,6 +1087,7 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 #include "lqm_partial.inc"
 #include "lqm_bdg.inc"
 #include "lqm_scf_bdg.inc"
+#include "lqm_autotune.inc"
 
 // ============================================================================
 // Allocation-free eigen pass.

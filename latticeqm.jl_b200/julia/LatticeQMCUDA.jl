@@ -252,6 +252,26 @@ function cuda_wilson_wannier2d(H, NX::Int, NY::Int, bands::AbstractVector{<:Inte
     p1, p2
 end
 
+"""Autotune the one-CTA eigensolver's block size for H's order on sample k-points
+(`lqm_autotune_eigh`); the choice stays on the device's context.  Returns
+(best block size, its ms, Dict(block size => ms))."""
+function cuda_autotune_eigh(H, ks::AbstractMatrix{Float64}, exec::CudaExec; want_rho::Bool=true)
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
+    best, bms, nc = Ref{Cint}(0), Ref{Float64}(0.0), Ref{Int64}(0)
+    cnt, cms = zeros(Cint, 16), zeros(Float64, 16)
+    check(ctx, ccall((:lqm_autotune_eigh, LIB[]), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Float64}, Cint, Ref{Cint}, Ref{Float64}, Int64, Ptr{Cint},
+         Ptr{Float64}, Ref{Int64}),
+        ctx.ptr, dh.ptr, size(ks, 2), Matrix{Float64}(ks), want_rho, best, bms, 16, cnt, cms, nc))
+    Int(best[]), bms[], Dict(Int(cnt[i]) => cms[i] for i in 1:nc[])
+end
+
+"""Set the one-CTA eigensolver's block size for order n (0: the built-in rule)."""
+cuda_set_eigh_threads(n::Int, nt::Int, exec::CudaExec) =
+    check(context(exec.device), ccall((:lqm_ctx_set_eigh_threads, LIB[]), Cint, (Ptr{Cvoid}, Int64, Cint),
+                                      context(exec.device).ptr, n, nt))
+
 """`Wilson2D(H, NX, NY, bandindices)` (Spectrum/berry.jl:258-268) on the device."""
 function cuda_wilson2d(H, NX::Int, NY::Int, bands::AbstractVector{<:Integer}, exec::CudaExec)
     en1, U1 = cuda_wilson_slices(H, NX, NY, bands, 1, exec)

@@ -43,7 +43,8 @@ EXPORTS = [
     "lqm_berry", "lqm_opticalconductivity", "lqm_bandmatrix_partial", "lqm_densitymatrix_partial",
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
-    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface", "lqm_wilson", "lqm_wilson_wannier",
+    "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface",
+    "lqm_wilson", "lqm_wilson_wannier", "lqm_ctx_set_eigh_threads", "lqm_autotune_eigh",
 ]
 
 
@@ -99,6 +100,9 @@ _SIG = {
     "lqm_berry_path": [_P, _P, _I64, _P, _P],
     "lqm_wilson": [_P, _P, _I64, _I64, _I64, _P, ctypes.c_int, _P, _P],
     "lqm_wilson_wannier": [_P, _P, _I64, _I64, _I64, _P, _P, _P],
+    "lqm_ctx_set_eigh_threads": [_P, _I64, ctypes.c_int],
+    "lqm_autotune_eigh": [_P, _P, _I64, _P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), _I64,
+                          _P, _P, ctypes.POINTER(_I64)],
     "lqm_fermisurface": [_P, _P, _I64, _P, _I64, _P, _D, _P, _P, ctypes.POINTER(_D)],
     "lqm_opticalconductivity": [_P, _P, _P, _P, _I64, _P, _I64, _P, _D, _D, _D, _P],
     "lqm_commutator_norm": [_P, _P, _P, _I64, _P, _P, ctypes.POINTER(_D)],
@@ -164,6 +168,10 @@ class Context:
         """Orders n >= n_min use the batched blocked eigensolver (0: only where the
         one-CTA-per-k kernel does not fit)."""
         self.check(_lib.lqm_ctx_set_blocked_min_n(self._h, int(n_min)))
+
+    def set_eigh_threads(self, n, nt):
+        """Block size of the one-CTA eigensolver for order n (0: the built-in rule)."""
+        self.check(_lib.lqm_ctx_set_eigh_threads(self._h, int(n), int(nt)))
 
     def last_kernel_ms(self):
         v = _D()
@@ -611,6 +619,22 @@ def wilson_wannier2d(H, NX, NY=0, bands=(0,), ctx=None):
     p1, p2 = np.zeros(len(b)), np.zeros(len(b))
     ctx.check(_lib.lqm_wilson_wannier(ctx.handle, Hd.handle, int(NX), int(NY), len(b), _ptr(b), _ptr(p1), _ptr(p2)))
     return p1, p2
+
+
+def autotune_eigh(H, ks, want_rho=True, ctx=None):
+    """Times every candidate block size of the one-CTA eigensolver for H's order on the
+    sample k-points ``ks`` (the rho_k pass when ``want_rho``, else eigenvectors) and keeps
+    the fastest on the context (``lqm_autotune_eigh``): (best_nt, best_ms, {nt: ms})."""
+    ctx = ctx or default_context()
+    Hd = _as_device_hops(H, ctx)
+    ks = _ks(ks, Hd.d)
+    best, bms, nc = ctypes.c_int(), _D(), _I64()
+    cnt = np.zeros(16, dtype=np.int32)
+    cms = np.zeros(16)
+    ctx.check(_lib.lqm_autotune_eigh(ctx.handle, Hd.handle, ks.shape[1], _ptr(ks), int(bool(want_rho)),
+                                     ctypes.byref(best), ctypes.byref(bms), 16, _ptr(cnt), _ptr(cms),
+                                     ctypes.byref(nc)))
+    return best.value, bms.value, {int(cnt[i]): float(cms[i]) for i in range(nc.value)}
 
 
 def getcherns(H, NX, NY=0, bands=None, multimode="cuda", ctx=None):

@@ -481,3 +481,39 @@ def test_bdg_scf_anderson_and_commutator_match_oracle(lqm, ctx):
         assert abs(res.energy - E_ref) <= tolr
         assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in rho) <= tolr
         assert abs(res.residual - resid) <= tolr * max(1.0, resid)
+
+
+def test_eigh_block_sizes_and_autotuner(lqm):
+    """Every block size the autotuner may choose for the batched models (n = 8, 24, 96)
+    gives the oracle's bands, eigenvectors and rho_L; the autotuner then keeps one of
+    them, and a repeated call with that block size is bit-identical."""
+    c = lqm.Context(0, timeout=600)
+    try:
+        rng = np.random.default_rng(21)
+        ks = rng.uniform(-0.5, 0.5, (2, 24))
+        w = np.full(24, 1 / 24)
+        for name, h in M.batch_models():
+            n = h[(0, 0)].shape[0]
+            base = 32 if n <= 16 else (64 if n <= 32 else (128 if n < 64 else 384))
+            cands = [nt for nt in (32, 64, 128, 256, 384, 512) if max(32, base // 2) <= nt <= max(4 * base, 512)]
+            bref, _ = K.bandmatrix(h, ks)
+            rref, _ = K.densitymatrix(h, ks, w, 0.0, 0.01, list(h.keys()))
+            for nt in cands:
+                c.set_eigh_threads(n, nt)
+                b, U = lqm.bandmatrix(h, ks, want_vectors=True, ctx=c)
+                assert rel_band_err(b, bref) <= BAND_TOL, (name, nt)
+                for j in range(ks.shape[1]):
+                    Hk = K.fouriersum(h, ks[:, j])
+                    assert np.max(np.abs(Hk @ U[:, :, j] - U[:, :, j] * b[:, j])) <= 1e-10 * max(1.0, np.ptp(bref))
+                rho = {R: None for R in h}
+                lqm.getdensitymatrix(rho, h, ks, mu=0.0, T=0.01, ctx=c)
+                assert max(np.max(np.abs(rho[R] - rref[R])) for R in h) <= RHO_TOL, (name, nt)
+            best, ms, table = lqm.autotune_eigh(h, rng.uniform(-0.5, 0.5, (2, 4096)), ctx=c)
+            assert best in cands and set(table) == set(cands) and ms == min(table.values())
+            rho1, rho2 = {R: None for R in h}, {R: None for R in h}
+            lqm.getdensitymatrix(rho1, h, ks, mu=0.0, T=0.01, ctx=c)
+            lqm.getdensitymatrix(rho2, h, ks, mu=0.0, T=0.01, ctx=c)
+            assert all(np.array_equal(rho1[R], rho2[R]) for R in h)
+            c.set_eigh_threads(n, 0)
+    finally:
+        c.close()
