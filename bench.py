@@ -484,9 +484,10 @@ def main():
                           om=d_om))
 
     # block size of the one-CTA eigensolver per model, chosen by the library's
-    # autotuner on 4096 of the grid's k-points (outside the timed region)
+    # autotuner on the step's own k-grid (outside the timed region; a sample that
+    # fits in one wave of CTAs would time latency, not throughput)
     block_sizes = {}
-    ks_tune = np.asfortranarray(ks_np[:, :: max(1, nk // 4096)][:, :4096])
+    ks_tune = np.asfortranarray(ks_np)
     for s in state:
         if s["n"] < 128:
             best, _, table = Q.autotune_eigh(s["Hd"], ks_tune, want_rho=True, ctx=ctx)

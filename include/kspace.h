@@ -86,7 +86,9 @@ int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt);
  * candidate (multiples of 32 around the built-in rule whose shared-memory plan
  * fits) runs the eigen pass on the nk sample k-points (rho_k at mu = 0, T = 0.01
  * when want_rho, else eigenvectors), warmed up once and timed once with CUDA
- * events; the fastest becomes the context's block size for n.  best_nt/best_ms
+ * events; the fastest becomes the context's block size for n (the sample should
+ * span several waves of CTAs, e.g. the production k-grid, or it times latency
+ * rather than throughput).  best_nt/best_ms
  * receive the choice, cand_nt/cand_ms (up to ncand_max, may be NULL) every
  * candidate, *ncand their number.  Block sizes differ in rounding, so a choice is
  * meant to be made once and reused.  No reference counterpart. */
