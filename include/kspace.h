@@ -97,15 +97,18 @@ int lqm_autotune_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 /* Milliseconds of device time of the last call's kernels (CUDA events). */
 int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
 
-/* Device-time statistics since the last reset (reset also switches event
- * timing of the eigensolver kernel on or off): eigh_ms / eigh_launches cover
+/* Device-time statistics since the last reset: eigh_ms / eigh_launches cover
  * the per-k eigensolver kernel, launches counts every kernel this library
- * launched. */
+ * launched.  The reset also sets what is recorded: enable_timing 0 = nothing,
+ * 1 = CUDA-event timing of the eigensolver launches, 2 = that plus the
+ * per-phase SM cycle counters of lqm_ctx_phase_cycles (clock reads inside the
+ * kernel, so a profiling mode, not a timing one). */
 int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing);
 int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches);
 /* SM cycles spent by the eigensolver kernel per stage, summed over CTAs while
- * timing is enabled: [0] Bloch sum, [1] Householder, [2] divide and conquer,
- * [3] bands + back-transformation, [4] end-of-k barrier, [5..12] the divide
+ * the phase counters are enabled (lqm_ctx_reset_stats(ctx, 2)): [0] Bloch
+ * sum, [1] Householder, [2] divide and conquer, [3] bands +
+ * back-transformation, [4] end-of-k barrier, [5..12] the divide
  * and conquer merge steps (z/sort, deflation, secular roots, Gu-Eisenstat z,
  * vectors/rotations/values, ranks, update, copy back), [13..15] the
  * Householder steps (trailing pass, mat-vec reduction, next column and

@@ -57,6 +57,7 @@ struct lqm_ctx {
   DevBuf ws[40];
   // per-kernel device-time statistics (CUDA events on the context stream)
   bool stats_on = false;
+  bool phases_on = false;  // per-phase cycle counters inside the eigensolver (clock reads)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending, ev_pool;
   double eigh_ms = 0.0;
   int64_t eigh_launches = 0, launches = 0;
@@ -74,14 +75,22 @@ struct lqm_ctx {
   std::vector<double> ex_blocks;  // ns x ns x nJ complex (interleaved)
   std::vector<int> ex_sf2idx;     // ns x nf, column-major: (site a, flavor f) -> orbital
   double scf_eJ = 0.0;            // exchange energy of the last SCF
+  // device buffers of freed Hops kept for the next uploads (base pointer, bytes):
+  // a caller that uploads H, runs one pass and frees it every call then makes no
+  // cudaMalloc/cudaFree, whose device-wide synchronisation and driver work cost
+  // from milliseconds to most of a second per call on B200
+  std::vector<std::pair<void*, size_t>> hops_cache;
+  size_t hops_cache_bytes = 0;
 };
 
 struct lqm_hops {
   int64_t n = 0, nR = 0;
   int32_t d = 0;
-  double2* blocks = nullptr;
+  double2* blocks = nullptr;  // base of one device buffer: the blocks, then (256-byte aligned) the keys
   int64_t* keys = nullptr;
   std::vector<int64_t> hkeys;
+  int device = -1;            // device of the buffer
+  size_t buf_bytes = 0;       // its size
 };
 
 namespace {
@@ -166,6 +175,39 @@ void* ws_get(lqm_ctx* ctx, int slot, size_t bytes) {
     b.bytes = want;
   }
   return b.p;
+}
+
+// Cache of freed Hops buffers (lqm_ctx::hops_cache): at most kHopsCacheCount
+// buffers and kHopsCacheBytes in total.  A buffer serves a request of `need`
+// bytes when it is at least that large and at most twice that plus 1 MiB, so a
+// small H does not pin a large buffer.
+constexpr size_t kHopsCacheBytes = size_t(1) << 30;
+constexpr size_t kHopsCacheCount = 16;
+
+void* hops_buffer_take(lqm_ctx* ctx, size_t need, size_t* got) {
+  size_t best = ctx->hops_cache.size();
+  for (size_t i = 0; i < ctx->hops_cache.size(); ++i) {
+    const size_t b = ctx->hops_cache[i].second;
+    if (b >= need && b <= 2 * need + (size_t(1) << 20) &&
+        (best == ctx->hops_cache.size() || b < ctx->hops_cache[best].second))
+      best = i;
+  }
+  if (best == ctx->hops_cache.size()) return nullptr;
+  void* p = ctx->hops_cache[best].first;
+  *got = ctx->hops_cache[best].second;
+  ctx->hops_cache_bytes -= *got;
+  ctx->hops_cache.erase(ctx->hops_cache.begin() + (std::ptrdiff_t)best);
+  return p;
+}
+
+// Keeps a freed buffer if the cache has room (true), else the caller frees it.
+bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
+  if (!p || bytes == 0 || ctx->hops_cache.size() >= kHopsCacheCount ||
+      ctx->hops_cache_bytes + bytes > kHopsCacheBytes)
+    return false;
+  ctx->hops_cache.emplace_back(p, bytes);
+  ctx->hops_cache_bytes += bytes;
+  return true;
 }
 
 enum WsSlot {
@@ -359,7 +401,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     DCLargeArgs da;
     da.n = n; da.nk = nbk; da.plan = plan; da.d = dd; da.e = ee; da.bands = d_bands + k0 * n;
     da.U = vec ? Ucur : nullptr; da.slots = slots; da.slot_doubles = slotd;
-    da.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
+    da.phase_cycles = ctx->phases_on ? ctx->d_phase : nullptr;
     if (dc_small)
       dc_large_kernel<128, 4><<<(unsigned)std::min<int64_t>(G, nbk), 128, 0, ctx->stream>>>(da);
     else
@@ -435,7 +477,7 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   a.w = ro ? ro->w : nullptr;
   a.mu = ro ? ro->mu : 0.0;
   a.T = ro ? ro->T : 0.0;
-  a.phase_cycles = ctx->stats_on ? ctx->d_phase : nullptr;
+  a.phase_cycles = ctx->phases_on ? ctx->d_phase : nullptr;
   std::pair<cudaEvent_t, cudaEvent_t> evs{};
   if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
   kfn<<<(unsigned)grid, nt, Ls.total, ctx->stream>>>(a);
@@ -644,6 +686,7 @@ int lqm_ctx_destroy(lqm_ctx* ctx) {
   for (auto& b : ctx->ws)
     if (b.p) cudaFree(b.p);
   for (auto& kv : ctx->plans) cudaFree(kv.second.d_buf);
+  for (auto& b : ctx->hops_cache) cudaFree(b.first);
   if (ctx->d_phase) cudaFree(ctx->d_phase);
   if (ctx->blas) cublasDestroy(ctx->blas);
   cudaEventDestroy(ctx->ev0);
@@ -760,6 +803,7 @@ int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing) {
     if (!ctx->d_phase) ck(cudaMalloc(&ctx->d_phase, PH_COUNT * sizeof(unsigned long long)), "cudaMalloc(stats)");
     ck(cudaMemset(ctx->d_phase, 0, PH_COUNT * sizeof(unsigned long long)), "memset(stats)");
     ctx->stats_on = enable_timing != 0;
+    ctx->phases_on = enable_timing >= 2;
     ctx->eigh_ms = 0.0;
     ctx->eigh_launches = 0;
     ctx->launches = 0;
@@ -795,16 +839,25 @@ int lqm_hops_upload_dense(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const 
     if (n > 4096) fail(LQM_EINVAL, "n=%lld exceeds the supported maximum 4096", (long long)n);
     if (!keys || !blocks) fail(LQM_EINVAL, "null keys or blocks");
     check_finite(blocks, 2 * n * n * nR, "blocks");
+    const size_t bb = (size_t)(n * n * nR) * sizeof(double2);
+    const size_t koff = (bb + 255) / 256 * 256;
+    const size_t need = koff + (size_t)(d * nR) * sizeof(int64_t);
+    size_t got = 0;
+    void* buf = hops_buffer_take(ctx, need, &got);
+    if (!buf) {
+      if (cudaMalloc(&buf, need) != cudaSuccess) {
+        cudaGetLastError();
+        fail(LQM_ENOMEM, "device allocation for hops failed");
+      }
+      got = need;
+    }
     lqm_hops* h = new lqm_hops();
     h->n = n; h->nR = nR; h->d = d;
     h->hkeys.assign(keys, keys + d * nR);
-    const size_t bb = (size_t)(n * n * nR) * sizeof(double2);
-    cudaError_t e1 = cudaMalloc(&h->blocks, bb);
-    cudaError_t e2 = cudaMalloc(&h->keys, (size_t)(d * nR) * sizeof(int64_t));
-    if (e1 != cudaSuccess || e2 != cudaSuccess) {
-      cudaFree(h->blocks); cudaFree(h->keys); delete h;
-      fail(LQM_ENOMEM, "device allocation for hops failed");
-    }
+    h->blocks = (double2*)buf;
+    h->keys = (int64_t*)((char*)buf + koff);
+    h->device = ctx->device;
+    h->buf_bytes = got;
     ck(cudaMemcpyAsync(h->blocks, blocks, bb, cudaMemcpyHostToDevice, ctx->stream), "hops upload");
     ck(cudaMemcpyAsync(h->keys, keys, (size_t)(d * nR) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream), "keys upload");
     wait_stream(ctx);
@@ -840,8 +893,11 @@ int lqm_hops_upload_csc(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const in
 int lqm_hops_free(lqm_ctx* ctx, lqm_hops* h) {
   if (!h) return LQM_EINVAL;
   if (ctx) { cudaSetDevice(ctx->device); cudaStreamSynchronize(ctx->stream); }
-  cudaFree(h->blocks);
-  cudaFree(h->keys);
+  if (!(ctx && ctx->device == h->device && hops_buffer_keep(ctx, h->blocks, h->buf_bytes))) {
+    if (h->device >= 0) cudaSetDevice(h->device);
+    cudaFree(h->blocks);
+    if (ctx) cudaSetDevice(ctx->device);
+  }
   delete h;
   return LQM_OK;
 }

@@ -178,8 +178,11 @@ class Context:
         self.check(_lib.lqm_ctx_last_kernel_ms(self._h, ctypes.byref(v)))
         return v.value
 
-    def reset_stats(self, timing=True):
-        self.check(_lib.lqm_ctx_reset_stats(self._h, int(bool(timing))))
+    def reset_stats(self, timing=True, phases=False):
+        """Zero the statistics; ``timing`` records CUDA-event times of the eigensolver
+        launches, ``phases`` also its per-phase cycle counters (see ``phase_cycles``)."""
+        mode = 2 if phases else int(bool(timing))
+        self.check(_lib.lqm_ctx_reset_stats(self._h, mode))
 
     def stats(self):
         """(eigensolver device ms, eigensolver launches, all kernel launches) since reset."""
@@ -189,7 +192,9 @@ class Context:
 
     def phase_cycles(self):
         """Eigensolver SM cycles per stage: bloch, householder, d&c, back-transform, sync,
-        then the d&c merge steps (zsort, deflate, secular, zhat, vectors, ranks, update, copy)."""
+        then the d&c merge steps (zsort, deflate, secular, zhat, vectors, ranks, update, copy),
+        then the householder steps (pass, mat-vec reduction, column); recorded after
+        ``reset_stats(phases=True)``."""
         out = (_D * 16)()
         self.check(_lib.lqm_ctx_phase_cycles(self._h, out))
         return list(out)

@@ -84,6 +84,48 @@ def test_batch_models_bands(lqm, ctx):
         assert rel_band_err(b, oracle_bands(h, ks)) <= BAND_TOL, name
 
 
+def test_hops_upload_free_reuse(lqm):
+    """Upload, one pass and free in a loop, the way a per-call user does: the context
+    hands freed Hops buffers to later uploads (of other orders and key counts too, so
+    the keys sit at another offset of a reused buffer), and every pass still matches
+    the oracle."""
+    c = lqm.Context(0, timeout=600)
+    try:
+        ks = np.hstack([L.regulargrid(8 * 8), np.random.default_rng(3).random((2, 16))])
+        models = [h for _, h in M.batch_models()]
+        models.append({R: models[0][R] for R in [(0, 0), (1, 0), (-1, 0)]})  # fewer keys, same order
+        ref = [oracle_bands(h, ks) for h in models]
+        for it in range(3):
+            for h, r in zip(models if it % 2 == 0 else models[::-1], ref if it % 2 == 0 else ref[::-1]):
+                Hd = lqm.DeviceHops(h, c)
+                b, _ = lqm.bandmatrix(Hd, ks, ctx=c)
+                Hd.free()
+                assert rel_band_err(b, r) <= BAND_TOL
+    finally:
+        c.close()
+
+
+def test_stats_modes(lqm):
+    """reset_stats(timing=True) times the eigensolver launches without its phase
+    counters; reset_stats(phases=True) records both."""
+    c = lqm.Context(0, timeout=600)
+    try:
+        h = M.batch_models()[1][1]
+        ks = L.regulargrid(8 * 8)
+        c.reset_stats(timing=True)
+        lqm.bandmatrix(h, ks, ctx=c)
+        ms, launches, _ = c.stats()
+        assert launches >= 1 and ms > 0.0
+        assert all(v == 0.0 for v in c.phase_cycles())
+        c.reset_stats(phases=True)
+        lqm.bandmatrix(h, ks, ctx=c)
+        ph = c.phase_cycles()
+        assert c.stats()[1] >= 1 and ph[1] > 0.0 and ph[2] > 0.0
+        c.reset_stats(timing=False)
+    finally:
+        c.close()
+
+
 def test_large_n_global_scratch_path(lqm):
     # n = 148 on the one-CTA kernel (the default context takes the blocked path from
     # n = 128 on): the Householder matrix lives in global scratch (does not fit shared memory)
