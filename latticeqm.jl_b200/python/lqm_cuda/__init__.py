@@ -228,7 +228,9 @@ def pack_hops(h):
     n = mats[0].shape[0]
     d = len(keys[0])
     K = np.asfortranarray(np.array(keys, dtype=np.int64).T)
-    B = np.asfortranarray(np.stack(mats, axis=-1))
+    B = np.empty((n, n, len(keys)), dtype=np.complex128, order="F")  # one copy per block
+    for r, m in enumerate(mats):
+        B[:, :, r] = m
     return n, len(keys), d, K, B
 
 
