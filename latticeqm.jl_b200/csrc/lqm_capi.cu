@@ -259,9 +259,22 @@ int eigh_threads_for(const lqm_ctx* ctx, int n) {
   return it != ctx->eigh_nt.end() ? it->second : eigh_threads(n);
 }
 
-// eigh_kernel instantiation for a block size (512 threads from n = 64 on).
+// eigh_kernel instantiation for a block size.  One-warp and four-warp blocks
+// (small n, where shared memory leaves room for many CTAs per SM) take
+// instantiations whose launch bounds cap registers at 128 per thread, so 16 or
+// 4 CTAs share an SM instead of the 8 or 2 that the 254 registers of the
+// 256-thread instantiation allow.  Measured on B200 (rho pass, 65 536 k):
+// n = 8 at 32 threads 10.7 -> 8.7 ms, n = 24 at 128 threads 53.6 -> 43.7 ms.
+// Two-warp blocks keep the uncapped code: capped, n = 24 at 64 threads (its
+// fastest size) went from 40.4 to 41.7 ms, the spills outweighing the
+// doubled residency.
 using EighFn = void (*)(EighArgs);
-EighFn eigh_fn(int nt) { return nt > 384 ? &eigh_kernel<512> : (nt > 256 ? &eigh_kernel<384> : &eigh_kernel<256>); }
+EighFn eigh_fn(int nt) {
+  if (nt <= 32) return &eigh_kernel<32, 16>;
+  if (nt <= 64) return &eigh_kernel<256>;
+  if (nt <= 128) return &eigh_kernel<128, 4>;
+  return nt > 384 ? &eigh_kernel<512> : (nt > 256 ? &eigh_kernel<384> : &eigh_kernel<256>);
+}
 
 void timer_start(lqm_ctx* ctx) { ck(cudaEventRecord(ctx->ev0, ctx->stream), "event"); }
 void timer_stop(lqm_ctx* ctx) {
