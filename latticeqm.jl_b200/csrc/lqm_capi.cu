@@ -212,7 +212,7 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
-  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2, WS_FOLD,
+  WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
   WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB
 };
 static_assert(WS_BDGB < 40, "workspace slots");
@@ -518,22 +518,15 @@ int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
 }
 
 // Density matrix on device arrays; accumulates eband into d_eb[0].
-// rho_L (+)= sum_k coef[k,L] rho_k over a batch: split-k partials, then an
-// ordered reduction (deterministic for a fixed batch size).
+// rho_L (+)= sum_k coef[k,L] rho_k over a batch, as one ZGEMM: with rho_k the
+// columns of R (nn x nb) and coef the nL x nb matrix C, rho_L (nn x nL) =
+// R C^T (+ rho_L).  A skinny product (nL ~ 9 outputs per element read) that
+// streams the rho_k batch once; cuBLAS's fixed kernel choice keeps it
+// deterministic for a given batch size.
 void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const double2* coef, int nL,
                  double2* d_rho, int accumulate) {
-  const int64_t tiles = (nn + 255) / 256;
-  int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(nb, (4 * (int64_t)ctx->num_sms + tiles - 1) / tiles));
-  chunks = std::min<int64_t>(chunks, 65535);
-  const int64_t kchunk = (nb + chunks - 1) / chunks;
-  chunks = (nb + kchunk - 1) / kchunk;
-  double2* part = (double2*)ws_get(ctx, WS_FOLD, (size_t)(chunks * nL * nn) * sizeof(double2));
-  fold_partial_kernel<16><<<dim3((unsigned)tiles, (unsigned)chunks), 256, 0, ctx->stream>>>(nn, nb, kchunk, rk, coef,
-                                                                                          nL, part);
-  const int64_t m = nL * nn;
-  fold_reduce_kernel<<<(unsigned)std::min<int64_t>((m + 255) / 256, 8192), 256, 0, ctx->stream>>>(
-      m, (int)chunks, part, d_rho, accumulate);
-  ck(cudaGetLastError(), "fold launch");
+  zgemm_sb(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_T, (int)nn, nL, (int)nb, 1.0, rk, (int)nn, 0, coef, nL, 0,
+           accumulate ? 1.0 : 0.0, d_rho, (int)nn, 0, 1);
 }
 
 // bands_out (n x nk, device) receives every k's eigenvalues when non-null.

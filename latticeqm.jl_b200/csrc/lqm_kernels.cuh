@@ -273,45 +273,6 @@ __global__ void fold_coef_kernel(int64_t nb, int dim, const double* __restrict__
   }
 }
 
-// Split-k Fourier fold, stage 1: part[chunk][l][e] = sum over the chunk's k
-// (in order) of coef[kb,l] * rhok[kb][e].  Grid: (element tiles, k-chunks).
-template <int LC>
-__global__ void __launch_bounds__(256) fold_partial_kernel(int64_t nn, int64_t nb, int64_t kchunk,
-                                                           const double2* __restrict__ rhok,
-                                                           const double2* __restrict__ coef, int nL,
-                                                           double2* __restrict__ part) {
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t k0 = blockIdx.y * kchunk;
-  const int64_t k1 = (k0 + kchunk < nb) ? k0 + kchunk : nb;
-  if (e >= nn) return;
-  double2* out = part + (int64_t)blockIdx.y * nL * nn;
-  for (int l0 = 0; l0 < nL; l0 += LC) {
-    double2 acc[LC];
-#pragma unroll
-    for (int l = 0; l < LC; ++l) acc[l] = cmk(0.0, 0.0);
-    for (int64_t kb = k0; kb < k1; ++kb) {
-      const double2 x = rhok[kb * nn + e];
-      const double2* cf = coef + kb * nL + l0;
-#pragma unroll
-      for (int l = 0; l < LC; ++l)
-        if (l0 + l < nL) acc[l] = cadd(acc[l], cmul(cf[l], x));
-    }
-#pragma unroll
-    for (int l = 0; l < LC; ++l)
-      if (l0 + l < nL) out[(int64_t)(l0 + l) * nn + e] = acc[l];
-  }
-}
-
-// Stage 2: rhoL[l][e] (+)= sum over chunks in order of part[chunk][l][e].
-__global__ void fold_reduce_kernel(int64_t m /* nL * nn */, int nchunks, const double2* __restrict__ part,
-                                   double2* __restrict__ rhoL, int accumulate) {
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
-    double2 s = accumulate ? rhoL[t] : cmk(0.0, 0.0);
-    for (int c = 0; c < nchunks; ++c) s = cadd(s, part[(int64_t)c * m + t]);
-    rhoL[t] = s;
-  }
-}
-
 // Fixed-order sum of x[0..m) into out[0] (single CTA).
 __global__ void ordered_sum_kernel(const double* __restrict__ x, int64_t m, double* out, int accumulate) {
   __shared__ double red[32];
