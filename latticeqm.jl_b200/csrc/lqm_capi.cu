@@ -259,19 +259,19 @@ int eigh_threads_for(const lqm_ctx* ctx, int n) {
   return it != ctx->eigh_nt.end() ? it->second : eigh_threads(n);
 }
 
-// eigh_kernel instantiation for a block size.  One-warp and four-warp blocks
+// eigh_kernel instantiation for a block size.  Blocks of up to 128 threads
 // (small n, where shared memory leaves room for many CTAs per SM) take
-// instantiations whose launch bounds cap registers at 128 per thread, so 16 or
-// 4 CTAs share an SM instead of the 8 or 2 that the 254 registers of the
-// 256-thread instantiation allow.  Measured on B200 (rho pass, 65 536 k):
-// n = 8 at 32 threads 10.7 -> 8.7 ms, n = 24 at 128 threads 53.6 -> 43.7 ms.
-// Two-warp blocks keep the uncapped code: capped, n = 24 at 64 threads (its
-// fastest size) went from 40.4 to 41.7 ms, the spills outweighing the
-// doubled residency.
+// instantiations whose launch bounds cap the registers per thread so that
+// more CTAs share an SM than the 254 registers of the 256-thread
+// instantiation allow.  Measured on B200 (rho pass, 65 536 k):
+//   32 threads, 128 registers (16 CTAs/SM instead of 8): n = 8 10.7 -> 8.7 ms;
+//   64 threads, 168 registers (6 instead of 4): n = 24 41.1 -> 37.0 ms
+//     (128 registers, 8 CTAs, spilled: 41.7 ms);
+//   128 threads, 128 registers (4 instead of 2): n = 24 53.6 -> 43.7 ms.
 using EighFn = void (*)(EighArgs);
 EighFn eigh_fn(int nt) {
   if (nt <= 32) return &eigh_kernel<32, 16>;
-  if (nt <= 64) return &eigh_kernel<256>;
+  if (nt <= 64) return &eigh_kernel<64, 6>;
   if (nt <= 128) return &eigh_kernel<128, 4>;
   return nt > 384 ? &eigh_kernel<512> : (nt > 256 ? &eigh_kernel<384> : &eigh_kernel<256>);
 }
