@@ -44,3 +44,21 @@ def test_context_creation_reports_missing_device(lqm):
     h = ctypes.c_void_p()
     st = lqm.lib().lqm_ctx_create(0, ctypes.byref(h))
     assert st == -2 and not h.value                   # LQM_ECUDA, no CPU fallback
+
+
+def test_pack_hops_layout(lqm):
+    """pack_hops hands the C-ABI the layout lqm_hops_upload_dense reads: keys d x nR
+    and blocks n x n x nR, both column-major (Julia's), block r = h[key r]."""
+    import numpy as np
+    rng = np.random.default_rng(4)
+    h = {(i, j): rng.normal(size=(5, 5)) + 1j * rng.normal(size=(5, 5)) for i in (-1, 0, 1) for j in (0, 2)}
+    n, nR, d, K, B = lqm.pack_hops(h)
+    assert (n, nR, d) == (5, 6, 2)
+    assert K.dtype == np.int64 and K.flags.f_contiguous and K.shape == (2, 6)
+    assert B.dtype == np.complex128 and B.flags.f_contiguous and B.shape == (5, 5, 6)
+    flat = np.frombuffer(B.tobytes(order="A"), dtype=np.complex128)
+    for r, R in enumerate(h):
+        assert tuple(K[:, r]) == R
+        # column-major block r starts at r * n * n; element (i, j) at i + j * n
+        blk = flat[r * 25:(r + 1) * 25].reshape(5, 5, order="F")
+        assert np.array_equal(blk, h[R])
