@@ -864,9 +864,16 @@ int lqm_hops_upload_dense(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const 
     h->keys = (int64_t*)((char*)buf + koff);
     h->device = ctx->device;
     h->buf_bytes = got;
-    ck(cudaMemcpyAsync(h->blocks, blocks, bb, cudaMemcpyHostToDevice, ctx->stream), "hops upload");
-    ck(cudaMemcpyAsync(h->keys, keys, (size_t)(d * nR) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream), "keys upload");
-    wait_stream(ctx);
+    try {
+      ck(cudaMemcpyAsync(h->blocks, blocks, bb, cudaMemcpyHostToDevice, ctx->stream), "hops upload");
+      ck(cudaMemcpyAsync(h->keys, keys, (size_t)(d * nR) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream),
+         "keys upload");
+      wait_stream(ctx);
+    } catch (const LqmError& e) {  // neither the buffer nor the handle outlives a failed upload
+      if (e.code != LQM_ETIMEOUT) cudaFree(buf);  // (after a timeout the copy may still run: leave it)
+      delete h;
+      throw;
+    }
     *out = h;
   });
 }
