@@ -100,10 +100,13 @@ precision_code(e::CudaExec) = e.precision === :fp64 ? Cint(0) :
 # ---------------------------------------------------------------- routines
 """bands (n x nk) and, with `vectors=true`, U (n x n x nk): `bandmatrix` without projectors."""
 function cuda_bandmatrix(H, ks::AbstractMatrix{Float64}, exec::CudaExec; vectors::Bool=false)
-    ctx = context(exec.device)
-    dh = upload(ctx, H)
     n = size(H[first(keys(H))], 1)
     nk = size(ks, 2)
+    if nk == 0  # an empty k-set: the k-loop runs zero times (Spectrum/bands.jl:164-204)
+        return vectors ? (zeros(Float64, n, 0), zeros(ComplexF64, n, n, 0)) : zeros(Float64, n, 0)
+    end
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
     bands = zeros(Float64, n, nk)
     U = vectors ? zeros(ComplexF64, n, n, nk) : ComplexF64[]
     check(ctx, ccall((:lqm_bandmatrix, LIB[]), Cint,
@@ -334,6 +337,12 @@ end
 """`getdensitymatrix!(ρs, H, ks, kweights, μ; T)` on the device; returns the band energy."""
 function cuda_densitymatrix!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
                              μ::Float64, T::Real, exec::CudaExec)
+    if size(ks, 2) == 0  # an empty k-set: ρ is zeroed and the k-sum is empty (densitymatrix.jl:17-49)
+        for k in keys(ρs)
+            ρs[k] .= 0
+        end
+        return 0.0
+    end
     ctx = context(exec.device)
     dh = upload(ctx, H)
     Lk = collect(keys(ρs))
@@ -410,10 +419,14 @@ const WHICH_CODE = Dict(:LM => Cint(0), :SR => Cint(1), :LR => Cint(2))
 (Eigen/eigen_sparse_krylovkit.jl:44-88), ascending."""
 function cuda_bandmatrix_partial(H, ks::AbstractMatrix{Float64}, num_bands::Int, exec::CudaExec;
                                  sigma::Float64=1e-8, which::Symbol=:LM, vectors::Bool=false)
-    ctx = context(exec.device)
-    dh = upload(ctx, H)
     n = size(H[first(keys(H))], 1)
     nk = size(ks, 2)
+    if nk == 0
+        return vectors ? (zeros(Float64, num_bands, 0), zeros(ComplexF64, n, num_bands, 0)) :
+               zeros(Float64, num_bands, 0)
+    end
+    ctx = context(exec.device)
+    dh = upload(ctx, H)
     bands = zeros(Float64, num_bands, nk)
     U = vectors ? zeros(ComplexF64, n, num_bands, nk) : ComplexF64[]
     check(ctx, ccall((:lqm_bandmatrix_partial, LIB[]), Cint,
@@ -428,6 +441,12 @@ end
 function cuda_densitymatrix_partial!(ρs::Hops, H, ks::AbstractMatrix{Float64}, kweights::AbstractVector{Float64},
                                      μ::Float64, T::Real, num_bands::Int, exec::CudaExec;
                                      sigma::Float64=1e-8, which::Symbol=:LM)
+    if size(ks, 2) == 0
+        for k in keys(ρs)
+            ρs[k] .= 0
+        end
+        return 0.0
+    end
     ctx = context(exec.device)
     dh = upload(ctx, H)
     Lk = collect(keys(ρs))

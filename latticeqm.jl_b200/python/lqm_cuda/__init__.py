@@ -267,6 +267,14 @@ def _as_device_hops(H, ctx):
     return H if isinstance(H, DeviceHops) else DeviceHops(H, ctx)
 
 
+def _hops_dims(H):
+    """(n, d) of a dict Hops or a DeviceHops, without touching the device."""
+    if isinstance(H, DeviceHops):
+        return H.n, H.d
+    R = next(iter(H))
+    return np.asarray(H[R]).shape[0], len(R)
+
+
 def _ks(ks, d=None):
     ks = np.asfortranarray(np.asarray(ks, dtype=np.float64))
     if ks.ndim == 1:
@@ -300,9 +308,13 @@ def bandmatrix(H, ks, multimode="cuda", want_vectors=False, precision=0, ctx=Non
     _check_mode(multimode)
     if str(format).lstrip(":") == "sparse" and num_bands is not None:
         return bandmatrix_partial(H, ks, num_bands, sigma=sigma, which=which, want_vectors=want_vectors, ctx=ctx)
+    n, d = _hops_dims(H)
+    ks = _ks(ks, d)
+    if ks.shape[1] == 0:  # an empty k-set: the reference's k-loop runs zero times (bands.jl:164-204)
+        return np.zeros((n, 0), order="F"), (np.zeros((n, n, 0), dtype=np.complex128, order="F")
+                                             if want_vectors else None)
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
-    ks = _ks(ks, Hd.d)
     nk = ks.shape[1]
     bands = np.zeros((Hd.n, nk), order="F")
     U = np.zeros((Hd.n, Hd.n, nk), dtype=np.complex128, order="F") if want_vectors else None
@@ -367,9 +379,13 @@ def bandmatrix_partial(H, ks, num_bands, sigma=1e-8, which="LM", want_vectors=Fa
     ``num_bands`` eigenvalues nearest ``sigma`` (:LM), smallest (:SR) or largest (:LR),
     ascending; bands (num_bands, nk) and optionally U (n, num_bands, nk)
     (``lqm_bandmatrix_partial``)."""
+    n, d = _hops_dims(H)
+    ks = _ks(ks, d)
+    if ks.shape[1] == 0:
+        return np.zeros((int(num_bands), 0), order="F"), (
+            np.zeros((n, int(num_bands), 0), dtype=np.complex128, order="F") if want_vectors else None)
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
-    ks = _ks(ks, Hd.d)
     nk = ks.shape[1]
     bands = np.zeros((int(num_bands), nk), order="F")
     U = np.zeros((Hd.n, int(num_bands), nk), dtype=np.complex128, order="F") if want_vectors else None
@@ -386,9 +402,14 @@ def getdensitymatrix(rhos, H, ks, kweights=None, mu=0.0, T=0.01, multimode="cuda
     ``format="sparse"`` only the ``num_bands`` states selected as in
     ``bandmatrix_partial`` enter (``lqm_densitymatrix_partial``)."""
     _check_mode(multimode)
+    n, d = _hops_dims(H)
+    ks = _ks(ks, d)
+    if ks.shape[1] == 0:  # an empty k-set: rho is zeroed and the k-sum is empty (densitymatrix.jl:17-49)
+        for L in list(rhos.keys()):
+            rhos[L] = np.zeros((n, n), dtype=np.complex128)
+        return 0.0
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
-    ks = _ks(ks, Hd.d)
     nk = ks.shape[1]
     Lkeys = list(rhos.keys())
     nL = len(Lkeys)

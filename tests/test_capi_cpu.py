@@ -62,3 +62,27 @@ def test_pack_hops_layout(lqm):
         # column-major block r starts at r * n * n; element (i, j) at i + j * n
         blk = flat[r * 25:(r + 1) * 25].reshape(5, 5, order="F")
         assert np.array_equal(blk, h[R])
+
+
+def test_empty_kset_matches_oracle_without_a_device(lqm):
+    """An empty k-set gives what the reference's loops give when they run zero times
+    (bands.jl:164-204, densitymatrix.jl:17-49): n x 0 bands, zeroed rho blocks and a
+    band energy of 0.  The mirror answers before any device work, so this holds on a
+    machine without a GPU as well."""
+    import numpy as np
+    from oracle import kspace as K
+    t = np.array([[0.1, 0.2], [0.0, 0.1]], complex)
+    h = {(0, 0): np.diag([0.3, -0.2]).astype(complex), (1, 0): t, (-1, 0): t.conj().T}
+    ks = np.zeros((2, 0))
+    b, U = lqm.bandmatrix(h, ks)
+    assert b.shape == K.bandmatrix(h, ks)[0].shape == (2, 0) and U is None
+    b, U = lqm.bandmatrix(h, ks, want_vectors=True)
+    assert b.shape == (2, 0) and U.shape == (2, 2, 0)
+    bp, _ = lqm.bandmatrix(h, ks, format="sparse", num_bands=1)
+    assert bp.shape == (1, 0)
+    rho = {(0, 0): np.ones((2, 2), complex), (1, 0): None}
+    eb = lqm.getdensitymatrix(rho, h, ks, mu=0.0, T=0.01)
+    ref, eb_ref = K.densitymatrix(h, ks, np.zeros(0), 0.0, 0.01, list(rho.keys()))
+    assert eb == eb_ref == 0.0
+    for R in rho:
+        assert np.array_equal(rho[R], ref[R]) and not rho[R].any()
