@@ -83,7 +83,8 @@ int lqm_ctx_scf_exchange_energy(const lqm_ctx* ctx, double* eJ);
  * counterpart (a device launch parameter). */
 int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt);
 /* Autotuner of that block size for H's order (below the blocked path): every
- * candidate (multiples of 32 around the built-in rule whose shared-memory plan
+ * candidate (the block sizes 32, 64, 128, 256, 384 and 512 from half the
+ * built-in rule's size up to four times it, or 512, whose shared-memory plan
  * fits) runs the eigen pass on the nk sample k-points (rho_k at mu = 0, T = 0.01
  * when want_rho, else eigenvectors), warmed up once and timed once with CUDA
  * events; the fastest becomes the context's block size for n (the sample should
