@@ -151,3 +151,99 @@ def test_emulated_backtransform_column_range(emul, name, h):
                                 cb, ce, ev2.ctypes.data_as(P), U.ctypes.data_as(P))
         assert np.array_equal(ev2, ev)
         assert np.array_equal(U[:, cb:ce], Ufull[:, cb:ce])
+
+
+def _stress_tridiagonals():
+    """Standard hard cases for divide and conquer: Wilkinson W+ (eigenvalue pairs
+    split near machine precision), glued Wilkinson blocks (clusters of up to five),
+    Clement (integer spectrum +-(n-1), +-(n-3), ...), the discrete Laplacian, graded
+    entries, zero / constant / decoupled matrices and extreme scales."""
+    out = []
+    for m in (21, 97):
+        k = (m - 1) // 2
+        out.append((f"wilkinson{m}", np.abs(np.arange(-k, k + 1)).astype(float), np.ones(m - 1)))
+    for delta in (1e-14, 1e-8):
+        d = np.tile(np.abs(np.arange(-10, 11)).astype(float), 5)
+        e = np.ones(len(d) - 1)
+        e[20::21] = delta
+        out.append((f"glued_wilkinson21x5_{delta:g}", d, e))
+    for n in (10, 96):
+        i = np.arange(1, n)
+        out.append((f"clement{n}", np.zeros(n), np.sqrt(i * (n - i))))
+    rng = np.random.default_rng(5)
+    n = 96
+    out += [("laplace96", np.full(n, 2.0), np.full(n - 1, -1.0)),
+            ("graded96", 10.0 ** (-0.3 * np.arange(n)), 10.0 ** (-0.3 * np.arange(n - 1) - 0.15)),
+            ("zero96", np.zeros(n), np.zeros(n - 1)),
+            ("const96", np.full(n, 3.0), np.zeros(n - 1)),
+            ("tiny_coupling96", rng.normal(size=n), np.full(n - 1, 1e-300)),
+            ("scale1e150", rng.normal(size=n) * 1e150, rng.normal(size=n - 1) * 1e150),
+            ("scale1e-150", rng.normal(size=n) * 1e-150, rng.normal(size=n - 1) * 1e-150)]
+    return out
+
+
+@pytest.mark.parametrize("name,d,e", _stress_tridiagonals(), ids=lambda x: x if isinstance(x, str) else "")
+def test_emulated_dc_stress_matrices(emul, name, d, e):
+    n = len(d)
+    T = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    ref = np.linalg.eigvalsh(T)
+    scale = max(np.max(np.abs(ref)), np.finfo(float).tiny)
+    for vec in (1, 0):
+        ev = np.zeros(n)
+        Z = np.zeros((n, n), order="F")
+        emul.lqm_emul_tridiag(n, np.ascontiguousarray(d).ctypes.data_as(P), np.ascontiguousarray(e).ctypes.data_as(P),
+                              ev.ctypes.data_as(P), Z.ctypes.data_as(P), vec)
+        assert np.all(np.isfinite(ev)) and np.all(np.diff(ev) >= 0)
+        assert np.max(np.abs(ev - ref)) <= 1e-13 * scale
+        if vec:
+            assert np.max(np.abs(Z.T @ Z - np.eye(n))) <= 1e-13
+            assert np.max(np.abs(T @ Z - Z * ev)) <= 1e-13 * scale
+
+
+def _hard_hermitian():
+    rng = np.random.default_rng(9)
+
+    def unitary(n):
+        return np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))[0]
+
+    def herm(n):
+        A = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+        return (A + A.conj().T) / 2
+
+    out = []
+    for n in (8, 96):
+        e = rng.normal(size=n - 1) * np.exp(1j * rng.uniform(0, 2 * np.pi, n - 1))
+        Q = unitary(n)
+        dv = np.repeat(rng.normal(size=(n + 3) // 4), 4)[:n]
+        Q2 = unitary(n)
+        dp = np.sort(rng.normal(size=n))
+        dp[1::2] = dp[0::2][:len(dp[1::2])] + 1e-13
+        Mz = herm(n)
+        Mz[:, n // 2] = 0
+        Mz[n // 2, :] = 0
+        out += [(f"diagonal{n}", np.diag(rng.normal(size=n)).astype(complex)),
+                (f"tridiagonal_complex{n}", np.diag(rng.normal(size=n)) + np.diag(e, -1) + np.diag(e.conj(), 1)),
+                (f"fourfold_degenerate{n}", Q @ np.diag(dv) @ Q.conj().T),
+                (f"pairs_split_1e-13_{n}", Q2 @ np.diag(dp) @ Q2.conj().T),
+                (f"zero{n}", np.zeros((n, n), complex)),
+                (f"identity{n}", np.eye(n, dtype=complex)),
+                (f"scale1e150_{n}", herm(n) * 1e150),
+                (f"scale1e-150_{n}", herm(n) * 1e-150),
+                (f"zero_row_and_column{n}", Mz),
+                (f"rank_one{n}", 3.0 * np.outer(Q[:, 0], Q[:, 0].conj()))]
+    return out
+
+
+@pytest.mark.parametrize("name,Hk", _hard_hermitian(), ids=lambda x: x if isinstance(x, str) else "")
+def test_emulated_eigh_hard_hermitian(emul, name, Hk):
+    """The whole one-CTA path (Householder, divide and conquer, back-transformation)
+    on inputs that exercise its special cases: zero reflectors, deflation of whole
+    clusters, near-degenerate pairs, extreme scales."""
+    ev, U = run(emul, {(0, 0): Hk}, (0.0, 0.0))
+    n = Hk.shape[0]
+    ref = K.eigh_upper(Hk, vectors=False)
+    scale = max(np.max(np.abs(ref)), np.finfo(float).tiny)
+    assert np.all(np.isfinite(U))
+    assert np.max(np.abs(ev - ref)) <= 1e-12 * scale
+    assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12
+    assert np.max(np.abs(Hk @ U - U * ev)) <= 1e-12 * scale

@@ -559,3 +559,29 @@ def test_eigh_block_sizes_and_autotuner(lqm):
             c.set_eigh_threads(n, 0)
     finally:
         c.close()
+
+
+def test_hard_hermitian_inputs_both_paths(lqm):
+    """The hard Hermitian inputs of the emulation suite (zero reflectors, whole
+    degenerate clusters, pairs split by 1e-13, zero rows, rank one, scales 1e+-150)
+    through the C-ABI on the one-CTA kernel and on the blocked path."""
+    from test_emulation import _hard_hermitian
+    cases = _hard_hermitian()
+    ks = np.zeros((2, 1))
+    for blocked in (False, True):
+        c = lqm.Context(0, timeout=600)
+        try:
+            if blocked:
+                c.set_blocked_min_n(1)
+            for name, Hk in cases:
+                b, U = lqm.bandmatrix({(0, 0): Hk}, ks, want_vectors=True, ctx=c)
+                n = Hk.shape[0]
+                ref = K.eigh_upper(Hk, vectors=False)
+                scale = max(np.max(np.abs(ref)), np.finfo(float).tiny)
+                Uk = U[:, :, 0]
+                assert np.all(np.isfinite(Uk)), (name, blocked)
+                assert np.max(np.abs(b[:, 0] - ref)) <= 1e-12 * scale, (name, blocked)
+                assert np.max(np.abs(Uk.conj().T @ Uk - np.eye(n))) <= 1e-12, (name, blocked)
+                assert np.max(np.abs(Hk @ Uk - Uk * b[:, 0])) <= 1e-12 * scale, (name, blocked)
+        finally:
+            c.close()
