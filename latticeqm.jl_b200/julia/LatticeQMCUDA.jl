@@ -538,7 +538,7 @@ function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractM
                                T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
                                log_callback=nothing, acceleration::Symbol=:linear, anderson_depth::Int=5,
                                residual_norm::Symbol=:density, hartree::Bool=true, fock::Bool=true,
-                               exchange=nothing)
+                               exchange=nothing, convergenceerror::Bool=false)
     ctx = context(exec.device)
     set_functional!(ctx, hartree, fock, exchange)
     acceleration in (:linear, :anderson) ||
@@ -573,7 +573,18 @@ function cuda_solvehartreefock(h, v, ρ_init::Hops, filling::Real, ks::AbstractM
     eJ = Ref{Float64}(0.0)
     check(ctx, ccall((:lqm_ctx_scf_exchange_energy, LIB[]), Cint, (Ptr{Cvoid}, Ref{Float64}), ctx.ptr, eJ))
     info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵJ=eJ[], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
+    scf_convergence_check(out, convergenceerror)
     ρ, out[1], info, out[8] != 0, out[7]
+end
+
+# Not converged: fixedpoint!'s warning (Meanfield/fixedpoint.jl:189-191) and, with
+# convergenceerror, solvehartreefock's error (Meanfield/selfconsistent.jl:315-317).
+function scf_convergence_check(out, convergenceerror::Bool)
+    if out[8] == 0
+        @warn("SCF stopped before reaching the tolerance; residual $(out[7]) after $(Int(out[9])) iterations")
+        convergenceerror && error("SCF did not converge (convergenceerror = true)")
+    end
+    nothing
 end
 
 """Device-resident `solvehartreefock` for `HartreeFockBDG` (Superconductivity/hartreefock.jl:5-159):
@@ -585,7 +596,7 @@ function cuda_solvehartreefock_bdg(h, v, ρ_init::Hops, filling::Real, ks::Abstr
                                    T::Real=0.0, β::Real=1.0, tol::Real=1e-7, iterations::Int=500,
                                    log_callback=nothing, hartree::Bool=true, fock::Bool=true,
                                    acceleration::Symbol=:linear, anderson_depth::Int=5,
-                                   residual_norm::Symbol=:density)
+                                   residual_norm::Symbol=:density, convergenceerror::Bool=false)
     ctx = context(exec.device)
     acceleration in (:linear, :anderson) ||
         throw(ArgumentError("acceleration must be :linear or :anderson, got $(acceleration)"))
@@ -618,6 +629,7 @@ function cuda_solvehartreefock_bdg(h, v, ρ_init::Hops, filling::Real, ks::Abstr
     LOG_CB[] = nothing
     ρ = Hops(Dict(k => rho[:, :, i] for (i, k) in enumerate(Lk)))
     info = (μ=out[2], ϵH=out[3], ϵF=out[4], ϵP=out[10], ϵband=out[5], ϵkin=out[6], iterations=Int(out[9]))
+    scf_convergence_check(out, convergenceerror)
     ρ, out[1], info, out[8] != 0, out[7]
 end
 

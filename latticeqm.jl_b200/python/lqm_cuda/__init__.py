@@ -19,6 +19,7 @@ Reference (LatticeQM.jl):
 """
 import ctypes
 import os
+import warnings
 from collections import namedtuple
 
 import numpy as np
@@ -849,14 +850,28 @@ def hartreefock_eval(h, v, rho, hartree=True, fock=True, exchange=None, keys=Non
     return {L: np.array(out[:, :, i]) for i, L in enumerate(keys)}, en[0], en[1], en[2]
 
 
+def _hf_result(rho_out, out, mf, convergenceerror):
+    """(ρ, ϵ_GS, mf, converged, residual) from lqm_scf_hf's scalars.  Not converged:
+    a warning as fixedpoint! gives (Meanfield/fixedpoint.jl:189-191), and with
+    ``convergenceerror`` an error (Meanfield/selfconsistent.jl:315-317)."""
+    converged = bool(out[7])
+    if not converged:
+        warnings.warn(f"SCF stopped before reaching the tolerance; residual {out[6]} after {int(out[8])} "
+                      f"iterations", stacklevel=3)
+        if convergenceerror:
+            raise LQMError(-5, "SCF did not converge (convergenceerror=True)")
+    return HFResult(rho_out, out[0], mf, converged, out[6])
+
+
 def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
                      kweights=None, log_callback=None, multimode="cuda", ctx=None, acceleration="linear",
-                     anderson_depth=5, residual_norm="density", hartree=True, fock=True, exchange=None):
+                     anderson_depth=5, residual_norm="density", hartree=True, fock=True, exchange=None,
+                     convergenceerror=False):
     """``solvehartreefock(h, v, ρ_init, filling, ks; T, β, tol, iterations, acceleration,
-    anderson_depth, residual_norm)``: linear damped mixing (default) or Anderson
-    acceleration; the relative density change (default) or the commutator norm
+    anderson_depth, residual_norm, convergenceerror)``: linear damped mixing (default) or
+    Anderson acceleration; the relative density change (default) or the commutator norm
     ||[H_MF, ρ]|| as the residual.  Returns (ρ, ϵ_GS, mf, converged, residual) like the
-    reference."""
+    reference; an unconverged SCF warns, and raises with ``convergenceerror=True``."""
     _check_mode(multimode)
     acceleration = str(acceleration).lstrip(":")
     residual_norm = str(residual_norm).lstrip(":")
@@ -892,7 +907,7 @@ def solvehartreefock(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, ite
     eJ = _D()
     ctx.check(_lib.lqm_ctx_scf_exchange_energy(ctx.handle, ctypes.byref(eJ)))
     mf = MFInfo(mu=out[1], eH=out[2], eF=out[3], eband=out[4], ekin=out[5], iterations=int(out[8]), eJ=eJ.value)
-    return HFResult(rho_out, out[0], mf, bool(out[7]), out[6])
+    return _hf_result(rho_out, out, mf, convergenceerror)
 
 
 BdGMFInfo = namedtuple("BdGMFInfo", ["mu", "eH", "eF", "eP", "eband", "ekin", "iterations"])
@@ -900,9 +915,9 @@ BdGMFInfo = namedtuple("BdGMFInfo", ["mu", "eH", "eF", "eP", "eband", "ekin", "i
 
 def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7, iterations=500,
                          log_callback=None, hartree=True, fock=True, acceleration="linear", anderson_depth=5,
-                         residual_norm="density", ctx=None):
+                         residual_norm="density", ctx=None, convergenceerror=False):
     """``solvehartreefock(h::BdGOperator, v, ρ_init::BdGOperator, filling, ks; T, β, tol,
-    iterations)``: Hartree-Fock with the pairing channel (HartreeFockBDG,
+    iterations, convergenceerror)``: Hartree-Fock with the pairing channel (HartreeFockBDG,
     Superconductivity/hartreefock.jl:5-159) on the device (``lqm_scf_hf_bdg``).  ``h`` and
     ``v`` are the electron-sector Hops (order d), ``rho_init`` the Nambu density matrix
     (order 2d).  Returns (ρ, ϵ_GS, mf, converged, residual)."""
@@ -936,4 +951,4 @@ def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
                                   _ptr(out)))
     rho_out = {L: np.array(rho[:, :, i]) for i, L in enumerate(Lkeys)}
     mf = BdGMFInfo(mu=out[1], eH=out[2], eF=out[3], eP=out[9], eband=out[4], ekin=out[5], iterations=int(out[8]))
-    return HFResult(rho_out, out[0], mf, bool(out[7]), out[6])
+    return _hf_result(rho_out, out, mf, convergenceerror)

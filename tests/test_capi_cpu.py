@@ -86,3 +86,22 @@ def test_empty_kset_matches_oracle_without_a_device(lqm):
     assert eb == eb_ref == 0.0
     for R in rho:
         assert np.array_equal(rho[R], ref[R]) and not rho[R].any()
+
+
+def test_scf_nonconvergence_warns_and_raises(lqm):
+    """An unconverged SCF warns (fixedpoint.jl:189-191) and, with convergenceerror,
+    raises LQM_ENOCONV (selfconsistent.jl:315-317); a converged one does neither.
+    out = lqm_scf_hf's scalars {E_GS, mu, eH, eF, eband, ekin, residual, converged, iterations}."""
+    import warnings
+    import pytest
+    out = [-1.5, 0.1, 0.2, -0.3, -1.0, -0.8, 0.25, 0.0, 3.0]
+    with pytest.warns(UserWarning, match="residual 0.25 after 3"):
+        r = lqm._hf_result({}, out, None, False)
+    assert r.converged is False and r.residual == 0.25 and r[1] == -1.5
+    with pytest.warns(UserWarning), pytest.raises(lqm.LQMError) as err:
+        lqm._hf_result({}, out, None, True)
+    assert err.value.status == -5
+    out[7] = 1.0
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        assert lqm._hf_result({}, out, None, True).converged is True
