@@ -24,6 +24,7 @@ import subprocess
 import sys
 import tempfile
 import time
+import warnings
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_PY = os.path.join(ROOT, "latticeqm.jl_b200", "python")
@@ -413,6 +414,8 @@ def profile_case_kubo(Q, ctx, M):
 
 
 def main():
+    # the SCF timings run a fixed number of iterations (tol = 0): no convergence warnings
+    warnings.filterwarnings("ignore", message="SCF stopped before reaching the tolerance")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
