@@ -63,11 +63,20 @@ mutable struct DeviceHops
     keys::Vector{Vector{Int}}
 end
 
+# Device bytes held by uploaded Hops that no finalizer has released yet.  The
+# routines below upload H per call and leave the buffer to the finalizer; past
+# LIVE_LIMIT a collection runs first, so that the finalizers of unreachable
+# uploads hand their buffers back (to the context's cache) before more are made.
+const LIVE_BYTES = Ref{Int}(0)
+const LIVE_LIMIT = 4 * 2^30
+
 """Upload H in its own key order (the Bloch-sum order of `fouriersum!`)."""
 function upload(ctx::Context, H)
     ks = collect(keys(H))
     d = length(first(ks))
     n = size(H[first(ks)], 1)
+    nbytes = 16 * n * n * length(ks)
+    LIVE_BYTES[] + nbytes > LIVE_LIMIT && GC.gc()
     K = Int64[k[i] for i in 1:d, k in ks]                 # d x nR
     out = Ref{Ptr{Cvoid}}(C_NULL)
     if first(values(H)) isa SparseMatrixCSC
@@ -89,8 +98,12 @@ function upload(ctx::Context, H)
             (Ptr{Cvoid}, Int64, Int64, Int32, Ptr{Int64}, Ptr{ComplexF64}, Ref{Ptr{Cvoid}}),
             ctx.ptr, n, length(ks), d, K, B, out))
     end
+    LIVE_BYTES[] += nbytes
     dh = DeviceHops(out[], ctx, ks)
-    finalizer(h -> ccall((:lqm_hops_free, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), h.ctx.ptr, h.ptr), dh)
+    finalizer(dh) do h
+        LIVE_BYTES[] -= nbytes
+        ccall((:lqm_hops_free, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), h.ctx.ptr, h.ptr)
+    end
     dh
 end
 
