@@ -585,3 +585,24 @@ def test_hard_hermitian_inputs_both_paths(lqm):
                 assert np.max(np.abs(Hk @ Uk - Uk * b[:, 0])) <= 1e-12 * scale, (name, blocked)
         finally:
             c.close()
+
+
+def test_parallelism_pin_filling_and_energy(lqm, ctx):
+    """test/test_parallelism.jl:49-106 on the CUDA path: graphene nearest neighbour,
+    mu = 0, T = 0.05, 12^2 and 8^2 grids: filling tr(rho_0)/2 and band energy equal
+    the oracle's serial k-loop to 1e-10, three runs give identical results, and the
+    band energy is not lost (nonzero)."""
+    h = M.nearestneighbor(L.honeycomb(), -1.0)
+    for nk_lin in (12, 8):
+        ks = L.regulargrid(nk_lin * nk_lin)
+        w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+        ref, eb_ref = K.densitymatrix(h, ks, w, 0.0, 0.05, list(h.keys()))
+        f_ref = np.real(np.trace(ref[(0, 0)])) / 2
+        runs = []
+        for _ in range(3):
+            rho = {R: None for R in h}
+            eb = lqm.getdensitymatrix(rho, h, ks, mu=0.0, T=0.05, ctx=ctx)
+            runs.append((np.real(np.trace(rho[(0, 0)])) / 2, eb))
+        assert runs[0] == runs[1] == runs[2]
+        f, eb = runs[0]
+        assert abs(f - f_ref) <= 1e-10 and abs(eb - eb_ref) <= 1e-10 and eb != 0.0

@@ -558,3 +558,30 @@ def test_wilson_loop_winding_is_the_chern_number():
             en, _ = K.wilson_slices(h, 21, 21, [0], direction)
             d = (np.diff(np.append(en[:, 0], en[0, 0])) + 0.5) % 1.0 - 0.5
             assert abs(d.sum() - sgn * s_dir) < 1e-9
+
+
+def test_chunked_k_reduction_matches_serial():
+    """test/test_parallelism.jl:49-106: getdensitymatrix! on graphene (nearest
+    neighbour, t = -1, 12^2 grid, mu = 0, T = 0.05) gives the same filling
+    tr(rho_0)/2 and band energy whether the k-loop runs serially or as per-task
+    partials folded at the end (atol 1e-10; the 8^2 case must not lose the energy
+    scalar).  Here the partials are k-chunks with the global weights; half filling
+    also follows from the particle-hole symmetry of the bipartite lattice."""
+    h = M.nearestneighbor(L.honeycomb(), -1.0)
+    for nk_lin in (12, 8):
+        ks = L.regulargrid(nk_lin * nk_lin)
+        nk = ks.shape[1]
+        w = np.full(nk, 1.0 / nk)
+        keys = list(h.keys())
+        rho_s, eb_s = K.densitymatrix(h, ks, w, 0.0, 0.05, keys)
+        rho_c = {R: np.zeros_like(rho_s[R]) for R in keys}
+        eb_c = 0.0
+        for chunk in np.array_split(np.arange(nk), 5):
+            r, e = K.densitymatrix(h, ks[:, chunk], w[chunk], 0.0, 0.05, keys)
+            for R in keys:
+                rho_c[R] += r[R]
+            eb_c += e
+        f_s = np.real(np.trace(rho_s[(0, 0)])) / 2
+        f_c = np.real(np.trace(rho_c[(0, 0)])) / 2
+        assert abs(f_c - f_s) <= 1e-10 and abs(eb_c - eb_s) <= 1e-10
+        assert abs(f_s - 0.5) <= 1e-12 and eb_s != 0.0
