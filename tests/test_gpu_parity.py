@@ -263,6 +263,24 @@ def test_hubbard_scf_matches_oracle(lqm, ctx):
     assert abs(res.residual - resid) <= 1e-9
 
 
+def test_scf_sanitizes_a_non_hermitian_initial_guess(lqm, ctx):
+    """Meanfield/selfconsistent.jl:107-113,262-264: a non-Hermitian initial guess is
+    made Hermitian (hermitianize!) before the first iteration; the device SCF and the
+    oracle then agree as for a Hermitian guess."""
+    lat, h, v = M.triangular_hubbard(L_super=2)
+    n = h[(0, 0)].shape[0]
+    rng = np.random.default_rng(11)
+    rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=3) + 0.05 * (rng.normal(size=(n, n))
+                                                                             + 1j * rng.normal(size=(n, n)))}
+    assert not MF.is_hermitian(rho0)
+    ks = L.regulargrid(6 * 6)
+    kw = dict(T=0.02, beta=0.3, tol=0.0, iterations=4)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, **kw)
+    rho_ref, E_ref, hf_ref, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, **kw)
+    assert np.max(np.abs(res.rho[(0, 0)] - rho_ref[(0, 0)])) <= RHO_TOL
+    assert abs(res.energy - E_ref) <= 1e-9 and abs(res.residual - resid) <= 1e-9
+
+
 def test_hubbard_scf_converges_with_log(lqm, ctx):
     lat, h, v = M.triangular_hubbard(L_super=2)
     rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=5)}

@@ -585,3 +585,18 @@ def test_chunked_k_reduction_matches_serial():
         f_c = np.real(np.trace(rho_c[(0, 0)])) / 2
         assert abs(f_c - f_s) <= 1e-10 and abs(eb_c - eb_s) <= 1e-10
         assert abs(f_s - 0.5) <= 1e-12 and eb_s != 0.0
+
+
+def test_hermitianize_pin():
+    """test/test_tightbinding.jl:61-72: an onsite Hermitian block is Hermitian as Hops;
+    a Hops whose R = +-1 blocks are not each other's adjoints is not, and
+    hermitianize! repairs it (the SCF applies this to its initial guess,
+    Meanfield/selfconsistent.jl:107-113,262-264)."""
+    good = {(0, 0): np.array([[1, 1j], [-1j, 2]], complex)}
+    assert MF.is_hermitian(good)
+    bad = {(0, 0): np.array([[0, 1], [0, 0]], complex), (1, 0): np.array([[0, 0], [0, 1]], complex),
+           (-1, 0): np.zeros((2, 2), complex)}
+    assert not MF.is_hermitian(bad)
+    MF.hermitianize(bad)
+    assert MF.is_hermitian(bad)
+    assert np.allclose(bad[(0, 0)], [[0, 0.5], [0.5, 0]]) and np.allclose(bad[(1, 0)], [[0, 0], [0, 0.5]])
