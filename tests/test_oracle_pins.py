@@ -600,3 +600,20 @@ def test_hermitianize_pin():
     MF.hermitianize(bad)
     assert MF.is_hermitian(bad)
     assert np.allclose(bad[(0, 0)], [[0, 0.5], [0.5, 0]]) and np.allclose(bad[(1, 0)], [[0, 0], [0, 0.5]])
+
+
+def test_grid_and_path_shapes():
+    """test/test_structure.jl:76-81,227-240: regulargrid returns the full requested
+    grid (1000 points in 3D, 100 in 2D, first index fastest); kpath returns
+    num_points 2D points; a sample that lands exactly on a tick is taken once."""
+    assert L.regulargrid(1000, dim=3).shape == (3, 1000)
+    g = L.regulargrid(100, dim=2)
+    assert g.shape == (2, 100) and np.allclose(g[:, 1], [0.1, 0.0]) and np.allclose(g[:, 10], [0.0, 0.1])
+    assert L.kpath(L.honeycomb(), 200).shape == (2, 200)
+
+    class _Line:  # three collinear equidistant special points, unit reciprocal basis
+        kdict = ({"a": (0.0, 0.0), "b": (1.0, 0.0), "c": (2.0, 0.0)}, ["a", "b", "c"])
+        B = np.eye(2)
+
+    p = L.kpath(_Line(), 5)
+    assert p.shape == (2, 5) and np.allclose(p[0], [0.0, 0.5, 1.0, 1.5, 2.0]) and np.allclose(p[1], 0.0)
