@@ -230,19 +230,26 @@ def batch_models(seed=2):
     return out
 
 
-def hubbard_v(lat, U=4.0, a=0.5, mode="σx"):
-    """``gethubbard(lat; mode, a, U)`` (Operators/interactions.jl:18-28): onsite key only,
-    V_0 = U * kron(I_sites, sigma_x) for mode=σx."""
+def hubbard_v(lat, U=4.0, a=0.5, mode="σx", neighbors=((0, 0),)):
+    """``gethubbard(lat, neighbors; mode, a, U)`` (Operators/interactions.jl:8,18-28):
+    for each cell offset dL in ``neighbors`` the block V_dL[i, j] = U * heaviside(a - r),
+    r = |r_i + A dL - r_j| (heaviside(0) = 1/2), then spin added in ``mode`` (σx: the
+    kron with sigma_x)."""
     N = lat.norb
-    V = np.zeros((N, N), complex)
     pos = lat.allpositions()
-    for i in range(N):
-        for j in range(N):
-            r = float(np.linalg.norm(pos[:3, i] - pos[:3, j]))
-            v = U * (0.0 if a - r < 0 else (1.0 if a - r > 0 else 0.5))
-            if abs(v) >= SQRT_EPS:
-                V[i, j] = v
-    return addspin({(0, 0): V}, mode)
+    out = {}
+    for dL in neighbors:
+        dL = tuple(int(x) for x in dL)
+        shift = lat.A @ np.array(dL, float)
+        V = np.zeros((N, N), complex)
+        for i in range(N):
+            for j in range(N):
+                r = float(np.linalg.norm(pos[:3, i] + shift - pos[:3, j]))
+                v = U * (0.0 if a - r < 0 else (1.0 if a - r > 0 else 0.5))
+                if abs(v) >= SQRT_EPS:
+                    V[i, j] = v
+        out[dL] = V
+    return addspin(out, mode)
 
 
 def triangular_hubbard(L_super=6, t=-1.0, tp=0.2, U=4.0):

@@ -617,3 +617,27 @@ def test_grid_and_path_shapes():
 
     p = L.kpath(_Line(), 5)
     assert p.shape == (2, 5) and np.allclose(p[0], [0.0, 0.5, 1.0, 1.5, 2.0]) and np.allclose(p[1], 0.0)
+
+
+def test_interaction_range_beyond_hopping_range():
+    """test/test_meanfield.jl:256-278: an interaction reaching farther than the
+    hopping (onsite-only staggered h, gethubbard on 9 neighbour cells with a = 1.8,
+    U = 2, mode sigma_x): the mean field gets blocks for keys(v) outside keys(h)
+    (hartreefock.jl:191-205), its energies are finite, hMF is Hermitian as Hops, and
+    the variational identity holds to 1e-10 on a 3 x 3 grid."""
+    lat = L.honeycomb()
+    h = {(0, 0): np.diag([0.3, 0.3, -0.3, -0.3]).astype(complex)}
+    nbrs = [(0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (1, 1), (-1, -1), (1, -1), (-1, 1)]
+    v = M.hubbard_v(lat, U=2.0, a=1.8, neighbors=nbrs)
+    assert not set(v) <= set(h)
+    rho = {R: np.zeros((4, 4), complex) for R in v}
+    rho[(0, 0)] = M.antiferro_density(lat)
+    hf = MF.HartreeFock(h, v)(rho)
+    assert np.isfinite(hf.eH) and np.isfinite(hf.eF)
+    assert set(hf.hMF) == set(h) | set(v) and MF.is_hermitian(hf.hMF)
+    ks = np.array([[i / 3, j / 3] for j in range(3) for i in range(3)]).T
+
+    def trprod(A, B):
+        return sum(np.real(np.trace(K.fouriersum(A, k) @ K.fouriersum(B, k))) for k in ks.T) / ks.shape[1]
+
+    assert abs(trprod(hf.hMF, rho) - trprod(h, rho) - 2 * (hf.eH + hf.eF)) < 1e-10
