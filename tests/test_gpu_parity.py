@@ -624,3 +624,22 @@ def test_parallelism_pin_filling_and_energy(lqm, ctx):
         assert runs[0] == runs[1] == runs[2]
         f, eb = runs[0]
         assert abs(f - f_ref) <= 1e-10 and abs(eb - eb_ref) <= 1e-10 and eb != 0.0
+
+
+def test_scf_interaction_range_beyond_hopping_range(lqm, ctx):
+    """test/test_meanfield.jl:256-278 through the device SCF: onsite-only h, a Hubbard
+    interaction on 9 neighbour cells (a = 1.8), antiferromagnetic start; 3 iterations
+    match the oracle's (the mean field carries the keys of v that h lacks)."""
+    lat = L.honeycomb()
+    h = {(0, 0): np.diag([0.3, 0.3, -0.3, -0.3]).astype(complex)}
+    nbrs = [(0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (1, 1), (-1, -1), (1, -1), (-1, 1)]
+    v = M.hubbard_v(lat, U=2.0, a=1.8, neighbors=nbrs)
+    rho0 = {R: np.zeros((4, 4), complex) for R in v}
+    rho0[(0, 0)] = M.antiferro_density(lat)
+    ks = L.regulargrid(6 * 6)
+    kw = dict(T=0.05, beta=0.3, tol=0.0, iterations=3)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, **kw)
+    rho_ref, E_ref, hf_ref, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, **kw)
+    for R in rho_ref:
+        assert np.max(np.abs(res.rho[R] - rho_ref[R])) <= RHO_TOL, R
+    assert abs(res.energy - E_ref) <= 1e-9 and abs(res.residual - resid) <= 1e-9
