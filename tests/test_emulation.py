@@ -247,3 +247,22 @@ def test_emulated_eigh_hard_hermitian(emul, name, Hk):
     assert np.max(np.abs(ev - ref)) <= 1e-12 * scale
     assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12
     assert np.max(np.abs(Hk @ U - U * ev)) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("name,Hk", _hard_hermitian(), ids=lambda x: x if isinstance(x, str) else "")
+def test_emulated_blocked_eigh_hard_hermitian(emul, name, Hk):
+    """The same hard inputs through the large-n path's code (panel reduction with
+    panels of 8, tiled merge updates from 8 rows, compact-WY back-transformation)."""
+    keys, blocks = pack({(0, 0): Hk})
+    n = Hk.shape[0]
+    kp = np.zeros(2)
+    ev = np.zeros(n)
+    U = np.zeros((n, n), complex, order="F")
+    emul.lqm_emul_eigh_blocked(n, 1, 2, blocks.ctypes.data_as(P), keys.ctypes.data_as(P), kp.ctypes.data_as(P),
+                               8, 8, 1, ev.ctypes.data_as(P), U.ctypes.data_as(P))
+    ref = K.eigh_upper(Hk, vectors=False)
+    scale = max(np.max(np.abs(ref)), np.finfo(float).tiny)
+    assert np.all(np.isfinite(U))
+    assert np.max(np.abs(ev - ref)) <= 1e-12 * scale
+    assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12
+    assert np.max(np.abs(Hk @ U - U * ev)) <= 1e-12 * scale
