@@ -16,6 +16,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kspace.h"
 #include "lqm_kernels.cuh"
 #include "lqm_large.cuh"
@@ -130,6 +132,16 @@ int guarded(lqm_ctx* ctx, F&& f) {
     return LQM_EINVAL;
   }
 }
+
+// A named NVTX range for the lifetime of a scope, so that the stages of a call
+// (eigen pass, fold, DOS, SCF iteration) show on a profiler's timeline.  NVTX
+// calls do nothing unless a profiling tool is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 void collect_stats(lqm_ctx* ctx) {
   for (auto& pr : ctx->ev_pending) {
@@ -326,6 +338,7 @@ bool use_blocked(const lqm_ctx* ctx, int n, int nR);
 // GEMMs.  k-points are processed in batches sized to ~24 GB of work buffers.
 void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands,
                        double2* d_U, double2* rhok, double* ebk, const double* w, double mu, double T) {
+  NvtxRange nvtx_("eigen pass (blocked)");
   const int n = (int)H->n;
   const int nb = kBlkNB;
   const int P = (n + nb - 1) / nb;
@@ -457,6 +470,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
 // Eigen pass over nk device k-points: bands (n x nk), optionally U and/or rho_k.
 void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands, double2* d_U,
                  const RhoOut* ro = nullptr) {
+  NvtxRange nvtx_("eigen pass");
   const int n = (int)H->n;
   if (use_blocked(ctx, n, (int)H->nR)) {
     launch_eigh_large(ctx, H, nk, d_ks, d_bands, d_U, ro ? ro->rhok : nullptr, ro ? ro->ebk : nullptr,
@@ -525,6 +539,7 @@ int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
 // deterministic for a given batch size.
 void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const double2* coef, int nL,
                  double2* d_rho, int accumulate) {
+  NvtxRange nvtx_("rho fold");
   zgemm_sb(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_T, (int)nn, nL, (int)nb, 1.0, rk, (int)nn, 0, coef, nL, 0,
            accumulate ? 1.0 : 0.0, d_rho, (int)nn, 0, 1);
 }
@@ -533,6 +548,7 @@ void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const 
 void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w, double mu,
                  double T, int64_t nL, const int64_t* d_Lkeys, double2* d_rho, double* d_eb,
                  double* bands_out = nullptr) {
+  NvtxRange nvtx_("density matrix");
   const int n = (int)H->n;
   const int64_t nn = (int64_t)n * n;
   // rho_k batch: 4 GB, or one k-point per SM for large n (the blocked path
@@ -622,6 +638,7 @@ double chempot_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, c
 
 void dos_dev(lqm_ctx* ctx, int64_t n, int64_t nk, const double* d_bands, const double* d_w, int64_t nw,
              const double* d_om, double gamma, double* d_dos) {
+  NvtxRange nvtx_("dos");
   const int64_t nv = n * nk;
   const int64_t nbk = std::max<int64_t>(1, std::min<int64_t>((nv + 1023) / 1024, (int64_t)ctx->num_sms * 2));
   const int64_t chunk = (nv + nbk - 1) / nbk;
