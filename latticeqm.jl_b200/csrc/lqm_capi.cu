@@ -997,6 +997,7 @@ int lqm_bandmatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks
     timer_start(ctx);
     launch_eigh(ctx, H, nk, dks, db, (double2*)dU);
     timer_stop(ctx);
+    wait_stream(ctx);  // poll with the context's limit: a copy into pageable host memory would block unbounded
     ck(cudaMemcpyAsync(bands, db, (size_t)(n * nk) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
     if (want_vectors)
       ck(cudaMemcpyAsync(U, dU, (size_t)(n * n * nk) * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
@@ -1020,6 +1021,7 @@ int lqm_densitymatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
     density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb);
     timer_stop(ctx);
     double eb = 0.0;
+    wait_stream(ctx);  // poll with the context's limit: a copy into pageable host memory would block unbounded
     ck(cudaMemcpyAsync(&eb, d_eb, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
     wait_stream(ctx);
     timer_collect(ctx);
@@ -1126,6 +1128,7 @@ int lqm_bands_dos_rho_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
     dos_dev(ctx, H->n, nk, d_bands, d_w, nw, d_omegas, gamma, d_dos);
     timer_stop(ctx);
     double eb = 0.0;
+    wait_stream(ctx);  // poll with the context's limit: a copy into pageable host memory would block unbounded
     ck(cudaMemcpyAsync(&eb, d_eb, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
     wait_stream(ctx);
     timer_collect(ctx);

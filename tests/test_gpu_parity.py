@@ -643,3 +643,35 @@ def test_scf_interaction_range_beyond_hopping_range(lqm, ctx):
     for R in rho_ref:
         assert np.max(np.abs(res.rho[R] - rho_ref[R])) <= RHO_TOL, R
     assert abs(res.energy - E_ref) <= 1e-9 and abs(res.residual - resid) <= 1e-9
+
+
+def test_host_wait_limit_reports_timeout_and_context_recovers(lqm):
+    """Failure handling without a GPU fault: the host waits for device work by
+    polling with a per-context limit (lqm_ctx_set_timeout).  A limit far below the
+    work's duration ends the call with LQM_ETIMEOUT while the kernel runs to
+    completion on its own; with the limit restored, the same context serves the
+    next call correctly.  (Device-pointer entry point: its only wait is the poll.)"""
+    import torch
+    c = lqm.Context(0, timeout=600)
+    try:
+        dev = torch.device("cuda", 0)
+        h = M.batch_models()[2][1]  # n = 96: 8192 k-points are tens of ms of device work
+        ks = np.random.default_rng(2).random((2, 8192))
+        Hd = lqm.DeviceHops(h, c)
+        d_ks = torch.from_numpy(np.ascontiguousarray(ks.T)).to(dev)
+        d_b = torch.zeros(ks.shape[1], Hd.n, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()  # the library runs on its own stream: inputs complete first
+
+        def call():
+            return lqm.lib().lqm_bandmatrix_dev(c.handle, Hd.handle, ks.shape[1], lqm._ptr(d_ks), 0, 0,
+                                                lqm._ptr(d_b), None)
+        c.check(call())  # plans and workspaces exist before the limit is lowered
+        c.check(lqm.lib().lqm_ctx_set_timeout(c.handle, 1e-6))
+        assert call() == -4
+        c.check(lqm.lib().lqm_ctx_set_timeout(c.handle, 600.0))
+        c.check(call())  # queued behind the first kernel on the context's stream; rewrites every band
+        b = d_b.cpu().numpy().T
+        assert rel_band_err(b[:, :64], oracle_bands(h, ks[:, :64])) <= BAND_TOL
+        Hd.free()
+    finally:
+        c.close()
