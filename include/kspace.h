@@ -47,7 +47,12 @@ typedef int (*lqm_scf_log_cb)(int64_t iter, double energy, double residual, doub
 int lqm_ctx_create(int device, lqm_ctx** out);
 int lqm_ctx_destroy(lqm_ctx* ctx);
 const char* lqm_last_error(const lqm_ctx* ctx);
-/* Host-side wait limit for device work, seconds (default 600). */
+/* Host-side wait limit for device work, seconds (default 600): a call whose
+ * device work runs longer returns LQM_ETIMEOUT (the work itself finishes on the
+ * context's stream and later calls queue behind it).  lqm_bandmatrix[_dev],
+ * lqm_densitymatrix[_dev] and lqm_bands_dos_rho[_dev] apply it before their
+ * copies into caller memory; other entry points copy first, and a copy into
+ * pageable memory waits for the device work without a limit. */
 int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
 /* Eigensolver path selection: orders n >= n_min use the batched blocked path
  * (panel reduction + batched GEMMs); 0 (default) selects it from n = 128 on.
