@@ -52,7 +52,12 @@ const char* lqm_last_error(const lqm_ctx* ctx);
  * context's stream and later calls queue behind it).  lqm_bandmatrix[_dev],
  * lqm_densitymatrix[_dev] and lqm_bands_dos_rho[_dev] apply it before their
  * copies into caller memory; other entry points copy first, and a copy into
- * pageable memory waits for the device work without a limit. */
+ * pageable memory waits for the device work without a limit.
+ * After LQM_ETIMEOUT, copies into the caller's output buffers may still be queued
+ * on the context's stream (at once for page-locked buffers): those buffers may
+ * still be written until the stream drains.  They are safe to reuse or free once
+ * a later call on the same context has returned LQM_OK (its work queues behind
+ * the earlier copies) or after lqm_ctx_destroy. */
 int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
 /* Eigensolver path selection: orders n >= n_min use the batched blocked path
  * (panel reduction + batched GEMMs); 0 (default) selects it from n = 128 on.
@@ -126,11 +131,22 @@ int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles /* [16] */);
  * key order.  The key order is the Bloch-sum order (types.jl:18-25). */
 int lqm_hops_upload_dense(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
                           const double* blocks, lqm_hops** out);
-/* Upload a SparseHops (types.jl:60): per key a Julia SparseMatrixCSC with
- * 1-based Int64 colptr (n+1) / rowval (nnz) and ComplexF64 nzval (2*nnz doubles). */
+/* Upload a SparseHops (types.jl:60; the form `autoconversion` gives every Hops
+ * with n > MAX_DENSE = 500, types.jl:102-103,272): per key a Julia
+ * SparseMatrixCSC with 1-based Int64 colptr (n+1), rowval and ComplexF64 nzval.
+ * nnz[r] is the length of rowval[r] (nzval[r] holds 2*nnz[r] doubles), i.e.
+ * Julia's length(m.rowval); the call reads only the colptr[r][n]-1 entries that
+ * colptr addresses and rejects a colptr that does not start at 1, decreases, or
+ * ends beyond nnz[r], rows outside 1..n and non-finite values (LQM_EINVAL).
+ * Only the stored entries are copied to the device; the dense blocks are built
+ * there (repeated entries are summed in storage order). */
 int lqm_hops_upload_csc(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
                         const int64_t* const* colptr, const int64_t* const* rowval,
-                        const double* const* nzval, lqm_hops** out);
+                        const double* const* nzval, const int64_t* nnz, lqm_hops** out);
+/* Release a Hops.  With a context, first waits (within the context's limit) for
+ * the work queued on its stream, which may still read the blocks; on LQM_ETIMEOUT
+ * nothing is released and h stays valid, to be freed by a later call.  With
+ * ctx == NULL the buffer is freed directly (cudaFree waits for the device). */
 int lqm_hops_free(lqm_ctx* ctx, lqm_hops* h);
 int lqm_hops_dims(const lqm_hops* h, int64_t* n, int64_t* nR, int32_t* d);
 

@@ -225,9 +225,9 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC
 };
-static_assert(WS_BDGB < 40, "workspace slots");
+static_assert(WS_CSC < 40, "workspace slots");
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
 const DCPlan& get_plan(lqm_ctx* ctx, int n) {
@@ -897,39 +897,111 @@ int lqm_hops_upload_dense(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const 
 
 int lqm_hops_upload_csc(lqm_ctx* ctx, int64_t n, int64_t nR, int32_t d, const int64_t* keys,
                         const int64_t* const* colptr, const int64_t* const* rowval, const double* const* nzval,
-                        lqm_hops** out) {
+                        const int64_t* nnz, lqm_hops** out) {
   return guarded(ctx, [&] {
-    if (!out || !colptr || !rowval || !nzval) fail(LQM_EINVAL, "null argument");
-    if (n < 1 || nR < 1) fail(LQM_EINVAL, "invalid sizes");
-    std::vector<double> dense((size_t)(2 * n * n * nR), 0.0);
+    if (!out) fail(LQM_EINVAL, "null output pointer");
+    *out = nullptr;
+    if (!colptr || !rowval || !nzval || !nnz || !keys) fail(LQM_EINVAL, "null argument");
+    if (n < 1 || nR < 1 || d < 1 || d > 3) fail(LQM_EINVAL, "invalid sizes n=%lld nR=%lld d=%d", (long long)n, (long long)nR, d);
+    if (n > 4096) fail(LQM_EINVAL, "n=%lld exceeds the supported maximum 4096", (long long)n);
+    // Host validation of every block before anything reaches the device: colptr is
+    // 1-based and non-decreasing, its last entry stays within the caller's nnz[r]
+    // (the lengths of rowval[r] and nzval[r]/2), rows lie in 1..n, values are finite.
+    std::vector<int64_t> used((size_t)nR);
+    size_t stage = 0;
     for (int64_t r = 0; r < nR; ++r) {
       const int64_t* cp = colptr[r];
-      for (int64_t j = 0; j < n; ++j) {
-        if (cp[j] < 1 || cp[j + 1] < cp[j]) fail(LQM_EINVAL, "invalid colptr in block %lld", (long long)r);
-        for (int64_t p = cp[j] - 1; p < cp[j + 1] - 1; ++p) {
-          const int64_t i = rowval[r][p] - 1;
-          if (i < 0 || i >= n) fail(LQM_EINVAL, "row index out of range in block %lld", (long long)r);
-          double* dst = &dense[(size_t)(2 * (r * n * n + i + j * n))];
-          dst[0] += nzval[r][2 * p];
-          dst[1] += nzval[r][2 * p + 1];
-        }
-      }
+      if (!cp || nnz[r] < 0) fail(LQM_EINVAL, "invalid colptr or nnz in block %lld", (long long)r);
+      if (cp[0] != 1) fail(LQM_EINVAL, "colptr of block %lld does not start at 1", (long long)r);
+      for (int64_t j = 0; j < n; ++j)
+        if (cp[j + 1] < cp[j]) fail(LQM_EINVAL, "colptr of block %lld decreases at column %lld", (long long)r, (long long)j);
+      const int64_t m = cp[n] - 1;
+      if (m > nnz[r])
+        fail(LQM_EINVAL, "block %lld: colptr ends at %lld entries, beyond its nnz %lld", (long long)r, (long long)m,
+             (long long)nnz[r]);
+      if (m > 0 && (!rowval[r] || !nzval[r])) fail(LQM_EINVAL, "null rowval or nzval in block %lld", (long long)r);
+      for (int64_t p = 0; p < m; ++p)
+        if (rowval[r][p] < 1 || rowval[r][p] > n)
+          fail(LQM_EINVAL, "row index out of range in block %lld", (long long)r);
+      if (m > 0) check_finite(nzval[r], 2 * m, "nzval");
+      used[(size_t)r] = m;
+      stage += (size_t)(n + 1 + m) * sizeof(int64_t) + (size_t)m * sizeof(double2);
     }
-    int st = lqm_hops_upload_dense(ctx, n, nR, d, keys, dense.data(), out);
-    if (st != LQM_OK) fail(st, "%s", ctx->err.c_str());
+    const size_t bb = (size_t)(n * n * nR) * sizeof(double2);
+    const size_t koff = (bb + 255) / 256 * 256;
+    const size_t need = koff + (size_t)(d * nR) * sizeof(int64_t);
+    size_t got = 0;
+    void* buf = hops_buffer_take(ctx, need, &got);
+    if (!buf) {
+      if (cudaMalloc(&buf, need) != cudaSuccess) {
+        cudaGetLastError();
+        fail(LQM_ENOMEM, "device allocation for hops failed");
+      }
+      got = need;
+    }
+    lqm_hops* h = new lqm_hops();
+    h->n = n; h->nR = nR; h->d = d;
+    h->hkeys.assign(keys, keys + d * nR);
+    h->blocks = (double2*)buf;
+    h->keys = (int64_t*)((char*)buf + koff);
+    h->device = ctx->device;
+    h->buf_bytes = got;
+    try {
+      // Only the stored entries cross PCIe (about a tenth of the dense bytes for the
+      // twisted bilayers); the blocks are zeroed and filled on the device.
+      char* st = (char*)ws_get(ctx, WS_CSC, stage + 256 * (size_t)(3 * nR + 1));
+      ck(cudaMemsetAsync(h->blocks, 0, bb, ctx->stream), "hops memset");
+      ck(cudaMemcpyAsync(h->keys, keys, (size_t)(d * nR) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream),
+         "keys upload");
+      size_t off = 0;
+      auto place = [&](size_t bytes) { char* p = st + off; off = (off + bytes + 255) / 256 * 256; return p; };
+      for (int64_t r = 0; r < nR; ++r) {
+        const int64_t m = used[(size_t)r];
+        int64_t* dcp = (int64_t*)place((size_t)(n + 1) * sizeof(int64_t));
+        int64_t* drv = (int64_t*)place((size_t)m * sizeof(int64_t));
+        double2* dnz = (double2*)place((size_t)m * sizeof(double2));
+        ck(cudaMemcpyAsync(dcp, colptr[r], (size_t)(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream),
+           "colptr upload");
+        if (m > 0) {
+          ck(cudaMemcpyAsync(drv, rowval[r], (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream),
+             "rowval upload");
+          ck(cudaMemcpyAsync(dnz, nzval[r], (size_t)m * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream),
+             "nzval upload");
+        }
+        csc_scatter_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(n, dcp, drv, dnz,
+                                                                               h->blocks + r * n * n);
+        ctx->launches += 1;
+      }
+      ck(cudaGetLastError(), "csc scatter launch");
+      wait_stream(ctx);
+    } catch (const LqmError& e) {  // neither the buffer nor the handle outlives a failed upload
+      if (e.code != LQM_ETIMEOUT) cudaFree(buf);
+      delete h;
+      throw;
+    }
+    *out = h;
   });
 }
 
 int lqm_hops_free(lqm_ctx* ctx, lqm_hops* h) {
   if (!h) return LQM_EINVAL;
-  if (ctx) { cudaSetDevice(ctx->device); cudaStreamSynchronize(ctx->stream); }
-  if (!(ctx && ctx->device == h->device && hops_buffer_keep(ctx, h->blocks, h->buf_bytes))) {
+  if (!ctx) {  // no context: cudaFree itself waits for the device's work
     if (h->device >= 0) cudaSetDevice(h->device);
     cudaFree(h->blocks);
-    if (ctx) cudaSetDevice(ctx->device);
+    delete h;
+    return LQM_OK;
   }
-  delete h;
-  return LQM_OK;
+  return guarded(ctx, [&] {
+    // Kernels queued on the context may still read the blocks: wait for them with the
+    // context's limit.  On LQM_ETIMEOUT nothing is released and h stays valid.
+    wait_stream(ctx);
+    if (!(ctx->device == h->device && hops_buffer_keep(ctx, h->blocks, h->buf_bytes))) {
+      if (h->device >= 0) cudaSetDevice(h->device);
+      cudaFree(h->blocks);
+      cudaSetDevice(ctx->device);
+    }
+    delete h;
+  });
 }
 
 int lqm_hops_dims(const lqm_hops* h, int64_t* n, int64_t* nR, int32_t* d) {

@@ -273,6 +273,25 @@ __global__ void fold_coef_kernel(int64_t nb, int dim, const double* __restrict__
   }
 }
 
+// SparseHops upload (SparseMatrixCSC blocks, 1-based, validated on the host): one
+// thread per column adds its stored entries into the zeroed dense block in storage
+// order, so repeated (row, column) entries sum in the same order as a host loop.
+__global__ void __launch_bounds__(128) csc_scatter_kernel(int64_t n, const int64_t* __restrict__ colptr,
+                                                          const int64_t* __restrict__ rowval,
+                                                          const double2* __restrict__ nzval, double2* block) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double2* col = block + j * n;
+  for (int64_t p = colptr[j] - 1; p < colptr[j + 1] - 1; ++p) {
+    const int64_t i = rowval[p] - 1;
+    const double2 v = nzval[p];
+    double2 c = col[i];
+    c.x += v.x;
+    c.y += v.y;
+    col[i] = c;
+  }
+}
+
 // Fixed-order sum of x[0..m) into out[0] (single CTA).
 __global__ void ordered_sum_kernel(const double* __restrict__ x, int64_t m, double* out, int accumulate) {
   __shared__ double red[32];

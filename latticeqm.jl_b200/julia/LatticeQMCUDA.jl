@@ -12,8 +12,7 @@ Usage:
     LatticeQMCUDA.enable!()              # adds :cuda to Parallel.to_executor
     bands = getbands(h, ks; multimode=:cuda)
 
-`enable!` installs the executor; the routine-level hooks listed in INTEGRATION.md
-(a few lines in LatticeQM's `bandmatrix`, `densitymatrix_compute_add!`,
+`enable!` installs the executor; routine-level hooks (a few lines in LatticeQM's `bandmatrix`, `densitymatrix_compute_add!`,
 `dos_compute!` and `solveselfconsistent!`) call the `cuda_*` functions below when
 the executor is a `CudaExec`.
 """
@@ -84,10 +83,11 @@ function upload(ctx::Context, H)
         colptr = [Ptr{Int64}(pointer(m.colptr)) for m in mats]
         rowval = [Ptr{Int64}(pointer(m.rowval)) for m in mats]
         nzval = [Ptr{Float64}(pointer(m.nzval)) for m in mats]
+        nnz = Int64[min(length(m.rowval), length(m.nzval)) for m in mats]
         GC.@preserve mats colptr rowval nzval begin
             check(ctx, ccall((:lqm_hops_upload_csc, LIB[]), Cint,
                 (Ptr{Cvoid}, Int64, Int64, Int32, Ptr{Int64}, Ptr{Ptr{Int64}}, Ptr{Ptr{Int64}}, Ptr{Ptr{Float64}},
-                 Ref{Ptr{Cvoid}}), ctx.ptr, n, length(ks), d, K, colptr, rowval, nzval, out))
+                 Ptr{Int64}, Ref{Ptr{Cvoid}}), ctx.ptr, n, length(ks), d, K, colptr, rowval, nzval, nnz, out))
         end
     else
         B = Array{ComplexF64}(undef, n, n, length(ks))

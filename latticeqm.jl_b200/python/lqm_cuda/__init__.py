@@ -29,6 +29,7 @@ LIB_PATH = os.environ.get(
     "LQM_KSPACE_LIB", os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libkspace.so")))
 
 LQM_OK = 0
+LQM_ETIMEOUT = -4
 STATUS_NAMES = {-1: "LQM_EINVAL", -2: "LQM_ECUDA", -3: "LQM_ENOMEM", -4: "LQM_ETIMEOUT",
                 -5: "LQM_ENOCONV", -6: "LQM_EDEVICE"}
 
@@ -71,7 +72,7 @@ _SIG = {
     "lqm_ctx_set_blocked_min_n": [_P, _I64],
     "lqm_ctx_last_kernel_ms": [_P, ctypes.POINTER(_D)],
     "lqm_hops_upload_dense": [_P, _I64, _I64, ctypes.c_int32, _P, _P, ctypes.POINTER(_P)],
-    "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, ctypes.POINTER(_P)],
+    "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.POINTER(_P)],
     "lqm_hops_free": [_P, _P],
     "lqm_hops_dims": [_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), ctypes.POINTER(ctypes.c_int32)],
     "lqm_bloch": [_P, _P, _I64, _P, _P],
@@ -235,17 +236,53 @@ def pack_hops(h):
     return n, len(keys), d, K, B
 
 
+def _is_sparse(m):
+    return hasattr(m, "tocsc") and hasattr(m, "nnz")
+
+
+def pack_hops_csc(h):
+    """dict Hops of sparse (or dense) blocks -> (n, nR, d, keys d x nR int64 (F), per key
+    the SparseMatrixCSC arrays as Julia holds them: 1-based int64 colptr and rowval,
+    complex128 nzval)."""
+    import scipy.sparse as sp
+    keys = list(h.keys())
+    d = len(keys[0])
+    K = np.asfortranarray(np.array(keys, dtype=np.int64).T)
+    cols = []
+    n = None
+    for R in keys:
+        m = h[R]
+        c = m.tocsc() if _is_sparse(m) else sp.csc_matrix(np.asarray(m))
+        n = c.shape[0]
+        cols.append((np.ascontiguousarray(c.indptr, dtype=np.int64) + 1,
+                     np.ascontiguousarray(c.indices, dtype=np.int64) + 1,
+                     np.ascontiguousarray(c.data, dtype=np.complex128)))
+    return n, len(keys), d, K, cols
+
+
 class DeviceHops:
     """A Hops resident on the device (``lqm_hops``)."""
 
     def __init__(self, h, ctx=None):
         self.ctx = ctx or default_context()
-        n, nR, d, K, B = pack_hops(h)
-        self.n, self.nR, self.d = n, nR, d
         self.keys = [tuple(R) for R in h.keys()]
         out = _P()
-        self.ctx.check(_lib.lqm_hops_upload_dense(self.ctx.handle, n, nR, d, _ptr(K), _ptr(B),
-                                                  ctypes.byref(out)))
+        if any(_is_sparse(m) for m in h.values()):
+            n, nR, d, K, cols = pack_hops_csc(h)
+            self.n, self.nR, self.d = n, nR, d
+            arr = ctypes.c_void_p * nR
+            cp = arr(*[c.ctypes.data for c, _, _ in cols])
+            rv = arr(*[r.ctypes.data for _, r, _ in cols])
+            nz = arr(*[v.ctypes.data for _, _, v in cols])
+            nnz = np.array([r.size for _, r, _ in cols], dtype=np.int64)
+            self.ctx.check(_lib.lqm_hops_upload_csc(self.ctx.handle, n, nR, d, _ptr(K), ctypes.cast(cp, _P),
+                                                    ctypes.cast(rv, _P), ctypes.cast(nz, _P), _ptr(nnz),
+                                                    ctypes.byref(out)))
+        else:
+            n, nR, d, K, B = pack_hops(h)
+            self.n, self.nR, self.d = n, nR, d
+            self.ctx.check(_lib.lqm_hops_upload_dense(self.ctx.handle, n, nR, d, _ptr(K), _ptr(B),
+                                                      ctypes.byref(out)))
         self._h = out
 
     @property
@@ -254,7 +291,9 @@ class DeviceHops:
 
     def free(self):
         if getattr(self, "_h", None):
-            _lib.lqm_hops_free(self.ctx.handle, self._h)
+            st = _lib.lqm_hops_free(self.ctx.handle, self._h)
+            if st == LQM_ETIMEOUT:  # device work still reads the blocks: the handle stays valid
+                self.ctx.check(st)
             self._h = None
 
     def __del__(self):

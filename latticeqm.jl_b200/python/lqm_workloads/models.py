@@ -233,7 +233,10 @@ def batch_models(seed=2):
 def hubbard_v(lat, U=4.0, a=0.5, mode="σx", neighbors=((0, 0),)):
     """``gethubbard(lat, neighbors; mode, a, U)`` (Operators/interactions.jl:8,18-28):
     for each cell offset dL in ``neighbors`` the block V_dL[i, j] = U * heaviside(a - r),
-    r = |r_i + A dL - r_j| (heaviside(0) = 1/2), then spin added in ``mode`` (σx: the
+    r = |r_i + A dL - r_j| (heaviside(0) = 1/2), and for dL != 0 its Hermitian partner
+    V_{-dL} = V_dL^H (Operators/gethops.jl:96-109, ``hops[-δL] = hops[δL]'``, so a
+    one-sided neighbour list still gives a Hermitian V); all-zero blocks are dropped
+    (``trim!``, TightBinding/types.jl:278-285); then spin added in ``mode`` (σx: the
     kron with sigma_x)."""
     N = lat.norb
     pos = lat.allpositions()
@@ -249,6 +252,9 @@ def hubbard_v(lat, U=4.0, a=0.5, mode="σx", neighbors=((0, 0),)):
                 if abs(v) >= SQRT_EPS:
                     V[i, j] = v
         out[dL] = V
+        if any(x != 0 for x in dL):
+            out[tuple(-x for x in dL)] = V.conj().T.copy()
+    out = {dL: V for dL, V in out.items() if np.any(V != 0)}
     return addspin(out, mode)
 
 

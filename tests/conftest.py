@@ -1,6 +1,11 @@
 import os
 import sys
 
+# The oracle makes many small LAPACK calls (n <= 144 per k-point); a multi-threaded
+# BLAS spends most of their time synchronising its threads (84 s against 2.6 s for
+# one SCF iteration of the n = 72, 36 x 36 model on 8 cores), so it runs on one.
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -1,7 +1,7 @@
 """Extract the twisted-bilayer eigenvalue pins from the reference's own test file.
 
-Reads LatticeQM.jl's ``test/test_tbg.jl`` (path given as argument, default
-/root/reference/test/test_tbg.jl) and writes ``reference_pins.json`` beside this
+Reads LatticeQM.jl's ``test/test_tbg.jl`` (its path is the required argument,
+``python extract_reference_pins.py <LatticeQM.jl checkout>/test/test_tbg.jl``) and writes ``reference_pins.json`` beside this
 script: for every ``@test isapprox(ev[...], value; atol=...)`` line in the
 spectrum fixtures, the lattice, the k-point, the 1-based index expression, the
 value, the tolerance and the source line.  Run once where the reference is
@@ -43,4 +43,6 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/test/test_tbg.jl")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python extract_reference_pins.py <path to LatticeQM.jl>/test/test_tbg.jl")
+    main(sys.argv[1])

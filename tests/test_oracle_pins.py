@@ -641,3 +641,19 @@ def test_interaction_range_beyond_hopping_range():
         return sum(np.real(np.trace(K.fouriersum(A, k) @ K.fouriersum(B, k))) for k in ks.T) / ks.shape[1]
 
     assert abs(trprod(hf.hMF, rho) - trprod(h, rho) - 2 * (hf.eH + hf.eF)) < 1e-10
+
+
+def test_hubbard_one_sided_neighbors_get_hermitian_partners():
+    """gethops' hops! (Operators/gethops.jl:96-109) sets hops[-δL] = hops[δL]' for every
+    nonzero δL and trim! drops all-zero blocks (TightBinding/types.jl:278-285): a
+    one-sided neighbour list gives the same Hermitian V as the two-sided one."""
+    lat = L.honeycomb()
+    one = M.hubbard_v(lat, U=2.0, a=1.8, neighbors=[(0, 0), (1, 0)])
+    two = M.hubbard_v(lat, U=2.0, a=1.8, neighbors=[(0, 0), (1, 0), (-1, 0)])
+    assert set(one) == {(0, 0), (1, 0), (-1, 0)} == set(two)
+    for R in one:
+        assert np.array_equal(one[R], two[R])
+        mR = tuple(-x for x in R)
+        assert np.array_equal(one[mR], one[R].conj().T)
+    far = M.hubbard_v(lat, U=2.0, a=0.5, neighbors=[(0, 0), (3, 0)])  # no pair within a = 0.5 at 3 cells
+    assert set(far) == {(0, 0)}

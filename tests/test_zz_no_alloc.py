@@ -6,7 +6,8 @@ CUDA.jl pool or a framework's caching allocator, or a latency-sensitive loop
 that cannot afford cudaMalloc's device-wide synchronisation).  It takes only
 caller-owned device buffers and uses a fixed device array inside the library
 for scratch.  This test owns the buffers (torch allocations on the test side),
-calls the entry point twice in a row through the C-ABI, and compares both
+calls the entry point twice in a row through the C-ABI, checks that the second
+call leaves the device's free memory unchanged, and compares both
 results with ``lqm_bandmatrix_dev`` at the band tolerance used elsewhere
 (1e-10 of the spectral width) and the eigenvectors to 1e-12.  The regular
 call runs on a context held to the same one-CTA-per-k eigensolver, so the two
@@ -61,10 +62,14 @@ def test_noalloc_matches_regular_entry_point(lqm, ctx1, name, h):
     for call in range(2):
         b = torch.full((nk, n), float("nan"), dtype=torch.float64, device=dev)
         U = torch.full((nk, n, n), float("nan"), dtype=torch.complex128, device=dev)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         st = lqm.lib().lqm_bandmatrix_noalloc(stream, n, nR, d, lqm._ptr(d_keys), lqm._ptr(d_blocks), nk,
                                               lqm._ptr(d_ks), lqm._ptr(b), lqm._ptr(U))
         assert st == 0, (name, call, st)
         torch.cuda.synchronize()
+        if call == 1:  # after the first call's one-time set-up, a call takes no device memory at all
+            assert torch.cuda.mem_get_info(dev)[0] == free_before, (name, call)
         b, U = b.cpu().numpy(), U.cpu().numpy()
         assert np.max(np.abs(b - ref_b)) <= BAND_TOL * scale, (name, call)
         assert np.max(np.abs(U - ref_U)) <= 1e-12, (name, call)
