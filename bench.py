@@ -1,17 +1,23 @@
 """Throughput of the LatticeQM k-space hot path, H(k) + eigh + rho_R, on B200.
 
-One step = the batched three-model workload: for each of square 2x2 (n=8),
-kagome 2x2 (n=24) and triangular 4x4 with spin-orbit phases (n=96), a 256x256
-k-grid per GPU processed through ``lqm_bands_dos_rho_dev``: Bloch sum,
-FP64 Hermitian eigendecomposition with vectors, rho_L for the 9 keys of H
-(mu = 0, T = 0.01), DOS (500 points, Gamma = 0.05) and the bands.  Seeded
-synthetic models (no dataset exists for this path).
+One step = one density-matrix pass of the twisted-bilayer workload: the
+commensurate twisted bilayer honeycomb (m = 10, r = 1; n = 1324 pz orbitals,
+spinless) with Slater-Koster hopping (Vpp_pi = -2.7, Vpp_sigma = 0.48, decay
+0.184 a, cutoff 3 a), its 24 x 24 k-grid per GPU through
+``lqm_densitymatrix_dev``: Bloch sum, FP64 Hermitian eigendecomposition with
+vectors (batched blocked reduction + divide and conquer + back-transformation),
+rho_k = U f U^H and the Fourier fold into rho_L for the 7 keys of H (mu = 0,
+T = 0.01), and the band energy.  Seeded synthetic model (no dataset exists for
+this path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
 
 Prints one JSON line on rank 0.  ``value`` is the device-resident throughput
 (inputs on the device before the timed region); ``e2e`` is the same step
-through the host-pointer C-ABI with host<->device copies inside the timing.
+through the host-pointer C-ABI from pinned host memory (H uploaded, rho_L copied
+back, every step).  ``--impl reference`` times the reference's :multithreaded
+k-loop restated in C++/OpenMP (oracle/cpu_kspace.cpp: zheevr + zgemm + fold per
+k-point, one BLAS thread per host thread) on a bounded sample of the same grid.
 """
 import argparse
 import ctypes
@@ -32,14 +38,19 @@ for _p in (ROOT, PKG_PY):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-METRIC = "k-pts/s H(k)+eigh+rho_R (FP64 plain; batched square/kagome/triangular)"
+METRIC = "k-pts/s H(k)+eigh+rho_R (FP64 plain), twisted bilayer m=10 (n=1324)"
+NK_SIDE = 24
+MU, TEMP = 0.0, 0.01
+WORKLOAD = ("tbg_m10_n1324: twisted bilayer honeycomb (m=10, r=1; n=1324 pz orbitals, spinless), Slater-Koster "
+            "Vpp_pi=-2.7, Vpp_sigma=0.48, decay 0.184a, cutoff 3a; 24x24 k-grid per GPU; rho_R for the 7 keys "
+            "of H (mu=0, T=0.01) + band energy")
+# the batched three-model workload, reported among the other configurations
 NK_LIN = 256
 NW = 500
 GAMMA = 0.05
-MU, TEMP = 0.0, 0.01
-WORKLOAD = ("batch3: square2x2 (n=8) + kagome2x2 (n=24) + triangular4x4 3-site SOC (n=96), "
-            "256x256 k-grid each per GPU; bands + DOS(500, Gamma=0.05) + rho_R (9 keys, mu=0, T=0.01)")
-CPU_SAMPLE_PER_CORE = {8: 3072, 24: 1536, 96: 288}  # host k-points per model and core (~8 s per sample)
+BATCH_WORKLOAD = ("batch3: square2x2 (n=8) + kagome2x2 (n=24) + triangular4x4 3-site SOC (n=96), "
+                  "256x256 k-grid each; bands + DOS(500, Gamma=0.05) + rho_R (9 keys, mu=0, T=0.01)")
+FALLBACK_HBM_GBS = 6650.0
 
 
 def flops_per_k(n, nR, nL):
@@ -62,12 +73,30 @@ def kgrid(rank, world, nk_lin=NK_LIN):
     return np.asfortranarray(np.vstack([kx, ky]))
 
 
-def reduce_shards(dist, tensors, world):
-    """rho_L and DOS are averages over the whole grid: sum the per-rank averages
-    and divide by the number of ranks (each rank weights its own k by 1/nk_local)."""
-    for t in tensors:
-        dist.all_reduce(t)
-        t.div_(world)
+def full_grid(world, side=NK_SIDE):
+    """The (side*world) x side grid whose k-points all ranks pass to the library; with a
+    communicator set the library processes rank r's contiguous share (side x side
+    points) and sums rho_L over the ranks."""
+    import numpy as np
+    n1 = side * world
+    kx = np.tile(np.arange(n1) / n1, side)
+    ky = np.repeat(np.arange(side) / side, n1)
+    return np.asfortranarray(np.vstack([kx, ky]))
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json, else the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        for key in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if key in d:
+                v = d[key]
+                v = v.get("burst", v.get("value")) if isinstance(v, dict) else v
+                return float(v), "MEASURED_PEAKS.json hbm_gbs (measured copy bandwidth)"
+    except Exception:
+        pass
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -123,80 +152,98 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- CPU legs
-def _cpu_worker(args):
-    """Oracle per-k work on a chunk (one BLAS thread): H(k), zheevr with vectors, rho_k,
-    Fourier fold into rho_L, band energy, DOS contribution."""
+def cpu_threads():
+    return os.cpu_count() or 1
+
+
+def cpu_density_sample(h, ks_all, start, count, threads, packed=None):
+    """The oracle's C++/OpenMP density-matrix k-loop (oracle/cpu_kspace.cpp) on `count`
+    consecutive points of the grid from `start` (cyclic): (k-points, seconds)."""
     import numpy as np
-    from oracle import kspace as K
-    h, ks, omegas = args
-    keys = list(h.keys())
-    n = next(iter(h.values())).shape[0]
-    rho = np.zeros((len(keys), n, n), complex)
-    dos = np.zeros(len(omegas))
-    eb = 0.0
-    w = 1.0 / ks.shape[1]
-    for j in range(ks.shape[1]):
-        k = ks[:, j]
-        e, U = K.eigh_upper(K.fouriersum(h, k), True)
-        f = K.fermidirac(e, MU, TEMP)
-        rk = (U * f) @ U.conj().T
-        for li, Lk in enumerate(keys):
-            rho[li] += w * np.exp(-2j * math.pi * float(np.dot(k, Lk))) * rk
-        eb += w * float(np.sum(e * f))
-        dos += np.sum(GAMMA / ((omegas[:, None] - e[None, :]) ** 2 + GAMMA ** 2), axis=1)
-    return ks.shape[1]
-
-
-def cpu_time_per_k(models, pool, cores):
-    """Seconds per k-point per model on `cores` host processes (bounded sample)."""
-    import numpy as np
-    out = {}
-    for name, h in models:
-        n = next(iter(h.values())).shape[0]
-        ns = CPU_SAMPLE_PER_CORE.get(n, 256) * cores
-        rng = np.random.default_rng(n)
-        ks = rng.random((2, ns))
-        om = np.linspace(-6, 6, NW)
-        chunks = [(h, np.ascontiguousarray(c), om) for c in np.array_split(ks, cores * 4, axis=1) if c.shape[1]]
-        t0 = time.perf_counter()
-        done = sum(pool.map(_cpu_worker, chunks))
-        out[name] = (time.perf_counter() - t0) / done
-    return out
-
-
-def _cpu_density_worker(args):
-    """Oracle per-k work of a density-matrix call (one BLAS thread): H(k), zheevr with
-    vectors, rho_k = U f U^H and its Fourier fold into every key of H."""
-    import numpy as np
-    from oracle import kspace as K
-    h, ks = args
-    keys = list(h.keys())
-    n = next(iter(h.values())).shape[0]
-    rho = np.zeros((len(keys), n, n), complex)
-    for j in range(ks.shape[1]):
-        k = ks[:, j]
-        e, U = K.eigh_upper(K.fouriersum(h, k), True)
-        rk = (U * K.fermidirac(e, MU, TEMP)) @ U.conj().T
-        for li, Lk in enumerate(keys):
-            rho[li] += np.exp(-2j * math.pi * float(np.dot(k, Lk))) * rk
-    return ks.shape[1]
-
-
-def cpu_density_rate(h, pool, cores, per_core, seed=0):
-    """Host k-points per second of the oracle density-matrix k-loop on `cores` processes."""
-    import numpy as np
-    ks = np.random.default_rng(seed).random((2, per_core * cores))
-    chunks = [(h, np.ascontiguousarray(c)) for c in np.array_split(ks, cores, axis=1) if c.shape[1]]
+    from oracle import cpu as C
+    nk = ks_all.shape[1]
+    idx = (start + np.arange(count)) % nk
+    ks = np.ascontiguousarray(ks_all[:, idx])
     t0 = time.perf_counter()
-    done = sum(pool.map(_cpu_density_worker, chunks))
-    return done / (time.perf_counter() - t0)
+    C.densitymatrix(h, ks, None, MU, TEMP, list(h.keys()), nthreads=threads, packed=packed)
+    return count, time.perf_counter() - t0
+
+
+def cpu_baseline_tbg(h, ks_all, threads):
+    """cpu_baseline of the headline: 2 k-points per host thread of the 24 x 24 grid."""
+    from oracle import cpu as C
+    pk = C._pack(h)
+    cpu_density_sample(h, ks_all, 0, threads, threads, pk)  # warm (allocation, thread pool)
+    done, sec = cpu_density_sample(h, ks_all, threads, 2 * threads, threads, pk)
+    return {"value": done / sec, "unit": "k-pts/s", "cores": threads, "kind": "port",
+            "sample": f"{done} consecutive k-points of the 24x24 grid, C++/OpenMP restatement of the "
+                      f":multithreaded k-loop (per k: H(k), LAPACK zheevr, zgemm rho_k, fold into 7 keys) on "
+                      f"{threads} threads, one BLAS thread each; {sec:.1f} s"}
+
+
+def cpu_rate(h, ks_all, threads, per_thread=1, bands_only=False):
+    """Host k-points per second of the C++ restatement on a bounded sample."""
+    import numpy as np
+    from oracle import cpu as C
+    pk = C._pack(h)
+    count = max(1, per_thread * threads)
+    ks = np.ascontiguousarray(ks_all[:, np.arange(count) % ks_all.shape[1]])
+    t0 = time.perf_counter()
+    if bands_only:
+        C.bandmatrix(h, ks, nthreads=threads, packed=pk)
+    else:
+        C.densitymatrix(h, ks, None, MU, TEMP, list(h.keys()), nthreads=threads, packed=pk)
+    return count / (time.perf_counter() - t0)
+
+
+def run_reference(args, rank, world):
+    """--impl reference: LatticeQM's :multithreaded density-matrix k-loop restated in
+    C++/OpenMP (oracle/cpu_kspace.cpp) on the host cores, on the headline's workload.
+    Each step is a bounded sample: one k-point per host thread, consecutive points of the
+    24 x 24 grid (cycling through it); the line's value is k-points over the summed step
+    times.  Under torchrun only rank 0 runs."""
+    if rank != 0:
+        return
+    from lqm_workloads import lattice as LL
+    from lqm_workloads import models as M
+    from oracle import cpu as C
+    threads = cpu_threads()
+    _, h = M.tbg_slater_koster(10)
+    ks_all = LL.regulargrid(NK_SIDE * NK_SIDE)
+    pk = C._pack(h)
+    pos = 0
+    for _ in range(args.warmup):
+        cpu_density_sample(h, ks_all, pos, threads, threads, pk)
+        pos += threads
+    t_all = time.perf_counter()
+    done, secs = 0, []
+    for _ in range(args.steps):
+        c, sec = cpu_density_sample(h, ks_all, pos, threads, threads, pk)
+        pos += threads
+        done += c
+        secs.append(sec)
+    wall = time.perf_counter() - t_all
+    v = done / sum(secs)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "k-pts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(secs) / len(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded model)",
+            "config": {"workload": WORKLOAD, "parallelism": f"dp{world} (k-grid shards)",
+                       "host_threads": threads, "k_points_per_step": threads},
+            "cpu_baseline": {"value": v, "unit": "k-pts/s", "cores": threads, "kind": "port",
+                             "sample": f"per step {threads} consecutive k-points of the 24x24 grid (one per host "
+                                       f"thread), C++/OpenMP restatement of the :multithreaded k-loop (H(k), "
+                                       f"LAPACK zheevr, zgemm rho_k, fold into the 7 keys), one BLAS thread per "
+                                       f"thread; {args.steps} timed steps, wall {wall:.1f} s"},
+            "e2e": {"value": v, "unit": "k-pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def ctx_device(ctx):
     return 0 if not hasattr(ctx, "device") else ctx.device
 
 
-def large_configs(Q, ctx, M, pool, cores):
+def large_configs(Q, ctx, M, threads):
     """The other configurations of the hot path, one call each after a warm-up call,
     through the host-pointer C-ABI: device time of the call's kernels (CUDA events
     inside the library) and wall time including uploads and result copies."""
@@ -226,20 +273,18 @@ def large_configs(Q, ctx, M, pool, cores):
     out["honeycomb6x6_n144"] = {
         "grid": "48x48", "bands_kpts_per_s": ks1.shape[1] / dv, "bands_wall_kpts_per_s": ks1.shape[1] / wl,
         "rho_kpts_per_s": ks1.shape[1] / dd, "rho_wall_kpts_per_s": ks1.shape[1] / wd,
-        "cpu_rho_kpts_per_s": cpu_density_rate(h1, pool, cores, 8) if pool else None,
+        "cpu_rho_kpts_per_s": cpu_rate(h1, ks1, threads, per_thread=8),
         "path": "batched blocked eigensolver (n >= 128)"}
-    # twisted bilayer m=10, n = 1324: 24 x 24 grid (bands + rho) and a 400-point k-path (bands)
+    # twisted bilayer m=10, n = 1324: the 400-point k-path (bands only; rho on the 24 x 24
+    # grid is the headline)
     lat3, h3 = M.tbg_slater_koster(10)
-    ks3 = LL.regulargrid(24 * 24)
     kp3 = LL.kpath(lat3, 400)
-    dd, wd = timed(density_call(h3, ks3))
     db, wb = timed(lambda: Q.bandmatrix(h3, kp3, ctx=ctx))
-    out["tbg_m10_n1324"] = {
-        "grid": "24x24", "rho_kpts_per_s": ks3.shape[1] / dd, "rho_wall_kpts_per_s": ks3.shape[1] / wd,
+    out["tbg_m10_n1324_kpath"] = {
         "kpath_points": kp3.shape[1], "kpath_bands_kpts_per_s": kp3.shape[1] / db,
         "kpath_bands_wall_kpts_per_s": kp3.shape[1] / wb,
-        "cpu_rho_kpts_per_s": cpu_density_rate(h3, pool, cores, 1) if pool else None,
-        "path": "batched blocked eigensolver"}
+        "cpu_kpath_bands_kpts_per_s": cpu_rate(h3, kp3, threads, per_thread=2, bands_only=True),
+        "path": "batched blocked eigensolver (eigenvalue-only merges)"}
     # twisted bilayer m=15, n = 2884: one eigen + rho pass over the 12 x 12 grid, then
     # the Hartree-Fock SCF with the screened Coulomb interaction (3 iterations, the
     # 2nd and 3rd replayed from a captured CUDA graph), on a context of its own so that
@@ -301,49 +346,9 @@ def large_configs(Q, ctx, M, pool, cores):
     return out
 
 
-def make_pool(cores):
-    import multiprocessing as mp
-    for var in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
-        os.environ[var] = "1"
-    return mp.get_context("spawn").Pool(cores)
-
-
-def run_reference(args, rank, world):
-    """--impl reference: the reference algorithm on the host cores (oracle port of
-    LatticeQM's :multithreaded k-loop, one BLAS thread per worker)."""
-    if rank != 0:
-        return
-    from lqm_workloads import models as M
-    models = M.batch_models()
-    cores = os.cpu_count() or 1
-    pool = make_pool(cores)
-    nk_total = 3 * NK_LIN * NK_LIN
-    for _ in range(args.warmup):
-        cpu_time_per_k(models, pool, cores)
-    vals = []
-    t_all = time.perf_counter()
-    for _ in range(args.steps):
-        tpk = cpu_time_per_k(models, pool, cores)
-        t_step = sum(NK_LIN * NK_LIN * t for t in tpk.values())
-        vals.append(nk_total / t_step)
-    wall = time.perf_counter() - t_all
-    pool.close()
-    v = statistics.median(vals)
-    sample = ", ".join(f"n={n}: {c * cores} k" for n, c in CPU_SAMPLE_PER_CORE.items())
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "k-pts/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * nk_total / v,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded models)", "config": {"workload": WORKLOAD, "parallelism": f"cpu{cores}"},
-            "cpu_baseline": {"value": v, "unit": "k-pts/s", "cores": cores, "kind": "port",
-                             "sample": f"per step, random k-points per orbital count ({sample}) timed on "
-                                       f"{cores} processes, extrapolated to 3x256x256 k; wall {wall:.1f}s"},
-            "e2e": {"value": v, "unit": "k-pts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-
-
-# ----------------------------------------------------------------------------- GPU arm
 def measured_fp64_peak(torch, dev):
-    """cuBLAS DGEMM (8192^3) best of 5, TFLOP/s; the FP64 denominator of the roofline."""
+    """cuBLAS DGEMM (8192^3) best of 5, TFLOP/s; the FP64 denominator of the pass's
+    flop rate (MEASURED_PEAKS.json carries no FP64 figure)."""
     a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
     b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
     for _ in range(2):
@@ -413,6 +418,70 @@ def profile_case_kubo(Q, ctx, M):
                       "wall_s": time.perf_counter() - t0}))
 
 
+def batch_config(Q, ctx, M, torch, dev, np, steps, fp64_peak):
+    """The batched three-model configuration (n = 8, 24, 96; 256 x 256 k each): bands +
+    DOS + rho_R through lqm_bands_dos_rho_dev with device-resident inputs, 3 warm-up
+    steps and `steps` timed steps; the one-CTA eigensolver's FP64 roofline per model."""
+    models = M.batch_models()
+    ks_np = kgrid(0, 1)
+    nk = ks_np.shape[1]
+    d_ks = torch.from_numpy(np.ascontiguousarray(ks_np.T)).to(dev)
+    state = []
+    for name, h in models:
+        Hd = Q.DeviceHops(h, ctx)
+        n = Hd.n
+        Lk = np.asfortranarray(np.array(list(h.keys()), dtype=np.int64).T)
+        d_bands = torch.zeros(nk, n, dtype=torch.float64, device=dev)
+        ctx.check(Q.lib().lqm_bandmatrix_dev(ctx.handle, Hd.handle, nk, Q._ptr(d_ks), 0, 0, Q._ptr(d_bands), None))
+        lo, hi = float(d_bands.min()), float(d_bands.max())
+        state.append(dict(name=name, Hd=Hd, n=n, nR=len(h), Lk=Lk, bands=d_bands,
+                          rho=torch.zeros(len(h), n, n, dtype=torch.complex128, device=dev),
+                          dos=torch.zeros(NW, dtype=torch.float64, device=dev),
+                          om=torch.linspace(lo, hi, NW, dtype=torch.float64, device=dev)))
+    block_sizes = {}
+    for s_ in state:
+        if s_["n"] < 128:
+            best, _, table = Q.autotune_eigh(s_["Hd"], ks_np, want_rho=True, ctx=ctx)
+            block_sizes[f"n{s_['n']}"] = best
+    eb = ctypes.c_double()
+
+    def step(per_model_ms=None):
+        for s_ in state:
+            m0 = ctx.stats()[0]
+            ctx.check(Q.lib().lqm_bands_dos_rho_dev(
+                ctx.handle, s_["Hd"].handle, nk, Q._ptr(d_ks), None, MU, TEMP, s_["nR"], Q._ptr(s_["Lk"]),
+                Q._ptr(s_["rho"]), ctypes.byref(eb), NW, Q._ptr(s_["om"]), GAMMA, Q._ptr(s_["dos"]),
+                Q._ptr(s_["bands"]), 0))
+            if per_model_ms is not None:
+                per_model_ms[s_["n"]] = per_model_ms.get(s_["n"], 0.0) + ctx.stats()[0] - m0
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    ctx.reset_stats(timing=True)
+    per_model_ms = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step(per_model_ms)
+    e1.record()
+    torch.cuda.synchronize()
+    el = e0.elapsed_time(e1) / 1e3
+    ctx.stats()  # collects the pending events
+    detail = {}
+    for s_ in state:
+        ms = per_model_ms.get(s_["n"], 0.0)
+        tf = steps * nk * eigh_flops_per_k(s_["n"], s_["nR"]) / (ms / 1e3) / 1e12 if ms > 0 else None
+        detail[f"n{s_['n']}"] = {"eigh_ms_per_step": ms / steps, "eigh_tflops": tf,
+                                 "eigh_frac_of_fp64": (tf / fp64_peak) if tf else None,
+                                 "eigh_block_size": block_sizes.get(f"n{s_['n']}")}
+    for s_ in state:
+        s_["Hd"].free()
+    return {"workload": BATCH_WORKLOAD, "kpts_per_s": len(state) * nk * steps / el, "ms_per_step": 1000 * el / steps,
+            "steps": steps, "warmup": 3, "per_model": detail,
+            "eigh_flops_per_k": "8 nR n^2 + 13.33 n^3 (Bloch sum + eigh with vectors; rho_k fused, not counted)"}
+
+
 def main():
     # the SCF timings run a fixed number of iterations (tol = 0): no convergence warnings
     warnings.filterwarnings("ignore", message="SCF stopped before reaching the tolerance")
@@ -423,7 +492,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the other configurations (n=144, 1324, 2884 and the adjoint)")
+                    help="skip the other configurations (batch of n=8/24/96, n=144, the k-path, n=2884, SCF, "
+                         "the adjoint, Kubo)")
     ap.add_argument("--profile-case", nargs="?", const="n96", default=None,
                     choices=["n96", "tbg10-bands576", "tbg10-density142", "tbg10-density16", "kubo144"],
                     help="one call of a small profiling case: n96 = the fused bench call on the n=96 model "
@@ -447,72 +517,45 @@ def main():
     if not os.path.exists(lqm_build.LIB):
         lqm_build.build()
     import lqm_cuda as Q
+    from lqm_workloads import lattice as LL
     from lqm_workloads import models as M
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    models = M.batch_models()
     ctx = Q.Context(local, timeout=900)
     if args.profile_case == "n96":
-        return profile_case(Q, ctx, models[2][1], torch, dev, np)
+        return profile_case(Q, ctx, M.batch_models()[2][1], torch, dev, np)
     if args.profile_case == "kubo144":
         return profile_case_kubo(Q, ctx, M)
     if args.profile_case:
         return profile_case_tbg(Q, ctx, M, args.profile_case)
 
+    # ---- the library's communicator: k-point shards, rho_L summed over the ranks ----
+    if world > 1:
+        uid = Q.comm_unique_id() if rank == 0 else None
+        box = [uid]
+        dist.broadcast_object_list(box, src=0)
+        ctx.set_comm(world, rank, box[0])
+
     # ---- device-resident inputs ----
-    ks_np = kgrid(rank, world)
+    _, h = M.tbg_slater_koster(10)
+    keys = list(h.keys())
+    ks_np = full_grid(world)
     nk = ks_np.shape[1]
+    nk_local = nk // world
     d_ks = torch.from_numpy(np.ascontiguousarray(ks_np.T)).to(dev)   # (nk, 2) row-major == (2, nk) col-major
-    state = []
-    for name, h in models:
-        Hd = Q.DeviceHops(h, ctx)
-        n = Hd.n
-        Lk = np.asfortranarray(np.array(list(h.keys()), dtype=np.int64).T)
-        d_rho = torch.zeros(len(h), n, n, dtype=torch.complex128, device=dev)
-        d_bands = torch.zeros(nk, n, dtype=torch.float64, device=dev)
-        d_dos = torch.zeros(NW, dtype=torch.float64, device=dev)
-        # DOS window [min eps, max eps] of this model, from one bands pass
-        ctx.check(Q.lib().lqm_bandmatrix_dev(ctx.handle, Hd.handle, nk, Q._ptr(d_ks), 0, 0,
-                                              Q._ptr(d_bands), None))
-        lo, hi = float(d_bands.min()), float(d_bands.max())
-        if world > 1:
-            t = torch.tensor([-lo, hi], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            lo, hi = -float(t[0]), float(t[1])
-        d_om = torch.linspace(lo, hi, NW, dtype=torch.float64, device=dev)
-        state.append(dict(name=name, h=h, Hd=Hd, n=n, nR=len(h), Lk=Lk, rho=d_rho, bands=d_bands, dos=d_dos,
-                          om=d_om))
-
-    # block size of the one-CTA eigensolver per model, chosen by the library's
-    # autotuner on the step's own k-grid (outside the timed region; a sample that
-    # fits in one wave of CTAs would time latency, not throughput)
-    block_sizes = {}
-    ks_tune = np.asfortranarray(ks_np)
-    for s in state:
-        if s["n"] < 128:
-            best, _, table = Q.autotune_eigh(s["Hd"], ks_tune, want_rho=True, ctx=ctx)
-            block_sizes[f"n{s['n']}"] = {"chosen": best, "ms_by_block_size": {str(k): round(v, 3) for k, v in
-                                                                              table.items()}}
-
+    Hd = Q.DeviceHops(h, ctx)
+    n, nR = Hd.n, Hd.nR
+    Lk = np.asfortranarray(np.array(keys, dtype=np.int64).T)
+    d_rho = torch.zeros(nR, n, n, dtype=torch.complex128, device=dev)
     eb = ctypes.c_double()
 
-    def step(per_model_ms=None):
-        for s in state:
-            if per_model_ms is not None:
-                m0 = ctx.stats()[0]
-            ctx.check(Q.lib().lqm_bands_dos_rho_dev(
-                ctx.handle, s["Hd"].handle, nk, Q._ptr(d_ks), None, MU, TEMP, s["nR"], Q._ptr(s["Lk"]),
-                Q._ptr(s["rho"]), ctypes.byref(eb), NW, Q._ptr(s["om"]), GAMMA, Q._ptr(s["dos"]),
-                Q._ptr(s["bands"]), 0))
-            if per_model_ms is not None:
-                per_model_ms[s["n"]] = per_model_ms.get(s["n"], 0.0) + ctx.stats()[0] - m0
-            if world > 1:  # rho_L and DOS are sums over the whole grid: one exchange per model
-                reduce_shards(dist, (s["rho"], s["dos"]), world)
+    def step():
+        ctx.check(Q.lib().lqm_densitymatrix_dev(ctx.handle, Hd.handle, nk, Q._ptr(d_ks), None, MU, TEMP, nR,
+                                                Q._ptr(Lk), Q._ptr(d_rho), ctypes.byref(eb), 0))
 
-    fp64_peak = measured_fp64_peak(torch, dev)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -521,7 +564,6 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    per_model_ms = {}
     ctx.reset_stats(timing=True)
     if world > 1:
         dist.barrier()
@@ -529,49 +571,46 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
-        step(per_model_ms)
+        step()
     e1.record()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     elapsed = e0.elapsed_time(e1) / 1e3
-    eigh_ms, eigh_launches, launches = ctx.stats()
     clocks = sampler.stop()
+    eigh_ms, eigh_launches, launches = ctx.stats()
+    symv_ms, symv_launches, symv_bytes = ctx.kernel_stats(1)
     if world > 1:
         t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t[0])
-    total_k = world * len(state) * nk * args.steps
+    total_k = nk * args.steps
     value = total_k / elapsed
 
-    # ---- e2e through the host-pointer C-ABI (pinned host buffers) ----
+    # ---- e2e through the host-pointer C-ABI from pinned host memory ----
+    _, _, d_, K_, B_ = Q.pack_hops(h)
+    blocks_pin = torch.from_numpy(np.ascontiguousarray(B_.transpose(2, 1, 0))).pin_memory()  # n x n x nR col-major
+    keys_pin = torch.from_numpy(np.ascontiguousarray(K_.T)).pin_memory()
     ks_pin = torch.from_numpy(np.ascontiguousarray(ks_np.T)).pin_memory()
-    host = []
-    for s in state:
-        host.append(dict(rho=torch.zeros(s["nR"], s["n"], s["n"], dtype=torch.complex128).pin_memory(),
-                         bands=torch.zeros(nk, s["n"], dtype=torch.float64).pin_memory(),
-                         dos=torch.zeros(NW, dtype=torch.float64).pin_memory(),
-                         om=s["om"].cpu().pin_memory()))
-    h2d = d2h = 0
-    for s, hb in zip(state, host):
-        h2d += s["nR"] * s["n"] ** 2 * 16 + s["Lk"].nbytes + ks_pin.numel() * 8 + NW * 8
-        d2h += hb["rho"].numel() * 16 + hb["bands"].numel() * 8 + NW * 8
+    rho_pin = torch.zeros(nR, n, n, dtype=torch.complex128).pin_memory()
+    h2d = blocks_pin.numel() * 16 + keys_pin.numel() * 8 + ks_pin.numel() * 8
+    d2h = rho_pin.numel() * 16 + 8
 
     def e2e_step():
-        for s, hb in zip(state, host):
-            Hd = Q.DeviceHops(s["h"], ctx)  # H uploaded per call, as a user call does
-            ctx.check(Q.lib().lqm_bands_dos_rho(
-                ctx.handle, Hd.handle, nk, Q._ptr(ks_pin), None, MU, TEMP, s["nR"], Q._ptr(s["Lk"]),
-                Q._ptr(hb["rho"]), ctypes.byref(eb), NW, Q._ptr(hb["om"]), GAMMA, Q._ptr(hb["dos"]),
-                Q._ptr(hb["bands"]), 0))
-            Hd.free()
+        hp = ctypes.c_void_p()
+        ctx.check(Q.lib().lqm_hops_upload_dense(ctx.handle, n, nR, d_, Q._ptr(keys_pin), Q._ptr(blocks_pin),
+                                                ctypes.byref(hp)))
+        ctx.check(Q.lib().lqm_densitymatrix(ctx.handle, hp, nk, Q._ptr(ks_pin), None, MU, TEMP, nR, Q._ptr(Lk),
+                                            Q._ptr(rho_pin), ctypes.byref(eb), 0))
+        ctx.check(Q.lib().lqm_hops_free(ctx.handle, hp))
 
+    e2e_steps = max(3, args.steps // 4)
     e2e_step()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize()
     e2e_el = time.perf_counter() - t0
@@ -579,47 +618,50 @@ def main():
         t = torch.tensor([e2e_el], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_el = float(t[0])
-    e2e_val = total_k / e2e_el
+    e2e_val = nk * e2e_steps / e2e_el
 
-    # ---- roofline of the dominant kernel: the per-k eigensolver on the n=96 model ----
-    detail = {}
-    for s_ in state:
-        ms = per_model_ms.get(s_["n"], 0.0)
-        if ms > 0:
-            detail[f"n{s_['n']}"] = {"eigh_ms_per_step": ms / args.steps,
-                                     "eigh_tflops": args.steps * nk * eigh_flops_per_k(s_["n"], s_["nR"])
-                                     / (ms / 1e3) / 1e12}
-    dom = max(state, key=lambda s_: s_["n"])
-    dom_ms = per_model_ms.get(dom["n"], 0.0)
-    achieved = (args.steps * nk * eigh_flops_per_k(dom["n"], dom["nR"]) / (dom_ms / 1e3) / 1e12
-                if dom_ms > 0 else None)
-    # k-points per launch of the dominant model (the library's rho_k batch: 4 GB / (16 n^2) k)
-    kb = max(1, min(nk, int(4.0e9 // (16.0 * dom["n"] ** 2))))
-    k_per_launch = nk / math.ceil(nk / kb)
+    # ---- roofline of the dominant kernel: the blocked path's lower-triangle mat-vec ----
+    peak, peak_src = hbm_peak()
+    achieved = symv_bytes / (symv_ms / 1e3) / 1e9 if symv_ms > 0 else None
+    per_launch = symv_bytes / symv_launches if symv_launches else None
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "eigh_traffic.json")
-    if os.path.exists(tfile):
+    tfile = os.path.join(ROOT, "profiles", "blk_symv_traffic.json")
+    if per_launch and os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile))["bytes_per_k"] * k_per_launch
+            traffic = json.load(open(tfile))["dram_bytes_per_algorithmic_byte"] * per_launch
         except Exception:
             traffic = None
-    roof = {"bound": "tensor", "pipe": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-            "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
-            "kernel": f"eigh_kernel on the n={dom['n']} model (Bloch sum + Householder + divide&conquer + "
-                      f"back-transform + fused rho_k, one CTA per k)",
-            "algorithmic_flops_per_k": eigh_flops_per_k(dom["n"], dom["nR"]),
-            "k_per_launch": k_per_launch,
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
-            "traffic_source": "ncu dram bytes per k-point of the 2048-k capture (profiles/eigh_kernel_n96_2048k.md) "
-                              "x k-points per launch",
-            "eigh_launches_all_models": eigh_launches, "eigh_ms_all_models": eigh_ms, "per_model": detail}
+    fl = flops_per_k(n, nR, nR)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "kernel": "blk_symv_pipe_kernel (Householder mat-vec y = A22 v over the lower triangle of the trailing "
+                      "block, all k-points of the batch per launch; one launch per column)",
+            "algorithmic_bytes_per_launch": per_launch,
+            "algorithmic_bytes_per_k": "16 B x m(m+1)/2 per column, m = n-1-j (sum ~ 16 n^3/6 = 6.2 GB at n=1324)",
+            "launches": symv_launches, "kernel_ms": symv_ms, "share_of_step": symv_ms / 1e3 / elapsed,
+            "peak_source": peak_src,
+            "traffic_source": "ncu dram bytes / algorithmic bytes of one capture (profiles/blk_symv_traffic.json) "
+                              "x this run's algorithmic bytes per launch",
+            "pass_tflops": value / world * fl / 1e12, "pass_flops_per_k": fl,
+            "eigh_pass_ms": eigh_ms, "eigh_passes": eigh_launches}
 
-    # ---- SCF seconds per iteration (triangular Hubbard HF workload) ----
+    threads = cpu_threads()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_tbg(h, LL.regulargrid(NK_SIDE * NK_SIDE), threads)
+
+    configs = None
     scf = None
-    if rank == 0:
-        lat, h4, v4 = M.triangular_hubbard(L_super=6)
-        rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=3)}
-        from lqm_workloads import lattice as LL
+    if rank == 0 and world == 1 and not args.no_configs:
+        fp64_peak = measured_fp64_peak(torch, dev)
+        roof["fp64_dgemm_tflops_measured"] = fp64_peak
+        roof["pass_frac_of_fp64"] = roof["pass_tflops"] / fp64_peak
+        Hd.free()
+        del d_rho
+        torch.cuda.empty_cache()
+        configs = {"batch3": batch_config(Q, ctx, M, torch, dev, np, 3, fp64_peak)}
+        lat4, h4, v4 = M.triangular_hubbard(L_super=6)
+        rho0 = {(0, 0): M.random_local_magnetization(lat4.norb, seed=3)}
         ks4 = LL.regulargrid(36 * 36)
         Q.solvehartreefock(h4, v4, rho0, 0.5, ks4, T=0.02, beta=0.3, tol=0.0, iterations=3, ctx=ctx)
         iters = 12
@@ -632,33 +674,19 @@ def main():
                "iterations": iters, "residual": res.residual,
                "note": "wall time of lqm_scf_hf per iteration incl. h/v upload and the returned rho; "
                        "iterations 2+ replay a captured CUDA graph"}
-
-    cpu = None
-    configs = None
-    pool = None
-    cores = os.cpu_count() or 1
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        pool = make_pool(cores)
-        tpk = cpu_time_per_k(models, pool, cores)
-        t_step = sum(NK_LIN * NK_LIN * t for t in tpk.values())
-        sample = ", ".join(f"n={n}: {c * cores} k" for n, c in CPU_SAMPLE_PER_CORE.items())
-        cpu = {"value": len(state) * NK_LIN * NK_LIN / t_step, "unit": "k-pts/s", "cores": cores, "kind": "port",
-               "sample": f"random k-points per model ({sample}), oracle per-k zheevr+rho+fold+DOS on {cores} "
-                         f"processes, extrapolated to 3x256x256 k"}
-    if rank == 0 and world == 1 and not args.no_configs:
-        configs = large_configs(Q, ctx, M, pool, cores)
-    if pool is not None:
-        pool.close()
+        configs.update(large_configs(Q, ctx, M, threads))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "k-pts/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded models)",
-                "config": {"workload": WORKLOAD, "k_points_per_gpu_per_step": len(state) * nk,
-                           "parallelism": f"dp{world} (k-grid shards; rho_R/DOS all-reduce)",
-                           "l2": "inputs larger than L2 (each step streams ~8 GB of U/rho_k through HBM)",
-                           "eigh_block_size": block_sizes},
-                "e2e": {"value": e2e_val, "unit": "k-pts/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded model)",
+                "config": {"workload": WORKLOAD, "k_points_per_gpu_per_step": nk_local,
+                           "parallelism": f"dp{world} (k-grid shards in the library; rho_R all-reduce over NCCL)"
+                           if world > 1 else "dp1",
+                           "l2": "inputs larger than L2 (each step streams ~32 GB of A/U through HBM)",
+                           "precision": "FP64 plain (the mixed-precision form is not built)"},
+                "e2e": {"value": e2e_val, "unit": "k-pts/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": e2e_steps},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "scf": scf,
                 "configs": configs}
         print(json.dumps(line), flush=True)

@@ -33,6 +33,8 @@ extern "C" {
 #define LQM_ENOCONV (-5)  /* SCF did not converge and the caller asked for an error */
 #define LQM_EDEVICE (-6)  /* a device-side check failed (e.g. no sign change for mu) */
 
+#define LQM_COMM_ID_BYTES 128 /* size of a communicator id (an NCCL unique id) */
+
 typedef struct lqm_ctx lqm_ctx;
 typedef struct lqm_hops lqm_hops;
 
@@ -116,6 +118,13 @@ int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
  * kernel, so a profiling mode, not a timing one). */
 int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing);
 int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches);
+/* The same statistics per kernel class: 0 = the eigensolver passes (as above),
+ * 1 = the blocked path's lower-triangle mat-vec (blk_symv_pipe_kernel), each
+ * launch timed with CUDA events, with its algorithmic bytes (the lower triangle
+ * of the trailing block read once per column and k-point, 16 B per element).
+ * No reference counterpart (profiling). */
+int lqm_ctx_kernel_stats(const lqm_ctx* ctx, int kernel_class, double* ms, int64_t* launches,
+                         double* algorithmic_bytes);
 /* SM cycles spent by the eigensolver kernel per stage, summed over CTAs while
  * the phase counters are enabled (lqm_ctx_reset_stats(ctx, 2)): [0] Bloch
  * sum, [1] Householder, [2] divide and conquer, [3] bands +
@@ -125,6 +134,37 @@ int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, i
  * Householder steps (trailing pass, mat-vec reduction, next column and
  * reflector).  New (profiling). */
 int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles /* [16] */);
+
+/* ---- k-point sharding over several GPUs, one process (and one context) per GPU.
+ * Replaces the reference's DistributedExec k-loops (src/modules/Parallel/Parallel.jl:
+ * 275-287 pmap over k-chunks, 415-467 the streaming fold of per-worker partial rho).
+ * Rank 0 makes an id with lqm_comm_unique_id and hands its LQM_COMM_ID_BYTES bytes to
+ * the other ranks (MPI, a TCP store, Distributed.jl); every rank then calls
+ * lqm_ctx_set_comm(ctx, nranks, rank, id) on its own context and device (collective:
+ * it returns once all ranks have joined, or LQM_ETIMEOUT after the context's wait
+ * limit).  With nranks > 1 set, these entry points shard the k list they are given:
+ * every rank passes the SAME full list (and weights) and processes its contiguous
+ * share lqm_shard_range(nk, nranks, rank):
+ *   lqm_densitymatrix[_dev], lqm_bands_dos_rho[_dev]: rho_L and the band energy are
+ *     summed over the ranks (NCCL all-reduce); bands are gathered on every rank;
+ *   lqm_bandmatrix[_dev]: bands (and U) gathered on every rank;
+ *   lqm_chemicalpotential, lqm_dos: the bands gathered, then the same mu / DOS on every
+ *     rank as on one GPU;
+ *   lqm_scf_hf: per iteration the eigen pass and rho on the shard, bands gathered for
+ *     mu, rho / band energy / commutator summed; mixing replicated (no graph replay).
+ * Every rank must make the same calls in the same order.  Other entry points ignore
+ * the communicator.  NCCL is loaded at run time (libnccl.so.2, or the path in
+ * LQM_NCCL_LIB); each NCCL call is polled with the context's wait limit, and a
+ * failed or timed-out collective aborts the communicator (the context continues
+ * unsharded).  nranks = 1 with id == NULL removes the communicator (nranks = 1 with
+ * an id makes a one-rank communicator: the same code path, whose collectives are
+ * copies). */
+int lqm_comm_unique_id(char* id_out /* LQM_COMM_ID_BYTES */);
+int lqm_ctx_set_comm(lqm_ctx* ctx, int nranks, int rank, const char* id);
+int lqm_ctx_comm(const lqm_ctx* ctx, int* nranks, int* rank);
+/* The share [k0, k1) of a k list of nk points that rank `rank` of nranks processes:
+ * k0 = floor(rank nk / nranks), k1 = floor((rank + 1) nk / nranks).  Host only. */
+int lqm_shard_range(int64_t nk, int nranks, int rank, int64_t* k0, int64_t* k1);
 
 /* Upload a dense Hops (src/modules/TightBinding/types.jl:54-60, DenseHops):
  * keys d x nR (Int64), blocks n x n x nR column-major ComplexF64 in the same

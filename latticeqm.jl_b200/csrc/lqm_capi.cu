@@ -56,13 +56,17 @@ struct lqm_ctx {
   double last_ms = 0.0;
   std::map<int, PlanDev> plans;
   std::map<int, int> eigh_nt;  // one-CTA eigensolver block size per order n (autotuned or set), else the rule
-  DevBuf ws[40];
+  DevBuf ws[48];
   // per-kernel device-time statistics (CUDA events on the context stream)
   bool stats_on = false;
   bool phases_on = false;  // per-phase cycle counters inside the eigensolver (clock reads)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending, ev_pool;
   double eigh_ms = 0.0;
   int64_t eigh_launches = 0, launches = 0;
+  // the blocked path's mat-vec kernel (the dominant kernel of a large-n pass), timed per launch
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> symv_pending;
+  double symv_ms = 0.0, symv_bytes = 0.0;
+  int64_t symv_launches = 0;
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
   cublasHandle_t blas = nullptr;          // batched GEMMs of the blocked large-n path
@@ -83,6 +87,9 @@ struct lqm_ctx {
   // from milliseconds to most of a second per call on B200
   std::vector<std::pair<void*, size_t>> hops_cache;
   size_t hops_cache_bytes = 0;
+  // NCCL communicator of the k-point shards (lqm_ctx_set_comm; lqm_comm.inc)
+  void* comm = nullptr;
+  int comm_nranks = 1, comm_rank = 0;
 };
 
 struct lqm_hops {
@@ -150,6 +157,12 @@ void collect_stats(lqm_ctx* ctx) {
     ctx->ev_pool.push_back(pr);
   }
   ctx->ev_pending.clear();
+  for (auto& pr : ctx->symv_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) ctx->symv_ms += ms;
+    ctx->ev_pool.push_back(pr);
+  }
+  ctx->symv_pending.clear();
 }
 
 void wait_stream(lqm_ctx* ctx) {
@@ -225,9 +238,13 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN
 };
-static_assert(WS_CSC < 40, "workspace slots");
+static_assert(WS_UNIW < 48, "workspace slots");
+
+}  // namespace
+#include "lqm_comm.inc"
+namespace {
 
 // ---- divide-and-conquer plan (lqm_plan.h), uploaded once per order n ----
 const DCPlan& get_plan(lqm_ctx* ctx, int n) {
@@ -393,8 +410,17 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           const int64_t nbl = (n - j - 1 + kSymvTB - 1) / kSymvTB;
           const int64_t nitems = nbl * (nbl + 1) / 2 * nbk;
           const int64_t grid = std::min<int64_t>(nitems, (int64_t)ctx->num_sms);
+          std::pair<cudaEvent_t, cudaEvent_t> sev{};
+          if (ctx->stats_on) { sev = stat_events(ctx); ck(cudaEventRecord(sev.first, ctx->stream), "event"); }
           blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
           ctx->launches++;
+          if (ctx->stats_on) {
+            ck(cudaEventRecord(sev.second, ctx->stream), "event");
+            ctx->symv_pending.push_back(sev);
+            const double m = (double)(n - j - 1);
+            ctx->symv_bytes += (double)nbk * m * (m + 1.0) / 2.0 * 16.0;  // lower triangle of A22, once
+            ctx->symv_launches++;
+          }
           if (i > 0) {
             const dim3 g2((unsigned)((n - j - 1 + 127) / 128), (unsigned)nbk);
             blk_t12_kernel<<<g2, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
@@ -435,27 +461,66 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     ctx->launches++;
     ck(cudaGetLastError(), "divide-and-conquer launch");
     if (!vec) continue;
-    blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A);
-    blk_larft_kernel<<<dim3((unsigned)P, (unsigned)nbk), kBlkThreads, nb * nb * sizeof(double2), ctx->stream>>>(
-        n, nb, P, A, tau, Tm);
-    ctx->launches += 2;
-    for (int p = P - 1; p >= 0; --p) {
+    // When only rho_k is wanted, the back-transformation forms just the columns of U
+    // that carry it: the states that are not exactly empty (rho_k = U_K f U_K^H) or,
+    // when fewer, those that are not exactly filled (rho_k = I - U_K (1 - f) U_K^H),
+    // K = the largest such count over the batch (a host read of two integers).
+    int c0 = 0, K = n;
+    bool complement = false;
+    if (rhok && !d_U) {
+      int* span = (int*)ws_get(ctx, WS_SPAN, 2 * sizeof(int));
+      ck(cudaMemsetAsync(span, 0, 2 * sizeof(int), ctx->stream), "memset");
+      blk_occ_span_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, d_bands + k0 * n, mu, T, span);
+      ctx->launches++;
+      int hspan[2] = {n, n};
+      ck(cudaMemcpyAsync(hspan, span, sizeof(hspan), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+      wait_stream(ctx);
+      if (hspan[0] < hspan[1]) {
+        complement = true;
+        K = hspan[0];
+        c0 = n - K;
+      } else {
+        K = hspan[1];
+      }
+    }
+    if (K > 0) {
+      blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A);
+      blk_larft_kernel<<<dim3((unsigned)P, (unsigned)nbk), kBlkThreads, nb * nb * sizeof(double2), ctx->stream>>>(
+          n, nb, P, A, tau, Tm);
+      ctx->launches += 2;
+    }
+    for (int p = P - 1; p >= 0 && K > 0; --p) {
       const int j0 = p * nb;
       const int nbr = std::min(nb, n - 1 - j0);
       if (nbr <= 0) continue;
       const int m = n - j0 - 1;
       const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
-      double2* Us = Ucur + (j0 + 1);
-      // X = V^H Us (nbr x n), Y = Tm X, Us -= V Y
-      zgemm_sb(h, CUBLAS_OP_C, CUBLAS_OP_N, nbr, n, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nb, (long long)n * nb,
+      double2* Us = Ucur + (j0 + 1) + (int64_t)c0 * n;
+      // X = V^H Us (nbr x K), Y = Tm X, Us -= V Y
+      zgemm_sb(h, CUBLAS_OP_C, CUBLAS_OP_N, nbr, K, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nb, (long long)n * nb,
                nbk);
-      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, nbr, n, nbr, 1.0, Tm + (int64_t)p * nb * nb, nb,
+      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, nbr, K, nbr, 1.0, Tm + (int64_t)p * nb * nb, nb,
                (long long)nb * nb * P, W, nb, (long long)n * nb, 0.0, Yb, nb, (long long)n * nb, nbk);
-      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, nbr, -1.0, V, n, nn, Yb, nb, (long long)n * nb, 1.0, Us, n, nn,
+      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, m, K, nbr, -1.0, V, n, nn, Yb, nb, (long long)n * nb, 1.0, Us, n, nn,
                nbk);
       ctx->launches += 3;
     }
-    if (rhok) {
+    if (rhok && !d_U) {
+      blk_scale_f_cols_kernel<<<nbk, kBlkThreads, n * sizeof(double), ctx->stream>>>(
+          n, Ucur, d_bands + k0 * n, mu, T, w + k0, A, ebk + k0, c0, K, complement ? 1 : 0);
+      ctx->launches++;
+      if (K > 0) {
+        zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, K, complement ? -1.0 : 1.0, A, n, nn, Ucur + (int64_t)c0 * n,
+                 n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
+        ctx->launches++;
+      } else {
+        ck(cudaMemsetAsync(rhok + k0 * nn, 0, (size_t)(nbk * nn) * sizeof(double2), ctx->stream), "memset");
+      }
+      if (complement) {
+        blk_add_identity_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, rhok + k0 * nn);
+        ctx->launches++;
+      }
+    } else if (rhok) {
       blk_scale_f_kernel<<<nbk, kBlkThreads, n * sizeof(double), ctx->stream>>>(
           n, nbk, Ucur, d_bands + k0 * n, mu, nullptr, T, w + k0, A, ebk + k0);
       zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, n, 1.0, A, n, nn, Ucur, n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
@@ -545,12 +610,29 @@ void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const 
 }
 
 // bands_out (n x nk, device) receives every k's eigenvalues when non-null.
+// With `shard` and a communicator on the context, this rank processes its share of
+// the k list, rho_L and the band energy are summed over the ranks and bands_out is
+// gathered (lqm_comm.inc).
 void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, const double* d_w, double mu,
                  double T, int64_t nL, const int64_t* d_Lkeys, double2* d_rho, double* d_eb,
-                 double* bands_out = nullptr) {
+                 double* bands_out = nullptr, bool shard = false) {
   NvtxRange nvtx_("density matrix");
   const int n = (int)H->n;
   const int64_t nn = (int64_t)n * n;
+  if (shard && sharded(ctx)) {
+    const KShard s = kshard(ctx, nk);
+    if (s.count() > 0)
+      density_dev(ctx, H, s.count(), d_ks + s.k0 * H->d, d_w + s.k0, mu, T, nL, d_Lkeys, d_rho, d_eb,
+                  bands_out ? bands_out + s.k0 * n : nullptr, false);
+    else {
+      ck(cudaMemsetAsync(d_rho, 0, (size_t)(nL * nn) * sizeof(double2), ctx->stream), "memset");
+      ck(cudaMemsetAsync(d_eb, 0, sizeof(double), ctx->stream), "memset");
+    }
+    comm_allreduce(ctx, (double*)d_rho, (size_t)(2 * nL * nn));
+    comm_allreduce(ctx, d_eb, 1);
+    if (bands_out) comm_gather_k(ctx, bands_out, n, nk);
+    return;
+  }
   // rho_k batch: 4 GB, or one k-point per SM for large n (the blocked path
   // runs one divide-and-conquer CTA per k-point)
   const double budget = std::max(4.0e9, 16.0 * (double)nn * (double)std::min<int64_t>(nk, ctx->num_sms));
@@ -570,6 +652,23 @@ void density_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
     launch_fold(ctx, nn, nb, rk, coef, (int)nL, d_rho, k0 > 0);
     ctx->launches += 2;
   }
+}
+
+// Eigen pass over a k list split over the ranks of the context's communicator:
+// each rank solves its share, then bands (and U) are gathered so that every rank
+// holds all of them.  Without a communicator this is launch_eigh.
+void eigh_sharded(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands,
+                  double2* d_U) {
+  if (!sharded(ctx)) {
+    launch_eigh(ctx, H, nk, d_ks, d_bands, d_U);
+    return;
+  }
+  const KShard s = kshard(ctx, nk);
+  const int64_t n = H->n;
+  if (s.count() > 0)
+    launch_eigh(ctx, H, s.count(), d_ks + s.k0 * H->d, d_bands + s.k0 * n, d_U ? d_U + s.k0 * n * n : nullptr);
+  comm_gather_k(ctx, d_bands, n, nk);
+  if (d_U) comm_gather_k(ctx, (double*)d_U, 2 * n * n, nk);
 }
 
 // Chemical potential entirely on the device: mu_out (device double) receives
@@ -659,9 +758,9 @@ T* upload(lqm_ctx* ctx, int slot, const T* h, size_t count) {
   return d;
 }
 
-double* uniform_weights(lqm_ctx* ctx, int64_t nk) {
+double* uniform_weights(lqm_ctx* ctx, int64_t nk, int slot = WS_W) {
   std::vector<double> w((size_t)nk, 1.0 / (double)nk);
-  double* d = upload(ctx, WS_W, w.data(), w.size());
+  double* d = upload(ctx, slot, w.data(), w.size());
   wait_stream(ctx);
   return d;
 }
@@ -706,6 +805,10 @@ int lqm_ctx_destroy(lqm_ctx* ctx) {
   if (!ctx) return LQM_EINVAL;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  try {
+    comm_release(ctx);
+  } catch (const LqmError&) {
+  }
   for (auto& b : ctx->ws)
     if (b.p) cudaFree(b.p);
   for (auto& kv : ctx->plans) cudaFree(kv.second.d_buf);
@@ -830,6 +933,9 @@ int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing) {
     ctx->eigh_ms = 0.0;
     ctx->eigh_launches = 0;
     ctx->launches = 0;
+    ctx->symv_ms = 0.0;
+    ctx->symv_bytes = 0.0;
+    ctx->symv_launches = 0;
   });
 }
 
@@ -843,6 +949,21 @@ int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles) {
     }
     for (int i = 0; i < 16; ++i) cycles[i] = (double)h[i];
   });
+}
+
+int lqm_ctx_kernel_stats(const lqm_ctx* ctx, int kernel_class, double* ms, int64_t* launches,
+                         double* algorithmic_bytes) {
+  if (!ctx || kernel_class < 0 || kernel_class > 1) return LQM_EINVAL;
+  if (kernel_class == 0) {
+    if (ms) *ms = ctx->eigh_ms;
+    if (launches) *launches = ctx->eigh_launches;
+    if (algorithmic_bytes) *algorithmic_bytes = 0.0;
+  } else {
+    if (ms) *ms = ctx->symv_ms;
+    if (launches) *launches = ctx->symv_launches;
+    if (algorithmic_bytes) *algorithmic_bytes = ctx->symv_bytes;
+  }
+  return LQM_OK;
 }
 
 int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches) {
@@ -1048,7 +1169,7 @@ int lqm_bandmatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     check_precision(precision);
     if (nk < 1 || !d_ks || !d_bands || (want_vectors && !d_U)) fail(LQM_EINVAL, "invalid arguments");
     timer_start(ctx);
-    launch_eigh(ctx, H, nk, d_ks, d_bands, want_vectors ? (double2*)d_U : nullptr);
+    eigh_sharded(ctx, H, nk, d_ks, d_bands, want_vectors ? (double2*)d_U : nullptr);
     timer_stop(ctx);
     wait_stream(ctx);
     timer_collect(ctx);
@@ -1067,7 +1188,7 @@ int lqm_bandmatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks
     double* db = (double*)ws_get(ctx, WS_BANDS, (size_t)(n * nk) * sizeof(double));
     double* dU = want_vectors ? (double*)ws_get(ctx, WS_U, (size_t)(n * n * nk) * sizeof(double2)) : nullptr;
     timer_start(ctx);
-    launch_eigh(ctx, H, nk, dks, db, (double2*)dU);
+    eigh_sharded(ctx, H, nk, dks, db, (double2*)dU);
     timer_stop(ctx);
     wait_stream(ctx);  // poll with the context's limit: a copy into pageable host memory would block unbounded
     ck(cudaMemcpyAsync(bands, db, (size_t)(n * nk) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
@@ -1090,7 +1211,7 @@ int lqm_densitymatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
     const double* dw = d_w ? d_w : uniform_weights(ctx, nk);
     double* d_eb = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double)) + 40;
     timer_start(ctx);
-    density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb);
+    density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb, nullptr, true);
     timer_stop(ctx);
     double eb = 0.0;
     wait_stream(ctx);  // poll with the context's limit: a copy into pageable host memory would block unbounded
@@ -1139,7 +1260,7 @@ int lqm_chemicalpotential(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
     const double* dw = w ? upload(ctx, WS_W, w, (size_t)nk) : nullptr;
     double* db = (double*)ws_get(ctx, WS_BANDS, (size_t)(H->n * nk) * sizeof(double));
     timer_start(ctx);
-    launch_eigh(ctx, H, nk, dks, db, nullptr);
+    eigh_sharded(ctx, H, nk, dks, db, nullptr);
     timer_stop(ctx);
     wait_stream(ctx);
     timer_collect(ctx);
@@ -1172,7 +1293,7 @@ int lqm_dos(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const
     double* db = (double*)ws_get(ctx, WS_BANDS, (size_t)(H->n * nk) * sizeof(double));
     double* dd = (double*)ws_get(ctx, WS_DOS, (size_t)nw * sizeof(double));
     timer_start(ctx);
-    launch_eigh(ctx, H, nk, dks, db, nullptr);
+    eigh_sharded(ctx, H, nk, dks, db, nullptr);
     dos_dev(ctx, H->n, nk, db, dw, nw, dom, gamma, dd);
     timer_stop(ctx);
     ck(cudaMemcpyAsync(dos, dd, (size_t)nw * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream), "D2H");
@@ -1196,7 +1317,7 @@ int lqm_bands_dos_rho_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
     const double* dw = d_w ? d_w : uniform_weights(ctx, nk);
     double* d_eb = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double)) + 40;
     timer_start(ctx);
-    density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb, d_bands);
+    density_dev(ctx, H, nk, d_ks, dw, mu, T, nL, dL, (double2*)d_rho, d_eb, d_bands, true);
     dos_dev(ctx, H->n, nk, d_bands, d_w, nw, d_omegas, gamma, d_dos);
     timer_stop(ctx);
     double eb = 0.0;

@@ -368,4 +368,67 @@ __global__ void __launch_bounds__(kBlkThreads) blk_scale_f_kernel(int n, int64_t
   }
 }
 
+// Occupation span of each k-point's states (eigenvalues ascending, so the exactly
+// filled states, f == 1, form a prefix and the exactly empty ones, f == 0, a suffix):
+// span[0] = max over k of the states that are not exactly filled, span[1] = max over k
+// of the states that are not exactly empty (integer maxima: order-independent).
+__global__ void __launch_bounds__(kBlkThreads) blk_occ_span_kernel(int n, const double* bands, double mu,
+                                                                   double T_, int* span) {
+  __shared__ int cnt[2];
+  const int64_t k = blockIdx.x;
+  if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  int notfull = 0, notempty = 0;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    const double fj = fermi(bands[k * n + j] - mu, T_);
+    notfull += fj != 1.0;
+    notempty += fj != 0.0;
+  }
+  atomicAdd(&cnt[0], notfull);
+  atomicAdd(&cnt[1], notempty);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicMax(&span[0], cnt[0]);
+    atomicMax(&span[1], cnt[1]);
+  }
+}
+
+// rho_k from the K columns [c0, c0 + K) of U that carry it: Y[:, c] = U[:, c0 + c] f
+// (direct: the first K states hold every nonzero f) or U[:, c0 + c] (1 - f)
+// (complement: the last K states hold every f < 1, rho_k = I - Y U_K^H); the band
+// energy sum_j w f_j eps_j over all states as blk_scale_f_kernel computes it.
+__global__ void __launch_bounds__(kBlkThreads) blk_scale_f_cols_kernel(int n, const double2* U, const double* bands,
+                                                                       double mu, double T_, const double* w,
+                                                                       double2* Y, double* eband_k, int c0, int K,
+                                                                       int complement) {
+  __shared__ double red[128];
+  extern __shared__ __align__(16) unsigned char smem[];
+  double* f = (double*)smem;
+  const Team T = make_team();
+  const int64_t k = blockIdx.x;
+  const int64_t nn = (int64_t)n * n;
+  double eb = 0.0;
+  for (int j = T.tid; j < n; j += T.nt) {
+    const double ej = bands[k * n + j];
+    const double fj = fermi(ej - mu, T_);
+    f[j] = fj;
+    eb += ej * fj;
+  }
+  eb = team_sum(T, eb, red);
+  if (T.tid == 0 && eband_k) eband_k[k] = w[k] * eb;
+  for (int c = T.wid; c < K; c += T.nw) {
+    const double fc = complement ? 1.0 - f[c0 + c] : f[c0 + c];
+    const double2* Uc = U + k * nn + (int64_t)(c0 + c) * n;
+    double2* Yc = Y + k * nn + (int64_t)c * n;
+    for (int r = T.lane; r < n; r += T.nl) Yc[r] = cscale(fc, Uc[r]);
+  }
+}
+
+// rho_k = I - (Y U_K^H): the identity added to the diagonal (complement form).
+__global__ void __launch_bounds__(kBlkThreads) blk_add_identity_kernel(int n, double2* R) {
+  const int64_t nn = (int64_t)n * n;
+  double2* Rk = R + blockIdx.x * nn;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) Rk[i + (int64_t)i * n].x += 1.0;
+}
+
 }  // namespace lqm

@@ -55,6 +55,43 @@ function check(ctx::Context, st::Integer)
     st == -1 ? throw(ArgumentError(msg)) : error("libkspace status $st: $msg")
 end
 
+# ---------------------------------------------------------------- k-point shards over GPUs
+"""
+    comm_unique_id() -> Vector{UInt8}
+
+A communicator id (128 bytes) made on one process and handed to the others (for
+example `MPI.Bcast!` or `Distributed.remotecall`), then passed to [`set_comm!`](@ref).
+"""
+function comm_unique_id()
+    id = zeros(UInt8, 128)
+    st = ccall((:lqm_comm_unique_id, LIB[]), Cint, (Ptr{UInt8},), id)
+    st == 0 || error("libkspace: lqm_comm_unique_id failed (status $st; is libnccl.so.2 loadable?)")
+    id
+end
+
+"""
+    set_comm!(nranks, rank, id; device=0)
+
+Join the k-point shards of `nranks` processes (one GPU each) as `rank` on the
+context of `device`.  Afterwards `getdensitymatrix!`, `bandmatrix`, `getdos`,
+`chemicalpotential` and `solvehartreefock` with `multimode=:cuda` split the k list
+over the ranks (every rank passes the same list) and return the whole-grid result on
+every rank, replacing `DistributedExec` (src/modules/Parallel/Parallel.jl:275-287,415-467).
+`set_comm!(1, 0, nothing)` removes the communicator.
+"""
+function set_comm!(nranks::Integer, rank::Integer, id; device::Int=0)
+    ctx = context(device)
+    if id === nothing
+        check(ctx, ccall((:lqm_ctx_set_comm, LIB[]), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{UInt8}),
+                         ctx.ptr, nranks, rank, C_NULL))
+    else
+        length(id) == 128 || throw(ArgumentError("communicator id must be 128 bytes"))
+        check(ctx, ccall((:lqm_ctx_set_comm, LIB[]), Cint, (Ptr{Cvoid}, Cint, Cint, Ptr{UInt8}),
+                         ctx.ptr, nranks, rank, Vector{UInt8}(id)))
+    end
+    nothing
+end
+
 # ---------------------------------------------------------------- Hops upload
 mutable struct DeviceHops
     ptr::Ptr{Cvoid}

@@ -46,7 +46,8 @@ EXPORTS = [
     "lqm_commutator_norm", "lqm_ctx_set_scf_residual", "lqm_ctx_set_scf_terms", "lqm_ctx_set_scf_exchange",
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
     "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface",
-    "lqm_wilson", "lqm_wilson_wannier", "lqm_ctx_set_eigh_threads", "lqm_autotune_eigh",
+    "lqm_wilson", "lqm_wilson_wannier", "lqm_ctx_set_eigh_threads", "lqm_autotune_eigh", "lqm_ctx_kernel_stats",
+    "lqm_comm_unique_id", "lqm_ctx_set_comm", "lqm_ctx_comm", "lqm_shard_range",
 ]
 
 
@@ -70,6 +71,11 @@ _SIG = {
     "lqm_ctx_destroy": [_P],
     "lqm_ctx_set_timeout": [_P, _D],
     "lqm_ctx_set_blocked_min_n": [_P, _I64],
+    "lqm_ctx_kernel_stats": [_P, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_D)],
+    "lqm_comm_unique_id": [_P],
+    "lqm_ctx_set_comm": [_P, ctypes.c_int, ctypes.c_int, _P],
+    "lqm_ctx_comm": [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+    "lqm_shard_range": [_I64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     "lqm_ctx_last_kernel_ms": [_P, ctypes.POINTER(_D)],
     "lqm_hops_upload_dense": [_P, _I64, _I64, ctypes.c_int32, _P, _P, ctypes.POINTER(_P)],
     "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.POINTER(_P)],
@@ -192,6 +198,32 @@ class Context:
         self.check(_lib.lqm_ctx_stats(self._h, ctypes.byref(ms), ctypes.byref(el), ctypes.byref(al)))
         return ms.value, el.value, al.value
 
+    def set_comm(self, nranks, rank, uid=None):
+        """Join the k-point shards of `nranks` processes (one GPU each) as `rank`, with the
+        communicator id from comm_unique_id() on rank 0 (bytes, shared by the caller);
+        nranks = 1 without an id removes the communicator (with an id: a one-rank
+        communicator, the sharded code path with copies for collectives)."""
+        buf = None
+        if nranks > 1 or uid is not None:
+            if uid is None or len(uid) != COMM_ID_BYTES:
+                raise ValueError(f"communicator id must be {COMM_ID_BYTES} bytes")
+            buf = ctypes.create_string_buffer(bytes(uid), COMM_ID_BYTES)
+        self.check(_lib.lqm_ctx_set_comm(self._h, int(nranks), int(rank), buf))
+
+    def comm(self):
+        """(nranks, rank) of the context's communicator ((1, 0) without one)."""
+        nr, r = ctypes.c_int(), ctypes.c_int()
+        self.check(_lib.lqm_ctx_comm(self._h, ctypes.byref(nr), ctypes.byref(r)))
+        return nr.value, r.value
+
+    def kernel_stats(self, kernel_class):
+        """(device ms, launches, algorithmic bytes) since reset for a kernel class:
+        0 = eigensolver passes, 1 = the blocked path's mat-vec kernel."""
+        ms, nl, by = _D(), _I64(), _D()
+        self.check(_lib.lqm_ctx_kernel_stats(self._h, int(kernel_class), ctypes.byref(ms), ctypes.byref(nl),
+                                             ctypes.byref(by)))
+        return ms.value, nl.value, by.value
+
     def phase_cycles(self):
         """Eigensolver SM cycles per stage: bloch, householder, d&c, back-transform, sync,
         then the d&c merge steps (zsort, deflate, secular, zhat, vectors, ranks, update, copy),
@@ -214,6 +246,27 @@ class Context:
 
 
 _default_ctx = None
+
+
+COMM_ID_BYTES = 128
+
+
+def comm_unique_id():
+    """A new communicator id (bytes) for Context.set_comm; made on one rank and shared."""
+    buf = ctypes.create_string_buffer(COMM_ID_BYTES)
+    st = _lib.lqm_comm_unique_id(buf)
+    if st != LQM_OK:
+        raise LQMError(st, "lqm_comm_unique_id failed (NCCL not loadable?)")
+    return buf.raw
+
+
+def shard_range(nk, nranks, rank):
+    """[k0, k1) of the k list that `rank` of `nranks` processes (host only, no device)."""
+    k0, k1 = _I64(), _I64()
+    st = _lib.lqm_shard_range(int(nk), int(nranks), int(rank), ctypes.byref(k0), ctypes.byref(k1))
+    if st != LQM_OK:
+        raise LQMError(st, "invalid shard arguments")
+    return k0.value, k1.value
 
 
 def default_context():

@@ -6,6 +6,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -105,3 +107,27 @@ def test_scf_nonconvergence_warns_and_raises(lqm):
     with warnings.catch_warnings():
         warnings.simplefilter("error")
         assert lqm._hf_result({}, out, None, True).converged is True
+
+
+def test_shard_ranges_tile_the_k_list_without_a_device(lqm):
+    """lqm_shard_range (host code of the multi-GPU sharding): contiguous shares that
+    tile [0, nk) in rank order, sizes differing by at most one; empty shares when
+    nk < nranks; invalid arguments rejected."""
+    for nk in (0, 1, 3, 7, 576, 1000003):
+        for nr in (1, 2, 3, 8):
+            spans = [lqm.shard_range(nk, nr, r) for r in range(nr)]
+            assert spans[0][0] == 0 and spans[-1][1] == nk
+            assert all(spans[i][1] == spans[i + 1][0] for i in range(nr - 1))
+            sizes = [b - a for a, b in spans]
+            assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 0
+    with pytest.raises(lqm.LQMError):
+        lqm.shard_range(10, 2, 2)
+    with pytest.raises(lqm.LQMError):
+        lqm.shard_range(-1, 2, 0)
+
+
+def test_comm_unique_id_without_a_device(lqm):
+    """NCCL loads at run time and makes a communicator id (no device needed)."""
+    uid = lqm.comm_unique_id()
+    assert isinstance(uid, bytes) and len(uid) == lqm.COMM_ID_BYTES == 128
+    assert lqm.comm_unique_id() != uid
