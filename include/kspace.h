@@ -439,6 +439,31 @@ int lqm_densitymatrix_vjp(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
 int lqm_bands_vjp(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, const double* eps_bar,
                   double* Hbar);
 
+/* Derivatives of the converged Hartree-Fock SCF with respect to the hopping
+ * blocks of h (the functional of src/modules/Meanfield/hartreefock.jl:143-289,392-410
+ * at the fixed point of src/modules/Meanfield/selfconsistent.jl:256-336).  Inputs:
+ * h, v and the converged rho (keys Lkeys, with its chemical potential mu, e.g. from
+ * lqm_scf_hf with the same k-points, weights (NULL: 1/nk), T and the context's
+ * Hartree/Fock switches; no exchange kernel).  Outputs:
+ *   out[5] = {F, Omega_band, N, adjoint residual, adjoint iterations}: the free
+ *     energy F = Omega_band + mu N - (eH + eF) of hMF = hf(rho),
+ *     Omega_band = -T sum_k w_k sum_j log(1 + e^{-(eps_j - mu)/T}) (T = 0: the sum of
+ *     eps_j - mu below mu), N = sum_k w_k sum_j f_j;
+ *   dF_dh (may be NULL): dF/dh_R for the keys of h (n x n x nR(h)), which at
+ *     self-consistency is the density matrix of hMF at those keys (Hellmann-Feynman);
+ *   dL_dh (with eps_bar): for a loss L of the mean-field bands eps(hMF) with band
+ *     cotangent eps_bar (n x nk, dL/d eps_jk), the total derivative dL/dh_R through
+ *     the fixed point, including the chemical potential's response at T > 0: the
+ *     implicit-function adjoint solved by the damped iteration of the SCF's linear
+ *     mixing (beta) until its relative change is below tol or maxiter iterations.
+ * Pairing: dL = Re sum_R <dL_dh_R, dh_R>, <A, B> = sum conj(A) B, for every
+ * Hermitian-consistent perturbation of h.  No reference counterpart (the reference
+ * has no derivatives). */
+int lqm_scf_hf_gradient(lqm_ctx* ctx, const lqm_hops* h, const lqm_hops* v, int64_t nk, const double* ks,
+                        const double* w, double T, double mu, int64_t nL, const int64_t* Lkeys, const double* rho,
+                        const double* eps_bar, double beta, double tol, int64_t maxiter, double* dF_dh,
+                        double* dL_dh, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -238,7 +238,7 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2
 };
 static_assert(WS_UNIW < 48, "workspace slots");
 
@@ -1362,6 +1362,7 @@ int lqm_bands_dos_rho(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double*
 #include "lqm_anderson.inc"
 #include "lqm_scf.inc"
 #include "lqm_adjoint.inc"
+#include "lqm_scfgrad.inc"
 #include "lqm_obs.inc"
 #include "lqm_sitedos.inc"
 #include "lqm_berry.inc"

@@ -47,7 +47,7 @@ EXPORTS = [
     "lqm_ctx_scf_exchange_energy", "lqm_hartreefock_eval", "lqm_bdg_densitymatrix", "lqm_bdg_filling",
     "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface",
     "lqm_wilson", "lqm_wilson_wannier", "lqm_ctx_set_eigh_threads", "lqm_autotune_eigh", "lqm_ctx_kernel_stats",
-    "lqm_comm_unique_id", "lqm_ctx_set_comm", "lqm_ctx_comm", "lqm_shard_range",
+    "lqm_comm_unique_id", "lqm_ctx_set_comm", "lqm_ctx_comm", "lqm_shard_range", "lqm_scf_hf_gradient",
 ]
 
 
@@ -76,6 +76,7 @@ _SIG = {
     "lqm_ctx_set_comm": [_P, ctypes.c_int, ctypes.c_int, _P],
     "lqm_ctx_comm": [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
     "lqm_shard_range": [_I64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
+    "lqm_scf_hf_gradient": [_P, _P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, _P, _D, _D, _I64, _P, _P, _P],
     "lqm_ctx_last_kernel_ms": [_P, ctypes.POINTER(_D)],
     "lqm_hops_upload_dense": [_P, _I64, _I64, ctypes.c_int32, _P, _P, ctypes.POINTER(_P)],
     "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.POINTER(_P)],
@@ -1044,3 +1045,37 @@ def solvehartreefock_bdg(h, v, rho_init, filling, ks, T=0.0, beta=1.0, tol=1e-7,
     rho_out = {L: np.array(rho[:, :, i]) for i, L in enumerate(Lkeys)}
     mf = BdGMFInfo(mu=out[1], eH=out[2], eF=out[3], eP=out[9], eband=out[4], ekin=out[5], iterations=int(out[8]))
     return _hf_result(rho_out, out, mf, convergenceerror)
+
+
+SCFGradient = namedtuple("SCFGradient", ["F", "omega", "N", "dF_dh", "dL_dh", "residual", "iterations"])
+
+
+def scf_hf_gradient(h, v, rho, mu, ks, T=0.0, kweights=None, eps_bar=None, beta=0.3, tol=1e-12, iterations=2000,
+                    hartree=True, fock=True, ctx=None):
+    """Derivatives of a converged Hartree-Fock SCF (``lqm_scf_hf_gradient``): the free
+    energy F of hMF = hf(rho) at mu, dF/dh_R (the density matrix of hMF at the keys of h),
+    and, with ``eps_bar`` (n, nk) the cotangent of the mean-field bands, the total
+    dL/dh_R through the fixed point.  ``rho`` and ``mu`` are the converged density
+    matrix and chemical potential (``solvehartreefock`` with the same ks, T, weights).
+    Gradients are dicts keyed like h, paired as dL = Re sum_R <G_R, dh_R>."""
+    ctx = ctx or default_context()
+    _set_functional(ctx, hartree, fock, None)
+    hd = _as_device_hops(h, ctx)
+    vd = _as_device_hops(v, ctx)
+    ks = _ks(ks, hd.d)
+    nk = ks.shape[1]
+    Lkeys = list(rho.keys())
+    Lk = np.asfortranarray(np.array(Lkeys, dtype=np.int64).T)
+    R = np.asfortranarray(np.stack([np.asarray(rho[L], np.complex128) for L in Lkeys], -1))
+    w = None if kweights is None else np.ascontiguousarray(kweights, dtype=np.float64)
+    hkeys = list(hd.keys) if isinstance(h, DeviceHops) else [tuple(k) for k in h.keys()]
+    dF = np.zeros((hd.n, hd.n, len(hkeys)), dtype=np.complex128, order="F")
+    eb = None if eps_bar is None else np.asfortranarray(np.asarray(eps_bar, dtype=np.float64))
+    dL = np.zeros_like(dF) if eb is not None else None
+    out = np.zeros(5)
+    ctx.check(_lib.lqm_scf_hf_gradient(ctx.handle, hd.handle, vd.handle, nk, _ptr(ks), _ptr(w), float(T), float(mu),
+                                       len(Lkeys), _ptr(Lk), _ptr(R), _ptr(eb), float(beta), float(tol),
+                                       int(iterations), _ptr(dF), _ptr(dL), _ptr(out)))
+    dFd = {Rk: np.array(dF[:, :, i]) for i, Rk in enumerate(hkeys)}
+    dLd = None if dL is None else {Rk: np.array(dL[:, :, i]) for i, Rk in enumerate(hkeys)}
+    return SCFGradient(out[0], out[1], out[2], dFd, dLd, out[3], int(out[4]))

@@ -91,3 +91,85 @@ def hermitian_direction(h, rng):
 def pairing(A, B):
     """Re sum_R <A_R, B_R>."""
     return float(sum(np.real(np.vdot(A[R], B[R])) for R in A if R in B))
+
+
+# ---------------------------------------------------------------- converged Hartree-Fock SCF
+def grand_potential(bands, w, mu, T):
+    """Omega_band = -T sum_k w_k sum_j log(1 + e^{-(eps_j - mu)/T}) (T = 0: sum of eps - mu
+    below mu) and N = sum_k w_k sum_j f_j, for bands (n, nk)."""
+    x = bands - mu
+    if T > 0:
+        y = x / T
+        om = -T * np.where(y > 0, np.log1p(np.exp(-np.abs(y))), -y + np.log1p(np.exp(-np.abs(y))))
+    else:
+        om = np.minimum(x, 0.0)
+    f = K.fermidirac(bands, mu, T)
+    return float(np.sum(w[None, :] * om)), float(np.sum(w[None, :] * f))
+
+
+def free_energy(hf, ks, w, mu, T):
+    """F = Omega_band(hMF) + mu N - (eH + eF + eJ) of a HartreeFock evaluated at rho
+    (Meanfield/hartreefock.jl:236 double counting; the Mermin free energy of the
+    mean-field bands at the filling's chemical potential)."""
+    bands, _ = K.bandmatrix(hf.hMF, ks)
+    om, ne = grand_potential(bands, w, mu, T)
+    return om + mu * ne - hf.doublecounting(), om, ne
+
+
+def hf_transpose(hf, gbar, rho_keys):
+    """Phi^T of the linear part of hMF(rho): Fock -v .* rho at the keys of v present in rho
+    (cotangent -conj(v_L) .* gbar_L), Hartree diag(V0 diag rho_0) (cotangent on the
+    diagonal of rho_0: Re sum_i conj(V0[i, j]) gbar_0[i, i]); Meanfield/hartreefock.jl:247-289."""
+    n = hf.V0.shape[0]
+    out = {L: np.zeros((n, n), complex) for L in rho_keys}
+    if hf.fock:
+        for L in rho_keys:
+            if L in hf.v and L in gbar:
+                out[L] = -np.conj(hf.v[L]) * gbar[L]
+    z = tuple(0 for _ in next(iter(rho_keys)))
+    if hf.hartree:
+        s = np.real(np.conj(hf.V0).T @ np.diag(gbar[z]))
+        out[z] = out[z] + np.diag(s)
+    return out
+
+
+def scf_band_loss_gradient(h, v, ks, w, mu, T, rho, eps_bar, beta=0.3, tol=1e-12, maxiter=2000):
+    """dL/dh_R through the converged SCF for a loss of the mean-field bands (cotangent
+    eps_bar, (n, nk)): gbar = bands VJP at hMF, z = D'^T Phi^T (gbar + z) with
+    D'^T(G) = VJP_mu(G) - (Re tr VJP_mu(G)_0 / Re tr Nbar_0) Nbar, Nbar the cotangent of
+    the electron count, solved by damped iteration; returns (gbar + z on the keys of h,
+    residual, iterations)."""
+    from .meanfield import HartreeFock
+    hf = HartreeFock(h, v)
+    hf(rho)
+    hmf = hf.hMF
+    z0 = tuple(0 for _ in next(iter(h)))
+    gbar = bands_vjp(hmf, ks, eps_bar)
+    if T > 0:
+        bands, _ = K.bandmatrix(hmf, ks)
+        x = bands - mu
+        fm = K.fermidirac(bands, mu, T)
+        slope = -fm * (1.0 - fm) / T
+        Nbar = bands_vjp(hmf, ks, w[None, :] * slope)
+        c = float(np.real(np.trace(Nbar[z0])))
+    else:
+        Nbar, c = None, 0.0
+    z = {R: np.zeros_like(M) for R, M in gbar.items()}
+    res, it = np.inf, 0
+    for it in range(1, maxiter + 1):
+        gin = {R: gbar[R] + z[R] for R in gbar}
+        rbar = hf_transpose(hf, gin, list(rho.keys()))
+        Hb = densitymatrix_vjp(hmf, ks, w, mu, T, rbar)
+        t = float(np.real(np.trace(Hb[z0])))
+        r = t / c if c != 0.0 else 0.0
+        dn = nz = 0.0
+        for R in z:
+            zn = Hb[R] - (r * Nbar[R] if Nbar is not None else 0.0)
+            y = (1 - beta) * z[R] + beta * zn
+            dn += np.sum(np.abs(y - z[R]) ** 2)
+            nz += np.sum(np.abs(y) ** 2)
+            z[R] = y
+        res = math.sqrt(dn) / math.sqrt(nz) if nz > 0 else math.sqrt(dn)
+        if res < tol:
+            break
+    return {R: gbar[R] + z[R] for R in h}, res, it

@@ -7,8 +7,11 @@ NNN t' = 0.2, U = 4 in the sigma_x mode; seeded random local magnetisation
 beta = 0.3, stopped at the relative residual 1e-9 (the reference's
 _scf_driver!/fixedpoint!, restated in oracle/meanfield.py).
 
-The oracle takes ~5 s per iteration on one core (1296 k-points, two eigen
-passes), so the run is done once here and its result committed:
+The oracle's SCF loop (oracle/meanfield.py) runs with its k-loops (eigenvalues
+for mu, then the density matrix) computed by the oracle's C++/OpenMP
+restatement (oracle/cpu.py, the same per-k zheevr, rho_k and fold; pinned to the
+Python k-loop in tests/test_oracle_pins.py), ~0.4 s per iteration on 8 cores
+instead of ~3 s; the run is done once here and its result committed:
 
     OPENBLAS_NUM_THREADS=1 python tests/golden/make_scf_c4.py
 
@@ -33,7 +36,7 @@ from lqm_workloads import models as M  # noqa: E402
 from oracle import meanfield as MF  # noqa: E402
 
 OUT = os.path.join(HERE, "scf_c4_oracle.npz")
-PARAMS = dict(L_super=6, seed=7, nk_side=36, T=0.02, filling=0.5, beta=0.3, tol=1e-9, iterations=600)
+PARAMS = dict(L_super=6, seed=7, nk_side=36, T=0.02, filling=0.5, beta=0.3, tol=1e-9, maxiter=600)
 
 
 def main():
@@ -46,8 +49,12 @@ def main():
     def log(it, E, res, *rest):
         print(f"iter {it:4d}  E {E:.15f}  residual {res:.3e}  ({time.time() - t0:.0f} s)", flush=True)
 
+    from oracle import cpu as C
+    from oracle import kspace as K
+    K.bandmatrix = lambda hh, kk, vectors=False: (C.bandmatrix(hh, kk), None)
+    K.densitymatrix = lambda hh, kk, w, mu, T, Lk, return_parts=False: C.densitymatrix(hh, kk, w, mu, T, Lk)
     rho, E, hf, conv, resid, it = MF.solvehartreefock(h, v, rho0, p["filling"], ks, T=p["T"], beta=p["beta"],
-                                                      tol=p["tol"], iterations=p["iterations"], log=log)
+                                                      tol=p["tol"], iterations=p["maxiter"], log=log)
     np.savez_compressed(OUT, rho0=rho[(0, 0)], E=E, mu=hf.mu, residual=resid, iterations=it, converged=conv,
                         eband=hf.eband, eH=hf.eH, eF=hf.eF, **{k: v for k, v in p.items()})
     print(f"wrote {OUT}: converged={conv} iterations={it} residual={resid:.3e} E={E:.15f} mu={hf.mu:.15f}")

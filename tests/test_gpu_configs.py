@@ -50,7 +50,7 @@ def test_c4_hubbard_scf_converged_matches_oracle(lqm, ctx):
     rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=int(g["seed"]))}
     ks = L.regulargrid(int(g["nk_side"]) ** 2)
     res = lqm.solvehartreefock(h, v, rho0, float(g["filling"]), ks, T=float(g["T"]), beta=float(g["beta"]),
-                               tol=float(g["tol"]), iterations=int(g["iterations"]) + 50, ctx=ctx)
+                               tol=float(g["tol"]), iterations=int(g["maxiter"]), ctx=ctx)
     assert res.converged and res.residual < 1e-9
     # the same trajectory: the device SCF stops within a step of the oracle's count
     assert abs(res.mf.iterations - int(g["iterations"])) <= 1

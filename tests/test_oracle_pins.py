@@ -657,3 +657,24 @@ def test_hubbard_one_sided_neighbors_get_hermitian_partners():
         assert np.array_equal(one[mR], one[R].conj().T)
     far = M.hubbard_v(lat, U=2.0, a=0.5, neighbors=[(0, 0), (3, 0)])  # no pair within a = 0.5 at 3 cells
     assert set(far) == {(0, 0)}
+
+
+def test_cpp_kloop_matches_python_oracle():
+    """oracle/cpu_kspace.cpp (the C++/OpenMP restatement used as the timed CPU baseline and
+    to generate the converged-SCF fixture) against the Python k-loop: bands, rho_L and the
+    band energy, with and without weights, T > 0 and T = 0."""
+    from oracle import cpu as C
+    for name, h in M.batch_models()[:2] + [("c1", M.honeycomb_disorder()[1])]:
+        ks = np.hstack([L.regulargrid(5 * 5), np.random.default_rng(3).random((2, 7))])
+        nk = ks.shape[1]
+        keys = list(h.keys())
+        for w, T in ((np.full(nk, 1.0 / nk), 0.01), (np.random.default_rng(4).random(nk), 0.0)):
+            r1, e1, b1 = C.densitymatrix(h, ks, w, 0.1, T, keys, want_bands=True)
+            r2, e2 = K.densitymatrix(h, ks, w, 0.1, T, keys)
+            assert max(np.max(np.abs(r1[R] - r2[R])) for R in keys) < 1e-12, name
+            assert abs(e1 - e2) < 1e-12 * max(1.0, abs(e2)), name
+            b2, _ = K.bandmatrix(h, ks)
+            assert np.max(np.abs(b1 - b2)) < 1e-12 and np.max(np.abs(C.bandmatrix(h, ks) - b2)) < 1e-12, name
+        r3, _ = C.densitymatrix(h, ks, None, 0.1, 0.01, keys)
+        r4, _ = K.densitymatrix(h, ks, np.full(nk, 1.0 / nk), 0.1, 0.01, keys)
+        assert max(np.max(np.abs(r3[R] - r4[R])) for R in keys) < 1e-12, name
