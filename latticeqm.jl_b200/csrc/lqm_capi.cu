@@ -1,6 +1,8 @@
 // C ABI of libkspace (declared in include/kspace.h).  Host side: argument
 // validation, device buffers, the k-batch loop and kernel launches.
 #include <cublas_v2.h>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,6 +89,10 @@ struct lqm_ctx {
   // from milliseconds to most of a second per call on B200
   std::vector<std::pair<void*, size_t>> hops_cache;
   size_t hops_cache_bytes = 0;
+  // device error word set by kernels whose waits are bounded (the TMA mat-vec);
+  // wait_stream reads it once such a kernel has been launched since the last check
+  int* d_err = nullptr;
+  bool err_armed = false;
   // NCCL communicator of the k-point shards (lqm_ctx_set_comm; lqm_comm.inc)
   void* comm = nullptr;
   int comm_nranks = 1, comm_rank = 0;
@@ -177,6 +183,15 @@ void wait_stream(lqm_ctx* ctx) {
   }
   ck(cudaGetLastError(), "kernel launch");
   collect_stats(ctx);
+  if (ctx->err_armed && ctx->d_err) {
+    ctx->err_armed = false;
+    int e = 0;
+    ck(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+    if (e != 0) {
+      ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "error word");
+      fail(LQM_EDEVICE, "a device-side wait gave up (TMA copy not completed within its limit)");
+    }
+  }
 }
 
 std::pair<cudaEvent_t, cudaEvent_t> stat_events(lqm_ctx* ctx) {
@@ -353,6 +368,31 @@ bool use_blocked(const lqm_ctx* ctx, int n, int nR);
 // zlatrd panels (column kernels + batched rank-2nb updates), divide and
 // conquer per k, compact-WY back-transformation and rho_k = U f U^H as batched
 // GEMMs.  k-points are processed in batches sized to ~24 GB of work buffers.
+// TMA descriptor of a batch of B matrices (n x n complex, column-major, contiguous):
+// 3-D (2n doubles, n columns, B k-points), box 16 doubles (8 complex rows) x 64
+// columns x 1, 128-byte swizzle, zero fill out of bounds.  cuTensorMapEncodeTiled is
+// taken from the driver through the runtime (no link-time libcuda dependency).
+bool make_symv_map(CUtensorMap* map, const double2* A, int n, int64_t B) {
+  static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    cudaGetLastError();
+  });
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)(2 * n), (cuuint64_t)n, (cuuint64_t)B};
+  const cuuint64_t strides[2] = {(cuuint64_t)n * 16, (cuuint64_t)n * n * 16};
+  const cuuint32_t box[3] = {16, (cuuint32_t)kSymvTB, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)A, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, double* d_bands,
                        double2* d_U, double2* rhok, double* ebk, const double* w, double mu, double T) {
   NvtxRange nvtx_("eigen pass (blocked)");
@@ -387,6 +427,16 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   cublasHandle_t h = blas_handle(ctx);
   ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
      "smem attr");
+  ck(cudaFuncSetAttribute(blk_symv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvTmaSmem),
+     "smem attr");
+  // the mat-vec moves its tiles by TMA from n = 64 on (the descriptor covers the batch)
+  CUtensorMap symv_map;
+  const char* pipe_env = std::getenv("LQM_SYMV_PIPE");
+  const bool symv_tma = n >= 64 && !(pipe_env && pipe_env[0] == '1') && make_symv_map(&symv_map, A, n, B);
+  if (symv_tma && !ctx->d_err) {
+    ck(cudaMalloc(&ctx->d_err, sizeof(int)), "cudaMalloc(error word)");
+    ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "memset(error word)");
+  }
   ck(cudaFuncSetAttribute(dc_large_kernel<kDcThreads, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           dc_tile_smem(n)),
      "smem attr");
@@ -412,7 +462,13 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           const int64_t grid = std::min<int64_t>(nitems, (int64_t)ctx->num_sms);
           std::pair<cudaEvent_t, cudaEvent_t> sev{};
           if (ctx->stats_on) { sev = stat_events(ctx); ck(cudaEventRecord(sev.first, ctx->stream), "event"); }
-          blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
+          if (symv_tma) {
+            blk_symv_tma_kernel<<<(unsigned)grid, kSymvTmaThreads, kSymvTmaSmem, ctx->stream>>>(symv_map, ba, j,
+                                                                                           nitems, ctx->d_err);
+            ctx->err_armed = true;
+          } else {
+            blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
+          }
           ctx->launches++;
           if (ctx->stats_on) {
             ck(cudaEventRecord(sev.second, ctx->stream), "event");
@@ -814,6 +870,7 @@ int lqm_ctx_destroy(lqm_ctx* ctx) {
   for (auto& kv : ctx->plans) cudaFree(kv.second.d_buf);
   for (auto& b : ctx->hops_cache) cudaFree(b.first);
   if (ctx->d_phase) cudaFree(ctx->d_phase);
+  if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->blas) cublasDestroy(ctx->blas);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);

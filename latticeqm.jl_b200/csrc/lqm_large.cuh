@@ -15,6 +15,8 @@
 //   (host)              U = (I - V T V^H) U per panel, batched ZGEMMs
 //   blk_scale_f_kernel  Y = U diag(f), band energy; (host) rho_k = Y U^H
 #pragma once
+#include <cuda.h>
+
 #include "lqm_blocked.cuh"
 #include "lqm_kernels.cuh"
 
@@ -239,6 +241,187 @@ __global__ void __launch_bounds__(kSymvThreads, 1) blk_symv_pipe_kernel(BlkArgs 
     stage = (stage + 1) % kSymvStages;
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ---- Hermitian mat-vec of one column, tiles moved by TMA ----
+// The same partial layout as blk_symv_pipe_kernel, with each 64 x 64 lower tile
+// brought into shared memory by eight 3-D tensor copies (cp.async.bulk.tensor:
+// box = 8 complex rows x 64 columns x 1 k-point, 128-byte swizzle) that complete
+// on one mbarrier per stage, issued by one thread; rows and columns beyond the
+// matrix read as zeros (out-of-bounds fill), so the tensor map covers the whole
+// batch for every column.  Thread (q', g), q' < 32, g < 16, owns rows q' and
+// q' + 32 of the direct product and the same two columns of the transposed
+// product over u = g + 16 h; with the swizzle both reads are free of bank
+// conflicts.  The 16 partial sums of a row are added by shuffles, and lane g == 0
+// writes them: one block barrier per tile.  Every mbarrier wait is bounded; on
+// expiry the kernel sets *err and stops (the host reports LQM_EDEVICE).
+constexpr int kSymvTmaThreads = 512;
+constexpr int kSymvTmaStages = 3;
+constexpr int kSymvTileBytes = kSymvTB * kSymvTB * 16;  // 64 KB
+constexpr int kSymvTmaSmem = kSymvTmaStages * kSymvTileBytes + 1024 /* alignment */ + 64 /* mbarriers */;
+static_assert(kSymvTmaSmem <= 227 * 1024, "TMA mat-vec pipeline exceeds shared memory");
+constexpr long long kSymvWaitLimit = 1LL << 22;  // mbarrier polls before giving up (well under a second)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// bounded wait: false when the limit ran out
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  for (long long i = 0; i < kSymvWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                            unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(dst),
+      "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+      : "memory");
+}
+
+// byte offset of element (row r, column c) of a staged tile (eight swizzled boxes)
+__device__ __forceinline__ int symv_sw(int r, int c) {
+  return ((r >> 3) << 13) + (c << 7) + ((((r & 7) ^ (c & 7))) << 4);
+}
+
+__device__ __forceinline__ void symv_tma_issue(const CUtensorMap* map, int j, int ntiles, int64_t it, unsigned dst,
+                                               unsigned bar) {
+  const int64_t b = it / ntiles;
+  int R, C;
+  symv_tile_rc((int)(it - b * ntiles), &R, &C);
+  mbar_arrive_expect_tx(bar, (unsigned)kSymvTileBytes);
+  const int row0 = j + 1 + R * kSymvTB, col0 = j + 1 + C * kSymvTB;
+#pragma unroll
+  for (int bx = 0; bx < kSymvTB / 8; ++bx)
+    tma_load_3d(dst + (unsigned)(bx << 13), map, 2 * (row0 + 8 * bx), col0, (int)b, bar);
+}
+
+__global__ void __launch_bounds__(kSymvTmaThreads, 1)
+    blk_symv_tma_kernel(const __grid_constant__ CUtensorMap map, BlkArgs a, int j, int64_t nitems, int* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const unsigned raw = smem_u32(smem_raw);
+  const unsigned base = (raw + 1023u) & ~1023u;                // 1024-byte aligned tiles (128-byte swizzle)
+  unsigned char* tiles = smem_raw + (base - raw);
+  const unsigned bars = base + kSymvTmaStages * kSymvTileBytes;  // one mbarrier per stage
+  const int m = a.n - j - 1;
+  const int nbk = (m + kSymvTB - 1) / kSymvTB;
+  const int ntiles = nbk * (nbk + 1) / 2;
+  const int64_t first = blockIdx.x, step = gridDim.x;
+  const int g = threadIdx.x & 15, qp = threadIdx.x >> 4;
+  if (*(volatile int*)err != 0) return;  // an earlier launch gave up: the pass is void, end at once
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kSymvTmaStages; ++s) mbar_init(bars + 8 * s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kSymvTmaStages - 1; ++s) {
+      const int64_t it = first + s * step;
+      if (it < nitems) symv_tma_issue(&map, j, ntiles, it, base + s * kSymvTileBytes, bars + 8 * s);
+    }
+  }
+  const double2* vcol = a.A + (j + 1) + (int64_t)j * a.n;  // reflector column j of k-point 0
+  int stage = 0;
+  unsigned parity = 0;
+  for (int64_t it = first; it < nitems; it += step) {
+    const int64_t b = it / ntiles;
+    int R, C;
+    symv_tile_rc((int)(it - b * ntiles), &R, &C);
+    const int x0 = R * kSymvTB, y0 = C * kSymvTB;
+    const double2* v = vcol + b * (int64_t)a.n * a.n;
+    double2 vr[4], vc[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const int u = g + 16 * h;
+      vr[h] = (x0 + u < m) ? v[x0 + u] : cmk(0.0, 0.0);
+      vc[h] = (y0 + u < m) ? v[y0 + u] : cmk(0.0, 0.0);
+    }
+    // the stage's copies have landed, and every thread is past the previous tile (so
+    // its stage may be refilled); the verdict of the bounded wait is the block's
+    const int ok = __syncthreads_and(mbar_wait_bounded(bars + 8 * stage, parity) ? 1 : 0);
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        // leave no copy in flight: the stage of this item and, if issued, the next one
+        mbar_wait_bounded(bars + 8 * stage, parity);
+        if (it + step < nitems) {
+          const int s1 = (stage + 1) % kSymvTmaStages;
+          mbar_wait_bounded(bars + 8 * s1, s1 == 0 ? parity ^ 1u : parity);
+        }
+      }
+      break;
+    }
+    if (threadIdx.x == 0) {
+      const int64_t nx = it + (kSymvTmaStages - 1) * step;
+      const int ns = (stage + kSymvTmaStages - 1) % kSymvTmaStages;
+      if (nx < nitems) symv_tma_issue(&map, j, ntiles, nx, base + ns * kSymvTileBytes, bars + 8 * ns);
+    }
+    const unsigned char* ts = tiles + stage * kSymvTileBytes;
+    const bool diag = (R == C);
+    double2 yd0 = cmk(0.0, 0.0), yd1 = yd0, yt0 = yd0, yt1 = yd0;
+    const int r0 = qp, r1 = qp + 32;
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const int u = g + 16 * h;
+      double2 d0 = *(const double2*)(ts + symv_sw(r0, u));
+      double2 d1 = *(const double2*)(ts + symv_sw(r1, u));
+      double2 t0 = *(const double2*)(ts + symv_sw(u, r0));
+      double2 t1 = *(const double2*)(ts + symv_sw(u, r1));
+      if (diag) {  // lower part only: direct uses u <= row (diagonal real), transposed u > column
+        if (u > r0) d0 = cmk(0.0, 0.0); else if (u == r0) d0.y = 0.0;
+        if (u > r1) d1 = cmk(0.0, 0.0); else if (u == r1) d1.y = 0.0;
+        if (u <= r0) t0 = cmk(0.0, 0.0);
+        if (u <= r1) t1 = cmk(0.0, 0.0);
+      }
+      yd0 = cadd(yd0, cmul(d0, vc[h]));
+      yd1 = cadd(yd1, cmul(d1, vc[h]));
+      yt0 = cadd(yt0, cmulc(t0, vr[h]));
+      yt1 = cadd(yt1, cmulc(t1, vr[h]));
+    }
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {
+      yd0.x += __shfl_xor_sync(0xffffffffu, yd0.x, o);
+      yd0.y += __shfl_xor_sync(0xffffffffu, yd0.y, o);
+      yd1.x += __shfl_xor_sync(0xffffffffu, yd1.x, o);
+      yd1.y += __shfl_xor_sync(0xffffffffu, yd1.y, o);
+      yt0.x += __shfl_xor_sync(0xffffffffu, yt0.x, o);
+      yt0.y += __shfl_xor_sync(0xffffffffu, yt0.y, o);
+      yt1.x += __shfl_xor_sync(0xffffffffu, yt1.x, o);
+      yt1.y += __shfl_xor_sync(0xffffffffu, yt1.y, o);
+    }
+    if (g == 0) {
+      double2* part = a.part + b * a.part_stride;
+      if (diag) {
+        double2* pd = part + ((int64_t)R * nbk + C) * kSymvTB;
+        pd[r0] = cadd(yd0, yt0);
+        pd[r1] = cadd(yd1, yt1);
+      } else {
+        double2* pd = part + ((int64_t)R * nbk + C) * kSymvTB;
+        double2* pt = part + ((int64_t)C * nbk + R) * kSymvTB;
+        pd[r0] = yd0;
+        pd[r1] = yd1;
+        pt[r0] = yt0;
+        pt[r1] = yt1;
+      }
+    }
+    stage = (stage + 1) % kSymvTmaStages;
+    if (stage == 0) parity ^= 1u;
+  }
 }
 
 __global__ void __launch_bounds__(kBlkThreads) blk_prep_kernel(int n, double2* A) {
