@@ -15,7 +15,7 @@ LIB = os.path.join(LIBDIR, "libkspace.so")
 SOURCES = ["lqm_capi.cu"]
 DEPS = ["lqm_capi.cu", "lqm_kernels.cuh", "lqm_eigh.cuh", "lqm_team.cuh", "lqm_hf.cuh", "lqm_scf.inc", "lqm_plan.h",
         "lqm_blocked.cuh", "lqm_large.cuh", "lqm_adjoint.inc", "lqm_obs.inc", "lqm_anderson.inc",
-        "lqm_sitedos.inc", "lqm_berry.inc", "lqm_kubo.inc", "lqm_partial.inc", "lqm_commutator.inc", "lqm_bdg.inc", "lqm_scf_bdg.inc", "lqm_autotune.inc", "lqm_comm.inc", "lqm_scfgrad.inc"]
+        "lqm_sitedos.inc", "lqm_berry.inc", "lqm_kubo.inc", "lqm_partial.inc", "lqm_commutator.inc", "lqm_bdg.inc", "lqm_scf_bdg.inc", "lqm_autotune.inc", "lqm_comm.inc", "lqm_scfgrad.inc", "lqm_zgemm.cuh"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -45,7 +45,7 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-I", CSRC, "-I", os.path.join(ROOT, "include"),
-           *[os.path.join(CSRC, s) for s in SOURCES], "-L", CUDA_LIB, "-lcublas",
+           *[os.path.join(CSRC, s) for s in SOURCES], "-L", CUDA_LIB,
            "-Xlinker", "-rpath=" + CUDA_LIB, "-o", LIB + ".tmp"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -1,11 +1,11 @@
 // C ABI of libkspace (declared in include/kspace.h).  Host side: argument
 // validation, device buffers, the k-batch loop and kernel launches.
-#include <cublas_v2.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
@@ -24,6 +24,7 @@
 #include "lqm_kernels.cuh"
 #include "lqm_large.cuh"
 #include "lqm_hf.cuh"
+#include "lqm_zgemm.cuh"
 #include "lqm_plan.h"
 
 using namespace lqm;
@@ -71,7 +72,6 @@ struct lqm_ctx {
   int64_t symv_launches = 0;
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
-  cublasHandle_t blas = nullptr;          // batched GEMMs of the blocked large-n path
   int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: the default switch)
   int scf_anderson_depth = 0;             // SCF acceleration: 0 linear mixing, > 0 Anderson history depth
   int scf_residual = 0;                   // SCF residual: 0 relative density change, 1 commutator norm
@@ -253,7 +253,7 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_LBLAS, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2
 };
 static_assert(WS_UNIW < 48, "workspace slots");
 
@@ -338,27 +338,43 @@ struct RhoOut {
 };
 
 // ---- blocked large-n path (lqm_large.cuh) ----
-void blas_ck(cublasStatus_t st, const char* what) {
-  if (st != CUBLAS_STATUS_SUCCESS) fail(st == CUBLAS_STATUS_ALLOC_FAILED ? LQM_ENOMEM : LQM_ECUDA, "%s: cuBLAS status %d", what, (int)st);
+// The queue of the library's batched GEMMs: the context's stream.
+cudaStream_t blas_handle(lqm_ctx* ctx) { return ctx->stream; }
+
+template <int BM, int BN, int WM, int WN>
+void launch_zgemm_dmma(cudaStream_t st, const GemmArgs& g, int batch) {
+  constexpr int nt = (BM / WM) * (BN / WN) * 32;
+  constexpr int smem = zgemm_smem_bytes<BM, BN, WM, WN>();
+  static std::atomic<unsigned long long> attr_done{0};  // devices on which the smem limit is raised
+  int dev = 0;
+  ck(cudaGetDevice(&dev), "cudaGetDevice");
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_done.load() & bit)) {
+    ck(cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+       "smem attr");
+    attr_done.fetch_or(bit);
+  }
+  const dim3 grid((unsigned)((g.m + BM - 1) / BM), (unsigned)((g.n + BN - 1) / BN), (unsigned)batch);
+  zgemm_dmma_kernel<BM, BN, WM, WN><<<grid, nt, smem, st>>>(g);
 }
 
-cublasHandle_t blas_handle(lqm_ctx* ctx) {
-  if (!ctx->blas) blas_ck(cublasCreate(&ctx->blas), "cublasCreate");
-  blas_ck(cublasSetStream(ctx->blas, ctx->stream), "cublasSetStream");
-  const size_t wsb = (size_t)32 << 20;  // fixed workspace: no allocation inside captured sequences
-  blas_ck(cublasSetWorkspace(ctx->blas, ws_get(ctx, WS_LBLAS, wsb), wsb), "cublasSetWorkspace");
-  return ctx->blas;
-}
-
-// C_b = alpha op(A_b) op(B_b) + beta C_b for b < batch (column-major, strided).
-void zgemm_sb(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, double alpha_re,
-              const double2* A, int lda, long long sA, const double2* B, int ldb, long long sB, double beta_re,
-              double2* C, int ldc, long long sC, int batch) {
+// C_b = alpha op(A_b) op(B_b) + beta C_b for b < batch (column-major, strided):
+// the library's DMMA kernel (lqm_zgemm.cuh), with the tile shape chosen by the
+// product's shape (skinny n: the Fourier fold; small m: the back-transformation's
+// panel products).
+void zgemm_sb(cudaStream_t h, GemmOp ta, GemmOp tb, int m, int n, int k, double alpha_re, const double2* A, int lda,
+              long long sA, const double2* B, int ldb, long long sB, double beta_re, double2* C, int ldc, long long sC,
+              int batch) {
   if (m <= 0 || n <= 0 || batch <= 0) return;
-  const cuDoubleComplex al = make_cuDoubleComplex(alpha_re, 0.0), be = make_cuDoubleComplex(beta_re, 0.0);
-  blas_ck(cublasZgemmStridedBatched(h, ta, tb, m, n, k, &al, (const cuDoubleComplex*)A, lda, sA,
-                                    (const cuDoubleComplex*)B, ldb, sB, &be, (cuDoubleComplex*)C, ldc, sC, batch),
-          "cublasZgemmStridedBatched");
+  if (batch > 65535) fail(LQM_EINVAL, "GEMM batch %d exceeds the grid limit", batch);
+  GemmArgs g{m, n, k, alpha_re, beta_re, A, lda, sA, B, ldb, sB, C, ldc, sC, (int)ta, (int)tb};
+  if (n <= 16)
+    launch_zgemm_dmma<64, 16, 16, 16>(h, g, batch);
+  else if (m <= 32)
+    launch_zgemm_dmma<32, 64, 32, 16>(h, g, batch);
+  else
+    launch_zgemm_dmma<64, 64, 32, 16>(h, g, batch);
+  ck(cudaGetLastError(), "zgemm launch");
 }
 
 struct RhoOut;
@@ -424,7 +440,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   double* ee = dd + B * (int64_t)n;                   // B x n
   double* slots = (double*)ws_get(ctx, WS_LDC, (size_t)G * slotd * sizeof(double));
   const DCPlan& plan = get_plan(ctx, n);
-  cublasHandle_t h = blas_handle(ctx);
+  cudaStream_t h = blas_handle(ctx);
   ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
      "smem attr");
   ck(cudaFuncSetAttribute(blk_symv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvTmaSmem),
@@ -496,9 +512,9 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           double2* Cb = A + (j0 + nbp + c0) + (int64_t)(j0 + nbp + c0) * n;
           const double2* Vr = A + (j0 + nbp + c0) + (int64_t)j0 * n;
           const double2* Wr = W + (j0 + nbp + c0);
-          zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, rows, cw, nbp, -1.0, Vr, n, nn, Wr, n, (long long)n * nb, 1.0, Cb, n,
+          zgemm_sb(h, OP_N, OP_C, rows, cw, nbp, -1.0, Vr, n, nn, Wr, n, (long long)n * nb, 1.0, Cb, n,
                    nn, nbk);
-          zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, rows, cw, nbp, -1.0, Wr, n, (long long)n * nb, Vr, n, nn, 1.0, Cb, n,
+          zgemm_sb(h, OP_N, OP_C, rows, cw, nbp, -1.0, Wr, n, (long long)n * nb, Vr, n, nn, 1.0, Cb, n,
                    nn, nbk);
           ctx->launches += 2;
         }
@@ -553,11 +569,11 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
       double2* Us = Ucur + (j0 + 1) + (int64_t)c0 * n;
       // X = V^H Us (nbr x K), Y = Tm X, Us -= V Y
-      zgemm_sb(h, CUBLAS_OP_C, CUBLAS_OP_N, nbr, K, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nb, (long long)n * nb,
+      zgemm_sb(h, OP_C, OP_N, nbr, K, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nb, (long long)n * nb,
                nbk);
-      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, nbr, K, nbr, 1.0, Tm + (int64_t)p * nb * nb, nb,
+      zgemm_sb(h, OP_N, OP_N, nbr, K, nbr, 1.0, Tm + (int64_t)p * nb * nb, nb,
                (long long)nb * nb * P, W, nb, (long long)n * nb, 0.0, Yb, nb, (long long)n * nb, nbk);
-      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_N, m, K, nbr, -1.0, V, n, nn, Yb, nb, (long long)n * nb, 1.0, Us, n, nn,
+      zgemm_sb(h, OP_N, OP_N, m, K, nbr, -1.0, V, n, nn, Yb, nb, (long long)n * nb, 1.0, Us, n, nn,
                nbk);
       ctx->launches += 3;
     }
@@ -566,7 +582,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           n, Ucur, d_bands + k0 * n, mu, T, w + k0, A, ebk + k0, c0, K, complement ? 1 : 0);
       ctx->launches++;
       if (K > 0) {
-        zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, K, complement ? -1.0 : 1.0, A, n, nn, Ucur + (int64_t)c0 * n,
+        zgemm_sb(h, OP_N, OP_C, n, n, K, complement ? -1.0 : 1.0, A, n, nn, Ucur + (int64_t)c0 * n,
                  n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
         ctx->launches++;
       } else {
@@ -579,7 +595,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     } else if (rhok) {
       blk_scale_f_kernel<<<nbk, kBlkThreads, n * sizeof(double), ctx->stream>>>(
           n, nbk, Ucur, d_bands + k0 * n, mu, nullptr, T, w + k0, A, ebk + k0);
-      zgemm_sb(h, CUBLAS_OP_N, CUBLAS_OP_C, n, n, n, 1.0, A, n, nn, Ucur, n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
+      zgemm_sb(h, OP_N, OP_C, n, n, n, 1.0, A, n, nn, Ucur, n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
       ctx->launches += 2;
     }
     ck(cudaGetLastError(), "back-transformation launch");
@@ -661,7 +677,7 @@ int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
 void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const double2* coef, int nL,
                  double2* d_rho, int accumulate) {
   NvtxRange nvtx_("rho fold");
-  zgemm_sb(blas_handle(ctx), CUBLAS_OP_N, CUBLAS_OP_T, (int)nn, nL, (int)nb, 1.0, rk, (int)nn, 0, coef, nL, 0,
+  zgemm_sb(blas_handle(ctx), OP_N, OP_T, (int)nn, nL, (int)nb, 1.0, rk, (int)nn, 0, coef, nL, 0,
            accumulate ? 1.0 : 0.0, d_rho, (int)nn, 0, 1);
 }
 
@@ -871,7 +887,6 @@ int lqm_ctx_destroy(lqm_ctx* ctx) {
   for (auto& b : ctx->hops_cache) cudaFree(b.first);
   if (ctx->d_phase) cudaFree(ctx->d_phase);
   if (ctx->d_err) cudaFree(ctx->d_err);
-  if (ctx->blas) cublasDestroy(ctx->blas);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   cudaStreamDestroy(ctx->stream);
