@@ -341,27 +341,28 @@ struct RhoOut {
 // The queue of the library's batched GEMMs: the context's stream.
 cudaStream_t blas_handle(lqm_ctx* ctx) { return ctx->stream; }
 
-template <int BM, int BN, int WM, int WN>
+template <int BM, int BN, int WM, int WN, int BK, int ST>
 void launch_zgemm_dmma(cudaStream_t st, const GemmArgs& g, int batch) {
   constexpr int nt = (BM / WM) * (BN / WN) * 32;
-  constexpr int smem = zgemm_smem_bytes<BM, BN, WM, WN>();
+  constexpr int smem = zgemm_smem_bytes<BM, BN, BK, ST>();
   static std::atomic<unsigned long long> attr_done{0};  // devices on which the smem limit is raised
   int dev = 0;
   ck(cudaGetDevice(&dev), "cudaGetDevice");
   const unsigned long long bit = 1ull << (dev & 63);
   if (!(attr_done.load() & bit)) {
-    ck(cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+    ck(cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN, BK, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            smem),
        "smem attr");
     attr_done.fetch_or(bit);
   }
   const dim3 grid((unsigned)((g.m + BM - 1) / BM), (unsigned)((g.n + BN - 1) / BN), (unsigned)batch);
-  zgemm_dmma_kernel<BM, BN, WM, WN><<<grid, nt, smem, st>>>(g);
+  zgemm_dmma_kernel<BM, BN, WM, WN, BK, ST><<<grid, nt, smem, st>>>(g);
 }
 
 // C_b = alpha op(A_b) op(B_b) + beta C_b for b < batch (column-major, strided):
 // the library's DMMA kernel (lqm_zgemm.cuh), with the tile shape chosen by the
 // product's shape (skinny n: the Fourier fold; small m: the back-transformation's
-// panel products).
+// panel products; short k: the rank-2nb updates).
 void zgemm_sb(cudaStream_t h, GemmOp ta, GemmOp tb, int m, int n, int k, double alpha_re, const double2* A, int lda,
               long long sA, const double2* B, int ldb, long long sB, double beta_re, double2* C, int ldc, long long sC,
               int batch) {
@@ -369,11 +370,13 @@ void zgemm_sb(cudaStream_t h, GemmOp ta, GemmOp tb, int m, int n, int k, double 
   if (batch > 65535) fail(LQM_EINVAL, "GEMM batch %d exceeds the grid limit", batch);
   GemmArgs g{m, n, k, alpha_re, beta_re, A, lda, sA, B, ldb, sB, C, ldc, sC, (int)ta, (int)tb};
   if (n <= 16)
-    launch_zgemm_dmma<64, 16, 16, 16>(h, g, batch);
+    launch_zgemm_dmma<128, 16, 32, 16, 8, 3>(h, g, batch);
   else if (m <= 32)
-    launch_zgemm_dmma<32, 64, 32, 16>(h, g, batch);
+    launch_zgemm_dmma<32, 64, 32, 16, 8, 3>(h, g, batch);
+  else if (k <= 64)
+    launch_zgemm_dmma<64, 64, 32, 16, 8, 3>(h, g, batch);
   else
-    launch_zgemm_dmma<64, 64, 32, 16>(h, g, batch);
+    launch_zgemm_dmma<64, 64, 32, 32, 8, 3>(h, g, batch);
   ck(cudaGetLastError(), "zgemm launch");
 }
 

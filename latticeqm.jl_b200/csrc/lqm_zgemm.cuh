@@ -6,10 +6,10 @@
 //   C_b = alpha op(A_b) op(B_b) + beta C_b,  b < batch,  column-major, strided,
 //   op in {N, T (transpose), C (conjugate transpose)}, alpha and beta real.
 //
-// A CTA computes a BM x BN tile of one batch entry, K in steps of 8 staged in
-// shared memory by a 3-deep cp.async ring (16-byte complex elements, zero fill past
+// A CTA computes a BM x BN tile of one batch entry, K in slices of BK staged in
+// shared memory by an ST-deep cp.async ring (16-byte complex elements, zero fill past
 // the matrix edges).  Both tiles are stored k-contiguous per row / column with a row
-// pitch of 12 elements, so the fragment reads of a quarter-warp fall on distinct
+// pitch of BK + 4 elements, so the fragment reads of a quarter-warp fall on distinct
 // 16-byte bank groups.  Each warp owns a WM x WN sub-tile: per 4-deep k-step it reads
 // one complex A element per 8-row strip and one complex B element per 8-column strip
 // and issues four real DMMAs per 8 x 8 output tile:
@@ -29,9 +29,8 @@ namespace lqm {
 
 enum GemmOp { OP_N = 0, OP_T = 1, OP_C = 2 };
 
-constexpr int kGemmBK = 8;       // k per stage
-constexpr int kGemmPitch = 12;   // complex elements per staged row (8 + 4: conflict-free fragment reads)
-constexpr int kGemmStages = 3;
+// complex elements per staged row: BK + 4 (== 4 mod 8: conflict-free fragment reads)
+__host__ __device__ constexpr int gemm_pitch(int BK) { return BK + 4; }
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -63,35 +62,38 @@ struct GemmArgs {
 // Stage one K-slice [k0, k0 + 8) of op(A) (BM rows) and op(B) (BN columns) into
 // As[row][kk], Bs[col][kk].  op N of A / op T,C of B are contiguous along the
 // row / column index, the other ops along k; threads follow the contiguous index.
-template <int BM, int BN, int NT>
+template <int BM, int BN, int NT, int BK>
 __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, const double2* B, int m0, int n0,
                                            int k0, double2* As, double2* Bs) {
+  constexpr int P = gemm_pitch(BK);
 #pragma unroll
-  for (int e = threadIdx.x; e < BM * kGemmBK; e += NT) {
+  for (int e = threadIdx.x; e < BM * BK; e += NT) {
     int r, kk;
-    if (g.opA == OP_N) { r = e % BM; kk = e / BM; } else { kk = e % kGemmBK; r = e / kGemmBK; }
+    if (g.opA == OP_N) { r = e % BM; kk = e / BM; } else { kk = e % BK; r = e / BK; }
     const int gm = m0 + r, gk = k0 + kk;
     const bool ok = gm < g.m && gk < g.k;
     const double2* src = (g.opA == OP_N) ? A + gm + (int64_t)gk * g.lda : A + gk + (int64_t)gm * g.lda;
-    gemm_cp16(As + r * kGemmPitch + kk, ok ? (const void*)src : (const void*)A, ok);
+    gemm_cp16(As + r * P + kk, ok ? (const void*)src : (const void*)A, ok);
   }
 #pragma unroll
-  for (int e = threadIdx.x; e < BN * kGemmBK; e += NT) {
+  for (int e = threadIdx.x; e < BN * BK; e += NT) {
     int c, kk;
-    if (g.opB == OP_N) { kk = e % kGemmBK; c = e / kGemmBK; } else { c = e % BN; kk = e / BN; }
+    if (g.opB == OP_N) { kk = e % BK; c = e / BK; } else { c = e % BN; kk = e / BN; }
     const int gn = n0 + c, gk = k0 + kk;
     const bool ok = gn < g.n && gk < g.k;
     const double2* src = (g.opB == OP_N) ? B + gk + (int64_t)gn * g.ldb : B + gn + (int64_t)gk * g.ldb;
-    gemm_cp16(Bs + c * kGemmPitch + kk, ok ? (const void*)src : (const void*)B, ok);
+    gemm_cp16(Bs + c * P + kk, ok ? (const void*)src : (const void*)B, ok);
   }
 }
 
-// grid (ceil(m / BM), ceil(n / BN), batch); block (BM / WM) * (BN / WN) warps.
-template <int BM, int BN, int WM, int WN>
+// grid (ceil(m / BM), ceil(n / BN), batch); block (BM / WM) * (BN / WN) warps; K in
+// slices of BK through an ST-deep ring.
+template <int BM, int BN, int WM, int WN, int BK, int ST>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(GemmArgs g) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int MI = WM / 8, NJ = WN / 8;
-  constexpr int STAGE = (BM + BN) * kGemmPitch;  // complex per stage
+  constexpr int P = gemm_pitch(BK);
+  constexpr int STAGE = (BM + BN) * P;  // complex per stage
   extern __shared__ __align__(16) unsigned char gemm_smem[];
   double2* sm = (double2*)gemm_smem;
   const int64_t b = blockIdx.z;
@@ -111,36 +113,41 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
 #pragma unroll
     for (int j = 0; j < NJ; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
 
-  const int nks = (g.k + kGemmBK - 1) / kGemmBK;
+  const int nks = (g.k + BK - 1) / BK;
 #pragma unroll
-  for (int s = 0; s < kGemmStages - 1; ++s) {
-    if (s < nks) gemm_stage<BM, BN, NT>(g, A, B, m0, n0, s * kGemmBK, sm + s * STAGE, sm + s * STAGE + BM * kGemmPitch);
+  for (int s = 0; s < ST - 1; ++s) {
+    if (s < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, s * BK, sm + s * STAGE, sm + s * STAGE + BM * P);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
   for (int ks = 0; ks < nks; ++ks) {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(kGemmStages - 2) : "memory");
-    __syncthreads();
-    {
-      const int nx = ks + kGemmStages - 1;
-      const int st = nx % kGemmStages;
-      if (nx < nks)
-        gemm_stage<BM, BN, NT>(g, A, B, m0, n0, nx * kGemmBK, sm + st * STAGE, sm + st * STAGE + BM * kGemmPitch);
+    if (ST > 1) {
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(ST > 1 ? ST - 2 : 0) : "memory");
+      __syncthreads();
+      const int nx = ks + ST - 1;
+      const int st = nx % ST;
+      if (nx < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, nx * BK, sm + st * STAGE, sm + st * STAGE + BM * P);
       asm volatile("cp.async.commit_group;\n" ::: "memory");
+    } else {  // one buffer: load, wait, compute, and fence the buffer before the next load
+      __syncthreads();
+      gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, ks * BK, sm, sm + BM * P);
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      __syncthreads();
     }
-    const double2* As = sm + (ks % kGemmStages) * STAGE;
-    const double2* Bs = As + BM * kGemmPitch;
+    const double2* As = sm + (ks % ST) * STAGE;
+    const double2* Bs = As + BM * P;
 #pragma unroll
-    for (int kk = 0; kk < kGemmBK; kk += 4) {
+    for (int kk = 0; kk < BK; kk += 4) {
       double ar[MI], ai[MI], br[NJ], bi[NJ];
 #pragma unroll
       for (int i = 0; i < MI; ++i) {
-        const double2 a = As[(wm0 + 8 * i + gr) * kGemmPitch + kk + gt];
+        const double2 a = As[(wm0 + 8 * i + gr) * P + kk + gt];
         ar[i] = a.x;
         ai[i] = sa * a.y;
       }
 #pragma unroll
       for (int j = 0; j < NJ; ++j) {
-        const double2 v = Bs[(wn0 + 8 * j + gr) * kGemmPitch + kk + gt];
+        const double2 v = Bs[(wn0 + 8 * j + gr) * P + kk + gt];
         br[j] = v.x;
         bi[j] = sb * v.y;
       }
@@ -182,9 +189,9 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
   }
 }
 
-template <int BM, int BN, int WM, int WN>
+template <int BM, int BN, int BK, int ST>
 constexpr int zgemm_smem_bytes() {
-  return kGemmStages * (BM + BN) * kGemmPitch * 16;
+  return ST * (BM + BN) * gemm_pitch(BK) * 16;
 }
 
 }  // namespace lqm
