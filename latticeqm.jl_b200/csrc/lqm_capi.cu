@@ -387,11 +387,12 @@ bool use_blocked(const lqm_ctx* ctx, int n, int nR);
 // zlatrd panels (column kernels + batched rank-2nb updates), divide and
 // conquer per k, compact-WY back-transformation and rho_k = U f U^H as batched
 // GEMMs.  k-points are processed in batches sized to ~24 GB of work buffers.
-// TMA descriptor of a batch of B matrices (n x n complex, column-major, contiguous):
-// 3-D (2n doubles, n columns, B k-points), box 16 doubles (8 complex rows) x 64
-// columns x 1, 128-byte swizzle, zero fill out of bounds.  cuTensorMapEncodeTiled is
+// TMA descriptors of a batch of B matrices (n x n complex, column-major, contiguous):
+// 3-D (2n doubles, n columns, B k-points), zero fill out of bounds; `map` boxes of 16
+// doubles (8 complex rows) x 64 columns x 1 with 128-byte swizzle (the tiles),
+// `vmap` boxes of 128 doubles x 1 column x 1 (the reflector segments).  cuTensorMapEncodeTiled is
 // taken from the driver through the runtime (no link-time libcuda dependency).
-bool make_symv_map(CUtensorMap* map, const double2* A, int n, int64_t B) {
+bool make_symv_map(CUtensorMap* map, CUtensorMap* vmap, const double2* A, int n, int64_t B) {
   static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -407,8 +408,14 @@ bool make_symv_map(CUtensorMap* map, const double2* A, int n, int64_t B) {
   const cuuint64_t strides[2] = {(cuuint64_t)n * 16, (cuuint64_t)n * n * 16};
   const cuuint32_t box[3] = {16, (cuuint32_t)kSymvTB, 1};
   const cuuint32_t es[3] = {1, 1, 1};
-  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)A, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  if (enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)A, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+      CUDA_SUCCESS)
+    return false;
+  // the reflector segments: 64 complex rows of one column, no swizzle
+  const cuuint32_t vbox[3] = {2 * (cuuint32_t)kSymvTB, 1, 1};
+  return enc(vmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)A, dims, strides, vbox, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -449,9 +456,10 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   ck(cudaFuncSetAttribute(blk_symv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvTmaSmem),
      "smem attr");
   // the mat-vec moves its tiles by TMA from n = 64 on (the descriptor covers the batch)
-  CUtensorMap symv_map;
+  CUtensorMap symv_map, symv_vmap;
   const char* pipe_env = std::getenv("LQM_SYMV_PIPE");
-  const bool symv_tma = n >= 64 && !(pipe_env && pipe_env[0] == '1') && make_symv_map(&symv_map, A, n, B);
+  const bool symv_tma =
+      n >= 64 && !(pipe_env && pipe_env[0] == '1') && make_symv_map(&symv_map, &symv_vmap, A, n, B);
   if (symv_tma && !ctx->d_err) {
     ck(cudaMalloc(&ctx->d_err, sizeof(int)), "cudaMalloc(error word)");
     ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "memset(error word)");
@@ -482,8 +490,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           std::pair<cudaEvent_t, cudaEvent_t> sev{};
           if (ctx->stats_on) { sev = stat_events(ctx); ck(cudaEventRecord(sev.first, ctx->stream), "event"); }
           if (symv_tma) {
-            blk_symv_tma_kernel<<<(unsigned)grid, kSymvTmaThreads, kSymvTmaSmem, ctx->stream>>>(symv_map, ba, j,
-                                                                                           nitems, ctx->d_err);
+            blk_symv_tma_kernel<<<(unsigned)grid, kSymvTmaThreads, kSymvTmaSmem, ctx->stream>>>(
+                symv_map, symv_vmap, ba, j, nitems, ctx->d_err);
             ctx->err_armed = true;
           } else {
             blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);

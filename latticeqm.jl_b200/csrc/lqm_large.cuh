@@ -258,7 +258,9 @@ __global__ void __launch_bounds__(kSymvThreads, 1) blk_symv_pipe_kernel(BlkArgs 
 constexpr int kSymvTmaThreads = 512;
 constexpr int kSymvTmaStages = 3;
 constexpr int kSymvTileBytes = kSymvTB * kSymvTB * 16;  // 64 KB
-constexpr int kSymvTmaSmem = kSymvTmaStages * kSymvTileBytes + 1024 /* alignment */ + 64 /* mbarriers */;
+constexpr int kSymvVecBytes = 2 * kSymvTB * 16;               // v over the tile's rows, then over its columns
+constexpr int kSymvTmaSmem =
+    kSymvTmaStages * (kSymvTileBytes + kSymvVecBytes) + 1024 /* alignment */ + 64 /* mbarriers */;
 static_assert(kSymvTmaSmem <= 227 * 1024, "TMA mat-vec pipeline exceeds shared memory");
 constexpr long long kSymvWaitLimit = 1LL << 22;  // mbarrier polls before giving up (well under a second)
 
@@ -299,25 +301,33 @@ __device__ __forceinline__ int symv_sw(int r, int c) {
   return ((r >> 3) << 13) + (c << 7) + ((((r & 7) ^ (c & 7))) << 4);
 }
 
-__device__ __forceinline__ void symv_tma_issue(const CUtensorMap* map, int j, int ntiles, int64_t it, unsigned dst,
-                                               unsigned bar) {
+// The tile of work item `it` (eight boxes) and the two 64-element segments of the
+// reflector v = A(j+1:, j) it multiplies (rows of the tile's row block and of its
+// column block; one box each from the vector map), all on the stage's mbarrier.
+__device__ __forceinline__ void symv_tma_issue(const CUtensorMap* map, const CUtensorMap* vmap, int j, int ntiles,
+                                               int64_t it, unsigned dst, unsigned vdst, unsigned bar) {
   const int64_t b = it / ntiles;
   int R, C;
   symv_tile_rc((int)(it - b * ntiles), &R, &C);
-  mbar_arrive_expect_tx(bar, (unsigned)kSymvTileBytes);
+  mbar_arrive_expect_tx(bar, (unsigned)(kSymvTileBytes + kSymvVecBytes));
   const int row0 = j + 1 + R * kSymvTB, col0 = j + 1 + C * kSymvTB;
 #pragma unroll
   for (int bx = 0; bx < kSymvTB / 8; ++bx)
     tma_load_3d(dst + (unsigned)(bx << 13), map, 2 * (row0 + 8 * bx), col0, (int)b, bar);
+  tma_load_3d(vdst, vmap, 2 * row0, j, (int)b, bar);
+  tma_load_3d(vdst + kSymvTB * 16, vmap, 2 * col0, j, (int)b, bar);
 }
 
 __global__ void __launch_bounds__(kSymvTmaThreads, 1)
-    blk_symv_tma_kernel(const __grid_constant__ CUtensorMap map, BlkArgs a, int j, int64_t nitems, int* err) {
+    blk_symv_tma_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap vmap, BlkArgs a,
+                        int j, int64_t nitems, int* err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const unsigned raw = smem_u32(smem_raw);
   const unsigned base = (raw + 1023u) & ~1023u;                // 1024-byte aligned tiles (128-byte swizzle)
   unsigned char* tiles = smem_raw + (base - raw);
-  const unsigned bars = base + kSymvTmaStages * kSymvTileBytes;  // one mbarrier per stage
+  const unsigned vbase = base + kSymvTmaStages * kSymvTileBytes;  // v segments of each stage
+  const unsigned char* vsm = tiles + kSymvTmaStages * kSymvTileBytes;
+  const unsigned bars = vbase + kSymvTmaStages * kSymvVecBytes;   // one mbarrier per stage
   const int m = a.n - j - 1;
   const int nbk = (m + kSymvTB - 1) / kSymvTB;
   const int ntiles = nbk * (nbk + 1) / 2;
@@ -332,25 +342,16 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
   if (threadIdx.x == 0) {
     for (int s = 0; s < kSymvTmaStages - 1; ++s) {
       const int64_t it = first + s * step;
-      if (it < nitems) symv_tma_issue(&map, j, ntiles, it, base + s * kSymvTileBytes, bars + 8 * s);
+      if (it < nitems)
+        symv_tma_issue(&map, &vmap, j, ntiles, it, base + s * kSymvTileBytes, vbase + s * kSymvVecBytes, bars + 8 * s);
     }
   }
-  const double2* vcol = a.A + (j + 1) + (int64_t)j * a.n;  // reflector column j of k-point 0
   int stage = 0;
   unsigned parity = 0;
   for (int64_t it = first; it < nitems; it += step) {
     const int64_t b = it / ntiles;
     int R, C;
     symv_tile_rc((int)(it - b * ntiles), &R, &C);
-    const int x0 = R * kSymvTB, y0 = C * kSymvTB;
-    const double2* v = vcol + b * (int64_t)a.n * a.n;
-    double2 vr[4], vc[4];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int u = g + 16 * h;
-      vr[h] = (x0 + u < m) ? v[x0 + u] : cmk(0.0, 0.0);
-      vc[h] = (y0 + u < m) ? v[y0 + u] : cmk(0.0, 0.0);
-    }
     // the stage's copies have landed, and every thread is past the previous tile (so
     // its stage may be refilled); the verdict of the bounded wait is the block's
     const int ok = __syncthreads_and(mbar_wait_bounded(bars + 8 * stage, parity) ? 1 : 0);
@@ -369,9 +370,19 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
     if (threadIdx.x == 0) {
       const int64_t nx = it + (kSymvTmaStages - 1) * step;
       const int ns = (stage + kSymvTmaStages - 1) % kSymvTmaStages;
-      if (nx < nitems) symv_tma_issue(&map, j, ntiles, nx, base + ns * kSymvTileBytes, bars + 8 * ns);
+      if (nx < nitems)
+        symv_tma_issue(&map, &vmap, j, ntiles, nx, base + ns * kSymvTileBytes, vbase + ns * kSymvVecBytes,
+                       bars + 8 * ns);
     }
     const unsigned char* ts = tiles + stage * kSymvTileBytes;
+    const double2* vR = (const double2*)(vsm + stage * kSymvVecBytes);  // zeros past the matrix edge
+    const double2* vC = vR + kSymvTB;
+    double2 vr[4], vc[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      vr[h] = vR[g + 16 * h];
+      vc[h] = vC[g + 16 * h];
+    }
     const bool diag = (R == C);
     double2 yd0 = cmk(0.0, 0.0), yd1 = yd0, yt0 = yd0, yt1 = yd0;
     const int r0 = qp, r1 = qp + 32;
