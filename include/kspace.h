@@ -246,6 +246,21 @@ int lqm_bands_dos_rho_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
                           int64_t nw, const double* d_omegas, double gamma, double* d_dos, double* d_bands,
                           int precision);
 
+/* lqm_bands_dos_rho_dev for several models of uneven order on the same k list, with
+ * ONE eigensolver launch for all of them: the batched form of the per-model loop of
+ * `bandmatrix` / `getdos` / `getdensitymatrix!` (src/modules/Spectrum/bands.jl:164-204,
+ * dos.jl:202-223, densitymatrix.jl:28-49), which the reference runs model by model.
+ * Each model's k-points go to CTA sub-teams of that model's one-CTA block size
+ * (several teams per CTA on named barriers), so small orders fill the SMs as large
+ * ones drain.  Models: 1..4, all below the blocked eigensolver's switch; arrays of
+ * nmodels entries (H, nL, Lkeys, d_rho, d_omegas, d_dos, d_bands; eband receives
+ * nmodels values); d_w NULL means 1/nk. */
+int lqm_bands_dos_rho_multi_dev(lqm_ctx* ctx, int nmodels, const lqm_hops* const* H, int64_t nk,
+                                const double* d_ks, const double* d_w, double mu, double T, const int64_t* nL,
+                                const int64_t* const* Lkeys, double* const* d_rho, double* eband, int64_t nw,
+                                const double* const* d_omegas, double gamma, double* const* d_dos,
+                                double* const* d_bands);
+
 /* Hartree-Fock SCF with linear mixing, device-resident, replaces
  * `solvehartreefock` (src/modules/Meanfield/selfconsistent.jl:19,256-336,366-381;
  * functional hartreefock.jl:143-289,392-410; mixing fixedpoint.jl:39-194).

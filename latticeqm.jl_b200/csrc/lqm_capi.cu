@@ -683,8 +683,8 @@ int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
 // rho_L (+)= sum_k coef[k,L] rho_k over a batch, as one ZGEMM: with rho_k the
 // columns of R (nn x nb) and coef the nL x nb matrix C, rho_L (nn x nL) =
 // R C^T (+ rho_L).  A skinny product (nL ~ 9 outputs per element read) that
-// streams the rho_k batch once; cuBLAS's fixed kernel choice keeps it
-// deterministic for a given batch size.
+// streams the rho_k batch once (the library's GEMM with 128 x 16 tiles, a fixed
+// summation order for a given batch size).
 void launch_fold(lqm_ctx* ctx, int64_t nn, int64_t nb, const double2* rk, const double2* coef, int nL,
                  double2* d_rho, int accumulate) {
   NvtxRange nvtx_("rho fold");
@@ -863,6 +863,84 @@ void check_precision(int precision) {
 // ============================================================================
 // C ABI
 // ============================================================================
+namespace {
+
+// One eigen pass over the k-points of several models of uneven order (the one-CTA
+// eigensolver's orders) as ONE launch of eigh_multi_kernel: model m's k-points go to
+// teams of its own block size, several teams per CTA on named barriers.  Writes
+// each model's bands and rho_k batch (with the band energies per k).
+void launch_eigh_multi(lqm_ctx* ctx, int nm, const lqm_hops* const* H, int64_t nk, const double* d_ks,
+                       double* const* bands, double2* const* rhok, double* const* ebk, const double* d_w, double mu,
+                       double T) {
+  NvtxRange nvtx_("eigen pass (several models, one launch)");
+  if (nm < 1 || nm > kMaxModels) fail(LQM_EINVAL, "between 1 and %d models per launch", kMaxModels);
+  int tnt[kMaxModels];
+  int NT = 0;
+  for (int m = 0; m < nm; ++m) {
+    const int n = (int)H[m]->n;
+    if (use_blocked(ctx, n, (int)H[m]->nR))
+      fail(LQM_EINVAL, "model %d (n=%d) is served by the blocked eigensolver, not the one-CTA one", m, n);
+    tnt[m] = eigh_threads_for(ctx, n);
+    NT = std::max(NT, tnt[m]);
+  }
+  NT = NT <= 384 ? 384 : 512;
+  for (int m = 0; m < nm; ++m) {
+    if (NT % tnt[m] != 0) tnt[m] = NT;            // a team size that does not tile the CTA runs CTA-wide
+    while (NT / tnt[m] > 15) tnt[m] *= 2;         // at most 15 named barriers per CTA
+  }
+  EighMultiArgs ma{};
+  ma.nmodels = nm;
+  int64_t smem = 0, slot = 0, slots_per_cta = 1;
+  for (int m = 0; m < nm; ++m) {
+    const int n = (int)H[m]->n, nR = (int)H[m]->nR;
+    const int teams = NT / tnt[m];
+    EighSmemLayout Ls = eigh_smem_layout(n, nR, tnt[m], 1);
+    int a_in_smem = (int64_t)teams * (int64_t)lqm_align16(Ls.total) <= 225 * 1024;
+    if (!a_in_smem) Ls = eigh_smem_layout(n, nR, tnt[m], 0);
+    const int64_t per_team = (int64_t)lqm_align16(Ls.total);
+    if ((int64_t)teams * per_team > 225 * 1024) fail(LQM_EINVAL, "model %d (n=%d) exceeds the shared-memory plan", m, n);
+    smem = std::max(smem, (int64_t)teams * per_team);
+    slot = std::max(slot, eigh_slot_doubles(n, a_in_smem, !a_in_smem));
+    slots_per_cta = std::max<int64_t>(slots_per_cta, teams);
+    EighArgs& a = ma.m[m];
+    a.n = n; a.nR = nR; a.dim = H[m]->d; a.blocks = H[m]->blocks; a.keys = H[m]->keys;
+    a.nk = nk; a.ks = d_ks; a.plan = get_plan(ctx, n); a.a_in_smem = a_in_smem;
+    a.bands = bands[m]; a.U = nullptr; a.rhok = rhok[m]; a.eband_k = ebk[m]; a.w = d_w; a.mu = mu; a.T = T;
+    a.phase_cycles = nullptr;
+    ma.team_nt[m] = tnt[m];
+    ma.smem_team[m] = per_team;
+  }
+  // items: model after model, k-points in groups of one per team of a CTA
+  ma.item_begin[0] = 0;
+  for (int m = 0; m < nm; ++m) {
+    const int teams = NT / tnt[m];
+    ma.item_begin[m + 1] = ma.item_begin[m] + (nk + teams - 1) / teams;
+  }
+  ma.slots_per_cta = slots_per_cta;
+  auto kfn = NT == 384 ? &eigh_multi_kernel<384> : &eigh_multi_kernel<512>;
+  ck(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
+  int per_sm = 0;
+  ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, NT, (size_t)smem), "occupancy");
+  if (per_sm < 1) fail(LQM_EINVAL, "the model-batched eigensolver cannot be resident");
+  int64_t grid = std::min<int64_t>(ma.item_begin[nm], (int64_t)per_sm * ctx->num_sms);
+  const int64_t max_cta = std::max<int64_t>(1, (int64_t)(16.0e9 / (8.0 * (double)slot * (double)slots_per_cta)));
+  grid = std::max<int64_t>(1, std::min(grid, max_cta));
+  double* scratch = (double*)ws_get(ctx, WS_SCRATCH, (size_t)(grid * slots_per_cta * slot) * sizeof(double));
+  for (int m = 0; m < nm; ++m) {
+    ma.m[m].scratch = scratch;
+    ma.m[m].slot_doubles = slot;
+  }
+  std::pair<cudaEvent_t, cudaEvent_t> evs{};
+  if (ctx->stats_on) { evs = stat_events(ctx); ck(cudaEventRecord(evs.first, ctx->stream), "event"); }
+  kfn<<<(unsigned)grid, NT, (size_t)smem, ctx->stream>>>(ma);
+  ck(cudaGetLastError(), "eigh_multi_kernel launch");
+  if (ctx->stats_on) { ck(cudaEventRecord(evs.second, ctx->stream), "event"); ctx->ev_pending.push_back(evs); }
+  ctx->eigh_launches++;
+  ctx->launches++;
+}
+
+}  // namespace
+
 extern "C" {
 
 int lqm_ctx_create(int device, lqm_ctx** out) {
@@ -1409,6 +1487,75 @@ int lqm_bands_dos_rho_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const dou
     wait_stream(ctx);
     timer_collect(ctx);
     if (eband) *eband = eb;
+  });
+}
+
+int lqm_bands_dos_rho_multi_dev(lqm_ctx* ctx, int nmodels, const lqm_hops* const* H, int64_t nk,
+                                const double* d_ks, const double* d_w, double mu, double T, const int64_t* nL,
+                                const int64_t* const* Lkeys, double* const* d_rho, double* eband, int64_t nw,
+                                const double* const* d_omegas, double gamma, double* const* d_dos,
+                                double* const* d_bands) {
+  return guarded(ctx, [&] {
+    if (nmodels < 1 || nmodels > kMaxModels || !H || !nL || !Lkeys || !d_rho || !d_omegas || !d_dos || !d_bands ||
+        nk < 1 || !d_ks || nw < 1)
+      fail(LQM_EINVAL, "invalid arguments");
+    if (!std::isfinite(mu) || !(T >= 0) || !std::isfinite(T) || !std::isfinite(gamma))
+      fail(LQM_EINVAL, "invalid mu/T/gamma");
+    const int d = H[0] ? H[0]->d : 0;
+    int64_t per_k = 0;
+    for (int m = 0; m < nmodels; ++m) {
+      check_hops(H[m]);
+      if (H[m]->d != d) fail(LQM_EINVAL, "models must share the key dimension");
+      if (nL[m] < 1 || !Lkeys[m] || !d_rho[m] || !d_omegas[m] || !d_dos[m] || !d_bands[m])
+        fail(LQM_EINVAL, "invalid arguments of model %d", m);
+      per_k += 16 * H[m]->n * H[m]->n;
+    }
+    const double* dw = d_w ? d_w : uniform_weights(ctx, nk);
+    // every model's rho_k of a chunk of k-points stays resident (24 GB per chunk)
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(24.0e9 / (double)per_k)));
+    std::vector<double2*> rk(nmodels);
+    std::vector<double*> bandsp(nmodels), ebk(nmodels);
+    char* rbuf = (char*)ws_get(ctx, WS_RHOK, (size_t)(chunk * per_k) + 256 * (size_t)nmodels);
+    double* ebuf = (double*)ws_get(ctx, WS_EBK, (size_t)(chunk * nmodels) * sizeof(double));
+    double* sc = (double*)ws_get(ctx, WS_MISC, 64 * sizeof(double));  // [48 ..) band energy per model
+    int64_t maxnl = 0;
+    for (int m = 0; m < nmodels; ++m) maxnl = std::max(maxnl, nL[m]);
+    double2* coef = (double2*)ws_get(ctx, WS_COEF, (size_t)(chunk * maxnl) * sizeof(double2));
+    int64_t* dL = (int64_t*)ws_get(ctx, WS_LKEYS, (size_t)(nmodels * maxnl * d) * sizeof(int64_t));
+    for (int m = 0; m < nmodels; ++m)
+      ck(cudaMemcpyAsync(dL + m * maxnl * d, Lkeys[m], (size_t)(nL[m] * d) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                         ctx->stream),
+         "H2D");
+    size_t off = 0;
+    for (int m = 0; m < nmodels; ++m) {
+      rk[m] = (double2*)(rbuf + off);
+      off += (size_t)(chunk * 16 * H[m]->n * H[m]->n + 255) / 256 * 256;
+      ebk[m] = ebuf + m * chunk;
+    }
+    timer_start(ctx);
+    for (int64_t k0 = 0; k0 < nk; k0 += chunk) {
+      const int64_t nb = std::min(chunk, nk - k0);
+      for (int m = 0; m < nmodels; ++m) bandsp[m] = d_bands[m] + k0 * H[m]->n;
+      launch_eigh_multi(ctx, nmodels, H, nb, d_ks + k0 * d, bandsp.data(), rk.data(), ebk.data(), dw + k0, mu, T);
+      for (int m = 0; m < nmodels; ++m) {
+        const int64_t nn = H[m]->n * H[m]->n;
+        ordered_sum_kernel<<<1, 256, 0, ctx->stream>>>(ebk[m], nb, sc + 48 + m, k0 > 0);
+        fold_coef_kernel<<<(unsigned)std::min<int64_t>((nb * nL[m] + 255) / 256, 4096), 256, 0, ctx->stream>>>(
+            nb, d, d_ks + k0 * d, dw + k0, (int)nL[m], dL + m * maxnl * d, coef);
+        launch_fold(ctx, nn, nb, rk[m], coef, (int)nL[m], (double2*)d_rho[m], k0 > 0);
+        ctx->launches += 2;
+      }
+    }
+    for (int m = 0; m < nmodels; ++m) dos_dev(ctx, H[m]->n, nk, d_bands[m], d_w, nw, d_omegas[m], gamma, d_dos[m]);
+    timer_stop(ctx);
+    std::vector<double> eb((size_t)nmodels, 0.0);
+    wait_stream(ctx);
+    ck(cudaMemcpyAsync(eb.data(), sc + 48, (size_t)nmodels * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+       "D2H");
+    wait_stream(ctx);
+    timer_collect(ctx);
+    if (eband)
+      for (int m = 0; m < nmodels; ++m) eband[m] = eb[(size_t)m];
   });
 }
 

@@ -42,7 +42,8 @@ struct EighVec {
 // 1. Bloch sum.  blocks: nR x (n x n) column-major complex; keys: d x nR int64.
 // Column j by warp, rows i <= j by lane; the lower triangle is the mirror.
 // ---------------------------------------------------------------------------
-LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __restrict__ blocks,
+template <class TeamT>
+LQM_FN void bloch_build(const TeamT& T, int n, int nR, int dim, const double2* __restrict__ blocks,
                         const int64_t* __restrict__ keys, const double* kpt, double2* ph,
                         double2* A, int lda) {
   for (int r = T.tid; r < nR; r += T.nt) {
@@ -52,7 +53,7 @@ LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __
     lqm_sincospi(2.0 * dot, &s, &co);
     ph[r] = cmk(co, s);
   }
-  team_sync();
+  team_sync(T);
   const int64_t nn = (int64_t)n * n;
   for (int j = T.wid; j < n; j += T.nw) {
     for (int i = T.lane; i <= j; i += T.nl) {
@@ -67,7 +68,7 @@ LQM_FN void bloch_build(const Team& T, int n, int nR, int dim, const double2* __
       }
     }
   }
-  team_sync();
+  team_sync(T);
 }
 
 // ---------------------------------------------------------------------------
@@ -104,7 +105,8 @@ LQM_FN void zlarfg_scalars(double2 alpha, double xnorm2, double2* tau, double* b
 //         by the warp owning column c, stored to xs[] and back into A)
 //   pbuf[warp][r] = sum over the warp's columns of B_new[r,c] x[c]
 // Rows across lanes (up to 4 per lane and pass), columns across warps.
-LQM_FN void trailing_pass(const Team& T, int mb, double2* A, int lda, int o, const double2* v, const double2* w,
+template <class TeamT>
+LQM_FN void trailing_pass(const TeamT& T, int mb, double2* A, int lda, int o, const double2* v, const double2* w,
                           bool upd, double2 scal, double2* xs, double2* pbuf, int pstride) {
   double2* B = A + o + (int64_t)o * lda;
   double2* xcol = A + o + (int64_t)(o - 1) * lda;
@@ -147,7 +149,8 @@ LQM_FN void trailing_pass(const Team& T, int mb, double2* A, int lda, int o, con
 
 // Stores the next reflector x (formed from column o-1 rows o..) into xs[] and
 // back into A.  Called after trailing_pass and a barrier.
-LQM_FN void store_reflector(const Team& T, int mb, double2* A, int lda, int o, double2 scal, double2* xs) {
+template <class TeamT>
+LQM_FN void store_reflector(const TeamT& T, int mb, double2* A, int lda, int o, double2 scal, double2* xs) {
   double2* xcol = A + o + (int64_t)(o - 1) * lda;
   for (int c = T.tid; c < mb; c += T.nt) {
     const double2 x = (c == 0) ? cmk(1.0, 0.0) : cmul(scal, xcol[c]);
@@ -159,7 +162,8 @@ LQM_FN void store_reflector(const Team& T, int mb, double2* A, int lda, int o, d
 // Householder tridiagonalisation with 3 barriers per step:
 //   pass (update j, mat-vec with reflector j+1) | p, p^H v -> alpha |
 //   w, update of the next column, its norm -> next reflector scalars.
-LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, EighVec& S,
+template <class TeamT>
+LQM_FN_NOINLINE void hetrd_lower(const TeamT& T, int n, double2* A, int lda, EighVec& S,
                                  unsigned long long* sub = nullptr) {
 #if defined(__CUDA_ARCH__)
   long long tsub = clock64();
@@ -176,7 +180,7 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
 #endif
   if (n == 1) {
     if (T.tid == 0) S.d[0] = A[0].x;
-    team_sync();
+    team_sync(T);
     return;
   }
   double* redA = S.red;
@@ -203,7 +207,7 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
     const int mb = n - o;
     LQM_HTICK(2);
     trailing_pass(T, mb, A, lda, o, vc, wc, j >= 0, scal, vx, pb, n);
-    team_sync();
+    team_sync(T);
     LQM_HTICK(0);
     store_reflector(T, mb, A, lda, o, scal, vx);
     // p = tau_{j+1} * row sums; alpha = -1/2 tau (p^H x)
@@ -252,7 +256,7 @@ LQM_FN_NOINLINE void hetrd_lower(const Team& T, int n, double2* A, int lda, Eigh
       if (T.tid == 0) d_out[n - 1] = col[0].x;
     }
   }
-  team_sync();
+  team_sync(T);
   LQM_HTICK(2);
 #undef LQM_HTICK
 }
@@ -435,7 +439,8 @@ __device__ __forceinline__ void lqm_cp_async8(void* sdst, const void* gsrc, bool
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(nbytes) : "memory");
 }
 #endif
-LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int* colnd, const int* newpos,
+template <class TeamT>
+LQM_FN void dc_tile_gemm(const TeamT& T, int n, int lo, int hi, int k, const int* colnd, const int* newpos,
                          const double* Q, double* Qt, const double* Ubn, double* tile) {
   const int s = hi - lo;
 #if defined(__CUDA_ARCH__)
@@ -444,7 +449,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
     const int tr = T.tid & 31, tc = T.tid >> 5;  // rows 2tr, 2tr+1, 64+2tr, 65+2tr; columns tc*8 .. +7
     int* cidx = (int*)(tile + NS * STG);         // the node's column indices, staged once
     for (int p = T.tid; p < k; p += T.nt) cidx[p] = colnd[p];
-    team_sync();
+    team_sync(T);
     for (int r0 = 0; r0 < s; r0 += BM) {
       for (int c0 = 0; c0 < k; c0 += BN) {
         double acc[4][8];
@@ -472,7 +477,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         for (int it = 0; it < nst; ++it) {
           asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-          team_sync();
+          team_sync(T);
           if (it + 2 < nst) issue((it + 2) * BK, (it + 2) % NS);
           asm volatile("cp.async.commit_group;\n" ::: "memory");
           const double* As = tile + (it % NS) * STG;
@@ -496,7 +501,7 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
           }
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
-        team_sync();  // the ring is free before the next tile's prologue
+        team_sync(T);  // the ring is free before the next tile's prologue
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -528,7 +533,8 @@ LQM_FN void dc_tile_gemm(const Team& T, int n, int lo, int hi, int k, const int*
 // Ub (n*n doubles, or null) enables the tiled update for heights whose largest
 // merge has >= tile_min rows: node [lo, hi) keeps its normalised secular
 // vectors at Ub + lo*n as the rows of a k x k block (vector it at it + p*k).
-LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
+template <class TeamT>
+LQM_FN_NOINLINE void dc_solve(const TeamT& T, int n, const DCPlan& P, EighVec& S, double* Q, double* Qt,
                               unsigned long long* sub = nullptr, bool vec = true, double* Ub = nullptr,
                               int tile_min = 1 << 30) {
   double* ubuf = (double*)S.pbuf;  // per-warp secular eigenvectors (2n doubles each)
@@ -559,7 +565,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
     const double er = (i < n - 1) ? fabs(S.e[i] * inv) : 0.0;
     S.D[i] = (S.d[i] * inv - el) - er;
   }
-  team_sync();
+  team_sync(T);
   for (int i = T.tid; i < n - 1; i += T.nt) S.e[i] *= inv;
   if (vec) {
     for (int c = T.wid; c < n; c += T.nw)
@@ -567,7 +573,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
   } else {
     for (int i = T.tid; i < n; i += T.nt) { QF[i] = 1.0; QL[i] = 1.0; }
   }
-  team_sync();
+  team_sync(T);
   for (int h = 0; h < P.nheights; ++h) {
     const int h0 = P.hstart[h], h1 = P.hstart[h + 1];
     const int* own = P.owner + (int64_t)h * n;
@@ -600,7 +606,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
         S.perm[lo + (i - m) + cnt] = i;
       }
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(0);
     // B: gather z and D in merged order, then deflation, one thread per node
     for (int i = T.tid; i < n; i += T.nt) {
@@ -609,10 +615,10 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       S.zhat[i] = S.z[j];
       S.vals[i] = S.D[j];
     }
-    team_sync();
+    team_sync(T);
     for (int nd = h0 + T.tid; nd < h1; nd += T.nt)
       deflate_node(nd, P, S, fabs(S.e[P.mid[nd] - 1]), S.zhat, S.vals);
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(1);
     // C: secular roots
     {
@@ -639,7 +645,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
         if (active && g == 0) { S.org[lo + q] = org; S.troot[lo + q] = tr; }
       }
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(2);
     // D: Gu-Eisenstat z
     for (int i = T.tid; i < n; i += T.nt) {
@@ -657,7 +663,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       const double zh = sqrt(fabs(prod));
       S.zhat[lo + q] = (S.zl[lo + q] < 0.0) ? -zh : zh;
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(3);
     // F: deflation rotations on the rows of Q (or on the two boundary rows)
     if (!vec) {
@@ -693,7 +699,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       const int lo = P.lo[nd], it = i - lo, k = S.nk[nd];
       S.vals[i] = (it < k) ? S.dl[lo + S.org[lo + it]] + S.troot[lo + it] : S.dval[lo + it - k];
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(4);
     for (int i = T.tid; i < n; i += T.nt) {
       const int nd = own[i];
@@ -704,7 +710,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       for (int j = lo; j < hi; ++j) { const double vj = S.vals[j]; cnt += (vj < v) || (vj == v && j < i); }
       S.newpos[i] = lo + cnt;
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(5);
     // H: eigenvector update into Qt.  Column c by warp: the warp first forms
     // the normalised secular eigenvector u_p = zhat_p / (d_p - lambda_it) in its
@@ -769,7 +775,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
           for (int r = lo + T.lane; r < hi; r += T.nl) dst[r] = src[r];
         }
       }
-      team_sync();
+      team_sync(T);
       for (int nd = h0; nd < h1; ++nd) {
         const int lo = P.lo[nd];
         dc_tile_gemm(T, n, lo, P.hi[nd], S.nk[nd], S.colnd + lo, S.newpos + lo, Q, Qt, Ub + (int64_t)lo * n,
@@ -862,7 +868,7 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       }
       team_syncwarp();
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(6);
     // I: write back
     for (int c = T.wid; c < n && vec; c += T.nw) {
@@ -875,11 +881,11 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
       if (own[i] < 0) continue;
       S.D[S.newpos[i]] = S.vals[i];
     }
-    team_sync();
+    team_sync(T);
     LQM_SUBTICK(7);
   }
   for (int i = T.tid; i < n; i += T.nt) S.D[i] *= scale;
-  team_sync();
+  team_sync(T);
 }
 
 // ---------------------------------------------------------------------------
@@ -893,7 +899,8 @@ LQM_FN_NOINLINE void dc_solve(const Team& T, int n, const DCPlan& P, EighVec& S,
 // V^H u over the group's rows, a group sum, T (V^H u), and the update of the
 // group's rows, with 8 independent accumulators per lane.
 // ---------------------------------------------------------------------------
-LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int ldr, EighVec& S, double2* U,
+template <class TeamT>
+LQM_FN_NOINLINE void backtransform(const TeamT& T, int n, const double2* R, int ldr, EighVec& S, double2* U,
                                    int ldu, int cbeg = 0, int cend = -1) {
   // only the columns [cbeg, cend) of U are transformed (and read)
   if (cend < 0) cend = n;
@@ -913,7 +920,7 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
         if (i < b && r >= i) v = R[(j0 + 1 + r) + (int64_t)(j0 + i) * ldr];
         Vs[r + (int64_t)i * n] = v;
       }
-    team_sync();
+    team_sync(T);
     for (int pidx = T.wid; pidx < NB * NB; pidx += T.nw) {
       const int q = pidx % NB, i = pidx / NB;
       if (!(q < i && i < b)) continue;
@@ -925,7 +932,7 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
       sr = warp_sum(sr); si = warp_sum(si);
       if (T.lane == 0) Gs[q + i * NB] = cmk(sr, si);
     }
-    team_sync();
+    team_sync(T);
     for (int l = T.tid; l < NB; l += T.nt) {  // row l of T: T[l,l] = tau_l, T[l,i] = -tau_i sum_{q=l}^{i-1} T[l,q] G[q,i]
       double2 trow[NB];
 #pragma unroll
@@ -945,7 +952,7 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
 #pragma unroll
       for (int i = 0; i < NB; ++i) Ts[l + i * NB] = trow[i];
     }
-    team_sync();
+    team_sync(T);
     // lanes per column: the largest power of two <= 8 with ncol * G <= nt (within a warp)
     int G = 1;
     while (G < 8 && 2 * G <= T.nl && ncol * (2 * G) <= T.nt) G *= 2;
@@ -989,7 +996,7 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
         }
       }
     }
-    team_sync();
+    team_sync(T);
   }
 }
 
@@ -1002,7 +1009,8 @@ LQM_FN_NOINLINE void backtransform(const Team& T, int n, const double2* R, int l
 // rho_k = I - sum_j (1 - f_j) u_j u_j^H skips the filled states, otherwise the
 // sum skips the empty ones.  Every output entry accumulates over j in order.
 // ---------------------------------------------------------------------------
-LQM_FN_NOINLINE void rho_from_U(const Team& T, int n, const double2* U, int ldu, const double* f, double2* out,
+template <class TeamT>
+LQM_FN_NOINLINE void rho_from_U(const TeamT& T, int n, const double2* U, int ldu, const double* f, double2* out,
                                 int64_t ldo) {
   int n0 = 0, n1 = 0;
   for (int j = 0; j < n; ++j) {
@@ -1055,5 +1063,5 @@ LQM_FN_NOINLINE void rho_from_U(const Team& T, int n, const double2* U, int ldu,
         }
     }
   }
-  team_sync();
+  team_sync(T);
 }

@@ -86,19 +86,38 @@ __device__ __forceinline__ void carve_vectors(unsigned char* smem, const EighSme
   S.ri = ibuf + 5 * n; S.rj = ibuf + 6 * n; S.nk = ibuf + 7 * n; S.nrot = ibuf + 8 * n; S.ndef = ibuf + 9 * n;
 }
 
-template <int NT, int MINB = 1>
-__global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const Team T = make_team();
+// Per-phase SM cycle accounting of the eigensolver (profiling mode only).
+struct EighProf {
+  bool on = false;
+  unsigned long long acc[5] = {0, 0, 0, 0, 0};
+  unsigned long long dsub[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long hsub[3] = {0, 0, 0};
+  long long tc = 0;
+  __device__ __forceinline__ void start() {
+    if (on) tc = clock64();
+  }
+  __device__ __forceinline__ void tick(int ph) {
+    if (on) {
+      const long long t = clock64();
+      acc[ph] += (unsigned long long)(t - tc);
+      tc = t;
+    }
+  }
+};
+
+// The whole per-k computation of one team on its shared-memory region `smem` and
+// global scratch slot: H(k), Householder, divide and conquer, bands, and (when
+// asked) the eigenvectors and/or rho_k with the band energy.
+template <class TeamT>
+__device__ __forceinline__ void eigh_point(const TeamT& T, const EighArgs& a, int64_t k, unsigned char* smem,
+                                           double* slot, EighProf& P) {
   const int n = a.n;
   const EighSmemLayout L = eigh_smem_layout(n, a.nR, T.nt, a.a_in_smem);
   EighVec S;
   double2* ph;
   double* kpt;
   carve_vectors(smem, L, n, a.nR, S, &ph, &kpt);
-
   const int64_t nn = (int64_t)n * n;
-  double* slot = a.scratch + (int64_t)blockIdx.x * a.slot_doubles;
   const bool in_smem = a.a_in_smem != 0;
   const int lda = in_smem ? n + 1 : n;
   double2* A = in_smem ? (double2*)(smem + L.offA) : (double2*)slot;
@@ -109,100 +128,133 @@ __global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
   double* Qs = slot + 2 * nn;                         // smem path: saved Q
   const bool need_vec = (a.U != nullptr) || (a.rhok != nullptr);
 
-  const bool prof = a.phase_cycles != nullptr;
-  unsigned long long acc[5] = {0, 0, 0, 0, 0};
-  unsigned long long dsub[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  unsigned long long hsub[3] = {0, 0, 0};
-  long long tc = 0;
-#define LQM_TICK(ph_)                                                                   \
-  if (prof) {                                                                          \
-    long long t_ = clock64();                                                          \
-    acc[ph_] += (unsigned long long)(t_ - tc);                                         \
-    tc = t_;                                                                           \
+  P.start();
+  if (T.tid < a.dim) kpt[T.tid] = a.ks[k * a.dim + T.tid];
+  team_sync(T);
+  bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, lda);
+  P.tick(PH_BLOCH);
+  hetrd_lower(T, n, A, lda, S, P.on ? P.hsub : nullptr);
+  if (in_smem && need_vec) {
+    for (int c = T.wid; c < n - 1; c += T.nw)
+      for (int r = c + 1 + T.lane; r < n; r += T.nl) R[r + (int64_t)c * n] = A[r + (int64_t)c * lda];
+    team_sync(T);
   }
-
-  for (int64_t k = blockIdx.x; k < a.nk; k += gridDim.x) {
-    if (prof) tc = clock64();
-    if (T.tid < a.dim) kpt[T.tid] = a.ks[k * a.dim + T.tid];
-    team_sync();
-    bloch_build(T, n, a.nR, a.dim, a.blocks, a.keys, kpt, ph, A, lda);
-    LQM_TICK(PH_BLOCH);
-    hetrd_lower(T, n, A, lda, S, prof ? hsub : nullptr);
-    if (in_smem && need_vec) {
-      for (int c = T.wid; c < n - 1; c += T.nw)
-        for (int r = c + 1 + T.lane; r < n; r += T.nl) R[r + (int64_t)c * n] = A[r + (int64_t)c * lda];
-      team_sync();
-    }
-    LQM_TICK(PH_HETRD);
-    dc_solve(T, n, a.plan, S, Q, Qt, prof ? dsub : nullptr, need_vec);
-    for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
-    LQM_TICK(PH_DC);
-    if (need_vec) {
-      // Columns of U to form: all of them when U is an output; for rho_k alone only
-      // the eigenvectors rho_from_U reads (its complement form skips the states with
-      // f = 1, the direct form those with f = 0), a contiguous range since f falls
-      // with the ascending eigenvalues.
-      int cbeg = 0, cend = n;
-      if (a.rhok) {
-        double eb = 0.0;
-        for (int j = T.tid; j < n; j += T.nt) {
-          const double fj = fermi(S.D[j] - a.mu, a.T);
-          S.vals[j] = fj;
-          eb += S.D[j] * fj;
+  P.tick(PH_HETRD);
+  dc_solve(T, n, a.plan, S, Q, Qt, P.on ? P.dsub : nullptr, need_vec);
+  for (int i = T.tid; i < n; i += T.nt) a.bands[k * n + i] = S.D[i];
+  P.tick(PH_DC);
+  if (need_vec) {
+    // Columns of U to form: all of them when U is an output; for rho_k alone only
+    // the eigenvectors rho_from_U reads (its complement form skips the states with
+    // f = 1, the direct form those with f = 0), a contiguous range since f falls
+    // with the ascending eigenvalues.
+    int cbeg = 0, cend = n;
+    if (a.rhok) {
+      double eb = 0.0;
+      for (int j = T.tid; j < n; j += T.nt) {
+        const double fj = fermi(S.D[j] - a.mu, a.T);
+        S.vals[j] = fj;
+        eb += S.D[j] * fj;
+      }
+      eb = team_sum(T, eb, S.red);  // (its barriers publish S.vals)
+      if (T.tid == 0) a.eband_k[k] = a.w[k] * eb;
+      if (!a.U) {
+        int n0 = 0, n1 = 0;
+        for (int j = 0; j < n; ++j) {
+          n0 += (S.vals[j] == 0.0);
+          n1 += (S.vals[j] == 1.0);
         }
-        eb = team_sum(T, eb, S.red);  // (its barriers publish S.vals)
-        if (T.tid == 0) a.eband_k[k] = a.w[k] * eb;
-        if (!a.U) {
-          int n0 = 0, n1 = 0;
-          for (int j = 0; j < n; ++j) {
-            n0 += (S.vals[j] == 0.0);
-            n1 += (S.vals[j] == 1.0);
+        const double skip = (n1 > n0) ? 1.0 : 0.0;
+        cbeg = n;
+        cend = 0;
+        for (int j = 0; j < n; ++j)
+          if (S.vals[j] != skip) {
+            cbeg = cbeg < j ? cbeg : j;
+            cend = j + 1;
           }
-          const double skip = (n1 > n0) ? 1.0 : 0.0;
-          cbeg = n;
-          cend = 0;
-          for (int j = 0; j < n; ++j)
-            if (S.vals[j] != skip) {
-              cbeg = cbeg < j ? cbeg : j;
-              cend = j + 1;
-            }
-          if (cend < cbeg) cend = cbeg;
-        }
+        if (cend < cbeg) cend = cbeg;
       }
-      double2* U;
-      int ldu;
-      if (in_smem) {
-        for (int c = cbeg + T.wid; c < cend; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) Qs[r + (int64_t)c * n] = Q[r + (int64_t)c * n];
-        team_sync();
-        U = (double2*)(smem + L.offA);
-        ldu = n + 1;
-        for (int c = cbeg + T.wid; c < cend; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Qs[r + (int64_t)c * n], 0.0);
-      } else {
-        U = a.U ? a.U + k * nn : (double2*)(slot + 4 * nn);
-        ldu = n;
-        for (int c = cbeg + T.wid; c < cend; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Q[r + (int64_t)c * n], 0.0);
-      }
-      team_sync();
-      backtransform(T, n, R, ldr, S, U, ldu, cbeg, cend);
-      LQM_TICK(PH_BACK);
-      if (in_smem && a.U) {
-        double2* Uo = a.U + k * nn;
-        for (int c = T.wid; c < n; c += T.nw)
-          for (int r = T.lane; r < n; r += T.nl) Uo[r + (int64_t)c * n] = U[r + (int64_t)c * ldu];
-      }
-      if (a.rhok) rho_from_U(T, n, U, ldu, S.vals, a.rhok + k * nn, n);
     }
-    team_sync();
-    LQM_TICK(PH_OUT);
+    double2* U;
+    int ldu;
+    if (in_smem) {
+      for (int c = cbeg + T.wid; c < cend; c += T.nw)
+        for (int r = T.lane; r < n; r += T.nl) Qs[r + (int64_t)c * n] = Q[r + (int64_t)c * n];
+      team_sync(T);
+      U = (double2*)(smem + L.offA);
+      ldu = n + 1;
+      for (int c = cbeg + T.wid; c < cend; c += T.nw)
+        for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Qs[r + (int64_t)c * n], 0.0);
+    } else {
+      U = a.U ? a.U + k * nn : (double2*)(slot + 4 * nn);
+      ldu = n;
+      for (int c = cbeg + T.wid; c < cend; c += T.nw)
+        for (int r = T.lane; r < n; r += T.nl) U[r + (int64_t)c * ldu] = cmk(Q[r + (int64_t)c * n], 0.0);
+    }
+    team_sync(T);
+    backtransform(T, n, R, ldr, S, U, ldu, cbeg, cend);
+    P.tick(PH_BACK);
+    if (in_smem && a.U) {
+      double2* Uo = a.U + k * nn;
+      for (int c = T.wid; c < n; c += T.nw)
+        for (int r = T.lane; r < n; r += T.nl) Uo[r + (int64_t)c * n] = U[r + (int64_t)c * ldu];
+    }
+    if (a.rhok) rho_from_U(T, n, U, ldu, S.vals, a.rhok + k * nn, n);
   }
-#undef LQM_TICK
-  if (prof && T.tid == 0) {
-    for (int i = 0; i < 5; ++i) atomicAdd(&a.phase_cycles[i], acc[i]);
-    for (int i = 0; i < 8; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + i], dsub[i]);
-    for (int i = 0; i < 3; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + 8 + i], hsub[i]);
+  team_sync(T);
+  P.tick(PH_OUT);
+}
+
+template <int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) eigh_kernel(EighArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const Team T = make_team();
+  double* slot = a.scratch + (int64_t)blockIdx.x * a.slot_doubles;
+  EighProf P;
+  P.on = a.phase_cycles != nullptr;
+  for (int64_t k = blockIdx.x; k < a.nk; k += gridDim.x) eigh_point(T, a, k, smem, slot, P);
+  if (P.on && T.tid == 0) {
+    for (int i = 0; i < 5; ++i) atomicAdd(&a.phase_cycles[i], P.acc[i]);
+    for (int i = 0; i < 8; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + i], P.dsub[i]);
+    for (int i = 0; i < 3; ++i) atomicAdd(&a.phase_cycles[PH_DCSUB + 8 + i], P.hsub[i]);
+  }
+}
+
+// Several models of uneven order in ONE launch.  Model m's k-points go to teams of
+// team_nt[m] threads (its one-CTA block size), blockDim.x / team_nt[m] teams per CTA,
+// each on its own shared-memory region (smem_team[m] bytes) and scratch slot; a work
+// item is one k-point per team of a CTA.  Items are numbered model after model
+// (item_begin[m] ..), and the CTAs take them round-robin, so the small orders fill
+// the SMs as the large ones drain.  Teams synchronise on named barriers.
+constexpr int kMaxModels = 4;
+struct EighMultiArgs {
+  int nmodels;
+  EighArgs m[kMaxModels];
+  int team_nt[kMaxModels];
+  int64_t smem_team[kMaxModels];
+  int64_t item_begin[kMaxModels + 1];
+  int64_t slots_per_cta;  // scratch slots per CTA (the largest team count)
+};
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) eigh_multi_kernel(EighMultiArgs ma) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  EighProf P;
+  for (int64_t it = blockIdx.x; it < ma.item_begin[ma.nmodels]; it += gridDim.x) {
+    int mdl = 0;
+    while (it >= ma.item_begin[mdl + 1]) ++mdl;
+    const EighArgs& a = ma.m[mdl];
+    const int tnt = ma.team_nt[mdl];
+    const int nteams = NT / tnt;
+    const int team = threadIdx.x / tnt;
+    const int64_t k = (it - ma.item_begin[mdl]) * nteams + team;
+    double* slot = a.scratch + ((int64_t)blockIdx.x * ma.slots_per_cta + team) * a.slot_doubles;
+    if (tnt == NT) {
+      eigh_point(make_team(), a, k, smem, slot, P);
+    } else if (k < a.nk) {
+      eigh_point(make_subteam(tnt), a, k, smem + team * ma.smem_team[mdl], slot, P);
+    }
+    __syncthreads();  // every team is done with the CTA's shared memory before the next item
   }
 }
 

@@ -40,6 +40,28 @@ LQM_FN Team make_team() {
   return t;
 }
 LQM_FN void team_sync() { __syncthreads(); }
+LQM_FN void team_sync(const Team&) { __syncthreads(); }
+
+// One of the independent teams of `size` threads (a multiple of 32) that split a
+// CTA: thread threadIdx.x belongs to team threadIdx.x / size, which synchronises on
+// its own named barrier (1 + team index; at most 15 teams per CTA).  The per-k
+// phases are templates on the team type, so the CTA-wide kernels keep
+// __syncthreads and only the split kernels pay for named barriers.
+struct SubTeam {
+  int tid, nt;
+  int lane, nl;
+  int wid, nw;
+  int bar;
+};
+LQM_FN SubTeam make_subteam(int size) {
+  SubTeam t;
+  t.tid = threadIdx.x % size; t.nt = size;
+  t.lane = threadIdx.x & 31; t.nl = 32;
+  t.wid = t.tid >> 5; t.nw = size >> 5;
+  t.bar = 1 + threadIdx.x / size;
+  return t;
+}
+LQM_FN void team_sync(const SubTeam& T) { asm volatile("bar.sync %0, %1;\n" ::"r"(T.bar), "r"(T.nt) : "memory"); }
 LQM_FN void team_syncwarp() { __syncwarp(); }
 LQM_FN double warp_sum(double v) {
 #pragma unroll
@@ -66,6 +88,7 @@ LQM_FN double group_sum_bcast(double v, int width) {
 #else
 LQM_FN Team make_host_team() { Team t = {0, 1, 0, 1, 0, 1}; return t; }
 LQM_FN void team_sync() {}
+LQM_FN void team_sync(const Team&) {}
 LQM_FN void team_syncwarp() {}
 LQM_FN double warp_sum(double v) { return v; }
 LQM_FN double warp_max(double v) { return v; }
@@ -75,14 +98,15 @@ LQM_FN double group_sum_bcast(double v, int width) { (void)width; return v; }
 
 // Deterministic team reduction: warp trees, then every thread sums the warp
 // partials in warp order.  `red` needs >= 32 doubles of shared memory.
-LQM_FN double team_sum(const Team& T, double v, double* red) {
+template <class TeamT>
+LQM_FN double team_sum(const TeamT& T, double v, double* red) {
 #if defined(__CUDACC__)
   v = warp_sum(v);
   if (T.lane == 0) red[T.wid] = v;
-  __syncthreads();
+  team_sync(T);
   double s = 0.0;
   for (int w = 0; w < T.nw; ++w) s += red[w];
-  __syncthreads();
+  team_sync(T);
   return s;
 #else
   (void)T; (void)red;
@@ -90,14 +114,15 @@ LQM_FN double team_sum(const Team& T, double v, double* red) {
 #endif
 }
 
-LQM_FN double team_max(const Team& T, double v, double* red) {
+template <class TeamT>
+LQM_FN double team_max(const TeamT& T, double v, double* red) {
 #if defined(__CUDACC__)
   v = warp_max(v);
   if (T.lane == 0) red[T.wid] = v;
-  __syncthreads();
+  team_sync(T);
   double s = red[0];
   for (int w = 1; w < T.nw; ++w) s = fmax(s, red[w]);
-  __syncthreads();
+  team_sync(T);
   return s;
 #else
   (void)T; (void)red;
@@ -108,12 +133,13 @@ LQM_FN double team_max(const Team& T, double v, double* red) {
 // Two sums with ONE barrier: each caller alternates between two disjoint
 // `red` halves (>= 64 doubles each) so that a half is only rewritten after
 // another barrier has separated it from its last reads.
-LQM_FN void team_sum2_1b(const Team& T, double& a, double& b, double* red) {
+template <class TeamT>
+LQM_FN void team_sum2_1b(const TeamT& T, double& a, double& b, double* red) {
 #if defined(__CUDACC__)
   a = warp_sum(a);
   b = warp_sum(b);
   if (T.lane == 0) { red[2 * T.wid] = a; red[2 * T.wid + 1] = b; }
-  __syncthreads();
+  team_sync(T);
   // four interleaved partial sums (in warp order within each) keep the
   // dependent-add chain short; the result is still fixed for a given team size
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;

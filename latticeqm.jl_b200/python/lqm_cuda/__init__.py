@@ -48,6 +48,7 @@ EXPORTS = [
     "lqm_bdg_chemicalpotential", "lqm_scf_hf_bdg", "lqm_berry_flux", "lqm_berry_path", "lqm_fermisurface",
     "lqm_wilson", "lqm_wilson_wannier", "lqm_ctx_set_eigh_threads", "lqm_autotune_eigh", "lqm_ctx_kernel_stats",
     "lqm_comm_unique_id", "lqm_ctx_set_comm", "lqm_ctx_comm", "lqm_shard_range", "lqm_scf_hf_gradient",
+    "lqm_bands_dos_rho_multi_dev",
 ]
 
 
@@ -77,6 +78,7 @@ _SIG = {
     "lqm_ctx_comm": [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
     "lqm_shard_range": [_I64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_I64), ctypes.POINTER(_I64)],
     "lqm_scf_hf_gradient": [_P, _P, _P, _I64, _P, _P, _D, _D, _I64, _P, _P, _P, _D, _D, _I64, _P, _P, _P],
+    "lqm_bands_dos_rho_multi_dev": [_P, ctypes.c_int, _P, _I64, _P, _P, _D, _D, _P, _P, _P, _P, _I64, _P, _D, _P, _P],
     "lqm_ctx_last_kernel_ms": [_P, ctypes.POINTER(_D)],
     "lqm_hops_upload_dense": [_P, _I64, _I64, ctypes.c_int32, _P, _P, ctypes.POINTER(_P)],
     "lqm_hops_upload_csc": [_P, _I64, _I64, ctypes.c_int32, _P, _P, _P, _P, _P, ctypes.POINTER(_P)],
@@ -1079,3 +1081,28 @@ def scf_hf_gradient(h, v, rho, mu, ks, T=0.0, kweights=None, eps_bar=None, beta=
     dFd = {Rk: np.array(dF[:, :, i]) for i, Rk in enumerate(hkeys)}
     dLd = None if dL is None else {Rk: np.array(dL[:, :, i]) for i, Rk in enumerate(hkeys)}
     return SCFGradient(out[0], out[1], out[2], dFd, dLd, out[3], int(out[4]))
+
+
+def bands_dos_rho_multi_dev(models, d_ks, nk, mu=0.0, T=0.01, gamma=0.05, d_w=None, ctx=None):
+    """``lqm_bands_dos_rho_multi_dev``: bands, DOS and rho_L of several models on one k list
+    (device arrays) with ONE eigensolver launch.  ``models``: list of dicts with
+    ``H`` (DeviceHops), ``Lk`` (keys d x nL int64, F order), ``rho`` (device nL x n x n
+    complex), ``om`` (device omegas), ``dos`` (device nw), ``bands`` (device nk x n).
+    Returns the band energies."""
+    ctx = ctx or default_context()
+    nm = len(models)
+    arr = ctypes.c_void_p * nm
+    Hs = arr(*[m["H"].handle.value if isinstance(m["H"].handle, ctypes.c_void_p) else m["H"].handle for m in models])
+    nL = np.array([m["Lk"].shape[1] for m in models], dtype=np.int64)
+    Lk = arr(*[m["Lk"].ctypes.data for m in models])
+    rho = arr(*[m["rho"].data_ptr() for m in models])
+    om = arr(*[m["om"].data_ptr() for m in models])
+    dos = arr(*[m["dos"].data_ptr() for m in models])
+    bands = arr(*[m["bands"].data_ptr() for m in models])
+    eb = np.zeros(nm)
+    nw = int(models[0]["om"].numel())
+    ctx.check(_lib.lqm_bands_dos_rho_multi_dev(ctx.handle, nm, ctypes.cast(Hs, _P), int(nk), _ptr(d_ks), _ptr(d_w),
+                                               float(mu), float(T), _ptr(nL), ctypes.cast(Lk, _P),
+                                               ctypes.cast(rho, _P), _ptr(eb), nw, ctypes.cast(om, _P), float(gamma),
+                                               ctypes.cast(dos, _P), ctypes.cast(bands, _P)))
+    return eb
