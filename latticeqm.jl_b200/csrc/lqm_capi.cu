@@ -253,7 +253,7 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2, WS_GEMMSPLIT
 };
 static_assert(WS_UNIW < 48, "workspace slots");
 
@@ -338,8 +338,8 @@ struct RhoOut {
 };
 
 // ---- blocked large-n path (lqm_large.cuh) ----
-// The queue of the library's batched GEMMs: the context's stream.
-cudaStream_t blas_handle(lqm_ctx* ctx) { return ctx->stream; }
+// The library's batched GEMMs run on the context's stream (and its workspace).
+lqm_ctx* blas_handle(lqm_ctx* ctx) { return ctx; }
 
 template <int BM, int BN, int WM, int WN, int BK, int ST>
 void launch_zgemm_dmma(cudaStream_t st, const GemmArgs& g, int batch) {
@@ -363,12 +363,31 @@ void launch_zgemm_dmma(cudaStream_t st, const GemmArgs& g, int batch) {
 // the library's DMMA kernel (lqm_zgemm.cuh), with the tile shape chosen by the
 // product's shape (skinny n: the Fourier fold; small m: the back-transformation's
 // panel products; short k: the rank-2nb updates).
-void zgemm_sb(cudaStream_t h, GemmOp ta, GemmOp tb, int m, int n, int k, double alpha_re, const double2* A, int lda,
+void zgemm_sb(lqm_ctx* ctx, GemmOp ta, GemmOp tb, int m, int n, int k, double alpha_re, const double2* A, int lda,
               long long sA, const double2* B, int ldb, long long sB, double beta_re, double2* C, int ldc, long long sC,
               int batch) {
   if (m <= 0 || n <= 0 || batch <= 0) return;
   if (batch > 65535) fail(LQM_EINVAL, "GEMM batch %d exceeds the grid limit", batch);
-  GemmArgs g{m, n, k, alpha_re, beta_re, A, lda, sA, B, ldb, sB, C, ldc, sC, (int)ta, (int)tb};
+  cudaStream_t h = ctx->stream;
+  GemmArgs g{m, n, k, alpha_re, beta_re, A, lda, sA, B, ldb, sB, C, ldc, sC, (int)ta, (int)tb, 0, k};
+  // a single product with few output tiles and a long k (the Fourier fold of small
+  // orders): split k over the SMs, partial products in a workspace, then an ordered sum
+  const int64_t tiles = (int64_t)((m + 127) / 128) * ((n + 15) / 16);
+  if (batch == 1 && n <= 16 && k >= 1024 && tiles < 2 * (int64_t)ctx->num_sms) {
+    int nsplit = (int)std::min<int64_t>((2 * ctx->num_sms + tiles - 1) / tiles, k / 512);
+    nsplit = std::max(2, std::min(nsplit, 64));
+    const int kc = (k + nsplit - 1) / nsplit;
+    nsplit = (k + kc - 1) / kc;
+    double2* P = (double2*)ws_get(ctx, WS_GEMMSPLIT, (size_t)nsplit * m * n * sizeof(double2));
+    GemmArgs gs = g;
+    gs.beta = 0.0; gs.C = P; gs.ldc = m; gs.sC = (long long)m * n; gs.split = 1; gs.k = kc; gs.ktot = k;
+    launch_zgemm_dmma<128, 16, 32, 16, 8, 3>(h, gs, nsplit);
+    const int64_t mn = (int64_t)m * n;
+    zgemm_split_reduce_kernel<<<(unsigned)std::min<int64_t>((mn + 255) / 256, 8 * ctx->num_sms), 256, 0, h>>>(
+        m, n, nsplit, P, beta_re, C, ldc);
+    ck(cudaGetLastError(), "zgemm split launch");
+    return;
+  }
   if (n <= 16)
     launch_zgemm_dmma<128, 16, 32, 16, 8, 3>(h, g, batch);
   else if (m <= 32)
@@ -450,7 +469,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   double* ee = dd + B * (int64_t)n;                   // B x n
   double* slots = (double*)ws_get(ctx, WS_LDC, (size_t)G * slotd * sizeof(double));
   const DCPlan& plan = get_plan(ctx, n);
-  cudaStream_t h = blas_handle(ctx);
+  lqm_ctx* h = blas_handle(ctx);
   ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
      "smem attr");
   ck(cudaFuncSetAttribute(blk_symv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvTmaSmem),

@@ -57,6 +57,9 @@ struct GemmArgs {
   int ldc;
   long long sC;
   int opA, opB;
+  // split-K (batch 1): blockIdx.z is the k-chunk, chunk z covers [z k, z k + k) of
+  // ktot and writes its own C_z = C + z sC with beta = 0; 0 = plain batched product
+  int split, ktot;
 };
 
 // Stage one K-slice [k0, k0 + 8) of op(A) (BM rows) and op(B) (BN columns) into
@@ -64,14 +67,14 @@ struct GemmArgs {
 // row / column index, the other ops along k; threads follow the contiguous index.
 template <int BM, int BN, int NT, int BK>
 __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, const double2* B, int m0, int n0,
-                                           int k0, double2* As, double2* Bs) {
+                                           int k0, int kend, double2* As, double2* Bs) {
   constexpr int P = gemm_pitch(BK);
 #pragma unroll
   for (int e = threadIdx.x; e < BM * BK; e += NT) {
     int r, kk;
     if (g.opA == OP_N) { r = e % BM; kk = e / BM; } else { kk = e % BK; r = e / BK; }
     const int gm = m0 + r, gk = k0 + kk;
-    const bool ok = gm < g.m && gk < g.k;
+    const bool ok = gm < g.m && gk < kend;
     const double2* src = (g.opA == OP_N) ? A + gm + (int64_t)gk * g.lda : A + gk + (int64_t)gm * g.lda;
     gemm_cp16(As + r * P + kk, ok ? (const void*)src : (const void*)A, ok);
   }
@@ -80,7 +83,7 @@ __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, 
     int c, kk;
     if (g.opB == OP_N) { kk = e % BK; c = e / BK; } else { c = e % BN; kk = e / BN; }
     const int gn = n0 + c, gk = k0 + kk;
-    const bool ok = gn < g.n && gk < g.k;
+    const bool ok = gn < g.n && gk < kend;
     const double2* src = (g.opB == OP_N) ? B + gk + (int64_t)gn * g.ldb : B + gn + (int64_t)gk * g.ldb;
     gemm_cp16(Bs + c * P + kk, ok ? (const void*)src : (const void*)B, ok);
   }
@@ -97,9 +100,19 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
   extern __shared__ __align__(16) unsigned char gemm_smem[];
   double2* sm = (double2*)gemm_smem;
   const int64_t b = blockIdx.z;
-  const double2* A = g.A + b * g.sA;
-  const double2* B = g.B + b * g.sB;
+  const double2* A = g.A;
+  const double2* B = g.B;
   double2* C = g.C + b * g.sC;
+  int kend = g.k;  // k bound of this block's slice, relative to A and B
+  if (g.split) {
+    const int64_t kb = b * (int64_t)g.k;  // first k of the chunk
+    A += (g.opA == OP_N) ? kb * g.lda : kb;
+    B += (g.opB == OP_N) ? kb : kb * g.ldb;
+    kend = (int)(g.ktot - kb < g.k ? g.ktot - kb : g.k);
+  } else {
+    A += b * g.sA;
+    B += b * g.sB;
+  }
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm0 = (warp % (BM / WM)) * WM, wn0 = (warp / (BM / WM)) * WN;
@@ -113,10 +126,10 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
 #pragma unroll
     for (int j = 0; j < NJ; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
 
-  const int nks = (g.k + BK - 1) / BK;
+  const int nks = (kend + BK - 1) / BK;
 #pragma unroll
   for (int s = 0; s < ST - 1; ++s) {
-    if (s < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, s * BK, sm + s * STAGE, sm + s * STAGE + BM * P);
+    if (s < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, s * BK, kend, sm + s * STAGE, sm + s * STAGE + BM * P);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
   for (int ks = 0; ks < nks; ++ks) {
@@ -125,11 +138,11 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
       __syncthreads();
       const int nx = ks + ST - 1;
       const int st = nx % ST;
-      if (nx < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, nx * BK, sm + st * STAGE, sm + st * STAGE + BM * P);
+      if (nx < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, nx * BK, kend, sm + st * STAGE, sm + st * STAGE + BM * P);
       asm volatile("cp.async.commit_group;\n" ::: "memory");
     } else {  // one buffer: load, wait, compute, and fence the buffer before the next load
       __syncthreads();
-      gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, ks * BK, sm, sm + BM * P);
+      gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, ks * BK, kend, sm, sm + BM * P);
       asm volatile("cp.async.commit_group;\n" ::: "memory");
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       __syncthreads();
@@ -186,6 +199,25 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
         *p = v;
       }
     }
+  }
+}
+
+// Split-K finish: C = sum_z P_z + beta C in chunk order (P_z = C_z of the chunks,
+// m x n each, leading dimension m).
+__global__ void __launch_bounds__(256) zgemm_split_reduce_kernel(int m, int n, int nsplit, const double2* P,
+                                                                 double beta, double2* C, int ldc) {
+  const int64_t mn = (int64_t)m * n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < mn; t += (int64_t)gridDim.x * blockDim.x) {
+    double2 acc = P[t];
+    for (int z = 1; z < nsplit; ++z) acc = cadd(acc, P[z * mn + t]);
+    const int64_t i = t % m, j = t / m;
+    double2* c = C + i + j * (int64_t)ldc;
+    if (beta != 0.0) {
+      const double2 o = *c;
+      acc.x += beta * o.x;
+      acc.y += beta * o.y;
+    }
+    *c = acc;
   }
 }
 
