@@ -612,9 +612,21 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
           n, Ucur, d_bands + k0 * n, mu, T, w + k0, A, ebk + k0, c0, K, complement ? 1 : 0);
       ctx->launches++;
       if (K > 0) {
-        zgemm_sb(h, OP_N, OP_C, n, n, K, complement ? -1.0 : 1.0, A, n, nn, Ucur + (int64_t)c0 * n,
-                 n, nn, 0.0, rhok + k0 * nn, n, nn, nbk);
-        ctx->launches++;
+        // rho_k is Hermitian: the lower column blocks by GEMM, the upper part mirrored
+        const int cb = 128;
+        const double al = complement ? -1.0 : 1.0;
+        for (int cs = 0; cs < n; cs += cb) {
+          const int cw = std::min(cb, n - cs);
+          zgemm_sb(h, OP_N, OP_C, n - cs, cw, K, al, A + cs, n, nn, Ucur + (int64_t)c0 * n + cs, n, nn, 0.0,
+                   rhok + k0 * nn + cs + (int64_t)cs * n, n, nn, nbk);
+          ctx->launches++;
+        }
+        const int nt32 = (n + 31) / 32;
+        if (nt32 > 1) {
+          blk_herm_mirror_kernel<<<dim3((unsigned)(nt32 * (nt32 - 1) / 2), (unsigned)nbk), 256, 0, ctx->stream>>>(
+              n, rhok + k0 * nn);
+          ctx->launches++;
+        }
       } else {
         ck(cudaMemsetAsync(rhok + k0 * nn, 0, (size_t)(nbk * nn) * sizeof(double2), ctx->stream), "memset");
       }

@@ -618,6 +618,31 @@ __global__ void __launch_bounds__(kBlkThreads) blk_scale_f_cols_kernel(int n, co
   }
 }
 
+// rho_k is Hermitian and only its lower column blocks are formed: the strictly upper
+// part of each 32 x 32 tile pair (I < J) is the conjugate transpose of tile (J, I),
+// moved through shared memory so both the reads and the writes are coalesced.
+// grid (tiles above the diagonal (J > I) of the 32-tile grid, nk).
+__global__ void __launch_bounds__(256) blk_herm_mirror_kernel(int n, double2* R) {
+  __shared__ double2 t[32][33];
+  const int nt = (n + 31) / 32;
+  int p = blockIdx.x, I = 0;  // p-th pair (I, J), J > I, row-major over I
+  while (p >= nt - 1 - I) { p -= nt - 1 - I; ++I; }
+  const int J = I + 1 + p;
+  double2* Rk = R + (int64_t)blockIdx.y * n * n;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  // read tile (J, I) of the lower part: rows 32J + tx, columns 32I + c
+  for (int c = ty; c < 32; c += 8) {
+    const int r = 32 * J + tx, col = 32 * I + c;
+    if (r < n && col < n) t[c][tx] = Rk[r + (int64_t)col * n];
+  }
+  __syncthreads();
+  // write tile (I, J): rows 32I + tx, columns 32J + c, value conj(R[32J + c, 32I + tx])
+  for (int c = ty; c < 32; c += 8) {
+    const int r = 32 * I + tx, col = 32 * J + c;
+    if (r < n && col < n) Rk[r + (int64_t)col * n] = cconj(t[tx][c]);
+  }
+}
+
 // rho_k = I - (Y U_K^H): the identity added to the diagonal (complement form).
 __global__ void __launch_bounds__(kBlkThreads) blk_add_identity_kernel(int n, double2* R) {
   const int64_t nn = (int64_t)n * n;
