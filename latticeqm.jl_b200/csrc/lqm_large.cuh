@@ -353,12 +353,8 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
     int R, C;
     symv_tile_rc((int)(it - b * ntiles), &R, &C);
     // the stage's copies have landed, and every thread is past the previous tile (so
-    // its stage may be refilled).  One thread polls the mbarrier (bounded) so that the
-    // spin does not take shared-memory bandwidth from the warps still summing; its
-    // verdict is the block's, and then every thread observes the completed phase
-    // once (an immediate test) to acquire the copied data.
-    const int ok = __syncthreads_and(threadIdx.x == 0 ? (mbar_wait_bounded(bars + 8 * stage, parity) ? 1 : 0) : 1);
-    if (ok) mbar_try_wait(bars + 8 * stage, parity);
+    // its stage may be refilled); the verdict of the bounded wait is the block's
+    const int ok = __syncthreads_and(mbar_wait_bounded(bars + 8 * stage, parity) ? 1 : 0);
     if (!ok) {
       if (threadIdx.x == 0) {
         atomicExch(err, 1);
