@@ -653,8 +653,8 @@ def main():
     fl = flops_per_k(n, nR, nR)
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-            "kernel": "blk_symv_pipe_kernel (Householder mat-vec y = A22 v over the lower triangle of the trailing "
-                      "block, all k-points of the batch per launch; one launch per column)",
+            "kernel": "blk_symv_tma_kernel (Householder mat-vec y = A22 v over the lower triangle of the trailing "
+                      "block, 64x64 tiles moved by TMA, all k-points of the batch per launch; one launch per column)",
             "algorithmic_bytes_per_launch": per_launch,
             "algorithmic_bytes_per_k": "16 B x m(m+1)/2 per column, m = n-1-j (sum ~ 16 n^3/6 = 6.2 GB at n=1324)",
             "launches": symv_launches, "kernel_ms": symv_ms, "share_of_step": symv_ms / 1e3 / elapsed,

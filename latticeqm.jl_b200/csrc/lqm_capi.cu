@@ -399,6 +399,21 @@ void zgemm_sb(lqm_ctx* ctx, GemmOp ta, GemmOp tb, int m, int n, int k, double al
   ck(cudaGetLastError(), "zgemm launch");
 }
 
+// Hermitian rank-2k update of the lower triangle of a batch of m x m blocks:
+//   C_b -= X_b Y_b^H + Y_b X_b^H  (X, Y: m x k, column-major, strided),
+// one launch, both products summed in one k-loop (C read and written once), tiles
+// entirely above the diagonal skipped.  The upper triangle's tiles that straddle the
+// diagonal are written too (it is never read).
+void zher2k_lower(lqm_ctx* ctx, int m, int k, const double2* X, int ldx, long long sX, const double2* Y, int ldy,
+                  long long sY, double2* C, int ldc, long long sC, int batch) {
+  if (m <= 0 || k <= 0 || batch <= 0) return;
+  if (batch > 65535) fail(LQM_EINVAL, "GEMM batch %d exceeds the grid limit", batch);
+  GemmArgs g{m, m, k, -1.0, 1.0, X, ldx, sX, Y, ldy, sY, C, ldc, sC, (int)OP_N, (int)OP_C, 0, k,
+             Y, ldy, sY, X, ldx, sX, k, 1};
+  launch_zgemm_dmma<64, 64, 32, 16, 8, 3>(ctx->stream, g, batch);
+  ck(cudaGetLastError(), "zher2k launch");
+}
+
 struct RhoOut;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR);
 
@@ -533,21 +548,13 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       if (j0 + nbp < n) {
         blk_finish_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0, nbp - 1);
         ctx->launches++;
-        // A22 -= V W^H + W V^H on the lower triangle: column blocks [c0, c1) x rows [c0, m2)
+        // A22 -= V W^H + W V^H on the lower triangle, one launch
         const int m2 = n - j0 - nbp;
-        const int cbw = 256;
-        for (int c0 = 0; c0 < m2; c0 += cbw) {
-          const int cw = std::min(cbw, m2 - c0);
-          const int rows = m2 - c0;
-          double2* Cb = A + (j0 + nbp + c0) + (int64_t)(j0 + nbp + c0) * n;
-          const double2* Vr = A + (j0 + nbp + c0) + (int64_t)j0 * n;
-          const double2* Wr = W + (j0 + nbp + c0);
-          zgemm_sb(h, OP_N, OP_C, rows, cw, nbp, -1.0, Vr, n, nn, Wr, n, (long long)n * nb, 1.0, Cb, n,
-                   nn, nbk);
-          zgemm_sb(h, OP_N, OP_C, rows, cw, nbp, -1.0, Wr, n, (long long)n * nb, Vr, n, nn, 1.0, Cb, n,
-                   nn, nbk);
-          ctx->launches += 2;
-        }
+        double2* Cb = A + (j0 + nbp) + (int64_t)(j0 + nbp) * n;
+        const double2* Vr = A + (j0 + nbp) + (int64_t)j0 * n;
+        const double2* Wr = W + (j0 + nbp);
+        zher2k_lower(h, m2, nbp, Vr, n, nn, Wr, n, (long long)n * nb, Cb, n, nn, nbk);
+        ctx->launches += 1;
       }
     }
     ck(cudaGetLastError(), "blocked reduction launch");

@@ -35,7 +35,7 @@ struct EighVec {
   double *d, *e, *D, *z, *dl, *zl, *troot, *zhat, *vals, *dval, *rc, *rs, *nrho, *red;  // red: 128
   int *perm, *colnd, *org, *dcol, *newpos, *ri, *rj, *nk, *nrot, *ndef;
   double2 *tau, *v, *w, *vn, *pn, *bc, *pbuf;
-  double* tile = nullptr;  // team scratch for the tiled merge update (large n): 6144 doubles + n ints, or null
+  double* tile = nullptr;  // team scratch for the tiled merge update (large n): kDcTileRing doubles + n ints, or null
 };
 
 // ---------------------------------------------------------------------------
@@ -425,13 +425,15 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 
 // Merge update of one node as a tiled GEMM (large merges):
 //   Qt[lo + r, newpos[it]] = sum_p Q[lo + r, colnd[p]] * Ubn[it + p*k],
-// r < hi - lo, it < k (Ubn holds the secular vectors as rows); p is summed in
-// ascending order.  A 512-thread team uses 128 x 128 output tiles (4 x 8 per
-// thread: rows 2t, 2t+1, 64+2t, 65+2t of the tile so that the lanes of a warp
-// read consecutive 16-byte words) and 8-deep p stages moved by cp.async
-// through a 3-stage ring in `tile` (3 x 2048 doubles, followed by room for k
-// column indices), two stages in flight while one is summed; other team sizes
-// (the host emulation) take the plain loop.
+// r < hi - lo, it < k (Ubn holds the secular vectors as rows).  A 512-thread
+// team computes 128 x 128 output tiles on the FP64 tensor path (DMMA
+// m8n8k4): 16 warps of 32 x 32, each a 4 x 4 grid of 8 x 8 accumulators.  The
+// p range moves in 8-deep stages by cp.async through a 3-stage ring in `tile`
+// (per stage 8 rows of 128 + 4 doubles for Q and for Ubn, p-major; the pitch of
+// 132 == 4 mod 16 puts the 16 fragment reads of a half-warp on distinct bank
+// pairs), followed by room for k column indices; two stages are in flight while
+// one is summed.  p is summed in ascending 4-deep steps.  Other team sizes (the
+// host emulation) take the plain loop.
 #if defined(__CUDA_ARCH__)
 __device__ __forceinline__ void lqm_cp_async8(void* sdst, const void* gsrc, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
@@ -439,35 +441,42 @@ __device__ __forceinline__ void lqm_cp_async8(void* sdst, const void* gsrc, bool
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(nbytes) : "memory");
 }
 #endif
+constexpr int kDcTileP = 132;                            // staged row pitch (doubles)
+constexpr int kDcTileStage = 8 * 2 * kDcTileP;           // doubles per stage (Q and Ubn slices)
+constexpr int kDcTileRing = 3 * kDcTileStage;            // doubles of the ring
 template <class TeamT>
 LQM_FN void dc_tile_gemm(const TeamT& T, int n, int lo, int hi, int k, const int* colnd, const int* newpos,
                          const double* Q, double* Qt, const double* Ubn, double* tile) {
   const int s = hi - lo;
 #if defined(__CUDA_ARCH__)
   if (T.nt == 512 && tile != nullptr) {
-    constexpr int BM = 128, BN = 128, BK = 8, STG = BK * BM + BK * BN, NS = 3;
-    const int tr = T.tid & 31, tc = T.tid >> 5;  // rows 2tr, 2tr+1, 64+2tr, 65+2tr; columns tc*8 .. +7
-    int* cidx = (int*)(tile + NS * STG);         // the node's column indices, staged once
+    constexpr int BM = 128, BN = 128, BK = 8, PT = kDcTileP, STG = kDcTileStage, NS = 3;
+    const int lane = T.tid & 31, warp = T.tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wr = (warp & 3) * 32, wc = (warp >> 2) * 32;  // the warp's 32 x 32 sub-tile
+    int* cidx = (int*)(tile + kDcTileRing);                  // the node's column indices, staged once
     for (int p = T.tid; p < k; p += T.nt) cidx[p] = colnd[p];
     team_sync(T);
     for (int r0 = 0; r0 < s; r0 += BM) {
       for (int c0 = 0; c0 < k; c0 += BN) {
-        double acc[4][8];
+        double acc[4][4][2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int b = 0; b < 8; ++b) acc[q][b] = 0.0;
-        // stage element e = tid + 512 h: A (pp = e / BM, rr = e % BM), B (pb = e / BN, cb = e % BN)
+          for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        // element e = tid + 512 h of a stage: pp = e / 128, row / column e % 128
         auto issue = [&](int p0, int st) {
           double* As = tile + st * STG;
-          double* Bs = As + BK * BM;
+          double* Bs = As + BK * PT;
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int e = T.tid + 512 * h;
-            const int p = p0 + (e >> 7), r = r0 + (e & 127), cc = c0 + (e & 127);
+            const int pp = e >> 7, x = e & 127;
+            const int p = p0 + pp, r = r0 + x, cc = c0 + x;
             const bool oka = p < k && r < s, okb = p < k && cc < k;
-            lqm_cp_async8(As + e, oka ? (const void*)(Q + (lo + r) + (int64_t)cidx[p] * n) : (const void*)Q, oka);
-            lqm_cp_async8(Bs + e, okb ? (const void*)(Ubn + cc + (int64_t)p * k) : (const void*)Ubn, okb);
+            lqm_cp_async8(As + pp * PT + x, oka ? (const void*)(Q + (lo + r) + (int64_t)cidx[p] * n) : (const void*)Q,
+                          oka);
+            lqm_cp_async8(Bs + pp * PT + x, okb ? (const void*)(Ubn + cc + (int64_t)p * k) : (const void*)Ubn, okb);
           }
         };
         const int nst = (k + BK - 1) / BK;
@@ -481,34 +490,33 @@ LQM_FN void dc_tile_gemm(const TeamT& T, int n, int lo, int hi, int k, const int
           if (it + 2 < nst) issue((it + 2) * BK, (it + 2) % NS);
           asm volatile("cp.async.commit_group;\n" ::: "memory");
           const double* As = tile + (it % NS) * STG;
-          const double* Bs = As + BK * BM;
+          const double* Bs = As + BK * PT;
 #pragma unroll
-          for (int pp = 0; pp < BK; ++pp) {
-            const double2 x01 = *(const double2*)(As + pp * BM + tr * 2);
-            const double2 x23 = *(const double2*)(As + pp * BM + 64 + tr * 2);
-            const double xa[4] = {x01.x, x01.y, x23.x, x23.y};
-            double ya[8];
+          for (int kk = 0; kk < BK; kk += 4) {
+            double a[4], b[4];
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-              const double2 y2 = *(const double2*)(Bs + pp * BN + tc * 8 + 2 * b);
-              ya[2 * b] = y2.x;
-              ya[2 * b + 1] = y2.y;
-            }
+            for (int i = 0; i < 4; ++i) a[i] = As[(kk + t) * PT + wr + 8 * i + g];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + t) * PT + wc + 8 * j + g];
 #pragma unroll
-              for (int b = 0; b < 8; ++b) acc[q][b] += xa[q] * ya[b];
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int j = 0; j < 4; ++j) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
           }
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
         team_sync(T);  // the ring is free before the next tile's prologue
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int i = 0; i < 4; ++i) {
+          const int r = r0 + wr + 8 * i + g;
 #pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            const int r = r0 + ((q < 2) ? tr * 2 + q : 64 + tr * 2 + (q - 2)), cc = c0 + tc * 8 + b;
-            if (r < s && cc < k) Qt[(lo + r) + (int64_t)newpos[cc] * n] = acc[q][b];
-          }
+          for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int cc = c0 + wc + 8 * j + 2 * t + h;
+              if (r < s && cc < k) Qt[(lo + r) + (int64_t)newpos[cc] * n] = acc[i][j][h];
+            }
+        }
       }
     }
     return;

@@ -478,7 +478,7 @@ __host__ __device__ inline int64_t dc_large_slot_doubles(int n, bool vec) {
 }
 
 // dynamic shared memory: the merge GEMM's cp.async ring and the column indices of one merge
-__host__ __device__ inline int dc_tile_smem(int n) { return 6144 * 8 + ((n + 3) / 4) * 16; }
+__host__ __device__ inline int dc_tile_smem(int n) { return kDcTileRing * 8 + ((n + 3) / 4) * 16; }
 
 // NT = 512 (one CTA per SM) for orders with tiled merges; below kDcTileMin the
 // merges are small and latency-bound, and NT = 128 with four CTAs per SM keeps

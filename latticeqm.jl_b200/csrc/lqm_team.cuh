@@ -42,6 +42,15 @@ LQM_FN Team make_team() {
 LQM_FN void team_sync() { __syncthreads(); }
 LQM_FN void team_sync(const Team&) { __syncthreads(); }
 
+// One FP64 tensor-core step D = A B + D of mma.sync.aligned.m8n8k4 (row-major A,
+// column-major B): with g = lane / 4, t = lane % 4 the lane holds a = A[g][t],
+// b = B[t][g] and d0, d1 = D[g][2t], D[g][2t + 1] (PTX ISA fragment layout).
+LQM_FN void dmma_884(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // One of the independent teams of `size` threads (a multiple of 32) that split a
 // CTA: thread threadIdx.x belongs to team threadIdx.x / size, which synchronises on
 // its own named barrier (1 + team index; at most 15 teams per CTA).  The per-k

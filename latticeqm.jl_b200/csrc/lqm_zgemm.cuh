@@ -32,11 +32,7 @@ enum GemmOp { OP_N = 0, OP_T = 1, OP_C = 2 };
 // complex elements per staged row: BK + 4 (== 4 mod 8: conflict-free fragment reads)
 __host__ __device__ constexpr int gemm_pitch(int BK) { return BK + 4; }
 
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) { dmma_884(d0, d1, a, b); }
 
 __device__ __forceinline__ void gemm_cp16(void* sdst, const void* gsrc, bool valid) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
@@ -60,14 +56,26 @@ struct GemmArgs {
   // split-K (batch 1): blockIdx.z is the k-chunk, chunk z covers [z k, z k + k) of
   // ktot and writes its own C_z = C + z sC with beta = 0; 0 = plain batched product
   int split, ktot;
+  // optional second operand pair summed after the first (k2 > 0, same ops):
+  //   C = alpha (op(A) op(B) + op(A2) op(B2)) + beta C,  the k-sum of A2 B2 after A B
+  const double2* A2;
+  int lda2;
+  long long sA2;
+  const double2* B2;
+  int ldb2;
+  long long sB2;
+  int k2;
+  // lower != 0: C starts on a diagonal of a Hermitian block; tiles entirely above
+  // it (every row < every column) are skipped
+  int lower;
 };
 
 // Stage one K-slice [k0, k0 + 8) of op(A) (BM rows) and op(B) (BN columns) into
 // As[row][kk], Bs[col][kk].  op N of A / op T,C of B are contiguous along the
 // row / column index, the other ops along k; threads follow the contiguous index.
 template <int BM, int BN, int NT, int BK>
-__device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, const double2* B, int m0, int n0,
-                                           int k0, int kend, double2* As, double2* Bs) {
+__device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, int lda, const double2* B, int ldb,
+                                           int m0, int n0, int k0, int kend, double2* As, double2* Bs) {
   constexpr int P = gemm_pitch(BK);
 #pragma unroll
   for (int e = threadIdx.x; e < BM * BK; e += NT) {
@@ -75,7 +83,7 @@ __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, 
     if (g.opA == OP_N) { r = e % BM; kk = e / BM; } else { kk = e % BK; r = e / BK; }
     const int gm = m0 + r, gk = k0 + kk;
     const bool ok = gm < g.m && gk < kend;
-    const double2* src = (g.opA == OP_N) ? A + gm + (int64_t)gk * g.lda : A + gk + (int64_t)gm * g.lda;
+    const double2* src = (g.opA == OP_N) ? A + gm + (int64_t)gk * lda : A + gk + (int64_t)gm * lda;
     gemm_cp16(As + r * P + kk, ok ? (const void*)src : (const void*)A, ok);
   }
 #pragma unroll
@@ -84,7 +92,7 @@ __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, 
     if (g.opB == OP_N) { kk = e % BK; c = e / BK; } else { c = e % BN; kk = e / BN; }
     const int gn = n0 + c, gk = k0 + kk;
     const bool ok = gn < g.n && gk < kend;
-    const double2* src = (g.opB == OP_N) ? B + gk + (int64_t)gn * g.ldb : B + gn + (int64_t)gk * g.ldb;
+    const double2* src = (g.opB == OP_N) ? B + gk + (int64_t)gn * ldb : B + gn + (int64_t)gk * ldb;
     gemm_cp16(Bs + c * P + kk, ok ? (const void*)src : (const void*)B, ok);
   }
 }
@@ -100,8 +108,12 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
   extern __shared__ __align__(16) unsigned char gemm_smem[];
   double2* sm = (double2*)gemm_smem;
   const int64_t b = blockIdx.z;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (g.lower && m0 + BM <= n0) return;  // above the diagonal (uniform per block)
   const double2* A = g.A;
   const double2* B = g.B;
+  const double2* A2 = g.A2 + b * g.sA2;
+  const double2* B2 = g.B2 + b * g.sB2;
   double2* C = g.C + b * g.sC;
   int kend = g.k;  // k bound of this block's slice, relative to A and B
   if (g.split) {
@@ -113,7 +125,6 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
     A += b * g.sA;
     B += b * g.sB;
   }
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int wm0 = (warp % (BM / WM)) * WM, wn0 = (warp / (BM / WM)) * WN;
   const int gr = lane >> 2, gt = lane & 3;
@@ -126,10 +137,18 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
 #pragma unroll
     for (int j = 0; j < NJ; ++j) re[i][j][0] = re[i][j][1] = im[i][j][0] = im[i][j][1] = 0.0;
 
-  const int nks = (kend + BK - 1) / BK;
+  // slices [0, nks1) from (A, B), then [nks1, nks) from (A2, B2)
+  const int nks1 = (kend + BK - 1) / BK;
+  const int nks = nks1 + (g.k2 > 0 ? (g.k2 + BK - 1) / BK : 0);
+  auto stage = [&](int s, double2* dst) {
+    if (s < nks1)
+      gemm_stage<BM, BN, NT, BK>(g, A, g.lda, B, g.ldb, m0, n0, s * BK, kend, dst, dst + BM * P);
+    else
+      gemm_stage<BM, BN, NT, BK>(g, A2, g.lda2, B2, g.ldb2, m0, n0, (s - nks1) * BK, g.k2, dst, dst + BM * P);
+  };
 #pragma unroll
   for (int s = 0; s < ST - 1; ++s) {
-    if (s < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, s * BK, kend, sm + s * STAGE, sm + s * STAGE + BM * P);
+    if (s < nks) stage(s, sm + s * STAGE);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
   for (int ks = 0; ks < nks; ++ks) {
@@ -138,11 +157,11 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
       __syncthreads();
       const int nx = ks + ST - 1;
       const int st = nx % ST;
-      if (nx < nks) gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, nx * BK, kend, sm + st * STAGE, sm + st * STAGE + BM * P);
+      if (nx < nks) stage(nx, sm + st * STAGE);
       asm volatile("cp.async.commit_group;\n" ::: "memory");
     } else {  // one buffer: load, wait, compute, and fence the buffer before the next load
       __syncthreads();
-      gemm_stage<BM, BN, NT, BK>(g, A, B, m0, n0, ks * BK, kend, sm, sm + BM * P);
+      stage(ks, sm);
       asm volatile("cp.async.commit_group;\n" ::: "memory");
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       __syncthreads();
