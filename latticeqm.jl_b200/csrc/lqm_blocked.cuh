@@ -261,22 +261,28 @@ LQM_FN void blk_prep_reflectors(const Team& T, int n, double2* A, int lda) {
 // Compact WY factor of reflectors j0 .. j0+nbr-1 (LAPACK zlarft, forward,
 // column-wise): H_{j0} ... H_{j0+nbr-1} = I - V Tm V^H, Tm upper triangular
 // (nb x nb, leading dimension nb, zero-padded).  V(:, l) = A(j0+1:, j0+l) after
-// blk_prep_reflectors.  G: nb*nb complex team scratch.
+// blk_prep_reflectors.  G: nb*nb complex team scratch for the Gram matrix V^H V,
+// formed here from V or, with Gg != null, copied from Gg (nb x nb, leading
+// dimension nb, formed beforehand by a GEMM).
 LQM_FN void blk_larft(const Team& T, int n, int nb, int j0, int nbr, const double2* A, int lda, const double2* tau,
-                      double2* Tm, double2* G) {
+                      double2* Tm, double2* G, const double2* Gg = nullptr) {
   const int m = n - j0 - 1;
   const double2* V = A + (int64_t)j0 * lda + (j0 + 1);
-  for (int p = T.wid; p < nb * nb; p += T.nw) {
-    const int q = p % nb, l = p / nb;
-    if (!(q < l && l < nbr)) continue;
-    double sr = 0.0, si = 0.0;
-    for (int r = l + T.lane; r < m; r += T.nl) {
-      const double2 x = cmulc(V[r + (int64_t)q * lda], V[r + (int64_t)l * lda]);
-      sr += x.x; si += x.y;
+  if (Gg) {
+    for (int p = T.tid; p < nb * nb; p += T.nt) G[p] = Gg[p];
+  } else {
+    for (int p = T.wid; p < nb * nb; p += T.nw) {
+      const int q = p % nb, l = p / nb;
+      if (!(q < l && l < nbr)) continue;
+      double sr = 0.0, si = 0.0;
+      for (int r = l + T.lane; r < m; r += T.nl) {
+        const double2 x = cmulc(V[r + (int64_t)q * lda], V[r + (int64_t)l * lda]);
+        sr += x.x; si += x.y;
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if (T.lane == 0) G[q + l * nb] = cmk(sr, si);
     }
-    sr = warp_sum(sr);
-    si = warp_sum(si);
-    if (T.lane == 0) G[q + l * nb] = cmk(sr, si);
   }
   for (int p = T.tid; p < nb * nb; p += T.nt) {
     const int q = p % nb, l = p / nb;

@@ -253,9 +253,9 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2, WS_GEMMSPLIT
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2, WS_GEMMSPLIT, WS_GRAM
 };
-static_assert(WS_UNIW < 48, "workspace slots");
+static_assert(WS_GRAM < 48, "workspace slots");
 
 }  // namespace
 #include "lqm_comm.inc"
@@ -459,10 +459,13 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   const int n = (int)H->n;
   const int nb = kBlkNB;
   const int P = (n + nb - 1) / nb;
+  const int nbt = kBlkNBT;                // back-transformation panels
+  const int P2 = (n + nbt - 1) / nbt;
+  const int wc = std::max(nb, nbt);       // columns of W / X and of Y per k-point
   const bool vec = d_U || rhok;
   const int64_t nn = (int64_t)n * n;
   const int64_t pstride = symv_part_stride(n), tstride = t12_part_stride(n, nb);
-  const int64_t auxk = 2 * (int64_t)n * nb /*W, Y*/ + (int64_t)nb * nb * P /*Tm*/ + n /*tau*/ + 2 * nb /*t12*/ +
+  const int64_t auxk = 2 * (int64_t)n * wc /*W, Y*/ + (int64_t)nbt * nbt * P2 /*Tm*/ + n /*tau*/ + 2 * nb /*t12*/ +
                        pstride /*mat-vec partials*/ + tstride /*panel-product partials*/;
   const double per_k = 16.0 * (double)nn * ((vec && !d_U) ? 2.0 : 1.0) + 16.0 * (double)auxk + 16.0 * n;
   int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(48.0e9 / per_k)));
@@ -473,10 +476,10 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   double2* A = (double2*)ws_get(ctx, WS_LA, (size_t)B * nn * sizeof(double2));
   double2* Uw = (vec && !d_U) ? (double2*)ws_get(ctx, WS_LU, (size_t)B * nn * sizeof(double2)) : nullptr;
   double2* aux = (double2*)ws_get(ctx, WS_LAUX, (size_t)B * (auxk + n) * sizeof(double2));
-  double2* W = aux;                                   // B x (n x nb); reused as X (nb x n) in the back-transform
-  double2* Yb = W + B * (int64_t)n * nb;              // B x (nb x n)
-  double2* Tm = Yb + B * (int64_t)n * nb;             // B x P x (nb x nb)
-  double2* tau = Tm + B * (int64_t)nb * nb * P;       // B x n
+  double2* W = aux;                                   // B x (n x nb); reused as X (nbt x n) in the back-transform
+  double2* Yb = W + B * (int64_t)n * wc;              // B x (nbt x n)
+  double2* Tm = Yb + B * (int64_t)n * wc;             // B x P2 x (nbt x nbt)
+  double2* tau = Tm + B * (int64_t)nbt * nbt * P2;    // B x n
   double2* t12 = tau + B * (int64_t)n;                // B x 2nb
   double2* part = t12 + B * 2 * (int64_t)nb;          // B x pstride
   double2* tpart = part + B * pstride;                // B x tstride
@@ -594,23 +597,39 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     }
     if (K > 0) {
       blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A);
-      blk_larft_kernel<<<dim3((unsigned)P, (unsigned)nbk), kBlkThreads, nb * nb * sizeof(double2), ctx->stream>>>(
-          n, nb, P, A, tau, Tm);
-      ctx->launches += 2;
+      ctx->launches++;
+      // Gram matrices G_p = V_p^H V_p of the back-transformation's panels (V explicit
+      // and zero above its unit diagonal after blk_prep_kernel), then Tm from them
+      const long long g2 = (long long)nbt * nbt;
+      double2* G = (double2*)ws_get(ctx, WS_GRAM, (size_t)nbk * P2 * g2 * sizeof(double2));
+      for (int p = 0; p < P2; ++p) {
+        const int j0 = p * nbt;
+        const int nbr = std::min(nbt, n - 1 - j0);
+        if (nbr <= 0) continue;
+        const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
+        zgemm_sb(h, OP_C, OP_N, nbr, nbr, n - j0 - 1, 1.0, V, n, nn, V, n, nn, 0.0, G + p * g2, nbt,
+                 (long long)P2 * g2, nbk);
+        ctx->launches++;
+      }
+      const size_t lsm = (size_t)g2 * sizeof(double2);
+      ck(cudaFuncSetAttribute(blk_larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm), "smem attr");
+      blk_larft_kernel<<<dim3((unsigned)P2, (unsigned)nbk), kBlkThreads, lsm, ctx->stream>>>(n, nbt, P2, A, tau,
+                                                                                             Tm, G);
+      ctx->launches++;
     }
-    for (int p = P - 1; p >= 0 && K > 0; --p) {
-      const int j0 = p * nb;
-      const int nbr = std::min(nb, n - 1 - j0);
+    for (int p = P2 - 1; p >= 0 && K > 0; --p) {
+      const int j0 = p * nbt;
+      const int nbr = std::min(nbt, n - 1 - j0);
       if (nbr <= 0) continue;
       const int m = n - j0 - 1;
       const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
       double2* Us = Ucur + (j0 + 1) + (int64_t)c0 * n;
       // X = V^H Us (nbr x K), Y = Tm X, Us -= V Y
-      zgemm_sb(h, OP_C, OP_N, nbr, K, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nb, (long long)n * nb,
+      zgemm_sb(h, OP_C, OP_N, nbr, K, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nbt, (long long)n * nbt,
                nbk);
-      zgemm_sb(h, OP_N, OP_N, nbr, K, nbr, 1.0, Tm + (int64_t)p * nb * nb, nb,
-               (long long)nb * nb * P, W, nb, (long long)n * nb, 0.0, Yb, nb, (long long)n * nb, nbk);
-      zgemm_sb(h, OP_N, OP_N, m, K, nbr, -1.0, V, n, nn, Yb, nb, (long long)n * nb, 1.0, Us, n, nn,
+      zgemm_sb(h, OP_N, OP_N, nbr, K, nbr, 1.0, Tm + (int64_t)p * nbt * nbt, nbt,
+               (long long)nbt * nbt * P2, W, nbt, (long long)n * nbt, 0.0, Yb, nbt, (long long)n * nbt, nbk);
+      zgemm_sb(h, OP_N, OP_N, m, K, nbr, -1.0, V, n, nn, Yb, nbt, (long long)n * nbt, 1.0, Us, n, nn,
                nbk);
       ctx->launches += 3;
     }

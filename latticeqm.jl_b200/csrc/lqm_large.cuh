@@ -22,7 +22,8 @@
 
 namespace lqm {
 
-constexpr int kBlkNB = 32;      // panel width (reflectors per panel)
+constexpr int kBlkNB = 32;      // panel width of the reduction (reflectors per panel)
+constexpr int kBlkNBT = 64;     // panel width of the compact-WY back-transformation
 constexpr int kBlkThreads = 256;
 constexpr int kSymvTB = 64;     // mat-vec tile (2 rows per lane of a 32-lane warp)
 constexpr int kDcThreads = 512;
@@ -249,18 +250,25 @@ __global__ void __launch_bounds__(kSymvThreads, 1) blk_symv_pipe_kernel(BlkArgs 
 // box = 8 complex rows x 64 columns x 1 k-point, 128-byte swizzle) that complete
 // on one mbarrier per stage, issued by one thread; rows and columns beyond the
 // matrix read as zeros (out-of-bounds fill), so the tensor map covers the whole
-// batch for every column.  Thread (q', g), q' < 32, g < 16, owns rows q' and
-// q' + 32 of the direct product and the same two columns of the transposed
-// product over u = g + 16 h; with the swizzle both reads are free of bank
-// conflicts.  The 16 partial sums of a row are added by shuffles, and lane g == 0
-// writes them: one block barrier per tile.  Every mbarrier wait is bounded; on
-// expiry the kernel sets *err and stops (the host reports LQM_EDEVICE).
+// batch for every column.
+// Each tile element is read from shared memory once and used for both products:
+// warp w owns the 16 x 16 sub-block (rows 16 (w % 4) .., columns 16 (w / 4) ..);
+// lane (a = lane % 8, b = lane / 8) holds rows a, a + 8 and columns b + 4 i
+// (i < 4) of it (with the swizzle, the eight lanes of each load phase hit eight
+// distinct 16-byte bank groups).  The direct partials (row sums over the lane's
+// columns) are reduced over b and the transposed ones (column sums over its rows)
+// over a, by reduce-scatter shuffles (each step halves what a lane keeps), then
+// written to a double-buffered slot per warp; after the next tile's barrier the
+// four column- (row-) blocks of each row (column) are added in order and written
+// out.  So there is one block barrier per tile.  Every mbarrier wait is bounded;
+// on expiry the kernel sets *err and stops (the host reports LQM_EDEVICE).
 constexpr int kSymvTmaThreads = 512;
 constexpr int kSymvTmaStages = 3;
 constexpr int kSymvTileBytes = kSymvTB * kSymvTB * 16;  // 64 KB
 constexpr int kSymvVecBytes = 2 * kSymvTB * 16;               // v over the tile's rows, then over its columns
-constexpr int kSymvTmaSmem =
-    kSymvTmaStages * (kSymvTileBytes + kSymvVecBytes) + 1024 /* alignment */ + 64 /* mbarriers */;
+constexpr int kSymvRedBytes = 2 * 2 * 4 * kSymvTB * 16;  // [buffer][direct, transposed][block][64] complex
+constexpr int kSymvTmaSmem = kSymvTmaStages * (kSymvTileBytes + kSymvVecBytes) + kSymvRedBytes +
+                             1024 /* alignment */ + 64 /* mbarriers */;
 static_assert(kSymvTmaSmem <= 227 * 1024, "TMA mat-vec pipeline exceeds shared memory");
 constexpr long long kSymvWaitLimit = 1LL << 22;  // mbarrier polls before giving up (well under a second)
 
@@ -318,6 +326,32 @@ __device__ __forceinline__ void symv_tma_issue(const CUtensorMap* map, const CUt
   tma_load_3d(vdst + kSymvTB * 16, vmap, 2 * col0, j, (int)b, bar);
 }
 
+// Finish of one tile from its warp partials (red: [direct, transposed][block][64 rows]
+// complex, as doubles): thread t < 256 adds the four blocks of output o = t / 2,
+// component t % 2, in block order; outputs 0..63 are the direct rows, 64..127 the
+// transposed columns (on a diagonal tile both go to the same row, summed).
+__device__ __forceinline__ void symv_tma_finish(const double* red, double2* part, int nbk, int R, int C) {
+  const int t = threadIdx.x;
+  if (t >= 2 * 2 * kSymvTB) return;
+  const int o = t >> 1, comp = t & 1;
+  const bool diag = (R == C);
+  if (diag && o >= kSymvTB) return;
+  const int kind = o >= kSymvTB ? 1 : 0, x = o & (kSymvTB - 1);
+  const double* src = red + kind * (4 * kSymvTB * 2) + x * 2 + comp;
+  double v = src[0];
+#pragma unroll
+  for (int q = 1; q < 4; ++q) v += src[q * kSymvTB * 2];
+  if (diag) {
+    const double* s2 = red + 4 * kSymvTB * 2 + x * 2 + comp;
+    double w = s2[0];
+#pragma unroll
+    for (int q = 1; q < 4; ++q) w += s2[q * kSymvTB * 2];
+    v += w;
+  }
+  double* dst = (double*)(part + ((int64_t)(kind ? C : R) * nbk + (kind ? R : C)) * kSymvTB + x);
+  dst[comp] = v;
+}
+
 __global__ void __launch_bounds__(kSymvTmaThreads, 1)
     blk_symv_tma_kernel(const __grid_constant__ CUtensorMap map, const __grid_constant__ CUtensorMap vmap, BlkArgs a,
                         int j, int64_t nitems, int* err) {
@@ -327,12 +361,15 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
   unsigned char* tiles = smem_raw + (base - raw);
   const unsigned vbase = base + kSymvTmaStages * kSymvTileBytes;  // v segments of each stage
   const unsigned char* vsm = tiles + kSymvTmaStages * kSymvTileBytes;
-  const unsigned bars = vbase + kSymvTmaStages * kSymvVecBytes;   // one mbarrier per stage
+  double* redsm = (double*)(tiles + kSymvTmaStages * (kSymvTileBytes + kSymvVecBytes));  // 2 buffers
+  const unsigned bars = vbase + kSymvTmaStages * kSymvVecBytes + kSymvRedBytes;  // one mbarrier per stage
   const int m = a.n - j - 1;
   const int nbk = (m + kSymvTB - 1) / kSymvTB;
   const int ntiles = nbk * (nbk + 1) / 2;
   const int64_t first = blockIdx.x, step = gridDim.x;
-  const int g = threadIdx.x & 15, qp = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int la = lane & 7, lb = lane >> 3;
+  const int rw = (warp & 3) * 16, cw = (warp >> 2) * 16;  // the warp's sub-block
   if (*(volatile int*)err != 0) return;  // an earlier launch gave up: the pass is void, end at once
   if (threadIdx.x == 0) {
     for (int s = 0; s < kSymvTmaStages; ++s) mbar_init(bars + 8 * s, 1);
@@ -348,12 +385,16 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
   }
   int stage = 0;
   unsigned parity = 0;
+  int64_t pk = -1;               // k-point of the previous tile (finished after this tile's barrier), or -1
+  int pR = 0, pC = 0;
+  int rb = 0;                    // reduction buffer of this tile
   for (int64_t it = first; it < nitems; it += step) {
     const int64_t b = it / ntiles;
     int R, C;
     symv_tile_rc((int)(it - b * ntiles), &R, &C);
     // the stage's copies have landed, and every thread is past the previous tile (so
-    // its stage may be refilled); the verdict of the bounded wait is the block's
+    // its stage may be refilled and its partials read); the verdict of the bounded
+    // wait is the block's
     const int ok = __syncthreads_and(mbar_wait_bounded(bars + 8 * stage, parity) ? 1 : 0);
     if (!ok) {
       if (threadIdx.x == 0) {
@@ -365,7 +406,7 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
           mbar_wait_bounded(bars + 8 * s1, s1 == 0 ? parity ^ 1u : parity);
         }
       }
-      break;
+      return;
     }
     if (threadIdx.x == 0) {
       const int64_t nx = it + (kSymvTmaStages - 1) * step;
@@ -374,65 +415,80 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
         symv_tma_issue(&map, &vmap, j, ntiles, nx, base + ns * kSymvTileBytes, vbase + ns * kSymvVecBytes,
                        bars + 8 * ns);
     }
+    if (pk >= 0) symv_tma_finish(redsm + (rb ^ 1) * (2 * 4 * kSymvTB * 2), a.part + pk * a.part_stride, nbk, pR, pC);
     const unsigned char* ts = tiles + stage * kSymvTileBytes;
     const double2* vR = (const double2*)(vsm + stage * kSymvVecBytes);  // zeros past the matrix edge
     const double2* vC = vR + kSymvTB;
-    double2 vr[4], vc[4];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      vr[h] = vR[g + 16 * h];
-      vc[h] = vC[g + 16 * h];
-    }
     const bool diag = (R == C);
-    double2 yd0 = cmk(0.0, 0.0), yd1 = yd0, yt0 = yd0, yt1 = yd0;
-    const int r0 = qp, r1 = qp + 32;
+    const int r0 = rw + la, r1 = r0 + 8;
+    const double2 vr0 = vR[r0], vr1 = vR[r1];
+    double2 yd0 = cmk(0.0, 0.0), yd1 = yd0, yt[4];
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int u = g + 16 * h;
-      double2 d0 = *(const double2*)(ts + symv_sw(r0, u));
-      double2 d1 = *(const double2*)(ts + symv_sw(r1, u));
-      double2 t0 = *(const double2*)(ts + symv_sw(u, r0));
-      double2 t1 = *(const double2*)(ts + symv_sw(u, r1));
-      if (diag) {  // lower part only: direct uses u <= row (diagonal real), transposed u > column
-        if (u > r0) d0 = cmk(0.0, 0.0); else if (u == r0) d0.y = 0.0;
-        if (u > r1) d1 = cmk(0.0, 0.0); else if (u == r1) d1.y = 0.0;
-        if (u <= r0) t0 = cmk(0.0, 0.0);
-        if (u <= r1) t1 = cmk(0.0, 0.0);
+    for (int i = 0; i < 4; ++i) {
+      const int u = cw + lb + 4 * i;
+      const double2 vc = vC[u];
+      double2 e0 = *(const double2*)(ts + symv_sw(r0, u));
+      double2 e1 = *(const double2*)(ts + symv_sw(r1, u));
+      double2 f0 = e0, f1 = e1;  // the transposed product's copies
+      if (diag) {  // lower part only: direct uses u <= row (diagonal real), transposed u < row
+        if (u > r0) e0 = cmk(0.0, 0.0); else if (u == r0) e0.y = 0.0;
+        if (u > r1) e1 = cmk(0.0, 0.0); else if (u == r1) e1.y = 0.0;
+        if (u >= r0) f0 = cmk(0.0, 0.0);
+        if (u >= r1) f1 = cmk(0.0, 0.0);
       }
-      yd0 = cadd(yd0, cmul(d0, vc[h]));
-      yd1 = cadd(yd1, cmul(d1, vc[h]));
-      yt0 = cadd(yt0, cmulc(t0, vr[h]));
-      yt1 = cadd(yt1, cmulc(t1, vr[h]));
+      yd0 = cadd(yd0, cmul(e0, vc));
+      yd1 = cadd(yd1, cmul(e1, vc));
+      yt[i] = cadd(cmulc(f0, vr0), cmulc(f1, vr1));
     }
-#pragma unroll
-    for (int o = 1; o < 16; o <<= 1) {
-      yd0.x += __shfl_xor_sync(0xffffffffu, yd0.x, o);
-      yd0.y += __shfl_xor_sync(0xffffffffu, yd0.y, o);
-      yd1.x += __shfl_xor_sync(0xffffffffu, yd1.x, o);
-      yd1.y += __shfl_xor_sync(0xffffffffu, yd1.y, o);
-      yt0.x += __shfl_xor_sync(0xffffffffu, yt0.x, o);
-      yt0.y += __shfl_xor_sync(0xffffffffu, yt0.y, o);
-      yt1.x += __shfl_xor_sync(0xffffffffu, yt1.x, o);
-      yt1.y += __shfl_xor_sync(0xffffffffu, yt1.y, o);
+    constexpr unsigned FULL = 0xffffffffu;
+    // direct: reduce over lb (lane bits 3, 4); the lane keeps row r0 + 8 (lb & 1), component lb >> 1
+    double dk;
+    {
+      const bool h = lb & 1;
+      double k0 = h ? yd1.x : yd0.x, k1 = h ? yd1.y : yd0.y;
+      const double s0 = h ? yd0.x : yd1.x, s1 = h ? yd0.y : yd1.y;
+      k0 += __shfl_xor_sync(FULL, s0, 8);
+      k1 += __shfl_xor_sync(FULL, s1, 8);
+      const bool h2 = lb & 2;
+      dk = h2 ? k1 : k0;
+      dk += __shfl_xor_sync(FULL, h2 ? k0 : k1, 16);
     }
-    if (g == 0) {
-      double2* part = a.part + b * a.part_stride;
-      if (diag) {
-        double2* pd = part + ((int64_t)R * nbk + C) * kSymvTB;
-        pd[r0] = cadd(yd0, yt0);
-        pd[r1] = cadd(yd1, yt1);
-      } else {
-        double2* pd = part + ((int64_t)R * nbk + C) * kSymvTB;
-        double2* pt = part + ((int64_t)C * nbk + R) * kSymvTB;
-        pd[r0] = yd0;
-        pd[r1] = yd1;
-        pt[r0] = yt0;
-        pt[r1] = yt1;
-      }
+    // transposed: reduce over la (lane bits 0..2); the lane keeps column
+    // cw + lb + 4 (2 (la & 1) + ((la >> 1) & 1)), component (la >> 2) & 1
+    double tk;
+    {
+      const bool g0 = la & 1;
+      double q0 = g0 ? yt[2].x : yt[0].x, q1 = g0 ? yt[2].y : yt[0].y;
+      double q2 = g0 ? yt[3].x : yt[1].x, q3 = g0 ? yt[3].y : yt[1].y;
+      const double s0 = g0 ? yt[0].x : yt[2].x, s1 = g0 ? yt[0].y : yt[2].y;
+      const double s2 = g0 ? yt[1].x : yt[3].x, s3 = g0 ? yt[1].y : yt[3].y;
+      q0 += __shfl_xor_sync(FULL, s0, 1);
+      q1 += __shfl_xor_sync(FULL, s1, 1);
+      q2 += __shfl_xor_sync(FULL, s2, 1);
+      q3 += __shfl_xor_sync(FULL, s3, 1);
+      const bool g1 = la & 2;
+      double p0 = g1 ? q2 : q0, p1 = g1 ? q3 : q1;
+      const double u0 = g1 ? q0 : q2, u1 = g1 ? q1 : q3;
+      p0 += __shfl_xor_sync(FULL, u0, 2);
+      p1 += __shfl_xor_sync(FULL, u1, 2);
+      const bool g2 = la & 4;
+      tk = g2 ? p1 : p0;
+      tk += __shfl_xor_sync(FULL, g2 ? p0 : p1, 4);
     }
+    {
+      double* red = redsm + rb * (2 * 4 * kSymvTB * 2);
+      const int xr = r0 + 8 * (lb & 1), cd = lb >> 1;
+      red[((warp >> 2) * kSymvTB + xr) * 2 + cd] = dk;
+      const int xc = cw + lb + 4 * (2 * (la & 1) + ((la >> 1) & 1)), ct = (la >> 2) & 1;
+      red[((4 + (warp & 3)) * kSymvTB + xc) * 2 + ct] = tk;
+    }
+    pk = b; pR = R; pC = C;
+    rb ^= 1;
     stage = (stage + 1) % kSymvTmaStages;
     if (stage == 0) parity ^= 1u;
   }
+  __syncthreads();
+  if (pk >= 0) symv_tma_finish(redsm + (rb ^ 1) * (2 * 4 * kSymvTB * 2), a.part + pk * a.part_stride, nbk, pR, pC);
 }
 
 __global__ void __launch_bounds__(kBlkThreads) blk_prep_kernel(int n, double2* A) {
@@ -440,9 +496,11 @@ __global__ void __launch_bounds__(kBlkThreads) blk_prep_kernel(int n, double2* A
   blk_prep_reflectors(T, n, A + (int64_t)blockIdx.x * n * n, n);
 }
 
-// grid (P, B); Tm: B x P x (nb x nb); dynamic smem: G (nb x nb double2)
+// grid (P, B); Tm: B x P x (nb x nb); dynamic smem: G (nb x nb double2); Gg: the
+// Gram matrices V_p^H V_p laid out as Tm, or null (formed in the kernel)
 __global__ void __launch_bounds__(kBlkThreads) blk_larft_kernel(int n, int nb, int P, const double2* A,
-                                                                const double2* tau, double2* Tm) {
+                                                                const double2* tau, double2* Tm,
+                                                                const double2* Gg) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Team T = make_team();
   const int p = blockIdx.x;
@@ -455,7 +513,8 @@ __global__ void __launch_bounds__(kBlkThreads) blk_larft_kernel(int n, int nb, i
     for (int q = T.tid; q < nb * nb; q += T.nt) Tp[q] = cmk(0.0, 0.0);
     return;
   }
-  blk_larft(T, n, nb, j0, nbr, A + b * (int64_t)n * n, n, tau + b * n, Tp, (double2*)smem);
+  blk_larft(T, n, nb, j0, nbr, A + b * (int64_t)n * n, n, tau + b * n, Tp, (double2*)smem,
+            Gg ? Gg + (b * P + p) * (int64_t)nb * nb : nullptr);
 }
 
 struct DCLargeArgs {
