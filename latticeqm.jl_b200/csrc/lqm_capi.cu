@@ -518,7 +518,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       const int nbp = std::min(nb, n - j0);
       for (int i = 0; i < nbp; ++i) {
         const int j = j0 + i;
-        blk_column_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
+        blk_column_kernel<<<nbk, kColThreads, 0, ctx->stream>>>(ba, j0, i);
         ctx->launches++;
         if (j <= n - 2) {
           const int64_t nbl = (n - j - 1 + kSymvTB - 1) / kSymvTB;
@@ -549,7 +549,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
         }
       }
       if (j0 + nbp < n) {
-        blk_finish_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(ba, j0, nbp - 1);
+        blk_finish_kernel<<<nbk, kColThreads, 0, ctx->stream>>>(ba, j0, nbp - 1);
         ctx->launches++;
         // A22 -= V W^H + W V^H on the lower triangle, one launch
         const int m2 = n - j0 - nbp;

@@ -428,8 +428,8 @@ LQM_FN void deflate_node(int node, const DCPlan& P, EighVec& S, double eabs_beta
 // r < hi - lo, it < k (Ubn holds the secular vectors as rows).  A 512-thread
 // team computes 128 x 128 output tiles on the FP64 tensor path (DMMA
 // m8n8k4): 16 warps of 32 x 32, each a 4 x 4 grid of 8 x 8 accumulators.  The
-// p range moves in 8-deep stages by cp.async through a 3-stage ring in `tile`
-// (per stage 8 rows of 128 + 4 doubles for Q and for Ubn, p-major; the pitch of
+// p range moves in 16-deep stages by cp.async through a 3-stage ring in `tile`
+// (per stage 16 rows of 128 + 4 doubles for Q and for Ubn, p-major; the pitch of
 // 132 == 4 mod 16 puts the 16 fragment reads of a half-warp on distinct bank
 // pairs), followed by room for k column indices; two stages are in flight while
 // one is summed.  p is summed in ascending 4-deep steps.  Other team sizes (the
@@ -442,7 +442,8 @@ __device__ __forceinline__ void lqm_cp_async8(void* sdst, const void* gsrc, bool
 }
 #endif
 constexpr int kDcTileP = 132;                            // staged row pitch (doubles)
-constexpr int kDcTileStage = 8 * 2 * kDcTileP;           // doubles per stage (Q and Ubn slices)
+constexpr int kDcTileBK = 16;                            // p depth of a stage
+constexpr int kDcTileStage = kDcTileBK * 2 * kDcTileP;   // doubles per stage (Q and Ubn slices)
 constexpr int kDcTileRing = 3 * kDcTileStage;            // doubles of the ring
 template <class TeamT>
 LQM_FN void dc_tile_gemm(const TeamT& T, int n, int lo, int hi, int k, const int* colnd, const int* newpos,
@@ -450,7 +451,7 @@ LQM_FN void dc_tile_gemm(const TeamT& T, int n, int lo, int hi, int k, const int
   const int s = hi - lo;
 #if defined(__CUDA_ARCH__)
   if (T.nt == 512 && tile != nullptr) {
-    constexpr int BM = 128, BN = 128, BK = 8, PT = kDcTileP, STG = kDcTileStage, NS = 3;
+    constexpr int BM = 128, BN = 128, BK = kDcTileBK, PT = kDcTileP, STG = kDcTileStage, NS = 3;
     const int lane = T.tid & 31, warp = T.tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wr = (warp & 3) * 32, wc = (warp >> 2) * 32;  // the warp's 32 x 32 sub-tile
@@ -469,7 +470,7 @@ LQM_FN void dc_tile_gemm(const TeamT& T, int n, int lo, int hi, int k, const int
           double* As = tile + st * STG;
           double* Bs = As + BK * PT;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
+          for (int h = 0; h < BK * 128 / 512; ++h) {
             const int e = T.tid + 512 * h;
             const int pp = e >> 7, x = e & 127;
             const int p = p0 + pp, r = r0 + x, cc = c0 + x;

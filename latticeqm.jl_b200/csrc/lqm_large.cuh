@@ -25,6 +25,7 @@ namespace lqm {
 constexpr int kBlkNB = 32;      // panel width of the reduction (reflectors per panel)
 constexpr int kBlkNBT = 64;     // panel width of the compact-WY back-transformation
 constexpr int kBlkThreads = 256;
+constexpr int kColThreads = 512;  // column step: latency-bound row passes, more rows in flight per k-point
 constexpr int kSymvTB = 64;     // mat-vec tile (2 rows per lane of a 32-lane warp)
 constexpr int kDcThreads = 512;
 constexpr int kDcTileMin = 160; // merges with at least this many rows use the tiled update
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(kBlkThreads) blk_bloch_kernel(int n, int nR, i
   bloch_build(T, n, nR, dim, blocks, keys, kpt, ph, A + k * (int64_t)n * n, n);
 }
 
-__global__ void __launch_bounds__(kBlkThreads) blk_column_kernel(BlkArgs a, int j0, int i) {
+__global__ void __launch_bounds__(kColThreads) blk_column_kernel(BlkArgs a, int j0, int i) {
   __shared__ double red[128];
   __shared__ __align__(16) double2 t12[2 * kBlkNB];
   const Team T = make_team();
@@ -80,7 +81,7 @@ __global__ void __launch_bounds__(kBlkThreads) blk_column_kernel(BlkArgs a, int 
 }
 
 // Last column of a panel: finish its w from the partials.
-__global__ void __launch_bounds__(kBlkThreads) blk_finish_kernel(BlkArgs a, int j0, int ip) {
+__global__ void __launch_bounds__(kColThreads) blk_finish_kernel(BlkArgs a, int j0, int ip) {
   __shared__ double red[128];
   __shared__ __align__(16) double2 t12[2 * kBlkNB];
   const Team T = make_team();

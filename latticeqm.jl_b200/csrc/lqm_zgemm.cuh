@@ -151,6 +151,27 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
     if (s < nks) stage(s, sm + s * STAGE);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
+  // beta != 0: the accumulators start at (beta / alpha) C, loaded while the first
+  // slices are in flight (the epilogue then writes alpha acc without reading C)
+  const bool cinit = g.beta != 0.0 && g.alpha != 0.0;
+  if (cinit) {
+    const double sc = g.beta / g.alpha;
+#pragma unroll
+    for (int i = 0; i < MI; ++i) {
+      const int r = m0 + wm0 + 8 * i + gr;
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int c = n0 + wn0 + 8 * j + 2 * gt + h;
+          if (r < g.m && c < g.n) {
+            const double2 o = C[r + (int64_t)c * g.ldc];
+            re[i][j][h] = sc * o.x;
+            im[i][j][h] = sc * o.y;
+          }
+        }
+    }
+  }
   for (int ks = 0; ks < nks; ++ks) {
     if (ST > 1) {
       asm volatile("cp.async.wait_group %0;\n" ::"n"(ST > 1 ? ST - 2 : 0) : "memory");
@@ -197,7 +218,7 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
     }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
-  // epilogue: C = alpha acc + beta C
+  // epilogue: C = alpha acc (+ beta C when C was not folded into acc)
 #pragma unroll
   for (int i = 0; i < MI; ++i) {
     const int r = m0 + wm0 + 8 * i + gr;
@@ -210,7 +231,7 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
         if (c >= g.n) continue;
         double2* p = C + r + (int64_t)c * g.ldc;
         double2 v = cmk(g.alpha * re[i][j][h], g.alpha * im[i][j][h]);
-        if (g.beta != 0.0) {
+        if (!cinit && g.beta != 0.0) {
           const double2 o = *p;
           v.x += g.beta * o.x;
           v.y += g.beta * o.y;
