@@ -65,6 +65,13 @@ int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
  * (panel reduction + batched GEMMs); 0 (default) selects it from n = 128 on.
  * No reference counterpart (the reference always calls LAPACK zheevr). */
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
+/* Reduction of the blocked path: 1 two-stage (dense -> band of half-bandwidth 16 by
+ * panel QRs and GEMM updates, band -> tridiagonal by bulge chasing, two-level
+ * back-transformation), 0 the one-stage panel reduction (LAPACK zhetrd/zlatrd
+ * form, one Hermitian mat-vec per column), -1 (default) by order.  Replaces no
+ * reference call: the reference's LAPACK zheevr (src/modules/Eigen/Eigen.jl:22-23)
+ * reduces in one stage; zheevr_2stage is LAPACK's two-stage form of the same solve. */
+int lqm_ctx_set_two_stage(lqm_ctx* ctx, int mode);
 /* SCF acceleration of lqm_scf_hf on this context: 0 (default) linear damped
  * mixing, 1..8 Anderson (Type-II) acceleration with that history depth
  * (src/modules/Meanfield/fixedpoint.jl:39-194,201-231: acceleration=:anderson,

@@ -248,26 +248,27 @@ LQM_FN void blk_symv_tile(const Team& T, int n, int j, int R, int C, const doubl
 }
 
 // After the reduction: make the reflector columns explicit for the blocked
-// back-transformation — zeros on and above the diagonal of columns 0..n-2,
-// v0 = 1 below it.  Column c by warp.
-LQM_FN void blk_prep_reflectors(const Team& T, int n, double2* A, int lda) {
+// back-transformation — reflector c starts at row c + off (off = 1 for the
+// one-stage reduction, the half-bandwidth for the two-stage one): zeros above
+// that row, v0 = 1 on it.  Column c by warp.
+LQM_FN void blk_prep_reflectors(const Team& T, int n, double2* A, int lda, int off = 1) {
   for (int c = T.wid; c < n; c += T.nw) {
     double2* col = A + (int64_t)c * lda;
-    for (int r = T.lane; r <= c && r < n; r += T.nl) col[r] = cmk(0.0, 0.0);
-    if (T.lane == 0 && c + 1 < n) col[c + 1] = cmk(1.0, 0.0);
+    for (int r = T.lane; r < c + off && r < n; r += T.nl) col[r] = cmk(0.0, 0.0);
+    if (T.lane == 0 && c + off < n) col[c + off] = cmk(1.0, 0.0);
   }
 }
 
 // Compact WY factor of reflectors j0 .. j0+nbr-1 (LAPACK zlarft, forward,
 // column-wise): H_{j0} ... H_{j0+nbr-1} = I - V Tm V^H, Tm upper triangular
-// (nb x nb, leading dimension nb, zero-padded).  V(:, l) = A(j0+1:, j0+l) after
+// (nb x nb, leading dimension nb, zero-padded).  V(:, l) = A(j0+off:, j0+l) after
 // blk_prep_reflectors.  G: nb*nb complex team scratch for the Gram matrix V^H V,
 // formed here from V or, with Gg != null, copied from Gg (nb x nb, leading
 // dimension nb, formed beforehand by a GEMM).
 LQM_FN void blk_larft(const Team& T, int n, int nb, int j0, int nbr, const double2* A, int lda, const double2* tau,
-                      double2* Tm, double2* G, const double2* Gg = nullptr) {
-  const int m = n - j0 - 1;
-  const double2* V = A + (int64_t)j0 * lda + (j0 + 1);
+                      double2* Tm, double2* G, const double2* Gg = nullptr, int off = 1) {
+  const int m = n - j0 - off;
+  const double2* V = A + (int64_t)j0 * lda + (j0 + off);
   if (Gg) {
     for (int p = T.tid; p < nb * nb; p += T.nt) G[p] = Gg[p];
   } else {

@@ -59,7 +59,7 @@ struct lqm_ctx {
   double last_ms = 0.0;
   std::map<int, PlanDev> plans;
   std::map<int, int> eigh_nt;  // one-CTA eigensolver block size per order n (autotuned or set), else the rule
-  DevBuf ws[48];
+  DevBuf ws[52];
   // per-kernel device-time statistics (CUDA events on the context stream)
   bool stats_on = false;
   bool phases_on = false;  // per-phase cycle counters inside the eigensolver (clock reads)
@@ -73,6 +73,7 @@ struct lqm_ctx {
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
   int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: the default switch)
+  int two_stage = -1;                     // blocked path reduction: 1 two-stage, 0 one-stage, -1 by order
   int scf_anderson_depth = 0;             // SCF acceleration: 0 linear mixing, > 0 Anderson history depth
   int scf_residual = 0;                   // SCF residual: 0 relative density change, 1 commutator norm
   bool scf_hartree = true, scf_fock = true;  // HartreeFock(h, v; hartree, fock)
@@ -253,9 +254,9 @@ bool hops_buffer_keep(lqm_ctx* ctx, void* p, size_t bytes) {
 enum WsSlot {
   WS_SCRATCH = 0, WS_KS, WS_BANDS, WS_U, WS_RHOK, WS_COEF, WS_EBK, WS_RHO, WS_W, WS_MISC, WS_PART,
   WS_OMEGA, WS_DOS, WS_LKEYS, WS_HF, WS_HF2, WS_MU, WS_BANDS2,
-  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2, WS_GEMMSPLIT, WS_GRAM
+  WS_LA, WS_LU, WS_LAUX, WS_LDC, WS_VU, WS_VB, WS_VX, WS_VT, WS_VG, WS_ONES, WS_SCFY, WS_AND, WS_EXCH, WS_HFPART, WS_BDG, WS_BDGE, WS_BDGI, WS_BDGK, WS_BDGP, WS_BDGB, WS_CSC, WS_UNIW, WS_SPAN, WS_GRAD, WS_GRADE, WS_HFPART2, WS_GEMMSPLIT, WS_GRAM, WS_TSP, WS_TSB, WS_TSV2
 };
-static_assert(WS_GRAM < 48, "workspace slots");
+static_assert(WS_TSV2 < 52, "workspace slots");
 
 }  // namespace
 #include "lqm_comm.inc"
@@ -373,7 +374,7 @@ void zgemm_sb(lqm_ctx* ctx, GemmOp ta, GemmOp tb, int m, int n, int k, double al
   // a single product with few output tiles and a long k (the Fourier fold of small
   // orders): split k over the SMs, partial products in a workspace, then an ordered sum
   const int64_t tiles = (int64_t)((m + 127) / 128) * ((n + 15) / 16);
-  if (batch == 1 && n <= 16 && k >= 1024 && tiles < 2 * (int64_t)ctx->num_sms) {
+  if (batch == 1 && n <= 16 && k >= 1024 && ta != OP_HL && tiles < 2 * (int64_t)ctx->num_sms) {
     int nsplit = (int)std::min<int64_t>((2 * ctx->num_sms + tiles - 1) / tiles, k / 512);
     nsplit = std::max(2, std::min(nsplit, 64));
     const int kc = (k + nsplit - 1) / nsplit;
@@ -416,6 +417,7 @@ void zher2k_lower(lqm_ctx* ctx, int m, int k, const double2* X, int ldx, long lo
 
 struct RhoOut;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR);
+bool use_two_stage(const lqm_ctx* ctx, int n);
 
 // Eigen pass of the blocked path: same outputs as launch_eigh.  Reduction by
 // zlatrd panels (column kernels + batched rank-2nb updates), divide and
@@ -463,13 +465,26 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   const int P2 = (n + nbt - 1) / nbt;
   const int wc = std::max(nb, nbt);       // columns of W / X and of Y per k-point
   const bool vec = d_U || rhok;
+  // two-stage: dense -> band (kTsB) -> tridiagonal; reflector j of the first stage
+  // starts at row j + off, n - off of them
+  const bool ts = use_two_stage(ctx, n);
+  const int off = ts ? kTsB : 1;
+  const int NR = n - off;
   const int64_t nn = (int64_t)n * n;
-  const int64_t pstride = symv_part_stride(n), tstride = t12_part_stride(n, nb);
+  const int64_t pstride = ts ? 0 : symv_part_stride(n), tstride = ts ? 0 : t12_part_stride(n, nb);
   const int64_t auxk = 2 * (int64_t)n * wc /*W, Y*/ + (int64_t)nbt * nbt * P2 /*Tm*/ + n /*tau*/ + 2 * nb /*t12*/ +
                        pstride /*mat-vec partials*/ + tstride /*panel-product partials*/;
-  const double per_k = 16.0 * (double)nn * ((vec && !d_U) ? 2.0 : 1.0) + 16.0 * (double)auxk + 16.0 * n;
-  int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(48.0e9 / per_k)));
+  const int64_t tspk = ts ? 3 * (int64_t)n * kTsB + 3 * kTsB * kTsB : 0;   // Vb, Y, X; T, S, Z
+  const int64_t tsbk = ts ? 2 * (int64_t)kTsB * n : 0;                        // the band
+  const int64_t tsvk = (ts && vec) ? ts_v2_stride(n) + ts_tau2_stride(n) : 0; // stage-2 reflectors
+  const double per_k = 16.0 * (double)nn * ((vec && !d_U) ? 2.0 : 1.0) + 16.0 * (double)(auxk + tspk + tsbk + tsvk) +
+                       16.0 * n;
+  int64_t B = std::max<int64_t>(1, std::min<int64_t>(nk, (int64_t)(64.0e9 / per_k)));
   B = std::min<int64_t>(B, 65535);
+  {  // batches of equal size (no short tail batch)
+    const int64_t nbat = (nk + B - 1) / B;
+    B = (nk + nbat - 1) / nbat;
+  }
   const int64_t slotd = dc_large_slot_doubles(n, vec);
   const bool dc_small = n < kDcTileMin;  // no tiled merges: 128-thread CTAs, four per SM
   const int64_t G = std::min<int64_t>(B, (int64_t)ctx->num_sms * (dc_small ? 4 : 1));
@@ -485,19 +500,25 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   double2* tpart = part + B * pstride;                // B x tstride
   double* dd = (double*)(tpart + B * tstride);        // B x n
   double* ee = dd + B * (int64_t)n;                   // B x n
+  double2* tsp = ts ? (double2*)ws_get(ctx, WS_TSP, (size_t)B * tspk * sizeof(double2)) : nullptr;
+  double2* Bd = ts ? (double2*)ws_get(ctx, WS_TSB, (size_t)B * tsbk * sizeof(double2)) : nullptr;
+  double2* V2 = (ts && vec) ? (double2*)ws_get(ctx, WS_TSV2, (size_t)B * tsvk * sizeof(double2)) : nullptr;
+  double2* tau2 = V2 ? V2 + B * ts_v2_stride(n) : nullptr;
   double* slots = (double*)ws_get(ctx, WS_LDC, (size_t)G * slotd * sizeof(double));
   const DCPlan& plan = get_plan(ctx, n);
   lqm_ctx* h = blas_handle(ctx);
-  ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
-     "smem attr");
-  ck(cudaFuncSetAttribute(blk_symv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvTmaSmem),
-     "smem attr");
-  // the mat-vec moves its tiles by TMA from n = 64 on (the descriptor covers the batch)
   CUtensorMap symv_map, symv_vmap;
-  const char* pipe_env = std::getenv("LQM_SYMV_PIPE");
-  const bool symv_tma =
-      n >= 64 && !(pipe_env && pipe_env[0] == '1') && make_symv_map(&symv_map, &symv_vmap, A, n, B);
-  if (symv_tma && !ctx->d_err) {
+  bool symv_tma = false;
+  if (!ts) {
+    ck(cudaFuncSetAttribute(blk_symv_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvPipeSmem),
+       "smem attr");
+    ck(cudaFuncSetAttribute(blk_symv_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSymvTmaSmem),
+       "smem attr");
+    // the mat-vec moves its tiles by TMA from n = 64 on (the descriptor covers the batch)
+    const char* pipe_env = std::getenv("LQM_SYMV_PIPE");
+    symv_tma = n >= 64 && !(pipe_env && pipe_env[0] == '1') && make_symv_map(&symv_map, &symv_vmap, A, n, B);
+  }
+  if ((symv_tma || ts) && !ctx->d_err) {
     ck(cudaMalloc(&ctx->d_err, sizeof(int)), "cudaMalloc(error word)");
     ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "memset(error word)");
   }
@@ -512,52 +533,80 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     blk_bloch_kernel<<<nbk, kBlkThreads, bsm, ctx->stream>>>(n, (int)H->nR, H->d, H->blocks, H->keys, nbk,
                                                               d_ks + k0 * H->d, A);
     ctx->launches++;
-    const BlkArgs ba{n, nb, A, W, tau, dd, ee, t12, part, pstride, tpart, tstride};
-    for (int p = 0; p < P; ++p) {
-      const int j0 = p * nb;
-      const int nbp = std::min(nb, n - j0);
-      for (int i = 0; i < nbp; ++i) {
-        const int j = j0 + i;
-        blk_column_kernel<<<nbk, kColThreads, 0, ctx->stream>>>(ba, j0, i);
-        ctx->launches++;
-        if (j <= n - 2) {
-          const int64_t nbl = (n - j - 1 + kSymvTB - 1) / kSymvTB;
-          const int64_t nitems = nbl * (nbl + 1) / 2 * nbk;
-          const int64_t grid = std::min<int64_t>(nitems, (int64_t)ctx->num_sms);
-          std::pair<cudaEvent_t, cudaEvent_t> sev{};
-          if (ctx->stats_on) { sev = stat_events(ctx); ck(cudaEventRecord(sev.first, ctx->stream), "event"); }
-          if (symv_tma) {
-            blk_symv_tma_kernel<<<(unsigned)grid, kSymvTmaThreads, kSymvTmaSmem, ctx->stream>>>(
-                symv_map, symv_vmap, ba, j, nitems, ctx->d_err);
-            ctx->err_armed = true;
-          } else {
-            blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
-          }
+    if (ts) {
+      // stage 1: per panel the QR below the band, then A22 <- Q^H A22 Q by GEMMs
+      double2* Vb = tsp;                              // nbk x (n x kTsB)
+      double2* Yt = Vb + B * (int64_t)n * kTsB;
+      double2* Xt = Yt + B * (int64_t)n * kTsB;
+      double2* Tt = Xt + B * (int64_t)n * kTsB;       // nbk x (kTsB x kTsB): T, S, Z
+      double2* St = Tt + B * (int64_t)kTsB * kTsB;
+      double2* Zt = St + B * (int64_t)kTsB * kTsB;
+      const long long sv = (long long)n * kTsB, s2 = (long long)kTsB * kTsB;
+      for (int j0 = 0; j0 + kTsB < n; j0 += kTsB) {
+        const int m = n - j0 - kTsB, nr = std::min(kTsB, m);
+        ts_panel_kernel<<<nbk, kTsPanelThreads, 0, ctx->stream>>>(n, j0, A, tau, Vb, Tt);
+        double2* A22 = A + (j0 + kTsB) + (int64_t)(j0 + kTsB) * n;
+        zgemm_sb(h, OP_HL, OP_N, m, nr, m, 1.0, A22, n, nn, Vb, n, sv, 0.0, Yt, n, sv, nbk);           // Y = A22 V
+        zgemm_sb(h, OP_N, OP_N, m, nr, nr, 1.0, Yt, n, sv, Tt, kTsB, s2, 0.0, Xt, n, sv, nbk);         // X = Y T
+        zgemm_sb(h, OP_C, OP_N, nr, nr, m, 1.0, Vb, n, sv, Xt, n, sv, 0.0, St, kTsB, s2, nbk);         // S = V^H X
+        zgemm_sb(h, OP_C, OP_N, nr, nr, nr, 0.5, Tt, kTsB, s2, St, kTsB, s2, 0.0, Zt, kTsB, s2, nbk);  // Z = T^H S / 2
+        zgemm_sb(h, OP_N, OP_N, m, nr, nr, -1.0, Vb, n, sv, Zt, kTsB, s2, 1.0, Xt, n, sv, nbk);        // W = X - V Z
+        zher2k_lower(h, m, nr, Vb, n, sv, Xt, n, sv, A22, n, nn, nbk);                                 // A22 -= V W^H + W V^H
+        ctx->launches += 7;
+      }
+      // stage 2: the band, then the bulge chase to the real tridiagonal
+      ts_band_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A, Bd);
+      ts_chase_kernel<<<nbk, kTsChaseWarps * 32, 0, ctx->stream>>>(n, Bd, V2, tau2, dd, ee, ctx->d_err);
+      ctx->err_armed = true;
+      ctx->launches += 2;
+    } else {
+      const BlkArgs ba{n, nb, A, W, tau, dd, ee, t12, part, pstride, tpart, tstride};
+      for (int p = 0; p < P; ++p) {
+        const int j0 = p * nb;
+        const int nbp = std::min(nb, n - j0);
+        for (int i = 0; i < nbp; ++i) {
+          const int j = j0 + i;
+          blk_column_kernel<<<nbk, kColThreads, 0, ctx->stream>>>(ba, j0, i);
           ctx->launches++;
-          if (ctx->stats_on) {
-            ck(cudaEventRecord(sev.second, ctx->stream), "event");
-            ctx->symv_pending.push_back(sev);
-            const double m = (double)(n - j - 1);
-            ctx->symv_bytes += (double)nbk * m * (m + 1.0) / 2.0 * 16.0;  // lower triangle of A22, once
-            ctx->symv_launches++;
-          }
-          if (i > 0) {
-            const dim3 g2((unsigned)((n - j - 1 + 127) / 128), (unsigned)nbk);
-            blk_t12_kernel<<<g2, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
+          if (j <= n - 2) {
+            const int64_t nbl = (n - j - 1 + kSymvTB - 1) / kSymvTB;
+            const int64_t nitems = nbl * (nbl + 1) / 2 * nbk;
+            const int64_t grid = std::min<int64_t>(nitems, (int64_t)ctx->num_sms);
+            std::pair<cudaEvent_t, cudaEvent_t> sev{};
+            if (ctx->stats_on) { sev = stat_events(ctx); ck(cudaEventRecord(sev.first, ctx->stream), "event"); }
+            if (symv_tma) {
+              blk_symv_tma_kernel<<<(unsigned)grid, kSymvTmaThreads, kSymvTmaSmem, ctx->stream>>>(
+                  symv_map, symv_vmap, ba, j, nitems, ctx->d_err);
+              ctx->err_armed = true;
+            } else {
+              blk_symv_pipe_kernel<<<(unsigned)grid, kSymvThreads, kSymvPipeSmem, ctx->stream>>>(ba, j, nitems);
+            }
             ctx->launches++;
+            if (ctx->stats_on) {
+              ck(cudaEventRecord(sev.second, ctx->stream), "event");
+              ctx->symv_pending.push_back(sev);
+              const double m = (double)(n - j - 1);
+              ctx->symv_bytes += (double)nbk * m * (m + 1.0) / 2.0 * 16.0;  // lower triangle of A22, once
+              ctx->symv_launches++;
+            }
+            if (i > 0) {
+              const dim3 g2((unsigned)((n - j - 1 + 127) / 128), (unsigned)nbk);
+              blk_t12_kernel<<<g2, kBlkThreads, 0, ctx->stream>>>(ba, j0, i);
+              ctx->launches++;
+            }
           }
         }
-      }
-      if (j0 + nbp < n) {
-        blk_finish_kernel<<<nbk, kColThreads, 0, ctx->stream>>>(ba, j0, nbp - 1);
-        ctx->launches++;
-        // A22 -= V W^H + W V^H on the lower triangle, one launch
-        const int m2 = n - j0 - nbp;
-        double2* Cb = A + (j0 + nbp) + (int64_t)(j0 + nbp) * n;
-        const double2* Vr = A + (j0 + nbp) + (int64_t)j0 * n;
-        const double2* Wr = W + (j0 + nbp);
-        zher2k_lower(h, m2, nbp, Vr, n, nn, Wr, n, (long long)n * nb, Cb, n, nn, nbk);
-        ctx->launches += 1;
+        if (j0 + nbp < n) {
+          blk_finish_kernel<<<nbk, kColThreads, 0, ctx->stream>>>(ba, j0, nbp - 1);
+          ctx->launches++;
+          // A22 -= V W^H + W V^H on the lower triangle, one launch
+          const int m2 = n - j0 - nbp;
+          double2* Cb = A + (j0 + nbp) + (int64_t)(j0 + nbp) * n;
+          const double2* Vr = A + (j0 + nbp) + (int64_t)j0 * n;
+          const double2* Wr = W + (j0 + nbp);
+          zher2k_lower(h, m2, nbp, Vr, n, nn, Wr, n, (long long)n * nb, Cb, n, nn, nbk);
+          ctx->launches += 1;
+        }
       }
     }
     ck(cudaGetLastError(), "blocked reduction launch");
@@ -595,8 +644,17 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
         K = hspan[1];
       }
     }
+    if (K > 0 && ts) {
+      // Z <- Q2 Z on the K columns: the stage-2 reflectors, sweeps in reverse order
+      const int cols = std::max(1, std::min(kTsQ2MaxCols, (200 * 1024) / (16 * n)));
+      const int qsm = 16 * n * cols;
+      ck(cudaFuncSetAttribute(ts_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm), "smem attr");
+      ts_q2_kernel<<<dim3((unsigned)((K + cols - 1) / cols), (unsigned)nbk), kTsQ2Threads, qsm, ctx->stream>>>(
+          n, c0, K, cols, V2, tau2, Ucur);
+      ctx->launches++;
+    }
     if (K > 0) {
-      blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A);
+      blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A, off);
       ctx->launches++;
       // Gram matrices G_p = V_p^H V_p of the back-transformation's panels (V explicit
       // and zero above its unit diagonal after blk_prep_kernel), then Tm from them
@@ -604,26 +662,26 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       double2* G = (double2*)ws_get(ctx, WS_GRAM, (size_t)nbk * P2 * g2 * sizeof(double2));
       for (int p = 0; p < P2; ++p) {
         const int j0 = p * nbt;
-        const int nbr = std::min(nbt, n - 1 - j0);
+        const int nbr = std::min(nbt, NR - j0);
         if (nbr <= 0) continue;
-        const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
-        zgemm_sb(h, OP_C, OP_N, nbr, nbr, n - j0 - 1, 1.0, V, n, nn, V, n, nn, 0.0, G + p * g2, nbt,
+        const double2* V = A + (j0 + off) + (int64_t)j0 * n;
+        zgemm_sb(h, OP_C, OP_N, nbr, nbr, n - j0 - off, 1.0, V, n, nn, V, n, nn, 0.0, G + p * g2, nbt,
                  (long long)P2 * g2, nbk);
         ctx->launches++;
       }
       const size_t lsm = (size_t)g2 * sizeof(double2);
       ck(cudaFuncSetAttribute(blk_larft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsm), "smem attr");
       blk_larft_kernel<<<dim3((unsigned)P2, (unsigned)nbk), kBlkThreads, lsm, ctx->stream>>>(n, nbt, P2, A, tau,
-                                                                                             Tm, G);
+                                                                                             Tm, G, off);
       ctx->launches++;
     }
     for (int p = P2 - 1; p >= 0 && K > 0; --p) {
       const int j0 = p * nbt;
-      const int nbr = std::min(nbt, n - 1 - j0);
+      const int nbr = std::min(nbt, NR - j0);
       if (nbr <= 0) continue;
-      const int m = n - j0 - 1;
-      const double2* V = A + (j0 + 1) + (int64_t)j0 * n;
-      double2* Us = Ucur + (j0 + 1) + (int64_t)c0 * n;
+      const int m = n - j0 - off;
+      const double2* V = A + (j0 + off) + (int64_t)j0 * n;
+      double2* Us = Ucur + (j0 + off) + (int64_t)c0 * n;
       // X = V^H Us (nbr x K), Y = Tm X, Us -= V Y
       zgemm_sb(h, OP_C, OP_N, nbr, K, m, 1.0, V, n, nn, Us, n, nn, 0.0, W, nbt, (long long)n * nbt,
                nbk);
@@ -728,6 +786,19 @@ bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
   const int64_t nmin = ctx->blocked_min_n > 0 ? ctx->blocked_min_n : kBlockedDefaultMinN;
   if (n >= nmin) return true;
   return eigh_smem_layout(n, nR, eigh_threads_for(ctx, n), 0).total > 225 * 1024;
+}
+
+// Reduction of the blocked path: two-stage (dense -> band -> tridiagonal) or the
+// one-stage zlatrd panels; ctx->two_stage when set (lqm_ctx_set_two_stage), else by
+// order from kTwoStageDefaultMinN on.  LQM_TWO_STAGE=0/1 in the environment overrides
+// both (development switch for measurements).
+constexpr int kTwoStageDefaultMinN = 1 << 30;
+bool use_two_stage(const lqm_ctx* ctx, int n) {
+  if (n <= kTsB + 1) return false;
+  const char* env = std::getenv("LQM_TWO_STAGE");
+  if (env && (env[0] == '0' || env[0] == '1')) return env[0] == '1';
+  if (ctx->two_stage >= 0) return ctx->two_stage == 1;
+  return n >= kTwoStageDefaultMinN;
 }
 
 int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
@@ -1132,6 +1203,12 @@ int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt) {
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min) {
   if (!ctx || n_min < 0) return LQM_EINVAL;
   ctx->blocked_min_n = n_min;
+  return LQM_OK;
+}
+
+int lqm_ctx_set_two_stage(lqm_ctx* ctx, int mode) {
+  if (!ctx || mode < -1 || mode > 1) return LQM_EINVAL;
+  ctx->two_stage = mode;
   return LQM_OK;
 }
 

@@ -19,6 +19,7 @@
 
 #include "lqm_blocked.cuh"
 #include "lqm_kernels.cuh"
+#include "lqm_twostage.cuh"
 
 namespace lqm {
 
@@ -492,22 +493,24 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
   if (pk >= 0) symv_tma_finish(redsm + (rb ^ 1) * (2 * 4 * kSymvTB * 2), a.part + pk * a.part_stride, nbk, pR, pC);
 }
 
-__global__ void __launch_bounds__(kBlkThreads) blk_prep_kernel(int n, double2* A) {
+// off: the row offset of the reflectors (1 one-stage, the half-bandwidth two-stage)
+__global__ void __launch_bounds__(kBlkThreads) blk_prep_kernel(int n, double2* A, int off) {
   const Team T = make_team();
-  blk_prep_reflectors(T, n, A + (int64_t)blockIdx.x * n * n, n);
+  blk_prep_reflectors(T, n, A + (int64_t)blockIdx.x * n * n, n, off);
 }
 
 // grid (P, B); Tm: B x P x (nb x nb); dynamic smem: G (nb x nb double2); Gg: the
 // Gram matrices V_p^H V_p laid out as Tm, or null (formed in the kernel)
+// off: the row offset of the reflectors; their count is n - off
 __global__ void __launch_bounds__(kBlkThreads) blk_larft_kernel(int n, int nb, int P, const double2* A,
                                                                 const double2* tau, double2* Tm,
-                                                                const double2* Gg) {
+                                                                const double2* Gg, int off) {
   extern __shared__ __align__(16) unsigned char smem[];
   const Team T = make_team();
   const int p = blockIdx.x;
   const int64_t b = blockIdx.y;
   const int j0 = p * nb;
-  int nbr = n - 1 - j0;
+  int nbr = n - off - j0;
   if (nbr > nb) nbr = nb;
   double2* Tp = Tm + (b * P + p) * (int64_t)nb * nb;
   if (nbr <= 0) {
@@ -515,7 +518,7 @@ __global__ void __launch_bounds__(kBlkThreads) blk_larft_kernel(int n, int nb, i
     return;
   }
   blk_larft(T, n, nb, j0, nbr, A + b * (int64_t)n * n, n, tau + b * n, Tp, (double2*)smem,
-            Gg ? Gg + (b * P + p) * (int64_t)nb * nb : nullptr);
+            Gg ? Gg + (b * P + p) * (int64_t)nb * nb : nullptr, off);
 }
 
 struct DCLargeArgs {
@@ -708,6 +711,152 @@ __global__ void __launch_bounds__(kBlkThreads) blk_add_identity_kernel(int n, do
   const int64_t nn = (int64_t)n * n;
   double2* Rk = R + blockIdx.x * nn;
   for (int i = threadIdx.x; i < n; i += blockDim.x) Rk[i + (int64_t)i * n].x += 1.0;
+}
+
+
+// ---- Two-stage reduction (lqm_twostage.cuh) ----
+constexpr int kTsB = 16;              // half-bandwidth of the stage-1 band
+constexpr int kTsPanelThreads = 512;  // panel QR: latency-bound row passes, CTA per k-point
+constexpr int kTsChaseWarps = 16;     // bulge chase: sweeps in flight per k-point (one warp each)
+constexpr int kTsQ2Threads = 256;
+constexpr int kTsQ2MaxCols = 8;       // columns of Z per CTA in the Q2 back-transformation
+constexpr int kTsWaitPolls = 1 << 22; // bound of one inter-warp wait of the chase (polls of ~0.1 us)
+
+// complex per k-point of the stage-2 reflector store (sweeps 0..n-2, tmax slots of kTsB each)
+__host__ __device__ inline int64_t ts_v2_stride(int n) {
+  return (int64_t)(n > 1 ? n - 1 : 1) * ts_tmax(n, kTsB) * kTsB;
+}
+__host__ __device__ inline int64_t ts_tau2_stride(int n) { return (int64_t)(n > 1 ? n - 1 : 1) * ts_tmax(n, kTsB); }
+
+// grid (B): panel j0 of every k-point.  Vb: B x (n x kTsB), Tm: B x (kTsB x kTsB).
+__global__ void __launch_bounds__(kTsPanelThreads) ts_panel_kernel(int n, int j0, double2* A, double2* tau,
+                                                                   double2* Vb, double2* Tm) {
+  __shared__ __align__(16) double2 sm[(kTsPanelThreads / 32 + 2) * kTsB + kTsB * kTsB];
+  const Team T = make_team();
+  const int64_t b = blockIdx.x;
+  ts_panel_qr<kTsB>(T, n, j0, A + b * (int64_t)n * n, n, tau + b * n, Vb + b * (int64_t)n * kTsB, n,
+                    Tm + b * kTsB * kTsB, sm);
+}
+
+// grid (B): the band (2 kTsB x n per k-point) out of the stage-1 result.
+__global__ void __launch_bounds__(kBlkThreads) ts_band_kernel(int n, const double2* A, double2* Bd) {
+  const Team T = make_team();
+  const int64_t b = blockIdx.x;
+  ts_band_extract<kTsB>(T, n, A + b * (int64_t)n * n, n, Bd + b * 2 * kTsB * (int64_t)n);
+}
+
+// grid (B), kTsChaseWarps warps: the bulge chase of one k-point.  Warp w takes the
+// sweeps s = w, w + W, ...; before task t of sweep s it waits until sweep s - 1 has
+// finished its tasks 0 .. t + 2 (the tasks whose rows and columns overlap task t's),
+// read from a per-warp progress word in shared memory.  The band stays in global
+// memory (L1/L2): a warp's stores are fenced at block scope before it publishes
+// progress, and a waiting warp fences after it reads it.  Every wait is bounded:
+// on expiry the kernel records an error in *err, every warp stops at its next wait,
+// and d / e are not written.  V2 / tau2 (or null): the reflectors for the
+// back-transformation.  Outputs: d (n) and e (n - 1) of the real tridiagonal.
+__global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, double2* Bd, double2* V2,
+                                                                      double2* tau2, double* d, double* e,
+                                                                      int* err) {
+  __shared__ __align__(16) double2 sv[kTsChaseWarps][2 * kTsB + 2];
+  __shared__ long long prog[kTsChaseWarps];
+  __shared__ int stop;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const WarpTeam T = make_warpteam();
+  const int64_t b = blockIdx.x;
+  constexpr int ldb = 2 * kTsB;
+  double2* Bk = Bd + b * ldb * (int64_t)n;
+  const int tmax = ts_tmax(n, kTsB);
+  const long long unit = tmax + 1;  // progress: s * unit + tasks done
+  if (lane == 0) prog[w] = -1;
+  if (threadIdx.x == 0) stop = (err && *(volatile int*)err) ? 1 : 0;
+  __syncthreads();
+  volatile long long* vprog = prog;
+  volatile int* vstop = &stop;
+  bool ok = *vstop == 0;
+  const int wp = (w + kTsChaseWarps - 1) % kTsChaseWarps;  // the warp of sweep s - 1
+  for (int s = w; ok && s <= n - 2; s += kTsChaseWarps) {
+    const int nt = ts_tasks(n, kTsB, s);
+    const int ntp = (s > 0) ? ts_tasks(n, kTsB, s - 1) : 0;
+    for (int t = 0; t < nt; ++t) {
+      if (s > 0) {
+        const long long need = (long long)(s - 1) * unit + (t + 3 < ntp ? t + 3 : ntp);
+        if (lane == 0) {
+          int polls = 0;
+          while (vprog[wp] < need) {
+            if (*vstop) { ok = false; break; }
+            if (++polls > kTsWaitPolls) {
+              *vstop = 1;
+              if (err) atomicExch(err, 2);
+              ok = false;
+              break;
+            }
+            __nanosleep(100);
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        __syncwarp();
+        __threadfence_block();
+      }
+      double2* vo = V2 ? V2 + b * ts_v2_stride(n) + ((int64_t)s * tmax + t) * kTsB : nullptr;
+      double2* to = tau2 ? tau2 + b * ts_tau2_stride(n) + (int64_t)s * tmax + t : nullptr;
+      ts_chase_task<kTsB>(T, n, s, t, Bk, vo, to, sv[w]);
+      __threadfence_block();
+      __syncwarp();
+      if (lane == 0) vprog[w] = (long long)s * unit + t + 1;
+    }
+  }
+  __syncthreads();
+  const bool fin = *vstop == 0;  // after a failed wait: zeros, so the solver that follows stays bounded
+  __threadfence_block();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    d[b * n + i] = fin ? Bk[(int64_t)i * ldb].x : 0.0;
+    e[b * n + i] = (fin && i + 1 < n) ? Bk[1 + (int64_t)i * ldb].x : 0.0;
+  }
+}
+
+// grid (ceil(K / cols), B): Z <- Q2 Z on columns c0 .. c0+K-1 of U (n x n per
+// k-point).  A CTA holds `cols` columns of Z in shared memory (n x cols complex,
+// dynamic) and applies the sweeps in reverse order; the reflectors of one sweep act
+// on disjoint rows, so each (task, column) pair is one thread's and a barrier
+// separates the sweeps.
+__global__ void __launch_bounds__(kTsQ2Threads) ts_q2_kernel(int n, int c0, int K, int cols, const double2* V2,
+                                                             const double2* tau2, double2* U) {
+  extern __shared__ __align__(16) double2 zs[];
+  const int64_t b = blockIdx.y;
+  const int cb = blockIdx.x * cols;
+  const int nc = (K - cb < cols) ? K - cb : cols;
+  if (nc <= 0) return;
+  double2* Uk = U + b * (int64_t)n * n + (int64_t)(c0 + cb) * n;
+  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) zs[i] = Uk[i];
+  const double2* Vk = V2 + b * ts_v2_stride(n);
+  const double2* tk = tau2 + b * ts_tau2_stride(n);
+  const int tmax = ts_tmax(n, kTsB);
+  __syncthreads();
+  for (int s = n - 2; s >= 0; --s) {
+    const int nt = ts_tasks(n, kTsB, s);
+    for (int p = threadIdx.x; p < nt * nc; p += blockDim.x) {
+      const int t = p / nc, c = p - t * nc;
+      const int R0 = (t == 0) ? s + 1 : s + 1 + t * kTsB;
+      const int L = (n - R0 < kTsB) ? n - R0 : kTsB;
+      const double2* v = Vk + ((int64_t)s * tmax + t) * kTsB;
+      const double2 tj = tk[(int64_t)s * tmax + t];
+      double2* z = zs + (int64_t)c * n + R0;
+      double2 vr[kTsB];
+      double2 acc = cmk(0.0, 0.0);
+#pragma unroll
+      for (int r = 0; r < kTsB; ++r) {
+        vr[r] = v[r];  // zero-padded past L
+        if (r < L) acc = cadd(acc, cmulc(vr[r], z[r]));
+      }
+      const double2 f = cmul(tj, acc);
+#pragma unroll
+      for (int r = 0; r < kTsB; ++r)
+        if (r < L) z[r] = csub(z[r], cmul(vr[r], f));
+    }
+    __syncthreads();
+  }
+  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) Uk[i] = zs[i];
 }
 
 }  // namespace lqm

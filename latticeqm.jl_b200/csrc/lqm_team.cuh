@@ -71,6 +71,20 @@ LQM_FN SubTeam make_subteam(int size) {
   return t;
 }
 LQM_FN void team_sync(const SubTeam& T) { asm volatile("bar.sync %0, %1;\n" ::"r"(T.bar), "r"(T.nt) : "memory"); }
+// One warp as a team (warp-synchronous phases, e.g. one bulge-chasing sweep per warp).
+struct WarpTeam {
+  int tid, nt;
+  int lane, nl;
+  int wid, nw;
+};
+LQM_FN WarpTeam make_warpteam() {
+  WarpTeam t;
+  t.tid = threadIdx.x & 31; t.nt = 32;
+  t.lane = t.tid; t.nl = 32;
+  t.wid = 0; t.nw = 1;
+  return t;
+}
+LQM_FN void team_sync(const WarpTeam&) { __syncwarp(); }
 LQM_FN void team_syncwarp() { __syncwarp(); }
 LQM_FN double warp_sum(double v) {
 #pragma unroll

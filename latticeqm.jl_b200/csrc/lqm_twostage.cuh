@@ -1,0 +1,290 @@
+// Two-stage Hermitian tridiagonalisation for the batched large-n path, written
+// as team phases so the CUDA kernels and the host emulation share the arithmetic.
+//
+//   stage 1, dense -> band of half-bandwidth b (LAPACK zhetrd_he2hb, lower): per
+//     panel of b columns a QR of the m x b block below the band (ts_panel_qr),
+//     then A22 <- Q^H A22 Q by GEMMs issued by the host:
+//       Y = A22 V (A22 Hermitian, lower storage),  X = Y T,
+//       W = X - 1/2 V (T^H (V^H X)),  A22 -= V W^H + W V^H  (lower triangle);
+//     reflector j (j < n - b) is A(j+b:, j) with v0 = 1 implicit, A(j+b, j) = beta.
+//   stage 2, band -> real tridiagonal (LAPACK zhetrd_hb2st): bulge chasing.
+//     Sweep s annihilates column s below its subdiagonal; task t of the sweep
+//     (ts_chase_task) makes one reflector from the first column of the block the
+//     previous task filled, applies it from the left to the rest of that block,
+//     two-sided to its diagonal block and from the right to the block below,
+//     which becomes the next task's block.  Only the first column of each bulge
+//     is removed; the rest lies in the columns the next sweep annihilates, so the
+//     band never grows beyond 2b - 1 subdiagonals.  Successive sweeps can run
+//     concurrently when sweep s+1 stays three tasks behind sweep s.
+//   back-transformation U = Q1 Q2 Z: the stage-2 reflectors sweep by sweep (the
+//     reflectors of one sweep act on disjoint rows), then Q1 as compact-WY
+//     products (blk_larft and the GEMMs of the one-stage path, rows offset by b).
+//
+// The reference reaches the same factorisation through Julia's LinearAlgebra
+// (LAPACK zheevr on Hermitian(M), Eigen.jl:22-23); LAPACK's own two-stage driver
+// (zheevr_2stage) reduces in these two steps.
+#pragma once
+#include "lqm_blocked.cuh"
+
+// Band storage of stage 2: element (i, j), 0 <= i - j < ldb (ldb = 2b), at
+// Bd[(i - j) + j * ldb]; the upper triangle is implied by Hermitian symmetry.
+LQM_FN double2 ts_bget(const double2* Bd, int ldb, int i, int j) { return Bd[(i - j) + (int64_t)j * ldb]; }
+LQM_FN double2* ts_bptr(double2* Bd, int ldb, int i, int j) { return Bd + (i - j) + (int64_t)j * ldb; }
+
+#if defined(__CUDACC__)
+#define LQM_HD __host__ __device__ inline
+#else
+#define LQM_HD static inline
+#endif
+// Tasks of sweep s: the row blocks [s+1+t b, s+1+(t+1) b) that start inside the matrix.
+LQM_HD int ts_tasks(int n, int b, int s) { return (n - 1 - s + b - 1) / b; }
+// Reflector slots per sweep in the stage-2 reflector store (the first sweep's count).
+LQM_HD int ts_tmax(int n, int b) { return n > 1 ? (n - 1 + b - 1) / b : 1; }
+
+// QR of the panel below the band (LAPACK zgeqr2 on rows j0+b..n-1 of columns
+// j0..j0+pw-1, pw = min(b, n - j0), m = n - j0 - b rows, nr = min(b, m) reflectors),
+// then the explicit reflectors Vb (m x nr, leading dimension ldv: zero above the
+// unit diagonal) and the compact-WY factor Tm (b x b, leading dimension b, zlarft
+// forward, upper triangular, zero-padded).  Per column c: zlarfg on A(j+b:, j),
+// j = j0 + c; then H^H = I - conj(tau) v v^H on the panel columns right of it.
+// sm: team scratch of >= (nw + 2) * B + B * B complex (nw = warps of the team).
+template <int B, class TeamT>
+LQM_FN void ts_panel_qr(const TeamT& T, int n, int j0, double2* A, int lda, double2* tau, double2* Vb, int ldv,
+                        double2* Tm, double2* sm) {
+  const int m = n - j0 - B;
+  const int pw = (n - j0 < B) ? n - j0 : B;
+  const int nr = (m < B) ? m : B;
+  double2* part = sm;               // nw x B warp partials
+  double2* wv = sm + T.nw * B;      // B: the reduced w_l
+  double2* G = wv + 2 * B;          // B x B Gram matrix V^H V
+  double* red = (double*)(wv + B);  // 2B doubles
+  for (int c = 0; c < nr; ++c) {
+    const int j = j0 + c;
+    double2* col = A + (int64_t)j * lda;
+    const int r0 = j + B;  // the reflector's first row
+    double s = 0.0;
+    for (int r = r0 + 1 + T.tid; r < n; r += T.nt) { const double2 x = col[r]; s += x.x * x.x + x.y * x.y; }
+#if defined(__CUDACC__)
+    s = warp_sum(s);
+    if (T.lane == 0) red[T.wid] = s;
+    team_sync(T);
+    s = 0.0;
+    for (int w = 0; w < T.nw; ++w) s += red[w];
+#endif
+    const double2 alpha = col[r0];
+    double2 tj, scal;
+    double beta;
+    zlarfg_scalars(alpha, s, &tj, &beta, &scal);
+    team_sync(T);  // alpha (and red) read by every thread
+    for (int r = r0 + 1 + T.tid; r < n; r += T.nt) col[r] = cmul(scal, col[r]);
+    if (T.tid == 0) { col[r0] = cmk(beta, 0.0); tau[j] = tj; }
+    team_sync(T);
+    if (c + 1 >= pw) continue;
+    // w_l = sum_r conj(v_r) A(r, j0 + l), l = c+1 .. pw-1 (v_{r0} = 1)
+    double2 acc[B];
+#pragma unroll
+    for (int l = 0; l < B; ++l) acc[l] = cmk(0.0, 0.0);
+    for (int r = r0 + T.tid; r < n; r += T.nt) {
+      const double2 vr = (r == r0) ? cmk(1.0, 0.0) : col[r];
+#pragma unroll
+      for (int l = 0; l < B; ++l)
+        if (l > c && l < pw) acc[l] = cadd(acc[l], cmulc(vr, A[r + (int64_t)(j0 + l) * lda]));
+    }
+#pragma unroll
+    for (int l = 0; l < B; ++l) {
+      if (!(l > c && l < pw)) continue;
+      const double ar = warp_sum(acc[l].x), ai = warp_sum(acc[l].y);
+      if (T.lane == 0) part[T.wid * B + l] = cmk(ar, ai);
+    }
+    team_sync(T);
+    for (int l = c + 1 + T.tid; l < pw; l += T.nt) {
+      double2 w = cmk(0.0, 0.0);
+      for (int q = 0; q < T.nw; ++q) w = cadd(w, part[q * B + l]);
+      wv[l] = cmul(cconj(tj), w);  // conj(tau) w_l
+    }
+    team_sync(T);
+    for (int r = r0 + T.tid; r < n; r += T.nt) {
+      const double2 vr = (r == r0) ? cmk(1.0, 0.0) : col[r];
+      for (int l = c + 1; l < pw; ++l) {
+        double2* a = A + r + (int64_t)(j0 + l) * lda;
+        *a = csub(*a, cmul(vr, wv[l]));
+      }
+    }
+    team_sync(T);
+  }
+  if (nr <= 0) return;
+  // explicit reflectors: Vb(r, c) = 0 (r < c), 1 (r == c), A(j0+B+r, j0+c) (r > c)
+  for (int64_t idx = T.tid; idx < (int64_t)m * nr; idx += T.nt) {
+    const int r = (int)(idx % m), c = (int)(idx / m);
+    Vb[r + (int64_t)c * ldv] =
+        (r < c) ? cmk(0.0, 0.0) : (r == c) ? cmk(1.0, 0.0) : A[(j0 + B + r) + (int64_t)(j0 + c) * lda];
+  }
+  team_sync(T);
+  // Gram matrix G(q, l) = sum_r conj(V(r, q)) V(r, l), q < l (rows r >= l), warp per pair
+  for (int p = T.wid; p < B * B; p += T.nw) {
+    const int q = p % B, l = p / B;
+    if (!(q < l && l < nr)) continue;
+    double sr = 0.0, si = 0.0;
+    for (int r = l + T.lane; r < m; r += T.nl) {
+      const double2 x = cmulc(Vb[r + (int64_t)q * ldv], Vb[r + (int64_t)l * ldv]);
+      sr += x.x; si += x.y;
+    }
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    if (T.lane == 0) G[q + l * B] = cmk(sr, si);
+  }
+  for (int p = T.tid; p < B * B; p += T.nt) {
+    const int q = p % B, l = p / B;
+    Tm[p] = (q == l && l < nr) ? tau[j0 + l] : cmk(0.0, 0.0);
+  }
+  team_sync(T);
+  // zlarft forward: Tm(0:l, l) = -tau_l Tm(0:l, 0:l) G(0:l, l)
+  for (int l = 1; l < nr; ++l) {
+    const double2 tl = tau[j0 + l];
+    for (int q = T.tid; q < l; q += T.nt) {
+      double2 acc = cmk(0.0, 0.0);
+      for (int s2 = q; s2 < l; ++s2) acc = cadd(acc, cmul(Tm[q + s2 * B], G[s2 + l * B]));
+      Tm[q + l * B] = cmul(cmk(-tl.x, -tl.y), acc);
+    }
+    team_sync(T);
+  }
+}
+
+// Band of half-bandwidth B out of the stage-1 result (lower triangle of A): the
+// diagonal blocks and the R factors; the fill diagonals B+1 .. 2B-1 start at zero.
+template <int B, class TeamT>
+LQM_FN void ts_band_extract(const TeamT& T, int n, const double2* A, int lda, double2* Bd) {
+  const int ldb = 2 * B;
+  for (int64_t idx = T.tid; idx < (int64_t)ldb * n; idx += T.nt) {
+    const int o = (int)(idx % ldb), j = (int)(idx / ldb);
+    const int i = j + o;
+    double2 v = cmk(0.0, 0.0);
+    if (i < n && o <= B) v = A[i + (int64_t)j * lda];
+    if (o == 0) v.y = 0.0;
+    Bd[idx] = v;
+  }
+}
+
+// One task (s, t) of the bulge chase on the band Bd (ldb = 2B).  The reflector
+// H = I - tau v v^H (zlarfg: H^H x = beta e1, v0 = 1) is made from
+//   t = 0:  x = column s, rows s+1 .. s+L
+//   t > 0:  x = column c = s+1+(t-1)B, rows R0 .. R0+L-1 (R0 = s+1+tB)
+// with L = min(B, n - R0); then
+//   F <- H^H F   F = rows R0.., columns c+1 .. c+B-1 (t > 0: the rest of the bulge)
+//   D <- H^H D H D = the diagonal block on rows R0 .. R0+L-1
+//   E <- E H     E = rows R0+L .. R0+L+L'-1 (L' = min(B, n-R0-L)), columns of D
+// v (B complex, zero-padded) and tau go to vout / tauout when they are non-null.
+// sv: team scratch of 2B complex + 2 doubles.  The team is one warp on the device.
+template <int B, class TeamT>
+LQM_FN void ts_chase_task(const TeamT& T, int n, int s, int t, double2* Bd, double2* vout, double2* tauout,
+                          double2* sv) {
+  const int ldb = 2 * B;
+  const int R0 = (t == 0) ? s + 1 : s + 1 + t * B;
+  const int c = (t == 0) ? s : s + 1 + (t - 1) * B;
+  const int L = (n - R0 < B) ? n - R0 : B;
+  if (L <= 0) return;
+  double2* v = sv;
+  double2* w = sv + B;
+  // x and zlarfg
+  double s2 = 0.0;
+  for (int r = 1 + T.tid; r < L; r += T.nt) { const double2 x = ts_bget(Bd, ldb, R0 + r, c); s2 += x.x * x.x + x.y * x.y; }
+  s2 = warp_sum_bcast(s2);
+  const double2 alpha = ts_bget(Bd, ldb, R0, c);
+  double2 tj, scal;
+  double beta;
+  zlarfg_scalars(alpha, s2, &tj, &beta, &scal);
+  for (int r = T.tid; r < B; r += T.nt) {
+    double2 vr = cmk(0.0, 0.0);
+    if (r == 0) vr = cmk(1.0, 0.0);
+    else if (r < L) vr = cmul(scal, ts_bget(Bd, ldb, R0 + r, c));
+    v[r] = vr;
+    if (vout) vout[r] = vr;
+  }
+  team_sync(T);
+  for (int r = T.tid; r < L; r += T.nt) *ts_bptr(Bd, ldb, R0 + r, c) = (r == 0) ? cmk(beta, 0.0) : cmk(0.0, 0.0);
+  if (tauout && T.tid == 0) *tauout = tj;
+  const double2 ctj = cconj(tj);
+  // F <- H^H F: column c + 1 + l (l < B - 1) by thread
+  if (t > 0) {
+    for (int l = T.tid; l < B - 1; l += T.nt) {
+      const int cc = c + 1 + l;
+      double2 acc = cmk(0.0, 0.0);
+      for (int r = 0; r < L; ++r) acc = cadd(acc, cmulc(v[r], ts_bget(Bd, ldb, R0 + r, cc)));
+      const double2 f = cmul(ctj, acc);
+      for (int r = 0; r < L; ++r) {
+        double2* p = ts_bptr(Bd, ldb, R0 + r, cc);
+        *p = csub(*p, cmul(v[r], f));
+      }
+    }
+  }
+  // D <- H^H D H: y = D v (row r by thread), gamma = v^H y, w = tau y - 1/2 |tau|^2 gamma v
+  double2 yr = cmk(0.0, 0.0);
+  double g = 0.0;
+  for (int r = T.tid; r < L; r += T.nt) {
+    double2 acc = cmk(0.0, 0.0);
+    for (int q = 0; q < L; ++q) {
+      const double2 dq = (q <= r) ? ts_bget(Bd, ldb, R0 + r, R0 + q) : cconj(ts_bget(Bd, ldb, R0 + q, R0 + r));
+      acc = cadd(acc, cmul(dq, v[q]));
+    }
+    yr = acc;
+    g += cmulc(v[r], acc).x;
+#if !defined(__CUDACC__)
+    w[r] = acc;  // one-thread team: y kept in w until gamma is complete
+#endif
+  }
+  g = warp_sum_bcast(g);
+  const double h = -0.5 * (tj.x * tj.x + tj.y * tj.y) * g;
+#if defined(__CUDACC__)
+  for (int r = T.tid; r < L; r += T.nt) w[r] = cadd(cmul(tj, yr), cscale(h, v[r]));
+#else
+  for (int r = 0; r < L; ++r) w[r] = cadd(cmul(tj, w[r]), cscale(h, v[r]));
+#endif
+  team_sync(T);  // every thread has read D before it is rewritten
+  for (int r = T.tid; r < L; r += T.nt) {
+    const double2 vr = v[r], wr = w[r];
+    for (int q = 0; q <= r; ++q) {
+      double2* p = ts_bptr(Bd, ldb, R0 + r, R0 + q);
+      double2 a = csub(*p, cadd(cmul(wr, cconj(v[q])), cmul(vr, cconj(w[q]))));
+      if (q == r) a.y = 0.0;
+      *p = a;
+    }
+  }
+  // E <- E H: row i by thread, z_i = sum_q E(i, q) v_q, E(i, q) -= tau z_i conj(v_q)
+  const int R1 = R0 + L;
+  const int L2 = (n - R1 < B) ? n - R1 : B;
+  for (int i = T.tid; i < L2; i += T.nt) {
+    double2 acc = cmk(0.0, 0.0);
+    for (int q = 0; q < L; ++q) acc = cadd(acc, cmul(ts_bget(Bd, ldb, R1 + i, R0 + q), v[q]));
+    const double2 z = cmul(tj, acc);
+    for (int q = 0; q < L; ++q) {
+      double2* p = ts_bptr(Bd, ldb, R1 + i, R0 + q);
+      *p = csub(*p, cmul(z, cconj(v[q])));
+    }
+  }
+  team_sync(T);
+}
+
+// Applies H = I - tau v v^H of every stage-2 task to the rows of Z (n x nc, leading
+// dimension ldz), in the reverse order of the chase (Z <- Q2 Z).  Host emulation
+// form: the kernel applies one sweep's reflectors in parallel.
+// V2: reflectors of sweep s, task t at V2 + (s * tmax + t) * B; tau2 at s * tmax + t.
+template <int B>
+LQM_FN void ts_q2_apply_host(int n, const double2* V2, const double2* tau2, double2* Z, int ldz, int nc) {
+  const int tmax = ts_tmax(n, B);
+  for (int s = n - 2; s >= 0; --s) {
+    const int nt = ts_tasks(n, B, s);
+    for (int t = 0; t < nt; ++t) {
+      const int R0 = (t == 0) ? s + 1 : s + 1 + t * B;
+      const int L = (n - R0 < B) ? n - R0 : B;
+      const double2* v = V2 + ((int64_t)s * tmax + t) * B;
+      const double2 tj = tau2[(int64_t)s * tmax + t];
+      for (int c = 0; c < nc; ++c) {
+        double2* z = Z + (int64_t)c * ldz + R0;
+        double2 acc = cmk(0.0, 0.0);
+        for (int r = 0; r < L; ++r) acc = cadd(acc, cmulc(v[r], z[r]));
+        const double2 f = cmul(tj, acc);
+        for (int r = 0; r < L; ++r) z[r] = csub(z[r], cmul(v[r], f));
+      }
+    }
+  }
+}

@@ -27,7 +27,10 @@
 
 namespace lqm {
 
-enum GemmOp { OP_N = 0, OP_T = 1, OP_C = 2 };
+// OP_HL (first operand only, no split and no second pair): the operand is a
+// Hermitian matrix of which only the lower triangle is stored; element (r, k) is
+// A(r, k) for r >= k and conj(A(k, r)) above, with the diagonal taken as real.
+enum GemmOp { OP_N = 0, OP_T = 1, OP_C = 2, OP_HL = 3 };
 
 // complex elements per staged row: BK + 4 (== 4 mod 8: conflict-free fragment reads)
 __host__ __device__ constexpr int gemm_pitch(int BK) { return BK + 4; }
@@ -80,10 +83,11 @@ __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, 
 #pragma unroll
   for (int e = threadIdx.x; e < BM * BK; e += NT) {
     int r, kk;
-    if (g.opA == OP_N) { r = e % BM; kk = e / BM; } else { kk = e % BK; r = e / BK; }
+    if (g.opA == OP_N || g.opA == OP_HL) { r = e % BM; kk = e / BM; } else { kk = e % BK; r = e / BK; }
     const int gm = m0 + r, gk = k0 + kk;
     const bool ok = gm < g.m && gk < kend;
-    const double2* src = (g.opA == OP_N) ? A + gm + (int64_t)gk * lda : A + gk + (int64_t)gm * lda;
+    const bool lower = g.opA == OP_N || (g.opA == OP_HL && gm >= gk);
+    const double2* src = lower ? A + gm + (int64_t)gk * lda : A + gk + (int64_t)gm * lda;
     gemm_cp16(As + r * P + kk, ok ? (const void*)src : (const void*)A, ok);
   }
 #pragma unroll
@@ -197,6 +201,14 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
         const double2 a = As[(wm0 + 8 * i + gr) * P + kk + gt];
         ar[i] = a.x;
         ai[i] = sa * a.y;
+      }
+      if (g.opA == OP_HL) {  // entries above the diagonal were staged from their mirror
+        const int kg = ks * BK + kk + gt;
+#pragma unroll
+        for (int i = 0; i < MI; ++i) {
+          const int rg = m0 + wm0 + 8 * i + gr;
+          ai[i] = (rg > kg) ? ai[i] : (rg < kg) ? -ai[i] : 0.0;
+        }
       }
 #pragma unroll
       for (int j = 0; j < NJ; ++j) {

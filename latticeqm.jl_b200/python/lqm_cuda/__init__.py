@@ -35,6 +35,7 @@ STATUS_NAMES = {-1: "LQM_EINVAL", -2: "LQM_ECUDA", -3: "LQM_ENOMEM", -4: "LQM_ET
 
 EXPORTS = [
     "lqm_ctx_create", "lqm_ctx_destroy", "lqm_last_error", "lqm_ctx_set_timeout", "lqm_ctx_set_blocked_min_n",
+    "lqm_ctx_set_two_stage",
     "lqm_ctx_last_kernel_ms", "lqm_hops_upload_dense", "lqm_hops_upload_csc", "lqm_hops_free",
     "lqm_hops_dims", "lqm_bloch", "lqm_bloch_dev", "lqm_bandmatrix", "lqm_bandmatrix_dev",
     "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
@@ -72,6 +73,7 @@ _SIG = {
     "lqm_ctx_destroy": [_P],
     "lqm_ctx_set_timeout": [_P, _D],
     "lqm_ctx_set_blocked_min_n": [_P, _I64],
+    "lqm_ctx_set_two_stage": [_P, ctypes.c_int],
     "lqm_ctx_kernel_stats": [_P, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_D)],
     "lqm_comm_unique_id": [_P],
     "lqm_ctx_set_comm": [_P, ctypes.c_int, ctypes.c_int, _P],
@@ -179,6 +181,11 @@ class Context:
         """Orders n >= n_min use the batched blocked eigensolver (0: only where the
         one-CTA-per-k kernel does not fit)."""
         self.check(_lib.lqm_ctx_set_blocked_min_n(self._h, int(n_min)))
+
+    def set_two_stage(self, mode):
+        """Reduction of the blocked eigensolver: 1 two-stage (dense -> band -> tridiagonal),
+        0 one-stage panels, -1 (default) by order."""
+        self.check(_lib.lqm_ctx_set_two_stage(self._h, int(mode)))
 
     def set_eigh_threads(self, n, nt):
         """Block size of the one-CTA eigensolver for order n (0: the built-in rule)."""

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "lqm_blocked.cuh"
+#include "lqm_twostage.cuh"
 #include "lqm_eigh.cuh"
 #include "lqm_plan.h"
 
@@ -248,6 +249,152 @@ extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* block
     }
   }
   return 0;
+}
+
+// The two-stage large-n path on one k-point: stage 1 (ts_panel_qr, the GEMM
+// chain of the trailing update done here as loops), band extraction, the bulge
+// chase (ts_chase_task, sweeps in order), divide and conquer, then U = Q1 Q2 Z
+// (ts_q2_apply_host, the compact-WY products of blk_larft with the rows offset
+// by the half-bandwidth).
+template <int B>
+static int emul_twostage(int n, int nR, int dim, const double* blocks, const int64_t* keys, const double* kpt,
+                         int want_vectors, double* evals, double* U, double* tri) {
+  const Team T = make_host_team();
+  const size_t nn = (size_t)n * n;
+  std::vector<double2> A(nn), ph(nR + 1), tau(n + 1), Vb(nn + 1), Tm(B * B), sm((T.nw + 2) * B + B * B + 8);
+  std::vector<double2> Y(nn + 1), X(nn + 1), S(B * B), Z(B * B);
+  bloch_build(T, n, nR, dim, (const double2*)blocks, keys, kpt, ph.data(), A.data(), n);
+  for (int j0 = 0; j0 + B < n; j0 += B) {
+    const int m = n - j0 - B, nr = std::min(B, m);
+    ts_panel_qr<B>(T, n, j0, A.data(), n, tau.data(), Vb.data(), n, Tm.data(), sm.data());
+    auto a22 = [&](int r, int c) -> double2 {
+      return r >= c ? A[(j0 + B + r) + (size_t)(j0 + B + c) * n] : cconj(A[(j0 + B + c) + (size_t)(j0 + B + r) * n]);
+    };
+    for (int r = 0; r < m; ++r)
+      for (int l = 0; l < nr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int q = 0; q < m; ++q) acc = cadd(acc, cmul(a22(r, q), Vb[q + (size_t)l * n]));
+        Y[r + (size_t)l * n] = acc;
+      }
+    for (int r = 0; r < m; ++r)
+      for (int l = 0; l < nr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int q = 0; q < nr; ++q) acc = cadd(acc, cmul(Y[r + (size_t)q * n], Tm[q + l * B]));
+        X[r + (size_t)l * n] = acc;
+      }
+    for (int q = 0; q < nr; ++q)
+      for (int l = 0; l < nr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int r = 0; r < m; ++r) acc = cadd(acc, cmulc(Vb[r + (size_t)q * n], X[r + (size_t)l * n]));
+        S[q + l * B] = acc;
+      }
+    for (int q = 0; q < nr; ++q)
+      for (int l = 0; l < nr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int p = 0; p < nr; ++p) acc = cadd(acc, cmulc(Tm[p + q * B], S[p + l * B]));
+        Z[q + l * B] = cscale(0.5, acc);
+      }
+    for (int r = 0; r < m; ++r)
+      for (int l = 0; l < nr; ++l) {
+        double2 acc = X[r + (size_t)l * n];
+        for (int q = 0; q < nr; ++q) acc = csub(acc, cmul(Vb[r + (size_t)q * n], Z[q + l * B]));
+        Y[r + (size_t)l * n] = acc;  // W
+      }
+    for (int c = 0; c < m; ++c)
+      for (int r = c; r < m; ++r) {
+        double2& a = A[(j0 + B + r) + (size_t)(j0 + B + c) * n];
+        for (int l = 0; l < nr; ++l) {
+          const double2 vr = Vb[r + (size_t)l * n], vc = Vb[c + (size_t)l * n];
+          const double2 wr = Y[r + (size_t)l * n], wc = Y[c + (size_t)l * n];
+          a = csub(a, cadd(cmul(vr, cconj(wc)), cmul(wr, cconj(vc))));
+        }
+      }
+  }
+  const int ldb = 2 * B, tmax = ts_tmax(n, B);
+  std::vector<double2> Bd((size_t)ldb * n), V2((size_t)std::max(n - 1, 1) * tmax * B), tau2((size_t)std::max(n - 1, 1) * tmax),
+      sv(2 * B + 2);
+  ts_band_extract<B>(T, n, A.data(), n, Bd.data());
+  for (int s = 0; s <= n - 2; ++s)
+    for (int t = 0; t < ts_tasks(n, B, s); ++t)
+      ts_chase_task<B>(T, n, s, t, Bd.data(), V2.data() + ((size_t)s * tmax + t) * B, tau2.data() + (size_t)s * tmax + t,
+                       sv.data());
+  std::vector<double> d(n), e(n, 0.0);
+  double offmax = 0.0;  // entries outside the tridiagonal after the chase (should be zero)
+  for (int j = 0; j < n; ++j) {
+    d[j] = Bd[(size_t)j * ldb].x;
+    if (j + 1 < n) e[j] = Bd[1 + (size_t)j * ldb].x;
+    if (j + 1 < n) offmax = std::max(offmax, std::fabs(Bd[1 + (size_t)j * ldb].y));
+    for (int o = 2; o < ldb && j + o < n; ++o) {
+      const double2 x = Bd[o + (size_t)j * ldb];
+      offmax = std::max(offmax, std::fabs(x.x) + std::fabs(x.y));
+    }
+  }
+  if (tri) { std::memcpy(tri, d.data(), sizeof(double) * n); std::memcpy(tri + n, e.data(), sizeof(double) * n); tri[2 * n] = offmax; }
+  const lqm::DCPlanHost PH = lqm::make_dc_plan_host(n);
+  const DCPlan PV = plan_view(PH);
+  std::vector<double> dbuf(13 * (size_t)n + 132), Q(nn + 4 * (size_t)n + 4), Qt(nn), Ub(nn);
+  std::vector<int> ibuf(10 * (size_t)n);
+  std::vector<double2> pb((size_t)n + 8);
+  EighVec SV;
+  double* db = dbuf.data();
+  SV.d = db; SV.e = db + n; SV.D = db + 2 * n; SV.z = db + 3 * n; SV.dl = db + 4 * n; SV.zl = db + 5 * n;
+  SV.troot = db + 6 * n; SV.zhat = db + 7 * n; SV.vals = db + 8 * n; SV.dval = db + 9 * n; SV.rc = db + 10 * n;
+  SV.rs = db + 11 * n; SV.nrho = db + 12 * n; SV.red = db + 13 * n;
+  int* ib = ibuf.data();
+  SV.perm = ib; SV.colnd = ib + n; SV.org = ib + 2 * n; SV.dcol = ib + 3 * n; SV.newpos = ib + 4 * n;
+  SV.ri = ib + 5 * n; SV.rj = ib + 6 * n; SV.nk = ib + 7 * n; SV.nrot = ib + 8 * n; SV.ndef = ib + 9 * n;
+  SV.pbuf = pb.data();
+  std::memcpy(SV.d, d.data(), sizeof(double) * n);
+  std::memcpy(SV.e, e.data(), sizeof(double) * n);
+  if (n > 0) SV.e[n - 1] = 0.0;
+  dc_solve(T, n, PV, SV, Q.data(), Qt.data(), nullptr, want_vectors != 0, Ub.data(), 1 << 30);
+  std::memcpy(evals, SV.D, sizeof(double) * n);
+  if (!want_vectors) return 0;
+  double2* Uc = (double2*)U;
+  for (size_t i = 0; i < nn; ++i) Uc[i] = cmk(Q[i], 0.0);
+  ts_q2_apply_host<B>(n, V2.data(), tau2.data(), Uc, n, n);
+  const int NR = n - B;
+  blk_prep_reflectors(T, n, A.data(), n, B);
+  const int nb = 2 * B;  // back-transformation panels of two stage-1 panels
+  std::vector<double2> Tb((size_t)nb * nb), G((size_t)nb * nb), Xb((size_t)nb * n);
+  for (int p = (NR + nb - 1) / nb - 1; p >= 0; --p) {
+    const int j0 = p * nb, nbr = std::min(nb, NR - j0);
+    if (nbr <= 0) continue;
+    const int m = n - j0 - B;
+    blk_larft(T, n, nb, j0, nbr, A.data(), n, tau.data(), Tb.data(), G.data(), nullptr, B);
+    const double2* V = A.data() + (j0 + B) + (size_t)j0 * n;
+    double2* Us = Uc + (j0 + B);
+    for (int c = 0; c < n; ++c)
+      for (int l = 0; l < nbr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int r = 0; r < m; ++r) acc = cadd(acc, cmulc(V[r + (size_t)l * n], Us[r + (size_t)c * n]));
+        Xb[l + (size_t)c * nb] = acc;
+      }
+    for (int c = 0; c < n; ++c) {
+      double2 y[64];
+      for (int l = 0; l < nbr; ++l) {
+        double2 acc = cmk(0.0, 0.0);
+        for (int q = 0; q < nbr; ++q) acc = cadd(acc, cmul(Tb[l + (size_t)q * nb], Xb[q + (size_t)c * nb]));
+        y[l] = acc;
+      }
+      for (int r = 0; r < m; ++r) {
+        double2 u = Us[r + (size_t)c * n];
+        for (int l = 0; l < nbr; ++l) u = csub(u, cmul(V[r + (size_t)l * n], y[l]));
+        Us[r + (size_t)c * n] = u;
+      }
+    }
+  }
+  return 0;
+}
+
+// b: the half-bandwidth (4 or 16); tri (or null): d, e and the largest entry
+// left outside the tridiagonal (3n doubles... 2n + 1 used).
+extern "C" int lqm_emul_eigh_twostage(int n, int nR, int dim, const double* blocks, const int64_t* keys,
+                                      const double* kpt, int b, int want_vectors, double* evals, double* U,
+                                      double* tri) {
+  if (b == 4) return emul_twostage<4>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri);
+  if (b == 16) return emul_twostage<16>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri);
+  return -1;
 }
 
 // rho_from_U on a given U (n x n, ld n) and occupations f.

@@ -40,6 +40,74 @@ def tbg10():
     return M.tbg_slater_koster(10)[1]
 
 
+@pytest.fixture(scope="module")
+def tsctx(lqm):
+    """The blocked path with the two-stage reduction on every order it accepts (n > 17)."""
+    c = lqm.Context(0, timeout=900)
+    c.set_blocked_min_n(1)
+    c.set_two_stage(1)
+    yield c
+    c.close()
+
+
+def test_two_stage_models_bands_vectors_rho(lqm, tsctx):
+    """Two-stage reduction (band of half-bandwidth 16, bulge chase, Q1 Q2 Z) on the
+    batched workload's models and the n = 144 honeycomb: bands, eigenpairs and rho_L."""
+    _, c1 = M.honeycomb_disorder()
+    rng = np.random.default_rng(12)
+    ks = np.hstack([L.regulargrid(6 * 6), rng.random((2, 7))])
+    w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+    for name, h in M.batch_models()[1:] + [("c1", c1)]:
+        b, _ = lqm.bandmatrix(h, ks, ctx=tsctx)
+        assert rel_band_err(b, K.bandmatrix(h, ks)[0]) <= BAND_TOL, name
+        b2, U = lqm.bandmatrix(h, ks[:, :4], want_vectors=True, ctx=tsctx)
+        n = b2.shape[0]
+        for j in range(4):
+            Hk = K.fouriersum(h, ks[:, j])
+            assert np.max(np.abs(U[:, :, j].conj().T @ U[:, :, j] - np.eye(n))) < 1e-12, name
+            assert np.max(np.abs(Hk @ U[:, :, j] - U[:, :, j] * b2[:, j])) < 1e-11, name
+        keys = list(h.keys())
+        rho = {R: None for R in keys}
+        eb = lqm.getdensitymatrix(rho, h, ks, kweights=w, mu=0.0, T=0.01, ctx=tsctx)
+        rref, ebref = K.densitymatrix(h, ks, w, 0.0, 0.01, keys)
+        assert max(np.max(np.abs(rho[L_] - rref[L_])) for L_ in keys) <= RHO_TOL, name
+        assert abs(eb - ebref) <= 1e-9 * max(1.0, abs(ebref)), name
+
+
+def test_two_stage_matches_one_stage(lqm, bctx, tsctx):
+    """The same bands through both reductions of the blocked path, to rounding."""
+    _, c1 = M.honeycomb_disorder()
+    ks = np.random.default_rng(6).random((2, 200))
+    one = lqm.Context(0, timeout=900)
+    try:
+        one.set_blocked_min_n(1)
+        one.set_two_stage(0)
+        for h in (M.batch_models()[2][1], c1):
+            b1, _ = lqm.bandmatrix(h, ks, ctx=one)
+            b2, _ = lqm.bandmatrix(h, ks, ctx=tsctx)
+            assert rel_band_err(b2, b1) <= 1e-12
+    finally:
+        one.close()
+
+
+def test_two_stage_hard_hermitian_inputs(lqm, tsctx):
+    """The emulation suite's hard Hermitian inputs (n = 96) through the two-stage path."""
+    from test_emulation import _hard_hermitian
+    ks = np.zeros((2, 1))
+    for name, Hk in _hard_hermitian():
+        n = Hk.shape[0]
+        if n <= 17:
+            continue
+        b, U = lqm.bandmatrix({(0, 0): Hk}, ks, want_vectors=True, ctx=tsctx)
+        ref = K.eigh_upper(Hk, vectors=False)
+        scale = max(np.max(np.abs(ref)), np.finfo(float).tiny)
+        Uk = U[:, :, 0]
+        assert np.all(np.isfinite(Uk)), name
+        assert np.max(np.abs(b[:, 0] - ref)) <= 1e-12 * scale, name
+        assert np.max(np.abs(Uk.conj().T @ Uk - np.eye(n))) <= 1e-12, name
+        assert np.max(np.abs(Hk @ Uk - Uk * b[:, 0])) <= 1e-12 * scale, name
+
+
 def test_blocked_tbg_golden_eigenvalues(lqm, bctx):
     pins = json.load(open(os.path.join(GOLD, "reference_pins.json")))["pins"]
     builders = {"honeycomb_twisted": L.honeycomb_twisted, "honeycomb_twisted_ABBA": L.honeycomb_twisted_ABBA,
@@ -89,9 +157,18 @@ def test_blocked_matches_one_cta_path(lqm, ctx, bctx):
     assert rel_band_err(b2, b1) <= 1e-12
 
 
-def test_tbg_1324_bands_vectors_rho(lqm, ctx, tbg10):
+@pytest.mark.parametrize("two_stage", [1, 0])
+def test_tbg_1324_bands_vectors_rho(lqm, ctx, tbg10, two_stage):
     """Twisted bilayer m=10 (n = 1324): beyond the one-CTA plan, so the default context
-    takes the blocked path.  Bands, eigenpairs and rho_L on a few k-points."""
+    takes the blocked path (both reductions).  Bands, eigenpairs and rho_L on a few k-points."""
+    ctx.set_two_stage(two_stage)
+    try:
+        _tbg_1324_check(lqm, ctx, tbg10)
+    finally:
+        ctx.set_two_stage(-1)
+
+
+def _tbg_1324_check(lqm, ctx, tbg10):
     h = tbg10
     n = next(iter(h.values())).shape[0]
     assert n == 1324
