@@ -284,7 +284,8 @@ def large_configs(Q, ctx, M, threads):
         "kpath_points": kp3.shape[1], "kpath_bands_kpts_per_s": kp3.shape[1] / db,
         "kpath_bands_wall_kpts_per_s": kp3.shape[1] / wb,
         "cpu_kpath_bands_kpts_per_s": cpu_rate(h3, kp3, threads, per_thread=2, bands_only=True),
-        "path": "batched blocked eigensolver (eigenvalue-only merges)"}
+        "path": "batched blocked eigensolver, two-stage reduction (dense -> band of half-bandwidth 16 by panel "
+                "QRs and GEMM updates, bulge chase to the tridiagonal), eigenvalue-only merges"}
     # twisted bilayer m=15, n = 2884: one eigen + rho pass over the 12 x 12 grid, then
     # the Hartree-Fock SCF with the screened Coulomb interaction (3 iterations, the
     # 2nd and 3rd replayed from a captured CUDA graph), on a context of its own so that

@@ -15,7 +15,7 @@ LIB = os.path.join(LIBDIR, "libkspace.so")
 SOURCES = ["lqm_capi.cu"]
 DEPS = ["lqm_capi.cu", "lqm_kernels.cuh", "lqm_eigh.cuh", "lqm_team.cuh", "lqm_hf.cuh", "lqm_scf.inc", "lqm_plan.h",
         "lqm_blocked.cuh", "lqm_large.cuh", "lqm_adjoint.inc", "lqm_obs.inc", "lqm_anderson.inc",
-        "lqm_sitedos.inc", "lqm_berry.inc", "lqm_kubo.inc", "lqm_partial.inc", "lqm_commutator.inc", "lqm_bdg.inc", "lqm_scf_bdg.inc", "lqm_autotune.inc", "lqm_comm.inc", "lqm_scfgrad.inc", "lqm_zgemm.cuh"]
+        "lqm_sitedos.inc", "lqm_berry.inc", "lqm_kubo.inc", "lqm_partial.inc", "lqm_commutator.inc", "lqm_bdg.inc", "lqm_scf_bdg.inc", "lqm_autotune.inc", "lqm_comm.inc", "lqm_scfgrad.inc", "lqm_zgemm.cuh", "lqm_twostage.cuh"]
 CUDA_LIB = "/usr/local/cuda/lib64"
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -417,7 +417,7 @@ void zher2k_lower(lqm_ctx* ctx, int m, int k, const double2* X, int ldx, long lo
 
 struct RhoOut;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR);
-bool use_two_stage(const lqm_ctx* ctx, int n);
+bool use_two_stage(const lqm_ctx* ctx, int n, bool vec);
 
 // Eigen pass of the blocked path: same outputs as launch_eigh.  Reduction by
 // zlatrd panels (column kernels + batched rank-2nb updates), divide and
@@ -467,7 +467,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   const bool vec = d_U || rhok;
   // two-stage: dense -> band (kTsB) -> tridiagonal; reflector j of the first stage
   // starts at row j + off, n - off of them
-  const bool ts = use_two_stage(ctx, n);
+  const bool ts = use_two_stage(ctx, n, vec);
   const int off = ts ? kTsB : 1;
   const int NR = n - off;
   const int64_t nn = (int64_t)n * n;
@@ -646,8 +646,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     }
     if (K > 0 && ts) {
       // Z <- Q2 Z on the K columns: the stage-2 reflectors, sweeps in reverse order
-      const int cols = std::max(1, std::min(kTsQ2MaxCols, (200 * 1024) / (16 * n)));
-      const int qsm = 16 * n * cols;
+      const int cols = std::max(1, std::min(kTsQ2MaxCols, (200 * 1024) / (16 * ts_q2_ld(n))));
+      const int qsm = 16 * ts_q2_ld(n) * cols;
       ck(cudaFuncSetAttribute(ts_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm), "smem attr");
       ts_q2_kernel<<<dim3((unsigned)((K + cols - 1) / cols), (unsigned)nbk), kTsQ2Threads, qsm, ctx->stream>>>(
           n, c0, K, cols, V2, tau2, Ucur);
@@ -789,16 +789,20 @@ bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
 }
 
 // Reduction of the blocked path: two-stage (dense -> band -> tridiagonal) or the
-// one-stage zlatrd panels; ctx->two_stage when set (lqm_ctx_set_two_stage), else by
-// order from kTwoStageDefaultMinN on.  LQM_TWO_STAGE=0/1 in the environment overrides
-// both (development switch for measurements).
-constexpr int kTwoStageDefaultMinN = 1 << 30;
-bool use_two_stage(const lqm_ctx* ctx, int n) {
+// one-stage zlatrd panels; ctx->two_stage when set (lqm_ctx_set_two_stage), else the
+// two-stage form for passes without eigenvectors from kTwoStageDefaultMinN on.  With
+// eigenvectors the stage-2 back-transformation (latency-bound reflector sweeps)
+// costs more than the reduction saves (measured on B200 at n = 1324: rho pass 3.55 s
+// two-stage against 1.90 s one-stage for 576 k-points; eigenvalues only 0.56 s
+// against 0.92 s for 400).  LQM_TWO_STAGE=0/1 in the environment overrides both
+// (development switch for measurements).
+constexpr int kTwoStageDefaultMinN = 128;
+bool use_two_stage(const lqm_ctx* ctx, int n, bool vec) {
   if (n <= kTsB + 1) return false;
   const char* env = std::getenv("LQM_TWO_STAGE");
   if (env && (env[0] == '0' || env[0] == '1')) return env[0] == '1';
   if (ctx->two_stage >= 0) return ctx->two_stage == 1;
-  return n >= kTwoStageDefaultMinN;
+  return !vec && n >= kTwoStageDefaultMinN;
 }
 
 int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
