@@ -274,7 +274,7 @@ def large_configs(Q, ctx, M, threads):
         "grid": "48x48", "bands_kpts_per_s": ks1.shape[1] / dv, "bands_wall_kpts_per_s": ks1.shape[1] / wl,
         "rho_kpts_per_s": ks1.shape[1] / dd, "rho_wall_kpts_per_s": ks1.shape[1] / wd,
         "cpu_rho_kpts_per_s": cpu_rate(h1, ks1, threads, per_thread=8),
-        "path": "batched blocked eigensolver (n >= 128)"}
+        "path": "one-CTA-per-k eigensolver, Householder matrix in global scratch (n < 224)"}
     # twisted bilayer m=10, n = 1324: the 400-point k-path (bands only; rho on the 24 x 24
     # grid is the headline)
     lat3, h3 = M.tbg_slater_koster(10)
@@ -515,7 +515,7 @@ def main():
                     help="skip the other configurations (batch of n=8/24/96, n=144, the k-path, n=2884, SCF, "
                          "the adjoint, Kubo)")
     ap.add_argument("--profile-case", nargs="?", const="n96", default=None,
-                    choices=["n96", "tbg10-bands576", "tbg10-density142", "tbg10-density16", "kubo144"],
+                    choices=["n96", "tbg10-bands576", "tbg10-bands16", "tbg10-density142", "tbg10-density16", "kubo144"],
                     help="one call of a small profiling case: n96 = the fused bench call on the n=96 model "
                          "over 2048 k; tbg10-* = bands or density of the n=1324 twisted bilayer over the "
                          "first 576 / 142 / 16 points of the 24x24 grid; kubo144 = the Kubo correlator "

@@ -62,7 +62,7 @@ const char* lqm_last_error(const lqm_ctx* ctx);
  * the earlier copies) or after lqm_ctx_destroy. */
 int lqm_ctx_set_timeout(lqm_ctx* ctx, double seconds);
 /* Eigensolver path selection: orders n >= n_min use the batched blocked path
- * (panel reduction + batched GEMMs); 0 (default) selects it from n = 128 on.
+ * (panel reduction + batched GEMMs); 0 (default) selects it from n = 224 on.
  * No reference counterpart (the reference always calls LAPACK zheevr). */
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
 /* Reduction of the blocked path: 1 two-stage (dense -> band of half-bandwidth 16 by

@@ -556,7 +556,9 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       }
       // stage 2: the band, then the bulge chase to the real tridiagonal
       ts_band_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A, Bd);
-      ts_chase_kernel<<<nbk, kTsChaseWarps * 32, 0, ctx->stream>>>(n, Bd, V2, tau2, dd, ee, ctx->d_err);
+      ck(cudaFuncSetAttribute(ts_chase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTsChaseSmem),
+         "smem attr");
+      ts_chase_kernel<<<nbk, kTsChaseWarps * 32, kTsChaseSmem, ctx->stream>>>(n, Bd, V2, tau2, dd, ee, ctx->d_err);
       ctx->err_armed = true;
       ctx->launches += 2;
     } else {
@@ -646,8 +648,10 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     }
     if (K > 0 && ts) {
       // Z <- Q2 Z on the K columns: the stage-2 reflectors, sweeps in reverse order
-      const int cols = std::max(1, std::min(kTsQ2MaxCols, (200 * 1024) / (16 * ts_q2_ld(n))));
-      const int qsm = 16 * ts_q2_ld(n) * cols;
+      int cols = kTsQ2MaxCols;
+      while (cols > 1 && ts_q2_smem(n, cols) > 220 * 1024) --cols;
+      const int qsm = ts_q2_smem(n, cols);
+      if (qsm > 227 * 1024) fail(LQM_EINVAL, "n=%d exceeds the stage-2 back-transformation's shared-memory plan", n);
       ck(cudaFuncSetAttribute(ts_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm), "smem attr");
       ts_q2_kernel<<<dim3((unsigned)((K + cols - 1) / cols), (unsigned)nbk), kTsQ2Threads, qsm, ctx->stream>>>(
           n, c0, K, cols, V2, tau2, Ucur);
@@ -777,11 +781,13 @@ void launch_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks
   ctx->launches++;
 }
 
-// Path choice: the blocked path from n = 128 on (measured on B200: 18% faster
-// than the one-CTA kernel's global-memory variant at n = 144, 21% slower at
-// n = 96), or from ctx->blocked_min_n when set, and always beyond the one-CTA
-// kernel's shared-memory plan.
-constexpr int kBlockedDefaultMinN = 128;
+// Path choice: the blocked path from n = 224 on, or from ctx->blocked_min_n when
+// set, and always beyond the one-CTA kernel's shared-memory plan.  Measured on
+// B200 (disordered honeycomb supercells, 1024 k-points, bands / rho k-points per
+// second, one-CTA kernel against the blocked path): n = 144: 76.6k / 53.1k against
+// 37.1k / 32.9k; n = 196: 31.2k / 19.8k against 23.5k / 18.8k; n = 256: 13.4k /
+// 9.6k against 16.3k / 12.1k; n = 400: 3.2k / 2.3k against 8.2k / 5.0k.
+constexpr int kBlockedDefaultMinN = 224;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
   const int64_t nmin = ctx->blocked_min_n > 0 ? ctx->blocked_min_n : kBlockedDefaultMinN;
   if (n >= nmin) return true;

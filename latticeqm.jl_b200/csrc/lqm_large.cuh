@@ -717,7 +717,7 @@ __global__ void __launch_bounds__(kBlkThreads) blk_add_identity_kernel(int n, do
 // ---- Two-stage reduction (lqm_twostage.cuh) ----
 constexpr int kTsB = 16;              // half-bandwidth of the stage-1 band
 constexpr int kTsPanelThreads = 512;  // panel QR: latency-bound row passes, CTA per k-point
-constexpr int kTsChaseWarps = 16;     // bulge chase: sweeps in flight per k-point (one warp each)
+constexpr int kTsChaseWarps = 8;      // bulge chase: sweeps in flight per k-point (one warp each)
 constexpr int kTsQ2Threads = 256;
 constexpr int kTsQ2MaxCols = 8;       // columns of Z per CTA in the Q2 back-transformation
 constexpr int kTsWaitPolls = 1 << 22; // bound of one inter-warp wait of the chase (polls of ~0.1 us)
@@ -746,18 +746,21 @@ __global__ void __launch_bounds__(kBlkThreads) ts_band_kernel(int n, const doubl
 }
 
 // grid (B), kTsChaseWarps warps: the bulge chase of one k-point.  Warp w takes the
-// sweeps s = w, w + W, ...; before task t of sweep s it waits until sweep s - 1 has
+// sweeps s = w, w + W, ... (ts_chase_sweep, its blocks in the warp's window of
+// dynamic shared memory); before task t of sweep s it waits until sweep s - 1 has
 // finished its tasks 0 .. t + 2 (the tasks whose rows and columns overlap task t's),
 // read from a per-warp progress word in shared memory.  The band stays in global
 // memory (L1/L2): a warp's stores are fenced at block scope before it publishes
 // progress, and a waiting warp fences after it reads it.  Every wait is bounded:
 // on expiry the kernel records an error in *err, every warp stops at its next wait,
-// and d / e are not written.  V2 / tau2 (or null): the reflectors for the
+// and d / e are written as zeros.  V2 / tau2 (or null): the reflectors for the
 // back-transformation.  Outputs: d (n) and e (n - 1) of the real tridiagonal.
+constexpr int kTsWin = 3 * kTsB * (kTsB + 1) + 2 * kTsB;  // complex per warp window
+constexpr int kTsChaseSmem = kTsChaseWarps * kTsWin * 16;
 __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, double2* Bd, double2* V2,
                                                                       double2* tau2, double* d, double* e,
                                                                       int* err) {
-  __shared__ __align__(16) double2 sv[kTsChaseWarps][2 * kTsB + 2];
+  extern __shared__ __align__(16) double2 tswin[];
   __shared__ long long prog[kTsChaseWarps];
   __shared__ int stop;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -775,36 +778,37 @@ __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, dou
   bool ok = *vstop == 0;
   const int wp = (w + kTsChaseWarps - 1) % kTsChaseWarps;  // the warp of sweep s - 1
   for (int s = w; ok && s <= n - 2; s += kTsChaseWarps) {
-    const int nt = ts_tasks(n, kTsB, s);
     const int ntp = (s > 0) ? ts_tasks(n, kTsB, s - 1) : 0;
-    for (int t = 0; t < nt; ++t) {
-      if (s > 0) {
-        const long long need = (long long)(s - 1) * unit + (t + 3 < ntp ? t + 3 : ntp);
-        if (lane == 0) {
-          int polls = 0;
-          while (vprog[wp] < need) {
-            if (*vstop) { ok = false; break; }
-            if (++polls > kTsWaitPolls) {
-              *vstop = 1;
-              if (err) atomicExch(err, 2);
-              ok = false;
-              break;
-            }
-            __nanosleep(100);
+    auto wait = [&](int t) -> bool {
+      if (s == 0) return true;
+      const long long need = (long long)(s - 1) * unit + (t + 3 < ntp ? t + 3 : ntp);
+      bool good = true;
+      if (lane == 0) {
+        int polls = 0;
+        while (vprog[wp] < need) {
+          if (*vstop) { good = false; break; }
+          if (++polls > kTsWaitPolls) {
+            *vstop = 1;
+            if (err) atomicExch(err, 2);
+            good = false;
+            break;
           }
+          __nanosleep(64);
         }
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) break;
-        __syncwarp();
-        __threadfence_block();
       }
-      double2* vo = V2 ? V2 + b * ts_v2_stride(n) + ((int64_t)s * tmax + t) * kTsB : nullptr;
-      double2* to = tau2 ? tau2 + b * ts_tau2_stride(n) + (int64_t)s * tmax + t : nullptr;
-      ts_chase_task<kTsB>(T, n, s, t, Bk, vo, to, sv[w]);
+      good = __shfl_sync(0xffffffffu, good, 0);
+      __syncwarp();
+      __threadfence_block();
+      return good;
+    };
+    auto done = [&](int t) {
       __threadfence_block();
       __syncwarp();
       if (lane == 0) vprog[w] = (long long)s * unit + t + 1;
-    }
+    };
+    double2* vo = V2 ? V2 + b * ts_v2_stride(n) + (int64_t)s * tmax * kTsB : nullptr;
+    double2* to = tau2 ? tau2 + b * ts_tau2_stride(n) + (int64_t)s * tmax : nullptr;
+    ok = ts_chase_sweep<kTsB>(T, n, s, Bk, vo, to, tswin + w * kTsWin, wait, done);
   }
   __syncthreads();
   const bool fin = *vstop == 0;  // after a failed wait: zeros, so the solver that follows stays bounded
@@ -816,10 +820,18 @@ __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, dou
 }
 
 // grid (ceil(K / cols), B): Z <- Q2 Z on columns c0 .. c0+K-1 of U (n x n per
-// k-point).  A CTA holds `cols` columns of Z in shared memory (n x cols complex,
-// dynamic) and applies the sweeps in reverse order; the reflectors of one sweep act
-// on disjoint rows, so each (task, column) pair is one thread's and a barrier
-// separates the sweeps.
+// k-point).  A CTA holds `cols` columns of Z in shared memory (leading dimension
+// ts_q2_ld(n), odd in 16-byte units so that the columns of one task fall on distinct
+// banks) and applies the sweeps in reverse order; the reflectors of one sweep act on
+// disjoint rows, so each (task, column) pair is one thread's and a barrier separates
+// the sweeps.  The next sweep's reflectors and taus (contiguous in the store) are
+// copied into a second shared buffer by cp.async while a sweep is applied.  A pair's
+// dot product runs on four partial sums.
+__host__ __device__ inline int ts_q2_ld(int n) { return n | 1; }
+__host__ __device__ inline int ts_q2_vstage(int n) { return ts_tmax(n, kTsB) * (kTsB + 1); }
+__host__ __device__ inline int ts_q2_smem(int n, int cols) {
+  return 16 * (ts_q2_ld(n) * cols + 2 * ts_q2_vstage(n));
+}
 __global__ void __launch_bounds__(kTsQ2Threads) ts_q2_kernel(int n, int c0, int K, int cols, const double2* V2,
                                                              const double2* tau2, double2* U) {
   extern __shared__ __align__(16) double2 zs[];
@@ -827,36 +839,61 @@ __global__ void __launch_bounds__(kTsQ2Threads) ts_q2_kernel(int n, int c0, int 
   const int cb = blockIdx.x * cols;
   const int nc = (K - cb < cols) ? K - cb : cols;
   if (nc <= 0) return;
+  const int ld = ts_q2_ld(n);
+  const int tmax = ts_tmax(n, kTsB);
+  const int vst = ts_q2_vstage(n);
+  double2* vb = zs + (int64_t)ld * cols;  // two stages of (tmax x kTsB reflectors, tmax taus)
   double2* Uk = U + b * (int64_t)n * n + (int64_t)(c0 + cb) * n;
-  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) zs[i] = Uk[i];
   const double2* Vk = V2 + b * ts_v2_stride(n);
   const double2* tk = tau2 + b * ts_tau2_stride(n);
-  const int tmax = ts_tmax(n, kTsB);
-  __syncthreads();
+  auto stage = [&](int s, double2* dst) {
+    const int nt = ts_tasks(n, kTsB, s);
+    const double2* src = Vk + (int64_t)s * tmax * kTsB;
+    for (int i = threadIdx.x; i < nt * kTsB; i += blockDim.x) cp_async16(dst + i, src + i, true);
+    const double2* ts = tk + (int64_t)s * tmax;
+    for (int i = threadIdx.x; i < nt; i += blockDim.x) cp_async16(dst + tmax * kTsB + i, ts + i, true);
+  };
+  if (n >= 2) stage(n - 2, vb);
+  cp_async_commit();
+  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) {
+    const int r = (int)(i % n), c = (int)(i / n);
+    zs[r + (int64_t)c * ld] = Uk[i];
+  }
   for (int s = n - 2; s >= 0; --s) {
+    const double2* buf = vb + ((n - 2 - s) & 1) * vst;
+    if (s > 0) stage(s - 1, vb + ((n - 1 - s) & 1) * vst);
+    cp_async_commit();
+    cp_async_wait_keep1();  // sweep s's copies have landed
+    __syncthreads();
     const int nt = ts_tasks(n, kTsB, s);
     for (int p = threadIdx.x; p < nt * nc; p += blockDim.x) {
       const int t = p / nc, c = p - t * nc;
       const int R0 = (t == 0) ? s + 1 : s + 1 + t * kTsB;
       const int L = (n - R0 < kTsB) ? n - R0 : kTsB;
-      const double2* v = Vk + ((int64_t)s * tmax + t) * kTsB;
-      const double2 tj = tk[(int64_t)s * tmax + t];
-      double2* z = zs + (int64_t)c * n + R0;
-      double2 vr[kTsB];
-      double2 acc = cmk(0.0, 0.0);
+      const double2* v = buf + t * kTsB;
+      const double2 tj = buf[tmax * kTsB + t];
+      double2* z = zs + (int64_t)c * ld + R0;
+      double2 vr[kTsB], zr[kTsB];
+      double2 acc[4] = {cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0)};
 #pragma unroll
       for (int r = 0; r < kTsB; ++r) {
         vr[r] = v[r];  // zero-padded past L
-        if (r < L) acc = cadd(acc, cmulc(vr[r], z[r]));
+        zr[r] = (r < L) ? z[r] : cmk(0.0, 0.0);
       }
-      const double2 f = cmul(tj, acc);
+#pragma unroll
+      for (int r = 0; r < kTsB; ++r) acc[r & 3] = cadd(acc[r & 3], cmulc(vr[r], zr[r]));
+      const double2 f = cmul(tj, cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
 #pragma unroll
       for (int r = 0; r < kTsB; ++r)
-        if (r < L) z[r] = csub(z[r], cmul(vr[r], f));
+        if (r < L) z[r] = csub(zr[r], cmul(vr[r], f));
     }
-    __syncthreads();
+    __syncthreads();  // the buffer of sweep s is free for sweep s - 2
   }
-  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) Uk[i] = zs[i];
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) {
+    const int r = (int)(i % n), c = (int)(i / n);
+    Uk[i] = zs[r + (int64_t)c * ld];
+  }
 }
 
 }  // namespace lqm

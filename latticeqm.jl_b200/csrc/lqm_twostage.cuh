@@ -9,7 +9,7 @@
 //     reflector j (j < n - b) is A(j+b:, j) with v0 = 1 implicit, A(j+b, j) = beta.
 //   stage 2, band -> real tridiagonal (LAPACK zhetrd_hb2st): bulge chasing.
 //     Sweep s annihilates column s below its subdiagonal; task t of the sweep
-//     (ts_chase_task) makes one reflector from the first column of the block the
+//     (ts_chase_sweep) makes one reflector from the first column of the block the
 //     previous task filled, applies it from the left to the rest of that block,
 //     two-sided to its diagonal block and from the right to the block below,
 //     which becomes the next task's block.  Only the first column of each bulge
@@ -165,103 +165,131 @@ LQM_FN void ts_band_extract(const TeamT& T, int n, const double2* A, int lda, do
   }
 }
 
-// One task (s, t) of the bulge chase on the band Bd (ldb = 2B).  The reflector
-// H = I - tau v v^H (zlarfg: H^H x = beta e1, v0 = 1) is made from
+// One sweep s of the bulge chase on the band Bd (ldb = 2B).  Task t makes the
+// reflector H = I - tau v v^H (zlarfg: H^H x = beta e1, v0 = 1) from
 //   t = 0:  x = column s, rows s+1 .. s+L
 //   t > 0:  x = column c = s+1+(t-1)B, rows R0 .. R0+L-1 (R0 = s+1+tB)
 // with L = min(B, n - R0); then
 //   F <- H^H F   F = rows R0.., columns c+1 .. c+B-1 (t > 0: the rest of the bulge)
 //   D <- H^H D H D = the diagonal block on rows R0 .. R0+L-1
 //   E <- E H     E = rows R0+L .. R0+L+L'-1 (L' = min(B, n-R0-L)), columns of D
-// v (B complex, zero-padded) and tau go to vout / tauout when they are non-null.
-// sv: team scratch of 2B complex + 2 doubles.  The team is one warp on the device.
-template <int B, class TeamT>
-LQM_FN void ts_chase_task(const TeamT& T, int n, int s, int t, double2* Bd, double2* vout, double2* tauout,
-                          double2* sv) {
+// The task's blocks live in the team's window `win` (3 B x (B+1) blocks + 2 B complex):
+// D and E are loaded from the band together (one batch of independent loads), E
+// stays in the window as the next task's x and F (the block it fills is the next
+// task's), and F, x and D go back to the band once they are final.  wait(t) is
+// called before task t's loads (false: give up, the sweep returns false) and done(t)
+// after its stores.  vout / tauout (or null): task t's v (B complex, zero-padded)
+// at vout + t B and tau at tauout[t].  The team is one warp on the device.
+template <int B, class TeamT, class WaitF, class DoneF>
+LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* vout, double2* tauout,
+                           double2* win, WaitF wait, DoneF done) {
   const int ldb = 2 * B;
-  const int R0 = (t == 0) ? s + 1 : s + 1 + t * B;
-  const int c = (t == 0) ? s : s + 1 + (t - 1) * B;
-  const int L = (n - R0 < B) ? n - R0 : B;
-  if (L <= 0) return;
-  double2* v = sv;
-  double2* w = sv + B;
-  // x and zlarfg
-  double s2 = 0.0;
-  for (int r = 1 + T.tid; r < L; r += T.nt) { const double2 x = ts_bget(Bd, ldb, R0 + r, c); s2 += x.x * x.x + x.y * x.y; }
-  s2 = warp_sum_bcast(s2);
-  const double2 alpha = ts_bget(Bd, ldb, R0, c);
-  double2 tj, scal;
-  double beta;
-  zlarfg_scalars(alpha, s2, &tj, &beta, &scal);
-  for (int r = T.tid; r < B; r += T.nt) {
-    double2 vr = cmk(0.0, 0.0);
-    if (r == 0) vr = cmk(1.0, 0.0);
-    else if (r < L) vr = cmul(scal, ts_bget(Bd, ldb, R0 + r, c));
-    v[r] = vr;
-    if (vout) vout[r] = vr;
-  }
-  team_sync(T);
-  for (int r = T.tid; r < L; r += T.nt) *ts_bptr(Bd, ldb, R0 + r, c) = (r == 0) ? cmk(beta, 0.0) : cmk(0.0, 0.0);
-  if (tauout && T.tid == 0) *tauout = tj;
-  const double2 ctj = cconj(tj);
-  // F <- H^H F: column c + 1 + l (l < B - 1) by thread
-  if (t > 0) {
-    for (int l = T.tid; l < B - 1; l += T.nt) {
-      const int cc = c + 1 + l;
-      double2 acc = cmk(0.0, 0.0);
-      for (int r = 0; r < L; ++r) acc = cadd(acc, cmulc(v[r], ts_bget(Bd, ldb, R0 + r, cc)));
-      const double2 f = cmul(ctj, acc);
-      for (int r = 0; r < L; ++r) {
-        double2* p = ts_bptr(Bd, ldb, R0 + r, cc);
-        *p = csub(*p, cmul(v[r], f));
+  constexpr int LW = B + 1;        // window leading dimension (odd: row and column walks conflict-free)
+  double2* EF = win;               // x (column 0) and F (columns 1 .. B-1): [r + l LW]
+  double2* EN = win + B * LW;      // the next task's block E: [i + q LW]
+  double2* D = win + 2 * B * LW;   // the diagonal block, lower triangle: [r + q LW], q <= r
+  double2* v = win + 3 * B * LW;
+  double2* w = v + B;
+  const int nt = ts_tasks(n, B, s);
+  for (int t = 0; t < nt; ++t) {
+    if (!wait(t)) return false;
+    const int R0 = (t == 0) ? s + 1 : s + 1 + t * B;
+    const int c = (t == 0) ? s : s + 1 + (t - 1) * B;
+    const int L = (n - R0 < B) ? n - R0 : B;
+    const int R1 = R0 + L;
+    const int L2 = (n - R1 < B) ? n - R1 : B;
+    // loads: x (t = 0; later tasks find it in the window), D, E
+    if (t == 0)
+      for (int r = T.tid; r < L; r += T.nt) EF[r] = ts_bget(Bd, ldb, R0 + r, s);
+    for (int idx = T.tid; idx < B * B; idx += T.nt) {
+      const int r = idx % B, q = idx / B;
+      if (q <= r && r < L) D[r + q * LW] = ts_bget(Bd, ldb, R0 + r, R0 + q);
+      if (r < L2 && q < L) EN[r + q * LW] = ts_bget(Bd, ldb, R1 + r, R0 + q);
+    }
+    team_sync(T);
+    // zlarfg on x
+    double s2 = 0.0;
+    for (int r = 1 + T.tid; r < L; r += T.nt) { const double2 x = EF[r]; s2 += x.x * x.x + x.y * x.y; }
+    s2 = warp_sum_bcast(s2);
+    const double2 alpha = EF[0];
+    double2 tj, scal;
+    double beta;
+    zlarfg_scalars(alpha, s2, &tj, &beta, &scal);
+    for (int r = T.tid; r < B; r += T.nt) {
+      double2 vr = cmk(0.0, 0.0);
+      if (r == 0) vr = cmk(1.0, 0.0);
+      else if (r < L) vr = cmul(scal, EF[r]);
+      v[r] = vr;
+      if (vout) vout[(int64_t)t * B + r] = vr;
+    }
+    if (tauout && T.tid == 0) tauout[t] = tj;
+    team_sync(T);
+    for (int r = T.tid; r < L; r += T.nt) EF[r] = (r == 0) ? cmk(beta, 0.0) : cmk(0.0, 0.0);
+    const double2 ctj = cconj(tj);
+    // F <- H^H F: column l (1 .. B-1) by thread
+    if (t > 0) {
+      for (int l = 1 + T.tid; l < B; l += T.nt) {
+        double2* f = EF + l * LW;
+        double2 acc = cmk(0.0, 0.0);
+        for (int r = 0; r < L; ++r) acc = cadd(acc, cmulc(v[r], f[r]));
+        const double2 fl = cmul(ctj, acc);
+        for (int r = 0; r < L; ++r) f[r] = csub(f[r], cmul(v[r], fl));
       }
     }
-  }
-  // D <- H^H D H: y = D v (row r by thread), gamma = v^H y, w = tau y - 1/2 |tau|^2 gamma v
-  double2 yr = cmk(0.0, 0.0);
-  double g = 0.0;
-  for (int r = T.tid; r < L; r += T.nt) {
-    double2 acc = cmk(0.0, 0.0);
-    for (int q = 0; q < L; ++q) {
-      const double2 dq = (q <= r) ? ts_bget(Bd, ldb, R0 + r, R0 + q) : cconj(ts_bget(Bd, ldb, R0 + q, R0 + r));
-      acc = cadd(acc, cmul(dq, v[q]));
+    team_sync(T);
+    // x and F are final: back to the band (columns c .. c+B-1, rows R0 ..)
+    const int ncol = (t > 0) ? B : 1;
+    for (int idx = T.tid; idx < B * ncol; idx += T.nt) {
+      const int r = idx % B, l = idx / B;
+      if (r < L) *ts_bptr(Bd, ldb, R0 + r, c + l) = EF[r + l * LW];
     }
-    yr = acc;
-    g += cmulc(v[r], acc).x;
+    // D <- H^H D H: y = D v (row r by thread), gamma = v^H y, w = tau y - 1/2 |tau|^2 gamma v
+    double2 yr = cmk(0.0, 0.0);
+    double g = 0.0;
+    for (int r = T.tid; r < L; r += T.nt) {
+      double2 acc = cmk(0.0, 0.0);
+      for (int q = 0; q < L; ++q) acc = cadd(acc, cmul((q <= r) ? D[r + q * LW] : cconj(D[q + r * LW]), v[q]));
+      yr = acc;
+      g += cmulc(v[r], acc).x;
 #if !defined(__CUDACC__)
-    w[r] = acc;  // one-thread team: y kept in w until gamma is complete
+      w[r] = acc;  // one-thread team: y kept in w until gamma is complete
 #endif
-  }
-  g = warp_sum_bcast(g);
-  const double h = -0.5 * (tj.x * tj.x + tj.y * tj.y) * g;
+    }
+    g = warp_sum_bcast(g);
+    const double h = -0.5 * (tj.x * tj.x + tj.y * tj.y) * g;
 #if defined(__CUDACC__)
-  for (int r = T.tid; r < L; r += T.nt) w[r] = cadd(cmul(tj, yr), cscale(h, v[r]));
+    for (int r = T.tid; r < L; r += T.nt) w[r] = cadd(cmul(tj, yr), cscale(h, v[r]));
 #else
-  for (int r = 0; r < L; ++r) w[r] = cadd(cmul(tj, w[r]), cscale(h, v[r]));
+    for (int r = 0; r < L; ++r) w[r] = cadd(cmul(tj, w[r]), cscale(h, v[r]));
 #endif
-  team_sync(T);  // every thread has read D before it is rewritten
-  for (int r = T.tid; r < L; r += T.nt) {
-    const double2 vr = v[r], wr = w[r];
-    for (int q = 0; q <= r; ++q) {
-      double2* p = ts_bptr(Bd, ldb, R0 + r, R0 + q);
-      double2 a = csub(*p, cadd(cmul(wr, cconj(v[q])), cmul(vr, cconj(w[q]))));
-      if (q == r) a.y = 0.0;
-      *p = a;
+    team_sync(T);  // every thread has read D before it is rewritten
+    for (int r = T.tid; r < L; r += T.nt) {
+      const double2 vr = v[r], wr = w[r];
+      for (int q = 0; q <= r; ++q) {
+        double2 a = csub(D[r + q * LW], cadd(cmul(wr, cconj(v[q])), cmul(vr, cconj(w[q]))));
+        if (q == r) a.y = 0.0;
+        D[r + q * LW] = a;
+      }
     }
-  }
-  // E <- E H: row i by thread, z_i = sum_q E(i, q) v_q, E(i, q) -= tau z_i conj(v_q)
-  const int R1 = R0 + L;
-  const int L2 = (n - R1 < B) ? n - R1 : B;
-  for (int i = T.tid; i < L2; i += T.nt) {
-    double2 acc = cmk(0.0, 0.0);
-    for (int q = 0; q < L; ++q) acc = cadd(acc, cmul(ts_bget(Bd, ldb, R1 + i, R0 + q), v[q]));
-    const double2 z = cmul(tj, acc);
-    for (int q = 0; q < L; ++q) {
-      double2* p = ts_bptr(Bd, ldb, R1 + i, R0 + q);
-      *p = csub(*p, cmul(z, cconj(v[q])));
+    // E <- E H: row i by thread, z_i = sum_q E(i, q) v_q, E(i, q) -= tau z_i conj(v_q)
+    for (int i = T.tid; i < L2; i += T.nt) {
+      double2 acc = cmk(0.0, 0.0);
+      for (int q = 0; q < L; ++q) acc = cadd(acc, cmul(EN[i + q * LW], v[q]));
+      const double2 z = cmul(tj, acc);
+      for (int q = 0; q < L; ++q) EN[i + q * LW] = csub(EN[i + q * LW], cmul(z, cconj(v[q])));
     }
+    team_sync(T);
+    for (int idx = T.tid; idx < B * B; idx += T.nt) {
+      const int r = idx % B, q = idx / B;
+      if (q <= r && r < L) *ts_bptr(Bd, ldb, R0 + r, R0 + q) = D[r + q * LW];
+    }
+    // E becomes the next task's x and F
+    double2* tmp = EF;
+    EF = EN;
+    EN = tmp;
+    done(t);
   }
-  team_sync(T);
+  return true;
 }
 
 // Applies H = I - tau v v^H of every stage-2 task to the rows of Z (n x nc, leading

@@ -253,7 +253,7 @@ extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* block
 
 // The two-stage large-n path on one k-point: stage 1 (ts_panel_qr, the GEMM
 // chain of the trailing update done here as loops), band extraction, the bulge
-// chase (ts_chase_task, sweeps in order), divide and conquer, then U = Q1 Q2 Z
+// chase (ts_chase_sweep, sweeps in order), divide and conquer, then U = Q1 Q2 Z
 // (ts_q2_apply_host, the compact-WY products of blk_larft with the rows offset
 // by the half-bandwidth).
 template <int B>
@@ -314,10 +314,10 @@ static int emul_twostage(int n, int nR, int dim, const double* blocks, const int
   std::vector<double2> Bd((size_t)ldb * n), V2((size_t)std::max(n - 1, 1) * tmax * B), tau2((size_t)std::max(n - 1, 1) * tmax),
       sv(2 * B + 2);
   ts_band_extract<B>(T, n, A.data(), n, Bd.data());
+  std::vector<double2> win(3 * B * (B + 1) + 2 * B);
   for (int s = 0; s <= n - 2; ++s)
-    for (int t = 0; t < ts_tasks(n, B, s); ++t)
-      ts_chase_task<B>(T, n, s, t, Bd.data(), V2.data() + ((size_t)s * tmax + t) * B, tau2.data() + (size_t)s * tmax + t,
-                       sv.data());
+    ts_chase_sweep<B>(T, n, s, Bd.data(), V2.data() + (size_t)s * tmax * B, tau2.data() + (size_t)s * tmax, win.data(),
+                      [](int) { return true; }, [](int) {});
   std::vector<double> d(n), e(n, 0.0);
   double offmax = 0.0;  // entries outside the tridiagonal after the chase (should be zero)
   for (int j = 0; j < n; ++j) {

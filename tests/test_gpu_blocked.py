@@ -197,7 +197,7 @@ def test_tbg_1324_kpath_eigenvalues_only(lqm, ctx, tbg10):
     assert rel_band_err(b, K.bandmatrix(h, ks)[0]) <= BAND_TOL
 
 
-def test_hubbard_scf_on_blocked_path_matches_oracle(lqm, ctx):
+def test_hubbard_scf_on_blocked_path_matches_oracle(lqm, bctx):
     """Hartree-Fock SCF at n = 128 (8x8 spinful triangular Hubbard): the eigen pass takes
     the blocked path, rho_k is formed by batched GEMMs, iterations 2+ replay a captured
     CUDA graph.  Same bounds as the n = 72 SCF test."""
@@ -207,7 +207,7 @@ def test_hubbard_scf_on_blocked_path_matches_oracle(lqm, ctx):
     rho0 = {(0, 0): M.random_local_magnetization(lat.norb, seed=7)}
     ks = L.regulargrid(4 * 4)
     kw = dict(T=0.02, beta=0.3, tol=0.0, iterations=4)
-    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, **kw)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=bctx, **kw)
     rho_ref, E_ref, hf_ref, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, **kw)
     assert res.mf.iterations == it == 4
     assert np.max(np.abs(res.rho[(0, 0)] - rho_ref[(0, 0)])) <= RHO_TOL
@@ -216,7 +216,7 @@ def test_hubbard_scf_on_blocked_path_matches_oracle(lqm, ctx):
     assert abs(res.residual - resid) <= 1e-9
 
 
-def test_screened_coulomb_hf_blocked_path_matches_oracle(lqm, ctx):
+def test_screened_coulomb_hf_blocked_path_matches_oracle(lqm, bctx):
     """Hartree-Fock with the long-range screened Coulomb interaction on the twisted
     bilayer m=3 (n = 148, blocked path): Fock terms on every key of v, rho on the same
     keys.  Same bounds as the other SCF tests."""
@@ -230,7 +230,7 @@ def test_screened_coulomb_hf_blocked_path_matches_oracle(lqm, ctx):
     rho0[(0, 0)] = 0.5 * np.eye(n) + (X + X.T)
     ks = L.regulargrid(4 * 4)
     kw = dict(T=0.05, beta=0.3, tol=0.0, iterations=4)
-    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=ctx, **kw)
+    res = lqm.solvehartreefock(h, v, rho0, 0.5, ks, ctx=bctx, **kw)
     rho_ref, E_ref, hf_ref, conv, resid, it = MF.solvehartreefock(h, v, rho0, 0.5, ks, **kw)
     assert res.mf.iterations == it == 4
     assert max(np.max(np.abs(res.rho[R] - rho_ref[R])) for R in rho0) <= RHO_TOL

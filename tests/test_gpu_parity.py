@@ -127,8 +127,8 @@ def test_stats_modes(lqm):
 
 
 def test_large_n_global_scratch_path(lqm):
-    # n = 148 on the one-CTA kernel (the default context takes the blocked path from
-    # n = 128 on): the Householder matrix lives in global scratch (does not fit shared memory)
+    # n = 148 on the one-CTA kernel (forced, whatever the default switch): the
+    # Householder matrix lives in global scratch (does not fit shared memory)
     ctx = lqm.Context(0, timeout=600)
     ctx.set_blocked_min_n(10 ** 9)
     h = M.graphene(L.honeycomb_twisted(3), tz=0.32)
