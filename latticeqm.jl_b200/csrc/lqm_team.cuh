@@ -191,6 +191,12 @@ LQM_FN double2 cmulc(double2 a, double2 b) { return cmk(a.x * b.x + a.y * b.y, a
 LQM_FN double2 cconj(double2 a) { return cmk(a.x, -a.y); }
 LQM_FN double2 cscale(double s, double2 a) { return cmk(s * a.x, s * a.y); }
 // a / b with Smith's scaling
+#if defined(__CUDACC__)
+// A complex value from lane `src` of the warp (all 32 lanes must call it).
+LQM_FN double2 shfl_c(double2 v, int src) {
+  return cmk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+#endif
 LQM_FN double2 cdiv(double2 a, double2 b) {
   if (fabs(b.x) >= fabs(b.y)) {
     double r = b.y / b.x, den = b.x + b.y * r;

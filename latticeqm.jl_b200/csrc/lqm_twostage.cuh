@@ -226,8 +226,29 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
     team_sync(T);
     for (int r = T.tid; r < L; r += T.nt) EF[r] = (r == 0) ? cmk(beta, 0.0) : cmk(0.0, 0.0);
     const double2 ctj = cconj(tj);
-    // F <- H^H F: column l (1 .. B-1) by thread
+    // F <- H^H F, column l (1 .. B-1).  Device: lanes l and l + 16 take rows 0..7 and
+    // 8..15 of column l, two partial sums each, added across the lane pair.
     if (t > 0) {
+#if defined(__CUDACC__)
+      const int l = T.lane & 15, hh = T.lane >> 4;
+      double2* f = EF + l * LW;
+      double2 a0 = cmk(0.0, 0.0), a1 = cmk(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {
+        const int r0 = 8 * hh + k;
+        if (r0 < L) a0 = cadd(a0, cmulc(v[r0], f[r0]));
+        if (r0 + 1 < L) a1 = cadd(a1, cmulc(v[r0 + 1], f[r0 + 1]));
+      }
+      const double2 pp = cadd(a0, a1);
+      const double2 fl = cmul(ctj, cadd(shfl_c(pp, l), shfl_c(pp, l + 16)));
+      if (l >= 1) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int r = 8 * hh + k;
+          if (r < L) f[r] = csub(f[r], cmul(v[r], fl));
+        }
+      }
+#else
       for (int l = 1 + T.tid; l < B; l += T.nt) {
         double2* f = EF + l * LW;
         double2 acc = cmk(0.0, 0.0);
@@ -235,6 +256,7 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
         const double2 fl = cmul(ctj, acc);
         for (int r = 0; r < L; ++r) f[r] = csub(f[r], cmul(v[r], fl));
       }
+#endif
     }
     team_sync(T);
     // x and F are final: back to the band (columns c .. c+B-1, rows R0 ..)
@@ -243,7 +265,55 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
       const int r = idx % B, l = idx / B;
       if (r < L) *ts_bptr(Bd, ldb, R0 + r, c + l) = EF[r + l * LW];
     }
-    // D <- H^H D H: y = D v (row r by thread), gamma = v^H y, w = tau y - 1/2 |tau|^2 gamma v
+    // D <- H^H D H: y = D v, gamma = v^H y, w = tau y - 1/2 |tau|^2 gamma v; then
+    // E <- E H: z_i = sum_q E(i, q) v_q, E(i, q) -= tau z_i conj(v_q).  Device: lanes
+    // r and r + 16 take columns 0..7 and 8..15 of row r, two partial sums each.
+#if defined(__CUDACC__)
+    {
+      const int r = T.lane & 15, hh = T.lane >> 4;
+      double2 a0 = cmk(0.0, 0.0), a1 = cmk(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {
+        const int q0 = 8 * hh + k, q1 = q0 + 1;
+        if (r < L && q0 < L) a0 = cadd(a0, cmul((q0 <= r) ? D[r + q0 * LW] : cconj(D[q0 + r * LW]), v[q0]));
+        if (r < L && q1 < L) a1 = cadd(a1, cmul((q1 <= r) ? D[r + q1 * LW] : cconj(D[q1 + r * LW]), v[q1]));
+      }
+      const double2 pp = cadd(a0, a1);
+      const double2 yr = cadd(shfl_c(pp, r), shfl_c(pp, r + 16));
+      const double g = warp_sum_bcast((hh == 0 && r < L) ? cmulc(v[r], yr).x : 0.0);
+      const double h = -0.5 * (tj.x * tj.x + tj.y * tj.y) * g;
+      if (hh == 0 && r < L) w[r] = cadd(cmul(tj, yr), cscale(h, v[r]));
+      team_sync(T);  // w complete; every lane has read D
+      if (r < L) {
+        const double2 vr = v[r], wr = w[r];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int q = 8 * hh + k;
+          if (q <= r) {
+            double2 a = csub(D[r + q * LW], cadd(cmul(wr, cconj(v[q])), cmul(vr, cconj(w[q]))));
+            if (q == r) a.y = 0.0;
+            D[r + q * LW] = a;
+          }
+        }
+      }
+      double2 e0 = cmk(0.0, 0.0), e1 = cmk(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {
+        const int q0 = 8 * hh + k, q1 = q0 + 1;
+        if (r < L2 && q0 < L) e0 = cadd(e0, cmul(EN[r + q0 * LW], v[q0]));
+        if (r < L2 && q1 < L) e1 = cadd(e1, cmul(EN[r + q1 * LW], v[q1]));
+      }
+      const double2 pe = cadd(e0, e1);
+      const double2 z = cmul(tj, cadd(shfl_c(pe, r), shfl_c(pe, r + 16)));
+      if (r < L2) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int q = 8 * hh + k;
+          if (q < L) EN[r + q * LW] = csub(EN[r + q * LW], cmul(z, cconj(v[q])));
+        }
+      }
+    }
+#else
     double2 yr = cmk(0.0, 0.0);
     double g = 0.0;
     for (int r = T.tid; r < L; r += T.nt) {
@@ -278,6 +348,7 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
       const double2 z = cmul(tj, acc);
       for (int q = 0; q < L; ++q) EN[i + q * LW] = csub(EN[i + q * LW], cmul(z, cconj(v[q])));
     }
+#endif
     team_sync(T);
     for (int idx = T.tid; idx < B * B; idx += T.nt) {
       const int r = idx % B, q = idx / B;
