@@ -720,7 +720,7 @@ constexpr int kTsPanelThreads = 512;  // panel QR: latency-bound row passes, CTA
 constexpr int kTsChaseWarps = 8;      // bulge chase: sweeps in flight per k-point (one warp each)
 constexpr int kTsQ2Threads = 256;
 constexpr int kTsQ2MaxCols = 8;       // columns of Z per CTA in the Q2 back-transformation
-constexpr int kTsWaitPolls = 1 << 22; // bound of one inter-warp wait of the chase (polls of ~0.1 us)
+constexpr int kTsWaitPolls = 1 << 26; // bound of one inter-warp wait of the chase (shared-memory polls, ~1 s)
 
 // complex per k-point of the stage-2 reflector store (sweeps 0..n-2, tmax slots of kTsB each)
 __host__ __device__ inline int64_t ts_v2_stride(int n) {
@@ -793,7 +793,6 @@ __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, dou
             good = false;
             break;
           }
-          __nanosleep(64);
         }
       }
       good = __shfl_sync(0xffffffffu, good, 0);
