@@ -381,15 +381,36 @@ void zgemm_sb(lqm_ctx* ctx, GemmOp ta, GemmOp tb, int m, int n, int k, double al
     nsplit = (k + kc - 1) / kc;
     double2* P = (double2*)ws_get(ctx, WS_GEMMSPLIT, (size_t)nsplit * m * n * sizeof(double2));
     GemmArgs gs = g;
-    gs.beta = 0.0; gs.C = P; gs.ldc = m; gs.sC = (long long)m * n; gs.split = 1; gs.k = kc; gs.ktot = k;
+    gs.beta = 0.0; gs.C = P; gs.ldc = m; gs.sC = (long long)m * n; gs.split = nsplit; gs.k = kc; gs.ktot = k;
     launch_zgemm_dmma<128, 16, 32, 16, 8, 3>(h, gs, nsplit);
     const int64_t mn = (int64_t)m * n;
     zgemm_split_reduce_kernel<<<(unsigned)std::min<int64_t>((mn + 255) / 256, 8 * ctx->num_sms), 256, 0, h>>>(
-        m, n, nsplit, P, beta_re, C, ldc);
+        m, n, nsplit, P, beta_re, C, ldc, 0, 1);
     ck(cudaGetLastError(), "zgemm split launch");
     return;
   }
-  if (n <= 16)
+  // batched products with a tiny output and a long k (V^H X of the two-stage panels):
+  // k in chunks of 128 on 16 x 16 tiles of one warp, then the ordered sum per entry
+  if (m <= 16 && n <= 16 && k >= 512 && ta != OP_HL) {
+    const int kc = 128;
+    const int nsplit = std::min((k + kc - 1) / kc, 65535 / batch);
+    if (nsplit >= 2) {
+      const int kcs = (k + nsplit - 1) / nsplit;
+      const int ns = (k + kcs - 1) / kcs;
+      double2* P = (double2*)ws_get(ctx, WS_GEMMSPLIT, (size_t)batch * ns * m * n * sizeof(double2));
+      GemmArgs gs = g;
+      gs.beta = 0.0; gs.C = P; gs.ldc = m; gs.sC = (long long)m * n; gs.split = ns; gs.k = kcs; gs.ktot = k;
+      launch_zgemm_dmma<16, 16, 16, 16, 8, 3>(h, gs, batch * ns);
+      const int64_t tot = (int64_t)m * n * batch;
+      zgemm_split_reduce_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 8 * ctx->num_sms), 256, 0, h>>>(
+          m, n, ns, P, beta_re, C, ldc, sC, batch);
+      ck(cudaGetLastError(), "zgemm split launch");
+      return;
+    }
+  }
+  if (n <= 16 && m >= 512)
+    launch_zgemm_dmma<128, 16, 16, 16, 8, 3>(h, g, batch);  // eight warps per tile: tall skinny products
+  else if (n <= 16)
     launch_zgemm_dmma<128, 16, 32, 16, 8, 3>(h, g, batch);
   else if (m <= 32)
     launch_zgemm_dmma<32, 64, 32, 16, 8, 3>(h, g, batch);

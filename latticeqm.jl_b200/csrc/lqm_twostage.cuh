@@ -387,3 +387,37 @@ LQM_FN void ts_q2_apply_host(int n, const double2* V2, const double2* tau2, doub
     }
   }
 }
+
+// Q2 Z in the grouped order of the device kernel (ts_q2g_kernel): the sweeps in
+// groups of B, the highest group first; within a group the task index t ascending,
+// and for each t the group's reflectors of task t from the highest sweep down.  Two
+// reflectors overlap only when they are of the same t, or of tasks t and t - 1 of
+// sweeps less than 2B apart; this order applies every later-generated overlapping
+// reflector first, as the reverse sweep order does, so the product is the same.  The
+// reflectors of one (group, t) step act on a window of 2B - 1 rows that slides by B
+// rows per step.
+template <int B>
+LQM_FN void ts_q2_apply_grouped_host(int n, const double2* V2, const double2* tau2, double2* Z, int ldz, int nc) {
+  const int tmax = ts_tmax(n, B);
+  const int ns = n - 1;  // sweeps 0 .. n-2
+  if (ns <= 0) return;
+  for (int s0 = ((ns - 1) / B) * B; s0 >= 0; s0 -= B) {
+    const int nt = ts_tasks(n, B, s0);
+    for (int t = 0; t < nt; ++t)
+      for (int i = B - 1; i >= 0; --i) {
+        const int s = s0 + i;
+        if (s >= ns || t >= ts_tasks(n, B, s)) continue;
+        const int R0 = s + 1 + t * B;
+        const int L = (n - R0 < B) ? n - R0 : B;
+        const double2* v = V2 + ((int64_t)s * tmax + t) * B;
+        const double2 tj = tau2[(int64_t)s * tmax + t];
+        for (int c = 0; c < nc; ++c) {
+          double2* z = Z + (int64_t)c * ldz + R0;
+          double2 acc = cmk(0.0, 0.0);
+          for (int r = 0; r < L; ++r) acc = cadd(acc, cmulc(v[r], z[r]));
+          const double2 f = cmul(tj, acc);
+          for (int r = 0; r < L; ++r) z[r] = csub(z[r], cmul(v[r], f));
+        }
+      }
+  }
+}

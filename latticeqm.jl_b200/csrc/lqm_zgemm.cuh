@@ -56,8 +56,9 @@ struct GemmArgs {
   int ldc;
   long long sC;
   int opA, opB;
-  // split-K (batch 1): blockIdx.z is the k-chunk, chunk z covers [z k, z k + k) of
-  // ktot and writes its own C_z = C + z sC with beta = 0; 0 = plain batched product
+  // split-K: split > 0 chunks per batch entry; blockIdx.z = entry * split + chunk,
+  // chunk covers [chunk k, chunk k + k) of ktot and writes its own C_z = C + z sC
+  // with beta = 0; 0 = plain batched product
   int split, ktot;
   // optional second operand pair summed after the first (k2 > 0, same ops):
   //   C = alpha (op(A) op(B) + op(A2) op(B2)) + beta C,  the k-sum of A2 B2 after A B
@@ -104,7 +105,9 @@ __device__ __forceinline__ void gemm_stage(const GemmArgs& g, const double2* A, 
 // grid (ceil(m / BM), ceil(n / BN), batch); block (BM / WM) * (BN / WN) warps; K in
 // slices of BK through an ST-deep ring.
 template <int BM, int BN, int WM, int WN, int BK, int ST>
-__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(GemmArgs g) {
+// eight-warp tiles keep two CTAs per SM (at most 128 registers per thread)
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32, (BM / WM) * (BN / WN) >= 8 ? 2 : 1)
+    zgemm_dmma_kernel(GemmArgs g) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr int MI = WM / 8, NJ = WN / 8;
   constexpr int P = gemm_pitch(BK);
@@ -121,9 +124,10 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
   double2* C = g.C + b * g.sC;
   int kend = g.k;  // k bound of this block's slice, relative to A and B
   if (g.split) {
-    const int64_t kb = b * (int64_t)g.k;  // first k of the chunk
-    A += (g.opA == OP_N) ? kb * g.lda : kb;
-    B += (g.opB == OP_N) ? kb : kb * g.ldb;
+    const int64_t e = b / g.split;                    // batch entry
+    const int64_t kb = (b - e * g.split) * (int64_t)g.k;  // first k of the chunk
+    A += e * g.sA + ((g.opA == OP_N) ? kb * g.lda : kb);
+    B += e * g.sB + ((g.opB == OP_N) ? kb : kb * g.ldb);
     kend = (int)(g.ktot - kb < g.k ? g.ktot - kb : g.k);
   } else {
     A += b * g.sA;
@@ -254,16 +258,20 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32) zgemm_dmma_kernel(
   }
 }
 
-// Split-K finish: C = sum_z P_z + beta C in chunk order (P_z = C_z of the chunks,
-// m x n each, leading dimension m).
+// Split-K finish: C_e = sum_z P_(e, z) + beta C_e in chunk order (P_(e, z) = C_z of
+// entry e's chunks, m x n each, leading dimension m), for every batch entry e.
 __global__ void __launch_bounds__(256) zgemm_split_reduce_kernel(int m, int n, int nsplit, const double2* P,
-                                                                 double beta, double2* C, int ldc) {
+                                                                 double beta, double2* C, int ldc, long long sC,
+                                                                 int batch) {
   const int64_t mn = (int64_t)m * n;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < mn; t += (int64_t)gridDim.x * blockDim.x) {
-    double2 acc = P[t];
-    for (int z = 1; z < nsplit; ++z) acc = cadd(acc, P[z * mn + t]);
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < mn * batch;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = u / mn, t = u - e * mn;
+    const double2* Pe = P + e * nsplit * mn;
+    double2 acc = Pe[t];
+    for (int z = 1; z < nsplit; ++z) acc = cadd(acc, Pe[z * mn + t]);
     const int64_t i = t % m, j = t / m;
-    double2* c = C + i + j * (int64_t)ldc;
+    double2* c = C + e * sC + i + j * (int64_t)ldc;
     if (beta != 0.0) {
       const double2 o = *c;
       acc.x += beta * o.x;

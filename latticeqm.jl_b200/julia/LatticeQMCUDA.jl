@@ -320,6 +320,12 @@ function cuda_autotune_eigh(H, ks::AbstractMatrix{Float64}, exec::CudaExec; want
     Int(best[]), bms[], Dict(Int(cnt[i]) => cms[i] for i in 1:nc[])
 end
 
+"""Reduction of the blocked eigensolver: 1 two-stage (dense -> band -> tridiagonal),
+0 one-stage panels, -1 the default (two-stage for passes without eigenvectors)."""
+cuda_set_two_stage(mode::Int, exec::CudaExec) =
+    check(context(exec.device), ccall((:lqm_ctx_set_two_stage, LIB[]), Cint, (Ptr{Cvoid}, Cint),
+                                      context(exec.device).ptr, mode))
+
 """Set the one-CTA eigensolver's block size for order n (0: the built-in rule)."""
 cuda_set_eigh_threads(n::Int, nt::Int, exec::CudaExec) =
     check(context(exec.device), ccall((:lqm_ctx_set_eigh_threads, LIB[]), Cint, (Ptr{Cvoid}, Int64, Cint),

@@ -258,7 +258,7 @@ extern "C" int lqm_emul_eigh_blocked(int n, int nR, int dim, const double* block
 // by the half-bandwidth).
 template <int B>
 static int emul_twostage(int n, int nR, int dim, const double* blocks, const int64_t* keys, const double* kpt,
-                         int want_vectors, double* evals, double* U, double* tri) {
+                         int want_vectors, double* evals, double* U, double* tri, bool q2_grouped) {
   const Team T = make_host_team();
   const size_t nn = (size_t)n * n;
   std::vector<double2> A(nn), ph(nR + 1), tau(n + 1), Vb(nn + 1), Tm(B * B), sm((T.nw + 2) * B + B * B + 8);
@@ -352,7 +352,10 @@ static int emul_twostage(int n, int nR, int dim, const double* blocks, const int
   if (!want_vectors) return 0;
   double2* Uc = (double2*)U;
   for (size_t i = 0; i < nn; ++i) Uc[i] = cmk(Q[i], 0.0);
-  ts_q2_apply_host<B>(n, V2.data(), tau2.data(), Uc, n, n);
+  if (q2_grouped)
+    ts_q2_apply_grouped_host<B>(n, V2.data(), tau2.data(), Uc, n, n);
+  else
+    ts_q2_apply_host<B>(n, V2.data(), tau2.data(), Uc, n, n);
   const int NR = n - B;
   blk_prep_reflectors(T, n, A.data(), n, B);
   const int nb = 2 * B;  // back-transformation panels of two stage-1 panels
@@ -387,13 +390,16 @@ static int emul_twostage(int n, int nR, int dim, const double* blocks, const int
   return 0;
 }
 
-// b: the half-bandwidth (4 or 16); tri (or null): d, e and the largest entry
+// b: the half-bandwidth (4 or 16; negative: the grouped Q2 order); tri (or null): d, e and the largest entry
 // left outside the tridiagonal (3n doubles... 2n + 1 used).
 extern "C" int lqm_emul_eigh_twostage(int n, int nR, int dim, const double* blocks, const int64_t* keys,
                                       const double* kpt, int b, int want_vectors, double* evals, double* U,
                                       double* tri) {
-  if (b == 4) return emul_twostage<4>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri);
-  if (b == 16) return emul_twostage<16>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri);
+  // b < 0: the Q2 back-transformation in the grouped order of the device kernel
+  const bool grouped = b < 0;
+  if (grouped) b = -b;
+  if (b == 4) return emul_twostage<4>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri, grouped);
+  if (b == 16) return emul_twostage<16>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri, grouped);
   return -1;
 }
 

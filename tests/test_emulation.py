@@ -281,12 +281,13 @@ def _run_two_stage(emul, h, k, b, want_vectors=True):
     return ev, U, tri
 
 
-@pytest.mark.parametrize("b", [4, 16])
+@pytest.mark.parametrize("b", [4, 16, -4, -16])
 @pytest.mark.parametrize("name,h", models(), ids=lambda x: x if isinstance(x, str) else "")
 def test_emulated_two_stage_eigh_matches_oracle(emul, name, h, b):
-    """The two-stage reduction (panel QRs below a band of half-bandwidth b with the
+    """The two-stage reduction (panel QRs below a band of half-bandwidth |b| with the
     GEMM-form trailing update, the bulge chase to a real tridiagonal), divide and
-    conquer, and the two-level back-transformation U = Q1 Q2 Z."""
+    conquer, and the two-level back-transformation U = Q1 Q2 Z (b < 0: Q2 applied in
+    the grouped order of the device kernel)."""
     for k in [(0.0, 0.0), (0.123, 0.77)]:
         ev, U, tri = _run_two_stage(emul, h, k, b)
         ev_only, _, _ = _run_two_stage(emul, h, k, b, want_vectors=False)
@@ -308,7 +309,7 @@ def test_emulated_two_stage_hard_hermitian(emul, name, Hk):
     n = Hk.shape[0]
     ref = K.eigh_upper(Hk, vectors=False)
     scale = max(np.max(np.abs(ref)), np.finfo(float).tiny)
-    for b in (4, 16):
+    for b in (4, 16, -16):
         ev, U, _ = _run_two_stage(emul, {(0, 0): Hk}, (0.0, 0.0), b)
         assert np.all(np.isfinite(U)), b
         assert np.max(np.abs(ev - ref)) <= 1e-12 * scale, b
