@@ -668,14 +668,10 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       }
     }
     if (K > 0 && ts) {
-      // Z <- Q2 Z on the K columns: the stage-2 reflectors, sweeps in reverse order
-      int cols = kTsQ2MaxCols;
-      while (cols > 1 && ts_q2_smem(n, cols) > 220 * 1024) --cols;
-      const int qsm = ts_q2_smem(n, cols);
-      if (qsm > 227 * 1024) fail(LQM_EINVAL, "n=%d exceeds the stage-2 back-transformation's shared-memory plan", n);
-      ck(cudaFuncSetAttribute(ts_q2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, qsm), "smem attr");
-      ts_q2_kernel<<<dim3((unsigned)((K + cols - 1) / cols), (unsigned)nbk), kTsQ2Threads, qsm, ctx->stream>>>(
-          n, c0, K, cols, V2, tau2, Ucur);
+      // Z <- Q2 Z on the K columns: the stage-2 reflectors in groups of 16 sweeps,
+      // a register window of each column per thread
+      ts_q2g_kernel<<<dim3((unsigned)((K + kTsQ2gThreads - 1) / kTsQ2gThreads), (unsigned)nbk), kTsQ2gThreads, 0,
+                      ctx->stream>>>(n, c0, K, V2, tau2, Ucur);
       ctx->launches++;
     }
     if (K > 0) {

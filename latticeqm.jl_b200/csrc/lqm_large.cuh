@@ -895,4 +895,86 @@ __global__ void __launch_bounds__(kTsQ2Threads) ts_q2_kernel(int n, int c0, int 
   }
 }
 
+// Q2 Z in the grouped order (ts_q2_apply_grouped_host): grid (ceil(K / 256), B),
+// thread = one of the columns c0 .. c0+K-1 of U (n x n per k-point, in place).
+// Each (group of 16 sweeps, task t) step applies 16 reflectors to a window of 31
+// rows of the thread's column, held in registers (all indices compile-time); the
+// window slides by 16 rows per step, so a group streams the column once.  The
+// step's reflectors and taus (16 x 16 + 16 complex; zeros where a sweep has no
+// task t) are copied into shared memory by cp.async one step ahead.
+constexpr int kTsQ2gThreads = 256;
+constexpr int kTsQ2gStep = kTsB * kTsB + kTsB;  // complex per staged step
+__global__ void __launch_bounds__(kTsQ2gThreads, 1) ts_q2g_kernel(int n, int c0, int K, const double2* V2,
+                                                                  const double2* tau2, double2* U) {
+  constexpr int B = kTsB, W = 2 * kTsB - 1;
+  __shared__ __align__(16) double2 sv[2][kTsQ2gStep];
+  const int64_t b = blockIdx.y;
+  const int col = blockIdx.x * kTsQ2gThreads + threadIdx.x;
+  const bool act = col < K;
+  double2* Uc = U + b * (int64_t)n * n + (int64_t)(c0 + (act ? col : 0)) * n;
+  const double2* Vk = V2 + b * ts_v2_stride(n);
+  const double2* tk = tau2 + b * ts_tau2_stride(n);
+  const int tmax = ts_tmax(n, B);
+  const int ns = n - 1;
+  if (ns <= 0) return;
+  const int g0 = (ns - 1) / B;  // highest group
+  // step (g, t) -> shared buffer: reflector i of the step = sweep g B + i, task t
+  auto stage = [&](int g, int t, double2* dst) {
+    for (int e = threadIdx.x; e < kTsQ2gStep; e += blockDim.x) {
+      const int i = (e < B * B) ? e / B : e - B * B;
+      const int s = g * B + i;
+      const bool ok = s < ns && t < ts_tasks(n, B, s);
+      const double2* src = (e < B * B) ? Vk + ((int64_t)s * tmax + t) * B + (e - i * B) : tk + (int64_t)s * tmax + t;
+      cp_async16(dst + e, ok ? (const void*)src : (const void*)Vk, ok);
+    }
+  };
+  int buf = 0;
+  stage(g0, 0, sv[0]);
+  cp_async_commit();
+  for (int g = g0; g >= 0; --g) {
+    const int s0 = g * B;
+    const int nt = ts_tasks(n, B, s0);
+    double2 z[W];
+    const int w0 = s0 + 1;
+#pragma unroll
+    for (int j = 0; j < W; ++j) z[j] = (act && w0 + j < n) ? Uc[w0 + j] : cmk(0.0, 0.0);
+    for (int t = 0; t < nt; ++t) {
+      // next step: (g, t + 1), or the next group's first
+      if (t + 1 < nt) stage(g, t + 1, sv[buf ^ 1]);
+      else if (g > 0) stage(g - 1, 0, sv[buf ^ 1]);
+      cp_async_commit();
+      cp_async_wait_keep1();
+      __syncthreads();
+      const double2* vs = sv[buf];
+#pragma unroll
+      for (int i = B - 1; i >= 0; --i) {
+        const double2 tj = vs[B * B + i];
+        double2 a[4] = {cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0)};
+#pragma unroll
+        for (int r = 0; r < B; ++r) a[r & 3] = cadd(a[r & 3], cmulc(vs[i * B + r], z[i + r]));
+        const double2 f = cmul(tj, cadd(cadd(a[0], a[1]), cadd(a[2], a[3])));
+#pragma unroll
+        for (int r = 0; r < B; ++r) z[i + r] = csub(z[i + r], cmul(vs[i * B + r], f));
+      }
+      __syncthreads();  // the buffer is refilled two steps on
+      buf ^= 1;
+      const int wt = w0 + t * B;  // first row of this step's window
+      if (t + 1 < nt) {
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (act && wt + j < n) Uc[wt + j] = z[j];
+#pragma unroll
+        for (int j = 0; j < W - B; ++j) z[j] = z[j + B];
+#pragma unroll
+        for (int j = W - B; j < W; ++j) z[j] = (act && wt + B + j < n) ? Uc[wt + B + j] : cmk(0.0, 0.0);
+      } else {
+#pragma unroll
+        for (int j = 0; j < W; ++j)
+          if (act && wt + j < n) Uc[wt + j] = z[j];
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 }  // namespace lqm
