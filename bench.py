@@ -600,6 +600,7 @@ def main():
     clocks = sampler.stop()
     eigh_ms, eigh_launches, launches = ctx.stats()
     symv_ms, symv_launches, symv_bytes = ctx.kernel_stats(1)
+    q2_ms, q2_launches, q2_flops = ctx.kernel_stats(2)
     if world > 1:
         t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -640,30 +641,64 @@ def main():
         e2e_el = float(t[0])
     e2e_val = nk * e2e_steps / e2e_el
 
-    # ---- roofline of the dominant kernel: the blocked path's lower-triangle mat-vec ----
-    peak, peak_src = hbm_peak()
-    achieved = symv_bytes / (symv_ms / 1e3) / 1e9 if symv_ms > 0 else None
-    per_launch = symv_bytes / symv_launches if symv_launches else None
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "blk_symv_traffic.json")
-    if per_launch and os.path.exists(tfile):
-        try:
-            traffic = json.load(open(tfile))["dram_bytes_per_algorithmic_byte"] * per_launch
-        except Exception:
-            traffic = None
+    # ---- roofline of the dominant kernel ----
+    # two-stage reduction (the default on the blocked path): the stage-2
+    # back-transformation, FP64-bound, against the FP64 GEMM rate measured in this run;
+    # one-stage (LQM_TWO_STAGE=0): the lower-triangle mat-vec, HBM-bound
     fl = flops_per_k(n, nR, nR)
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-            "kernel": "blk_symv_tma_kernel (Householder mat-vec y = A22 v over the lower triangle of the trailing "
-                      "block, 64x64 tiles moved by TMA, all k-points of the batch per launch; one launch per column)",
-            "algorithmic_bytes_per_launch": per_launch,
-            "algorithmic_bytes_per_k": "16 B x m(m+1)/2 per column, m = n-1-j (sum ~ 16 n^3/6 = 6.2 GB at n=1324)",
-            "launches": symv_launches, "kernel_ms": symv_ms, "share_of_step": symv_ms / 1e3 / elapsed,
-            "peak_source": peak_src,
-            "traffic_source": "ncu dram bytes / algorithmic bytes of one capture (profiles/blk_symv_traffic.json) "
-                              "x this run's algorithmic bytes per launch",
-            "pass_tflops": value / world * fl / 1e12, "pass_flops_per_k": fl,
-            "eigh_pass_ms": eigh_ms, "eigh_passes": eigh_launches}
+    fp64_peak = measured_fp64_peak(torch, dev)
+    if q2_launches:
+        achieved = q2_flops / (q2_ms / 1e3) / 1e12 if q2_ms > 0 else None
+        per_launch = q2_flops / q2_launches
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "q2g_traffic.json")
+        if os.path.exists(tfile):
+            try:
+                traffic = json.load(open(tfile))["dram_bytes_per_algorithmic_flop"] * per_launch
+            except Exception:
+                traffic = None
+        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
+                "kernel": "ts_q2g_kernel (two-stage reduction: the bulge-chasing reflectors applied to the needed "
+                          "eigenvector columns in groups of 16 sweeps, a 31-row register window per column; "
+                          "one launch per batch)",
+                "algorithmic_flops_per_launch": per_launch,
+                "algorithmic_flops_per_k": "8 n (n-1) per eigenvector column formed (each reflector row: dot and "
+                                           "update, 8 real flops each; the columns that carry rho_k)",
+                "launches": q2_launches, "kernel_ms": q2_ms, "share_of_step": q2_ms / 1e3 / elapsed,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; MEASURED_PEAKS.json has no FP64 "
+                               "figure); the kernel runs on the FP64 FMA pipe, whose rate matches the FP64 tensor "
+                               "rate on B200",
+                "traffic_source": "ncu dram bytes / algorithmic flops of one capture (profiles/q2g_traffic.json) "
+                                  "x this run's algorithmic flops per launch",
+                "pass_tflops": value / world * fl / 1e12, "pass_flops_per_k": fl,
+                "eigh_pass_ms": eigh_ms, "eigh_passes": eigh_launches}
+    else:
+        peak, peak_src = hbm_peak()
+        achieved = symv_bytes / (symv_ms / 1e3) / 1e9 if symv_ms > 0 else None
+        per_launch = symv_bytes / symv_launches if symv_launches else None
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "blk_symv_traffic.json")
+        if per_launch and os.path.exists(tfile):
+            try:
+                traffic = json.load(open(tfile))["dram_bytes_per_algorithmic_byte"] * per_launch
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": "blk_symv_tma_kernel (Householder mat-vec y = A22 v over the lower triangle of the "
+                          "trailing block, 64x64 tiles moved by TMA, all k-points of the batch per launch; one "
+                          "launch per column)",
+                "algorithmic_bytes_per_launch": per_launch,
+                "algorithmic_bytes_per_k": "16 B x m(m+1)/2 per column, m = n-1-j (sum ~ 16 n^3/6 = 6.2 GB at n=1324)",
+                "launches": symv_launches, "kernel_ms": symv_ms, "share_of_step": symv_ms / 1e3 / elapsed,
+                "peak_source": peak_src,
+                "traffic_source": "ncu dram bytes / algorithmic bytes of one capture (profiles/blk_symv_traffic.json) "
+                                  "x this run's algorithmic bytes per launch",
+                "pass_tflops": value / world * fl / 1e12, "pass_flops_per_k": fl,
+                "eigh_pass_ms": eigh_ms, "eigh_passes": eigh_launches}
+    roof["fp64_dgemm_tflops_measured"] = fp64_peak
+    roof["pass_frac_of_fp64"] = roof["pass_tflops"] / fp64_peak
 
     threads = cpu_threads()
     cpu = None
@@ -673,9 +708,6 @@ def main():
     configs = None
     scf = None
     if rank == 0 and world == 1 and not args.no_configs:
-        fp64_peak = measured_fp64_peak(torch, dev)
-        roof["fp64_dgemm_tflops_measured"] = fp64_peak
-        roof["pass_frac_of_fp64"] = roof["pass_tflops"] / fp64_peak
         Hd.free()
         del d_rho
         torch.cuda.empty_cache()

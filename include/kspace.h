@@ -70,7 +70,11 @@ int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
  * back-transformation), 0 the one-stage panel reduction (LAPACK zhetrd/zlatrd
  * form, one Hermitian mat-vec per column), -1 (default) by order.  Replaces no
  * reference call: the reference's LAPACK zheevr (src/modules/Eigen/Eigen.jl:22-23)
- * reduces in one stage; zheevr_2stage is LAPACK's two-stage form of the same solve. */
+ * reduces in one stage; zheevr_2stage is LAPACK's two-stage form of the same solve.
+ * By default the blocked path (n >= 224) takes the two-stage form for passes that
+ * return no eigenvectors (bands; rho, which forms only the columns it needs): on
+ * B200 1.8x faster for eigenvalue-only passes at n = 1324 and not slower for rho;
+ * passes that return all eigenvectors keep the one-stage form. */
 int lqm_ctx_set_two_stage(lqm_ctx* ctx, int mode);
 /* SCF acceleration of lqm_scf_hf on this context: 0 (default) linear damped
  * mixing, 1..8 Anderson (Type-II) acceleration with that history depth
@@ -126,9 +130,12 @@ int lqm_ctx_last_kernel_ms(const lqm_ctx* ctx, double* ms);
 int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing);
 int lqm_ctx_stats(const lqm_ctx* ctx, double* eigh_ms, int64_t* eigh_launches, int64_t* launches);
 /* The same statistics per kernel class: 0 = the eigensolver passes (as above),
- * 1 = the blocked path's lower-triangle mat-vec (blk_symv_pipe_kernel), each
- * launch timed with CUDA events, with its algorithmic bytes (the lower triangle
- * of the trailing block read once per column and k-point, 16 B per element).
+ * 1 = the one-stage blocked reduction's lower-triangle mat-vec, each launch timed
+ * with CUDA events, with its algorithmic bytes (the lower triangle of the trailing
+ * block read once per column and k-point, 16 B per element); 2 = the two-stage
+ * path's stage-2 back-transformation (applying the bulge-chasing reflectors to the
+ * needed eigenvector columns), timed the same way, with its algorithmic flops in
+ * the last argument (8 n (n-1) per column and k-point).
  * No reference counterpart (profiling). */
 int lqm_ctx_kernel_stats(const lqm_ctx* ctx, int kernel_class, double* ms, int64_t* launches,
                          double* algorithmic_bytes);

@@ -69,6 +69,10 @@ struct lqm_ctx {
   // the blocked path's mat-vec kernel (the dominant kernel of a large-n pass), timed per launch
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> symv_pending;
   double symv_ms = 0.0, symv_bytes = 0.0;
+  // the two-stage path's stage-2 back-transformation (its dominant kernel with vectors), timed per launch
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> q2_pending;
+  double q2_ms = 0.0, q2_flops = 0.0;
+  int64_t q2_launches = 0;
   int64_t symv_launches = 0;
   unsigned long long* d_phase = nullptr;  // per-phase cycle counters (profiling)
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
@@ -170,6 +174,12 @@ void collect_stats(lqm_ctx* ctx) {
     ctx->ev_pool.push_back(pr);
   }
   ctx->symv_pending.clear();
+  for (auto& pr : ctx->q2_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) ctx->q2_ms += ms;
+    ctx->ev_pool.push_back(pr);
+  }
+  ctx->q2_pending.clear();
 }
 
 void wait_stream(lqm_ctx* ctx) {
@@ -438,7 +448,7 @@ void zher2k_lower(lqm_ctx* ctx, int m, int k, const double2* X, int ldx, long lo
 
 struct RhoOut;
 bool use_blocked(const lqm_ctx* ctx, int n, int nR);
-bool use_two_stage(const lqm_ctx* ctx, int n, bool vec);
+bool use_two_stage(const lqm_ctx* ctx, int n, bool all_vectors);
 
 // Eigen pass of the blocked path: same outputs as launch_eigh.  Reduction by
 // zlatrd panels (column kernels + batched rank-2nb updates), divide and
@@ -488,7 +498,7 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
   const bool vec = d_U || rhok;
   // two-stage: dense -> band (kTsB) -> tridiagonal; reflector j of the first stage
   // starts at row j + off, n - off of them
-  const bool ts = use_two_stage(ctx, n, vec);
+  const bool ts = use_two_stage(ctx, n, d_U != nullptr);
   const int off = ts ? kTsB : 1;
   const int NR = n - off;
   const int64_t nn = (int64_t)n * n;
@@ -670,9 +680,19 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
     if (K > 0 && ts) {
       // Z <- Q2 Z on the K columns: the stage-2 reflectors in groups of 16 sweeps,
       // a register window of each column per thread
+      std::pair<cudaEvent_t, cudaEvent_t> qev{};
+      if (ctx->stats_on) { qev = stat_events(ctx); ck(cudaEventRecord(qev.first, ctx->stream), "event"); }
       ts_q2g_kernel<<<dim3((unsigned)((K + kTsQ2gThreads - 1) / kTsQ2gThreads), (unsigned)nbk), kTsQ2gThreads, 0,
                       ctx->stream>>>(n, c0, K, V2, tau2, Ucur);
       ctx->launches++;
+      if (ctx->stats_on) {
+        ck(cudaEventRecord(qev.second, ctx->stream), "event");
+        ctx->q2_pending.push_back(qev);
+        // each reflector row meets each column twice (dot and update), 8 real flops each;
+        // the reflectors of sweep s cover rows s+1 .. n-1 once: sum n(n-1)/2
+        ctx->q2_flops += (double)nbk * 8.0 * (double)n * (double)(n - 1) * (double)K;
+        ctx->q2_launches++;
+      }
     }
     if (K > 0) {
       blk_prep_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A, off);
@@ -813,19 +833,25 @@ bool use_blocked(const lqm_ctx* ctx, int n, int nR) {
 
 // Reduction of the blocked path: two-stage (dense -> band -> tridiagonal) or the
 // one-stage zlatrd panels; ctx->two_stage when set (lqm_ctx_set_two_stage), else the
-// two-stage form for passes without eigenvectors from kTwoStageDefaultMinN on.  With
-// eigenvectors the stage-2 back-transformation (latency-bound reflector sweeps)
-// costs more than the reduction saves (measured on B200 at n = 1324: rho pass 3.55 s
-// two-stage against 1.90 s one-stage for 576 k-points; eigenvalues only 0.56 s
-// against 0.92 s for 400).  LQM_TWO_STAGE=0/1 in the environment overrides both
-// (development switch for measurements).
+// two-stage form from kTwoStageDefaultMinN on (every order the blocked path serves)
+// for passes that return no eigenvectors: eigenvalue-only passes, and density passes,
+// which back-transform only the columns that carry rho_k.  Passes that return all n
+// eigenvectors keep the one-stage reduction: the stage-2 back-transformation of n
+// columns costs 8 n^3 flops per k-point.  Measured on B200 (576 k-points of the
+// 24 x 24 grid unless noted): eigenvalues only at n = 1324 (400-point path) 0.50 s
+// against 0.92 s; rho passes of 1024 k-points: n = 256 70 ms against 78, n = 400 163
+// against 187; n = 508 177 against 178, n = 868 674 against 693, n = 1324 1.90 s
+// against 1.92 s, n = 2884 (144 k-points) 3.94 s against 4.07 s; all vectors (the
+// Hartree-Fock iteration at n = 2884, 144 k-points): 6.5 s against 5.3 s.
+// LQM_TWO_STAGE=0/1 in the environment overrides both (development switch for
+// measurements).
 constexpr int kTwoStageDefaultMinN = 128;
-bool use_two_stage(const lqm_ctx* ctx, int n, bool vec) {
+bool use_two_stage(const lqm_ctx* ctx, int n, bool all_vectors) {
   if (n <= kTsB + 1) return false;
   const char* env = std::getenv("LQM_TWO_STAGE");
   if (env && (env[0] == '0' || env[0] == '1')) return env[0] == '1';
   if (ctx->two_stage >= 0) return ctx->two_stage == 1;
-  return !vec && n >= kTwoStageDefaultMinN;
+  return !all_vectors && n >= kTwoStageDefaultMinN;
 }
 
 int64_t batch_size_for(int64_t n, int64_t nk, double budget_bytes) {
@@ -1256,6 +1282,9 @@ int lqm_ctx_reset_stats(lqm_ctx* ctx, int enable_timing) {
     ctx->eigh_launches = 0;
     ctx->launches = 0;
     ctx->symv_ms = 0.0;
+    ctx->q2_ms = 0.0;
+    ctx->q2_flops = 0.0;
+    ctx->q2_launches = 0;
     ctx->symv_bytes = 0.0;
     ctx->symv_launches = 0;
   });
@@ -1275,11 +1304,15 @@ int lqm_ctx_phase_cycles(lqm_ctx* ctx, double* cycles) {
 
 int lqm_ctx_kernel_stats(const lqm_ctx* ctx, int kernel_class, double* ms, int64_t* launches,
                          double* algorithmic_bytes) {
-  if (!ctx || kernel_class < 0 || kernel_class > 1) return LQM_EINVAL;
+  if (!ctx || kernel_class < 0 || kernel_class > 2) return LQM_EINVAL;
   if (kernel_class == 0) {
     if (ms) *ms = ctx->eigh_ms;
     if (launches) *launches = ctx->eigh_launches;
     if (algorithmic_bytes) *algorithmic_bytes = 0.0;
+  } else if (kernel_class == 2) {
+    if (ms) *ms = ctx->q2_ms;
+    if (launches) *launches = ctx->q2_launches;
+    if (algorithmic_bytes) *algorithmic_bytes = ctx->q2_flops;  // algorithmic flops for this class
   } else {
     if (ms) *ms = ctx->symv_ms;
     if (launches) *launches = ctx->symv_launches;

@@ -951,10 +951,10 @@ __global__ void __launch_bounds__(kTsQ2gThreads, 1) ts_q2g_kernel(int n, int c0,
         const double2 tj = vs[B * B + i];
         double2 a[4] = {cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0)};
 #pragma unroll
-        for (int r = 0; r < B; ++r) a[r & 3] = cadd(a[r & 3], cmulc(vs[i * B + r], z[i + r]));
+        for (int r = 0; r < B; ++r) a[r & 3] = cfma_conj(a[r & 3], vs[i * B + r], z[i + r]);
         const double2 f = cmul(tj, cadd(cadd(a[0], a[1]), cadd(a[2], a[3])));
 #pragma unroll
-        for (int r = 0; r < B; ++r) z[i + r] = csub(z[i + r], cmul(vs[i * B + r], f));
+        for (int r = 0; r < B; ++r) z[i + r] = cfms(z[i + r], vs[i * B + r], f);
       }
       __syncthreads();  // the buffer is refilled two steps on
       buf ^= 1;

@@ -191,6 +191,29 @@ LQM_FN double2 cmulc(double2 a, double2 b) { return cmk(a.x * b.x + a.y * b.y, a
 LQM_FN double2 cconj(double2 a) { return cmk(a.x, -a.y); }
 LQM_FN double2 cscale(double s, double2 a) { return cmk(s * a.x, s * a.y); }
 // a / b with Smith's scaling
+// acc + conj(a) b, acc + a b and z - a b as four fused multiply-adds each (one rounding per
+// real product-sum instead of a product, a sum and a second rounding)
+LQM_FN double2 cfma_conj(double2 acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(-a.y, b.x, acc.y);
+  return acc;
+}
+LQM_FN double2 cfma(double2 acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+  return acc;
+}
+LQM_FN double2 cfms(double2 z, double2 a, double2 b) {
+  z.x = fma(-a.x, b.x, z.x);
+  z.x = fma(a.y, b.y, z.x);
+  z.y = fma(-a.x, b.y, z.y);
+  z.y = fma(-a.y, b.x, z.y);
+  return z;
+}
 #if defined(__CUDACC__)
 // A complex value from lane `src` of the warp (all 32 lanes must call it).
 LQM_FN double2 shfl_c(double2 v, int src) {

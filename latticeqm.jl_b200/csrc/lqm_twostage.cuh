@@ -236,8 +236,8 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
 #pragma unroll
       for (int k = 0; k < 8; k += 2) {
         const int r0 = 8 * hh + k;
-        if (r0 < L) a0 = cadd(a0, cmulc(v[r0], f[r0]));
-        if (r0 + 1 < L) a1 = cadd(a1, cmulc(v[r0 + 1], f[r0 + 1]));
+        if (r0 < L) a0 = cfma_conj(a0, v[r0], f[r0]);
+        if (r0 + 1 < L) a1 = cfma_conj(a1, v[r0 + 1], f[r0 + 1]);
       }
       const double2 pp = cadd(a0, a1);
       const double2 fl = cmul(ctj, cadd(shfl_c(pp, l), shfl_c(pp, l + 16)));
@@ -245,7 +245,7 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int r = 8 * hh + k;
-          if (r < L) f[r] = csub(f[r], cmul(v[r], fl));
+          if (r < L) f[r] = cfms(f[r], v[r], fl);
         }
       }
 #else
@@ -275,8 +275,8 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
 #pragma unroll
       for (int k = 0; k < 8; k += 2) {
         const int q0 = 8 * hh + k, q1 = q0 + 1;
-        if (r < L && q0 < L) a0 = cadd(a0, cmul((q0 <= r) ? D[r + q0 * LW] : cconj(D[q0 + r * LW]), v[q0]));
-        if (r < L && q1 < L) a1 = cadd(a1, cmul((q1 <= r) ? D[r + q1 * LW] : cconj(D[q1 + r * LW]), v[q1]));
+        if (r < L && q0 < L) a0 = cfma(a0, (q0 <= r) ? D[r + q0 * LW] : cconj(D[q0 + r * LW]), v[q0]);
+        if (r < L && q1 < L) a1 = cfma(a1, (q1 <= r) ? D[r + q1 * LW] : cconj(D[q1 + r * LW]), v[q1]);
       }
       const double2 pp = cadd(a0, a1);
       const double2 yr = cadd(shfl_c(pp, r), shfl_c(pp, r + 16));
@@ -290,7 +290,7 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
         for (int k = 0; k < 8; ++k) {
           const int q = 8 * hh + k;
           if (q <= r) {
-            double2 a = csub(D[r + q * LW], cadd(cmul(wr, cconj(v[q])), cmul(vr, cconj(w[q]))));
+            double2 a = cfms(cfms(D[r + q * LW], wr, cconj(v[q])), vr, cconj(w[q]));
             if (q == r) a.y = 0.0;
             D[r + q * LW] = a;
           }
@@ -300,8 +300,8 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
 #pragma unroll
       for (int k = 0; k < 8; k += 2) {
         const int q0 = 8 * hh + k, q1 = q0 + 1;
-        if (r < L2 && q0 < L) e0 = cadd(e0, cmul(EN[r + q0 * LW], v[q0]));
-        if (r < L2 && q1 < L) e1 = cadd(e1, cmul(EN[r + q1 * LW], v[q1]));
+        if (r < L2 && q0 < L) e0 = cfma(e0, EN[r + q0 * LW], v[q0]);
+        if (r < L2 && q1 < L) e1 = cfma(e1, EN[r + q1 * LW], v[q1]);
       }
       const double2 pe = cadd(e0, e1);
       const double2 z = cmul(tj, cadd(shfl_c(pe, r), shfl_c(pe, r + 16)));
@@ -309,7 +309,7 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int q = 8 * hh + k;
-          if (q < L) EN[r + q * LW] = csub(EN[r + q * LW], cmul(z, cconj(v[q])));
+          if (q < L) EN[r + q * LW] = cfms(EN[r + q * LW], z, cconj(v[q]));
         }
       }
     }

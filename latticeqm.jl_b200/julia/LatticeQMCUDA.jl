@@ -321,7 +321,7 @@ function cuda_autotune_eigh(H, ks::AbstractMatrix{Float64}, exec::CudaExec; want
 end
 
 """Reduction of the blocked eigensolver: 1 two-stage (dense -> band -> tridiagonal),
-0 one-stage panels, -1 the default (two-stage for passes without eigenvectors)."""
+0 one-stage panels, -1 the default (two-stage for bands and density passes)."""
 cuda_set_two_stage(mode::Int, exec::CudaExec) =
     check(context(exec.device), ccall((:lqm_ctx_set_two_stage, LIB[]), Cint, (Ptr{Cvoid}, Cint),
                                       context(exec.device).ptr, mode))

@@ -184,7 +184,8 @@ class Context:
 
     def set_two_stage(self, mode):
         """Reduction of the blocked eigensolver: 1 two-stage (dense -> band -> tridiagonal),
-        0 one-stage panels, -1 (default) by order."""
+        0 one-stage panels, -1 (default): two-stage on the blocked path for passes that
+        return no eigenvectors."""
         self.check(_lib.lqm_ctx_set_two_stage(self._h, int(mode)))
 
     def set_eigh_threads(self, n, nt):
@@ -227,8 +228,9 @@ class Context:
         return nr.value, r.value
 
     def kernel_stats(self, kernel_class):
-        """(device ms, launches, algorithmic bytes) since reset for a kernel class:
-        0 = eigensolver passes, 1 = the blocked path's mat-vec kernel."""
+        """(device ms, launches, algorithmic amount) since reset for a kernel class:
+        0 = eigensolver passes, 1 = the one-stage mat-vec kernel (bytes), 2 = the
+        two-stage path's stage-2 back-transformation (flops)."""
         ms, nl, by = _D(), _I64(), _D()
         self.check(_lib.lqm_ctx_kernel_stats(self._h, int(kernel_class), ctypes.byref(ms), ctypes.byref(nl),
                                              ctypes.byref(by)))
