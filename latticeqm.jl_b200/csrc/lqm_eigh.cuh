@@ -133,11 +133,11 @@ LQM_FN void trailing_pass(const TeamT& T, int mb, double2* A, int lda, int o, co
         if (r < mb) {
           double2 a = Bc[r];
           if (upd) {
-            a = csub(a, cadd(cmul(vr[q], cw), cmul(wr[q], cv)));
+            a = cfms(cfms(a, vr[q], cw), wr[q], cv);
             if (r == c) a.y = 0.0;
             Bc[r] = a;
           }
-          acc[q] = cadd(acc[q], cmul(a, xc));
+          acc[q] = cfma(acc[q], a, xc);
         }
       }
     }
@@ -979,7 +979,7 @@ LQM_FN_NOINLINE void backtransform(const TeamT& T, int n, const double2* R, int 
         for (int r = g; r < m; r += G) {
           const double2 u = Uc[r];
 #pragma unroll
-          for (int i = 0; i < NB; ++i) w[i] = cadd(w[i], cmulc(Vs[r + (int64_t)i * n], u));
+          for (int i = 0; i < NB; ++i) w[i] = cfma_conj(w[i], Vs[r + (int64_t)i * n], u);
         }
       }
 #pragma unroll
@@ -993,14 +993,14 @@ LQM_FN_NOINLINE void backtransform(const TeamT& T, int n, const double2* R, int 
         double2 acc = cmk(0.0, 0.0);
 #pragma unroll
         for (int l = 0; l < NB; ++l)
-          if (l >= i) acc = cadd(acc, cmul(Ts[i + l * NB], w[l]));
+          if (l >= i) acc = cfma(acc, Ts[i + l * NB], w[l]);
         wp[i] = acc;
       }
       if (act) {
         for (int r = g; r < m; r += G) {
           double2 u = Uc[r];
 #pragma unroll
-          for (int i = 0; i < NB; ++i) u = csub(u, cmul(Vs[r + (int64_t)i * n], wp[i]));
+          for (int i = 0; i < NB; ++i) u = cfms(u, Vs[r + (int64_t)i * n], wp[i]);
           Uc[r] = u;
         }
       }
@@ -1056,7 +1056,7 @@ LQM_FN_NOINLINE void rho_from_U(const TeamT& T, int n, const double2* U, int ldu
         for (int q = 0; q < 4; ++q)
           if (q < qn)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[q][b] = cadd(acc[q][b], cmul(ua[q], cb[b]));
+            for (int b = 0; b < 4; ++b) acc[q][b] = cfma(acc[q][b], ua[q], cb[b]);
       }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
