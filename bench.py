@@ -569,6 +569,13 @@ def main():
     Hd = Q.DeviceHops(h, ctx)
     n, nR = Hd.n, Hd.nR
     Lk = np.asfortranarray(np.array(keys, dtype=np.int64).T)
+    # the reduction (one- or two-stage) measured on half of this model's grid before the
+    # warm-up (one GPU; with several, every rank keeps the library's default)
+    reduction = {"choice": "two-stage (library default for density passes)"}
+    if world == 1:
+        best_r, _, table_r = Q.autotune_eigh(Hd, ks_np[:, :288], want_rho=True, ctx=ctx)
+        reduction = {"choice": "two-stage" if best_r == 1 else "one-stage", "autotuned": True,
+                     "pass_ms": {("two-stage" if k == 1 else "one-stage"): v for k, v in table_r.items()}}
     d_rho = torch.zeros(nR, n, n, dtype=torch.complex128, device=dev)
     eb = ctypes.c_double()
 
@@ -732,7 +739,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "k-pts/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded model)",
-                "config": {"workload": WORKLOAD, "k_points_per_gpu_per_step": nk_local,
+                "config": {"workload": WORKLOAD, "k_points_per_gpu_per_step": nk_local, "reduction": reduction,
                            "parallelism": f"dp{world} (k-grid shards in the library; rho_R all-reduce over NCCL)"
                            if world > 1 else "dp1",
                            "l2": "inputs larger than L2 (each step streams ~32 GB of A/U through HBM)",

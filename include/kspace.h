@@ -115,7 +115,11 @@ int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt);
  * rather than throughput).  best_nt/best_ms
  * receive the choice, cand_nt/cand_ms (up to ncand_max, may be NULL) every
  * candidate, *ncand their number.  Block sizes differ in rounding, so a choice is
- * meant to be made once and reused.  No reference counterpart. */
+ * meant to be made once and reused.  For an order on the blocked path the
+ * reduction is tuned instead: candidates 0 (one-stage) and 1 (two-stage), timed the
+ * same way for the sample's pass kind (rho_k when want_rho, else all eigenvectors);
+ * the faster is kept for that order and kind unless lqm_ctx_set_two_stage fixed the
+ * reduction (then LQM_EINVAL).  No reference counterpart. */
 int lqm_autotune_eigh(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int want_rho, int* best_nt,
                       double* best_ms, int64_t ncand_max, int* cand_nt, double* cand_ms, int64_t* ncand);
 /* Milliseconds of device time of the last call's kernels (CUDA events). */

@@ -78,6 +78,8 @@ struct lqm_ctx {
   bool scf_graph_used = false;            // the last SCF replayed a captured iteration
   int64_t blocked_min_n = 0;              // n >= this uses the blocked path (0: the default switch)
   int two_stage = -1;                     // blocked path reduction: 1 two-stage, 0 one-stage, -1 by order
+  // autotuned reduction per (order, pass kind): key 2 n + (pass returns all eigenvectors)
+  std::map<int, int> two_stage_tuned;
   int scf_anderson_depth = 0;             // SCF acceleration: 0 linear mixing, > 0 Anderson history depth
   int scf_residual = 0;                   // SCF residual: 0 relative density change, 1 commutator norm
   bool scf_hartree = true, scf_fock = true;  // HartreeFock(h, v; hartree, fock)
@@ -851,6 +853,8 @@ bool use_two_stage(const lqm_ctx* ctx, int n, bool all_vectors) {
   const char* env = std::getenv("LQM_TWO_STAGE");
   if (env && (env[0] == '0' || env[0] == '1')) return env[0] == '1';
   if (ctx->two_stage >= 0) return ctx->two_stage == 1;
+  const auto tuned = ctx->two_stage_tuned.find(2 * n + (all_vectors ? 1 : 0));
+  if (tuned != ctx->two_stage_tuned.end()) return tuned->second == 1;
   return !all_vectors && n >= kTwoStageDefaultMinN;
 }
 

@@ -757,7 +757,9 @@ def wilson_wannier2d(H, NX, NY=0, bands=(0,), ctx=None):
 def autotune_eigh(H, ks, want_rho=True, ctx=None):
     """Times every candidate block size of the one-CTA eigensolver for H's order on the
     sample k-points ``ks`` (the rho_k pass when ``want_rho``, else eigenvectors) and keeps
-    the fastest on the context (``lqm_autotune_eigh``): (best_nt, best_ms, {nt: ms})."""
+    the fastest on the context (``lqm_autotune_eigh``): (best_nt, best_ms, {nt: ms}).
+    For an order on the blocked path the candidates are the reductions instead, 0
+    (one-stage) and 1 (two-stage), kept for that order and pass kind."""
     ctx = ctx or default_context()
     Hd = _as_device_hops(H, ctx)
     ks = _ks(ks, Hd.d)

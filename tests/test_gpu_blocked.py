@@ -74,6 +74,34 @@ def test_two_stage_models_bands_vectors_rho(lqm, tsctx):
         assert abs(eb - ebref) <= 1e-9 * max(1.0, abs(ebref)), name
 
 
+def test_autotuner_picks_the_reduction_on_the_blocked_path(lqm):
+    """On the blocked path (n = 256) the autotuner times the one- and the two-stage
+    reduction for the sample's pass kind and keeps the faster; the tuned context's rho
+    and eigenvectors still match the oracle."""
+    c = lqm.Context(0, timeout=900)
+    try:
+        _, h = M.honeycomb_disorder(L_super=8)
+        ks = L.regulargrid(16 * 16)
+        for want_rho in (True, False):
+            best, bms, table = lqm.autotune_eigh(h, ks, want_rho=want_rho, ctx=c)
+            assert best in (0, 1) and sorted(table) == [0, 1] and bms == table[best] and bms > 0.0
+        w = np.full(ks.shape[1], 1.0 / ks.shape[1])
+        keys = list(h.keys())
+        rho = {R: None for R in keys}
+        lqm.getdensitymatrix(rho, h, ks, kweights=w, mu=0.0, T=0.01, ctx=c)
+        rref, _ = K.densitymatrix(h, ks, w, 0.0, 0.01, keys)
+        assert max(np.max(np.abs(rho[L_] - rref[L_])) for L_ in keys) <= RHO_TOL
+        b, U = lqm.bandmatrix(h, ks[:, :3], want_vectors=True, ctx=c)
+        for j in range(3):
+            Hk = K.fouriersum(h, ks[:, j])
+            assert np.max(np.abs(Hk @ U[:, :, j] - U[:, :, j] * b[:, j])) < 1e-11
+        c.set_two_stage(1)
+        with pytest.raises(lqm.LQMError):
+            lqm.autotune_eigh(h, ks, ctx=c)
+    finally:
+        c.close()
+
+
 def test_two_stage_matches_one_stage(lqm, bctx, tsctx):
     """The same bands through both reductions of the blocked path, to rounding."""
     _, c1 = M.honeycomb_disorder()
