@@ -76,6 +76,13 @@ int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min);
  * B200 1.8x faster for eigenvalue-only passes at n = 1324 and not slower for rho;
  * passes that return all eigenvectors keep the one-stage form. */
 int lqm_ctx_set_two_stage(lqm_ctx* ctx, int mode);
+/* Device-side wait limit of the bulge chase (the two-stage reduction's stage 2):
+ * the polls of a warp's progress word before a wait gives up (0, the default: about
+ * 2^26 polls, well over a second of waiting).  On expiry the kernel records an error,
+ * every warp stops, and the call returns LQM_EDEVICE at its next wait on the stream;
+ * the context then serves later calls.  A small limit makes the waits run out on
+ * purpose (a test of that path; no fault is involved).  No reference counterpart. */
+int lqm_ctx_set_device_wait_limit(lqm_ctx* ctx, int64_t polls);
 /* SCF acceleration of lqm_scf_hf on this context: 0 (default) linear damped
  * mixing, 1..8 Anderson (Type-II) acceleration with that history depth
  * (src/modules/Meanfield/fixedpoint.jl:39-194,201-231: acceleration=:anderson,

@@ -100,6 +100,7 @@ struct lqm_ctx {
   // wait_stream reads it once such a kernel has been launched since the last check
   int* d_err = nullptr;
   bool err_armed = false;
+  int64_t dev_wait_limit = 0;  // polls before a device-side wait of the bulge chase gives up (0: the default)
   // NCCL communicator of the k-point shards (lqm_ctx_set_comm; lqm_comm.inc)
   void* comm = nullptr;
   int comm_nranks = 1, comm_rank = 0;
@@ -202,7 +203,7 @@ void wait_stream(lqm_ctx* ctx) {
     ck(cudaMemcpy(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost), "error word");
     if (e != 0) {
       ck(cudaMemset(ctx->d_err, 0, sizeof(int)), "error word");
-      fail(LQM_EDEVICE, "a device-side wait gave up (TMA copy not completed within its limit)");
+      fail(LQM_EDEVICE, "a device-side wait gave up (a TMA copy or a bulge-chase dependency not complete within its limit)");
     }
   }
 }
@@ -591,7 +592,8 @@ void launch_eigh_large(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double
       ts_band_kernel<<<nbk, kBlkThreads, 0, ctx->stream>>>(n, A, Bd);
       ck(cudaFuncSetAttribute(ts_chase_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTsChaseSmem),
          "smem attr");
-      ts_chase_kernel<<<nbk, kTsChaseWarps * 32, kTsChaseSmem, ctx->stream>>>(n, Bd, V2, tau2, dd, ee, ctx->d_err);
+      ts_chase_kernel<<<nbk, kTsChaseWarps * 32, kTsChaseSmem, ctx->stream>>>(
+          n, Bd, V2, tau2, dd, ee, ctx->d_err, ctx->dev_wait_limit > 0 ? ctx->dev_wait_limit : kTsWaitPolls);
       ctx->err_armed = true;
       ctx->launches += 2;
     } else {
@@ -1260,6 +1262,12 @@ int lqm_ctx_set_eigh_threads(lqm_ctx* ctx, int64_t n, int nt) {
 int lqm_ctx_set_blocked_min_n(lqm_ctx* ctx, int64_t n_min) {
   if (!ctx || n_min < 0) return LQM_EINVAL;
   ctx->blocked_min_n = n_min;
+  return LQM_OK;
+}
+
+int lqm_ctx_set_device_wait_limit(lqm_ctx* ctx, int64_t polls) {
+  if (!ctx || polls < 0) return LQM_EINVAL;
+  ctx->dev_wait_limit = polls;
   return LQM_OK;
 }
 

@@ -751,15 +751,15 @@ __global__ void __launch_bounds__(kBlkThreads) ts_band_kernel(int n, const doubl
 // finished its tasks 0 .. t + 2 (the tasks whose rows and columns overlap task t's),
 // read from a per-warp progress word in shared memory.  The band stays in global
 // memory (L1/L2): a warp's stores are fenced at block scope before it publishes
-// progress, and a waiting warp fences after it reads it.  Every wait is bounded:
-// on expiry the kernel records an error in *err, every warp stops at its next wait,
-// and d / e are written as zeros.  V2 / tau2 (or null): the reflectors for the
+// progress, and a waiting warp fences after it reads it.  Every wait is bounded
+// (wait_polls polls of the progress word): on expiry the kernel records an error in
+// *err, every warp stops at its next wait, and d / e are written as zeros.  V2 / tau2 (or null): the reflectors for the
 // back-transformation.  Outputs: d (n) and e (n - 1) of the real tridiagonal.
 constexpr int kTsWin = 3 * kTsB * (kTsB + 1) + 2 * kTsB;  // complex per warp window
 constexpr int kTsChaseSmem = kTsChaseWarps * kTsWin * 16;
 __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, double2* Bd, double2* V2,
                                                                       double2* tau2, double* d, double* e,
-                                                                      int* err) {
+                                                                      int* err, long long wait_polls) {
   extern __shared__ __align__(16) double2 tswin[];
   __shared__ long long prog[kTsChaseWarps];
   __shared__ int stop;
@@ -784,10 +784,10 @@ __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, dou
       const long long need = (long long)(s - 1) * unit + (t + 3 < ntp ? t + 3 : ntp);
       bool good = true;
       if (lane == 0) {
-        int polls = 0;
+        long long polls = 0;
         while (vprog[wp] < need) {
           if (*vstop) { good = false; break; }
-          if (++polls > kTsWaitPolls) {
+          if (++polls > wait_polls) {
             *vstop = 1;
             if (err) atomicExch(err, 2);
             good = false;

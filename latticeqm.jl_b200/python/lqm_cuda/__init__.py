@@ -35,7 +35,7 @@ STATUS_NAMES = {-1: "LQM_EINVAL", -2: "LQM_ECUDA", -3: "LQM_ENOMEM", -4: "LQM_ET
 
 EXPORTS = [
     "lqm_ctx_create", "lqm_ctx_destroy", "lqm_last_error", "lqm_ctx_set_timeout", "lqm_ctx_set_blocked_min_n",
-    "lqm_ctx_set_two_stage",
+    "lqm_ctx_set_two_stage", "lqm_ctx_set_device_wait_limit",
     "lqm_ctx_last_kernel_ms", "lqm_hops_upload_dense", "lqm_hops_upload_csc", "lqm_hops_free",
     "lqm_hops_dims", "lqm_bloch", "lqm_bloch_dev", "lqm_bandmatrix", "lqm_bandmatrix_dev",
     "lqm_densitymatrix", "lqm_densitymatrix_dev", "lqm_chemicalpotential",
@@ -74,6 +74,7 @@ _SIG = {
     "lqm_ctx_set_timeout": [_P, _D],
     "lqm_ctx_set_blocked_min_n": [_P, _I64],
     "lqm_ctx_set_two_stage": [_P, ctypes.c_int],
+    "lqm_ctx_set_device_wait_limit": [_P, _I64],
     "lqm_ctx_kernel_stats": [_P, ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_D)],
     "lqm_comm_unique_id": [_P],
     "lqm_ctx_set_comm": [_P, ctypes.c_int, ctypes.c_int, _P],
@@ -187,6 +188,10 @@ class Context:
         0 one-stage panels, -1 (default): two-stage on the blocked path for passes that
         return no eigenvectors."""
         self.check(_lib.lqm_ctx_set_two_stage(self._h, int(mode)))
+
+    def set_device_wait_limit(self, polls):
+        """Polls before a device-side wait of the bulge chase gives up (0: the default)."""
+        self.check(_lib.lqm_ctx_set_device_wait_limit(self._h, int(polls)))
 
     def set_eigh_threads(self, n, nt):
         """Block size of the one-CTA eigensolver for order n (0: the built-in rule)."""

@@ -102,6 +102,27 @@ def test_autotuner_picks_the_reduction_on_the_blocked_path(lqm):
         c.close()
 
 
+def test_chase_bounded_wait_expiry_reports_and_recovers(lqm):
+    """The bulge chase's inter-warp waits are bounded: with a limit of one poll the
+    waits of the second and later sweeps run out at once (the sweep before them has not
+    finished its first tasks), the kernel records the failure and stops, and the call
+    returns LQM_EDEVICE; with the default limit the same context then gives the
+    oracle's bands.  No fault is involved."""
+    c = lqm.Context(0, timeout=600)
+    try:
+        _, h = M.honeycomb_disorder(L_super=8)  # n = 256: the blocked path, two-stage for bands
+        ks = L.regulargrid(4 * 4)
+        c.set_device_wait_limit(1)
+        with pytest.raises(lqm.LQMError) as ei:
+            lqm.bandmatrix(h, ks, ctx=c)
+        assert ei.value.status == -6, ei.value
+        c.set_device_wait_limit(0)
+        b, _ = lqm.bandmatrix(h, ks, ctx=c)
+        assert rel_band_err(b, K.bandmatrix(h, ks)[0]) <= BAND_TOL
+    finally:
+        c.close()
+
+
 def test_two_stage_matches_one_stage(lqm, bctx, tsctx):
     """The same bands through both reductions of the blocked path, to rounding."""
     _, c1 = M.honeycomb_disorder()
