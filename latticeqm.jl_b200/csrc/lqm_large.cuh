@@ -718,8 +718,6 @@ __global__ void __launch_bounds__(kBlkThreads) blk_add_identity_kernel(int n, do
 constexpr int kTsB = 16;              // half-bandwidth of the stage-1 band
 constexpr int kTsPanelThreads = 512;  // panel QR: latency-bound row passes, CTA per k-point
 constexpr int kTsChaseWarps = 8;      // bulge chase: sweeps in flight per k-point (one warp each)
-constexpr int kTsQ2Threads = 256;
-constexpr int kTsQ2MaxCols = 8;       // columns of Z per CTA in the Q2 back-transformation
 constexpr int kTsWaitPolls = 1 << 26; // bound of one inter-warp wait of the chase (shared-memory polls, ~1 s)
 
 // complex per k-point of the stage-2 reflector store (sweeps 0..n-2, tmax slots of kTsB each)
@@ -815,83 +813,6 @@ __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, dou
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     d[b * n + i] = fin ? Bk[(int64_t)i * ldb].x : 0.0;
     e[b * n + i] = (fin && i + 1 < n) ? Bk[1 + (int64_t)i * ldb].x : 0.0;
-  }
-}
-
-// grid (ceil(K / cols), B): Z <- Q2 Z on columns c0 .. c0+K-1 of U (n x n per
-// k-point).  A CTA holds `cols` columns of Z in shared memory (leading dimension
-// ts_q2_ld(n), odd in 16-byte units so that the columns of one task fall on distinct
-// banks) and applies the sweeps in reverse order; the reflectors of one sweep act on
-// disjoint rows, so each (task, column) pair is one thread's and a barrier separates
-// the sweeps.  The next sweep's reflectors and taus (contiguous in the store) are
-// copied into a second shared buffer by cp.async while a sweep is applied.  A pair's
-// dot product runs on four partial sums.
-__host__ __device__ inline int ts_q2_ld(int n) { return n | 1; }
-__host__ __device__ inline int ts_q2_vstage(int n) { return ts_tmax(n, kTsB) * (kTsB + 1); }
-__host__ __device__ inline int ts_q2_smem(int n, int cols) {
-  return 16 * (ts_q2_ld(n) * cols + 2 * ts_q2_vstage(n));
-}
-__global__ void __launch_bounds__(kTsQ2Threads) ts_q2_kernel(int n, int c0, int K, int cols, const double2* V2,
-                                                             const double2* tau2, double2* U) {
-  extern __shared__ __align__(16) double2 zs[];
-  const int64_t b = blockIdx.y;
-  const int cb = blockIdx.x * cols;
-  const int nc = (K - cb < cols) ? K - cb : cols;
-  if (nc <= 0) return;
-  const int ld = ts_q2_ld(n);
-  const int tmax = ts_tmax(n, kTsB);
-  const int vst = ts_q2_vstage(n);
-  double2* vb = zs + (int64_t)ld * cols;  // two stages of (tmax x kTsB reflectors, tmax taus)
-  double2* Uk = U + b * (int64_t)n * n + (int64_t)(c0 + cb) * n;
-  const double2* Vk = V2 + b * ts_v2_stride(n);
-  const double2* tk = tau2 + b * ts_tau2_stride(n);
-  auto stage = [&](int s, double2* dst) {
-    const int nt = ts_tasks(n, kTsB, s);
-    const double2* src = Vk + (int64_t)s * tmax * kTsB;
-    for (int i = threadIdx.x; i < nt * kTsB; i += blockDim.x) cp_async16(dst + i, src + i, true);
-    const double2* ts = tk + (int64_t)s * tmax;
-    for (int i = threadIdx.x; i < nt; i += blockDim.x) cp_async16(dst + tmax * kTsB + i, ts + i, true);
-  };
-  if (n >= 2) stage(n - 2, vb);
-  cp_async_commit();
-  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) {
-    const int r = (int)(i % n), c = (int)(i / n);
-    zs[r + (int64_t)c * ld] = Uk[i];
-  }
-  for (int s = n - 2; s >= 0; --s) {
-    const double2* buf = vb + ((n - 2 - s) & 1) * vst;
-    if (s > 0) stage(s - 1, vb + ((n - 1 - s) & 1) * vst);
-    cp_async_commit();
-    cp_async_wait_keep1();  // sweep s's copies have landed
-    __syncthreads();
-    const int nt = ts_tasks(n, kTsB, s);
-    for (int p = threadIdx.x; p < nt * nc; p += blockDim.x) {
-      const int t = p / nc, c = p - t * nc;
-      const int R0 = (t == 0) ? s + 1 : s + 1 + t * kTsB;
-      const int L = (n - R0 < kTsB) ? n - R0 : kTsB;
-      const double2* v = buf + t * kTsB;
-      const double2 tj = buf[tmax * kTsB + t];
-      double2* z = zs + (int64_t)c * ld + R0;
-      double2 vr[kTsB], zr[kTsB];
-      double2 acc[4] = {cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0)};
-#pragma unroll
-      for (int r = 0; r < kTsB; ++r) {
-        vr[r] = v[r];  // zero-padded past L
-        zr[r] = (r < L) ? z[r] : cmk(0.0, 0.0);
-      }
-#pragma unroll
-      for (int r = 0; r < kTsB; ++r) acc[r & 3] = cadd(acc[r & 3], cmulc(vr[r], zr[r]));
-      const double2 f = cmul(tj, cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])));
-#pragma unroll
-      for (int r = 0; r < kTsB; ++r)
-        if (r < L) z[r] = csub(zr[r], cmul(vr[r], f));
-    }
-    __syncthreads();  // the buffer of sweep s is free for sweep s - 2
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  for (int64_t i = threadIdx.x; i < (int64_t)n * nc; i += blockDim.x) {
-    const int r = (int)(i % n), c = (int)(i / n);
-    Uk[i] = zs[r + (int64_t)c * ld];
   }
 }
 
