@@ -315,3 +315,20 @@ def test_emulated_two_stage_hard_hermitian(emul, name, Hk):
         assert np.max(np.abs(ev - ref)) <= 1e-12 * scale, b
         assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12, b
         assert np.max(np.abs(Hk @ U - U * ev)) <= 1e-12 * scale, b
+
+
+@pytest.mark.parametrize("n", [3, 17, 18, 31, 33, 47, 65])
+def test_emulated_two_stage_edge_orders(emul, n):
+    """Orders around the half-bandwidth and its multiples (a last panel of 1 or b - 1
+    rows, tasks cut at the matrix edge), dense random Hermitian H, both Q2 orders."""
+    rng = np.random.default_rng(100 + n)
+    A = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    Hk = (A + A.conj().T) / 2
+    ref = K.eigh_upper(Hk, vectors=False)
+    scale = max(ref[-1] - ref[0], 1.0)
+    for b in (4, 16, -4, -16):
+        ev, U, tri = _run_two_stage(emul, {(0, 0): Hk}, (0.0, 0.0), b)
+        assert tri[2 * n] == 0.0, b
+        assert np.max(np.abs(ev - ref)) / scale <= 1e-12, b
+        assert np.max(np.abs(U.conj().T @ U - np.eye(n))) <= 1e-12, b
+        assert np.max(np.abs(Hk @ U - U * ev)) / scale <= 1e-12, b
