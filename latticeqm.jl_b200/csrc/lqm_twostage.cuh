@@ -16,8 +16,10 @@
 //     is removed; the rest lies in the columns the next sweep annihilates, so the
 //     band never grows beyond 2b - 1 subdiagonals.  Successive sweeps can run
 //     concurrently when sweep s+1 stays three tasks behind sweep s.
-//   back-transformation U = Q1 Q2 Z: the stage-2 reflectors sweep by sweep (the
-//     reflectors of one sweep act on disjoint rows), then Q1 as compact-WY
+//   back-transformation U = Q1 Q2 Z: the stage-2 reflectors in the reverse order of
+//     the chase (ts_q2_apply_host) or, as the device applies them, grouped by 16
+//     sweeps and task index (ts_q2_apply_grouped_host: the same product, since the
+//     reorder only exchanges reflectors on disjoint rows), then Q1 as compact-WY
 //     products (blk_larft and the GEMMs of the one-stage path, rows offset by b).
 //
 // The reference reaches the same factorisation through Julia's LinearAlgebra
@@ -364,8 +366,8 @@ LQM_FN bool ts_chase_sweep(const TeamT& T, int n, int s, double2* Bd, double2* v
 }
 
 // Applies H = I - tau v v^H of every stage-2 task to the rows of Z (n x nc, leading
-// dimension ldz), in the reverse order of the chase (Z <- Q2 Z).  Host emulation
-// form: the kernel applies one sweep's reflectors in parallel.
+// dimension ldz), in the reverse order of the chase (Z <- Q2 Z): the defining order,
+// against which the emulation checks the grouped order of the device kernel.
 // V2: reflectors of sweep s, task t at V2 + (s * tmax + t) * B; tau2 at s * tmax + t.
 template <int B>
 LQM_FN void ts_q2_apply_host(int n, const double2* V2, const double2* tau2, double2* Z, int ldz, int nc) {
