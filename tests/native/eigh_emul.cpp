@@ -7,6 +7,10 @@
 #include <algorithm>
 #include <cstring>
 #include <vector>
+#include <atomic>
+#include <chrono>
+#include <random>
+#include <thread>
 
 #include "lqm_blocked.cuh"
 #include "lqm_twostage.cuh"
@@ -400,6 +404,68 @@ extern "C" int lqm_emul_eigh_twostage(int n, int nR, int dim, const double* bloc
   if (grouped) b = -b;
   if (b == 4) return emul_twostage<4>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri, grouped);
   if (b == 16) return emul_twostage<16>(n, nR, dim, blocks, keys, kpt, want_vectors, evals, U, tri, grouped);
+  return -1;
+}
+
+// The bulge chase of a band (ldb = 2B, n x ldb complex, lower band storage) run
+// twice: sweep after sweep, and on `workers` threads with the device kernel's
+// protocol (worker w takes sweeps w, w + workers, ...; before task t of sweep s it
+// waits until sweep s - 1 has finished its tasks 0 .. t + 2, read from the previous
+// worker's progress word with acquire / release ordering), with random pauses after
+// tasks to vary the interleaving.  Returns 1 when the band, the reflectors and the
+// taus of the two runs are bitwise equal, 0 when they differ.
+template <int B>
+static int emul_chase_schedules(int n, const double* band, int workers, unsigned seed) {
+  const Team T = make_host_team();
+  const int ldb = 2 * B, tmax = ts_tmax(n, B);
+  const size_t nb = (size_t)ldb * n, nv = (size_t)std::max(n - 1, 1) * tmax;
+  std::vector<double2> B1(nb), B2(nb), V1(nv * B), V2(nv * B), t1(nv), t2(nv);
+  std::memcpy(B1.data(), band, nb * sizeof(double2));
+  std::memcpy(B2.data(), band, nb * sizeof(double2));
+  std::vector<double2> win(3 * B * (B + 1) + 2 * B);
+  for (int s = 0; s <= n - 2; ++s)
+    ts_chase_sweep<B>(T, n, s, B1.data(), V1.data() + (size_t)s * tmax * B, t1.data() + (size_t)s * tmax, win.data(),
+                      [](int) { return true; }, [](int) {});
+  const long long unit = tmax + 1;
+  std::vector<std::atomic<long long>> prog(workers);
+  for (auto& p : prog) p.store(-1);
+  std::vector<std::thread> th;
+  for (int w = 0; w < workers; ++w)
+    th.emplace_back([&, w] {
+      std::mt19937 rng(seed * 7919u + (unsigned)w);
+      std::vector<double2> wwin(3 * B * (B + 1) + 2 * B);
+      const int wp = (w + workers - 1) % workers;
+      for (int s = w; s <= n - 2; s += workers) {
+        const int ntp = (s > 0) ? ts_tasks(n, B, s - 1) : 0;
+        auto wait = [&](int t) {
+          if (s == 0) return true;
+          const long long need = (long long)(s - 1) * unit + (t + 3 < ntp ? t + 3 : ntp);
+          while (prog[wp].load(std::memory_order_acquire) < need) std::this_thread::yield();
+          return true;
+        };
+        auto done = [&](int t) {
+          prog[w].store((long long)s * unit + t + 1, std::memory_order_release);
+          if (rng() % 16 == 0) std::this_thread::sleep_for(std::chrono::microseconds(rng() % 50));
+        };
+        ts_chase_sweep<B>(T, n, s, B2.data(), V2.data() + (size_t)s * tmax * B, t2.data() + (size_t)s * tmax,
+                          wwin.data(), wait, done);
+      }
+    });
+  for (auto& t : th) t.join();
+  // slots of tasks that do not exist are never written by either run: compare the written ones
+  bool same = std::memcmp(B1.data(), B2.data(), nb * sizeof(double2)) == 0;
+  for (int s = 0; s <= n - 2 && same; ++s)
+    for (int t = 0; t < ts_tasks(n, B, s) && same; ++t) {
+      const size_t q = (size_t)s * tmax + t;
+      same = std::memcmp(&V1[q * B], &V2[q * B], B * sizeof(double2)) == 0 &&
+             std::memcmp(&t1[q], &t2[q], sizeof(double2)) == 0;
+    }
+  return same ? 1 : 0;
+}
+
+extern "C" int lqm_emul_chase_schedules(int n, int b, const double* band, int workers, unsigned seed) {
+  if (b == 4) return emul_chase_schedules<4>(n, band, workers, seed);
+  if (b == 16) return emul_chase_schedules<16>(n, band, workers, seed);
   return -1;
 }
 
