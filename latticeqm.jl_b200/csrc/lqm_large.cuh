@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(kSymvTmaThreads, 1)
     int R, C;
     symv_tile_rc((int)(it - b * ntiles), &R, &C);
     // the stage's copies have landed, and every thread is past the previous tile (so
-    // its stage may be refilled and its partials read); the verdict of the bounded
+    // its stage may be refilled and its partials read); the outcome of the bounded
     // wait is the block's
     const int ok = __syncthreads_and(mbar_wait_bounded(bars + 8 * stage, parity) ? 1 : 0);
     if (!ok) {
