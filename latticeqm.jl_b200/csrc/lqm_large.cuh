@@ -117,6 +117,9 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool va
   const int nbytes = valid ? 16 : 0;  // 0: the 16 bytes are zero-filled, nothing is read
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(nbytes) : "memory");
 }
+// a hint: the 128-byte line holding *p into L1 (and L2), no register written; callers
+// pass only addresses inside their own buffers
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.L1 [%0];\n" ::"l"(p)); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_keep1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
@@ -822,8 +825,19 @@ __global__ void __launch_bounds__(kTsChaseWarps * 32) ts_chase_kernel(int n, dou
 // rows of the thread's column, held in registers (all indices compile-time); the
 // window slides by 16 rows per step, so a group streams the column once.  The
 // step's reflectors and taus (16 x 16 + 16 complex; zeros where a sweep has no
-// task t) are copied into shared memory by cp.async one step ahead.
+// task t) are copied into shared memory by cp.async one step ahead, and the 16 rows
+// of the next slide are prefetched into L1.  A reflector's dot product runs in two
+// partial sums: with four the prefetch addresses no longer fit the 255 registers
+// (spills), and two with the prefetch measured 5% faster than four without it.
 constexpr int kTsQ2gThreads = 256;
+// rows r0 .. r0 + kTsB - 1 (those below n) of column c: 256 bytes, at most three lines,
+// requested one step before the slide that loads them, so that they arrive while the
+// step's reflectors are applied
+__device__ __forceinline__ void prefetch_rows(const double2* c, int r0, int n) {
+  if (r0 < n) prefetch_l1(c + r0);
+  if (r0 + 8 < n) prefetch_l1(c + r0 + 8);
+  if (r0 + kTsB - 1 < n) prefetch_l1(c + r0 + kTsB - 1);
+}
 constexpr int kTsQ2gStep = kTsB * kTsB + kTsB;  // complex per staged step
 __global__ void __launch_bounds__(kTsQ2gThreads, 1) ts_q2g_kernel(int n, int c0, int K, const double2* V2,
                                                                   const double2* tau2, double2* U) {
@@ -870,10 +884,10 @@ __global__ void __launch_bounds__(kTsQ2gThreads, 1) ts_q2g_kernel(int n, int c0,
 #pragma unroll
       for (int i = B - 1; i >= 0; --i) {
         const double2 tj = vs[B * B + i];
-        double2 a[4] = {cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0), cmk(0.0, 0.0)};
+        double2 a[2] = {cmk(0.0, 0.0), cmk(0.0, 0.0)};
 #pragma unroll
-        for (int r = 0; r < B; ++r) a[r & 3] = cfma_conj(a[r & 3], vs[i * B + r], z[i + r]);
-        const double2 f = cmul(tj, cadd(cadd(a[0], a[1]), cadd(a[2], a[3])));
+        for (int r = 0; r < B; ++r) a[r & 1] = cfma_conj(a[r & 1], vs[i * B + r], z[i + r]);
+        const double2 f = cmul(tj, cadd(a[0], a[1]));
 #pragma unroll
         for (int r = 0; r < B; ++r) z[i + r] = cfms(z[i + r], vs[i * B + r], f);
       }
@@ -888,6 +902,7 @@ __global__ void __launch_bounds__(kTsQ2gThreads, 1) ts_q2g_kernel(int n, int c0,
         for (int j = 0; j < W - B; ++j) z[j] = z[j + B];
 #pragma unroll
         for (int j = W - B; j < W; ++j) z[j] = (act && wt + B + j < n) ? Uc[wt + B + j] : cmk(0.0, 0.0);
+        if (act && t + 2 < nt) prefetch_rows(Uc, wt + B + W, n);  // the next step's slide
       } else {
 #pragma unroll
         for (int j = 0; j < W; ++j)
