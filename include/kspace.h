@@ -223,7 +223,9 @@ int lqm_bloch_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_k
 /* Bands (and optionally eigenvectors) on a k list, replaces `bandmatrix`
  * without projectors (src/modules/Spectrum/bands.jl:164-227; per-k eigen of
  * `Hermitian(H(k))`, upper triangle, src/modules/Eigen/Eigen.jl:22-23,32).
- * bands: n x nk ascending per column; U: n x n x nk (may be NULL). */
+ * bands: n x nk ascending per column; U: n x n x nk (may be NULL).
+ * `precision` (here and in the eigen-pass entry points below): 0 = FP64, the only
+ * form built; any other value returns LQM_EINVAL. */
 int lqm_bandmatrix(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* ks, int want_vectors,
                    int precision, double* bands, double* U);
 int lqm_bandmatrix_dev(lqm_ctx* ctx, const lqm_hops* H, int64_t nk, const double* d_ks, int want_vectors,
